@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""P(D)+logL evaluations per second on one B200 (or N, weak scaling).
+
+Workload: the 1D batched configuration -- a 10-knot spline model over
+1-800 mJy, three beam sets (Gaussian FWHM 3.0 / 4.2 / 6.0 px at 6", 150-bin
+beam histograms) with one map each (2000x2000 at 2.0 mJy, 1200x900 at
+3.1 mJy, 600x600 at 5.0 mJy noise; seeded synthetic, mean-subtracted, 1000
+data bins), FFT size n = 65536, 2048 R interpolation nodes.  A step is one
+launch sequence evaluating the full likelihood (all beam sets and datasets)
+for a batch of 128 proposals (128 walkers); each rank evaluates its own
+batch (weak scaling, no data-path collective).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+    python bench.py --impl reference ...   # the CPU path on host cores
+
+Prints one JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BATCH = 128
+METRIC = "P(D)+logL evals/s"
+WORKLOAD = ("1D batched plain method: 10-knot spline 1-800 mJy, 3 beam sets "
+            "(FWHM 3.0/4.2/6.0 px, 150-bin beam histograms), maps 2000x2000 "
+            "@2.0 mJy, 1200x900 @3.1 mJy, 600x600 @5.0 mJy, n=65536, "
+            "ninterp=2048, 1000 data bins, 128 proposals per launch")
+
+
+def args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cpu-seconds", type=float, default=12.0,
+                   help="CPU-baseline sample length")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx = [], []
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------- CPU baseline
+def cpu_baseline(cfg, seconds, nthreads=None):
+    """The oracle port of the reference path (calcLike::getLogLike per
+    proposal) on the host cores, thread farm over proposals."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from pofd_affine_b200 import synth
+    nthreads = nthreads or os.cpu_count() or 1
+    O = pyoracle.Like1(cfg["knotpos"], cfg["fftsize"], cfg["ninterp"], True,
+                       cfg["nbins"])
+    for b in cfg["beams"]:
+        O.add_beamset(b, cfg["pixsize"], 1e-5, True, cfg["nbeamhist"])
+    for m, bi, s in zip(cfg["maps"], cfg["map_beam"], cfg["sigmas"]):
+        O.add_dataset(bi, m, s)
+    O.set_rranges(cfg["theta0"])
+    th = synth.proposals(cfg["theta0"], 4 * nthreads, 0.02, rng=99)
+    O.loglike_batch(th[:nthreads], nthreads)  # builds the thread copies
+    done, t0 = 0, time.perf_counter()
+    while True:
+        O.loglike_batch(th, nthreads)
+        done += th.shape[0]
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": done / el, "unit": "evals/s", "cores": nthreads,
+            "kind": "port",
+            "sample": "%d proposals of the workload in %.1f s on %d threads "
+                      "(oracle restatement of the reference CPU path; the "
+                      "reference needs GSL/FFTW/cfitsio/HDF5/MPI, absent "
+                      "here)" % (done, el, nthreads)}
+
+
+def reference_arm(a, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cpu = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from pofd_affine_b200 import synth
+    O = pyoracle.Like1(cfg["knotpos"], cfg["fftsize"], cfg["ninterp"], True,
+                       cfg["nbins"])
+    for b in cfg["beams"]:
+        O.add_beamset(b, cfg["pixsize"], 1e-5, True, cfg["nbeamhist"])
+    for m, bi, s in zip(cfg["maps"], cfg["map_beam"], cfg["sigmas"]):
+        O.add_dataset(bi, m, s)
+    O.set_rranges(cfg["theta0"])
+    per_step = 2 * cpu  # bounded sample per step
+    th = synth.proposals(cfg["theta0"], per_step, 0.02, rng=99)
+    for _ in range(a.warmup):
+        O.loglike_batch(th, cpu)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        O.loglike_batch(th, cpu)
+    el = time.perf_counter() - t0
+    v = per_step * a.steps / el
+    line = {"metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": 0,
+            "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * el / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD,
+                       "proposals_per_step": per_step},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": cpu,
+                             "kind": "port",
+                             "sample": "%d proposals per step, %d steps, %d "
+                                       "threads (oracle restatement of the "
+                                       "reference CPU path)"
+                                       % (per_step, a.steps, cpu)},
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- roofline
+def stage_bytes(stage, P, B, D, n):
+    """Algorithmic HBM bytes per launch of an HBM-bound stage (one
+    compulsory FP64 read/write of each array it streams)."""
+    nc = n // 2 + 1
+    return {
+        "k_rfill1": 8.0 * n * P * B,                         # write R
+        "k_spectrum1": 16.0 * nc * P * B + 16.0 * nc * P * D,  # read R~, write per-dataset spectra
+        "k_pscan1": 8.0 * n * P * D,                          # read P(D)
+        "cufft_d2z": 8.0 * n * P * B + 16.0 * nc * P * B,
+        "cufft_z2d": 16.0 * nc * P * D + 8.0 * n * P * D,
+    }.get(stage)
+
+
+def read_traffic(stage):
+    """dram bytes per launch of a kernel from the committed ncu summary
+    (profiles/<kernel>_1d_batched.md, line 'traffic_bytes_per_launch: N')."""
+    path = os.path.join(ROOT, "profiles", "%s_1d_batched.md" % stage)
+    try:
+        for line in open(path):
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1].split()[0])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def main():
+    a = args()
+    from pofd_affine_b200 import synth
+    cfg = synth.config_1d_batched(seed=2)
+    if a.impl == "reference":
+        reference_arm(a, cfg)
+        return
+
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+    from pofd_affine_b200 import Context, build
+    build.build()
+    from pofd_affine_b200._lib import lib
+    import ctypes as C
+
+    ctx = Context(local)
+    L = synth.build_like1(cfg, ctx)
+    L.reserve(BATCH)
+    npar = cfg["theta0"].size
+    nbatches = 4  # distinct resident proposal batches, cycled
+    host = [synth.proposals(cfg["theta0"], BATCH, 0.02, rng=100 * rank + k)
+            for k in range(nbatches)]
+    dth = [torch.from_numpy(h).cuda() for h in host]
+    dll = [torch.empty(BATCH, dtype=torch.float64, device="cuda")
+           for _ in range(nbatches)]
+    dst = [torch.empty(BATCH, dtype=torch.int32, device="cuda")
+           for _ in range(nbatches)]
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def step(k):
+        j = k % nbatches
+        L.getLogLikeDevice(BATCH, dth[j].data_ptr(), npar, dll[j].data_ptr(),
+                           dst[j].data_ptr(), sptr)
+
+    # correctness gate: device path equals the host path, all statuses ok
+    ref_ll, ref_st = L.getLogLikeBatch(host[0])
+    step(0)
+    torch.cuda.synchronize()
+    assert np.all(ref_st == 0), ref_st
+    assert np.array_equal(dll[0].cpu().numpy(), ref_ll)
+
+    for k in range(max(a.warmup, 3)):
+        step(k)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(a.steps):
+        step(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * BATCH * a.steps / (ms * 1e-3)
+
+    # end to end through the public API with host buffers
+    L.getLogLikeBatch(host[1])
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(a.steps):
+        L.getLogLikeBatch(host[k % nbatches])
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * BATCH * a.steps / e2e_s
+
+    # per-stage device times of the same launch sequence (CUDA events)
+    stages = L.profileStages(host[0], reps=5)
+    own = {k: v for k, v in stages.items() if k.startswith("k_")}
+    dom = max(own, key=own.get)
+    B, D, n = 3, 3, cfg["fftsize"]
+    hb = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = hb.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in hb else "fallback"
+    nbytes = stage_bytes(dom, BATCH, B, D, n)
+    if nbytes is not None:
+        ach = nbytes / (own[dom] * 1e-3) / 1e9
+        traffic = read_traffic(dom)
+        roof = {"bound": "hbm", "kernel": dom, "achieved": ach,
+                "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                "traffic": traffic, "algorithmic_bytes": nbytes,
+                "ms_per_launch": own[dom], "peak_source": peak_src}
+    else:
+        # FP64-bound R builder: FP64 flops of the R terms against the
+        # measured FP64 FMA peak
+        pk = C.c_double()
+        lib().pofd_fp64_peak(local, C.byref(pk))
+        roof = {"bound": "fp64", "kernel": dom, "ms_per_launch": own[dom],
+                "peak": pk.value, "unit": "TFLOP/s",
+                "peak_source": "measured (pofd_fp64_peak DFMA loop)",
+                "achieved": None, "frac": None,
+                "traffic": read_traffic(dom)}
+    hbm_pipe = sum(stage_bytes(s, BATCH, B, D, n) or 0 for s in stages)
+    nk = L.kernelsPerEval()
+
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu_baseline and world == 1:
+            cpu = cpu_baseline(cfg, a.cpu_seconds)
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded maps of the workload's shapes)",
+            "config": {"workload": WORKLOAD, "proposals_per_step": BATCH,
+                       "fftsize": n, "beam_sets": B, "datasets": D,
+                       "l2": "working set per step ~400 MB > 126 MB L2 "
+                             "(no flush needed)"},
+            "e2e": {"value": e2e, "unit": "evals/s",
+                    "h2d_bytes_per_step": BATCH * npar * 4,
+                    "d2h_bytes_per_step": BATCH * (8 + 4)},
+            "roofline": roof,
+            "stage_ms": stages,
+            "pipeline_hbm_bytes_per_step": hbm_pipe,
+            "gpu_launches": nk * a.steps,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,186 @@
+/*
+ * pofd_b200.h -- C ABI of the B200 P(D) likelihood library (libpofd_b200.so).
+ *
+ * Drop-in boundary for the likelihood hot path of aconley/pofd_affine 0.5.1:
+ * number counts -> R(x) -> FFT -> exp(R~(w) - R~(0)) * noise -> inverse FFT
+ * -> unwrap / normalise / log -> binned log-likelihood, computed in FP64 by
+ * hand-written sm_100a kernels with batched cuFFT as the only library call.
+ *
+ * Plain C types only (pointers, sizes, doubles, floats); no CUDA or torch
+ * types appear in the signatures -- streams are passed as void*
+ * (a cudaStream_t).  Every function returns an int status:
+ *     0   POFD_OK
+ *     1   POFD_REJECTED    parameters rejected (the reference's
+ *                          pars_invalid; it never sets it in 0.5.1)
+ *    <0   an error; pofd_last_error() returns the message (thread-local).
+ * The negative codes name the exception the reference would have thrown
+ * (affineExcept) at the same point.  Model parameters are float, as in the
+ * reference's paramSet (include/paramSet.h:20), and are widened to double
+ * exactly as numberCountsKnots::setParams does (numberCountsKnots.cc:265).
+ *
+ * Objects are not thread-safe (like the reference's PDFactory, which keeps
+ * mutable buffers, calcLike.h:47-48): use one object per host thread.
+ */
+#ifndef POFD_B200_H
+#define POFD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define POFD_OK 0
+#define POFD_REJECTED 1
+#define POFD_E_INVALID_MODEL (-1) /* "Invalid model" (PDFactory.cc:1050) */
+#define POFD_E_SPLIT_RANGE (-2)   /* "Not enough flux range" (PDFactory.cc:770) */
+#define POFD_E_SPLIT_PEAK (-3)    /* "Peak P(D) value was zero" (PDFactory.cc:787) */
+#define POFD_E_SPLIT_MIN (-4)     /* "Minimum in pd is too large" (PDFactory.cc:818) */
+#define POFD_E_SPLIT_LOGIC (-5)   /* botidx/topidx logic errors (PDFactory.cc:797-802, 873) */
+#define POFD_E_SPLIT_TOP (-6)     /* "Topidx is already below jitter" (PDFactory.cc:886) */
+#define POFD_E_SPLIT_NONE (-7)    /* "Unable to find split point" (PDFactory.cc:905) */
+#define POFD_E_UNSHIFT (-8)       /* "Un-shift amounts not finite" (PDFactory.cc:996) */
+#define POFD_E_ARG (-10)          /* invalid argument / state */
+#define POFD_E_CUDA (-11)         /* CUDA or cuFFT failure */
+#define POFD_E_NOMEM (-12)        /* device allocation failed */
+
+typedef struct pofd_ctx pofd_ctx;
+typedef struct pofd_beam1 pofd_beam1;
+typedef struct pofd_like1 pofd_like1;
+typedef struct pofd_pdfactory1 pofd_pdfactory1;
+
+/* Message of the last error raised on this thread ("" if none). */
+const char* pofd_last_error(void);
+/* Library version string. */
+const char* pofd_version(void);
+
+/* ---------------------------------------------------------------- context
+ * One context per GPU: selects the device and owns a CUDA stream.
+ * (Replaces the per-rank process set-up of the reference's MPI farm,
+ * pofd_affine_mcmc.cc:42 / pofdMCMC.cc:42.)  device = -1 makes a host-only
+ * context: the set-up entry points (beams, datasets, R ranges, dataset
+ * info) work on it, anything that needs a GPU returns POFD_E_CUDA. */
+int pofd_ctx_create(int device, pofd_ctx** out);
+int pofd_ctx_destroy(pofd_ctx* ctx);
+/* The context's stream (a cudaStream_t), for callers that enqueue work. */
+int pofd_ctx_stream(pofd_ctx* ctx, void** stream_out);
+int pofd_ctx_synchronize(pofd_ctx* ctx);
+
+/* ------------------------------------------------------------- 1D beam
+ * Replaces beam::beam(filename, histogram, NBINS, MINVAL) (beam.h:69) with
+ * an in-memory pixel array: beam::readFile's selection and sorting
+ * (beam.cc:295-458) and, if nhist > 0, beam::makeHistogram(nhist)
+ * (beam.cc:467-556).  pix holds npix beam values (any order, NaN/inf
+ * skipped); pixsize in arcsec. */
+int pofd_beam1_create(const double* pix, size_t npix, double pixsize,
+                      double minval, unsigned nhist, pofd_beam1** out);
+int pofd_beam1_destroy(pofd_beam1* b);
+/* info[15] = {haspos, hasneg, npos, nneg, poshist, neghist, nposhist,
+ *  nneghist, minpos, maxpos, minneg, maxneg, pixsize, totpos, totneg}
+ * (beam.h accessors hasPos..getMinMaxNeg). */
+int pofd_beam1_info(const pofd_beam1* b, double* info15);
+/* The weight / inverse-beam lists the R sum runs over for one side
+ * (numberCountsKnotsSpline.cc:463-477), written to caller arrays of at least
+ * *nterms entries (pass NULL arrays to query *nterms). */
+int pofd_beam1_terms(const pofd_beam1* b, int negative_side, size_t* nterms,
+                     double* weights, double* inv_beam);
+
+/* ------------------------------------------------------- 1D P(D) factory
+ * PDFactory (PDFactory.h:136-140).  initPD computes R on the GPU from the
+ * knot model (numberCountsKnotsSpline: knots at knotpos[nknots] Jy, log10
+ * values knotvals[nknots]), FFTs it and forms exp(R~ - R~0) with the mean
+ * shift; getPD applies the noise, inverse-FFTs, unwraps, normalises and
+ * (setlog) takes log2, writing n values to pd_out (host) plus the flux of
+ * element 0 and the step. */
+int pofd_pdfactory1_create(pofd_ctx* ctx, unsigned ninterp,
+                           pofd_pdfactory1** out);
+int pofd_pdfactory1_destroy(pofd_pdfactory1* f);
+int pofd_pdfactory1_initpd(pofd_pdfactory1* f, unsigned n, double minflux,
+                           double maxflux, unsigned nknots,
+                           const double* knotpos, const float* knotvals,
+                           const pofd_beam1* beam);
+int pofd_pdfactory1_getpd(pofd_pdfactory1* f, double sigma, int setlog,
+                          double* pd_out, double* minflux_out,
+                          double* dflux_out);
+/* R (times dflux, as the factory holds it) on the n-point wrapped grid. */
+int pofd_pdfactory1_get_r(pofd_pdfactory1* f, double* rvals_out);
+
+/* ---------------------------------------------------------- 1D likelihood
+ * calcLike (calcLike.h:166-275): datasets grouped into beam sets, one
+ * P(D) per beam set and proposal, one noise level per dataset.
+ *   create          calcLike(fftsize, ninterp, binned, nbins) + knot
+ *                   positions (setKnotPositions)
+ *   add_beamset     one beam group (calcLike.cc:741-755); exp_conf is the
+ *                   expected confusion noise used by setSigmaBase/setRRange
+ *   add_dataset     fitsData read + optional mean subtraction + binning
+ *                   (fitsData.cc:393-437) with its sigma_base and like_norm
+ *   set_rranges     setRRanges(p) (calcLike.cc:827): freezes the R range
+ *   reserve         sizes device work space and cuFFT plans for batches of
+ *                   up to max_batch proposals
+ *   loglike         getLogLike(p, pars_invalid) for one proposal
+ *   eval_batch      getLogLike for nprop proposals theta[nprop][npar]
+ *                   (host arrays; synchronous).  status[i] as above.
+ *   eval_batch_device  same with device pointers, enqueued on stream
+ *                   (void* cudaStream_t, NULL = the context's stream);
+ *                   returns after enqueue.
+ * The parameter layout is the reference's: nknots log10 knot values, then
+ * the sigma multiplier (calcLike.cc:909), then any bonus slots (ignored). */
+int pofd_like1_create(pofd_ctx* ctx, unsigned nknots, const double* knotpos,
+                      unsigned fftsize, unsigned ninterp, int bin_data,
+                      unsigned nbins, pofd_like1** out);
+int pofd_like1_destroy(pofd_like1* L);
+int pofd_like1_add_beamset(pofd_like1* L, const pofd_beam1* beam,
+                           double exp_conf);
+int pofd_like1_add_dataset(pofd_like1* L, int beamset, const double* data,
+                           size_t ndata, int meansub, double sigma_base,
+                           double like_norm);
+int pofd_like1_set_rranges(pofd_like1* L, const float* theta, unsigned npar);
+/* range2 = {minRFlux, maxRFlux} of a beam set. */
+int pofd_like1_get_rrange(const pofd_like1* L, int beamset, double* range2);
+/* info9 = {ndata, nbins, bincent0, bindelta, like_offset, sigma_base,
+ *  like_norm, minDataFlux, maxDataFlux}; bins (may be NULL) gets nbins
+ *  counts. */
+int pofd_like1_dataset_info(const pofd_like1* L, int beamset, int dataset,
+                            double* info9, uint32_t* bins);
+int pofd_like1_reserve(pofd_like1* L, unsigned max_batch);
+int pofd_like1_loglike(pofd_like1* L, const float* theta, unsigned npar,
+                       double* logl, int* pars_invalid);
+int pofd_like1_eval_batch(pofd_like1* L, unsigned nprop, const float* theta,
+                          unsigned npar, double* logl, int* status);
+int pofd_like1_eval_batch_device(pofd_like1* L, unsigned nprop,
+                                 const float* theta_dev, unsigned npar,
+                                 double* logl_dev, int* status_dev,
+                                 void* stream);
+/* The P(D) of one dataset for one proposal (getPD after initPD), n values
+ * to pd_out; info12 (may be NULL) = {dflux, minflux_R, wrapRidx, mean,
+ * var_noi, doshift, shift, splitidx, sgpos, sgneg, pd_minflux, 0}. */
+int pofd_like1_pd(pofd_like1* L, int beamset, int dataset, const float* theta,
+                  unsigned npar, int setlog, double* pd_out, double* info12);
+/* R at the ninterp interpolation nodes of a beam set (negative_side 0/1):
+ * node fluxes and R (PDFactory.cc:426-527). */
+int pofd_like1_rnodes(pofd_like1* L, int beamset, int negative_side,
+                      const float* theta, unsigned npar, double* x_out,
+                      double* r_out);
+/* Number of this library's kernels one eval_batch launches (cuFFT's own
+ * kernels not counted). */
+int pofd_like1_kernels_per_eval(const pofd_like1* L, int* nkernels);
+/* Per-stage device time of one launch sequence over nprop proposals
+ * (host theta), averaged over reps runs timed with CUDA events between the
+ * stages: stage_ms[i] for i < *nstages (at most 16), names from
+ * pofd_like1_stage_name(i).  Replaces the reference's -DTIMING clock()
+ * accumulators (PDFactory.cc:93-126). */
+int pofd_like1_profile(pofd_like1* L, unsigned nprop, const float* theta,
+                       unsigned npar, int reps, double* stage_ms,
+                       int* nstages);
+const char* pofd_like1_stage_name(int i);
+
+/* Measured FP64 FMA throughput of a device (TFLOP/s, 2 flops per FMA): the
+ * denominator of the FP64-bound kernels' roofline.  No counterpart in the
+ * reference (which has no GPU code). */
+int pofd_fp64_peak(int device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

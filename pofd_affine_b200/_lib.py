@@ -1,0 +1,103 @@
+"""ctypes binding of libpofd_b200.so (the C ABI in include/pofd_b200.h).
+
+The library is built in-tree (pofd_affine_b200/_lib/libpofd_b200.so) by
+``python -m pofd_affine_b200.build``.  There is no CPU fallback: if the
+library is missing or cannot be loaded, every use raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "_lib", "libpofd_b200.so")
+HEADER = os.path.join(HERE, "..", "include", "pofd_b200.h")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_up = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+V, I, U, D, S = C.c_void_p, C.c_int, C.c_uint, C.c_double, C.c_size_t
+PV = C.POINTER(C.c_void_p)
+
+# name -> (restype, argtypes); pointer-typed outputs that may be NULL are
+# declared as c_void_p.
+SIGNATURES = {
+    "pofd_last_error": (C.c_char_p, []),
+    "pofd_version": (C.c_char_p, []),
+    "pofd_ctx_create": (I, [I, PV]),
+    "pofd_ctx_destroy": (I, [V]),
+    "pofd_ctx_stream": (I, [V, PV]),
+    "pofd_ctx_synchronize": (I, [V]),
+    "pofd_beam1_create": (I, [_dp, S, D, D, U, PV]),
+    "pofd_beam1_destroy": (I, [V]),
+    "pofd_beam1_info": (I, [V, _dp]),
+    "pofd_beam1_terms": (I, [V, I, C.POINTER(S), V, V]),
+    "pofd_pdfactory1_create": (I, [V, U, PV]),
+    "pofd_pdfactory1_destroy": (I, [V]),
+    "pofd_pdfactory1_initpd": (I, [V, U, D, D, U, _dp, _fp, V]),
+    "pofd_pdfactory1_getpd": (I, [V, D, I, _dp, C.POINTER(D),
+                                  C.POINTER(D)]),
+    "pofd_pdfactory1_get_r": (I, [V, _dp]),
+    "pofd_like1_create": (I, [V, U, _dp, U, U, I, U, PV]),
+    "pofd_like1_destroy": (I, [V]),
+    "pofd_like1_add_beamset": (I, [V, V, D]),
+    "pofd_like1_add_dataset": (I, [V, I, _dp, S, I, D, D]),
+    "pofd_like1_set_rranges": (I, [V, _fp, U]),
+    "pofd_like1_get_rrange": (I, [V, I, _dp]),
+    "pofd_like1_dataset_info": (I, [V, I, I, _dp, V]),
+    "pofd_like1_reserve": (I, [V, U]),
+    "pofd_like1_loglike": (I, [V, _fp, U, C.POINTER(D), C.POINTER(I)]),
+    "pofd_like1_eval_batch": (I, [V, U, _fp, U, _dp, _ip]),
+    "pofd_like1_eval_batch_device": (I, [V, U, V, U, V, V, V]),
+    "pofd_like1_pd": (I, [V, I, I, _fp, U, I, _dp, V]),
+    "pofd_like1_rnodes": (I, [V, I, I, _fp, U, _dp, _dp]),
+    "pofd_like1_kernels_per_eval": (I, [V, C.POINTER(I)]),
+    "pofd_like1_profile": (I, [V, U, _fp, U, I, _dp, C.POINTER(I)]),
+    "pofd_like1_stage_name": (C.c_char_p, [I]),
+    "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
+}
+
+_lib = None
+
+
+class PofdError(RuntimeError):
+    """Raised for a negative status; .code is the POFD_E_* value."""
+
+    def __init__(self, code, msg):
+        super().__init__("pofd error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise RuntimeError(
+            "libpofd_b200.so is not built (%s); run python -m "
+            "pofd_affine_b200.build" % LIBPATH)
+    L = C.CDLL(LIBPATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(st):
+    if st < 0:
+        raise PofdError(st, lib().pofd_last_error().decode())
+    return st
+
+
+def declared_functions():
+    """Function names declared in include/pofd_b200.h."""
+    import re
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(pofd_[a-z0-9_]+)\s*\(", txt)))
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)

@@ -1,0 +1,408 @@
+// capi.cu -- extern "C" entry points of libpofd_b200.so (include/pofd_b200.h).
+//
+// Each entry point converts C++ exceptions into the status codes of the
+// header, so callers see the reference's error behaviour (an affineExcept
+// at the same point) as a negative return plus pofd_last_error().
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/pofd_b200.h"
+#include "engine1d.cuh"
+#include "setup.hh"
+
+namespace {
+thread_local std::string g_err;
+
+template <class F>
+int guard(F&& f) {
+  try {
+    return f();
+  } catch (const pofd::Error& e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return POFD_E_NOMEM;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return POFD_E_ARG;
+  }
+}
+
+void need(bool ok, const char* msg) {
+  if (!ok) throw pofd::Error(POFD_E_ARG, msg);
+}
+}  // namespace
+
+struct pofd_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+};
+
+struct pofd_beam1 {
+  pofd::Beam1 b;
+};
+
+struct pofd_like1 {
+  pofd_ctx* ctx = nullptr;
+  std::unique_ptr<pofd::Engine1> eng;
+};
+
+struct pofd_pdfactory1 {
+  pofd_ctx* ctx = nullptr;
+  unsigned ninterp = 2048;
+  std::unique_ptr<pofd::Engine1> eng;
+  std::vector<float> theta;  // knot values + noise slot
+  bool inited = false;
+};
+
+extern "C" {
+
+const char* pofd_last_error(void) { return g_err.c_str(); }
+const char* pofd_version(void) { return "pofd_b200 0.1.0 (reference pofd_affine 0.5.1)"; }
+
+// ------------------------------------------------------------- context
+int pofd_ctx_create(int device, pofd_ctx** out) {
+  return guard([&] {
+    need(out != nullptr, "null output pointer");
+    if (device == -1) {
+      // host-only context: set-up calls (beams, data, R ranges) work,
+      // anything that needs a GPU returns POFD_E_CUDA
+      std::unique_ptr<pofd_ctx> c(new pofd_ctx());
+      c->device = -1;
+      *out = c.release();
+      return POFD_OK;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+      throw pofd::Error(POFD_E_CUDA, "no CUDA device available");
+    need(device >= 0 && device < ndev, "invalid device index");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) throw pofd::Error(POFD_E_CUDA, cudaGetErrorString(e));
+    std::unique_ptr<pofd_ctx> c(new pofd_ctx());
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) throw pofd::Error(POFD_E_CUDA, cudaGetErrorString(e));
+    *out = c.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_ctx_destroy(pofd_ctx* ctx) {
+  if (!ctx) return POFD_OK;
+  if (ctx->device < 0) {
+    delete ctx;
+    return POFD_OK;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return POFD_OK;
+}
+
+int pofd_ctx_stream(pofd_ctx* ctx, void** s) {
+  return guard([&] {
+    need(ctx && s, "null argument");
+    *s = ctx->stream;
+    return POFD_OK;
+  });
+}
+
+int pofd_ctx_synchronize(pofd_ctx* ctx) {
+  return guard([&] {
+    need(ctx != nullptr, "null context");
+    cudaSetDevice(ctx->device);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) throw pofd::Error(POFD_E_CUDA, cudaGetErrorString(e));
+    return POFD_OK;
+  });
+}
+
+// ------------------------------------------------------------- 1D beam
+int pofd_beam1_create(const double* pix, size_t npix, double pixsize,
+                      double minval, unsigned nhist, pofd_beam1** out) {
+  return guard([&] {
+    need(pix && out, "null argument");
+    std::unique_ptr<pofd_beam1> b(new pofd_beam1());
+    b->b.build(pix, npix, pixsize, minval);
+    if (nhist > 0) b->b.histogram(nhist);
+    *out = b.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_beam1_destroy(pofd_beam1* b) {
+  delete b;
+  return POFD_OK;
+}
+
+int pofd_beam1_info(const pofd_beam1* bp, double* o) {
+  return guard([&] {
+    need(bp && o, "null argument");
+    const pofd::Beam1& b = bp->b;
+    o[0] = b.haspos; o[1] = b.hasneg;
+    o[2] = static_cast<double>(b.pos.size()); o[3] = static_cast<double>(b.neg.size());
+    o[4] = b.poshist; o[5] = b.neghist;
+    o[6] = static_cast<double>(b.poswt.size()); o[7] = static_cast<double>(b.negwt.size());
+    o[8] = b.haspos ? b.pos.front() : pofd::nan(); o[9] = b.maxpos();
+    o[10] = b.hasneg ? b.neg.front() : pofd::nan(); o[11] = b.maxneg();
+    o[12] = b.pixsize; o[13] = b.totpos; o[14] = b.totneg;
+    return POFD_OK;
+  });
+}
+
+int pofd_beam1_terms(const pofd_beam1* bp, int negside, size_t* nterms,
+                     double* weights, double* inv_beam) {
+  return guard([&] {
+    need(bp && nterms, "null argument");
+    std::vector<double> w, ie;
+    bp->b.terms(negside != 0, w, ie);
+    *nterms = ie.size();
+    if (weights) std::memcpy(weights, w.data(), w.size() * sizeof(double));
+    if (inv_beam) std::memcpy(inv_beam, ie.data(), ie.size() * sizeof(double));
+    return POFD_OK;
+  });
+}
+
+// ------------------------------------------------------- 1D P(D) factory
+int pofd_pdfactory1_create(pofd_ctx* ctx, unsigned ninterp,
+                           pofd_pdfactory1** out) {
+  return guard([&] {
+    need(ctx && out, "null argument");
+    need(ninterp >= 4, "Invalid (0) ninterp");
+    std::unique_ptr<pofd_pdfactory1> f(new pofd_pdfactory1());
+    f->ctx = ctx;
+    f->ninterp = ninterp;
+    *out = f.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_pdfactory1_destroy(pofd_pdfactory1* f) {
+  if (f && f->ctx) cudaSetDevice(f->ctx->device);
+  delete f;
+  return POFD_OK;
+}
+
+// PDFactory::initPD argument checks (PDFactory.cc:1031-1054), then the
+// engine is configured for one beam set with one noise-only dataset.
+int pofd_pdfactory1_initpd(pofd_pdfactory1* f, unsigned n, double minflux,
+                           double maxflux, unsigned nknots,
+                           const double* knotpos, const float* knotvals,
+                           const pofd_beam1* beam) {
+  return guard([&] {
+    need(f && knotpos && knotvals && beam, "null argument");
+    if (n == 0) throw pofd::Error(POFD_E_ARG, "Invalid (zero) n");
+    if (n == 1) throw pofd::Error(POFD_E_ARG, "Invalid (==0) n");
+    if (maxflux <= 0.0) throw pofd::Error(POFD_E_ARG, "Invalid (non-positive) maxflux");
+    if (minflux == maxflux) throw pofd::Error(POFD_E_ARG, "Invalid (0) range between min/max flux");
+    for (unsigned k = 0; k < nknots; ++k)
+      if (std::isnan(static_cast<double>(knotvals[k])))
+        throw pofd::Error(POFD_E_INVALID_MODEL, "Invalid model");
+    cudaSetDevice(f->ctx->device);
+    f->eng.reset(new pofd::Engine1(f->ctx->device, f->ctx->stream));
+    f->eng->configure(nknots, knotpos, n, f->ninterp, true, 1);
+    const int bs = f->eng->add_beamset(beam->b, 0.0);
+    f->eng->add_virtual_dataset(bs, 1.0);
+    f->eng->set_rrange_explicit(bs, minflux, maxflux);
+    f->eng->reserve(1);
+    f->theta.assign(knotvals, knotvals + nknots);
+    f->theta.push_back(1.0f);  // sigma multiplier; the noise level is the dataset's
+    f->inited = true;
+    return POFD_OK;
+  });
+}
+
+int pofd_pdfactory1_getpd(pofd_pdfactory1* f, double sigma, int setlog,
+                          double* pd_out, double* minflux_out,
+                          double* dflux_out) {
+  return guard([&] {
+    need(f && pd_out, "null argument");
+    if (!f->inited) throw pofd::Error(POFD_E_ARG, "Must call initPD first");
+    cudaSetDevice(f->ctx->device);
+    double info[12];
+    f->eng->set_virtual_sigma(0, sigma);
+    const int st = f->eng->pd_host(0, 0, f->theta.data(),
+                                   static_cast<unsigned>(f->theta.size()),
+                                   setlog != 0, pd_out, info);
+    if (minflux_out) *minflux_out = info[10];
+    if (dflux_out) *dflux_out = info[0];
+    if (st != 0) throw pofd::Error(st, "P(D) unwrap failed (split point or mean)");
+    return POFD_OK;
+  });
+}
+
+int pofd_pdfactory1_get_r(pofd_pdfactory1* f, double* rvals_out) {
+  return guard([&] {
+    need(f && rvals_out, "null argument");
+    if (!f->inited) throw pofd::Error(POFD_E_ARG, "Must call initPD first");
+    cudaSetDevice(f->ctx->device);
+    f->eng->rgrid_host(0, f->theta.data(), static_cast<unsigned>(f->theta.size()), rvals_out);
+    return POFD_OK;
+  });
+}
+
+// ---------------------------------------------------------- 1D likelihood
+int pofd_like1_create(pofd_ctx* ctx, unsigned nknots, const double* knotpos,
+                      unsigned fftsize, unsigned ninterp, int bin_data,
+                      unsigned nbins, pofd_like1** out) {
+  return guard([&] {
+    need(ctx && knotpos && out, "null argument");
+    cudaSetDevice(ctx->device);
+    std::unique_ptr<pofd_like1> L(new pofd_like1());
+    L->ctx = ctx;
+    L->eng.reset(new pofd::Engine1(ctx->device, ctx->stream));
+    L->eng->configure(nknots, knotpos, fftsize, ninterp, bin_data != 0, nbins);
+    *out = L.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_destroy(pofd_like1* L) {
+  if (L && L->ctx) cudaSetDevice(L->ctx->device);
+  delete L;
+  return POFD_OK;
+}
+
+int pofd_like1_add_beamset(pofd_like1* L, const pofd_beam1* beam,
+                           double exp_conf) {
+  return guard([&] {
+    need(L && beam, "null argument");
+    return L->eng->add_beamset(beam->b, exp_conf);
+  });
+}
+
+int pofd_like1_add_dataset(pofd_like1* L, int beamset, const double* data,
+                           size_t ndata, int meansub, double sigma_base,
+                           double like_norm) {
+  return guard([&] {
+    need(L && data, "null argument");
+    L->eng->add_dataset(beamset, data, ndata, meansub != 0, sigma_base, like_norm);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_set_rranges(pofd_like1* L, const float* theta, unsigned npar) {
+  return guard([&] {
+    need(L && theta, "null argument");
+    L->eng->set_rranges(theta, npar);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_get_rrange(const pofd_like1* L, int beamset, double* r) {
+  return guard([&] {
+    need(L && r, "null argument");
+    const auto rr = L->eng->rrange(beamset);
+    r[0] = rr.first;
+    r[1] = rr.second;
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_dataset_info(const pofd_like1* L, int beamset, int dataset,
+                            double* info9, uint32_t* bins) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->dataset_info(beamset, dataset, info9, bins);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_reserve(pofd_like1* L, unsigned max_batch) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    cudaSetDevice(L->ctx->device);
+    L->eng->reserve(max_batch);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_loglike(pofd_like1* L, const float* theta, unsigned npar,
+                       double* logl, int* pars_invalid) {
+  return guard([&] {
+    need(L && theta && logl, "null argument");
+    cudaSetDevice(L->ctx->device);
+    int st = 0;
+    L->eng->eval_host(1, theta, npar, logl, &st);
+    if (pars_invalid) *pars_invalid = (st == POFD_REJECTED) ? 1 : 0;
+    if (st < 0) throw pofd::Error(st, "likelihood evaluation failed");
+    return st;
+  });
+}
+
+int pofd_like1_eval_batch(pofd_like1* L, unsigned nprop, const float* theta,
+                          unsigned npar, double* logl, int* status) {
+  return guard([&] {
+    need(L && theta && logl && status, "null argument");
+    cudaSetDevice(L->ctx->device);
+    L->eng->eval_host(nprop, theta, npar, logl, status);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_eval_batch_device(pofd_like1* L, unsigned nprop,
+                                 const float* theta_dev, unsigned npar,
+                                 double* logl_dev, int* status_dev,
+                                 void* stream) {
+  return guard([&] {
+    need(L && theta_dev && logl_dev && status_dev, "null argument");
+    cudaSetDevice(L->ctx->device);
+    L->eng->enqueue(nprop, theta_dev, npar, logl_dev, status_dev,
+                    static_cast<cudaStream_t>(stream));
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_pd(pofd_like1* L, int beamset, int dataset, const float* theta,
+                  unsigned npar, int setlog, double* pd_out, double* info12) {
+  return guard([&] {
+    need(L && theta && pd_out, "null argument");
+    cudaSetDevice(L->ctx->device);
+    const int st = L->eng->pd_host(beamset, dataset, theta, npar, setlog != 0,
+                                   pd_out, info12);
+    if (st != 0) throw pofd::Error(st, "P(D) unwrap failed (split point or mean)");
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_rnodes(pofd_like1* L, int beamset, int negative_side,
+                      const float* theta, unsigned npar, double* x_out,
+                      double* r_out) {
+  return guard([&] {
+    need(L && theta && x_out && r_out, "null argument");
+    cudaSetDevice(L->ctx->device);
+    L->eng->rnodes_host(beamset, negative_side ? 1 : 0, theta, npar, x_out, r_out);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_kernels_per_eval(const pofd_like1* L, int* nk) {
+  return guard([&] {
+    need(L && nk, "null argument");
+    *nk = L->eng->kernels_per_eval();
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_profile(pofd_like1* L, unsigned nprop, const float* theta,
+                       unsigned npar, int reps, double* stage_ms,
+                       int* nstages) {
+  return guard([&] {
+    need(L && theta && stage_ms && nstages, "null argument");
+    need(reps > 0, "reps must be > 0");
+    cudaSetDevice(L->ctx->device);
+    L->eng->profile_stages(nprop, theta, npar, reps, stage_ms);
+    *nstages = pofd::Engine1::kNumStages;
+    return POFD_OK;
+  });
+}
+
+const char* pofd_like1_stage_name(int i) { return pofd::Engine1::stage_name(i); }
+
+}  // extern "C"

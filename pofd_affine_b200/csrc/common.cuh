@@ -1,0 +1,175 @@
+// common.cuh -- device helpers shared by the P(D) kernels.
+#ifndef POFD_COMMON_CUH
+#define POFD_COMMON_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pofd {
+namespace dev {
+
+constexpr double kTwoPi = 6.283185307179586476925286766559005768394;
+constexpr double kSmallLogVal = -30.0;
+
+// -------------------------------------------------------------- reductions
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < NT / 32) ? sh[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (l == 0) sh[0] = v;
+  }
+  __syncthreads();
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// max that ignores nothing special: plain (a > b ? a : b) semantics
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < NT / 32) ? sh[l] : -1.0e308;
+    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (l == 0) sh[0] = v;
+  }
+  __syncthreads();
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// (value, index) minimum; ties go to the smaller index, matching a forward
+// scan that replaces the minimum only on strictly smaller values.
+__device__ __forceinline__ void argmin_merge(double& v, int& i, double v2, int i2) {
+  if (v2 < v || (v2 == v && i2 < i)) { v = v2; i = i2; }
+}
+
+template <int NT>
+__device__ __forceinline__ void block_argmin(double& v, int& i, double* shv,
+                                             int* shi) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+    const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+    argmin_merge(v, i, v2, i2);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) { shv[w] = v; shi[w] = i; }
+  __syncthreads();
+  if (w == 0) {
+    v = (l < NT / 32) ? shv[l] : 1.0e308;
+    i = (l < NT / 32) ? shi[l] : 0x7fffffff;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+      argmin_merge(v, i, v2, i2);
+    }
+    if (l == 0) { shv[0] = v; shi[0] = i; }
+  }
+  __syncthreads();
+  v = shv[0];
+  i = shi[0];
+  __syncthreads();
+}
+
+template <int NT>
+__device__ __forceinline__ int block_max_int(int v, int* sh) {
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < NT / 32) ? sh[l] : -0x7fffffff;
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (l == 0) sh[0] = v;
+  }
+  __syncthreads();
+  const int r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// ------------------------------------------------------ affine-map scans
+// Inclusive scan over threads of affine maps z -> a z + b, composed in
+// thread order (thread t's result = map_t o ... o map_0).  NT threads,
+// shared scratch of 2*NT doubles.  Returns the composed (a, b).
+template <int NT>
+__device__ __forceinline__ void block_affine_scan(double& a, double& b,
+                                                  double* sh) {
+  double* sa = sh;
+  double* sb = sh + NT;
+  const int t = threadIdx.x;
+  sa[t] = a;
+  sb[t] = b;
+  __syncthreads();
+  for (int off = 1; off < NT; off <<= 1) {
+    double pa = 1.0, pb = 0.0;
+    const bool has = t >= off;
+    if (has) { pa = sa[t - off]; pb = sb[t - off]; }
+    __syncthreads();
+    if (has) {
+      // (a,b) o (pa,pb): z -> a (pa z + pb) + b
+      b = a * pb + b;
+      a = a * pa;
+      sa[t] = a;
+      sb[t] = b;
+    }
+    __syncthreads();
+  }
+}
+
+// Same, composed in reverse thread order (thread t's result =
+// map_t o map_{t+1} o ... o map_{NT-1}).
+template <int NT>
+__device__ __forceinline__ void block_affine_rscan(double& a, double& b,
+                                                   double* sh) {
+  double* sa = sh;
+  double* sb = sh + NT;
+  const int t = threadIdx.x;
+  sa[t] = a;
+  sb[t] = b;
+  __syncthreads();
+  for (int off = 1; off < NT; off <<= 1) {
+    double pa = 1.0, pb = 0.0;
+    const bool has = t + off < NT;
+    if (has) { pa = sa[t + off]; pb = sb[t + off]; }
+    __syncthreads();
+    if (has) {
+      b = a * pb + b;
+      a = a * pa;
+      sa[t] = a;
+      sb[t] = b;
+    }
+    __syncthreads();
+  }
+}
+
+// Largest i in [lo, hi-1] with x[i] <= v (x increasing): the bisection of
+// the interpolation library the reference uses, clamped to [lo, hi-1].
+__device__ __forceinline__ int bsearch_lo(const double* __restrict__ x,
+                                          double v, int lo, int hi) {
+  int ilo = lo, ihi = hi;
+  while (ihi > ilo + 1) {
+    const int i = (ihi + ilo) >> 1;
+    if (x[i] > v) ihi = i; else ilo = i;
+  }
+  return ilo;
+}
+
+}  // namespace dev
+}  // namespace pofd
+#endif

@@ -1,0 +1,1461 @@
+// engine1d.cu -- 1D P(D) likelihood: sm_100a kernels and the batched engine.
+//
+// Reference path restated (aconley/pofd_affine 0.5.1):
+//   numberCountsKnotsSpline::setParams / getR  numberCountsKnotsSpline.cc:265-274, 436-529
+//   PDFactory::initRInterp / initR             PDFactory.cc:426-527, 541-620
+//   PDFactory::getMeanVarFromR                 PDFactory.cc:625-679
+//   PDFactory::initPD (FFT, exp, shift)        PDFactory.cc:1031-1141
+//   PDFactory::getPD (noise, inverse FFT)      PDFactory.cc:1154-1243
+//   PDFactory::findSplitPoint / unwrap         PDFactory.cc:691-1009
+//   PD::normalize / getMean / applyLog         PD.cc:146-184, 245-274
+//   PD::getLogLikeBinned / Unbinned            PD.cc:557-677
+//   calcLikeSingle::getLogLike / calcLike      calcLike.cc:389-443, 884-955
+//
+// Layout in HBM (P proposals, B beam sets, D datasets, n FFT size, NI
+// interpolation nodes, nc = n/2+1):
+//   nodes [P][B][2][NI]        R at the nodes (pos/neg side)
+//   spl   [P][B][2][4][NI]     node spline y, b, c, d per interval
+//   rbuf  [P][B][2*nc]         R grid (x dflux), then its D2Z spectrum in place
+//   pbuf  [P][D][2*nc]         per-dataset spectrum, then its Z2D P(D) in place
+//   ppart/pmidx [P][D][nchunk] chunk reductions of the P(D)
+//   pinfo [P][D]               split, normalisation, mean, log-likelihood
+// Each proposal's R and P(D) rows are contiguous so the D2Z/Z2D run as two
+// batched cuFFT calls over P*B and P*D rows.
+#include "engine1d.cuh"
+
+#include <cstring>
+#include <sstream>
+
+#include "common.cuh"
+
+namespace pofd {
+
+namespace {
+
+constexpr int NT = 256;           // threads per block for the streaming kernels
+constexpr int TILE = NT * 8;      // R grid points per block
+constexpr int CHUNK = NT * 16;    // P(D) elements per reduction block
+constexpr int KMAX = Engine1::KMAX;
+constexpr int MAXTERMS = 6144;    // beam terms held in shared memory
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    std::ostringstream s;
+    s << what << ": " << cudaGetErrorString(e);
+    throw Error(e == cudaErrorMemoryAllocation ? POFD_E_NOMEM : POFD_E_CUDA,
+                s.str());
+  }
+}
+void cufft_check(cufftResult r, const char* what) {
+  if (r != CUFFT_SUCCESS) {
+    std::ostringstream s;
+    s << what << ": cuFFT error " << static_cast<int>(r);
+    throw Error(r == CUFFT_ALLOC_FAILED ? POFD_E_NOMEM : POFD_E_CUDA, s.str());
+  }
+}
+
+// ------------------------------------------------------------- kernels
+
+// Model set-up per proposal: log2 knot values from the float parameters and
+// the natural cubic spline through (log2 S_k, log2 n_k), stored per interval
+// as (y, b, c, d) exactly as the spline library forms them at evaluation.
+__global__ void k_model1(Model1Dev m, const float* __restrict__ theta,
+                         int npar, int nprop, double logfac,
+                         double* __restrict__ cnt, int* __restrict__ mstatus,
+                         double* __restrict__ sigmult) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nprop) return;
+  const float* th = theta + static_cast<size_t>(w) * npar;
+  const int K = m.K;
+  double y[KMAX], c[KMAX], g[KMAX], diag[KMAX], off[KMAX], alp[KMAX],
+      gam[KMAX], z[KMAX];
+  bool ok = true;
+  for (int k = 0; k < K; ++k) {
+    y[k] = logfac * static_cast<double>(th[k]);
+    if (isnan(y[k])) ok = false;
+  }
+  sigmult[w] = static_cast<double>(th[K]);
+  double* out = cnt + static_cast<size_t>(w) * 4 * KMAX;
+  if (!ok) {
+    mstatus[w] = POFD_E_INVALID_MODEL;
+    return;
+  }
+  const double* x = m.logknots;
+  for (int k = 0; k < K; ++k) c[k] = 0.0;
+  const int N = K - 2;
+  for (int i = 0; i < N; ++i) {
+    const double h_i = x[i + 1] - x[i], h_ip1 = x[i + 2] - x[i + 1];
+    const double g_i = (h_i != 0.0) ? 1.0 / h_i : 0.0;
+    const double g_ip1 = (h_ip1 != 0.0) ? 1.0 / h_ip1 : 0.0;
+    off[i] = h_ip1;
+    diag[i] = 2.0 * (h_ip1 + h_i);
+    g[i] = 3.0 * ((y[i + 2] - y[i + 1]) * g_ip1 - (y[i + 1] - y[i]) * g_i);
+  }
+  if (N == 1) {
+    c[1] = g[0] / diag[0];
+  } else if (N > 1) {
+    // symmetric tridiagonal L D L^T solve
+    alp[0] = diag[0];
+    gam[0] = off[0] / alp[0];
+    for (int i = 1; i < N - 1; ++i) {
+      alp[i] = diag[i] - off[i - 1] * gam[i - 1];
+      gam[i] = off[i] / alp[i];
+    }
+    alp[N - 1] = diag[N - 1] - off[N - 2] * gam[N - 2];
+    z[0] = g[0];
+    for (int i = 1; i < N; ++i) z[i] = g[i] - gam[i - 1] * z[i - 1];
+    for (int i = 0; i < N; ++i) z[i] = z[i] / alp[i];
+    c[N] = z[N - 1];
+    for (int i = N - 2; i >= 0; --i) c[1 + i] = z[i] - gam[i] * c[2 + i];
+  }
+  for (int i = 0; i < K - 1; ++i) {
+    const double dx = x[i + 1] - x[i];
+    const double dy = y[i + 1] - y[i];
+    out[4 * i + 0] = y[i];
+    out[4 * i + 1] = (dy / dx) - dx * (c[i + 1] + 2.0 * c[i]) / 3.0;
+    out[4 * i + 2] = c[i];
+    out[4 * i + 3] = (c[i + 1] - c[i]) / (3.0 * dx);
+  }
+  mstatus[w] = 0;
+}
+
+__device__ __forceinline__ double counts_log2(const double* __restrict__ lk,
+                                              const double* __restrict__ cs,
+                                              int K, double u) {
+  const int k = dev::bsearch_lo(lk, u, 0, K - 1);
+  const double delx = u - lk[k];
+  const double* q = cs + 4 * k;
+  return q[0] + delx * (q[1] + delx * (q[2] + delx * q[3]));
+}
+
+// R at the interpolation nodes, one node per thread, terms summed in the
+// beam's order: numberCountsKnotsSpline.cc:495-526.
+__global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
+                          int B, int NI, int maxterms,
+                          const double* __restrict__ cnt,
+                          const int* __restrict__ mstatus,
+                          double* __restrict__ nodes) {
+  extern __shared__ double sm[];
+  const int row = blockIdx.y;  // (w*B + b)*2 + side
+  const int side = row & 1;
+  const int wb = row >> 1;
+  const int w = wb / B, b = wb - w * B;
+  const BSet1Dev& bs = bsets[b];
+  const Side1Dev& sd = bs.side[side];
+  if (!sd.nodes || mstatus[w] != 0) return;
+  const int K = m.K;
+  double* s_lk = sm;
+  double* s_cs = s_lk + KMAX;
+  double* s_w = s_cs + 4 * KMAX;
+  double* s_ie = s_w + maxterms;
+  const double* cs = cnt + static_cast<size_t>(w) * 4 * KMAX;
+  for (int i = threadIdx.x; i < K; i += blockDim.x) s_lk[i] = m.logknots[i];
+  for (int i = threadIdx.x; i < 4 * (K - 1); i += blockDim.x) s_cs[i] = cs[i];
+  const int nt = sd.nterms;
+  for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+    s_w[i] = sd.w[i];
+    s_ie[i] = sd.ieta[i];
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NI) return;
+  const double f = sd.x[i];
+  const double minknot = m.minknot, maxknot = m.maxknot;
+  double workval = 0.0;
+  const bool posb = (f > 0 && bs.haspos && f <= bs.rr_hi);
+  const bool negb = !posb && (bs.hasneg && f < 0 && f >= bs.rr_lo);
+  if (posb || negb) {
+    const double af = posb ? f : -f;
+    for (int j = 0; j < nt; ++j) {
+      const double ieta = s_ie[j];
+      const double currarg = af * ieta;
+      if (currarg < minknot || currarg >= maxknot) continue;
+      const double cts = exp2(counts_log2(s_lk, s_cs, K, log2(currarg)));
+      if (cts > 0) workval += s_w[j] * cts * ieta;
+    }
+  }
+  nodes[static_cast<size_t>(row) * NI + i] = bs.prefac * workval;
+}
+
+// Natural cubic spline through (x_i, log2 R_i) over the NI nodes: RHS of
+// the tridiagonal system, forward and back substitution against the
+// precomputed LDL^T factors as two block-wide affine-map scans, then the
+// per-interval (y, b, c, d) (PDFactory.cc:466-474, 522).
+__global__ void __launch_bounds__(NT)
+k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
+           const int* __restrict__ mstatus, const double* __restrict__ nodes,
+           double* __restrict__ spl) {
+  extern __shared__ double sm[];
+  const int row = blockIdx.x;
+  const int side = row & 1;
+  const int wb = row >> 1;
+  const int w = wb / B, b = wb - w * B;
+  const Side1Dev& sd = bsets[b].side[side];
+  if (!sd.nodes || mstatus[w] != 0) return;
+  double* y = sm;             // NI
+  double* c = y + NI;         // NI (full second-derivative/2 array)
+  double* scr = c + NI;       // 2*NT
+  const double* R = nodes + static_cast<size_t>(row) * NI;
+  for (int i = threadIdx.x; i < NI; i += NT) {
+    const double v = R[i];
+    y[i] = (v > 0) ? log2(v) : dev::kSmallLogVal;
+  }
+  __syncthreads();
+  const int N = NI - 2;
+  const int E = (N + NT - 1) / NT;
+  const int s0 = threadIdx.x * E;
+  const int s1 = min(s0 + E, N);
+  const double* ih = sd.ih;
+  const double* al = sd.alpha;
+  const double* ga = sd.gamma;
+  // forward: z_i = g_i - gamma_{i-1} z_{i-1}, z_0 = g_0; stored in c[1+i]
+  double A = 1.0, Bv = 0.0;
+  for (int i = s0; i < s1; ++i) {
+    const double gi = 3.0 * ((y[i + 2] - y[i + 1]) * ih[i + 1] - (y[i + 1] - y[i]) * ih[i]);
+    c[1 + i] = gi;
+    const double a = (i == 0) ? 0.0 : -ga[i - 1];
+    Bv = a * Bv + gi;
+    A = a * A;
+  }
+  dev::block_affine_scan<NT>(A, Bv, scr);
+  double zin = 0.0;
+  {
+    // exclusive prefix: inclusive result of the previous thread
+    __syncthreads();
+    scr[threadIdx.x] = Bv;
+    __syncthreads();
+    zin = (threadIdx.x > 0) ? scr[threadIdx.x - 1] : 0.0;
+    __syncthreads();
+  }
+  {
+    double z = zin;
+    for (int i = s0; i < s1; ++i) {
+      const double gi = c[1 + i];
+      z = (i == 0) ? gi : gi - ga[i - 1] * z;
+      c[1 + i] = z / al[i];  // cc_i
+    }
+  }
+  __syncthreads();
+  // back: c_i = cc_i - gamma_i c_{i+1}, c_{N-1} = cc_{N-1}
+  A = 1.0;
+  Bv = 0.0;
+  for (int i = s1 - 1; i >= s0; --i) {
+    const double a = (i == N - 1) ? 0.0 : -ga[i];
+    Bv = a * Bv + c[1 + i];
+    A = a * A;
+  }
+  dev::block_affine_rscan<NT>(A, Bv, scr);
+  double cin = 0.0;
+  {
+    __syncthreads();
+    scr[threadIdx.x] = Bv;
+    __syncthreads();
+    cin = (threadIdx.x + 1 < NT) ? scr[threadIdx.x + 1] : 0.0;
+    __syncthreads();
+  }
+  {
+    double cn = cin;
+    for (int i = s1 - 1; i >= s0; --i) {
+      const double cc = c[1 + i];
+      cn = (i == N - 1) ? cc : cc - ga[i] * cn;
+      c[1 + i] = cn;
+    }
+  }
+  if (threadIdx.x == 0) {
+    c[0] = 0.0;
+    c[NI - 1] = 0.0;
+  }
+  __syncthreads();
+  double* out = spl + static_cast<size_t>(row) * 4 * NI;
+  const double* x = sd.x;
+  for (int i = threadIdx.x; i < NI - 1; i += NT) {
+    const double dx = x[i + 1] - x[i];
+    const double dy = y[i + 1] - y[i];
+    out[i] = y[i];
+    out[NI + i] = (dy / dx) - dx * (c[i + 1] + 2.0 * c[i]) / 3.0;
+    out[2 * NI + i] = c[i];
+    out[3 * NI + i] = (c[i + 1] - c[i]) / (3.0 * dx);
+  }
+}
+
+// The wrapped R grid: 2^spline(flux) * dflux inside each side's covered
+// index range, zero elsewhere (PDFactory.cc:556-613), plus block partial
+// sums of the first and second flux moments (PDFactory.cc:634-665).
+__global__ void __launch_bounds__(NT)
+k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
+         int nc2, int ntile, const int* __restrict__ mstatus,
+         const double* __restrict__ spl, double* __restrict__ rbuf,
+         double* __restrict__ rpart) {
+  __shared__ double shr[32];
+  const int wb = blockIdx.y;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet1Dev& bs = bsets[b];
+  const double dflux = bs.dflux;
+  const int wrap = bs.wrapRidx;
+  const double minflux_R = bs.minflux_R;
+  double* R = rbuf + static_cast<size_t>(wb) * nc2;
+  double mn = 0.0, var = 0.0;
+  const int base = blockIdx.x * TILE;
+#pragma unroll 4
+  for (int k = 0; k < TILE / NT; ++k) {
+    const int i = base + k * NT + threadIdx.x;
+    if (i >= n) break;
+    const int side = (i <= wrap) ? 0 : 1;
+    const Side1Dev& sd = bs.side[side];
+    double r = 0.0;
+    if (i >= sd.grid_lo && i <= sd.grid_hi) {
+      const double cflux = static_cast<double>(i) * dflux + sd.grid_off;
+      const double* x = sd.x;
+      const int q = dev::bsearch_lo(x, cflux, 0, NI - 1);
+      const double* S = spl + (static_cast<size_t>(wb) * 2 + side) * 4 * NI;
+      const double delx = cflux - x[q];
+      const double v = S[q] + delx * (S[NI + q] + delx * (S[2 * NI + q] + delx * S[3 * NI + q]));
+      r = exp2(v) * dflux;
+    }
+    R[i] = r;
+    if (i >= 1 && i <= wrap - 1) {
+      const double cf = static_cast<double>(i) * dflux;
+      const double prod = cf * r;
+      mn += prod;
+      var += cf * prod;
+    } else if (i == wrap && i > 0) {
+      const double cf = static_cast<double>(wrap) * dflux;
+      const double prod = 0.5 * cf * r;
+      mn += prod;
+      var += cf * prod;
+    } else if (i > wrap) {
+      const double cf = static_cast<double>(i - wrap - 1) * dflux + minflux_R;
+      const double prod = cf * r;
+      mn += prod;
+      var += cf * prod;
+    }
+  }
+  mn = dev::block_sum<NT>(mn, shr);
+  var = dev::block_sum<NT>(var, shr);
+  if (threadIdx.x == 0) {
+    double* o = rpart + (static_cast<size_t>(wb) * ntile + blockIdx.x) * 2;
+    o[0] = mn;
+    o[1] = var;
+  }
+}
+
+// Moments, sigma estimate and the shift decision (PDFactory.cc:660-679,
+// 1067-1076), one thread per (proposal, beam set).
+__global__ void k_moments1(const BSet1Dev* __restrict__ bsets, int B, int n,
+                           int nc2, int ntile, int nrow,
+                           const int* __restrict__ mstatus,
+                           const double* __restrict__ rbuf,
+                           const double* __restrict__ rpart,
+                           double* __restrict__ mom) {
+  const int wb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (wb >= nrow) return;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet1Dev& bs = bsets[b];
+  double mn = 0.0, var = 0.0;
+  const double* p = rpart + static_cast<size_t>(wb) * ntile * 2;
+  for (int t = 0; t < ntile; ++t) {
+    mn += p[2 * t];
+    var += p[2 * t + 1];
+  }
+  const int wrap = bs.wrapRidx;
+  if (wrap < n - 1) {
+    const double cf = bs.minflux_R;
+    const double prod = 0.5 * cf * rbuf[static_cast<size_t>(wb) * nc2 + (wrap - 1)];
+    mn -= prod;
+    var -= cf * prod;
+  }
+  const double sg = sqrt(var);
+  const bool doshift = (sg > bs.dflux) && (fabs(mn) > bs.dflux);
+  double* o = mom + static_cast<size_t>(wb) * 4;
+  o[0] = mn;
+  o[1] = var;
+  o[2] = doshift ? -mn : 0.0;
+  o[3] = doshift ? 1.0 : 0.0;
+}
+
+// exp(R~ - R~0) with the mean shift, then one noise-multiplied copy per
+// dataset of the beam set (PDFactory.cc:1106-1132, 1174-1188).  The
+// self-conjugate Nyquist bin keeps only its real part, which is what the
+// c2r transform uses of it.
+__global__ void __launch_bounds__(NT)
+k_spectrum1(const BSet1Dev* __restrict__ bsets,
+            const DSet1Dev* __restrict__ dsets, int B, int D, int n, int nc,
+            const int* __restrict__ mstatus, const double* __restrict__ sigmult,
+            const double* __restrict__ mom, const double* __restrict__ rbuf,
+            double* __restrict__ pbuf) {
+  const int wb = blockIdx.y;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const int k = blockIdx.x * NT + threadIdx.x;
+  if (k >= nc) return;
+  const BSet1Dev& bs = bsets[b];
+  const double2* Rt = reinterpret_cast<const double2*>(rbuf + static_cast<size_t>(wb) * 2 * nc);
+  const double dflux = bs.dflux;
+  const double iflux = dev::kTwoPi / (static_cast<double>(n) * dflux);
+  const double* mo = mom + static_cast<size_t>(wb) * 4;
+  const bool doshift = mo[3] != 0.0;
+  double2 p;
+  if (k == 0) {
+    p = make_double2(1.0, 0.0);
+  } else {
+    const double r0 = Rt[0].x;
+    const double2 v = Rt[k];
+    const double expfac = exp(v.x - r0);
+    const double ival = doshift ? v.y - (mo[2] * iflux) * static_cast<double>(k) : v.y;
+    double s, c;
+    sincos(ival, &s, &c);
+    p = make_double2(expfac * c, expfac * s);
+  }
+  if ((n & 1) == 0 && k == n / 2) p.y = 0.0;
+  const double sm = sigmult[w];
+  for (int dd = 0; dd < bs.nds; ++dd) {
+    const int d = bs.ds_begin + dd;
+    const double sigma = sm * dsets[d].sigma_base;
+    double2 o = p;
+    if (sigma > 0 && k > 0) {
+      const double sigfac = -0.5 * sigma * sigma;
+      const double wv = iflux * static_cast<double>(k);
+      const double ef = exp(sigfac * wv * wv);
+      o = make_double2(ef * p.x, ef * p.y);
+    }
+    reinterpret_cast<double2*>(pbuf + (static_cast<size_t>(w) * D + d) * 2 * nc)[k] = o;
+  }
+}
+
+struct SplitParams {
+  double sgpos, sgneg, n1sigpos, n1signeg;
+  long long botidx, topidx;
+};
+
+__device__ __forceinline__ long long to_index(double v) {
+  // (int) conversion of the reference, saturated so that huge values stay
+  // out of range instead of wrapping.
+  if (!(v < 9.0e15)) return 0x7fffffffffffLL;
+  if (!(v > -9.0e15)) return -0x7fffffffffffLL;
+  return static_cast<long long>(v);
+}
+
+__device__ __forceinline__ SplitParams split_params(const BSet1Dev& bs,
+                                                    double var, double sigma) {
+  SplitParams sp;
+  sp.sgpos = sqrt(var + sigma * sigma);
+  sp.sgneg = (9 * sigma * sigma > var) ? sigma : sp.sgpos;
+  sp.n1sigpos = 2.5 * sp.sgpos;
+  sp.n1signeg = 2.5 * sp.sgneg;
+  sp.botidx = to_index(sp.n1sigpos / bs.dflux);
+  if (sp.n1sigpos > fabs(bs.minflux_R))
+    sp.topidx = bs.wrapRidx;
+  else
+    sp.topidx = to_index(-(sp.n1signeg + bs.minflux_R) / bs.dflux + bs.wrapRidx + 1);
+  return sp;
+}
+
+__device__ __forceinline__ double clip0(double v) { return (v < 0) ? 0.0 : v; }
+
+// Chunk reductions over the P(D) after the inverse transform: peak, sum,
+// index-weighted sum and the minimum inside the split search window
+// (PDFactory.cc:779-815, PD.cc:123-140, 245-274).
+__global__ void __launch_bounds__(NT)
+k_pscan1(const BSet1Dev* __restrict__ bsets, const DSet1Dev* __restrict__ dsets,
+         int B, int D, int n, int nc2, int nchunk,
+         const int* __restrict__ mstatus, const double* __restrict__ sigmult,
+         const double* __restrict__ mom, const double* __restrict__ pbuf,
+         double* __restrict__ ppart, int* __restrict__ pmidx) {
+  __shared__ double shd[32];
+  __shared__ int shi[32];
+  const int wd = blockIdx.y;
+  const int w = wd / D, d = wd - w * D;
+  if (mstatus[w] != 0) return;
+  const DSet1Dev& ds = dsets[d];
+  const BSet1Dev& bs = bsets[ds.bs];
+  const double var = mom[(static_cast<size_t>(w) * B + ds.bs) * 4 + 1];
+  const SplitParams sp = split_params(bs, var, sigmult[w] * ds.sigma_base);
+  const double* p = pbuf + static_cast<size_t>(wd) * nc2;
+  const int base = blockIdx.x * CHUNK;
+  double mx = 0.0, sum = 0.0, wsum = 0.0, mnv = 1.0e308;
+  int mni = 0x7fffffff;
+  bool any = false;
+#pragma unroll 4
+  for (int k = 0; k < CHUNK / NT; ++k) {
+    const int li = k * NT + threadIdx.x;
+    const int i = base + li;
+    if (i >= n) break;
+    const double v = clip0(p[i]);
+    if (!any || v > mx) mx = v;
+    any = true;
+    sum += v;
+    wsum += static_cast<double>(li) * v;
+    if (i >= sp.botidx && i <= sp.topidx) dev::argmin_merge(mnv, mni, v, i);
+  }
+  if (!any) mx = -1.0e308;
+  mx = dev::block_max<NT>(mx, shd);
+  sum = dev::block_sum<NT>(sum, shd);
+  wsum = dev::block_sum<NT>(wsum, shd);
+  dev::block_argmin<NT>(mnv, mni, shd, shi);
+  if (threadIdx.x == 0) {
+    double* o = ppart + (static_cast<size_t>(wd) * nchunk + blockIdx.x) * 4;
+    o[0] = mx;
+    o[1] = sum;
+    o[2] = wsum;
+    o[3] = mnv;
+    pmidx[static_cast<size_t>(wd) * nchunk + blockIdx.x] = mni;
+  }
+}
+
+__device__ __forceinline__ double logp_at(const double* __restrict__ p, int n,
+                                          int split, double itot, int j) {
+  int s = j + split;
+  if (s >= n) s -= n;
+  const double v = clip0(p[s]) * itot;
+  return (v > 0.0) ? log2(v) : dev::kSmallLogVal;
+}
+
+// Split point, unwrap, normalisation, mean and the log-likelihood of one
+// (proposal, dataset): PDFactory.cc:691-1009, PD.cc:146-274, 557-677,
+// calcLike.cc:419-425.
+__global__ void __launch_bounds__(NT)
+k_pfinish1(const BSet1Dev* __restrict__ bsets,
+           const DSet1Dev* __restrict__ dsets, int B, int D, int n, int nc2,
+           int nchunk, double log2toe, const int* __restrict__ mstatus,
+           const double* __restrict__ sigmult, const double* __restrict__ mom,
+           const double* __restrict__ pbuf, const double* __restrict__ ppart,
+           const int* __restrict__ pmidx, PDInfo1* __restrict__ pinfo) {
+  __shared__ double shd[32];
+  __shared__ int shi[32];
+  __shared__ int s_state;   // 0 need search, 1 done, <0 error
+  __shared__ int s_split;
+  __shared__ double s_jitter;
+  const int wd = blockIdx.x;
+  const int w = wd / D, d = wd - w * D;
+  PDInfo1& info = pinfo[wd];
+  if (mstatus[w] != 0) {
+    if (threadIdx.x == 0) info.status = mstatus[w];
+    return;
+  }
+  const DSet1Dev& ds = dsets[d];
+  const BSet1Dev& bs = bsets[ds.bs];
+  const double var = mom[(static_cast<size_t>(w) * B + ds.bs) * 4 + 1];
+  const SplitParams sp = split_params(bs, var, sigmult[w] * ds.sigma_base);
+  const double* p = pbuf + static_cast<size_t>(wd) * nc2;
+  const double dflux = bs.dflux;
+  const double* pp = ppart + static_cast<size_t>(wd) * nchunk * 4;
+  const int* pm = pmidx + static_cast<size_t>(wd) * nchunk;
+
+  if (threadIdx.x == 0) {
+    int st = 0;
+    int split = -1;
+    double jitter = 0.0;
+    const double fluxrange = n * dflux;
+    double peak = -1.0e308, minval = 1.0e308;
+    int minidx = 0x7fffffff;
+    for (int c = 0; c < nchunk; ++c) {
+      if (pp[4 * c] > peak) peak = pp[4 * c];
+      dev::argmin_merge(minval, minidx, pp[4 * c + 3], pm[c]);
+    }
+    const long long botidx = sp.botidx, topidx = sp.topidx;
+    if (sp.sgpos <= 0 || sp.sgneg <= 0) st = POFD_E_SPLIT_RANGE;
+    else if (fluxrange < (sp.n1sigpos + sp.n1signeg)) st = POFD_E_SPLIT_RANGE;
+    // a NaN peak (non-finite P(D)) is reported here too, where the
+    // reference would carry the NaN on to its un-shift check
+    else if (!(peak > 0.0)) st = POFD_E_SPLIT_PEAK;
+    else if (botidx >= n || topidx >= n || botidx < 0 || topidx < 0) st = POFD_E_SPLIT_LOGIC;
+    if (st == 0) {
+      if (botidx > topidx) {
+        minidx = static_cast<int>(botidx);
+        minval = clip0(p[minidx]);
+      }
+      if (minidx < 0 || minidx >= n) st = POFD_E_SPLIT_MIN;  // no finite minimum
+      else if (minval > 1e-5 * peak) st = POFD_E_SPLIT_MIN;
+    }
+    if (st == 0) {
+      const int pre = 17;
+      bool found = false;
+      if (minidx > pre) {
+        bool mono = true;
+        const int initidx = minidx - pre;
+        double prevval = clip0(p[initidx]);
+        jitter = prevval;
+        for (int i = initidx + 1; i < minidx; ++i) {
+          const double cv = clip0(p[i]);
+          if (cv >= prevval) mono = false;
+          jitter += cv;
+          prevval = cv;
+        }
+        if (mono) { split = minidx; found = true; }
+        else {
+          jitter += minval;
+          jitter = 1.1 * jitter / static_cast<double>(pre + 1);
+        }
+      } else {
+        jitter = 5e-14 * peak;
+        if (minval > jitter) { split = minidx; found = true; }
+      }
+      if (!found) {
+        if (minval <= 0.0) {
+          const int nminup = 3;
+          long long bi, ti;
+          if (minidx < botidx) bi = botidx; else bi = minidx - nminup;
+          if (minidx > topidx - nminup) ti = topidx - nminup; else ti = minidx + nminup;
+          if (bi < 0) bi = 0;
+          for (long long i = bi; i < ti; ++i) {
+            const double cv = clip0(p[i]);
+            if (cv > minval) minval = cv;
+          }
+        }
+        if (minval > 0) jitter = (5.0 * minval) < jitter ? (5.0 * minval) : jitter;
+        if (botidx >= topidx) st = POFD_E_SPLIT_LOGIC;
+        else if (clip0(p[topidx]) < jitter) st = POFD_E_SPLIT_TOP;
+      }
+      if (st == 0 && found) { s_state = 1; s_split = split; }
+      else if (st == 0) { s_state = 0; s_jitter = jitter; }
+    }
+    if (st != 0) s_state = st;
+  }
+  __syncthreads();
+  int state = s_state;
+  if (state == 0) {
+    // search down from topidx-1 for the first value below the jitter level
+    const double jitter = s_jitter;
+    int found = -1;
+    for (long long top = sp.topidx - 1; top >= sp.botidx; top -= NT) {
+      const long long i = top - threadIdx.x;
+      int hit = -1;
+      if (i >= sp.botidx && clip0(p[i]) < jitter) hit = static_cast<int>(i);
+      const int m = dev::block_max_int<NT>(hit, shi);
+      if (m >= 0) { found = m; break; }
+    }
+    if (found >= 0) { state = 1; if (threadIdx.x == 0) s_split = found + 1; }
+    else state = POFD_E_SPLIT_NONE;
+    __syncthreads();
+  }
+  if (state < 0) {
+    if (threadIdx.x == 0) {
+      info.status = state;
+      info.ll = 0.0;
+    }
+    return;
+  }
+  const int split = s_split;
+  // Sum below the split: whole chunks from the partials, the rest read.
+  const int cfull = split / CHUNK;
+  double part = 0.0;
+  for (int i = cfull * CHUNK + threadIdx.x; i < split; i += NT) part += clip0(p[i]);
+  part = dev::block_sum<NT>(part, shd);
+  double S = 0.0, W = 0.0, T = 0.0;
+  for (int c = 0; c < nchunk; ++c) {
+    S += pp[4 * c + 1];
+    W += static_cast<double>(c) * CHUNK * pp[4 * c + 1] + pp[4 * c + 2];
+    if (c < cfull) T += pp[4 * c + 1];
+  }
+  T += part;
+  const double q0 = clip0(p[split]);
+  const double qlast = clip0(p[split == 0 ? n - 1 : split - 1]);
+  const double tot = (S - 0.5 * q0 - 0.5 * qlast) * dflux;
+  const double itot = 1.0 / tot;
+  const double srot = W - static_cast<double>(split) * S + static_cast<double>(n) * T;
+  const double msum = itot * (srot - 0.5 * static_cast<double>(n - 1) * qlast);
+  const double tmn = msum * dflux * dflux;
+  if (isinf(tmn) || isnan(tmn)) {
+    if (threadIdx.x == 0) { info.status = POFD_E_UNSHIFT; info.ll = 0.0; }
+    return;
+  }
+  const double minflux = -tmn;
+  const double maxflux = minflux + static_cast<double>(n - 1) * dflux;
+  const double maxfluxval = maxflux - dflux;
+  const double idflux = 1.0 / dflux;
+  double ll = 0.0;
+  if (ds.binned) {
+    for (int e = threadIdx.x; e < ds.nnz; e += NT) {
+      const double cnt = ds.nzcnt[e];
+      const double cflux = ds.bincent0 + static_cast<double>(ds.nzidx[e]) * ds.bindelta;
+      double v;
+      if (cflux < minflux) v = cnt * logp_at(p, n, split, itot, 0);
+      else if (cflux > maxfluxval) v = cnt * logp_at(p, n, split, itot, n - 1);
+      else {
+        const double delt = (cflux - minflux) * idflux;
+        const int idx = static_cast<int>(delt);
+        const double t = delt - static_cast<double>(idx);
+        v = ((1.0 - t) * logp_at(p, n, split, itot, idx) +
+             t * logp_at(p, n, split, itot, idx + 1)) * cnt;
+      }
+      ll += v;
+    }
+  } else {
+    for (int e = threadIdx.x; e < ds.nnz; e += NT) {
+      const double cflux = ds.flux[e];
+      double v;
+      if (cflux <= minflux) v = logp_at(p, n, split, itot, 0);
+      else if (cflux >= maxfluxval) v = logp_at(p, n, split, itot, n - 1);
+      else {
+        const double delt = (cflux - minflux) * idflux;
+        const int idx = static_cast<int>(delt);
+        const double t = delt - static_cast<double>(idx);
+        v = (1.0 - t) * logp_at(p, n, split, itot, idx) +
+            t * logp_at(p, n, split, itot, idx + 1);
+      }
+      ll += v;
+    }
+  }
+  ll = dev::block_sum<NT>(ll, shd);
+  if (threadIdx.x == 0) {
+    info.status = 0;
+    info.split = split;
+    info.itot = itot;
+    info.minflux = minflux;
+    info.sgpos = sp.sgpos;
+    info.sgneg = sp.sgneg;
+    info.ll = (log2toe * ll - ds.like_offset) / ds.like_norm;
+  }
+}
+
+// Per-proposal sum over beam sets and datasets in the reference's order;
+// a negative sigma multiplier gives bad_like for the beam set
+// (calcLike.cc:404, 916-920).
+__global__ void k_reduce1(const BSet1Dev* __restrict__ bsets, int B, int D,
+                          int nprop, const int* __restrict__ mstatus,
+                          const double* __restrict__ sigmult,
+                          const PDInfo1* __restrict__ pinfo,
+                          double* __restrict__ logl, int* __restrict__ status) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nprop) return;
+  if (mstatus[w] != 0) {
+    logl[w] = __longlong_as_double(0x7ff8000000000000LL);
+    status[w] = mstatus[w];
+    return;
+  }
+  const double sm = sigmult[w];
+  double LogLike = 0.0;
+  int st = 0;
+  for (int b = 0; b < B; ++b) {
+    const BSet1Dev& bs = bsets[b];
+    if (bs.maxsb * sm < 0.0) { LogLike += 1e25; continue; }
+    double s = 0.0;
+    for (int dd = 0; dd < bs.nds; ++dd) {
+      const PDInfo1& in = pinfo[static_cast<size_t>(w) * D + bs.ds_begin + dd];
+      if (in.status != 0 && st == 0) st = in.status;
+      s += in.ll;
+    }
+    LogLike += s;
+  }
+  status[w] = st;
+  logl[w] = (st == 0) ? LogLike : __longlong_as_double(0x7ff8000000000000LL);
+}
+
+// The unwrapped, normalised (optionally log2) P(D) of one row.
+__global__ void k_pdwrite1(const double* __restrict__ p, int n, int split,
+                           double itot, int setlog, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int s = i + split;
+  if (s >= n) s -= n;
+  const double v = clip0(p[s]) * itot;
+  out[i] = setlog ? ((v > 0.0) ? log2(v) : dev::kSmallLogVal) : v;
+}
+
+template <class T>
+T* dalloc(size_t n) {
+  void* p = nullptr;
+  cuda_check(cudaMalloc(&p, n * sizeof(T) + 16), "cudaMalloc");
+  return static_cast<T*>(p);
+}
+
+}  // namespace
+
+// ===================================================================== host
+
+Engine1::Engine1(int device, cudaStream_t stream)
+    : device_(device), stream_(stream) {}
+
+Engine1::~Engine1() {
+  if (device_ < 0) return;  // host-only: nothing was allocated on a GPU
+  cudaSetDevice(device_);
+  drop_graphs();
+  for (auto& kv : plans_) {
+    if (kv.second.fwd) cufftDestroy(kv.second.fwd);
+    if (kv.second.inv) cufftDestroy(kv.second.inv);
+  }
+  free_work();
+  free_static();
+}
+
+void Engine1::configure(unsigned nknots, const double* knotpos,
+                        unsigned fftsize, unsigned ninterp, bool bin_data,
+                        unsigned nbins) {
+  if (nknots < 3 || nknots > static_cast<unsigned>(KMAX))
+    throw Error(POFD_E_ARG, "nknots must be in [3, 64]");
+  for (unsigned i = 0; i < nknots; ++i)
+    if (!(knotpos[i] > 0) || (i > 0 && !(knotpos[i] > knotpos[i - 1])))
+      throw Error(POFD_E_ARG, "knot positions must be positive and increasing");
+  if (fftsize < 64) throw Error(POFD_E_ARG, "fftsize must be >= 64");
+  if (ninterp < 4 || ninterp > 8192) throw Error(POFD_E_ARG, "ninterp must be in [4, 8192]");
+  knots_.assign(knotpos, knotpos + nknots);
+  n_ = fftsize;
+  ninterp_ = ninterp;
+  bin_data_ = bin_data;
+  nbins_ = nbins;
+  static_ok_ = false;
+}
+
+int Engine1::add_beamset(const Beam1& bm, double exp_conf) {
+  HostSet s;
+  s.bm = bm;
+  s.exp_conf = exp_conf;
+  sets_.push_back(std::move(s));
+  static_ok_ = false;
+  return static_cast<int>(sets_.size()) - 1;
+}
+
+void Engine1::refresh_set(HostSet& s) {
+  s.maxsb = s.sb[0];
+  for (size_t i = 1; i < s.sb.size(); ++i)
+    if (s.sb[i] > s.maxsb) s.maxsb = s.sb[i];
+  for (size_t i = 0; i < s.data.size(); ++i) {
+    const double var = s.sb[i] * s.sb[i] + s.exp_conf * s.exp_conf;
+    if (var > 0) {
+      const double ndd = static_cast<double>(s.data[i].data.size());
+      s.lo[i] = -0.5 * ndd * (std::log(kTwoPi * var) + 1.0);
+    }
+  }
+  auto mm = s.data[0].minmax();
+  s.minDF = mm.first;
+  s.maxDF = mm.second;
+  for (size_t i = 1; i < s.data.size(); ++i) {
+    mm = s.data[i].minmax();
+    if (mm.first < s.minDF) s.minDF = mm.first;
+    if (mm.second > s.maxDF) s.maxDF = mm.second;
+  }
+  s.rr_set = false;
+}
+
+void Engine1::add_dataset(int bs, const double* data, size_t nd, bool meansub,
+                          double sigma_base, double like_norm) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size()))
+    throw Error(POFD_E_ARG, "invalid beam set index");
+  if (nd == 0) throw Error(POFD_E_ARG, "No pixels in data");
+  HostSet& s = sets_[bs];
+  Data1 d;
+  d.data.assign(data, data + nd);
+  if (meansub) d.meanSubtract();
+  if (bin_data_) d.applyBinning(nbins_);
+  s.data.push_back(std::move(d));
+  s.sb.push_back(sigma_base);
+  s.lo.push_back(0.0);
+  s.ln.push_back(like_norm);
+  refresh_set(s);
+  static_ok_ = false;
+}
+
+// calcLikeSingle::setRRange (calcLike.cc:346-371), for every beam set.
+void Engine1::set_rranges(const float* theta, unsigned npar) {
+  if (npar < knots_.size()) throw Error(POFD_E_ARG, "Number of knot values different than expected");
+  for (size_t k = 0; k < knots_.size(); ++k)
+    if (std::isnan(static_cast<double>(theta[k])))
+      throw Error(POFD_E_INVALID_MODEL, "Model is not valid");
+  const double safetyfac = 1.05;
+  for (auto& s : sets_) {
+    if (s.data.empty()) throw Error(POFD_E_ARG, "Data not loaded");
+    const auto raw = rrange_knots(knots_.back(), s.bm);
+    const double sigma = std::sqrt(s.exp_conf * s.exp_conf + s.maxsb * s.maxsb);
+    s.minR = safetyfac * raw.first;
+    s.maxR = safetyfac * raw.second + kNZeroPad * sigma;
+    if (s.minDF < s.minR && s.bm.hasneg) s.minR = s.minDF;
+    if (s.maxDF > s.maxR && s.bm.haspos) s.maxR = s.maxDF;
+    s.rr_set = true;
+  }
+  static_ok_ = false;
+}
+
+// A dataset without pixels whose noise level is set per call: the P(D)
+// factory path (getPD(sigma)) runs through the same kernels with it.
+void Engine1::add_virtual_dataset(int bs, double sigma_base) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size()))
+    throw Error(POFD_E_ARG, "invalid beam set index");
+  HostSet& s = sets_[bs];
+  Data1 d;
+  d.binned = true;
+  d.nbins = 0;
+  s.data.push_back(std::move(d));
+  s.sb.push_back(sigma_base);
+  s.lo.push_back(0.0);
+  s.ln.push_back(1.0);
+  s.maxsb = sigma_base;
+  static_ok_ = false;
+}
+
+void Engine1::set_virtual_sigma(int bs, double sigma) {
+  HostSet& s = sets_.at(bs);
+  s.sb.back() = sigma;
+  s.maxsb = sigma;
+  if (!static_ok_) return;
+  const int d = h_bsets_[bs].ds_begin + h_bsets_[bs].nds - 1;
+  h_dsets_[d].sigma_base = sigma;
+  h_bsets_[bs].maxsb = sigma;
+  cuda_check(cudaMemcpy(d_dsets_ + d, &h_dsets_[d], sizeof(DSet1Dev), cudaMemcpyHostToDevice), "upload");
+  cuda_check(cudaMemcpy(d_bsets_ + bs, &h_bsets_[bs], sizeof(BSet1Dev), cudaMemcpyHostToDevice), "upload");
+}
+
+void Engine1::set_rrange_explicit(int bs, double minR, double maxR) {
+  HostSet& s = sets_.at(bs);
+  s.minR = minR;
+  s.maxR = maxR;
+  s.rr_set = true;
+  static_ok_ = false;
+}
+
+std::pair<double, double> Engine1::rrange(int bs) const {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size()))
+    throw Error(POFD_E_ARG, "invalid beam set index");
+  return {sets_[bs].minR, sets_[bs].maxR};
+}
+
+void Engine1::dataset_info(int bs, int ds, double* o, uint32_t* bins) const {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size()))
+    throw Error(POFD_E_ARG, "invalid beam set index");
+  const HostSet& s = sets_[bs];
+  if (ds < 0 || ds >= static_cast<int>(s.data.size()))
+    throw Error(POFD_E_ARG, "invalid dataset index");
+  const Data1& d = s.data[ds];
+  if (o) {
+    o[0] = static_cast<double>(d.data.size());
+    o[1] = d.nbins;
+    o[2] = d.bincent0;
+    o[3] = d.bindelta;
+    o[4] = s.lo[ds];
+    o[5] = s.sb[ds];
+    o[6] = s.ln[ds];
+    o[7] = s.minDF;
+    o[8] = s.maxDF;
+  }
+  if (bins && d.binned) std::memcpy(bins, d.bins.data(), d.bins.size() * sizeof(uint32_t));
+}
+
+void Engine1::free_static() {
+  for (void* p : static_allocs_) cudaFree(p);
+  static_allocs_.clear();
+  d_bsets_ = nullptr;
+  d_dsets_ = nullptr;
+  static_ok_ = false;
+}
+
+// Upload the parameter-independent data: beam terms, interpolation nodes
+// and their spline factorisation, grid ranges, binned data.
+void Engine1::build_static() {
+  if (device_ < 0) throw Error(POFD_E_CUDA, "host-only context has no GPU");
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  free_static();
+  if (sets_.empty()) throw Error(POFD_E_ARG, "no beam sets");
+  auto up = [&](const std::vector<double>& v) -> const double* {
+    double* p = dalloc<double>(v.size() ? v.size() : 1);
+    static_allocs_.push_back(p);
+    if (!v.empty())
+      cuda_check(cudaMemcpy(p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice), "upload");
+    return p;
+  };
+  auto upi = [&](const std::vector<int>& v) -> const int* {
+    int* p = dalloc<int>(v.size() ? v.size() : 1);
+    static_allocs_.push_back(p);
+    if (!v.empty())
+      cuda_check(cudaMemcpy(p, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice), "upload");
+    return p;
+  };
+  const unsigned K = static_cast<unsigned>(knots_.size());
+  std::vector<double> lk(K);
+  for (unsigned i = 0; i < K; ++i) lk[i] = std::log2(knots_[i]);
+  model_.K = static_cast<int>(K);
+  model_.logknots = up(lk);
+  model_.minknot = knots_.front();
+  model_.maxknot = knots_.back();
+
+  B_ = static_cast<unsigned>(sets_.size());
+  maxterms_ = 1;
+  h_bsets_.assign(B_, BSet1Dev{});
+  h_dsets_.clear();
+  const unsigned NI = ninterp_;
+  const double ininterpm1 = 1.0 / static_cast<double>(NI - 1);
+  const double subedgemult = 1e-5;  // PDFactory.h:30
+  for (unsigned b = 0; b < B_; ++b) {
+    HostSet& s = sets_[b];
+    if (!s.rr_set) throw Error(POFD_E_ARG, "R range not set");
+    if (s.data.empty()) throw Error(POFD_E_ARG, "Data not loaded");
+    const double maxflux = s.maxR, minflux = s.minR;
+    if (maxflux <= 0.0) throw Error(POFD_E_ARG, "Invalid (non-positive) maxflux");
+    if (minflux == maxflux) throw Error(POFD_E_ARG, "Invalid (0) range between min/max flux");
+    RGrid1 g;
+    g.init(n_, minflux, maxflux);
+    BSet1Dev& bd = h_bsets_[b];
+    double prefac = s.bm.pixsize / 3600.0;
+    prefac = prefac * prefac;
+    bd.prefac = prefac;
+    const auto rr = rrange_knots(knots_.back(), s.bm);
+    bd.rr_lo = rr.first;
+    bd.rr_hi = rr.second;
+    bd.haspos = s.bm.haspos;
+    bd.hasneg = s.bm.hasneg;
+    bd.dflux = g.dflux;
+    bd.minflux_R = g.minflux_R;
+    bd.wrapRidx = static_cast<int>(g.wrapRidx);
+    bd.maxsb = s.maxsb;
+    for (int side = 0; side < 2; ++side) {
+      Side1Dev& sd = bd.side[side];
+      sd.nodes = 0;
+      sd.grid_lo = 1;
+      sd.grid_hi = 0;
+      sd.grid_off = 0.0;
+      const bool has = side == 0 ? s.bm.haspos : s.bm.hasneg;
+      if (!has) continue;
+      std::vector<double> x(NI);
+      if (side == 0) {
+        const double mini = knots_.front() * subedgemult;
+        double maxi = knots_.back() * s.bm.maxpos();
+        const double dinterp = 0.001 * (maxi - mini) * ininterpm1;
+        maxi -= dinterp;
+        const double dif = (std::log2(maxi / mini)) * ininterpm1;
+        for (unsigned i = 0; i < NI; ++i) x[i] = mini * std::exp2(static_cast<double>(i) * dif);
+      } else {
+        double maxi = -knots_.front() * subedgemult;
+        double mini = -knots_.back() * s.bm.maxneg();
+        const double dinterp = 0.001 * (maxi - mini) * ininterpm1;
+        mini += dinterp;
+        maxi -= dinterp;
+        const double dif = (std::log2(mini / maxi)) * ininterpm1;
+        for (unsigned i = 0; i < NI; ++i)
+          x[i] = maxi * std::exp2(static_cast<double>(NI - i - 1) * dif);
+      }
+      SplineSystem sys;
+      sys.factor(x);
+      std::vector<double> tw, tie;
+      s.bm.terms(side == 1, tw, tie);
+      if (tie.size() > static_cast<size_t>(MAXTERMS))
+        throw Error(POFD_E_ARG, "beam has too many terms; histogram it");
+      sd.nodes = 1;
+      sd.nterms = static_cast<int>(tie.size());
+      if (sd.nterms > maxterms_) maxterms_ = sd.nterms;
+      sd.w = up(tw);
+      sd.ieta = up(tie);
+      sd.x = up(sys.x);
+      sd.ih = up(sys.ih);
+      sd.alpha = up(sys.alpha);
+      sd.gamma = up(sys.gamma);
+      // grid ranges (PDFactory.cc:563-606)
+      if (side == 0 && maxflux > 0) {
+        const double minI = x[0], maxI = x[NI - 1];
+        const unsigned lo = static_cast<unsigned>(minI / g.dflux + 0.9999999999999999);
+        unsigned hi = static_cast<unsigned>(maxI / g.dflux);
+        if (hi > g.wrapRidx) hi = g.wrapRidx;
+        sd.grid_lo = static_cast<int>(lo);
+        sd.grid_hi = static_cast<int>(hi);
+        sd.grid_off = 0.0;
+      }
+      if (side == 1 && minflux < 0 && g.wrapRidx > 0) {
+        const double minI = x[0], maxI = x[NI - 1];
+        unsigned lo = static_cast<unsigned>((minI - g.minflux_R) / g.dflux + g.wrapRidx + 1 + 0.9999999999999999);
+        if (lo <= g.wrapRidx) lo = g.wrapRidx + 1;
+        unsigned hi = static_cast<unsigned>((maxI - g.minflux_R) / g.dflux + g.wrapRidx + 1);
+        if (hi > n_ - 1) hi = n_ - 1;
+        sd.grid_lo = static_cast<int>(lo);
+        sd.grid_hi = static_cast<int>(hi);
+        sd.grid_off = g.minflux_R - static_cast<double>(g.wrapRidx + 1) * g.dflux;
+      }
+    }
+    bd.ds_begin = static_cast<int>(h_dsets_.size());
+    bd.nds = static_cast<int>(s.data.size());
+    for (size_t i = 0; i < s.data.size(); ++i) {
+      const Data1& d = s.data[i];
+      DSet1Dev dd{};
+      dd.bs = static_cast<int>(b);
+      dd.sigma_base = s.sb[i];
+      dd.like_offset = s.lo[i];
+      dd.like_norm = s.ln[i];
+      dd.binned = d.binned ? 1 : 0;
+      if (d.binned) {
+        std::vector<int> idx;
+        std::vector<double> cnt;
+        for (unsigned k = 0; k < d.nbins; ++k)
+          if (d.bins[k]) { idx.push_back(static_cast<int>(k)); cnt.push_back(static_cast<double>(d.bins[k])); }
+        dd.nnz = static_cast<int>(idx.size());
+        dd.nzidx = upi(idx);
+        dd.nzcnt = up(cnt);
+        dd.flux = nullptr;
+        dd.bincent0 = d.bincent0;
+        dd.bindelta = d.bindelta;
+      } else {
+        dd.nnz = static_cast<int>(d.data.size());
+        dd.flux = up(d.data);
+        dd.nzidx = nullptr;
+        dd.nzcnt = nullptr;
+      }
+      h_dsets_.push_back(dd);
+    }
+  }
+  D_ = static_cast<unsigned>(h_dsets_.size());
+  d_bsets_ = dalloc<BSet1Dev>(B_);
+  static_allocs_.push_back(d_bsets_);
+  cuda_check(cudaMemcpy(d_bsets_, h_bsets_.data(), B_ * sizeof(BSet1Dev), cudaMemcpyHostToDevice), "upload");
+  d_dsets_ = dalloc<DSet1Dev>(D_);
+  static_allocs_.push_back(d_dsets_);
+  cuda_check(cudaMemcpy(d_dsets_, h_dsets_.data(), D_ * sizeof(DSet1Dev), cudaMemcpyHostToDevice), "upload");
+  ntile_ = (n_ + TILE - 1) / TILE;
+  nchunk_ = (n_ + CHUNK - 1) / CHUNK;
+  static_ok_ = true;
+  // shapes changed: old plans/graphs/work space no longer match
+  drop_graphs();
+  for (auto& kv : plans_) {
+    if (kv.second.fwd) cufftDestroy(kv.second.fwd);
+    if (kv.second.inv) cufftDestroy(kv.second.inv);
+  }
+  plans_.clear();
+  const unsigned P = ws_.P;
+  free_work();
+  if (P) reserve(P);
+}
+
+void Engine1::drop_graphs() {
+  for (auto& kv : plans_) {
+    for (auto& g : kv.second.graphs) cudaGraphExecDestroy(g.second);
+    kv.second.graphs.clear();
+  }
+}
+
+// Times each stage of one launch sequence with CUDA events, reps times.
+void Engine1::profile_stages(unsigned nprop, const float* theta, unsigned npar,
+                             int reps, double* stage_ms) {
+  double ll;
+  std::vector<double> lls(nprop);
+  std::vector<int> sts(nprop);
+  eval_host(nprop, theta, npar, lls.data(), sts.data());  // staging + warm
+  cudaEvent_t ev[kNumStages + 1];
+  for (auto& e : ev) cuda_check(cudaEventCreate(&e), "event create");
+  for (int k = 0; k < kNumStages; ++k) stage_ms[k] = 0.0;
+  (void)ll;
+  for (int r = 0; r < reps; ++r) {
+    launch_all(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_, ev);
+    cuda_check(cudaStreamSynchronize(stream_), "synchronize");
+    for (int k = 0; k < kNumStages; ++k) {
+      float ms = 0.f;
+      cuda_check(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]), "elapsed");
+      stage_ms[k] += ms / reps;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+}
+
+const char* Engine1::stage_name(int i) {
+  static const char* names[kNumStages] = {
+      "k_model1", "k_rnodes1", "k_rspline1", "k_rfill1", "k_moments1",
+      "cufft_d2z", "k_spectrum1", "cufft_z2d", "k_pscan1", "k_pfinish1",
+      "k_reduce1"};
+  return (i >= 0 && i < kNumStages) ? names[i] : "";
+}
+
+void Engine1::free_work() {
+  void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.nodes, ws_.spl,
+                  ws_.rbuf, ws_.rpart, ws_.mom, ws_.pbuf, ws_.ppart,
+                  ws_.pmidx, ws_.pinfo, ws_.pdout, ws_.theta_in, ws_.logl,
+                  ws_.status};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
+  if (ws_.h_logl) cudaFreeHost(ws_.h_logl);
+  if (ws_.h_status) cudaFreeHost(ws_.h_status);
+  ws_ = Workspace1{};
+}
+
+void Engine1::reserve(unsigned P) {
+  if (P == 0) throw Error(POFD_E_ARG, "max_batch must be > 0");
+  if (!static_ok_) {
+    ws_.P = std::max(ws_.P, P);
+    build_static();  // calls reserve again with the stored capacity
+    return;
+  }
+  if (ws_.P >= P && ws_.rbuf) return;
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  free_work();
+  drop_graphs();
+  const size_t nc2 = 2 * (static_cast<size_t>(n_) / 2 + 1);
+  const size_t NI = ninterp_;
+  ws_.P = P;
+  ws_.cnt = dalloc<double>(static_cast<size_t>(P) * 4 * KMAX);
+  ws_.mstatus = dalloc<int>(P);
+  ws_.sigmult = dalloc<double>(P);
+  ws_.nodes = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * NI);
+  ws_.spl = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * 4 * NI);
+  ws_.rbuf = dalloc<double>(static_cast<size_t>(P) * B_ * nc2);
+  ws_.rpart = dalloc<double>(static_cast<size_t>(P) * B_ * ntile_ * 2);
+  ws_.mom = dalloc<double>(static_cast<size_t>(P) * B_ * 4);
+  ws_.pbuf = dalloc<double>(static_cast<size_t>(P) * D_ * nc2);
+  ws_.ppart = dalloc<double>(static_cast<size_t>(P) * D_ * nchunk_ * 4);
+  ws_.pmidx = dalloc<int>(static_cast<size_t>(P) * D_ * nchunk_);
+  ws_.pinfo = dalloc<PDInfo1>(static_cast<size_t>(P) * D_);
+  ws_.pdout = dalloc<double>(n_);
+  ws_.logl = dalloc<double>(P);
+  ws_.status = dalloc<int>(P);
+  cuda_check(cudaFuncSetAttribute(k_rnodes1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>((KMAX + 4 * KMAX + 2 * MAXTERMS) * sizeof(double))),
+             "smem attribute");
+  cuda_check(cudaFuncSetAttribute(k_rspline1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>((2 * 8192 + 2 * NT) * sizeof(double))),
+             "smem attribute");
+  cuda_check(cudaMemset(ws_.nodes, 0, static_cast<size_t>(P) * B_ * 2 * NI * sizeof(double)), "memset");
+}
+
+void Engine1::ensure_plans(unsigned nprop) {
+  auto it = plans_.find(nprop);
+  if (it != plans_.end() && it->second.fwd) return;
+  Plans pl;
+  int n = static_cast<int>(n_);
+  const int nc = n / 2 + 1;
+  int inemb[1] = {2 * nc}, onemb[1] = {nc};
+  cufft_check(cufftPlanMany(&pl.fwd, 1, &n, inemb, 1, 2 * nc, onemb, 1, nc,
+                            CUFFT_D2Z, static_cast<int>(nprop * B_)),
+              "cufftPlanMany D2Z");
+  int inemb2[1] = {nc}, onemb2[1] = {2 * nc};
+  cufft_check(cufftPlanMany(&pl.inv, 1, &n, inemb2, 1, nc, onemb2, 1, 2 * nc,
+                            CUFFT_Z2D, static_cast<int>(nprop * D_)),
+              "cufftPlanMany Z2D");
+  plans_[nprop] = pl;
+}
+
+void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
+                         double* logl, int* status, cudaStream_t st,
+                         cudaEvent_t* ev) {
+  // ev (optional): kNumStages+1 events recorded between the stages
+  auto mark = [&](int i) {
+    if (ev) cuda_check(cudaEventRecord(ev[i], st), "event record");
+  };
+  const int NI = static_cast<int>(ninterp_);
+  const int n = static_cast<int>(n_);
+  const int nc = n / 2 + 1;
+  const int nc2 = 2 * nc;
+  const int P = static_cast<int>(nprop);
+  const int B = static_cast<int>(B_), D = static_cast<int>(D_);
+  Plans& pl = plans_.at(nprop);
+
+  mark(0);
+  k_model1<<<(P + 63) / 64, 64, 0, st>>>(model_, theta, static_cast<int>(npar), P,
+                                          std::log2(10.0), ws_.cnt, ws_.mstatus,
+                                          ws_.sigmult);
+  mark(1);
+  {
+    const size_t smem = (KMAX + 4 * KMAX + 2 * static_cast<size_t>(maxterms_)) * sizeof(double);
+    dim3 grid((NI + 127) / 128, P * B * 2);
+    k_rnodes1<<<grid, 128, smem, st>>>(d_bsets_, model_, B, NI, maxterms_,
+                                       ws_.cnt, ws_.mstatus, ws_.nodes);
+  }
+  mark(2);
+  {
+    const size_t smem = (2 * static_cast<size_t>(NI) + 2 * NT) * sizeof(double);
+    k_rspline1<<<P * B * 2, NT, smem, st>>>(d_bsets_, B, NI, ws_.mstatus,
+                                            ws_.nodes, ws_.spl);
+  }
+  mark(3);
+  {
+    dim3 grid(ntile_, P * B);
+    k_rfill1<<<grid, NT, 0, st>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+                                  ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+  }
+  mark(4);
+  k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, B, n, nc2,
+                                                  static_cast<int>(ntile_), P * B,
+                                                  ws_.mstatus, ws_.rbuf,
+                                                  ws_.rpart, ws_.mom);
+  mark(5);
+  cufft_check(cufftSetStream(pl.fwd, st), "cufftSetStream");
+  cufft_check(cufftExecD2Z(pl.fwd, ws_.rbuf, reinterpret_cast<cufftDoubleComplex*>(ws_.rbuf)),
+              "cufftExecD2Z");
+  mark(6);
+  {
+    dim3 grid((nc + NT - 1) / NT, P * B);
+    k_spectrum1<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc, ws_.mstatus,
+                                     ws_.sigmult, ws_.mom, ws_.rbuf, ws_.pbuf);
+  }
+  mark(7);
+  cufft_check(cufftSetStream(pl.inv, st), "cufftSetStream");
+  cufft_check(cufftExecZ2D(pl.inv, reinterpret_cast<cufftDoubleComplex*>(ws_.pbuf), ws_.pbuf),
+              "cufftExecZ2D");
+  mark(8);
+  {
+    dim3 grid(nchunk_, P * D);
+    k_pscan1<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
+                                  static_cast<int>(nchunk_), ws_.mstatus,
+                                  ws_.sigmult, ws_.mom, ws_.pbuf, ws_.ppart,
+                                  ws_.pmidx);
+  }
+  mark(9);
+  k_pfinish1<<<P * D, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
+                                   static_cast<int>(nchunk_), std::log(2.0),
+                                   ws_.mstatus, ws_.sigmult, ws_.mom, ws_.pbuf,
+                                   ws_.ppart, ws_.pmidx, ws_.pinfo);
+  mark(10);
+  k_reduce1<<<(P + 127) / 128, 128, 0, st>>>(d_bsets_, B, D, P, ws_.mstatus,
+                                            ws_.sigmult, ws_.pinfo, logl, status);
+  mark(11);
+  cuda_check(cudaGetLastError(), "kernel launch");
+}
+
+// Replays a CUDA graph of the whole launch sequence for these pointers,
+// captured on the first call that sees them.  If the caller's stream is
+// itself being captured, the launches are recorded into the caller's graph.
+void Engine1::enqueue(unsigned nprop, const float* theta_dev, unsigned npar,
+                      double* logl_dev, int* status_dev, cudaStream_t st) {
+  if (nprop == 0) return;
+  if (npar < knots_.size() + 1) throw Error(POFD_E_ARG, "Not enough elements in paramSet");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  ensure_plans(nprop);
+  if (!st) st = stream_;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cuda_check(cudaStreamIsCapturing(st, &cs), "cudaStreamIsCapturing");
+  if (cs != cudaStreamCaptureStatusNone) {
+    launch_all(nprop, theta_dev, npar, logl_dev, status_dev, st, nullptr);
+    return;
+  }
+  cudaGraphExec_t g = graph_for(nprop, theta_dev, npar, logl_dev, status_dev);
+  if (g) cuda_check(cudaGraphLaunch(g, st), "graph launch");
+  else launch_all(nprop, theta_dev, npar, logl_dev, status_dev, st, nullptr);
+}
+
+cudaGraphExec_t Engine1::graph_for(unsigned nprop, const float* theta,
+                                   unsigned npar, double* logl, int* status) {
+  Plans& pl = plans_.at(nprop);
+  if (pl.no_graph) return nullptr;
+  const GraphKey key{theta, npar, logl, status};
+  for (auto& kv : pl.graphs)
+    if (kv.first == key) return kv.second;
+  if (!pl.warmed) {  // first use of this batch size runs eagerly
+    pl.warmed = true;
+    return nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    bool threw = false;
+    try {
+      launch_all(nprop, theta, npar, logl, status, stream_, nullptr);
+    } catch (...) {
+      threw = true;
+    }
+    const cudaError_t ec = cudaStreamEndCapture(stream_, &g);
+    if (threw || ec != cudaSuccess || !g || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+      ge = nullptr;
+    if (g) cudaGraphDestroy(g);
+  }
+  cudaGetLastError();
+  if (!ge) {
+    pl.no_graph = true;  // cannot be captured: always run eagerly
+    return nullptr;
+  }
+  if (pl.graphs.size() >= 8) {
+    cudaGraphExecDestroy(pl.graphs.front().second);
+    pl.graphs.erase(pl.graphs.begin());
+  }
+  pl.graphs.push_back({key, ge});
+  return ge;
+}
+
+void Engine1::eval_host(unsigned nprop, const float* theta, unsigned npar,
+                        double* logl, int* status) {
+  if (nprop == 0) return;
+  if (npar < knots_.size() + 1) throw Error(POFD_E_ARG, "Not enough elements in paramSet");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  if (!ws_.theta_in || ws_.h_npar < npar) {
+    if (ws_.theta_in) cudaFree(ws_.theta_in);
+    if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
+    ws_.theta_in = dalloc<float>(static_cast<size_t>(ws_.P) * npar);
+    cuda_check(cudaMallocHost(&ws_.h_theta, static_cast<size_t>(ws_.P) * npar * sizeof(float)), "cudaMallocHost");
+    ws_.h_npar = npar;
+    drop_graphs();
+  }
+  if (!ws_.h_logl) {
+    cuda_check(cudaMallocHost(&ws_.h_logl, ws_.P * sizeof(double)), "cudaMallocHost");
+    cuda_check(cudaMallocHost(&ws_.h_status, ws_.P * sizeof(int)), "cudaMallocHost");
+  }
+  std::memcpy(ws_.h_theta, theta, static_cast<size_t>(nprop) * npar * sizeof(float));
+  cuda_check(cudaMemcpyAsync(ws_.theta_in, ws_.h_theta,
+                             static_cast<size_t>(nprop) * npar * sizeof(float),
+                             cudaMemcpyHostToDevice, stream_), "H2D theta");
+  enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);
+  cuda_check(cudaMemcpyAsync(ws_.h_logl, ws_.logl, nprop * sizeof(double),
+                             cudaMemcpyDeviceToHost, stream_), "D2H logl");
+  cuda_check(cudaMemcpyAsync(ws_.h_status, ws_.status, nprop * sizeof(int),
+                             cudaMemcpyDeviceToHost, stream_), "D2H status");
+  cuda_check(cudaStreamSynchronize(stream_), "synchronize");
+  std::memcpy(logl, ws_.h_logl, nprop * sizeof(double));
+  std::memcpy(status, ws_.h_status, nprop * sizeof(int));
+}
+
+int Engine1::pd_host(int bs, int ds, const float* theta, unsigned npar,
+                     bool setlog, double* pd_out, double* info12) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size())) throw Error(POFD_E_ARG, "invalid beam set index");
+  if (ds < 0 || ds >= static_cast<int>(sets_[bs].data.size())) throw Error(POFD_E_ARG, "invalid dataset index");
+  double ll;
+  int st;
+  eval_host(1, theta, npar, &ll, &st);
+  const int d = h_bsets_[bs].ds_begin + ds;
+  PDInfo1 info;
+  cuda_check(cudaMemcpy(&info, ws_.pinfo + d, sizeof(PDInfo1), cudaMemcpyDeviceToHost), "D2H info");
+  double mom[4] = {0, 0, 0, 0};
+  cuda_check(cudaMemcpy(mom, ws_.mom + static_cast<size_t>(bs) * 4, sizeof(mom), cudaMemcpyDeviceToHost), "D2H mom");
+  if (info12) {
+    const BSet1Dev& b = h_bsets_[bs];
+    info12[0] = b.dflux; info12[1] = b.minflux_R; info12[2] = b.wrapRidx;
+    info12[3] = mom[0]; info12[4] = mom[1]; info12[5] = mom[3]; info12[6] = mom[2];
+    info12[7] = info.split; info12[8] = info.sgpos; info12[9] = info.sgneg;
+    info12[10] = info.minflux; info12[11] = 0.0;
+  }
+  const int bst = info.status;
+  if (bst != 0) return bst;
+  const size_t nc2 = 2 * (static_cast<size_t>(n_) / 2 + 1);
+  k_pdwrite1<<<(n_ + 255) / 256, 256, 0, stream_>>>(ws_.pbuf + static_cast<size_t>(d) * nc2,
+                                                    static_cast<int>(n_), info.split, info.itot,
+                                                    setlog ? 1 : 0, ws_.pdout);
+  cuda_check(cudaGetLastError(), "pdwrite");
+  cuda_check(cudaMemcpyAsync(pd_out, ws_.pdout, n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H pd");
+  cuda_check(cudaStreamSynchronize(stream_), "synchronize");
+  return 0;
+}
+
+void Engine1::rnodes_host(int bs, int side, const float* theta, unsigned npar,
+                          double* x_out, double* r_out) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size())) throw Error(POFD_E_ARG, "invalid beam set index");
+  double ll;
+  int st;
+  eval_host(1, theta, npar, &ll, &st);
+  const Side1Dev& sd = h_bsets_[bs].side[side & 1];
+  if (!sd.nodes) throw Error(POFD_E_ARG, "beam has no such side");
+  const size_t NI = ninterp_;
+  cuda_check(cudaMemcpy(x_out, sd.x, NI * sizeof(double), cudaMemcpyDeviceToHost), "D2H x");
+  cuda_check(cudaMemcpy(r_out, ws_.nodes + (static_cast<size_t>(bs) * 2 + (side & 1)) * NI,
+                        NI * sizeof(double), cudaMemcpyDeviceToHost), "D2H R");
+}
+
+void Engine1::rgrid_host(int bs, const float* theta, unsigned npar, double* out) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size())) throw Error(POFD_E_ARG, "invalid beam set index");
+  if (!static_ok_ || ws_.P < 1) reserve(std::max(1u, ws_.P));
+  if (!ws_.theta_in || ws_.h_npar < npar) {
+    double ll;
+    int st;
+    eval_host(1, theta, npar, &ll, &st);  // allocates staging
+  }
+  cuda_check(cudaMemcpy(ws_.theta_in, theta, npar * sizeof(float), cudaMemcpyHostToDevice), "H2D");
+  const int NI = static_cast<int>(ninterp_), n = static_cast<int>(n_);
+  const int nc2 = 2 * (n / 2 + 1);
+  const int B = static_cast<int>(B_);
+  k_model1<<<1, 64, 0, stream_>>>(model_, ws_.theta_in, static_cast<int>(npar), 1, std::log2(10.0),
+                                  ws_.cnt, ws_.mstatus, ws_.sigmult);
+  k_rnodes1<<<dim3((NI + 127) / 128, B * 2), 128,
+              (KMAX + 4 * KMAX + 2 * static_cast<size_t>(maxterms_)) * sizeof(double), stream_>>>(
+      d_bsets_, model_, B, NI, maxterms_, ws_.cnt, ws_.mstatus, ws_.nodes);
+  k_rspline1<<<B * 2, NT, (2 * static_cast<size_t>(NI) + 2 * NT) * sizeof(double), stream_>>>(
+      d_bsets_, B, NI, ws_.mstatus, ws_.nodes, ws_.spl);
+  k_rfill1<<<dim3(ntile_, B), NT, 0, stream_>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+                                                ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+  cuda_check(cudaGetLastError(), "rgrid kernels");
+  cuda_check(cudaMemcpyAsync(out, ws_.rbuf + static_cast<size_t>(bs) * nc2, n_ * sizeof(double),
+                             cudaMemcpyDeviceToHost, stream_), "D2H R grid");
+  cuda_check(cudaStreamSynchronize(stream_), "synchronize");
+}
+
+}  // namespace pofd

@@ -1,0 +1,207 @@
+// engine1d.cuh -- batched 1D P(D) likelihood engine (host class).
+//
+// One Engine1 evaluates calcLike::getLogLike (calcLike.cc:884-955) for a
+// batch of proposals in one stream-ordered sequence of launches: model set-up,
+// R at the interpolation nodes, the node spline, the wrapped R grid with its
+// moments, a batched D2Z, the spectrum (exp/shift/noise, one output per
+// dataset), a batched Z2D, the P(D) reduction/split pass and the finishing
+// kernel (split point, normalisation, mean, binned log-likelihood), then the
+// per-proposal sum.  The sequence is captured once per batch size into a CUDA
+// graph and replayed.
+#ifndef POFD_ENGINE1D_CUH
+#define POFD_ENGINE1D_CUH
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "setup.hh"
+
+namespace pofd {
+
+// ---- device-side descriptors (plain structs, arrays live in device memory)
+struct Side1Dev {
+  int nodes;        // 1 if this side's R nodes are computed (beam has it)
+  int nterms;       // beam terms summed by R
+  const double* w;  // term weights
+  const double* ieta;
+  const double* x;      // ninterp node fluxes
+  const double* ih;     // 1/(x[i+1]-x[i])
+  const double* alpha;  // LDL^T diagonal (ninterp-2)
+  const double* gamma;  // LDL^T sub-diagonal ratio (ninterp-2)
+  int grid_lo, grid_hi; // inclusive grid index range filled from this side
+  double grid_off;      // grid flux = i*dflux + grid_off
+};
+
+struct BSet1Dev {
+  Side1Dev side[2];
+  double prefac;        // (pixsize/3600)^2
+  double rr_lo, rr_hi;  // R range of the model over this beam
+  int haspos, hasneg;
+  double dflux, minflux_R;
+  int wrapRidx;
+  double maxsb;         // max sigma_base of the set
+  int ds_begin, nds;
+};
+
+struct DSet1Dev {
+  int bs;
+  double sigma_base, like_offset, like_norm;
+  int binned;
+  int nnz;               // nonzero bins (binned) or pixels (unbinned)
+  const int* nzidx;      // bin indices of nonzero bins
+  const double* nzcnt;   // their counts
+  const double* flux;    // unbinned pixel values
+  double bincent0, bindelta;
+};
+
+struct Model1Dev {
+  int K;
+  const double* logknots;  // log2 knot positions
+  double minknot, maxknot;
+};
+
+// Per-(proposal, dataset) record written by the finishing kernel.
+struct PDInfo1 {
+  int status;
+  int split;
+  double itot;     // 1 / trapezoid integral of the unwrapped P(D)
+  double minflux;  // flux of the first unwrapped element (-mean)
+  double sgpos, sgneg;
+  double ll;       // (logL - like_offset) / like_norm
+  double pad;
+};
+
+struct Workspace1 {
+  unsigned P = 0;  // capacity (proposals)
+  double* theta = nullptr;   // unused: theta is read from the caller pointer
+  double* cnt = nullptr;     // [P][4*KMAX] model spline: y, b, c, d per knot
+  int* mstatus = nullptr;    // [P] model status
+  double* sigmult = nullptr; // [P]
+  double* nodes = nullptr;   // [P][B][2][NI] R at nodes -> log2 R
+  double* spl = nullptr;     // [P][B][2][4][NI] spline y,b,c,d per interval
+  double* rbuf = nullptr;    // [P][B][2*(n/2+1)] R grid / spectrum
+  double* rpart = nullptr;   // [P][B][ntile][2]
+  double* mom = nullptr;     // [P][B][4] mean, var, shift, doshift
+  double* pbuf = nullptr;    // [P][D][2*(n/2+1)] spectrum / P(D)
+  double* ppart = nullptr;   // [P][D][nchunk][4] max, sum, wsum, minval
+  int* pmidx = nullptr;      // [P][D][nchunk] argmin index
+  PDInfo1* pinfo = nullptr;  // [P][D]
+  double* pdout = nullptr;   // [n] one P(D) for the full-array path
+  float* theta_in = nullptr; // [P][npar] staging for host calls
+  double* logl = nullptr;    // [P]
+  int* status = nullptr;     // [P]
+  // pinned host staging
+  float* h_theta = nullptr;
+  double* h_logl = nullptr;
+  int* h_status = nullptr;
+  unsigned h_npar = 0;
+};
+
+class Engine1 {
+ public:
+  static constexpr int KMAX = 64;
+  Engine1(int device, cudaStream_t stream);
+  ~Engine1();
+
+  // configuration (host set-up)
+  void configure(unsigned nknots, const double* knotpos, unsigned fftsize,
+                 unsigned ninterp, bool bin_data, unsigned nbins);
+  int add_beamset(const Beam1& bm, double exp_conf);
+  void add_dataset(int bs, const double* data, size_t nd, bool meansub,
+                   double sigma_base, double like_norm);
+  void set_rranges(const float* theta, unsigned npar);
+  void set_rrange_explicit(int bs, double minR, double maxR);
+  void add_virtual_dataset(int bs, double sigma_base);
+  void set_virtual_sigma(int bs, double sigma);
+  std::pair<double, double> rrange(int bs) const;
+  void dataset_info(int bs, int ds, double* info9, uint32_t* bins) const;
+
+  // device preparation
+  void reserve(unsigned max_batch);
+  // enqueue a batch (device pointers)
+  void enqueue(unsigned nprop, const float* theta_dev, unsigned npar,
+               double* logl_dev, int* status_dev, cudaStream_t st);
+  // host convenience: H2D theta, graph launch, D2H results, synchronize
+  void eval_host(unsigned nprop, const float* theta, unsigned npar,
+                 double* logl, int* status);
+  // P(D) of one dataset for one proposal
+  int pd_host(int bs, int ds, const float* theta, unsigned npar, bool setlog,
+              double* pd_out, double* info12);
+  void rnodes_host(int bs, int side, const float* theta, unsigned npar,
+                   double* x_out, double* r_out);
+  void rgrid_host(int bs, const float* theta, unsigned npar, double* out);
+  int kernels_per_eval() const { return 9; }
+  static constexpr int kNumStages = 11;
+  void profile_stages(unsigned nprop, const float* theta, unsigned npar,
+                      int reps, double* stage_ms);
+  static const char* stage_name(int i);
+  unsigned fftsize() const { return n_; }
+  unsigned nknots() const { return static_cast<unsigned>(knots_.size()); }
+
+ private:
+  struct HostSet {
+    Beam1 bm;
+    double exp_conf = 0;
+    std::vector<Data1> data;
+    std::vector<double> sb, lo, ln;
+    double maxsb = nan(), minDF = nan(), maxDF = nan();
+    double minR = nan(), maxR = nan();
+    bool rr_set = false;
+  };
+  void refresh_set(HostSet& s);
+  void build_static();
+  void free_static();
+  void free_work();
+  void ensure_plans(unsigned nprop);
+  void launch_all(unsigned nprop, const float* theta, unsigned npar,
+                  double* logl, int* status, cudaStream_t st, cudaEvent_t* ev);
+
+  int device_;
+  cudaStream_t stream_;
+  // configuration
+  std::vector<double> knots_;
+  unsigned n_ = 0, ninterp_ = 2048, nbins_ = 1000;
+  bool bin_data_ = true;
+  std::vector<HostSet> sets_;
+  bool static_ok_ = false;
+  // static device data
+  std::vector<void*> static_allocs_;
+  BSet1Dev* d_bsets_ = nullptr;
+  DSet1Dev* d_dsets_ = nullptr;
+  Model1Dev model_{};
+  std::vector<BSet1Dev> h_bsets_;
+  std::vector<DSet1Dev> h_dsets_;
+  unsigned B_ = 0, D_ = 0;
+  unsigned ntile_ = 0, nchunk_ = 0;
+  int maxterms_ = 1;
+  // work space
+  Workspace1 ws_;
+  // cuFFT plans and graphs per batch size
+  struct GraphKey {
+    const float* theta;
+    unsigned npar;
+    double* logl;
+    int* status;
+    bool operator==(const GraphKey& o) const {
+      return theta == o.theta && npar == o.npar && logl == o.logl &&
+             status == o.status;
+    }
+  };
+  struct Plans {
+    cufftHandle fwd = 0, inv = 0;
+    std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
+    bool warmed = false;
+    bool no_graph = false;
+  };
+  cudaGraphExec_t graph_for(unsigned nprop, const float* theta, unsigned npar,
+                            double* logl, int* status);
+  void drop_graphs();
+  std::map<unsigned, Plans> plans_;
+};
+
+}  // namespace pofd
+#endif

@@ -1,0 +1,380 @@
+// setup.cc -- host-side set-up of the P(D) likelihood (see setup.hh).
+#include "setup.hh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace pofd {
+
+// ---------------------------------------------------------------- Beam1
+// Pixel selection (|v| > minval, NaN/inf skipped), ascending sort, totals
+// and inverses: beam.cc:331-458.
+void Beam1::build(const double* pix, size_t n, double PIXSIZE,
+                  double MINVAL) {
+  if (PIXSIZE <= 0.0) throw Error(POFD_E_ARG, "Invalid (non-positive) pixel size");
+  minval = (MINVAL <= 0.0) ? 0.0 : MINVAL;
+  pixsize = PIXSIZE;
+  pos.clear();
+  neg.clear();
+  for (size_t i = 0; i < n; ++i) {
+    const double v = pix[i];
+    if (!std::isfinite(v)) continue;
+    if (v > minval) pos.push_back(v);
+    if (v < -minval) neg.push_back(std::fabs(v));
+  }
+  if (pos.empty() && neg.empty())
+    throw Error(POFD_E_ARG, "Beam file has only zero values");
+  haspos = !pos.empty();
+  hasneg = !neg.empty();
+  std::sort(pos.begin(), pos.end());
+  std::sort(neg.begin(), neg.end());
+  totpos = 0.0;
+  totneg = 0.0;
+  if (haspos) {
+    totpos = pos[0];
+    for (size_t i = 1; i < pos.size(); ++i) totpos += pos[i];
+  }
+  if (hasneg) {
+    totneg = neg[0];
+    for (size_t i = 1; i < neg.size(); ++i) totneg += neg[i];
+  }
+  posinv.resize(pos.size());
+  neginv.resize(neg.size());
+  for (size_t i = 0; i < pos.size(); ++i) posinv[i] = 1.0 / pos[i];
+  for (size_t i = 0; i < neg.size(); ++i) neginv[i] = 1.0 / neg[i];
+  poshist = neghist = false;
+  poswt.clear(); posival.clear(); negwt.clear(); negival.clear();
+}
+
+namespace {
+// Log2-spaced histogram of sorted values with 0.1% padding on both ends;
+// non-empty bins keep (count, 1/mean): beam.cc:487-553.
+void loghist(const std::vector<double>& v, unsigned nbins,
+             std::vector<double>& wt, std::vector<double>& ival) {
+  const double pad = 0.0014419741739063218;  // log2(1.001)
+  const double lo = std::log2(v.front()) - pad;
+  const double hi = std::log2(v.back()) + pad;
+  const double step = (hi - lo) / static_cast<double>(nbins);
+  std::vector<unsigned> cnt(nbins, 0);
+  std::vector<double> sum(nbins, 0.0);
+  for (double x : v) {
+    const unsigned b = static_cast<unsigned>((std::log2(x) - lo) / step);
+    cnt[b] += 1;
+    sum[b] += x;
+  }
+  wt.clear();
+  ival.clear();
+  for (unsigned b = 0; b < nbins; ++b) {
+    if (cnt[b] == 0) continue;
+    const double w = static_cast<double>(cnt[b]);
+    wt.push_back(w);
+    ival.push_back(1.0 / (sum[b] / w));
+  }
+}
+}  // namespace
+
+void Beam1::histogram(unsigned nbins) {
+  if (nbins == 0) throw Error(POFD_E_ARG, "Invalid (non-positive) nbins");
+  const unsigned thresh = 20;  // beam.h:31
+  poshist = neghist = false;
+  poswt.clear(); posival.clear(); negwt.clear(); negival.clear();
+  if (haspos && pos.size() >= thresh) {
+    loghist(pos, nbins, poswt, posival);
+    poshist = true;
+  }
+  if (hasneg && neg.size() >= thresh) {
+    loghist(neg, nbins, negwt, negival);
+    neghist = true;
+  }
+}
+
+void Beam1::terms(bool negside, std::vector<double>& w,
+                  std::vector<double>& ieta) const {
+  const bool hist = poshist;  // beam::isNegHist() returns the positive flag
+  if (!negside) {
+    if (!haspos) { w.clear(); ieta.clear(); return; }
+    if (hist) { w = poswt; ieta = posival; }
+    else { ieta = posinv; w.assign(posinv.size(), 1.0); }
+  } else {
+    if (!hasneg) { w.clear(); ieta.clear(); return; }
+    if (hist) { w = negwt; ieta = negival; }
+    else { ieta = neginv; w.assign(neginv.size(), 1.0); }
+  }
+}
+
+// ---------------------------------------------------------- SplineSystem
+// The x-dependent half of the natural-spline equations: diag 2(h_i+h_i+1),
+// off-diagonal h_i+1, factored as L D L^T (the factorisation the reference's
+// spline library performs each time it fits the spline, e.g.
+// PDFactory.cc:522 for the R nodes).
+void SplineSystem::factor(const std::vector<double>& xn) {
+  x = xn;
+  const size_t n = x.size();
+  if (n < 3) throw Error(POFD_E_ARG, "spline needs at least 3 nodes");
+  ih.resize(n - 1);
+  for (size_t i = 0; i + 1 < n; ++i) {
+    const double h = x[i + 1] - x[i];
+    if (!(h > 0)) throw Error(POFD_E_ARG, "spline nodes must increase");
+    ih[i] = 1.0 / h;
+  }
+  const size_t N = n - 2;
+  std::vector<double> diag(N), off(N);
+  for (size_t i = 0; i < N; ++i) {
+    const double h_i = x[i + 1] - x[i];
+    const double h_ip1 = x[i + 2] - x[i + 1];
+    off[i] = h_ip1;
+    diag[i] = 2.0 * (h_ip1 + h_i);
+  }
+  alpha.assign(N, 0.0);
+  gamma.assign(N, 0.0);
+  alpha[0] = diag[0];
+  gamma[0] = off[0] / alpha[0];
+  for (size_t i = 1; i + 1 < N; ++i) {
+    alpha[i] = diag[i] - off[i - 1] * gamma[i - 1];
+    gamma[i] = off[i] / alpha[i];
+  }
+  if (N > 1) alpha[N - 1] = diag[N - 1] - off[N - 2] * gamma[N - 2];
+}
+
+// ---------------------------------------------------------------- Data1
+void Data1::meanSubtract() {
+  double m = data[0];
+  for (size_t i = 1; i < data.size(); ++i) m += data[i];
+  m /= static_cast<double>(data.size());
+  for (auto& v : data) v -= m;
+  if (binned) bincent0 -= m;
+}
+
+std::pair<double, double> Data1::minmax() const {
+  if (binned)
+    return {bincent0, bincent0 + static_cast<double>(nbins - 1) * bindelta};
+  double lo = data[0], hi = data[0];
+  for (size_t i = 1; i < data.size(); ++i) {
+    if (data[i] < lo) lo = data[i];
+    if (data[i] > hi) hi = data[i];
+  }
+  return {lo, hi};
+}
+
+// Bin centres at min and max: fitsData.cc:406-437.
+void Data1::applyBinning(unsigned NB) {
+  if (NB == 0) throw Error(POFD_E_ARG, "Trying to bin with no bins");
+  binned = false;
+  const auto mm = minmax();
+  nbins = NB;
+  bins.assign(NB, 0u);
+  bincent0 = mm.first;
+  bindelta = (NB == 1) ? 2 * (mm.second - mm.first)
+                       : (mm.second - mm.first) / static_cast<double>(NB - 1);
+  const double ib = 1.0 / bindelta;
+  for (double v : data) {
+    const unsigned idx = static_cast<unsigned>((v - bincent0) * ib + 0.5);
+    bins[idx] += 1;
+  }
+  binned = true;
+}
+
+// --------------------------------------------------------------- RGrid1
+void RGrid1::init(unsigned N, double minflux, double maxflux) {
+  if (N == 0) throw Error(POFD_E_ARG, "Invalid (0) n");
+  if (maxflux < minflux) std::swap(minflux, maxflux);
+  n = N;
+  if (N == 1) {
+    if (minflux < 0.0) throw Error(POFD_E_ARG, "n must be > 1 with negative fluxes");
+    dflux = maxflux - minflux;
+    minflux_R = minflux;
+    wrapRidx = 0;
+    return;
+  }
+  const double inm1 = 1.0 / static_cast<double>(N - 1);
+  if (maxflux > 0) {
+    if (minflux > 0) minflux = 0.0;
+    if (minflux == 0) {
+      wrapRidx = N - 1;
+      minflux_R = 0.0;
+      dflux = maxflux * inm1;
+    } else {
+      dflux = (maxflux - minflux) * inm1;
+      dflux = maxflux / (N - std::floor(-minflux / dflux) - 1.0);
+      wrapRidx = static_cast<unsigned>(maxflux / dflux + 0.9999999999);
+      minflux_R = (wrapRidx + 1) * dflux - static_cast<double>(N) * dflux;
+    }
+  } else {
+    if (minflux >= 0) throw Error(POFD_E_ARG, "No effective range in R fluxes");
+    dflux = -minflux * inm1;
+    wrapRidx = 0;
+    minflux_R = minflux;
+  }
+}
+
+std::pair<double, double> rrange_knots(double maxknot, const Beam1& bm) {
+  if (bm.haspos)
+    return {bm.hasneg ? -maxknot * bm.maxneg() : 0.0, maxknot * bm.maxpos()};
+  return {-maxknot * bm.maxneg(), 0.0};
+}
+
+// ---------------------------------------------------------------- Beam2
+// Sign components pp/pn/np/nn of pixels with |v1|,|v2| > minval, input
+// order kept: doublebeam.cc:331-462.
+void Beam2::build(const double* b1, const double* b2, size_t n,
+                  double PIXSIZE, double MINVAL) {
+  if (n == 0) throw Error(POFD_E_ARG, "Invalid (zero) n");
+  if (MINVAL < 0.0) throw Error(POFD_E_ARG, "Invalid (negative) MINVAL");
+  if (PIXSIZE <= 0.0) throw Error(POFD_E_ARG, "Invalid (non-positive) pixel size");
+  minval = MINVAL;
+  pixsize = PIXSIZE;
+  for (int s = 0; s < 4; ++s) {
+    hassign[s] = ishist[s] = false;
+    pix1[s].clear(); pix2[s].clear();
+    minbm1[s] = maxbm1[s] = minbm2[s] = maxbm2[s] = nan();
+  }
+  for (size_t i = 0; i < n; ++i) {
+    const double v1 = b1[i], v2 = b2[i];
+    const double a1 = std::fabs(v1), a2 = std::fabs(v2);
+    if (a1 > minval && a2 > minval) {
+      const int s = (v1 > 0) ? ((v2 > 0) ? 0 : 1) : ((v2 > 0) ? 2 : 3);
+      pix1[s].push_back(a1);
+      pix2[s].push_back(a2);
+    }
+  }
+  if (!(pix1[0].size() + pix1[1].size() + pix1[2].size() + pix1[3].size()))
+    throw Error(POFD_E_ARG, "No acceptable values found");
+  for (int s = 0; s < 4; ++s) {
+    const size_t m = pix1[s].size();
+    if (!m) continue;
+    hassign[s] = true;
+    inv1[s].resize(m); inv2[s].resize(m); logratio[s].resize(m);
+    for (size_t j = 0; j < m; ++j) inv1[s][j] = 1.0 / pix1[s][j];
+    for (size_t j = 0; j < m; ++j) inv2[s][j] = 1.0 / pix2[s][j];
+    for (size_t j = 0; j < m; ++j)
+      logratio[s][j] = std::log(pix1[s][j] * inv2[s][j]);
+    double lo = pix1[s][0], hi = pix1[s][0];
+    for (size_t j = 1; j < m; ++j) {
+      const double v = pix1[s][j];
+      if (v > hi) hi = v; else if (v < lo) lo = v;
+    }
+    minbm1[s] = lo; maxbm1[s] = hi;
+    lo = hi = pix2[s][0];
+    for (size_t j = 1; j < m; ++j) {
+      const double v = pix2[s][j];
+      if (v > hi) hi = v; else if (v < lo) lo = v;
+    }
+    minbm2[s] = lo; maxbm2[s] = hi;
+  }
+}
+
+// 2D log2 histogram, components with at least 30 pixels:
+// doublebeam.cc:467-584; log ratios doublebeam.cc:750-772.
+void Beam2::histogram(unsigned nbins) {
+  if (!hasData()) throw Error(POFD_E_ARG, "Trying to histogram empty beam");
+  if (nbins == 0) throw Error(POFD_E_ARG, "Invalid (zero) NBINS");
+  const double pad = 0.0014419741739063218;
+  const unsigned nb2 = nbins * nbins;
+  const double dn = static_cast<double>(nbins);
+  for (int s = 0; s < 4; ++s) {
+    ishist[s] = false;
+    binwt[s].clear(); binv1[s].clear(); binv2[s].clear(); binlogratio[s].clear();
+    if (!(hassign[s] && pix1[s].size() >= 30)) continue;
+    const double lo1 = std::log2(minbm1[s]) - pad, hi1 = std::log2(maxbm1[s]) + pad;
+    const double is1 = dn / (hi1 - lo1);
+    const double lo2 = std::log2(minbm2[s]) - pad, hi2 = std::log2(maxbm2[s]) + pad;
+    const double is2 = dn / (hi2 - lo2);
+    std::vector<unsigned> cnt(nb2, 0);
+    std::vector<double> s1(nb2, 0.0), s2(nb2, 0.0);
+    for (size_t i = 0; i < pix1[s].size(); ++i) {
+      const double v1 = pix1[s][i], v2 = pix2[s][i];
+      const unsigned i1 = static_cast<unsigned>((std::log2(v1) - lo1) * is1);
+      const unsigned i2 = static_cast<unsigned>((std::log2(v2) - lo2) * is2);
+      const unsigned t = i1 * nbins + i2;
+      cnt[t] += 1; s1[t] += v1; s2[t] += v2;
+    }
+    for (unsigned t = 0; t < nb2; ++t) {
+      if (!cnt[t]) continue;
+      const double w = static_cast<double>(cnt[t]);
+      binwt[s].push_back(w);
+      binv1[s].push_back(w / s1[t]);
+      binv2[s].push_back(w / s2[t]);
+    }
+    for (size_t i = 0; i < binwt[s].size(); ++i)
+      binlogratio[s].push_back(std::log(binv2[s][i] / binv1[s][i]));
+    ishist[s] = true;
+  }
+}
+
+// ---------------------------------------------------------------- Data2
+void Data2::meanSubtract() {
+  const size_t n = d1.size();
+  double m = d1[0];
+  for (size_t i = 1; i < n; ++i) m += d1[i];
+  m /= static_cast<double>(n);
+  for (auto& v : d1) v -= m;
+  if (binned) bc1 -= m;
+  m = d2[0];
+  for (size_t i = 1; i < n; ++i) m += d2[i];
+  m /= static_cast<double>(n);
+  for (auto& v : d2) v -= m;
+  if (binned) bc2 -= m;
+}
+
+void Data2::minmax(double* mm) const {
+  if (binned) {
+    mm[0] = bc1; mm[1] = bc1 + static_cast<double>(nbins1 - 1) * bd1;
+    mm[2] = bc2; mm[3] = bc2 + static_cast<double>(nbins2 - 1) * bd2;
+    return;
+  }
+  mm[0] = mm[1] = d1[0];
+  for (size_t i = 1; i < d1.size(); ++i) {
+    if (d1[i] < mm[0]) mm[0] = d1[i];
+    if (d1[i] > mm[1]) mm[1] = d1[i];
+  }
+  mm[2] = mm[3] = d2[0];
+  for (size_t i = 1; i < d2.size(); ++i) {
+    if (d2[i] < mm[2]) mm[2] = d2[i];
+    if (d2[i] > mm[3]) mm[3] = d2[i];
+  }
+}
+
+void Data2::applyBinning(unsigned nb1, unsigned nb2) {
+  if (nb1 == 0 || nb2 == 0) throw Error(POFD_E_ARG, "Trying to bin with no bins");
+  binned = false;
+  double mm[4];
+  minmax(mm);
+  for (double v : mm)
+    if (!std::isfinite(v)) throw Error(POFD_E_ARG, "Non-valid min or max");
+  nbins1 = nb1; nbins2 = nb2;
+  bins.assign(static_cast<size_t>(nb1) * nb2, 0u);
+  bc1 = mm[0];
+  bd1 = (nb1 == 1) ? 2 * (mm[1] - mm[0]) : (mm[1] - mm[0]) / static_cast<double>(nb1 - 1);
+  bc2 = mm[2];
+  bd2 = (nb2 == 1) ? 2 * (mm[3] - mm[2]) : (mm[3] - mm[2]) / static_cast<double>(nb2 - 1);
+  const double ib1 = 1.0 / bd1, ib2 = 1.0 / bd2;
+  for (size_t i = 0; i < d1.size(); ++i) {
+    const unsigned i1 = static_cast<unsigned>((d1[i] - bc1) * ib1 + 0.5);
+    const unsigned i2 = static_cast<unsigned>((d2[i] - bc2) * ib2 + 0.5);
+    bins[static_cast<size_t>(i1) * nb2 + i2] += 1;
+  }
+  binned = true;
+}
+
+// ----------------------------------------------------------- RGrid2Axis
+void RGrid2Axis::init(unsigned N, double minflux, double maxflux) {
+  n = N;
+  flux.assign(N, 0.0);
+  const double inm1 = 1.0 / static_cast<double>(N - 1);
+  dflux = (maxflux - minflux) * inm1;
+  if (minflux >= 0.0) {
+    flux[0] = minflux;
+    for (unsigned i = 1; i < N; ++i) flux[i] = static_cast<double>(i) * dflux + minflux;
+    wrapidx = N - 1;
+  } else {
+    dflux = maxflux / (N - std::floor(-minflux / dflux) - 1.0);
+    wrapidx = static_cast<unsigned>(maxflux / dflux + 0.999999999);
+    flux[0] = 0.0;
+    for (unsigned i = 1; i <= wrapidx; ++i) flux[i] = static_cast<double>(i) * dflux;
+    const double wrapval = -static_cast<double>(N) * dflux;
+    for (unsigned i = wrapidx + 1; i < N; ++i)
+      flux[i] = static_cast<double>(i) * dflux + wrapval;
+  }
+}
+
+}  // namespace pofd

@@ -1,0 +1,136 @@
+// setup.hh -- host-side, theta-independent set-up of the P(D) likelihood.
+//
+// This is the once-per-run work the reference does before sampling: beam
+// pixel selection and log-binned histogram (beam.cc:295-556,
+// doublebeam.cc:331-584), data mean subtraction and binning
+// (fitsData.cc:393-437, fitsDataDouble.cc:480-608), likelihood offsets
+// (calcLike.cc:283-308, calcLikeDouble.cc:377-487) and the frozen R ranges
+// (calcLike.cc:346-371, calcLikeDouble.cc:496-534).  It also precomputes
+// everything of the per-proposal path that does not depend on the
+// parameters -- the R interpolation nodes, the natural-spline system
+// factorisation over them and the wrapped flux grids -- so that the GPU
+// kernels only do parameter-dependent work.
+#ifndef POFD_SETUP_HH
+#define POFD_SETUP_HH
+
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/pofd_b200.h"
+
+namespace pofd {
+
+struct Error : public std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+constexpr double kPi = 3.141592653589793238462643383279502884197;
+constexpr double kTwoPi = 2.0 * kPi;
+constexpr double kSmallLogVal = -30.0;  // pofd_mcmc::smalllogval
+constexpr double kNZeroPad = 7.5;       // pofd_mcmc::n_zero_pad
+constexpr double kBadLike = 1e25;       // calcLike::bad_like
+inline double logfac() { return std::log2(10.0); }
+inline double log2toe() { return std::log(2.0); }
+inline double nan() { return std::numeric_limits<double>::quiet_NaN(); }
+
+// ------------------------------------------------------------- 1D beam
+struct Beam1 {
+  bool haspos = false, hasneg = false;
+  double pixsize = 0, minval = 0;
+  std::vector<double> pos, neg;        // sorted |values| > minval
+  std::vector<double> posinv, neginv;  // 1 / values
+  double totpos = 0, totneg = 0;
+  bool poshist = false, neghist = false;
+  std::vector<double> poswt, posival, negwt, negival;  // histogram
+
+  void build(const double* pix, size_t n, double PIXSIZE, double MINVAL);
+  void histogram(unsigned nbins);
+  double maxpos() const { return haspos ? pos.back() : nan(); }
+  double maxneg() const { return hasneg ? neg.back() : nan(); }
+  // Terms the R sum runs over for one side (weights 1 for a raw beam).  The
+  // negative side follows beam::isNegHist(), which reports the positive
+  // side's histogram flag (beam.h:86).
+  void terms(bool negside, std::vector<double>& w,
+             std::vector<double>& ieta) const;
+};
+
+// Natural cubic spline through nodes x: the x-only part of the tridiagonal
+// system (LDL^T factors) and 1/h, so that per-parameter work is the RHS
+// and two first-order recurrences.
+struct SplineSystem {
+  std::vector<double> x, ih, alpha, gamma;  // ih: 1/h_i (n-1); alpha,gamma: n-2
+  void factor(const std::vector<double>& xn);
+};
+
+// Data set: mean-subtracted pixels, binned.
+struct Data1 {
+  std::vector<double> data;
+  bool binned = false;
+  unsigned nbins = 0;
+  std::vector<uint32_t> bins;
+  double bincent0 = 0, bindelta = 0;
+  void meanSubtract();
+  std::pair<double, double> minmax() const;
+  void applyBinning(unsigned nbins);
+};
+
+// The wrapped R flux grid of PDFactory::initRFlux (PDFactory.cc:361-414).
+struct RGrid1 {
+  unsigned n = 0, wrapRidx = 0;
+  double dflux = 0, minflux_R = 0;
+  void init(unsigned N, double minflux, double maxflux);
+};
+
+// The flux range of a knot model over a beam (numberCountsKnots.cc:345-365).
+std::pair<double, double> rrange_knots(double maxknot, const Beam1& bm);
+
+// ------------------------------------------------------------- 2D beam
+struct Beam2 {
+  double pixsize = 0, minval = 0;
+  bool hassign[4] = {false, false, false, false};
+  std::vector<double> pix1[4], pix2[4];  // |values|, input order
+  std::vector<double> inv1[4], inv2[4], logratio[4];
+  double minbm1[4], maxbm1[4], minbm2[4], maxbm2[4];
+  bool ishist[4] = {false, false, false, false};
+  std::vector<double> binwt[4], binv1[4], binv2[4], binlogratio[4];
+
+  void build(const double* b1, const double* b2, size_t n, double PIXSIZE,
+             double MINVAL);
+  void histogram(unsigned nbins);
+  bool hasData() const {
+    return hassign[0] || hassign[1] || hassign[2] || hassign[3];
+  }
+  // Terms of one sign component: weights (1 for raw), inverse beam 1,
+  // inverse beam 2, log(beam1/beam2).
+  size_t nterms(int s) const {
+    return hassign[s] ? (ishist[s] ? binwt[s].size() : pix1[s].size()) : 0;
+  }
+};
+
+struct Data2 {
+  std::vector<double> d1, d2;
+  unsigned nbins1 = 0, nbins2 = 0;
+  std::vector<uint32_t> bins;
+  double bc1 = 0, bc2 = 0, bd1 = 0, bd2 = 0;
+  bool binned = false;
+  void meanSubtract();
+  void minmax(double* mm4) const;
+  void applyBinning(unsigned nb1, unsigned nb2);
+};
+
+// PDFactoryDouble's wrapped grid along one axis (PDFactoryDouble.cc:18-49).
+struct RGrid2Axis {
+  unsigned n = 0, wrapidx = 0;
+  double dflux = 0;
+  std::vector<double> flux;
+  void init(unsigned N, double minflux, double maxflux);
+};
+
+}  // namespace pofd
+#endif
