@@ -39,7 +39,7 @@ WORKLOAD = ("1D batched plain method: 10-knot spline 1-800 mJy, 3 beam sets "
 def args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-seconds", type=float, default=12.0,
@@ -244,7 +244,10 @@ def main():
            for _ in range(nbatches)]
     dst = [torch.empty(BATCH, dtype=torch.int32, device="cuda")
            for _ in range(nbatches)]
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library reads a NULL stream as "the context's
+    # own stream", so the events must sit on the stream we pass
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
     def step(k):

@@ -1,0 +1,161 @@
+// pofd_b200.hpp -- header-only C++ shim over the C ABI (pofd_b200.h) with
+// the reference's class shapes, for dropping into the pofd_affine C++ code.
+//
+//   pofd_b200::Context ctx(0);
+//   pofd_b200::Beam1 bm(pixels, npix, pixsize, true, 120, 1e-5);
+//   pofd_b200::Like1 like(ctx, knotpos, fftsize, ninterp, true, nbins);
+//   like.addBeamSet(bm); like.addDataset(0, data, ndata, sigma);
+//   like.setRRanges(theta, npar);
+//   double L = like.getLogLike(theta, npar, pars_invalid);   // calcLike.h:275
+//   like.getLogLikeBatch(nprop, thetas, npar, logl, status); // batched
+//
+// Errors are thrown as pofd_b200::Exception carrying the status code and the
+// library's message, in the place where the reference throws affineExcept.
+#ifndef POFD_B200_HPP
+#define POFD_B200_HPP
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pofd_b200.h"
+
+namespace pofd_b200 {
+
+class Exception : public std::runtime_error {
+ public:
+  Exception(int code, const std::string& method)
+      : std::runtime_error(method + ": " + pofd_last_error()), code_(code) {}
+  int code() const { return code_; }
+
+ private:
+  int code_;
+};
+
+inline int check(int st, const char* method) {
+  if (st < 0) throw Exception(st, method);
+  return st;
+}
+
+class Context {
+ public:
+  explicit Context(int device = 0) {
+    check(pofd_ctx_create(device, &h_), "pofd_ctx_create");
+  }
+  ~Context() { pofd_ctx_destroy(h_); }
+  Context(const Context&) = delete;
+  Context& operator=(const Context&) = delete;
+  pofd_ctx* get() const { return h_; }
+
+ private:
+  pofd_ctx* h_ = nullptr;
+};
+
+// beam::beam(filename, histogram, NBINS, MINVAL) from a pixel array.
+class Beam1 {
+ public:
+  Beam1(const double* pix, size_t npix, double pixsize, bool histogram = false,
+        unsigned nbins = 120, double minval = 1e-5) {
+    check(pofd_beam1_create(pix, npix, pixsize, minval,
+                            histogram ? nbins : 0u, &h_),
+          "beam::beam");
+  }
+  ~Beam1() { pofd_beam1_destroy(h_); }
+  Beam1(const Beam1&) = delete;
+  Beam1& operator=(const Beam1&) = delete;
+  const pofd_beam1* get() const { return h_; }
+  bool hasPos() const { return info(0) != 0.0; }
+  bool hasNeg() const { return info(1) != 0.0; }
+
+ private:
+  double info(int i) const {
+    double o[15];
+    check(pofd_beam1_info(h_, o), "beam::info");
+    return o[i];
+  }
+  pofd_beam1* h_ = nullptr;
+};
+
+// PDFactory (PDFactory.h:136-140).
+class PDFactory1 {
+ public:
+  explicit PDFactory1(Context& ctx, unsigned ninterp = 2048) {
+    check(pofd_pdfactory1_create(ctx.get(), ninterp, &h_), "PDFactory");
+  }
+  ~PDFactory1() { pofd_pdfactory1_destroy(h_); }
+  PDFactory1(const PDFactory1&) = delete;
+  PDFactory1& operator=(const PDFactory1&) = delete;
+  bool initPD(unsigned n, double minflux, double maxflux, unsigned nknots,
+              const double* knotpos, const float* knotvals, const Beam1& bm) {
+    check(pofd_pdfactory1_initpd(h_, n, minflux, maxflux, nknots, knotpos,
+                                 knotvals, bm.get()),
+          "PDFactory::initPD");
+    n_ = n;
+    return true;
+  }
+  // Fills pd (n values), returns the flux of element 0; dflux via *dflux.
+  double getPD(double sigma, std::vector<double>& pd, bool setLog = true,
+               double* dflux = nullptr) {
+    pd.resize(n_);
+    double mf = 0.0, df = 0.0;
+    check(pofd_pdfactory1_getpd(h_, sigma, setLog ? 1 : 0, pd.data(), &mf, &df),
+          "PDFactory::getPD");
+    if (dflux) *dflux = df;
+    return mf;
+  }
+
+ private:
+  pofd_pdfactory1* h_ = nullptr;
+  unsigned n_ = 0;
+};
+
+// calcLike (calcLike.h:166-275).
+class Like1 {
+ public:
+  Like1(Context& ctx, unsigned nknots, const double* knotpos,
+        unsigned fftsize = 131072, unsigned ninterp = 2048,
+        bool bin_data = true, unsigned nbins = 1000) {
+    check(pofd_like1_create(ctx.get(), nknots, knotpos, fftsize, ninterp,
+                            bin_data ? 1 : 0, nbins, &h_),
+          "calcLike::calcLike");
+  }
+  ~Like1() { pofd_like1_destroy(h_); }
+  Like1(const Like1&) = delete;
+  Like1& operator=(const Like1&) = delete;
+  int addBeamSet(const Beam1& bm, double exp_conf = 0.0) {
+    return check(pofd_like1_add_beamset(h_, bm.get(), exp_conf),
+                 "calcLike::readDataFromFiles");
+  }
+  void addDataset(int beamset, const double* data, size_t ndata,
+                  double sigma_base, double like_norm = 1.0,
+                  bool meansub = true) {
+    check(pofd_like1_add_dataset(h_, beamset, data, ndata, meansub ? 1 : 0,
+                                 sigma_base, like_norm),
+          "calcLike::readDataFromFiles");
+  }
+  void setRRanges(const float* p, unsigned npar) {
+    check(pofd_like1_set_rranges(h_, p, npar), "calcLike::setRRanges");
+  }
+  void reserve(unsigned max_batch) {
+    check(pofd_like1_reserve(h_, max_batch), "calcLike::reserve");
+  }
+  double getLogLike(const float* p, unsigned npar, bool& pars_invalid) {
+    double ll = 0.0;
+    int inv = 0;
+    check(pofd_like1_loglike(h_, p, npar, &ll, &inv), "calcLike::getLogLike");
+    pars_invalid = inv != 0;
+    return ll;
+  }
+  void getLogLikeBatch(unsigned nprop, const float* p, unsigned npar,
+                       double* logl, int* status) {
+    check(pofd_like1_eval_batch(h_, nprop, p, npar, logl, status),
+          "calcLike::getLogLikeBatch");
+  }
+  pofd_like1* get() const { return h_; }
+
+ private:
+  pofd_like1* h_ = nullptr;
+};
+
+}  // namespace pofd_b200
+#endif

@@ -36,7 +36,7 @@ constexpr int NT = 256;           // threads per block for the streaming kernels
 constexpr int TILE = NT * 8;      // R grid points per block
 constexpr int CHUNK = NT * 16;    // P(D) elements per reduction block
 constexpr int KMAX = Engine1::KMAX;
-constexpr int MAXTERMS = 6144;    // beam terms held in shared memory
+constexpr int MAXTERMS = 4096;    // beam terms held in shared memory
 
 void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -56,29 +56,25 @@ void cufft_check(cufftResult r, const char* what) {
 
 // ------------------------------------------------------------- kernels
 
-// Model set-up per proposal: log2 knot values from the float parameters and
-// the natural cubic spline through (log2 S_k, log2 n_k), stored per interval
-// as (y, b, c, d) exactly as the spline library forms them at evaluation.
-__global__ void k_model1(Model1Dev m, const float* __restrict__ theta,
-                         int npar, int nprop, double logfac,
-                         double* __restrict__ cnt, int* __restrict__ mstatus,
-                         double* __restrict__ sigmult) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= nprop) return;
-  const float* th = theta + static_cast<size_t>(w) * npar;
+// Model set-up for one proposal: log2 knot values from the float parameters
+// and the natural cubic spline through (log2 S_k, log2 n_k), stored per
+// interval as (y, b, c, d) exactly as the spline library forms them at
+// evaluation (numberCountsKnotsSpline.cc:265-274).  Returns the status.
+__device__ int model_solve(const Model1Dev& m, const float* __restrict__ th,
+                           double logfac, double* __restrict__ out,
+                           double* __restrict__ wk /* 8*KMAX */) {
   const int K = m.K;
-  double y[KMAX], c[KMAX], g[KMAX], diag[KMAX], off[KMAX], alp[KMAX],
-      gam[KMAX], z[KMAX];
-  bool ok = true;
+  double* y = wk;
+  double* c = y + KMAX;
+  double* g = c + KMAX;
+  double* diag = g + KMAX;
+  double* off = diag + KMAX;
+  double* alp = off + KMAX;
+  double* gam = alp + KMAX;
+  double* z = gam + KMAX;
   for (int k = 0; k < K; ++k) {
     y[k] = logfac * static_cast<double>(th[k]);
-    if (isnan(y[k])) ok = false;
-  }
-  sigmult[w] = static_cast<double>(th[K]);
-  double* out = cnt + static_cast<size_t>(w) * 4 * KMAX;
-  if (!ok) {
-    mstatus[w] = POFD_E_INVALID_MODEL;
-    return;
+    if (isnan(y[k])) return POFD_E_INVALID_MODEL;
   }
   const double* x = m.logknots;
   for (int k = 0; k < K; ++k) c[k] = 0.0;
@@ -116,7 +112,7 @@ __global__ void k_model1(Model1Dev m, const float* __restrict__ theta,
     out[4 * i + 2] = c[i];
     out[4 * i + 3] = (c[i + 1] - c[i]) / (3.0 * dx);
   }
-  mstatus[w] = 0;
+  return POFD_OK;
 }
 
 __device__ __forceinline__ double counts_log2(const double* __restrict__ lk,
@@ -128,8 +124,30 @@ __device__ __forceinline__ double counts_log2(const double* __restrict__ lk,
   return q[0] + delx * (q[1] + delx * (q[2] + delx * q[3]));
 }
 
+// Knot spline of every proposal: one block per proposal, thread 0 solving
+// in shared memory.  Publishes the model status and the sigma multiplier.
+__global__ void k_model1(Model1Dev m, const float* __restrict__ theta,
+                         int npar, double logfac, double* __restrict__ cnt,
+                         int* __restrict__ mstatus,
+                         double* __restrict__ sigmult) {
+  __shared__ double wk[8 * KMAX];
+  __shared__ double cs[4 * KMAX];
+  const int w = blockIdx.x;
+  const float* th = theta + static_cast<size_t>(w) * npar;
+  if (threadIdx.x == 0) {
+    const int st = model_solve(m, th, logfac, cs, wk);
+    mstatus[w] = st;
+    sigmult[w] = static_cast<double>(th[m.K]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 4 * (m.K - 1); i += blockDim.x)
+    cnt[static_cast<size_t>(w) * 4 * KMAX + i] = cs[i];
+}
+
 // R at the interpolation nodes, one node per thread, terms summed in the
-// beam's order: numberCountsKnotsSpline.cc:495-526.
+// beam's order (numberCountsKnotsSpline.cc:495-526).  log2(x * ieta) is
+// formed as log2|x| + log2(ieta) from host-computed logs; the range test uses
+// the product itself, as the reference does.
 __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
                           int B, int NI, int maxterms,
                           const double* __restrict__ cnt,
@@ -147,19 +165,22 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
   double* s_lk = sm;
   double* s_cs = s_lk + KMAX;
   double* s_w = s_cs + 4 * KMAX;
-  double* s_ie = s_w + maxterms;
+  double* s_le = s_w + maxterms;
+  double* s_ie = s_le + maxterms;
   const double* cs = cnt + static_cast<size_t>(w) * 4 * KMAX;
   for (int i = threadIdx.x; i < K; i += blockDim.x) s_lk[i] = m.logknots[i];
   for (int i = threadIdx.x; i < 4 * (K - 1); i += blockDim.x) s_cs[i] = cs[i];
   const int nt = sd.nterms;
   for (int i = threadIdx.x; i < nt; i += blockDim.x) {
     s_w[i] = sd.w[i];
+    s_le[i] = sd.lie[i];
     s_ie[i] = sd.ieta[i];
   }
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= NI) return;
   const double f = sd.x[i];
+  const double lf = sd.lxa[i];
   const double minknot = m.minknot, maxknot = m.maxknot;
   double workval = 0.0;
   const bool posb = (f > 0 && bs.haspos && f <= bs.rr_hi);
@@ -170,7 +191,7 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
       const double ieta = s_ie[j];
       const double currarg = af * ieta;
       if (currarg < minknot || currarg >= maxknot) continue;
-      const double cts = exp2(counts_log2(s_lk, s_cs, K, log2(currarg)));
+      const double cts = exp2(counts_log2(s_lk, s_cs, K, lf + s_le[j]));
       if (cts > 0) workval += s_w[j] * cts * ieta;
     }
   }
@@ -280,7 +301,9 @@ k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
 
 // The wrapped R grid: 2^spline(flux) * dflux inside each side's covered
 // index range, zero elsewhere (PDFactory.cc:556-613), plus block partial
-// sums of the first and second flux moments (PDFactory.cc:634-665).
+// sums of the first and second flux moments (PDFactory.cc:634-665).  The
+// node interval of every grid point is parameter-independent and comes from
+// a host-built table (gidx, -1 outside the covered ranges).
 __global__ void __launch_bounds__(NT)
 k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
          int nc2, int ntile, const int* __restrict__ mstatus,
@@ -294,42 +317,43 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
   const double dflux = bs.dflux;
   const int wrap = bs.wrapRidx;
   const double minflux_R = bs.minflux_R;
+  const int* __restrict__ gidx = bs.gidx;
   double* R = rbuf + static_cast<size_t>(wb) * nc2;
+  const double* S0 = spl + static_cast<size_t>(wb) * 2 * 4 * NI;
+  const double off0 = bs.side[0].grid_off, off1 = bs.side[1].grid_off;
+  const double* __restrict__ x0 = bs.side[0].x;
+  const double* __restrict__ x1 = bs.side[1].x;
+  constexpr int PER = TILE / NT;
+  const int base = blockIdx.x * TILE + threadIdx.x;
+  int q[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int i = base + k * NT;
+    q[k] = (i < n) ? gidx[i] : -2;
+  }
   double mn = 0.0, var = 0.0;
-  const int base = blockIdx.x * TILE;
-#pragma unroll 4
-  for (int k = 0; k < TILE / NT; ++k) {
-    const int i = base + k * NT + threadIdx.x;
-    if (i >= n) break;
-    const int side = (i <= wrap) ? 0 : 1;
-    const Side1Dev& sd = bs.side[side];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int i = base + k * NT;
+    if (q[k] == -2) break;
+    const bool neg = i > wrap;
     double r = 0.0;
-    if (i >= sd.grid_lo && i <= sd.grid_hi) {
-      const double cflux = static_cast<double>(i) * dflux + sd.grid_off;
-      const double* x = sd.x;
-      const int q = dev::bsearch_lo(x, cflux, 0, NI - 1);
-      const double* S = spl + (static_cast<size_t>(wb) * 2 + side) * 4 * NI;
-      const double delx = cflux - x[q];
-      const double v = S[q] + delx * (S[NI + q] + delx * (S[2 * NI + q] + delx * S[3 * NI + q]));
+    if (q[k] >= 0) {
+      const double cflux = __dadd_rn(__dmul_rn(static_cast<double>(i), dflux), neg ? off1 : off0);
+      const double* S = S0 + (neg ? 4 * NI : 0);
+      const int j = q[k];
+      const double delx = cflux - (neg ? x1 : x0)[j];
+      const double v = S[j] + delx * (S[NI + j] + delx * (S[2 * NI + j] + delx * S[3 * NI + j]));
       r = exp2(v) * dflux;
     }
     R[i] = r;
-    if (i >= 1 && i <= wrap - 1) {
-      const double cf = static_cast<double>(i) * dflux;
-      const double prod = cf * r;
-      mn += prod;
-      var += cf * prod;
-    } else if (i == wrap && i > 0) {
-      const double cf = static_cast<double>(wrap) * dflux;
-      const double prod = 0.5 * cf * r;
-      mn += prod;
-      var += cf * prod;
-    } else if (i > wrap) {
-      const double cf = static_cast<double>(i - wrap - 1) * dflux + minflux_R;
-      const double prod = cf * r;
-      mn += prod;
-      var += cf * prod;
-    }
+    // moment weights: 0 at i = 0, 1/2 at the positive edge, 1 elsewhere
+    const double cf = neg ? static_cast<double>(i - wrap - 1) * dflux + minflux_R
+                          : static_cast<double>(i) * dflux;
+    const double wt = (i == 0) ? 0.0 : ((i == wrap) ? 0.5 : 1.0);
+    const double prod = wt * cf * r;
+    mn += prod;
+    var += cf * prod;
   }
   mn = dev::block_sum<NT>(mn, shr);
   var = dev::block_sum<NT>(var, shr);
@@ -378,7 +402,9 @@ __global__ void k_moments1(const BSet1Dev* __restrict__ bsets, int B, int n,
 // exp(R~ - R~0) with the mean shift, then one noise-multiplied copy per
 // dataset of the beam set (PDFactory.cc:1106-1132, 1174-1188).  The
 // self-conjugate Nyquist bin keeps only its real part, which is what the
-// c2r transform uses of it.
+// c2r transform uses of it.  Where every dataset's noise exponent is below
+// -750, exp() underflows to exactly 0 and the reference's product is 0: those
+// bins are written as 0 without evaluating exp/sincos of the R spectrum.
 __global__ void __launch_bounds__(NT)
 k_spectrum1(const BSet1Dev* __restrict__ bsets,
             const DSet1Dev* __restrict__ dsets, int B, int D, int n, int nc,
@@ -391,9 +417,24 @@ k_spectrum1(const BSet1Dev* __restrict__ bsets,
   const int k = blockIdx.x * NT + threadIdx.x;
   if (k >= nc) return;
   const BSet1Dev& bs = bsets[b];
-  const double2* Rt = reinterpret_cast<const double2*>(rbuf + static_cast<size_t>(wb) * 2 * nc);
   const double dflux = bs.dflux;
   const double iflux = dev::kTwoPi / (static_cast<double>(n) * dflux);
+  const double sm = sigmult[w];
+  const double wv = iflux * static_cast<double>(k);
+  bool all_zero = k > 0;
+  for (int dd = 0; dd < bs.nds && all_zero; ++dd) {
+    const double sigma = sm * dsets[bs.ds_begin + dd].sigma_base;
+    if (!(sigma > 0)) { all_zero = false; break; }
+    const double sigfac = -0.5 * sigma * sigma;
+    if (!(sigfac * wv * wv < -750.0)) all_zero = false;
+  }
+  if (all_zero) {
+    for (int dd = 0; dd < bs.nds; ++dd)
+      reinterpret_cast<double2*>(pbuf + (static_cast<size_t>(w) * D + bs.ds_begin + dd) * 2 * nc)[k] =
+          make_double2(0.0, 0.0);
+    return;
+  }
+  const double2* Rt = reinterpret_cast<const double2*>(rbuf + static_cast<size_t>(wb) * 2 * nc);
   const double* mo = mom + static_cast<size_t>(wb) * 4;
   const bool doshift = mo[3] != 0.0;
   double2 p;
@@ -409,14 +450,12 @@ k_spectrum1(const BSet1Dev* __restrict__ bsets,
     p = make_double2(expfac * c, expfac * s);
   }
   if ((n & 1) == 0 && k == n / 2) p.y = 0.0;
-  const double sm = sigmult[w];
   for (int dd = 0; dd < bs.nds; ++dd) {
     const int d = bs.ds_begin + dd;
     const double sigma = sm * dsets[d].sigma_base;
     double2 o = p;
     if (sigma > 0 && k > 0) {
       const double sigfac = -0.5 * sigma * sigma;
-      const double wv = iflux * static_cast<double>(k);
       const double ef = exp(sigfac * wv * wv);
       o = make_double2(ef * p.x, ef * p.y);
     }
@@ -474,20 +513,27 @@ k_pscan1(const BSet1Dev* __restrict__ bsets, const DSet1Dev* __restrict__ dsets,
   const SplitParams sp = split_params(bs, var, sigmult[w] * ds.sigma_base);
   const double* p = pbuf + static_cast<size_t>(wd) * nc2;
   const int base = blockIdx.x * CHUNK;
+  constexpr int PER = CHUNK / NT;
+  double v[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int i = base + k * NT + threadIdx.x;
+    v[k] = (i < n) ? p[i] : -1.0;
+  }
   double mx = 0.0, sum = 0.0, wsum = 0.0, mnv = 1.0e308;
   int mni = 0x7fffffff;
   bool any = false;
-#pragma unroll 4
-  for (int k = 0; k < CHUNK / NT; ++k) {
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
     const int li = k * NT + threadIdx.x;
     const int i = base + li;
     if (i >= n) break;
-    const double v = clip0(p[i]);
-    if (!any || v > mx) mx = v;
+    const double x = clip0(v[k]);
+    if (!any || x > mx) mx = x;
     any = true;
-    sum += v;
-    wsum += static_cast<double>(li) * v;
-    if (i >= sp.botidx && i <= sp.topidx) dev::argmin_merge(mnv, mni, v, i);
+    sum += x;
+    wsum += static_cast<double>(li) * x;
+    if (i >= sp.botidx && i <= sp.topidx) dev::argmin_merge(mnv, mni, x, i);
   }
   if (!any) mx = -1.0e308;
   mx = dev::block_max<NT>(mx, shd);
@@ -997,6 +1043,7 @@ void Engine1::build_static() {
     bd.minflux_R = g.minflux_R;
     bd.wrapRidx = static_cast<int>(g.wrapRidx);
     bd.maxsb = s.maxsb;
+    std::vector<int> gidx(n_, -1);
     for (int side = 0; side < 2; ++side) {
       Side1Dev& sd = bd.side[side];
       sd.nodes = 0;
@@ -1029,6 +1076,11 @@ void Engine1::build_static() {
       s.bm.terms(side == 1, tw, tie);
       if (tie.size() > static_cast<size_t>(MAXTERMS))
         throw Error(POFD_E_ARG, "beam has too many terms; histogram it");
+      std::vector<double> lxa(NI), lie(tie.size());
+      for (unsigned i = 0; i < NI; ++i) lxa[i] = std::log2(std::fabs(x[i]));
+      for (size_t j = 0; j < tie.size(); ++j) lie[j] = std::log2(tie[j]);
+      sd.lxa = up(lxa);
+      sd.lie = up(lie);
       sd.nodes = 1;
       sd.nterms = static_cast<int>(tie.size());
       if (sd.nterms > maxterms_) maxterms_ = sd.nterms;
@@ -1058,7 +1110,18 @@ void Engine1::build_static() {
         sd.grid_hi = static_cast<int>(hi);
         sd.grid_off = g.minflux_R - static_cast<double>(g.wrapRidx + 1) * g.dflux;
       }
+      // interval of every covered grid point (gsl-style bisection)
+      for (int i = sd.grid_lo; i <= sd.grid_hi; ++i) {
+        const double cflux = static_cast<double>(i) * g.dflux + sd.grid_off;
+        size_t lo = 0, hi = NI - 1;
+        while (hi > lo + 1) {
+          const size_t mid = (hi + lo) / 2;
+          if (x[mid] > cflux) hi = mid; else lo = mid;
+        }
+        gidx[i] = static_cast<int>(lo);
+      }
     }
+    bd.gidx = upi(gidx);
     bd.ds_begin = static_cast<int>(h_dsets_.size());
     bd.nds = static_cast<int>(s.data.size());
     for (size_t i = 0; i < s.data.size(); ++i) {
@@ -1143,7 +1206,7 @@ void Engine1::profile_stages(unsigned nprop, const float* theta, unsigned npar,
 
 const char* Engine1::stage_name(int i) {
   static const char* names[kNumStages] = {
-      "k_model1", "k_rnodes1", "k_rspline1", "k_rfill1", "k_moments1",
+      "k_model1+k_rnodes1", "k_rspline1", "k_rfill1", "k_moments1",
       "cufft_d2z", "k_spectrum1", "cufft_z2d", "k_pscan1", "k_pfinish1",
       "k_reduce1"};
   return (i >= 0 && i < kNumStages) ? names[i] : "";
@@ -1192,7 +1255,7 @@ void Engine1::reserve(unsigned P) {
   ws_.logl = dalloc<double>(P);
   ws_.status = dalloc<int>(P);
   cuda_check(cudaFuncSetAttribute(k_rnodes1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>((KMAX + 4 * KMAX + 2 * MAXTERMS) * sizeof(double))),
+                                  static_cast<int>((KMAX + 4 * KMAX + 3 * MAXTERMS) * sizeof(double))),
              "smem attribute");
   cuda_check(cudaFuncSetAttribute(k_rspline1, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>((2 * 8192 + 2 * NT) * sizeof(double))),
@@ -1233,48 +1296,46 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
   Plans& pl = plans_.at(nprop);
 
   mark(0);
-  k_model1<<<(P + 63) / 64, 64, 0, st>>>(model_, theta, static_cast<int>(npar), P,
-                                          std::log2(10.0), ws_.cnt, ws_.mstatus,
-                                          ws_.sigmult);
-  mark(1);
+  k_model1<<<P, 32, 0, st>>>(model_, theta, static_cast<int>(npar), std::log2(10.0),
+                             ws_.cnt, ws_.mstatus, ws_.sigmult);
   {
-    const size_t smem = (KMAX + 4 * KMAX + 2 * static_cast<size_t>(maxterms_)) * sizeof(double);
+    const size_t smem = (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double);
     dim3 grid((NI + 127) / 128, P * B * 2);
     k_rnodes1<<<grid, 128, smem, st>>>(d_bsets_, model_, B, NI, maxterms_,
                                        ws_.cnt, ws_.mstatus, ws_.nodes);
   }
-  mark(2);
+  mark(1);
   {
     const size_t smem = (2 * static_cast<size_t>(NI) + 2 * NT) * sizeof(double);
     k_rspline1<<<P * B * 2, NT, smem, st>>>(d_bsets_, B, NI, ws_.mstatus,
                                             ws_.nodes, ws_.spl);
   }
-  mark(3);
+  mark(2);
   {
     dim3 grid(ntile_, P * B);
     k_rfill1<<<grid, NT, 0, st>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
                                   ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
   }
-  mark(4);
+  mark(3);
   k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, B, n, nc2,
                                                   static_cast<int>(ntile_), P * B,
                                                   ws_.mstatus, ws_.rbuf,
                                                   ws_.rpart, ws_.mom);
-  mark(5);
+  mark(4);
   cufft_check(cufftSetStream(pl.fwd, st), "cufftSetStream");
   cufft_check(cufftExecD2Z(pl.fwd, ws_.rbuf, reinterpret_cast<cufftDoubleComplex*>(ws_.rbuf)),
               "cufftExecD2Z");
-  mark(6);
+  mark(5);
   {
     dim3 grid((nc + NT - 1) / NT, P * B);
     k_spectrum1<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc, ws_.mstatus,
                                      ws_.sigmult, ws_.mom, ws_.rbuf, ws_.pbuf);
   }
-  mark(7);
+  mark(6);
   cufft_check(cufftSetStream(pl.inv, st), "cufftSetStream");
   cufft_check(cufftExecZ2D(pl.inv, reinterpret_cast<cufftDoubleComplex*>(ws_.pbuf), ws_.pbuf),
               "cufftExecZ2D");
-  mark(8);
+  mark(7);
   {
     dim3 grid(nchunk_, P * D);
     k_pscan1<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
@@ -1282,15 +1343,15 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                   ws_.sigmult, ws_.mom, ws_.pbuf, ws_.ppart,
                                   ws_.pmidx);
   }
-  mark(9);
+  mark(8);
   k_pfinish1<<<P * D, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
                                    static_cast<int>(nchunk_), std::log(2.0),
                                    ws_.mstatus, ws_.sigmult, ws_.mom, ws_.pbuf,
                                    ws_.ppart, ws_.pmidx, ws_.pinfo);
-  mark(10);
+  mark(9);
   k_reduce1<<<(P + 127) / 128, 128, 0, st>>>(d_bsets_, B, D, P, ws_.mstatus,
                                             ws_.sigmult, ws_.pinfo, logl, status);
-  mark(11);
+  mark(10);
   cuda_check(cudaGetLastError(), "kernel launch");
 }
 
@@ -1443,10 +1504,10 @@ void Engine1::rgrid_host(int bs, const float* theta, unsigned npar, double* out)
   const int NI = static_cast<int>(ninterp_), n = static_cast<int>(n_);
   const int nc2 = 2 * (n / 2 + 1);
   const int B = static_cast<int>(B_);
-  k_model1<<<1, 64, 0, stream_>>>(model_, ws_.theta_in, static_cast<int>(npar), 1, std::log2(10.0),
-                                  ws_.cnt, ws_.mstatus, ws_.sigmult);
+  k_model1<<<1, 32, 0, stream_>>>(model_, ws_.theta_in, static_cast<int>(npar),
+                                  std::log2(10.0), ws_.cnt, ws_.mstatus, ws_.sigmult);
   k_rnodes1<<<dim3((NI + 127) / 128, B * 2), 128,
-              (KMAX + 4 * KMAX + 2 * static_cast<size_t>(maxterms_)) * sizeof(double), stream_>>>(
+              (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double), stream_>>>(
       d_bsets_, model_, B, NI, maxterms_, ws_.cnt, ws_.mstatus, ws_.nodes);
   k_rspline1<<<B * 2, NT, (2 * static_cast<size_t>(NI) + 2 * NT) * sizeof(double), stream_>>>(
       d_bsets_, B, NI, ws_.mstatus, ws_.nodes, ws_.spl);

@@ -32,6 +32,8 @@ struct Side1Dev {
   const double* ih;     // 1/(x[i+1]-x[i])
   const double* alpha;  // LDL^T diagonal (ninterp-2)
   const double* gamma;  // LDL^T sub-diagonal ratio (ninterp-2)
+  const double* lxa;    // log2|x| of the nodes
+  const double* lie;    // log2 of the inverse beam terms
   int grid_lo, grid_hi; // inclusive grid index range filled from this side
   double grid_off;      // grid flux = i*dflux + grid_off
 };
@@ -45,6 +47,7 @@ struct BSet1Dev {
   int wrapRidx;
   double maxsb;         // max sigma_base of the set
   int ds_begin, nds;
+  const int* gidx;      // node interval of each grid point, -1 if uncovered
 };
 
 struct DSet1Dev {
@@ -135,7 +138,7 @@ class Engine1 {
                    double* x_out, double* r_out);
   void rgrid_host(int bs, const float* theta, unsigned npar, double* out);
   int kernels_per_eval() const { return 9; }
-  static constexpr int kNumStages = 11;
+  static constexpr int kNumStages = 10;
   void profile_stages(unsigned nprop, const float* theta, unsigned npar,
                       int reps, double* stage_ms);
   static const char* stage_name(int i);

@@ -14,6 +14,10 @@ P_TOL = 1e-10
 LL_TOL = 1e-6
 
 
+def _beam2d(beams, name):
+    return beams[name].reshape(tuple(beams[name + "_dims"])[::-1])
+
+
 def _spec(seed=0, n=4096, ni=512, shape=(128, 128), noise=0.002, fwhm=3.0,
           nbins=500, nh=120, beam_pix=None, ps=6.0, ndata=1, sig2=None,
           knots=None, bin_data=True):
@@ -48,7 +52,7 @@ def _build(orc, ctx, s, minval=1e-5):
 
 def test_r_nodes_match_oracle(orc, gpu_ctx, beams):
     for bp, ps, nh in ((None, 6.0, 120), (None, 6.0, 0),
-                       (beams["band12_0"], 8.0, 200)):
+                       (_beam2d(beams, "band12_0"), 8.0, 200)):
         s = _spec(beam_pix=bp, ps=ps, nh=nh)
         O, G = _build(orc, gpu_ctx, s)
         sides = [False, True] if bp is not None else [False]
@@ -68,7 +72,7 @@ def test_pd_and_r_grid_match_oracle(orc, gpu_ctx, beams, case):
     if case == "raw":
         kw = dict(nh=0)
     elif case == "neg":
-        kw = dict(beam_pix=beams["band12_0"], ps=8.0, nh=200)
+        kw = dict(beam_pix=_beam2d(beams, "band12_0"), ps=8.0, nh=200)
     elif case == "n3000":
         kw = dict(n=3000)
     elif case == "lownoise":
@@ -121,7 +125,7 @@ def test_loglike_batch_matches_oracle(orc, gpu_ctx, beams, case):
     elif case == "unbinned":
         kw = dict(bin_data=False, shape=(48, 48))
     elif case == "neg":
-        kw = dict(beam_pix=beams["band12_0"], ps=8.0, nh=200)
+        kw = dict(beam_pix=_beam2d(beams, "band12_0"), ps=8.0, nh=200)
     elif case == "n3000":
         kw = dict(n=3000)
     s = _spec(**kw)
