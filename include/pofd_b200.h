@@ -175,6 +175,32 @@ int pofd_like1_profile(pofd_like1* L, unsigned nprop, const float* theta,
                        int* nstages);
 const char* pofd_like1_stage_name(int i);
 
+/* Allocation-free split / unwrap / normalise / binned log-likelihood of
+ * one wrapped 1D P(D) (the inverse-FFT output), for callers that cannot
+ * allocate GPU memory when they evaluate: a program whose device memory is
+ * already reserved by another allocator, or a latency-sensitive caller that
+ * cannot take the synchronisation cudaMalloc/cudaFree imply.  No counterpart
+ * in the reference.  All pointers are device pointers owned by the caller:
+ * pofd_dev[n] (n <= 262144, larger n returns POFD_E_ARG), the non-zero bins
+ * (nzidx_dev[nnz] bin indices, nzcnt_dev[nnz] counts) of data binned at
+ * bincent0 + i*bindelta; out_dev[3] receives {(logL - like_offset) /
+ * like_norm, split index, flux of the first unwrapped element} and
+ * *status_dev the POFD_* status of the split/unwrap.  The grid (dflux,
+ * minflux_R, wrapRidx), the variance of R without noise (var_noi) and the
+ * noise sigma are those of PDFactory.  Work is enqueued on stream (a
+ * cudaStream_t; NULL = the legacy default stream) of the current device; the
+ * call returns after enqueueing.  Its scratch is a fixed static device array
+ * shared by all calls (one per GPU, held until exit): calls that overlap on
+ * the GPU race, so serialise them.  The first call on a device looks the
+ * array up with cudaGetSymbolAddress; make it before any stream capture. */
+int pofd_pd1_loglike_noalloc(const double* pofd_dev, unsigned n, double dflux,
+                             double minflux_R, unsigned wrapRidx,
+                             double var_noi, double sigma,
+                             const int* nzidx_dev, const double* nzcnt_dev,
+                             unsigned nnz, double bincent0, double bindelta,
+                             double like_offset, double like_norm,
+                             double* out_dev, int* status_dev, void* stream);
+
 /* Measured FP64 FMA throughput of a device (TFLOP/s, 2 flops per FMA): the
  * denominator of the FP64-bound kernels' roofline.  No counterpart in the
  * reference (which has no GPU code). */

@@ -56,6 +56,8 @@ SIGNATURES = {
     "pofd_like1_profile": (I, [V, U, _fp, U, I, _dp, C.POINTER(I)]),
     "pofd_like1_stage_name": (C.c_char_p, [I]),
     "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
+    "pofd_pd1_loglike_noalloc": (I, [V, U, D, D, U, D, D, V, V, U, D, D, D, D,
+                                     V, V, V]),
 }
 
 _lib = None
