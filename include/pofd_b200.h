@@ -49,6 +49,8 @@ typedef struct pofd_ctx pofd_ctx;
 typedef struct pofd_beam1 pofd_beam1;
 typedef struct pofd_like1 pofd_like1;
 typedef struct pofd_pdfactory1 pofd_pdfactory1;
+typedef struct pofd_beam2 pofd_beam2;
+typedef struct pofd_like2 pofd_like2;
 
 /* Message of the last error raised on this thread ("" if none). */
 const char* pofd_last_error(void);
@@ -174,6 +176,74 @@ int pofd_like1_profile(pofd_like1* L, unsigned nprop, const float* theta,
                        unsigned npar, int reps, double* stage_ms,
                        int* nstages);
 const char* pofd_like1_stage_name(int i);
+
+/* ------------------------------------------------------------- 2D beam
+ * Replaces doublebeam::doublebeam(file1, file2, histogram, NBINS, MINVAL)
+ * (doublebeam.h:81) with two in-memory pixel arrays of npix values each:
+ * doublebeam::setBeams (doublebeam.cc:331-462) and, if nhist > 0,
+ * makeHistogram(nhist) (doublebeam.cc:467-584). */
+int pofd_beam2_create(const double* pix1, const double* pix2, size_t npix,
+                      double pixsize, double minval, unsigned nhist,
+                      pofd_beam2** out);
+int pofd_beam2_destroy(pofd_beam2* b);
+/* info17 = {hassign[4], npix[4], ishist[4], nhist[4], pixsize} */
+int pofd_beam2_info(const pofd_beam2* b, double* info17);
+
+/* ---------------------------------------------------------- 2D likelihood
+ * calcLikeDouble (calcLikeDouble.h:192-347) with the log-normal colour
+ * model numberCountsDoubleLogNormal: nknots band-1 knots (log10 values),
+ * nsigma sigma knots and noffset offset knots (1: constant, 2: linear, >= 3:
+ * natural cubic spline, as numberCountsDoubleLogNormal.cc:109-139).  One
+ * square fftsize for all beam sets (calcLikeDouble.h:241); edge integration
+ * with nedge steps as PDFactoryDouble::initR (PDFactoryDouble.cc:355-585).
+ * Parameter layout: knot values, sigma values, offset values, sigma
+ * multiplier band 1, band 2 (calcLikeDouble.cc:1217-1218), bonus slots
+ * ignored.  Data are always binned (nbins x nbins). */
+int pofd_like2_create(pofd_ctx* ctx, unsigned nknots, const double* knotpos,
+                      unsigned nsigma, const double* sigmapos,
+                      unsigned noffset, const double* offsetpos,
+                      unsigned fftsize, unsigned nedge, int edge_integ,
+                      unsigned nbins, pofd_like2** out);
+int pofd_like2_destroy(pofd_like2* L);
+int pofd_like2_add_beamset(pofd_like2* L, const pofd_beam2* beam,
+                           double exp_conf1, double exp_conf2);
+int pofd_like2_add_dataset(pofd_like2* L, int beamset, const double* data1,
+                           const double* data2, size_t ndata, int meansub,
+                           double sigma_base1, double sigma_base2,
+                           double like_norm);
+/* setRRanges (calcLikeDouble.h:279, calcLikeDouble.cc:496-534). */
+int pofd_like2_set_rranges(pofd_like2* L, const float* theta, unsigned npar);
+/* range4 = {minRFlux1, maxRFlux1, minRFlux2, maxRFlux2} */
+int pofd_like2_get_rrange(const pofd_like2* L, int beamset, double* range4);
+/* info10 = {ndata, nbins, bincent01, bincent02, bindelta1, bindelta2,
+ *  like_offset, sigma_base1, sigma_base2, like_norm}; bins (may be NULL)
+ *  gets nbins*nbins counts. */
+int pofd_like2_dataset_info(const pofd_like2* L, int beamset, int dataset,
+                            double* info10, uint32_t* bins);
+int pofd_like2_reserve(pofd_like2* L, unsigned max_batch);
+/* getLogLike(p, pars_invalid) (calcLikeDouble.h:347). */
+int pofd_like2_loglike(pofd_like2* L, const float* theta, unsigned npar,
+                       double* logl, int* pars_invalid);
+int pofd_like2_eval_batch(pofd_like2* L, unsigned nprop, const float* theta,
+                          unsigned npar, double* logl, int* status);
+int pofd_like2_eval_batch_device(pofd_like2* L, unsigned nprop,
+                                 const float* theta_dev, unsigned npar,
+                                 double* logl_dev, int* status_dev,
+                                 void* stream);
+/* PDFactoryDouble::initPD + getPD (PDFactoryDouble.h:142-148) for one
+ * dataset: fftsize^2 values (row = band 1); info16 = {dflux1, dflux2, mean1,
+ * mean2, var1, var2, shift1, shift2, split1, split2, minflux1, minflux2,
+ * sg1pos, sg1neg, sg2pos, sg2neg}. */
+int pofd_like2_pd(pofd_like2* L, int beamset, int dataset, const float* theta,
+                  unsigned npar, int setlog, double* pd_out, double* info16);
+/* R (times dflux1*dflux2, edges filled) on the wrapped fftsize^2 grid. */
+int pofd_like2_get_r(pofd_like2* L, int beamset, const float* theta,
+                     unsigned npar, double* rvals_out);
+int pofd_like2_kernels_per_eval(const pofd_like2* L, int* nkernels);
+int pofd_like2_profile(pofd_like2* L, unsigned nprop, const float* theta,
+                       unsigned npar, int reps, double* stage_ms,
+                       int* nstages);
+const char* pofd_like2_stage_name(int i);
 
 /* Allocation-free split / unwrap / normalise / binned log-likelihood of
  * one wrapped 1D P(D) (the inverse-FFT output), for callers that cannot

@@ -56,6 +56,25 @@ SIGNATURES = {
     "pofd_like1_profile": (I, [V, U, _fp, U, I, _dp, C.POINTER(I)]),
     "pofd_like1_stage_name": (C.c_char_p, [I]),
     "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
+    "pofd_beam2_create": (I, [_dp, _dp, S, D, D, U, PV]),
+    "pofd_beam2_destroy": (I, [V]),
+    "pofd_beam2_info": (I, [V, _dp]),
+    "pofd_like2_create": (I, [V, U, _dp, U, _dp, U, _dp, U, U, I, U, PV]),
+    "pofd_like2_destroy": (I, [V]),
+    "pofd_like2_add_beamset": (I, [V, V, D, D]),
+    "pofd_like2_add_dataset": (I, [V, I, _dp, _dp, S, I, D, D, D]),
+    "pofd_like2_set_rranges": (I, [V, _fp, U]),
+    "pofd_like2_get_rrange": (I, [V, I, _dp]),
+    "pofd_like2_dataset_info": (I, [V, I, I, _dp, V]),
+    "pofd_like2_reserve": (I, [V, U]),
+    "pofd_like2_loglike": (I, [V, _fp, U, C.POINTER(D), C.POINTER(I)]),
+    "pofd_like2_eval_batch": (I, [V, U, _fp, U, _dp, _ip]),
+    "pofd_like2_eval_batch_device": (I, [V, U, V, U, V, V, V]),
+    "pofd_like2_pd": (I, [V, I, I, _fp, U, I, _dp, V]),
+    "pofd_like2_get_r": (I, [V, I, _fp, U, _dp]),
+    "pofd_like2_kernels_per_eval": (I, [V, C.POINTER(I)]),
+    "pofd_like2_profile": (I, [V, U, _fp, U, I, _dp, C.POINTER(I)]),
+    "pofd_like2_stage_name": (C.c_char_p, [I]),
     "pofd_pd1_loglike_noalloc": (I, [V, U, D, D, U, D, D, V, V, U, D, D, D, D,
                                      V, V, V]),
 }

@@ -1,0 +1,174 @@
+"""Python mirror of the reference's 2D (two-band) interfaces.
+
+  * doublebeam      doublebeam::doublebeam(file1, file2, histogram, NBINS,
+                    MINVAL) (doublebeam.h:81) from two in-memory pixel arrays
+  * calcLikeDouble  calcLikeDouble (calcLikeDouble.h:192-347) with the
+                    log-normal colour model: setRRanges(p), getLogLike(p) ->
+                    (logL, pars_invalid), getLogLikeBatch, getPD, getR.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, PofdError  # noqa: F401
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class doublebeam:
+    """Two-band beam split into pp/pn/np/nn sign components."""
+
+    def __init__(self, pix1, pix2, pixsize, histogram=False, nbins=150,
+                 minval=1e-6):
+        p1, p2 = _f64(pix1).ravel(), _f64(pix2).ravel()
+        if p1.size != p2.size:
+            raise PofdError(-10, "beams must have the same size")
+        h = C.c_void_p()
+        check(lib().pofd_beam2_create(p1, p2, p1.size, float(pixsize),
+                                      float(minval),
+                                      int(nbins) if histogram else 0,
+                                      C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pofd_beam2_destroy(self.h)
+            self.h = None
+
+    def info(self):
+        o = np.empty(17)
+        check(lib().pofd_beam2_info(self.h, o))
+        return {"hassign": o[0:4].astype(bool), "npix": o[4:8].astype(int),
+                "ishist": o[8:12].astype(bool), "nhist": o[12:16].astype(int),
+                "pixsize": o[16]}
+
+
+class calcLikeDouble:
+    """2D likelihood over beam sets and datasets."""
+
+    def __init__(self, ctx, knotpos, sigmapos, offsetpos, fftsize=4096,
+                 nedge=256, edge_integ=True, nbins=1000):
+        self.ctx = ctx
+        k, s, o = _f64(knotpos), _f64(sigmapos), _f64(offsetpos)
+        self.nmodel = k.size + s.size + o.size
+        self.fftsize = int(fftsize)
+        h = C.c_void_p()
+        check(lib().pofd_like2_create(ctx.h, k.size, k, s.size, s, o.size, o,
+                                      self.fftsize, int(nedge),
+                                      int(edge_integ), int(nbins),
+                                      C.byref(h)))
+        self.h = h
+        self._beams = []
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pofd_like2_destroy(self.h)
+            self.h = None
+
+    def addBeamSet(self, bm, exp_conf1=0.0, exp_conf2=0.0):
+        idx = check(lib().pofd_like2_add_beamset(self.h, bm.h,
+                                                 float(exp_conf1),
+                                                 float(exp_conf2)))
+        self._beams.append(bm)
+        return idx
+
+    def addDataset(self, beamset, data1, data2, sigma1, sigma2,
+                   like_norm=1.0, meansub=True):
+        a, b = _f64(data1).ravel(), _f64(data2).ravel()
+        if a.size != b.size:
+            raise PofdError(-10, "band maps differ in size")
+        check(lib().pofd_like2_add_dataset(self.h, int(beamset), a, b, a.size,
+                                           int(meansub), float(sigma1),
+                                           float(sigma2), float(like_norm)))
+
+    def setRRanges(self, p):
+        th = _f32(p)
+        check(lib().pofd_like2_set_rranges(self.h, th, th.size))
+
+    def getRRange(self, beamset):
+        out = np.empty(4)
+        check(lib().pofd_like2_get_rrange(self.h, int(beamset), out))
+        return out
+
+    def datasetInfo(self, beamset, ds):
+        o = np.empty(10)
+        check(lib().pofd_like2_dataset_info(self.h, int(beamset), int(ds), o,
+                                            None))
+        keys = ["ndata", "nbins", "bincent01", "bincent02", "bindelta1",
+                "bindelta2", "like_offset", "sigma_base1", "sigma_base2",
+                "like_norm"]
+        info = dict(zip(keys, o))
+        nb = int(info["nbins"])
+        bins = np.zeros(nb * nb, dtype=np.uint32)
+        check(lib().pofd_like2_dataset_info(self.h, int(beamset), int(ds), o,
+                                            _lib.ptr(bins)))
+        info["bins"] = bins.reshape(nb, nb)
+        return info
+
+    def reserve(self, max_batch):
+        check(lib().pofd_like2_reserve(self.h, int(max_batch)))
+
+    def getLogLike(self, p):
+        th = _f32(p)
+        ll = C.c_double()
+        inv = C.c_int()
+        check(lib().pofd_like2_loglike(self.h, th, th.size, C.byref(ll),
+                                       C.byref(inv)))
+        return ll.value, bool(inv.value)
+
+    def getLogLikeBatch(self, thetas):
+        th = _f32(thetas)
+        nprop, npar = th.shape
+        ll = np.empty(nprop)
+        st = np.empty(nprop, dtype=np.int32)
+        check(lib().pofd_like2_eval_batch(self.h, nprop, th.ravel(), npar, ll,
+                                          st))
+        return ll, st
+
+    def getLogLikeDevice(self, nprop, theta_ptr, npar, logl_ptr, status_ptr,
+                         stream=None):
+        check(lib().pofd_like2_eval_batch_device(
+            self.h, int(nprop), C.c_void_p(theta_ptr), int(npar),
+            C.c_void_p(logl_ptr), C.c_void_p(status_ptr),
+            C.c_void_p(stream) if stream else None))
+
+    def getPD(self, beamset, ds, p, setLog=True):
+        th = _f32(p)
+        n = self.fftsize
+        out = np.empty(n * n)
+        info = np.empty(16)
+        check(lib().pofd_like2_pd(self.h, int(beamset), int(ds), th, th.size,
+                                  int(setLog), out, _lib.ptr(info)))
+        keys = ["dflux1", "dflux2", "mn1", "mn2", "var1", "var2", "shift1",
+                "shift2", "split1", "split2", "pd_minflux1", "pd_minflux2",
+                "sg1pos", "sg1neg", "sg2pos", "sg2neg"]
+        return out.reshape(n, n), dict(zip(keys, info))
+
+    def getR(self, beamset, p):
+        th = _f32(p)
+        n = self.fftsize
+        out = np.empty(n * n)
+        check(lib().pofd_like2_get_r(self.h, int(beamset), th, th.size, out))
+        return out.reshape(n, n)
+
+    def profileStages(self, thetas, reps=3):
+        th = _f32(thetas)
+        nprop, npar = th.shape
+        ms = np.zeros(16)
+        ns = C.c_int()
+        check(lib().pofd_like2_profile(self.h, nprop, th.ravel(), npar,
+                                       int(reps), ms, C.byref(ns)))
+        return {lib().pofd_like2_stage_name(i).decode(): ms[i]
+                for i in range(ns.value)}
+
+    def kernelsPerEval(self):
+        k = C.c_int()
+        check(lib().pofd_like2_kernels_per_eval(self.h, C.byref(k)))
+        return k.value

@@ -11,6 +11,7 @@
 
 #include "../../include/pofd_b200.h"
 #include "engine1d.cuh"
+#include "engine2d.cuh"
 #include "setup.hh"
 
 namespace {
@@ -49,6 +50,15 @@ struct pofd_beam1 {
 struct pofd_like1 {
   pofd_ctx* ctx = nullptr;
   std::unique_ptr<pofd::Engine1> eng;
+};
+
+struct pofd_beam2 {
+  pofd::Beam2 b;
+};
+
+struct pofd_like2 {
+  pofd_ctx* ctx = nullptr;
+  std::unique_ptr<pofd::Engine2> eng;
 };
 
 struct pofd_pdfactory1 {
@@ -404,5 +414,190 @@ int pofd_like1_profile(pofd_like1* L, unsigned nprop, const float* theta,
 }
 
 const char* pofd_like1_stage_name(int i) { return pofd::Engine1::stage_name(i); }
+
+// ------------------------------------------------------------- 2D beam
+int pofd_beam2_create(const double* pix1, const double* pix2, size_t npix,
+                      double pixsize, double minval, unsigned nhist,
+                      pofd_beam2** out) {
+  return guard([&] {
+    need(pix1 && pix2 && out, "null argument");
+    std::unique_ptr<pofd_beam2> b(new pofd_beam2());
+    b->b.build(pix1, pix2, npix, pixsize, minval);
+    if (nhist > 0) b->b.histogram(nhist);
+    *out = b.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_beam2_destroy(pofd_beam2* b) {
+  delete b;
+  return POFD_OK;
+}
+
+int pofd_beam2_info(const pofd_beam2* bp, double* o) {
+  return guard([&] {
+    need(bp && o, "null argument");
+    const pofd::Beam2& b = bp->b;
+    for (int s = 0; s < 4; ++s) {
+      o[s] = b.hassign[s];
+      o[4 + s] = static_cast<double>(b.pix1[s].size());
+      o[8 + s] = b.ishist[s];
+      o[12 + s] = static_cast<double>(b.binwt[s].size());
+    }
+    o[16] = b.pixsize;
+    return POFD_OK;
+  });
+}
+
+// ---------------------------------------------------------- 2D likelihood
+int pofd_like2_create(pofd_ctx* ctx, unsigned nknots, const double* knotpos,
+                      unsigned nsigma, const double* sigmapos,
+                      unsigned noffset, const double* offsetpos,
+                      unsigned fftsize, unsigned nedge, int edge_integ,
+                      unsigned nbins, pofd_like2** out) {
+  return guard([&] {
+    need(ctx && knotpos && sigmapos && offsetpos && out, "null argument");
+    if (ctx->device >= 0) cudaSetDevice(ctx->device);
+    std::unique_ptr<pofd_like2> L(new pofd_like2());
+    L->ctx = ctx;
+    L->eng.reset(new pofd::Engine2(ctx->device, ctx->stream));
+    L->eng->configure(nknots, knotpos, nsigma, sigmapos, noffset, offsetpos,
+                      fftsize, nedge, edge_integ != 0, nbins);
+    *out = L.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_destroy(pofd_like2* L) {
+  if (L && L->ctx && L->ctx->device >= 0) cudaSetDevice(L->ctx->device);
+  delete L;
+  return POFD_OK;
+}
+
+int pofd_like2_add_beamset(pofd_like2* L, const pofd_beam2* beam,
+                           double ec1, double ec2) {
+  return guard([&] {
+    need(L && beam, "null argument");
+    return L->eng->add_beamset(beam->b, ec1, ec2);
+  });
+}
+
+int pofd_like2_add_dataset(pofd_like2* L, int beamset, const double* d1,
+                           const double* d2, size_t nd, int meansub,
+                           double sb1, double sb2, double like_norm) {
+  return guard([&] {
+    need(L && d1 && d2, "null argument");
+    L->eng->add_dataset(beamset, d1, d2, nd, meansub != 0, sb1, sb2, like_norm);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_set_rranges(pofd_like2* L, const float* theta, unsigned npar) {
+  return guard([&] {
+    need(L && theta, "null argument");
+    L->eng->set_rranges(theta, npar);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_get_rrange(const pofd_like2* L, int beamset, double* r4) {
+  return guard([&] {
+    need(L && r4, "null argument");
+    L->eng->rrange(beamset, r4);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_dataset_info(const pofd_like2* L, int beamset, int dataset,
+                            double* info10, uint32_t* bins) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->dataset_info(beamset, dataset, info10, bins);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_reserve(pofd_like2* L, unsigned max_batch) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->reserve(max_batch);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_loglike(pofd_like2* L, const float* theta, unsigned npar,
+                       double* logl, int* pars_invalid) {
+  return guard([&] {
+    need(L && theta && logl, "null argument");
+    int st = 0;
+    L->eng->eval_host(1, theta, npar, logl, &st);
+    if (pars_invalid) *pars_invalid = (st == POFD_REJECTED) ? 1 : 0;
+    if (st < 0) throw pofd::Error(st, "likelihood evaluation failed");
+    return st;
+  });
+}
+
+int pofd_like2_eval_batch(pofd_like2* L, unsigned nprop, const float* theta,
+                          unsigned npar, double* logl, int* status) {
+  return guard([&] {
+    need(L && theta && logl && status, "null argument");
+    L->eng->eval_host(nprop, theta, npar, logl, status);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_eval_batch_device(pofd_like2* L, unsigned nprop,
+                                 const float* theta_dev, unsigned npar,
+                                 double* logl_dev, int* status_dev,
+                                 void* stream) {
+  return guard([&] {
+    need(L && theta_dev && logl_dev && status_dev, "null argument");
+    L->eng->enqueue(nprop, theta_dev, npar, logl_dev, status_dev,
+                    static_cast<cudaStream_t>(stream));
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_pd(pofd_like2* L, int beamset, int dataset, const float* theta,
+                  unsigned npar, int setlog, double* pd_out, double* info16) {
+  return guard([&] {
+    need(L && theta && pd_out, "null argument");
+    const int st = L->eng->pd_host(beamset, dataset, theta, npar, setlog != 0,
+                                   pd_out, info16);
+    if (st != 0) throw pofd::Error(st, "P(D) unwrap failed (split point or mean)");
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_get_r(pofd_like2* L, int beamset, const float* theta,
+                     unsigned npar, double* out) {
+  return guard([&] {
+    need(L && theta && out, "null argument");
+    L->eng->rgrid_host(beamset, theta, npar, out);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_kernels_per_eval(const pofd_like2* L, int* nk) {
+  return guard([&] {
+    need(L && nk, "null argument");
+    *nk = L->eng->kernels_per_eval();
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_profile(pofd_like2* L, unsigned nprop, const float* theta,
+                       unsigned npar, int reps, double* stage_ms,
+                       int* nstages) {
+  return guard([&] {
+    need(L && theta && stage_ms && nstages, "null argument");
+    need(reps > 0, "reps must be > 0");
+    L->eng->profile_stages(nprop, theta, npar, reps, stage_ms);
+    *nstages = pofd::Engine2::kNumStages;
+    return POFD_OK;
+  });
+}
+
+const char* pofd_like2_stage_name(int i) { return pofd::Engine2::stage_name(i); }
 
 }  // extern "C"

@@ -1,0 +1,1633 @@
+// engine2d.cu -- 2D (two-band) P(D) likelihood: sm_100a kernels + engine.
+//
+// Reference path restated (aconley/pofd_affine 0.5.1):
+//   numberCountsDoubleLogNormal::setParams / sigma / offset
+//                          numberCountsDoubleLogNormal.cc:1010-1052, 1172-1193
+//   numberCountsDoubleLogNormal::getR (row precompute + column loop)
+//                          numberCountsDoubleLogNormal.cc:1788-2007
+//   PDFactoryDouble::initRFlux / initR (edge integrals) / getRStats
+//                          PDFactoryDouble.cc:18-49, 313-722
+//   PDFactoryDouble::initPD / getPD                PDFactoryDouble.cc:1145-1499
+//   PDFactoryDouble::findSplitPoint / unwrap       PDFactoryDouble.cc:784-1118
+//   PDDouble::normalize / getMeans / applyLog / getLogLikeBinned
+//                          PDDouble.cc:142-447, 1103-1222
+//   calcLikeDoubleSingle::getLogLike / calcLikeDouble::getLogLike
+//                          calcLikeDouble.cc:553-616, 1195-1277
+//
+// HBM layout (P proposals, B beam sets, D datasets, n grid, nc = n/2+1,
+// T terms per row slot):
+//   rw    [P][B][n + nedge][T][3]  per-row colour terms (c0, c1, c2)
+//   rbuf  [P][B][n][2nc]           R grid (x dflux1 dflux2), then its 2D
+//                                  spectrum in place
+//   pbuf  [P][D][n][2nc]           per-dataset spectrum, then the P(D)
+//   rowpart/colpart                marginal partial sums of the P(D)
+#include "engine2d.cuh"
+
+#include <cstring>
+#include <sstream>
+
+#include "common.cuh"
+
+namespace pofd {
+
+namespace {
+
+constexpr int NT = 256;
+constexpr int RB = 4;        // R-grid rows per block
+constexpr int RTILE = 32;    // P(D) rows per scan block
+constexpr int GCH = 1024;    // data bins per gather block
+constexpr int KMAX = Engine2::KMAX;
+constexpr int MAXT = 2048;   // colour terms per row slot held in shared memory
+constexpr int SNT = 1024;    // threads of the split kernel
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    std::ostringstream s;
+    s << what << ": " << cudaGetErrorString(e);
+    throw Error(e == cudaErrorMemoryAllocation ? POFD_E_NOMEM : POFD_E_CUDA, s.str());
+  }
+}
+void fk(cufftResult r, const char* what) {
+  if (r != CUFFT_SUCCESS) {
+    std::ostringstream s;
+    s << what << ": cuFFT error " << static_cast<int>(r);
+    throw Error(r == CUFFT_ALLOC_FAILED ? POFD_E_NOMEM : POFD_E_CUDA, s.str());
+  }
+}
+template <class T>
+T* dal(size_t n) {
+  void* p = nullptr;
+  ck(cudaMalloc(&p, n * sizeof(T) + 16), "cudaMalloc");
+  return static_cast<T*>(p);
+}
+
+__device__ __forceinline__ long long sat_index(double v) {
+  if (!(v < 9.0e15)) return 0x7fffffffffffLL;
+  if (!(v > -9.0e15)) return -0x7fffffffffffLL;
+  return static_cast<long long>(v);
+}
+__device__ __forceinline__ double clip0(double v) { return (v < 0) ? 0.0 : v; }
+
+// ------------------------------------------------------------- model
+// Natural cubic spline through (x, y), written per interval as (y,b,c,d);
+// out[4*(n-1)] holds y[n-1].
+__device__ void nat_spline(const double* x, const double* y, int n,
+                           double* out, double* wk) {
+  double* c = wk;
+  double* g = c + KMAX;
+  double* diag = g + KMAX;
+  double* off = diag + KMAX;
+  double* alp = off + KMAX;
+  double* gam = alp + KMAX;
+  for (int k = 0; k < n; ++k) c[k] = 0.0;
+  const int N = n - 2;
+  for (int i = 0; i < N; ++i) {
+    const double h_i = x[i + 1] - x[i], h_ip1 = x[i + 2] - x[i + 1];
+    const double g_i = (h_i != 0.0) ? 1.0 / h_i : 0.0;
+    const double g_ip1 = (h_ip1 != 0.0) ? 1.0 / h_ip1 : 0.0;
+    off[i] = h_ip1;
+    diag[i] = 2.0 * (h_ip1 + h_i);
+    g[i] = 3.0 * ((y[i + 2] - y[i + 1]) * g_ip1 - (y[i + 1] - y[i]) * g_i);
+  }
+  if (N == 1) {
+    c[1] = g[0] / diag[0];
+  } else if (N > 1) {
+    alp[0] = diag[0];
+    gam[0] = off[0] / alp[0];
+    for (int i = 1; i < N - 1; ++i) {
+      alp[i] = diag[i] - off[i - 1] * gam[i - 1];
+      gam[i] = off[i] / alp[i];
+    }
+    alp[N - 1] = diag[N - 1] - off[N - 2] * gam[N - 2];
+    for (int i = 1; i < N; ++i) g[i] = g[i] - gam[i - 1] * g[i - 1];
+    for (int i = 0; i < N; ++i) g[i] = g[i] / alp[i];
+    c[N] = g[N - 1];
+    for (int i = N - 2; i >= 0; --i) c[1 + i] = g[i] - gam[i] * c[2 + i];
+  }
+  for (int i = 0; i < n - 1; ++i) {
+    const double dx = x[i + 1] - x[i];
+    const double dy = y[i + 1] - y[i];
+    out[4 * i + 0] = y[i];
+    out[4 * i + 1] = (dy / dx) - dx * (c[i + 1] + 2.0 * c[i]) / 3.0;
+    out[4 * i + 2] = c[i];
+    out[4 * i + 3] = (c[i + 1] - c[i]) / (3.0 * dx);
+  }
+  out[4 * (n - 1)] = y[n - 1];
+}
+
+// Knot counts (log2-log2 natural spline), sigma and offset curves of one
+// proposal (numberCountsDoubleLogNormal.cc:1010-1052): cnt layout
+// [0,4K) counts, [4K,8K) sigma, [8K,12K) offset; values of 1- or 2-knot
+// curves sit at stride 4.
+__global__ void k_model2(Model2Dev m, const float* __restrict__ theta,
+                         int npar, double logfac, double* __restrict__ cnt,
+                         int* __restrict__ mstatus,
+                         double* __restrict__ sigmult) {
+  __shared__ double wk[6 * KMAX];
+  __shared__ double y[KMAX];
+  __shared__ double o[12 * KMAX];
+  const int w = blockIdx.x;
+  const float* th = theta + static_cast<size_t>(w) * npar;
+  if (threadIdx.x == 0) {
+    int st = 0;
+    const int K = m.K, ns = m.ns, no = m.no;
+    for (int k = 0; k < K; ++k) {
+      y[k] = logfac * static_cast<double>(th[k]);
+      if (isnan(y[k])) st = POFD_E_INVALID_MODEL;
+    }
+    if (st == 0) nat_spline(m.logknots, y, K, o, wk);
+    for (int k = 0; k < ns; ++k) {
+      const double v = static_cast<double>(th[K + k]);
+      if (isnan(v) || isinf(v)) st = POFD_E_INVALID_MODEL;
+      y[k] = v;
+    }
+    if (st == 0) {
+      if (ns > 2) nat_spline(m.sk, y, ns, o + 4 * KMAX, wk);
+      else for (int k = 0; k < ns; ++k) o[4 * KMAX + 4 * k] = y[k];
+    }
+    for (int k = 0; k < no; ++k) {
+      const double v = static_cast<double>(th[K + ns + k]);
+      if (isnan(v)) st = POFD_E_INVALID_MODEL;
+      y[k] = v;
+    }
+    if (st == 0) {
+      if (no > 2) nat_spline(m.ok, y, no, o + 8 * KMAX, wk);
+      else for (int k = 0; k < no; ++k) o[8 * KMAX + 4 * k] = y[k];
+    }
+    mstatus[w] = st;
+    sigmult[2 * w] = static_cast<double>(th[K + ns + no]);
+    sigmult[2 * w + 1] = static_cast<double>(th[K + ns + no + 1]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 12 * KMAX; i += blockDim.x)
+    cnt[static_cast<size_t>(w) * 12 * KMAX + i] = o[i];
+}
+
+__device__ __forceinline__ double spline_at(const double* x, const double* s,
+                                            int n, double v) {
+  const int k = dev::bsearch_lo(x, v, 0, n - 1);
+  const double dl = v - x[k];
+  const double* q = s + 4 * k;
+  return q[0] + dl * (q[1] + dl * (q[2] + dl * q[3]));
+}
+
+// getSigmaInner / getOffsetInner: constant (1 knot), linear (2), natural
+// cspline (>= 3), clamped outside the knots; sigma floored at min_sigma
+// inside the knot range only.
+__device__ __forceinline__ double curve_at(const double* x, const double* s,
+                                           int n, double v, bool floor_sig,
+                                           double min_sigma) {
+  if (n == 1) return s[0];
+  if (v <= x[0]) return s[0];
+  if (v >= x[n - 1]) return s[4 * (n - 1)];
+  double val;
+  if (n == 2) val = s[0] + (v - x[0]) / (x[1] - x[0]) * (s[4] - s[0]);
+  else val = spline_at(x, s, n, v);
+  if (floor_sig) val = (val < min_sigma) ? min_sigma : val;
+  return val;
+}
+
+// Per-row colour terms (numberCountsDoubleLogNormal.cc:1883-1963), one thread
+// per (row, term slot): c0 = weight * counts / sigma * prefac (0 marks a
+// term to skip), c1 = log f1 + offset - log(beam1/beam2), c2 = -1/(2 ln2
+// sigma^2).
+__global__ void __launch_bounds__(NT)
+k_rows2(const BSet2Dev* __restrict__ bsets, Model2Dev m, int B,
+        double ilog2toe, const int* __restrict__ mstatus,
+        const double* __restrict__ cnt, double* __restrict__ rw) {
+  const int wb = blockIdx.y;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet2Dev& bs = bsets[b];
+  const int T = bs.T;
+  const long long t = static_cast<long long>(blockIdx.x) * NT + threadIdx.x;
+  if (t >= static_cast<long long>(bs.nrows) * T) return;
+  const int r = static_cast<int>(t / T), k = static_cast<int>(t - static_cast<long long>(r) * T);
+  double* out = rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3 + 3 * k;
+  const int sgn1 = bs.rowsgn[r];
+  double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+  if (sgn1 >= 0) {
+    const int np = bs.hassign[sgn1] ? bs.sg[sgn1].nt : 0;
+    const int nn = bs.hassign[sgn1 + 1] ? bs.sg[sgn1 + 1].nt : 0;
+    int sgn = -1, j = 0;
+    if (k < np) { sgn = sgn1; j = k; }
+    else if (k < np + nn) { sgn = sgn1 + 1; j = k - np; }
+    if (sgn >= 0) {
+      const Sign2Dev& sg = bs.sg[sgn];
+      const double f1val = fabs(bs.rowflux[r]);
+      if (f1val < sg.maxf1) {
+        const double ieta1 = sg.ieta1[j];
+        const double f1prod = f1val * ieta1;
+        if (f1prod >= m.minknot && f1prod < m.maxknot) {
+          const double* cs = cnt + static_cast<size_t>(w) * 12 * KMAX;
+          const double cts = exp2(spline_at(m.logknots, cs, m.K, log2(f1prod)));
+          if (cts > 0) {
+            const double isigma =
+                1.0 / curve_at(m.sk, cs + 4 * KMAX, m.ns, f1prod, true, m.min_sigma);
+            if (sg.ishist) c0 = sg.w[j] * ieta1 * isigma * cts * bs.prefac;
+            else c0 = cts * ieta1 * isigma * bs.prefac;
+            c1 = bs.rowlog[r] + curve_at(m.ok, cs + 8 * KMAX, m.no, f1prod, false, 0.0) -
+                 sg.logratio[j];
+            c2 = -0.5 * isigma * isigma * ilog2toe;
+          }
+        }
+      }
+    }
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+}
+
+// Stable block-wide compaction count: exclusive position of this thread's
+// set flag among the block's set flags, and the total.
+__device__ __forceinline__ int block_excl_count(bool flag, int& total, int* sh) {
+  const unsigned ballot = __ballot_sync(0xffffffffu, flag);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int within = __popc(ballot & ((1u << lane) - 1u));
+  if (lane == 0) sh[warp] = __popc(ballot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int i = 0; i < nw; ++i) {
+      const int c = sh[i];
+      sh[i] = acc;
+      acc += c;
+    }
+    sh[nw] = acc;
+  }
+  __syncthreads();
+  const int pos = sh[warp] + within;
+  total = sh[nw];
+  __syncthreads();
+  return pos;
+}
+
+// Stage one row's non-zero terms in shared memory, positive-f2 and
+// negative-f2 lists separately, in the reference's order.
+__device__ void stage_row(const BSet2Dev& bs, const double* __restrict__ rwrow,
+                          int sgn1, double* s_pos, double* s_neg, int* s_cnt,
+                          int* sh) {
+  int np = 0, nn = 0;
+  if (sgn1 >= 0) {
+    np = bs.hassign[sgn1] ? bs.sg[sgn1].nt : 0;
+    nn = bs.hassign[sgn1 + 1] ? bs.sg[sgn1 + 1].nt : 0;
+  }
+  int bp = 0, bn = 0;
+  for (int k0 = 0; k0 < np + nn; k0 += blockDim.x) {
+    const int k = k0 + threadIdx.x;
+    const bool valid = k < np + nn;
+    double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+    if (valid) {
+      c0 = rwrow[3 * k];
+      c1 = rwrow[3 * k + 1];
+      c2 = rwrow[3 * k + 2];
+    }
+    const bool fp = valid && k < np && c0 != 0.0;
+    const bool fn = valid && k >= np && c0 != 0.0;
+    int tp, tn;
+    const int ip = block_excl_count(fp, tp, sh);
+    const int in = block_excl_count(fn, tn, sh);
+    if (fp) {
+      double* q = s_pos + 3 * (bp + ip);
+      q[0] = c0; q[1] = c1; q[2] = c2;
+    }
+    if (fn) {
+      double* q = s_neg + 3 * (bn + in);
+      q[0] = c0; q[1] = c1; q[2] = c2;
+    }
+    bp += tp;
+    bn += tn;
+  }
+  if (threadIdx.x == 0) {
+    s_cnt[0] = bp;
+    s_cnt[1] = bn;
+  }
+  __syncthreads();
+}
+
+// R(f1 row, f2 column j) from a staged row (numberCountsDoubleLogNormal.cc:
+// 1972-2002): (sum_k c0 2^{(log|f2| - c1)^2 c2}) / |f2|.
+__device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
+                                       const double* s_pos,
+                                       const double* s_neg, int npos,
+                                       int nneg, int j) {
+  if (sgn1 < 0) return 0.0;
+  const double if2 = bs.colinv[j];
+  if (if2 == 0) return 0.0;
+  const int fs = bs.colsgn[j];
+  if (!bs.hassign[sgn1 + fs]) return 0.0;
+  const double* L = fs ? s_neg : s_pos;
+  const int cnt = fs ? nneg : npos;
+  const double lf2 = bs.collog[j];
+  double wv = 0.0;
+  for (int k = 0; k < cnt; ++k) {
+    const double tfac = lf2 - L[3 * k + 1];
+    wv += L[3 * k] * exp2(tfac * tfac * L[3 * k + 2]);
+  }
+  return wv * if2;
+}
+
+// Main R grid, rows 1..n-1 x columns 1..n-1 (row 0 and column 0 are the
+// edge cells), times dflux1*dflux2, with block partial sums of the
+// trapezoid moments of getRStats (PDFactoryDouble.cc:593-722).
+__global__ void __launch_bounds__(NT)
+k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
+         const int* __restrict__ mstatus, const double* __restrict__ rw,
+         double* __restrict__ rbuf, double* __restrict__ rpart) {
+  extern __shared__ double sm[];
+  __shared__ int sh[40];
+  __shared__ int s_cnt[2];
+  __shared__ double shr[32];
+  const int wb = blockIdx.z;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet2Dev& bs = bsets[b];
+  const int T = bs.T;
+  double* s_pos = sm;
+  double* s_neg = sm + 3 * T;
+  const int j = blockIdx.x * NT + threadIdx.x;
+  const double fluxfac = bs.dflux1 * bs.dflux2;
+  const double cf2 = (j < n) ? bs.rflux2[j] : 0.0;
+  const double wc = (j == n - 1) ? 0.5 : 1.0;
+  double m1 = 0.0, v1 = 0.0, m2 = 0.0, v2 = 0.0;
+  for (int rr = 0; rr < RB; ++rr) {
+    const int r = 1 + blockIdx.y * RB + rr;
+    if (r >= n) break;
+    const int sgn1 = bs.rowsgn[r];
+    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3, sgn1,
+              s_pos, s_neg, s_cnt, sh);
+    if (j >= 1 && j < n) {
+      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j) * fluxfac;
+      rbuf[(static_cast<size_t>(wb) * n + r) * nc2 + j] = R;
+      const double cf1 = bs.rowflux[r];
+      const double cR = (r == n - 1) ? 0.5 * R : R;
+      const double p1 = wc * cf1 * cR;
+      const double p2 = wc * cf2 * cR;
+      m1 += p1;
+      v1 += cf1 * p1;
+      m2 += p2;
+      v2 += cf2 * p2;
+    }
+    __syncthreads();
+  }
+  m1 = dev::block_sum<NT>(m1, shr);
+  v1 = dev::block_sum<NT>(v1, shr);
+  m2 = dev::block_sum<NT>(m2, shr);
+  v2 = dev::block_sum<NT>(v2, shr);
+  if (threadIdx.x == 0) {
+    double* o = rpart + ((static_cast<size_t>(wb) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * 4;
+    o[0] = m1; o[1] = v1; o[2] = m2; o[3] = v2;
+  }
+}
+
+// Edge integral along band 1 for row 0 (PDFactoryDouble.cc:472-514):
+// Rx[j] = iRxnorm * log-trapezoid over the edge band-1 fluxes of R.
+__global__ void __launch_bounds__(NT)
+k_rx2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
+      const int* __restrict__ mstatus, const double* __restrict__ rw,
+      double* __restrict__ redge) {
+  extern __shared__ double sm[];
+  __shared__ int sh[40];
+  __shared__ int s_cnt[2];
+  const int wb = blockIdx.y;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet2Dev& bs = bsets[b];
+  const int T = bs.T;
+  double* s_pos = sm;
+  double* s_neg = sm + 3 * T;
+  const int j = blockIdx.x * NT + threadIdx.x;
+  double acc = 0.0;
+  for (int i = 0; i < nedge; ++i) {
+    const int r = n + i;
+    const int sgn1 = bs.rowsgn[r];
+    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3, sgn1,
+              s_pos, s_neg, s_cnt, sh);
+    if (j < n) {
+      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j);
+      const double rf = bs.e1[i];
+      if (i == 0) acc = 0.5 * rf * R;
+      else if (i == nedge - 1) acc += 0.5 * rf * R;
+      else acc += rf * R;
+    }
+    __syncthreads();
+  }
+  if (j < n) redge[static_cast<size_t>(wb) * (2 * n + 1) + j] = acc * bs.iRxnorm;
+}
+
+// Edge integral along band 2 for column 0 (PDFactoryDouble.cc:518-550):
+// one block per row, threads over the edge band-2 fluxes.
+__global__ void __launch_bounds__(NT)
+k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
+      const int* __restrict__ mstatus, const double* __restrict__ rw,
+      double* __restrict__ redge) {
+  extern __shared__ double sm[];
+  __shared__ int sh[40];
+  __shared__ int s_cnt[2];
+  __shared__ double shr[32];
+  const int wb = blockIdx.y;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet2Dev& bs = bsets[b];
+  const int T = bs.T;
+  const int r = blockIdx.x + 1;  // main rows 1..n-1
+  if (r >= n) return;
+  double* s_pos = sm;
+  double* s_neg = sm + 3 * T;
+  const int sgn1 = bs.rowsgn[r];
+  stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3, sgn1,
+            s_pos, s_neg, s_cnt, sh);
+  double acc = 0.0;
+  for (int jj = threadIdx.x; jj < nedge; jj += NT) {
+    const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], n + jj);
+    acc += (jj == 0 || jj == nedge - 1) ? 0.5 * R : R;
+  }
+  acc = dev::block_sum<NT>(acc, shr);
+  if (threadIdx.x == 0)
+    redge[static_cast<size_t>(wb) * (2 * n + 1) + n + r] = acc * bs.iRynorm;
+}
+
+// r[0,0]: the double edge integral (PDFactoryDouble.cc:426-467).
+__global__ void __launch_bounds__(NT)
+k_r002(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
+       const int* __restrict__ mstatus, const double* __restrict__ rw,
+       double* __restrict__ redge) {
+  extern __shared__ double sm[];
+  __shared__ int sh[40];
+  __shared__ int s_cnt[2];
+  __shared__ double shr[32];
+  const int wb = blockIdx.x;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet2Dev& bs = bsets[b];
+  const int T = bs.T;
+  double* s_pos = sm;
+  double* s_neg = sm + 3 * T;
+  double s = 0.0;
+  for (int i = 0; i < nedge; ++i) {
+    const int r = n + i;
+    const int sgn1 = bs.rowsgn[r];
+    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3, sgn1,
+              s_pos, s_neg, s_cnt, sh);
+    double acc = 0.0;
+    for (int jj = threadIdx.x; jj < nedge; jj += NT) {
+      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], n + jj);
+      acc += (jj == 0 || jj == nedge - 1) ? 0.5 * R : R;
+    }
+    acc = dev::block_sum<NT>(acc, shr);
+    const double rf = bs.e1[i];
+    if (i == 0) s = 0.5 * rf * acc;
+    else if (i == nedge - 1) s += 0.5 * rf * acc;
+    else s += rf * acc;
+  }
+  if (threadIdx.x == 0) redge[static_cast<size_t>(wb) * (2 * n + 1) + 2 * n] = s * bs.iR00norm;
+}
+
+// Edge cells into the grid (times dflux1*dflux2), the remaining moment
+// contributions and the shift decisions (PDFactoryDouble.cc:560-585,
+// 1198-1213).
+__global__ void __launch_bounds__(NT)
+k_rfinish2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
+           int edge, int nparts, const int* __restrict__ mstatus,
+           const double* __restrict__ redge, const double* __restrict__ rpart,
+           double* __restrict__ rbuf, double* __restrict__ mom) {
+  __shared__ double shr[32];
+  const int wb = blockIdx.x;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet2Dev& bs = bsets[b];
+  const double fluxfac = bs.dflux1 * bs.dflux2;
+  const double* E = redge + static_cast<size_t>(wb) * (2 * n + 1);
+  double* R = rbuf + static_cast<size_t>(wb) * n * nc2;
+  double m1 = 0.0, v1 = 0.0, m2 = 0.0, v2 = 0.0;
+  // row 0 (row factor 1/2), all columns
+  const double cf1r0 = bs.rowflux[0];
+  for (int j = threadIdx.x; j < n; j += NT) {
+    const double val = edge ? ((j == 0) ? E[2 * n] : E[j]) * fluxfac : 0.0;
+    R[j] = val;
+    const double cR = 0.5 * val;
+    const double wc = (j == 0 || j == n - 1) ? 0.5 : 1.0;
+    const double cf2 = bs.rflux2[j];
+    const double p1 = wc * cf1r0 * cR, p2 = wc * cf2 * cR;
+    m1 += p1; v1 += cf1r0 * p1; m2 += p2; v2 += cf2 * p2;
+  }
+  // column 0 (column factor 1/2), rows 1..n-1
+  const double cf20 = bs.rflux2[0];
+  for (int i = 1 + threadIdx.x; i < n; i += NT) {
+    const double val = edge ? E[n + i] * fluxfac : 0.0;
+    R[static_cast<size_t>(i) * nc2] = val;
+    const double cR = (i == n - 1) ? 0.5 * val : val;
+    const double cf1 = bs.rowflux[i];
+    const double p1 = 0.5 * cf1 * cR, p2 = 0.5 * cf20 * cR;
+    m1 += p1; v1 += cf1 * p1; m2 += p2; v2 += cf20 * p2;
+  }
+  const double* pp = rpart + static_cast<size_t>(wb) * nparts * 4;
+  for (int k = threadIdx.x; k < nparts; k += NT) {
+    m1 += pp[4 * k]; v1 += pp[4 * k + 1]; m2 += pp[4 * k + 2]; v2 += pp[4 * k + 3];
+  }
+  m1 = dev::block_sum<NT>(m1, shr);
+  v1 = dev::block_sum<NT>(v1, shr);
+  m2 = dev::block_sum<NT>(m2, shr);
+  v2 = dev::block_sum<NT>(v2, shr);
+  if (threadIdx.x == 0) {
+    const double s1 = sqrt(v1), s2 = sqrt(v2);
+    const bool d1 = (s1 > bs.dflux1) && (fabs(m1) > bs.dflux1);
+    const bool d2 = (s2 > bs.dflux2) && (fabs(m2) > bs.dflux2);
+    double* o = mom + static_cast<size_t>(wb) * 8;
+    o[0] = m1; o[1] = m2; o[2] = v1; o[3] = v2;
+    o[4] = d1 ? -m1 : 0.0; o[5] = d2 ? -m2 : 0.0;
+    o[6] = d1 ? 1.0 : 0.0; o[7] = d2 ? 1.0 : 0.0;
+  }
+}
+
+__device__ __forceinline__ double2 pval2(const double2* Rt, int nc, int n,
+                                         int i1, int i2, double r0,
+                                         const double* mo, double sf1,
+                                         double sf2) {
+  const double2 v = Rt[static_cast<size_t>(i1) * nc + i2];
+  double ival = v.y;
+  if (mo[6] != 0.0) {
+    const double sp1 = (i1 < nc) ? sf1 * static_cast<double>(i1)
+                                 : -sf1 * static_cast<double>(n - i1);
+    ival = ival - sp1;
+  }
+  if (mo[7] != 0.0) ival = ival - sf2 * static_cast<double>(i2);
+  const double e = exp(v.x - r0);
+  double s, c;
+  sincos(ival, &s, &c);
+  return make_double2(e * c, e * s);
+}
+
+// exp(R~ - R~00) with the shifts, the Hermitian part of the self-conjugate
+// columns (0 and n/2), then one noise product per dataset
+// (PDFactoryDouble.cc:1241-1342, 1383-1437).  Bins where every dataset's
+// noise exponent is below -750 are exactly 0 in the reference and are
+// written as 0 directly.
+__global__ void __launch_bounds__(NT)
+k_spectrum2(const BSet2Dev* __restrict__ bsets,
+            const DSet2Dev* __restrict__ dsets, int B, int D, int n, int nc,
+            const int* __restrict__ mstatus, const double* __restrict__ sigmult,
+            const double* __restrict__ mom, const double* __restrict__ rbuf,
+            double* __restrict__ pbuf) {
+  const int wb = blockIdx.y;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const long long e = static_cast<long long>(blockIdx.x) * NT + threadIdx.x;
+  if (e >= static_cast<long long>(n) * nc) return;
+  const int i1 = static_cast<int>(e / nc), i2 = static_cast<int>(e - static_cast<long long>(i1) * nc);
+  const BSet2Dev& bs = bsets[b];
+  const double iflux1 = dev::kTwoPi / (static_cast<double>(n) * bs.dflux1);
+  const double iflux2 = dev::kTwoPi / (static_cast<double>(n) * bs.dflux2);
+  const double sm1 = sigmult[2 * w], sm2 = sigmult[2 * w + 1];
+  const double didx1 = (i1 < nc) ? static_cast<double>(i1) : static_cast<double>(n - i1);
+  const double didx2 = static_cast<double>(i2);
+  bool all_zero = (i1 != 0 || i2 != 0);
+  for (int dd = 0; dd < bs.nds && all_zero; ++dd) {
+    const DSet2Dev& ds = dsets[bs.ds_begin + dd];
+    const double s1 = sm1 * ds.sb1, s2 = sm2 * ds.sb2;
+    if (!(s1 > 0 || s2 > 0)) { all_zero = false; break; }
+    const double sf1 = -0.5 * s1 * s1 * iflux1 * iflux1;
+    const double sf2 = -0.5 * s2 * s2 * iflux2 * iflux2;
+    if (!(sf1 * didx1 * didx1 + sf2 * didx2 * didx2 < -750.0)) all_zero = false;
+  }
+  if (all_zero) {
+    for (int dd = 0; dd < bs.nds; ++dd)
+      reinterpret_cast<double2*>(pbuf + (static_cast<size_t>(w) * D + bs.ds_begin + dd) * n * 2 * nc)[e] =
+          make_double2(0.0, 0.0);
+    return;
+  }
+  const double2* Rt = reinterpret_cast<const double2*>(rbuf + static_cast<size_t>(wb) * n * 2 * nc);
+  const double* mo = mom + static_cast<size_t>(wb) * 8;
+  const double r0 = Rt[0].x;
+  const double sf1 = mo[4] * iflux1, sf2 = mo[5] * iflux2;
+  double2 p;
+  if (i1 == 0 && i2 == 0) {
+    p = make_double2(1.0, 0.0);
+  } else {
+    p = pval2(Rt, nc, n, i1, i2, r0, mo, sf1, sf2);
+    if (i2 == 0 || ((n & 1) == 0 && i2 == n / 2)) {
+      const int j1 = (n - i1) % n;
+      if (j1 == i1) {
+        p.y = 0.0;
+      } else {
+        double2 q;
+        if (j1 == 0 && i2 == 0) q = make_double2(1.0, 0.0);
+        else q = pval2(Rt, nc, n, j1, i2, r0, mo, sf1, sf2);
+        p = make_double2(0.5 * (p.x + q.x), 0.5 * (p.y - q.y));
+      }
+    }
+  }
+  for (int dd = 0; dd < bs.nds; ++dd) {
+    const int d = bs.ds_begin + dd;
+    const DSet2Dev& ds = dsets[d];
+    const double s1 = sm1 * ds.sb1, s2 = sm2 * ds.sb2;
+    double2 o = p;
+    if (s1 > 0 || s2 > 0) {
+      if (i1 == 0 && i2 == 0) {
+        o = make_double2(1.0, 0.0);
+      } else {
+        const double sf1n = -0.5 * s1 * s1 * iflux1 * iflux1;
+        const double sf2n = -0.5 * s2 * s2 * iflux2 * iflux2;
+        const double sp1 = sf1n * didx1 * didx1;
+        const double ef = exp(sp1 + sf2n * didx2 * didx2);
+        o = make_double2(ef * p.x, ef * p.y);
+      }
+    }
+    reinterpret_cast<double2*>(pbuf + (static_cast<size_t>(w) * D + d) * n * 2 * nc)[e] = o;
+  }
+}
+
+// Marginal partial sums of the clipped P(D): per (row tile, column) and per
+// (row, column tile).
+__global__ void __launch_bounds__(NT)
+k_pscan2(int D, int n, int nc2, const int* __restrict__ mstatus,
+         const double* __restrict__ pbuf, double* __restrict__ rowpart,
+         double* __restrict__ colpart) {
+  __shared__ double srow[RTILE][NT / 32];
+  const int wd = blockIdx.z;
+  const int w = wd / D;
+  if (mstatus[w] != 0) return;
+  const int c = blockIdx.x * NT + threadIdx.x;
+  const int r0 = blockIdx.y * RTILE;
+  const double* p = pbuf + static_cast<size_t>(wd) * n * nc2;
+  double cs = 0.0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int rr = 0; rr < RTILE; ++rr) {
+    const int r = r0 + rr;
+    double v = 0.0;
+    if (r < n && c < n) v = clip0(p[static_cast<size_t>(r) * nc2 + c]);
+    cs += v;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) srow[rr][warp] = v;
+  }
+  if (c < n) colpart[(static_cast<size_t>(wd) * gridDim.y + blockIdx.y) * n + c] = cs;
+  __syncthreads();
+  if (threadIdx.x < RTILE) {
+    const int r = r0 + threadIdx.x;
+    double s = 0.0;
+    for (int k = 0; k < NT / 32; ++k) s += srow[threadIdx.x][k];
+    if (r < n) rowpart[(static_cast<size_t>(wd) * n + r) * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// PDFactoryDouble::findSplitPoint (PDFactoryDouble.cc:784-968) on a
+// marginal held in shared memory, block-wide.  Returns the status; the
+// split index lands in *out.
+__device__ int split_marginal(const double* data, int n, double dflux,
+                              double sgpos, double sgneg, double* shd,
+                              int* shi, int* out, int* s_state,
+                              double* s_jit) {
+  const double n1 = 2.25, f1 = 5e-14, f2 = 1.5e-5, f3 = 5;
+  if (sgpos <= 0 || sgneg <= 0) return POFD_E_SPLIT_RANGE;
+  const double n1sigpos = n1 * sgpos, n1signeg = n1 * sgneg;
+  if (n * dflux < (n1sigpos + n1signeg)) return POFD_E_SPLIT_RANGE;
+  double mx = -1.0e308;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) mx = dev::dmax(mx, data[i]);
+  const double peak = dev::block_max<SNT>(mx, shd);
+  if (!(peak > 0.0)) return POFD_E_SPLIT_PEAK;
+  const long long top = static_cast<long long>(n) - sat_index(n1signeg / dflux) - 1;
+  const long long bot = sat_index(n1sigpos / dflux);
+  if (top >= n || bot < 0 || bot > top) return POFD_E_SPLIT_LOGIC;
+  double mv = 1.0e308;
+  int mi = 0x7fffffff;
+  for (long long i = bot + threadIdx.x; i <= top; i += blockDim.x)
+    dev::argmin_merge(mv, mi, data[i], static_cast<int>(i));
+  dev::block_argmin<SNT>(mv, mi, shd, shi);
+  if (mv > f2 * peak) return POFD_E_SPLIT_MIN;
+  if (threadIdx.x == 0) {
+    int st = 0;
+    double minval = mv, jitter = 0.0;
+    const int minidx = mi;
+    bool found = false;
+    const int pre = 17;
+    if (minidx > pre) {
+      bool mono = true;
+      double prev = data[minidx - pre];
+      jitter = prev;
+      for (int i = minidx - pre + 1; i < minidx; ++i) {
+        const double cv = data[i];
+        if (cv >= prev) mono = false;
+        jitter += cv;
+        prev = cv;
+      }
+      if (mono) { *out = minidx; found = true; }
+      else jitter = 1.1 * (jitter + minval) / static_cast<double>(pre + 1);
+    } else {
+      jitter = f1 * peak;
+      if (minval > jitter) { *out = minidx; found = true; }
+    }
+    if (!found) {
+      if (minval <= 0.0) {
+        long long bi, ti;
+        if (minidx < bot) bi = bot; else bi = (minidx >= 3) ? (minidx - 3) : minidx;
+        if (minidx > top - 3) ti = top - 3; else ti = minidx + 3;
+        ti = (ti >= n) ? (n - 1) : ti;
+        for (long long i = bi; i < ti; ++i)
+          if (data[i] > minval) minval = data[i];
+      }
+      if (minval > 0) jitter = (f3 * minval) < jitter ? (f3 * minval) : jitter;
+      if (bot >= top) st = POFD_E_SPLIT_LOGIC;
+      else if (data[top] < jitter) st = POFD_E_SPLIT_TOP;
+    }
+    *s_state = (st != 0) ? st : (found ? 1 : 0);
+    *s_jit = jitter;
+  }
+  __syncthreads();
+  const int state = *s_state;
+  if (state != 0) return (state == 1) ? 0 : state;
+  const double jitter = *s_jit;
+  for (long long t = top - 1; t >= bot; t -= blockDim.x) {
+    const long long i = t - threadIdx.x;
+    int hit = -1;
+    if (i >= bot && data[i] < jitter) hit = static_cast<int>(i);
+    const int m = dev::block_max_int<SNT>(hit, shi);
+    if (m >= 0) {
+      if (threadIdx.x == 0) *out = m + 1;
+      __syncthreads();
+      return 0;
+    }
+  }
+  return POFD_E_SPLIT_NONE;
+}
+
+// Marginals, split points, normalisation and means of one (proposal,
+// dataset) (PDFactoryDouble.cc:978-1118, PDDouble.cc:142-208, 355-447).
+__global__ void __launch_bounds__(SNT)
+k_psplit2(const BSet2Dev* __restrict__ bsets,
+          const DSet2Dev* __restrict__ dsets, int B, int D, int n, int nc2,
+          int nct, int nrt, const int* __restrict__ mstatus,
+          const double* __restrict__ sigmult, const double* __restrict__ mom,
+          const double* __restrict__ pbuf, const double* __restrict__ rowpart,
+          const double* __restrict__ colpart, PDInfo2* __restrict__ pinfo) {
+  extern __shared__ double sm[];
+  __shared__ double shd[64];
+  __shared__ int shi[64];
+  __shared__ int s_state, s_s1, s_s2;
+  __shared__ double s_jit;
+  const int wd = blockIdx.x;
+  const int w = wd / D, d = wd - w * D;
+  PDInfo2& info = pinfo[wd];
+  if (mstatus[w] != 0) {
+    if (threadIdx.x == 0) info.status = mstatus[w];
+    return;
+  }
+  const DSet2Dev& ds = dsets[d];
+  const BSet2Dev& bs = bsets[ds.bs];
+  const double* mo = mom + (static_cast<size_t>(w) * B + ds.bs) * 8;
+  const double sigma1 = sigmult[2 * w] * ds.sb1, sigma2 = sigmult[2 * w + 1] * ds.sb2;
+  const double var1 = mo[2], var2 = mo[3];
+  const double sg1pos = sqrt(var1 + sigma1 * sigma1);
+  const double sg2pos = sqrt(var2 + sigma2 * sigma2);
+  const double sg1neg = (9 * sigma1 * sigma1 > var1) ? sigma1 : sg1pos;
+  const double sg2neg = (9 * sigma2 * sigma2 > var2) ? sigma2 : sg2pos;
+  const double* p = pbuf + static_cast<size_t>(wd) * n * nc2;
+  double* Srow = sm;
+  double* Scol = sm + n;
+  double* marg = sm + 2 * n;
+  const double* rp = rowpart + static_cast<size_t>(wd) * n * nct;
+  const double* cp = colpart + static_cast<size_t>(wd) * nrt * n;
+  for (int i = threadIdx.x; i < n; i += SNT) {
+    double s = 0.0;
+    for (int k = 0; k < nct; ++k) s += rp[static_cast<size_t>(i) * nct + k];
+    Srow[i] = s;
+    double c = 0.0;
+    for (int k = 0; k < nrt; ++k) c += cp[static_cast<size_t>(k) * n + i];
+    Scol[i] = c;
+  }
+  __syncthreads();
+  // band-1 marginal: trapezoid over columns of each row
+  for (int i = threadIdx.x; i < n; i += SNT)
+    marg[i] = Srow[i] - 0.5 * clip0(p[static_cast<size_t>(i) * nc2]) -
+              0.5 * clip0(p[static_cast<size_t>(i) * nc2 + n - 1]);
+  __syncthreads();
+  int st = split_marginal(marg, n, bs.dflux1, sg1pos, sg1neg, shd, shi, &s_s1,
+                          &s_state, &s_jit);
+  __syncthreads();
+  if (st == 0) {
+    for (int j = threadIdx.x; j < n; j += SNT)
+      marg[j] = Scol[j] - 0.5 * clip0(p[j]) -
+                0.5 * clip0(p[static_cast<size_t>(n - 1) * nc2 + j]);
+    __syncthreads();
+    st = split_marginal(marg, n, bs.dflux2, sg2pos, sg2neg, shd, shi, &s_s2,
+                        &s_state, &s_jit);
+    __syncthreads();
+  }
+  if (st != 0) {
+    if (threadIdx.x == 0) info.status = st;
+    return;
+  }
+  const int s1 = s_s1, s2 = s_s2;
+  const int s1m = (s1 == 0) ? n - 1 : s1 - 1;
+  const int s2m = (s2 == 0) ? n - 1 : s2 - 1;
+  auto P = [&](int i, int j) { return clip0(p[static_cast<size_t>(i) * nc2 + j]); };
+  // total, rotated-row trapezoid (mean1) and rotated-column trapezoid (mean2)
+  double tot = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int i = threadIdx.x; i < n; i += SNT) {
+    tot += Srow[i];
+    const int a = (i - s1 + n) % n;
+    const double rowtrap = Srow[i] - 0.5 * (P(i, s2) + P(i, s2m));
+    a1 += ((a == n - 1) ? 0.5 : 1.0) * static_cast<double>(a) * rowtrap;
+    const int bb = (i - s2 + n) % n;
+    const double coltrap = Scol[i] - 0.5 * (P(s1, i) + P(s1m, i));
+    a2 += ((bb == n - 1) ? 0.5 : 1.0) * static_cast<double>(bb) * coltrap;
+  }
+  tot = dev::block_sum<SNT>(tot, shd);
+  a1 = dev::block_sum<SNT>(a1, shd);
+  a2 = dev::block_sum<SNT>(a2, shd);
+  if (threadIdx.x == 0) {
+    const double iraw = tot - 0.5 * (Srow[s1] + Srow[s1m]) - 0.5 * (Scol[s2] + Scol[s2m]) +
+                        0.25 * (P(s1, s2) + P(s1, s2m) + P(s1m, s2) + P(s1m, s2m));
+    const double itot = 1.0 / (iraw * bs.dflux1 * bs.dflux2);
+    const double mean1 = itot * a1 * (bs.dflux1 * bs.dflux1 * bs.dflux2);
+    const double mean2 = itot * a2 * (bs.dflux1 * bs.dflux2 * bs.dflux2);
+    if (isinf(mean1) || isnan(mean1) || isinf(mean2) || isnan(mean2)) {
+      info.status = POFD_E_UNSHIFT;
+    } else {
+      info.status = 0;
+      info.s1 = s1;
+      info.s2 = s2;
+      info.itot = itot;
+      info.minflux1 = -mean1;
+      info.minflux2 = -mean2;
+      info.sg1pos = sg1pos; info.sg1neg = sg1neg;
+      info.sg2pos = sg2pos; info.sg2neg = sg2neg;
+    }
+  }
+}
+
+__device__ __forceinline__ double lq2(const double* __restrict__ p, int n,
+                                      int nc2, int s1, int s2, double itot,
+                                      int a, int b) {
+  int i = a + s1; if (i >= n) i -= n;
+  int j = b + s2; if (j >= n) j -= n;
+  const double v = clip0(p[static_cast<size_t>(i) * nc2 + j]) * itot;
+  return (v <= 0.0) ? dev::kSmallLogVal : log2(v);
+}
+
+// Bilinear log2 P(D) at the non-zero data bins (PDDouble.cc:1103-1172),
+// block partial sums.  The reference reads one cell past the grid when a
+// bin centre falls in the last row or column; here the last cell is used.
+__global__ void __launch_bounds__(NT)
+k_pgather2(const BSet2Dev* __restrict__ bsets,
+           const DSet2Dev* __restrict__ dsets, int D, int n, int nc2,
+           int gchunks, const int* __restrict__ mstatus,
+           const double* __restrict__ pbuf, const PDInfo2* __restrict__ pinfo,
+           double* __restrict__ gpart) {
+  __shared__ double shr[32];
+  const int wd = blockIdx.y;
+  const int w = wd / D, d = wd - w * D;
+  if (mstatus[w] != 0) return;
+  const PDInfo2 in = pinfo[wd];
+  double acc = 0.0;
+  const DSet2Dev& ds = dsets[d];
+  if (in.status == 0) {
+    const BSet2Dev& bs = bsets[ds.bs];
+    const double* p = pbuf + static_cast<size_t>(wd) * n * nc2;
+    const double mf1 = in.minflux1, mf2 = in.minflux2;
+    const double d1 = bs.dflux1, d2 = bs.dflux2;
+    const double maxflux1 = mf1 + static_cast<double>(n - 1) * d1;
+    const double maxflux2 = mf2 + static_cast<double>(n - 1) * d2;
+    const double id1 = 1.0 / d1, id2 = 1.0 / d2;
+    const int s1 = in.s1, s2 = in.s2;
+    const double itot = in.itot;
+    const int e1 = min(ds.nnz, (blockIdx.x + 1) * GCH);
+    for (int e = blockIdx.x * GCH + threadIdx.x; e < e1; e += NT) {
+      const double cnt = ds.nzcnt[e];
+      const double cflux1 = ds.bc1 + static_cast<double>(ds.nzi1[e]) * ds.bd1;
+      const double cflux2 = ds.bc2 + static_cast<double>(ds.nzi2[e]) * ds.bd2;
+      const int idx1 = static_cast<int>((cflux1 - mf1) * id1);
+      const int idx2 = static_cast<int>((cflux2 - mf2) * id2);
+      double iv;
+      if (cflux1 < mf1) {
+        if (cflux2 < mf2) iv = lq2(p, n, nc2, s1, s2, itot, 0, 0);
+        else if (cflux2 > maxflux2) iv = lq2(p, n, nc2, s1, s2, itot, 0, n - 1);
+        else iv = lq2(p, n, nc2, s1, s2, itot, 0, idx2);
+      } else if (cflux1 > maxflux1) {
+        if (cflux2 < mf2) iv = lq2(p, n, nc2, s1, s2, itot, n - 1, 0);
+        else if (cflux2 > maxflux2) iv = lq2(p, n, nc2, s1, s2, itot, n - 1, n - 1);
+        else iv = lq2(p, n, nc2, s1, s2, itot, n - 1, idx2);
+      } else if (cflux2 < mf2) {
+        iv = lq2(p, n, nc2, s1, s2, itot, idx1, 0);
+      } else if (cflux2 > maxflux2) {
+        iv = lq2(p, n, nc2, s1, s2, itot, idx1, n - 1);
+      } else {
+        double t = (cflux1 - mf1) * id1 - static_cast<double>(idx1);
+        double u = (cflux2 - mf2) * id2 - static_cast<double>(idx2);
+        int i1 = idx1, i2 = idx2;
+        if (i1 > n - 2) { i1 = n - 2; t = 1.0; }
+        if (i2 > n - 2) { i2 = n - 2; u = 1.0; }
+        const double omu = 1.0 - u, omt = 1.0 - t;
+        iv = omt * (omu * lq2(p, n, nc2, s1, s2, itot, i1, i2) +
+                    u * lq2(p, n, nc2, s1, s2, itot, i1, i2 + 1)) +
+             t * (omu * lq2(p, n, nc2, s1, s2, itot, i1 + 1, i2) +
+                  u * lq2(p, n, nc2, s1, s2, itot, i1 + 1, i2 + 1));
+      }
+      acc += cnt * iv;
+    }
+  }
+  acc = dev::block_sum<NT>(acc, shr);
+  if (threadIdx.x == 0) gpart[static_cast<size_t>(wd) * gchunks + blockIdx.x] = acc;
+}
+
+// Per-proposal sum over beam sets and datasets; a negative sigma multiplier
+// gives bad_like for the beam set (calcLikeDouble.cc:571-576, 1219-1224).
+__global__ void k_reduce2(const BSet2Dev* __restrict__ bsets,
+                          const DSet2Dev* __restrict__ dsets, int B, int D,
+                          int nprop, int gchunks, double log2toe,
+                          const int* __restrict__ mstatus,
+                          const double* __restrict__ sigmult,
+                          const PDInfo2* __restrict__ pinfo,
+                          const double* __restrict__ gpart,
+                          double* __restrict__ logl, int* __restrict__ status) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nprop) return;
+  const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+  if (mstatus[w] != 0) {
+    logl[w] = qnan;
+    status[w] = mstatus[w];
+    return;
+  }
+  const double sm1 = sigmult[2 * w], sm2 = sigmult[2 * w + 1];
+  double LogLike = 0.0;
+  int st = 0;
+  for (int b = 0; b < B; ++b) {
+    const BSet2Dev& bs = bsets[b];
+    if (bs.maxsb1 * sm1 < 0.0 || bs.maxsb2 * sm2 < 0.0) { LogLike += 1e25; continue; }
+    double s = 0.0;
+    for (int dd = 0; dd < bs.nds; ++dd) {
+      const int d = bs.ds_begin + dd;
+      const PDInfo2& in = pinfo[static_cast<size_t>(w) * D + d];
+      if (in.status != 0) {
+        if (st == 0) st = in.status;
+        continue;
+      }
+      double ll = 0.0;
+      const double* g = gpart + (static_cast<size_t>(w) * D + d) * gchunks;
+      for (int c = 0; c < gchunks; ++c) ll += g[c];
+      s += (log2toe * ll - dsets[d].like_offset) / dsets[d].like_norm;
+    }
+    LogLike += s;
+  }
+  status[w] = st;
+  logl[w] = (st == 0) ? LogLike : qnan;
+}
+
+// The unwrapped, normalised (optionally log2) 2D P(D) of one row.
+__global__ void k_pdwrite2(const double* __restrict__ p, int n, int nc2,
+                           int s1, int s2, double itot, int setlog,
+                           double* __restrict__ out) {
+  const long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= static_cast<long long>(n) * n) return;
+  const int a = static_cast<int>(e / n), b = static_cast<int>(e - static_cast<long long>(a) * n);
+  int i = a + s1; if (i >= n) i -= n;
+  int j = b + s2; if (j >= n) j -= n;
+  const double v = clip0(p[static_cast<size_t>(i) * nc2 + j]) * itot;
+  out[e] = setlog ? ((v <= 0.0) ? dev::kSmallLogVal : log2(v)) : v;
+}
+
+}  // namespace
+
+// ===================================================================== host
+
+Engine2::Engine2(int device, cudaStream_t stream)
+    : device_(device), stream_(stream) {}
+
+Engine2::~Engine2() {
+  if (device_ < 0) return;
+  cudaSetDevice(device_);
+  drop_graphs();
+  for (auto& kv : plans_) {
+    if (kv.second.fwd) cufftDestroy(kv.second.fwd);
+    if (kv.second.inv) cufftDestroy(kv.second.inv);
+  }
+  free_work();
+  free_static();
+}
+
+void Engine2::configure(unsigned nknots, const double* knotpos,
+                        unsigned nsigma, const double* sigmapos,
+                        unsigned noffset, const double* offsetpos,
+                        unsigned fftsize, unsigned nedge, bool edge_integ,
+                        unsigned nbins) {
+  auto incr = [](unsigned n, const double* v, const char* what) {
+    for (unsigned i = 0; i < n; ++i)
+      if (!(v[i] > 0) || (i > 0 && !(v[i] > v[i - 1])))
+        throw Error(POFD_E_ARG, std::string(what) + " positions must be positive and increasing");
+  };
+  if (nknots < 3 || nknots > static_cast<unsigned>(KMAX))
+    throw Error(POFD_E_ARG, "nknots must be in [3, 64]");
+  if (nsigma < 1 || nsigma > static_cast<unsigned>(KMAX) || noffset < 1 ||
+      noffset > static_cast<unsigned>(KMAX))
+    throw Error(POFD_E_ARG, "sigma and offset knots must number 1..64");
+  incr(nknots, knotpos, "knot");
+  incr(nsigma, sigmapos, "sigma knot");
+  incr(noffset, offsetpos, "offset knot");
+  if (fftsize < 16 || fftsize > 8192) throw Error(POFD_E_ARG, "fftsize must be in [16, 8192]");
+  if (edge_integ && (nedge < 2 || nedge > fftsize))
+    throw Error(POFD_E_ARG, "Nedge is less than R fill size");
+  if (nbins == 0) throw Error(POFD_E_ARG, "Trying to bin with no bins");
+  knots_.assign(knotpos, knotpos + nknots);
+  sigk_.assign(sigmapos, sigmapos + nsigma);
+  offk_.assign(offsetpos, offsetpos + noffset);
+  n_ = fftsize;
+  nedge_ = nedge;
+  edge_ = edge_integ;
+  nbins_ = nbins;
+  static_ok_ = false;
+}
+
+int Engine2::add_beamset(const Beam2& bm, double ec1, double ec2) {
+  HostSet s;
+  s.bm = bm;
+  s.ec1 = ec1;
+  s.ec2 = ec2;
+  sets_.push_back(std::move(s));
+  static_ok_ = false;
+  return static_cast<int>(sets_.size()) - 1;
+}
+
+// calcLikeDoubleSingle::setSigmaBase1/2 (calcLikeDouble.cc:377-487) and the
+// data flux range of the beam set.
+void Engine2::refresh_set(HostSet& s) {
+  s.maxsb1 = s.sb1[0];
+  s.maxsb2 = s.sb2[0];
+  for (size_t i = 1; i < s.sb1.size(); ++i) {
+    if (s.sb1[i] > s.maxsb1) s.maxsb1 = s.sb1[i];
+    if (s.sb2[i] > s.maxsb2) s.maxsb2 = s.sb2[i];
+  }
+  for (size_t i = 0; i < s.data.size(); ++i) {
+    const double v1 = s.sb1[i] * s.sb1[i] + s.ec1 * s.ec1;
+    const double v2 = s.sb2[i] * s.sb2[i] + s.ec2 * s.ec2;
+    const double sp = std::sqrt(v1 * v2);
+    if (sp > 0) {
+      const double ndd = static_cast<double>(s.data[i].d1.size());
+      s.lo[i] = -ndd * (std::log(kTwoPi * sp) + 1.0);
+    }
+  }
+  double mm[4];
+  s.data[0].minmax(mm);
+  for (int k = 0; k < 4; ++k) s.mdf[k] = mm[k];
+  for (size_t i = 1; i < s.data.size(); ++i) {
+    s.data[i].minmax(mm);
+    if (mm[0] < s.mdf[0]) s.mdf[0] = mm[0];
+    if (mm[1] > s.mdf[1]) s.mdf[1] = mm[1];
+    if (mm[2] < s.mdf[2]) s.mdf[2] = mm[2];
+    if (mm[3] > s.mdf[3]) s.mdf[3] = mm[3];
+  }
+  s.rr_set = false;
+}
+
+void Engine2::add_dataset(int bs, const double* d1, const double* d2,
+                          size_t nd, bool meansub, double sigma1,
+                          double sigma2, double like_norm) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size()))
+    throw Error(POFD_E_ARG, "invalid beam set index");
+  if (nd == 0) throw Error(POFD_E_ARG, "No pixels in data");
+  HostSet& s = sets_[bs];
+  Data2 d;
+  d.d1.assign(d1, d1 + nd);
+  d.d2.assign(d2, d2 + nd);
+  if (meansub) d.meanSubtract();
+  d.applyBinning(nbins_, nbins_);
+  s.data.push_back(std::move(d));
+  s.sb1.push_back(sigma1);
+  s.sb2.push_back(sigma2);
+  s.lo.push_back(0.0);
+  s.ln.push_back(like_norm);
+  refresh_set(s);
+  static_ok_ = false;
+}
+
+// calcLikeDoubleSingle::setRRange (calcLikeDouble.cc:496-534).
+void Engine2::set_rranges(const float* theta, unsigned npar) {
+  if (npar < nparams()) throw Error(POFD_E_ARG, "Not enough parameters present to set");
+  Model2Host m;
+  m.set(knots_, sigk_, offk_, theta);
+  const double safetyfac = 1.1;
+  for (auto& s : sets_) {
+    if (s.data.empty()) throw Error(POFD_E_ARG, "Data not loaded");
+    double raw[4];
+    m.rrange(s.bm, raw);
+    const double sg1 = std::sqrt(s.ec1 * s.ec1 + s.maxsb1 * s.maxsb1);
+    const double sg2 = std::sqrt(s.ec2 * s.ec2 + s.maxsb2 * s.maxsb2);
+    s.rr[0] = safetyfac * raw[0];
+    s.rr[1] = safetyfac * raw[1] + kNZeroPad * sg1;
+    s.rr[2] = safetyfac * raw[2];
+    s.rr[3] = safetyfac * raw[3] + kNZeroPad * sg2;
+    const bool* hs = s.bm.hassign;
+    if (s.mdf[0] < s.rr[0] && (hs[2] || hs[3])) s.rr[0] = s.mdf[0];
+    if (s.mdf[1] > s.rr[1] && (hs[0] || hs[1])) s.rr[1] = s.mdf[1];
+    if (s.mdf[2] < s.rr[2] && (hs[1] || hs[3])) s.rr[2] = s.mdf[2];
+    if (s.mdf[3] > s.rr[3] && (hs[0] || hs[2])) s.rr[3] = s.mdf[3];
+    s.rr_set = true;
+  }
+  static_ok_ = false;
+}
+
+void Engine2::rrange(int bs, double* r4) const {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size())) throw Error(POFD_E_ARG, "invalid beam set index");
+  for (int k = 0; k < 4; ++k) r4[k] = sets_[bs].rr[k];
+}
+
+void Engine2::dataset_info(int bs, int ds, double* o, uint32_t* bins) const {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size())) throw Error(POFD_E_ARG, "invalid beam set index");
+  const HostSet& s = sets_[bs];
+  if (ds < 0 || ds >= static_cast<int>(s.data.size())) throw Error(POFD_E_ARG, "invalid dataset index");
+  const Data2& d = s.data[ds];
+  if (o) {
+    o[0] = static_cast<double>(d.d1.size()); o[1] = d.nbins1;
+    o[2] = d.bc1; o[3] = d.bc2; o[4] = d.bd1; o[5] = d.bd2;
+    o[6] = s.lo[ds]; o[7] = s.sb1[ds]; o[8] = s.sb2[ds]; o[9] = s.ln[ds];
+  }
+  if (bins) std::memcpy(bins, d.bins.data(), d.bins.size() * sizeof(uint32_t));
+}
+
+void Engine2::free_static() {
+  for (void* q : static_allocs_) cudaFree(q);
+  static_allocs_.clear();
+  d_bsets_ = nullptr;
+  d_dsets_ = nullptr;
+  static_ok_ = false;
+}
+
+void Engine2::drop_graphs() {
+  for (auto& kv : plans_) {
+    for (auto& g : kv.second.graphs) cudaGraphExecDestroy(g.second);
+    kv.second.graphs.clear();
+  }
+}
+
+void Engine2::build_static() {
+  if (device_ < 0) throw Error(POFD_E_CUDA, "host-only context has no GPU");
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  free_static();
+  if (sets_.empty()) throw Error(POFD_E_ARG, "no beam sets");
+  auto up = [&](const std::vector<double>& v) -> const double* {
+    double* q = dal<double>(v.size() ? v.size() : 1);
+    static_allocs_.push_back(q);
+    if (!v.empty()) ck(cudaMemcpy(q, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice), "upload");
+    return q;
+  };
+  auto upi = [&](const std::vector<int>& v) -> const int* {
+    int* q = dal<int>(v.size() ? v.size() : 1);
+    static_allocs_.push_back(q);
+    if (!v.empty()) ck(cudaMemcpy(q, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice), "upload");
+    return q;
+  };
+  std::vector<double> lk(knots_.size());
+  for (size_t i = 0; i < knots_.size(); ++i) lk[i] = std::log2(knots_[i]);
+  model_.K = static_cast<int>(knots_.size());
+  model_.ns = static_cast<int>(sigk_.size());
+  model_.no = static_cast<int>(offk_.size());
+  model_.logknots = up(lk);
+  model_.sk = up(sigk_);
+  model_.ok = up(offk_);
+  model_.minknot = knots_.front();
+  model_.maxknot = knots_.back();
+  model_.min_sigma = 0.0;
+
+  const unsigned n = n_;
+  B_ = static_cast<unsigned>(sets_.size());
+  h_bsets_.assign(B_, BSet2Dev{});
+  h_dsets_.clear();
+  Tmax_ = 1;
+  unsigned maxnnz = 1;
+  const double normfac = 1.0 / std::sqrt(2 * kPi);
+  for (unsigned b = 0; b < B_; ++b) {
+    HostSet& s = sets_[b];
+    if (!s.rr_set) throw Error(POFD_E_ARG, "R range not set");
+    double mn1 = s.rr[0], mx1 = s.rr[1], mn2 = s.rr[2], mx2 = s.rr[3];
+    if (mx1 <= 0.0) throw Error(POFD_E_ARG, "Invalid (non-positive) maxflux1");
+    if (mx2 <= 0.0) throw Error(POFD_E_ARG, "Invalid (non-positive) maxflux2");
+    if (mx1 == mn1) throw Error(POFD_E_ARG, "Invalid range (0) between min/max flux in band 1");
+    if (mx2 == mn2) throw Error(POFD_E_ARG, "Invalid range (0) between min/max flux in band 2");
+    if (mx1 < mn1) std::swap(mn1, mx1);
+    if (mx2 < mn2) std::swap(mn2, mx2);
+    RGrid2Axis a1, a2;
+    a1.init(n, mn1, mx1);
+    a2.init(n, mn2, mx2);
+    BSet2Dev& bd = h_bsets_[b];
+    bd.dflux1 = a1.dflux;
+    bd.dflux2 = a2.dflux;
+    bd.wrap1 = static_cast<int>(a1.wrapidx);
+    bd.wrap2 = static_cast<int>(a2.wrapidx);
+    const double pixdeg = s.bm.pixsize / 3600.0;
+    bd.prefac = pixdeg * pixdeg * normfac;
+    std::vector<double> E1, E2;
+    if (edge_) {
+      const double lowm = 1e-9;  // PDFactoryDouble.h:33
+      const double me1 = a1.dflux * lowm, me2 = a2.dflux * lowm;
+      const double ine = 1.0 / static_cast<double>(nedge_ - 1);
+      const double di1 = -std::log(lowm) * ine;
+      E1.resize(nedge_);
+      for (unsigned i = 0; i < nedge_; ++i) E1[i] = me1 * std::exp(static_cast<double>(i) * di1);
+      const double di2 = (a2.dflux - me2) * ine;
+      E2.resize(nedge_);
+      for (unsigned i = 0; i < nedge_; ++i) E2[i] = me2 + static_cast<double>(i) * di2;
+      bd.iRxnorm = di1 / (a1.dflux - me1);
+      bd.iRynorm = di2 / (a2.dflux - me2);
+      bd.iR00norm = di1 * di2 / ((a1.dflux - me1) * (a2.dflux - me2));
+    }
+    const bool hasNegX1 = s.bm.hassign[2] || s.bm.hassign[3];
+    std::vector<double> rowf(a1.flux), rowl, colinv, coll;
+    rowf.insert(rowf.end(), E1.begin(), E1.end());
+    std::vector<int> rows, cols;
+    for (double f : rowf) {
+      if (f == 0 || (f < 0 && !hasNegX1)) { rows.push_back(-1); rowl.push_back(0.0); }
+      else { rows.push_back(f > 0 ? 0 : 2); rowl.push_back(std::log(std::fabs(f))); }
+    }
+    std::vector<double> colf(a2.flux);
+    colf.insert(colf.end(), E2.begin(), E2.end());
+    for (double f : colf) {
+      if (f == 0) { colinv.push_back(0.0); coll.push_back(0.0); cols.push_back(0); continue; }
+      cols.push_back(f > 0 ? 0 : 1);
+      colinv.push_back(1.0 / std::fabs(f));
+      coll.push_back(std::log(std::fabs(f)));
+    }
+    bd.nrows = static_cast<int>(rowf.size());
+    bd.rowflux = up(rowf);
+    bd.rowlog = up(rowl);
+    bd.rowsgn = upi(rows);
+    bd.colinv = up(colinv);
+    bd.collog = up(coll);
+    bd.colsgn = upi(cols);
+    bd.rflux2 = up(a2.flux);
+    bd.e1 = up(E1);
+    int nt[4];
+    for (int g = 0; g < 4; ++g) {
+      Sign2Dev& sg = bd.sg[g];
+      bd.hassign[g] = s.bm.hassign[g] ? 1 : 0;
+      nt[g] = static_cast<int>(s.bm.nterms(g));
+      sg.nt = nt[g];
+      sg.ishist = s.bm.ishist[g] ? 1 : 0;
+      if (s.bm.ishist[g]) {
+        sg.w = up(s.bm.binwt[g]);
+        sg.ieta1 = up(s.bm.binv1[g]);
+        sg.logratio = up(s.bm.binlogratio[g]);
+      } else {
+        sg.w = up(std::vector<double>(s.bm.pix1[g].size(), 1.0));
+        sg.ieta1 = up(s.bm.inv1[g]);
+        sg.logratio = up(s.bm.logratio[g]);
+      }
+      sg.maxf1 = s.bm.hassign[g] ? knots_.back() * s.bm.maxbm1[g] : 0.0;
+    }
+    bd.T = std::max(nt[0] * bd.hassign[0] + nt[1] * bd.hassign[1],
+                    nt[2] * bd.hassign[2] + nt[3] * bd.hassign[3]);
+    if (bd.T < 1) bd.T = 1;
+    if (bd.T > MAXT) throw Error(POFD_E_ARG, "beam has too many terms; histogram it");
+    if (bd.T > Tmax_) Tmax_ = bd.T;
+    bd.maxsb1 = s.maxsb1;
+    bd.maxsb2 = s.maxsb2;
+    bd.ds_begin = static_cast<int>(h_dsets_.size());
+    bd.nds = static_cast<int>(s.data.size());
+    for (size_t i = 0; i < s.data.size(); ++i) {
+      const Data2& d = s.data[i];
+      DSet2Dev dd{};
+      dd.bs = static_cast<int>(b);
+      dd.sb1 = s.sb1[i];
+      dd.sb2 = s.sb2[i];
+      dd.like_offset = s.lo[i];
+      dd.like_norm = s.ln[i];
+      std::vector<int> i1, i2;
+      std::vector<double> c;
+      for (unsigned a = 0; a < d.nbins1; ++a)
+        for (unsigned bb = 0; bb < d.nbins2; ++bb) {
+          const uint32_t v = d.bins[static_cast<size_t>(a) * d.nbins2 + bb];
+          if (v) { i1.push_back(static_cast<int>(a)); i2.push_back(static_cast<int>(bb)); c.push_back(v); }
+        }
+      dd.nnz = static_cast<int>(c.size());
+      dd.nzi1 = upi(i1);
+      dd.nzi2 = upi(i2);
+      dd.nzcnt = up(c);
+      dd.bc1 = d.bc1; dd.bc2 = d.bc2; dd.bd1 = d.bd1; dd.bd2 = d.bd2;
+      if (c.size() > maxnnz) maxnnz = static_cast<unsigned>(c.size());
+      h_dsets_.push_back(dd);
+    }
+  }
+  D_ = static_cast<unsigned>(h_dsets_.size());
+  d_bsets_ = dal<BSet2Dev>(B_);
+  static_allocs_.push_back(d_bsets_);
+  ck(cudaMemcpy(d_bsets_, h_bsets_.data(), B_ * sizeof(BSet2Dev), cudaMemcpyHostToDevice), "upload");
+  d_dsets_ = dal<DSet2Dev>(D_);
+  static_allocs_.push_back(d_dsets_);
+  ck(cudaMemcpy(d_dsets_, h_dsets_.data(), D_ * sizeof(DSet2Dev), cudaMemcpyHostToDevice), "upload");
+  gx_ = (n + NT - 1) / NT;
+  gy_ = (n - 1 + RB - 1) / RB;
+  nrt_ = (n + RTILE - 1) / RTILE;
+  nct_ = (n + NT - 1) / NT;
+  gchunks_ = (maxnnz + GCH - 1) / GCH;
+  static_ok_ = true;
+  drop_graphs();
+  for (auto& kv : plans_) {
+    if (kv.second.fwd) cufftDestroy(kv.second.fwd);
+    if (kv.second.inv) cufftDestroy(kv.second.inv);
+  }
+  plans_.clear();
+  const unsigned P = ws_.P;
+  free_work();
+  if (P) reserve(P);
+}
+
+void Engine2::free_work() {
+  void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.rw, ws_.rbuf,
+                  ws_.rpart, ws_.redge, ws_.mom, ws_.pbuf, ws_.rowpart,
+                  ws_.colpart, ws_.pinfo, ws_.gpart, ws_.pdout,
+                  ws_.theta_in, ws_.logl, ws_.status};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
+  if (ws_.h_logl) cudaFreeHost(ws_.h_logl);
+  if (ws_.h_status) cudaFreeHost(ws_.h_status);
+  ws_ = Work{};
+}
+
+void Engine2::reserve(unsigned P) {
+  if (P == 0) throw Error(POFD_E_ARG, "max_batch must be > 0");
+  if (!static_ok_) {
+    ws_.P = std::max(ws_.P, P);
+    build_static();
+    return;
+  }
+  if (ws_.P >= P && ws_.rbuf) return;
+  // (proposal, beam set) and (proposal, dataset) pairs index grid y / z
+  if (static_cast<size_t>(P) * std::max(B_, D_) > 65535u)
+    throw Error(POFD_E_ARG, "batch x (beam sets or datasets) exceeds 65535");
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  drop_graphs();
+  free_work();
+  const size_t n = n_, nc2 = 2 * (n / 2 + 1);
+  size_t nrows = n + (edge_ ? nedge_ : 0);
+  ws_.P = P;
+  ws_.cnt = dal<double>(static_cast<size_t>(P) * 12 * KMAX);
+  ws_.mstatus = dal<int>(P);
+  ws_.sigmult = dal<double>(2 * static_cast<size_t>(P));
+  ws_.rw = dal<double>(static_cast<size_t>(P) * B_ * nrows * Tmax_ * 3);
+  ws_.rbuf = dal<double>(static_cast<size_t>(P) * B_ * n * nc2);
+  ws_.rpart = dal<double>(static_cast<size_t>(P) * B_ * gx_ * gy_ * 4);
+  ws_.redge = dal<double>(static_cast<size_t>(P) * B_ * (2 * n + 1));
+  ws_.mom = dal<double>(static_cast<size_t>(P) * B_ * 8);
+  ws_.pbuf = dal<double>(static_cast<size_t>(P) * D_ * n * nc2);
+  ws_.rowpart = dal<double>(static_cast<size_t>(P) * D_ * n * nct_);
+  ws_.colpart = dal<double>(static_cast<size_t>(P) * D_ * nrt_ * n);
+  ws_.pinfo = dal<PDInfo2>(static_cast<size_t>(P) * D_);
+  ws_.gpart = dal<double>(static_cast<size_t>(P) * D_ * gchunks_);
+  ws_.pdout = dal<double>(n * n);
+  ws_.logl = dal<double>(P);
+  ws_.status = dal<int>(P);
+  ck(cudaMemset(ws_.redge, 0, static_cast<size_t>(P) * B_ * (2 * n + 1) * sizeof(double)), "memset");
+  const int smem_rows = static_cast<int>(6 * MAXT * sizeof(double));
+  ck(cudaFuncSetAttribute(k_rgrid2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
+  ck(cudaFuncSetAttribute(k_rx2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
+  ck(cudaFuncSetAttribute(k_ry2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
+  ck(cudaFuncSetAttribute(k_r002, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
+  ck(cudaFuncSetAttribute(k_psplit2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          static_cast<int>(3 * 8192 * sizeof(double))), "attr");
+}
+
+void Engine2::ensure_plans(unsigned nprop) {
+  auto it = plans_.find(nprop);
+  if (it != plans_.end() && it->second.fwd) return;
+  Plans pl;
+  int nn[2] = {static_cast<int>(n_), static_cast<int>(n_)};
+  const int nc = static_cast<int>(n_) / 2 + 1;
+  int inemb[2] = {nn[0], 2 * nc}, onemb[2] = {nn[0], nc};
+  fk(cufftPlanMany(&pl.fwd, 2, nn, inemb, 1, nn[0] * 2 * nc, onemb, 1, nn[0] * nc,
+                   CUFFT_D2Z, static_cast<int>(nprop * B_)), "cufftPlanMany 2D D2Z");
+  int inemb2[2] = {nn[0], nc}, onemb2[2] = {nn[0], 2 * nc};
+  fk(cufftPlanMany(&pl.inv, 2, nn, inemb2, 1, nn[0] * nc, onemb2, 1, nn[0] * 2 * nc,
+                   CUFFT_Z2D, static_cast<int>(nprop * D_)), "cufftPlanMany 2D Z2D");
+  plans_[nprop] = pl;
+}
+
+void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
+                         double* logl, int* status, cudaStream_t st,
+                         cudaEvent_t* ev, bool r_only) {
+  auto mark = [&](int i) {
+    if (ev) ck(cudaEventRecord(ev[i], st), "event record");
+  };
+  const int n = static_cast<int>(n_), nc = n / 2 + 1, nc2 = 2 * nc;
+  const int P = static_cast<int>(nprop), B = static_cast<int>(B_), D = static_cast<int>(D_);
+  const int ne = edge_ ? static_cast<int>(nedge_) : 0;
+  const size_t smem_rows = 6 * static_cast<size_t>(Tmax_) * sizeof(double);
+  Plans& pl = plans_.at(nprop);
+  mark(0);
+  k_model2<<<P, 32, 0, st>>>(model_, theta, static_cast<int>(npar), std::log2(10.0),
+                             ws_.cnt, ws_.mstatus, ws_.sigmult);
+  mark(1);
+  {
+    const size_t nrows = static_cast<size_t>(n + ne);
+    const unsigned gxr = static_cast<unsigned>((nrows * Tmax_ + NT - 1) / NT);
+    k_rows2<<<dim3(gxr, P * B), NT, 0, st>>>(d_bsets_, model_, B, 1.0 / std::log(2.),
+                                             ws_.mstatus, ws_.cnt, ws_.rw);
+  }
+  mark(2);
+  k_rgrid2<<<dim3(gx_, gy_, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, nc2, ws_.mstatus,
+                                                         ws_.rw, ws_.rbuf, ws_.rpart);
+  mark(3);
+  if (edge_) {
+    k_rx2<<<dim3(gx_, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.redge);
+    k_ry2<<<dim3(n - 1, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.redge);
+    k_r002<<<P * B, NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.redge);
+  }
+  mark(4);
+  k_rfinish2<<<P * B, NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0,
+                                   static_cast<int>(gx_ * gy_), ws_.mstatus, ws_.redge,
+                                   ws_.rpart, ws_.rbuf, ws_.mom);
+  mark(5);
+  if (r_only) {
+    ck(cudaGetLastError(), "kernel launch");
+    return;
+  }
+  fk(cufftSetStream(pl.fwd, st), "cufftSetStream");
+  fk(cufftExecD2Z(pl.fwd, ws_.rbuf, reinterpret_cast<cufftDoubleComplex*>(ws_.rbuf)), "cufftExecD2Z 2D");
+  mark(6);
+  {
+    const unsigned gs = static_cast<unsigned>((static_cast<size_t>(n) * nc + NT - 1) / NT);
+    k_spectrum2<<<dim3(gs, P * B), NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc, ws_.mstatus,
+                                                ws_.sigmult, ws_.mom, ws_.rbuf, ws_.pbuf);
+  }
+  mark(7);
+  fk(cufftSetStream(pl.inv, st), "cufftSetStream");
+  fk(cufftExecZ2D(pl.inv, reinterpret_cast<cufftDoubleComplex*>(ws_.pbuf), ws_.pbuf), "cufftExecZ2D 2D");
+  mark(8);
+  k_pscan2<<<dim3(nct_, nrt_, P * D), NT, 0, st>>>(D, n, nc2, ws_.mstatus, ws_.pbuf,
+                                                    ws_.rowpart, ws_.colpart);
+  mark(9);
+  k_psplit2<<<P * D, SNT, 3 * static_cast<size_t>(n) * sizeof(double), st>>>(
+      d_bsets_, d_dsets_, B, D, n, nc2, static_cast<int>(nct_), static_cast<int>(nrt_),
+      ws_.mstatus, ws_.sigmult, ws_.mom, ws_.pbuf, ws_.rowpart, ws_.colpart, ws_.pinfo);
+  mark(10);
+  k_pgather2<<<dim3(gchunks_, P * D), NT, 0, st>>>(d_bsets_, d_dsets_, D, n, nc2,
+                                                    static_cast<int>(gchunks_), ws_.mstatus,
+                                                    ws_.pbuf, ws_.pinfo, ws_.gpart);
+  mark(11);
+  k_reduce2<<<(P + 127) / 128, 128, 0, st>>>(d_bsets_, d_dsets_, B, D, P,
+                                            static_cast<int>(gchunks_), std::log(2.0),
+                                            ws_.mstatus, ws_.sigmult, ws_.pinfo,
+                                            ws_.gpart, logl, status);
+  mark(12);
+  ck(cudaGetLastError(), "kernel launch");
+}
+
+cudaGraphExec_t Engine2::graph_for(unsigned nprop, const float* theta,
+                                   unsigned npar, double* logl, int* status) {
+  Plans& pl = plans_.at(nprop);
+  if (pl.no_graph) return nullptr;
+  const GraphKey key{theta, npar, logl, status};
+  for (auto& kv : pl.graphs)
+    if (kv.first == key) return kv.second;
+  if (!pl.warmed) {
+    pl.warmed = true;
+    return nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    bool threw = false;
+    try {
+      launch_all(nprop, theta, npar, logl, status, stream_, nullptr);
+    } catch (...) {
+      threw = true;
+    }
+    const cudaError_t ec = cudaStreamEndCapture(stream_, &g);
+    if (threw || ec != cudaSuccess || !g || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+      ge = nullptr;
+    if (g) cudaGraphDestroy(g);
+  }
+  cudaGetLastError();
+  if (!ge) {
+    pl.no_graph = true;
+    return nullptr;
+  }
+  if (pl.graphs.size() >= 8) {
+    cudaGraphExecDestroy(pl.graphs.front().second);
+    pl.graphs.erase(pl.graphs.begin());
+  }
+  pl.graphs.push_back({key, ge});
+  return ge;
+}
+
+void Engine2::enqueue(unsigned nprop, const float* theta_dev, unsigned npar,
+                      double* logl_dev, int* status_dev, cudaStream_t st) {
+  if (nprop == 0) return;
+  if (npar < nparams() + 2) throw Error(POFD_E_ARG, "Not enough elements in params");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  ensure_plans(nprop);
+  if (!st) st = stream_;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  ck(cudaStreamIsCapturing(st, &cs), "cudaStreamIsCapturing");
+  if (cs != cudaStreamCaptureStatusNone) {
+    launch_all(nprop, theta_dev, npar, logl_dev, status_dev, st, nullptr);
+    return;
+  }
+  cudaGraphExec_t g = graph_for(nprop, theta_dev, npar, logl_dev, status_dev);
+  if (g) ck(cudaGraphLaunch(g, st), "graph launch");
+  else launch_all(nprop, theta_dev, npar, logl_dev, status_dev, st, nullptr);
+}
+
+void Engine2::eval_host(unsigned nprop, const float* theta, unsigned npar,
+                        double* logl, int* status) {
+  if (nprop == 0) return;
+  if (npar < nparams() + 2) throw Error(POFD_E_ARG, "Not enough elements in params");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  if (!ws_.theta_in || ws_.h_npar < npar) {
+    if (ws_.theta_in) cudaFree(ws_.theta_in);
+    if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
+    ws_.theta_in = dal<float>(static_cast<size_t>(ws_.P) * npar);
+    ck(cudaMallocHost(&ws_.h_theta, static_cast<size_t>(ws_.P) * npar * sizeof(float)), "cudaMallocHost");
+    ws_.h_npar = npar;
+    drop_graphs();
+  }
+  if (!ws_.h_logl) {
+    ck(cudaMallocHost(&ws_.h_logl, ws_.P * sizeof(double)), "cudaMallocHost");
+    ck(cudaMallocHost(&ws_.h_status, ws_.P * sizeof(int)), "cudaMallocHost");
+  }
+  std::memcpy(ws_.h_theta, theta, static_cast<size_t>(nprop) * npar * sizeof(float));
+  ck(cudaMemcpyAsync(ws_.theta_in, ws_.h_theta, static_cast<size_t>(nprop) * npar * sizeof(float),
+                     cudaMemcpyHostToDevice, stream_), "H2D theta");
+  enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);
+  ck(cudaMemcpyAsync(ws_.h_logl, ws_.logl, nprop * sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H");
+  ck(cudaMemcpyAsync(ws_.h_status, ws_.status, nprop * sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  ck(cudaStreamSynchronize(stream_), "synchronize");
+  std::memcpy(logl, ws_.h_logl, nprop * sizeof(double));
+  std::memcpy(status, ws_.h_status, nprop * sizeof(int));
+}
+
+int Engine2::pd_host(int bs, int ds, const float* theta, unsigned npar,
+                     bool setlog, double* pd_out, double* info16) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size())) throw Error(POFD_E_ARG, "invalid beam set index");
+  if (ds < 0 || ds >= static_cast<int>(sets_[bs].data.size())) throw Error(POFD_E_ARG, "invalid dataset index");
+  double ll;
+  int st;
+  eval_host(1, theta, npar, &ll, &st);
+  const int d = h_bsets_[bs].ds_begin + ds;
+  PDInfo2 info;
+  ck(cudaMemcpy(&info, ws_.pinfo + d, sizeof(PDInfo2), cudaMemcpyDeviceToHost), "D2H info");
+  double mom[8];
+  ck(cudaMemcpy(mom, ws_.mom + static_cast<size_t>(bs) * 8, sizeof(mom), cudaMemcpyDeviceToHost), "D2H mom");
+  if (info16) {
+    const BSet2Dev& b = h_bsets_[bs];
+    info16[0] = b.dflux1; info16[1] = b.dflux2; info16[2] = mom[0]; info16[3] = mom[1];
+    info16[4] = mom[2]; info16[5] = mom[3]; info16[6] = mom[4]; info16[7] = mom[5];
+    info16[8] = info.s1; info16[9] = info.s2; info16[10] = info.minflux1; info16[11] = info.minflux2;
+    info16[12] = info.sg1pos; info16[13] = info.sg1neg; info16[14] = info.sg2pos; info16[15] = info.sg2neg;
+  }
+  if (info.status != 0) return info.status;
+  const size_t n = n_, nc2 = 2 * (n / 2 + 1);
+  const unsigned blocks = static_cast<unsigned>((n * n + 255) / 256);
+  k_pdwrite2<<<blocks, 256, 0, stream_>>>(ws_.pbuf + static_cast<size_t>(d) * n * nc2,
+                                          static_cast<int>(n), static_cast<int>(nc2), info.s1,
+                                          info.s2, info.itot, setlog ? 1 : 0, ws_.pdout);
+  ck(cudaGetLastError(), "pdwrite2");
+  ck(cudaMemcpyAsync(pd_out, ws_.pdout, n * n * sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H pd");
+  ck(cudaStreamSynchronize(stream_), "synchronize");
+  return 0;
+}
+
+void Engine2::rgrid_host(int bs, const float* theta, unsigned npar, double* out) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size())) throw Error(POFD_E_ARG, "invalid beam set index");
+  double ll;
+  int st;
+  eval_host(1, theta, npar, &ll, &st);  // staging, plans
+  ck(cudaMemcpy(ws_.theta_in, theta, npar * sizeof(float), cudaMemcpyHostToDevice), "H2D");
+  launch_all(1, ws_.theta_in, npar, ws_.logl, ws_.status, stream_, nullptr, true);
+  const size_t n = n_, nc2 = 2 * (n / 2 + 1);
+  ck(cudaMemcpy2DAsync(out, n * sizeof(double), ws_.rbuf + static_cast<size_t>(bs) * n * nc2,
+                       nc2 * sizeof(double), n * sizeof(double), n, cudaMemcpyDeviceToHost, stream_),
+     "D2H R grid");
+  ck(cudaStreamSynchronize(stream_), "synchronize");
+}
+
+void Engine2::profile_stages(unsigned nprop, const float* theta, unsigned npar,
+                             int reps, double* stage_ms) {
+  std::vector<double> lls(nprop);
+  std::vector<int> sts(nprop);
+  eval_host(nprop, theta, npar, lls.data(), sts.data());
+  cudaEvent_t ev[kNumStages + 1];
+  for (auto& e : ev) ck(cudaEventCreate(&e), "event create");
+  for (int k = 0; k < kNumStages; ++k) stage_ms[k] = 0.0;
+  for (int r = 0; r < reps; ++r) {
+    launch_all(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_, ev);
+    ck(cudaStreamSynchronize(stream_), "synchronize");
+    for (int k = 0; k < kNumStages; ++k) {
+      float ms = 0.f;
+      ck(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]), "elapsed");
+      stage_ms[k] += ms / reps;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+}
+
+const char* Engine2::stage_name(int i) {
+  static const char* names[kNumStages] = {
+      "k_model2", "k_rows2", "k_rgrid2", "k_rx2+k_ry2+k_r002", "k_rfinish2",
+      "cufft_d2z_2d", "k_spectrum2", "cufft_z2d_2d", "k_pscan2", "k_psplit2",
+      "k_pgather2", "k_reduce2"};
+  return (i >= 0 && i < kNumStages) ? names[i] : "";
+}
+
+}  // namespace pofd

@@ -1,0 +1,196 @@
+// engine2d.cuh -- batched 2D (two-band) P(D) likelihood engine.
+//
+// One Engine2 evaluates calcLikeDouble::getLogLike (calcLikeDouble.cc:
+// 1195-1277) for a batch of proposals: model set-up (knot counts, sigma and
+// offset curves), per-row precompute of the log-normal colour terms,
+// the direct n x n R grid with the edge integrals, R moments and shifts, a
+// batched 2D D2Z, the spectrum (exp/shift, Hermitian projection of the
+// self-conjugate columns, one noise product per dataset), a batched 2D Z2D,
+// marginal sums, split points, normalisation and means, and the bilinear
+// log-likelihood gather.  Captured into a CUDA graph per batch size and
+// pointer set.
+#ifndef POFD_ENGINE2D_CUH
+#define POFD_ENGINE2D_CUH
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <map>
+#include <vector>
+
+#include "setup.hh"
+
+namespace pofd {
+
+struct Sign2Dev {
+  int nt;                 // terms (histogram bins or pixels)
+  int ishist;             // weight/product order of the reference
+  const double* w;        // weights (1 for raw)
+  const double* ieta1;    // inverse band-1 beam
+  const double* logratio; // log(beam1 / beam2)
+  double maxf1;           // maxknot * max band-1 beam
+};
+
+struct BSet2Dev {
+  Sign2Dev sg[4];
+  int hassign[4];
+  int T;                  // terms per row slot (max of np+nn over row signs)
+  double prefac;          // (pixsize/3600)^2 / sqrt(2 pi)
+  double dflux1, dflux2;
+  int wrap1, wrap2;
+  int nrows;              // n (+ nedge edge rows)
+  const double* rowflux;  // [nrows] RFlux1 then edge band-1 fluxes
+  const double* rowlog;   // log|f1|
+  const int* rowsgn;      // 0 (f1 > 0), 2 (f1 < 0), -1 (R row is zero)
+  const double* colinv;   // [n + nedge] 1/|f2| (0 where f2 == 0)
+  const double* collog;   // log|f2|
+  const int* colsgn;      // 0 (f2 > 0), 1 (f2 < 0)
+  const double* rflux2;   // RFlux2 [n]
+  const double* e1;       // edge band-1 fluxes [nedge]
+  double iRxnorm, iRynorm, iR00norm;
+  double maxsb1, maxsb2;
+  int ds_begin, nds;
+};
+
+struct DSet2Dev {
+  int bs;
+  double sb1, sb2, like_offset, like_norm;
+  int nnz;
+  const int* nzi1;
+  const int* nzi2;
+  const double* nzcnt;
+  double bc1, bc2, bd1, bd2;
+};
+
+struct Model2Dev {
+  int K, ns, no;
+  const double* logknots;
+  const double* sk;
+  const double* ok;
+  double minknot, maxknot, min_sigma;
+};
+
+struct PDInfo2 {
+  int status, s1, s2, pad;
+  double itot, minflux1, minflux2, sg1pos, sg1neg, sg2pos, sg2neg, pad2;
+};
+
+class Engine2 {
+ public:
+  static constexpr int KMAX = 64;
+  static constexpr int kNumStages = 12;
+  Engine2(int device, cudaStream_t stream);
+  ~Engine2();
+
+  void configure(unsigned nknots, const double* knotpos, unsigned nsigma,
+                 const double* sigmapos, unsigned noffset,
+                 const double* offsetpos, unsigned fftsize, unsigned nedge,
+                 bool edge_integ, unsigned nbins);
+  int add_beamset(const Beam2& bm, double exp_conf1, double exp_conf2);
+  void add_dataset(int bs, const double* d1, const double* d2, size_t nd,
+                   bool meansub, double sigma1, double sigma2,
+                   double like_norm);
+  void set_rranges(const float* theta, unsigned npar);
+  void rrange(int bs, double* r4) const;
+  void dataset_info(int bs, int ds, double* info10, uint32_t* bins) const;
+  void reserve(unsigned max_batch);
+  void enqueue(unsigned nprop, const float* theta_dev, unsigned npar,
+               double* logl_dev, int* status_dev, cudaStream_t st);
+  void eval_host(unsigned nprop, const float* theta, unsigned npar,
+                 double* logl, int* status);
+  int pd_host(int bs, int ds, const float* theta, unsigned npar, bool setlog,
+              double* pd_out, double* info16);
+  void rgrid_host(int bs, const float* theta, unsigned npar, double* out);
+  void profile_stages(unsigned nprop, const float* theta, unsigned npar,
+                      int reps, double* stage_ms);
+  static const char* stage_name(int i);
+  int kernels_per_eval() const { return edge_ ? 13 : 10; }
+  unsigned nparams() const {
+    return static_cast<unsigned>(knots_.size() + sigk_.size() + offk_.size());
+  }
+
+ private:
+  struct HostSet {
+    Beam2 bm;
+    double ec1 = 0, ec2 = 0;
+    std::vector<Data2> data;
+    std::vector<double> sb1, sb2, lo, ln;
+    double maxsb1 = nan(), maxsb2 = nan();
+    double mdf[4] = {nan(), nan(), nan(), nan()};
+    double rr[4] = {nan(), nan(), nan(), nan()};
+    bool rr_set = false;
+  };
+  struct GraphKey {
+    const float* theta;
+    unsigned npar;
+    double* logl;
+    int* status;
+    bool operator==(const GraphKey& o) const {
+      return theta == o.theta && npar == o.npar && logl == o.logl &&
+             status == o.status;
+    }
+  };
+  struct Plans {
+    cufftHandle fwd = 0, inv = 0;
+    std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
+    bool warmed = false, no_graph = false;
+  };
+  void refresh_set(HostSet& s);
+  void build_static();
+  void free_static();
+  void free_work();
+  void drop_graphs();
+  void ensure_plans(unsigned nprop);
+  cudaGraphExec_t graph_for(unsigned nprop, const float* theta, unsigned npar,
+                            double* logl, int* status);
+  void launch_all(unsigned nprop, const float* theta, unsigned npar,
+                  double* logl, int* status, cudaStream_t st, cudaEvent_t* ev,
+                  bool r_only = false);
+
+  int device_;
+  cudaStream_t stream_;
+  std::vector<double> knots_, sigk_, offk_;
+  unsigned n_ = 0, nedge_ = 256, nbins_ = 1000;
+  bool edge_ = true;
+  std::vector<HostSet> sets_;
+  bool static_ok_ = false;
+  std::vector<void*> static_allocs_;
+  BSet2Dev* d_bsets_ = nullptr;
+  DSet2Dev* d_dsets_ = nullptr;
+  Model2Dev model_{};
+  std::vector<BSet2Dev> h_bsets_;
+  std::vector<DSet2Dev> h_dsets_;
+  unsigned B_ = 0, D_ = 0;
+  int Tmax_ = 1;
+  unsigned gx_ = 0, gy_ = 0;      // R grid blocks (columns, row groups)
+  unsigned nrt_ = 0, nct_ = 0;    // P(D) row / column tiles
+  unsigned gchunks_ = 1;          // gather chunks per dataset
+  std::map<unsigned, Plans> plans_;
+  struct Work {
+    unsigned P = 0;
+    double* cnt = nullptr;      // [P][12*KMAX]
+    int* mstatus = nullptr;
+    double* sigmult = nullptr;  // [P][2]
+    double* rw = nullptr;       // [P][B][nrows][T][3]
+    double* rbuf = nullptr;     // [P][B][n][2nc]
+    double* rpart = nullptr;    // [P][B][gy][gx][4]
+    double* redge = nullptr;    // [P][B][2n+1]: Rx (n), Ry (n), r00
+    double* mom = nullptr;      // [P][B][8]
+    double* pbuf = nullptr;     // [P][D][n][2nc]
+    double* rowpart = nullptr;  // [P][D][n][nct]
+    double* colpart = nullptr;  // [P][D][nrt][n]
+    PDInfo2* pinfo = nullptr;   // [P][D]
+    double* gpart = nullptr;    // [P][D][gchunks]
+    double* pdout = nullptr;    // [n*n]
+    float* theta_in = nullptr;
+    double* logl = nullptr;
+    int* status = nullptr;
+    float* h_theta = nullptr;
+    double* h_logl = nullptr;
+    int* h_status = nullptr;
+    unsigned h_npar = 0;
+  } ws_;
+};
+
+}  // namespace pofd
+#endif

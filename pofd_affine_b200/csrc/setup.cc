@@ -378,3 +378,224 @@ void RGrid2Axis::init(unsigned N, double minflux, double maxflux) {
 }
 
 }  // namespace pofd
+
+namespace pofd {
+
+// ------------------------------------------------------------- NatSpline
+void NatSpline::init(const double* xa, const double* ya, size_t n) {
+  if (n < 3) throw Error(POFD_E_ARG, "spline needs at least 3 points");
+  SplineSystem sys;
+  std::vector<double> xv(xa, xa + n);
+  sys.factor(xv);
+  x = xv;
+  y.assign(ya, ya + n);
+  const size_t N = n - 2;
+  std::vector<double> cc(n, 0.0), z(N);
+  for (size_t i = 0; i < N; ++i)
+    z[i] = 3.0 * ((y[i + 2] - y[i + 1]) * sys.ih[i + 1] - (y[i + 1] - y[i]) * sys.ih[i]);
+  for (size_t i = 1; i < N; ++i) z[i] = z[i] - sys.gamma[i - 1] * z[i - 1];
+  for (size_t i = 0; i < N; ++i) z[i] = z[i] / sys.alpha[i];
+  cc[N] = z[N - 1];
+  for (size_t k = N - 1; k-- > 0;) cc[1 + k] = z[k] - sys.gamma[k] * cc[2 + k];
+  b.assign(n - 1, 0.0);
+  c.assign(n, 0.0);
+  d.assign(n - 1, 0.0);
+  for (size_t i = 0; i < n; ++i) c[i] = cc[i];
+  for (size_t i = 0; i + 1 < n; ++i) {
+    const double dx = x[i + 1] - x[i], dy = y[i + 1] - y[i];
+    b[i] = (dy / dx) - dx * (c[i + 1] + 2.0 * c[i]) / 3.0;
+    d[i] = (c[i + 1] - c[i]) / (3.0 * dx);
+  }
+}
+
+size_t NatSpline::find(double v) const {
+  size_t lo = 0, hi = x.size() - 1;
+  while (hi > lo + 1) {
+    const size_t m = (hi + lo) / 2;
+    if (x[m] > v) hi = m; else lo = m;
+  }
+  return lo;
+}
+
+double NatSpline::eval(double v) const {
+  const size_t i = find(v);
+  const double dl = v - x[i];
+  return y[i] + dl * (b[i] + dl * (c[i] + dl * d[i]));
+}
+
+// ---------------------------------------------------------- Model2Host
+void Model2Host::set(const std::vector<double>& k, const std::vector<double>& s,
+                     const std::vector<double>& o, const float* th) {
+  knots = k;
+  sigk = s;
+  offk = o;
+  const size_t nk = k.size(), ns = s.size(), no = o.size();
+  for (size_t i = 0; i < nk; ++i)
+    if (std::isnan(static_cast<double>(th[i])))
+      throw Error(POFD_E_INVALID_MODEL, "Model is not valid");
+  sigv.resize(ns);
+  offv.resize(no);
+  for (size_t i = 0; i < ns; ++i) {
+    sigv[i] = static_cast<double>(th[nk + i]);
+    if (!std::isfinite(sigv[i])) throw Error(POFD_E_INVALID_MODEL, "Model is not valid");
+  }
+  for (size_t i = 0; i < no; ++i) {
+    offv[i] = static_cast<double>(th[nk + ns + i]);
+    if (std::isnan(offv[i])) throw Error(POFD_E_INVALID_MODEL, "Model is not valid");
+  }
+  if (ns > 2) sigspl.init(sigk.data(), sigv.data(), ns);
+  if (no > 2) offspl.init(offk.data(), offv.data(), no);
+}
+
+double Model2Host::sigma(double f1) const {
+  const size_t ns = sigk.size();
+  if (ns == 1) return sigv[0];
+  if (f1 <= sigk[0]) return sigv[0];
+  if (f1 >= sigk[ns - 1]) return sigv[ns - 1];
+  double val;
+  if (ns == 2) {
+    val = sigv[0] + (f1 - sigk[0]) / (sigk[1] - sigk[0]) * (sigv[1] - sigv[0]);
+  } else {
+    val = sigspl.eval(f1);
+  }
+  return (val < min_sigma) ? min_sigma : val;
+}
+
+double Model2Host::offset(double f1) const {
+  const size_t no = offk.size();
+  if (no == 1) return offv[0];
+  if (f1 <= offk[0]) return offv[0];
+  if (f1 >= offk[no - 1]) return offv[no - 1];
+  if (no == 2)
+    return offv[0] + (f1 - offk[0]) / (offk[1] - offk[0]) * (offv[1] - offv[0]);
+  return offspl.eval(f1);
+}
+
+namespace {
+struct LogNormF {
+  double mu, isig, isig2, target;
+  double operator()(double u) const {
+    const double prefac = 1.0 / std::sqrt(2 * kPi);
+    const double eu = std::exp(-u);
+    const double arg = u - mu;
+    return prefac * std::exp(-0.5 * arg * arg * isig2) * isig * eu - target;
+  }
+};
+}  // namespace
+
+// Brent's method (Brent 1973, ch. 4) with the bracket and the relative
+// interval test the reference applies (numberCountsDoubleLogNormal.cc:
+// 1426-1471).
+double Model2Host::logNormalSolver(double mu, double sig, double nsig) const {
+  const double prefac = 1.0 / std::sqrt(kTwoPi);
+  if (sig <= 0.0) throw Error(POFD_E_ARG, "Invalid (non-positive) sigma");
+  const double sig2 = sig * sig;
+  const double mode_u = mu - sig2;
+  if (nsig == 0) return std::exp(mode_u);
+  const double isig = 1.0 / sig;
+  const double val_mode = prefac * isig * std::exp(0.5 * sig2 - mu);
+  LogNormF F{mu, isig, isig * isig, val_mode * std::exp(-0.5 * nsig * nsig)};
+  double u_low = mode_u;
+  double delta_u = std::log(std::exp(mode_u) + 2 * sig) - mode_u;
+  double fval = F(u_low + delta_u);
+  if (fval >= 0.0) {
+    for (int i = 0; i < 20; ++i) {
+      delta_u *= 1.5;
+      fval = F(u_low + delta_u);
+      if (fval < 0.0) break;
+    }
+    if (fval >= 0.0) throw Error(POFD_E_ARG, "Unable to bracket Log Normal");
+  }
+  double u_high = u_low + delta_u;
+  // Brent state
+  double a = u_low, b = u_high, c = u_high;
+  double fa = F(a), fb = F(b), fc = fb;
+  double d = b - a, e = b - a;
+  if ((fa < 0.0 && fb < 0.0) || (fa > 0.0 && fb > 0.0))
+    throw Error(POFD_E_ARG, "endpoints do not straddle y=0");
+  const double eps = 2.2204460492503131e-16;
+  double root = 0.5 * (u_low + u_high);
+  for (int it = 0; it < 20; ++it) {
+    bool ac_equal = false;
+    if ((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) {
+      ac_equal = true;
+      c = a; fc = fa;
+      d = b - a; e = b - a;
+    }
+    if (std::fabs(fc) < std::fabs(fb)) {
+      ac_equal = true;
+      a = b; b = c; c = a;
+      fa = fb; fb = fc; fc = fa;
+    }
+    const double tol = 0.5 * eps * std::fabs(b);
+    const double m = 0.5 * (c - b);
+    double xl, xu;
+    if (fb == 0 || std::fabs(m) <= tol) {
+      root = b;
+      xl = (b < c) ? b : c;
+      xu = (b < c) ? c : b;
+      if (fb == 0) xl = xu = b;
+    } else {
+      if (std::fabs(e) < tol || std::fabs(fa) <= std::fabs(fb)) {
+        d = m; e = m;
+      } else {
+        double p, q, r;
+        const double s = fb / fa;
+        if (ac_equal) {
+          p = 2 * m * s;
+          q = 1 - s;
+        } else {
+          q = fa / fc;
+          r = fb / fc;
+          p = s * (2 * m * q * (q - r) - (b - a) * (r - 1));
+          q = (q - 1) * (r - 1) * (s - 1);
+        }
+        if (p > 0) q = -q; else p = -p;
+        const double l1 = 3 * m * q - std::fabs(tol * q), l2 = std::fabs(e * q);
+        if (2 * p < (l1 < l2 ? l1 : l2)) { e = d; d = p / q; }
+        else { d = m; e = m; }
+      }
+      a = b; fa = fb;
+      if (std::fabs(d) > tol) b += d; else b += (m > 0 ? +tol : -tol);
+      fb = F(b);
+      root = b;
+      double cc = c;
+      if ((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) cc = a;
+      xl = (b < cc) ? b : cc;
+      xu = (b < cc) ? cc : b;
+    }
+    const double al = std::fabs(xl), au = std::fabs(xu);
+    const double min_abs = ((xl > 0 && xu > 0) || (xl < 0 && xu < 0)) ? (al < au ? al : au) : 0.0;
+    if (std::fabs(xu - xl) < 1e-3 * min_abs) return std::exp(root);
+  }
+  throw Error(POFD_E_ARG, "Unable to brent bracket Log Normal");
+}
+
+std::pair<double, double> Model2Host::maxFlux() const {
+  const double kv = knots.back();
+  return {kv, kv * logNormalSolver(offset(kv), sigma(kv), 3.0)};
+}
+
+void Model2Host::rrange(const Beam2& bm, double* r) const {
+  double min1 = 0, max1 = 0, min2 = 0, max2 = 0, cv;
+  const auto mf = maxFlux();
+  if (bm.hassign[0]) {
+    cv = mf.first * bm.maxbm1[0]; if (cv > max1) max1 = cv;
+    cv = mf.second * bm.maxbm2[0]; if (cv > max2) max2 = cv;
+  }
+  if (bm.hassign[1]) {
+    cv = mf.first * bm.maxbm1[1]; if (cv > max1) max1 = cv;
+    cv = -mf.second * bm.maxbm2[1]; if (cv < min2) min2 = cv;
+  }
+  if (bm.hassign[2]) {
+    cv = -mf.first * bm.maxbm1[2]; if (cv < min1) min1 = cv;
+    cv = mf.second * bm.maxbm2[2]; if (cv > max2) max2 = cv;
+  }
+  if (bm.hassign[3]) {
+    cv = -mf.first * bm.maxbm1[3]; if (cv < min1) min1 = cv;
+    cv = -mf.second * bm.maxbm2[3]; if (cv < min2) min2 = cv;
+  }
+  r[0] = min1; r[1] = max1; r[2] = min2; r[3] = max2;
+}
+
+}  // namespace pofd

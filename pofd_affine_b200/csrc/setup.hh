@@ -132,5 +132,35 @@ struct RGrid2Axis {
   void init(unsigned N, double minflux, double maxflux);
 };
 
+
+
+// Natural cubic spline (host), per-interval y,b,c,d as the reference's
+// spline library forms them at evaluation (used for the 2D model's sigma
+// and offset curves and its knot counts on the host).
+struct NatSpline {
+  std::vector<double> x, y, b, c, d;
+  void init(const double* xa, const double* ya, size_t n);
+  size_t find(double v) const;
+  double eval(double v) const;
+};
+
+// Log-normal colour model on the host (numberCountsDoubleLogNormal.cc:
+// setParams 1010-1052, getSigmaInner 1172-1179, getOffsetInner 1187-1193,
+// getMaxFlux 1365-1379, logNormalSolver 1389-1472, getRRangeInternal
+// 1481-1521): only what the frozen R range needs.
+struct Model2Host {
+  std::vector<double> knots, sigk, offk;
+  std::vector<double> sigv, offv;
+  NatSpline sigspl, offspl;
+  double min_sigma = 0.0;
+  void set(const std::vector<double>& k, const std::vector<double>& s,
+           const std::vector<double>& o, const float* theta);
+  double sigma(double f1) const;
+  double offset(double f1) const;
+  double logNormalSolver(double mu, double sig, double nsig) const;
+  std::pair<double, double> maxFlux() const;
+  void rrange(const Beam2& bm, double* r4) const;
+};
+
 }  // namespace pofd
 #endif

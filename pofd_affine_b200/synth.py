@@ -170,3 +170,44 @@ def proposals(theta0, nprop, scale=0.02, rng=None, fixed_last=True):
     nfree = th.shape[1] - (1 if fixed_last else 0)
     th[:, :nfree] += rng.normal(0.0, scale, (nprop, nfree)).astype(np.float32)
     return th
+
+
+def config_2d(seed=3, scale=1.0, n=2048, nbins=500):
+    """2D plain fit: 8 band-1 knots over 2-500 mJy (power law, jittered),
+    log-normal colour with 3 sigma knots (0.15-0.3) and 3 offset knots
+    (about ln 0.7), both log-spaced over 2-500 mJy; Gaussian beams FWHM 3.0
+    and 4.2 px at 6" on 39x39 maps, minval 1e-6, 100-bin 2D histogram; a
+    1500x1500 map pair at 2.5 / 2.8 mJy noise; n = 2048, nedge = 256,
+    500x500 data bins.  scale < 1 shrinks the maps (for fast tests)."""
+    rng = np.random.default_rng(seed)
+    kp, kv = knot_model(8, 0.002, 0.500, rng=rng)
+    sk = np.logspace(np.log10(0.002), np.log10(0.5), 3)
+    sv = np.array([0.15, 0.22, 0.3], np.float32)
+    ok = sk.copy()
+    ov = (np.log(0.7) + rng.normal(0, 0.02, 3)).astype(np.float32)
+    b1 = gaussian_beam(3.0, nfwhm=39 / 3.0)
+    b2 = gaussian_beam(4.2)
+    sig_fn = lambda f: np.interp(f, sk, sv)  # noqa: E731
+    off_fn = lambda f: np.interp(f, ok, ov)  # noqa: E731
+    sh = (max(32, int(1500 * scale)), max(32, int(1500 * scale)))
+    m1, m2 = make_map_pair(sh, 6.0, b1, b2, kp, kv, sig_fn, off_fn, 0.0025,
+                           0.0028, rng)
+    theta0 = np.concatenate([kv, sv, ov, [1.0, 1.0]]).astype(np.float32)
+    return dict(knotpos=kp, knotvals=kv, sigmapos=sk, sigmavals=sv,
+                offsetpos=ok, offsetvals=ov, beam1=b1, beam2=b2, pixsize=6.0,
+                nbeamhist=100, minval=1e-6, maps=[(m1, m2)], sigmas=[(0.0025,
+                                                                     0.0028)],
+                fftsize=n, nedge=256, nbins=nbins, theta0=theta0)
+
+
+def build_like2(cfg, ctx):
+    from .api2d import calcLikeDouble, doublebeam
+    L = calcLikeDouble(ctx, cfg["knotpos"], cfg["sigmapos"], cfg["offsetpos"],
+                       cfg["fftsize"], cfg["nedge"], True, cfg["nbins"])
+    bm = doublebeam(cfg["beam1"], cfg["beam2"], cfg["pixsize"], True,
+                    cfg["nbeamhist"], cfg["minval"])
+    L.addBeamSet(bm)
+    for (m1, m2), (s1, s2) in zip(cfg["maps"], cfg["sigmas"]):
+        L.addDataset(0, m1, m2, s1, s2)
+    L.setRRanges(cfg["theta0"])
+    return L
