@@ -203,7 +203,7 @@ k_rows2(const BSet2Dev* __restrict__ bsets, Model2Dev m, int B,
   const long long t = static_cast<long long>(blockIdx.x) * NT + threadIdx.x;
   if (t >= static_cast<long long>(bs.nrows) * T) return;
   const int r = static_cast<int>(t / T), k = static_cast<int>(t - static_cast<long long>(r) * T);
-  double* out = rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3 + 3 * k;
+  double* out = rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3 + 3 * k;
   const int sgn1 = bs.rowsgn[r];
   double c0 = 0.0, c1 = 0.0, c2 = 0.0;
   if (sgn1 >= 0) {
@@ -356,7 +356,7 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
     const int r = 1 + blockIdx.y * RB + rr;
     if (r >= n) break;
     const int sgn1 = bs.rowsgn[r];
-    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3, sgn1,
+    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
               s_pos, s_neg, s_cnt, sh);
     if (j >= 1 && j < n) {
       const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j) * fluxfac;
@@ -403,7 +403,7 @@ k_rx2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   for (int i = 0; i < nedge; ++i) {
     const int r = n + i;
     const int sgn1 = bs.rowsgn[r];
-    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3, sgn1,
+    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
               s_pos, s_neg, s_cnt, sh);
     if (j < n) {
       const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j);
@@ -437,7 +437,7 @@ k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   double* s_pos = sm;
   double* s_neg = sm + 3 * T;
   const int sgn1 = bs.rowsgn[r];
-  stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3, sgn1,
+  stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
             s_pos, s_neg, s_cnt, sh);
   double acc = 0.0;
   for (int jj = threadIdx.x; jj < nedge; jj += NT) {
@@ -469,7 +469,7 @@ k_r002(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   for (int i = 0; i < nedge; ++i) {
     const int r = n + i;
     const int sgn1 = bs.rowsgn[r];
-    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * T * 3, sgn1,
+    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
               s_pos, s_neg, s_cnt, sh);
     double acc = 0.0;
     for (int jj = threadIdx.x; jj < nedge; jj += NT) {
@@ -1307,6 +1307,7 @@ void Engine2::build_static() {
     }
   }
   D_ = static_cast<unsigned>(h_dsets_.size());
+  for (auto& bd : h_bsets_) bd.Ts = Tmax_;  // common row stride of rw
   d_bsets_ = dal<BSet2Dev>(B_);
   static_allocs_.push_back(d_bsets_);
   ck(cudaMemcpy(d_bsets_, h_bsets_.data(), B_ * sizeof(BSet2Dev), cudaMemcpyHostToDevice), "upload");

@@ -35,6 +35,7 @@ struct BSet2Dev {
   Sign2Dev sg[4];
   int hassign[4];
   int T;                  // terms per row slot (max of np+nn over row signs)
+  int Ts;                 // row stride of the term buffer (max T over sets)
   double prefac;          // (pixsize/3600)^2 / sqrt(2 pi)
   double dflux1, dflux2;
   int wrap1, wrap2;
