@@ -271,6 +271,156 @@ int pofd_pd1_loglike_noalloc(const double* pofd_dev, unsigned n, double dflux,
                              double like_offset, double like_norm,
                              double* out_dev, int* status_dev, void* stream);
 
+/* ------------------------------------------------------------------ MCMC
+ * Batched affine-invariant stretch-move ensemble: replaces affineEnsemble
+ * (affineEnsemble.h:60-200) and its MPI master/worker farm with one process
+ * that evaluates each half of the ensemble in one batched likelihood launch.
+ * Parameter states are the reference's mcmc_affine flags
+ * (global_settings.h:57). */
+#define POFD_PARAM_FIXED 1    /* mcmc_affine::FIXED */
+#define POFD_PARAM_ACIGNORE 2 /* mcmc_affine::ACIGNORE */
+#define POFD_PARAM_BONUS 4    /* mcmc_affine::BONUS */
+
+/* A batched likelihood: evaluates nprop proposals theta_dev[nprop][npar]
+ * (device) into logl_dev[nprop] and status_dev[nprop] (POFD_OK,
+ * POFD_REJECTED or an error), enqueued on stream; graph-capturable once it
+ * has run once at that batch size.  pofd_like1_eval_batch_device and
+ * pofd_like2_eval_batch_device have this signature; it replaces the
+ * per-proposal virtual affineEnsemble::getLogLike (affineEnsemble.h:175). */
+typedef int (*pofd_batch_loglike_fn)(void* like, unsigned nprop,
+                                     const float* theta_dev, unsigned npar,
+                                     double* logl_dev, int* status_dev,
+                                     void* stream);
+
+typedef struct pofd_ensemble pofd_ensemble;
+
+/* affineEnsemble(nwalkers, nparams, ..., scalefac) (affineEnsemble.h:100);
+ * seed keys the counter-based generator (the reference seeds ran from the
+ * clock). */
+int pofd_ensemble_create(pofd_ctx* ctx, unsigned nwalkers, unsigned nparams,
+                         double scalefac, unsigned long long seed,
+                         pofd_ensemble** out);
+int pofd_ensemble_destroy(pofd_ensemble* e);
+int pofd_ensemble_set_likelihood(pofd_ensemble* e, pofd_batch_loglike_fn fn,
+                                 void* like);
+/* Convenience: the 1D / 2D likelihoods of this library. */
+int pofd_ensemble_use_like1(pofd_ensemble* e, pofd_like1* like);
+int pofd_ensemble_use_like2(pofd_ensemble* e, pofd_like2* like);
+/* setParamFixed / setParamIgnoreAcor / setParamBonus
+ * (affineEnsemble.h:131-140): state is an OR of POFD_PARAM_*. */
+int pofd_ensemble_set_param_state(pofd_ensemble* e, unsigned idx, int state);
+/* areParamsValid (affineEnsemble.h:183): a proposal is valid when every
+ * non-fixed, non-bonus parameter lies in [lo, hi] (pofdMCMC uses the
+ * initialisation file's limits and sigma multiplier > 0). */
+int pofd_ensemble_set_param_limits(pofd_ensemble* e, unsigned idx, float lo,
+                                   float hi);
+int pofd_ensemble_set_temperature(pofd_ensemble* e, double temp);
+/* Initial walker positions walkers[nwalkers][nparams] (host) and their
+ * log-likelihoods (NULL = -infinity, so the first step is always taken, as
+ * pofdMCMC::generateInitialPosition does, pofdMCMC.cc:242-290). */
+int pofd_ensemble_init(pofd_ensemble* e, const float* walkers,
+                       const double* logl);
+int pofd_ensemble_reserve_chain(pofd_ensemble* e, unsigned nsteps);
+int pofd_ensemble_clear_chain(pofd_ensemble* e);
+/* doSteps (affineEnsemble.cc:529-620, doMasterStep 1233-1284): nsteps full
+ * steps, recorded into the chain when record != 0 (burn-in passes 0). */
+int pofd_ensemble_do_steps(pofd_ensemble* e, unsigned nsteps, int record);
+int pofd_ensemble_nrecorded(pofd_ensemble* e, unsigned* n);
+/* Recorded chain: theta[nrec][nwalkers][nparams], logl[nrec][nwalkers]
+ * (either may be NULL). */
+int pofd_ensemble_chain(pofd_ensemble* e, float* theta, double* logl);
+int pofd_ensemble_last(pofd_ensemble* e, float* theta, double* logl);
+/* Accepted steps per walker (getAcceptanceFrac numerator,
+ * affineEnsemble.h:157). */
+int pofd_ensemble_naccept(pofd_ensemble* e, unsigned* naccept);
+/* getAcor (affineEnsemble.h:155, affineChainSet.cc:824-1030): tau[nparams]
+ * over the recorded chain, NaN for ACIGNORE parameters; returns POFD_OK, or
+ * POFD_REJECTED when some parameter's series was too short (< 50). */
+int pofd_ensemble_acor(pofd_ensemble* e, double* tau);
+/* A multivariate Gaussian test likelihood, log N(theta[0:k]; mean, icov^-1)
+ * up to a constant, batched on the device with the pofd_batch_loglike_fn
+ * signature (pofd_gauss_eval_batch_device): a target with a known
+ * posterior for checking the sampler and the surrogate.  No counterpart in
+ * the reference. */
+typedef struct pofd_gauss pofd_gauss;
+int pofd_gauss_create(pofd_ctx* ctx, unsigned k, const double* mean,
+                      const double* icov, pofd_gauss** out);
+int pofd_gauss_destroy(pofd_gauss* g);
+int pofd_gauss_eval_batch_device(void* g, unsigned nprop,
+                                 const float* theta_dev, unsigned npar,
+                                 double* logl_dev, int* status_dev,
+                                 void* stream);
+
+/* ------------------------------------------------------------- surrogate
+ * An MLP surrogate of the log-likelihood (inputs: the listed parameters,
+ * standardised; 3 hidden layers of `hidden` SiLU units; output logL - max),
+ * trained online with Adam on exact (theta, logL) pairs by hand-written
+ * BF16 tensor-core (tcgen05, FP32 accumulate) forward and backward kernels.
+ * It is the first stage of the delayed-acceptance stretch move.  No
+ * counterpart in the reference. */
+typedef struct pofd_surrogate pofd_surrogate;
+int pofd_surrogate_create(pofd_ctx* ctx, unsigned nparams,
+                          const int* input_idx, unsigned ninputs,
+                          unsigned hidden, unsigned capacity,
+                          unsigned long long seed, pofd_surrogate** out);
+int pofd_surrogate_destroy(pofd_surrogate* s);
+/* Appends the POFD_OK, finite pairs of device arrays theta_dev[n][npar],
+ * logl_dev[n] (status_dev may be NULL) to the ring buffer of capacity
+ * pairs; enqueued on stream. */
+int pofd_surrogate_add_pairs(pofd_surrogate* s, unsigned n,
+                             const float* theta_dev, unsigned npar,
+                             const double* logl_dev, const int* status_dev,
+                             void* stream);
+int pofd_surrogate_npairs(pofd_surrogate* s, unsigned* n);
+/* iters Adam steps (lr, beta 0.9/0.999) on minibatches of batch pairs drawn
+ * with replacement; the scaling is refreshed from the pairs first. */
+int pofd_surrogate_train(pofd_surrogate* s, unsigned iters, unsigned batch,
+                         float lr, float* last_loss);
+/* Predicted logL, with the pofd_batch_loglike_fn signature. */
+int pofd_surrogate_predict_device(void* s, unsigned nprop,
+                                  const float* theta_dev, unsigned npar,
+                                  double* logl_dev, int* status_dev,
+                                  void* stream);
+/* Parameters (FP32 masters) by tensor t = 0..7: W1 [hidden][16], b1, W2
+ * [hidden][hidden], b2, W3, b3, w4 [hidden], b4 [1]; *size receives the
+ * element count.  set_params takes all eight and resets Adam. */
+int pofd_surrogate_get_params(pofd_surrogate* s, int t, float* out,
+                              size_t* size);
+int pofd_surrogate_set_params(pofd_surrogate* s, const float* const* tensors);
+/* Mean-square-loss gradients over the first n pairs held, without an
+ * update: grads[8] host buffers of the tensor sizes. */
+int pofd_surrogate_gradients(pofd_surrogate* s, unsigned n,
+                             float* const* grads, float* loss);
+/* Input mean[16], 1/sd[16], then the target offset and scale (34 values). */
+int pofd_surrogate_scaling(pofd_surrogate* s, double* out34);
+/* The tensor-core main loop on its own, on device pointers of the current
+ * device: C[M][N] (fp32, ldc) = A[M][K] * B[N][K]^T, A and B bf16 with
+ * leading dimensions multiple of 8, N in [16, 512] and K >= 16 multiples of
+ * 16. */
+int pofd_bf16_gemm(int M, int N, int K, const void* A, int lda, const void* B,
+                   int ldb, float* C, int ldc, void* stream);
+
+/* Delayed acceptance (Christen & Fox 2005) with the stretch move: stage one
+ * accepts with min(1, z^(nparams-nfixed-1) e^{(S'-S)/T}) on the surrogate S;
+ * only stage-one survivors get the exact likelihood L, accepted with
+ * min(1, e^{((L'-L) - (S'-S))/T}), so the chain targets the exact
+ * posterior.  sfn/sur evaluate the first stage (pofd_surrogate_predict_device
+ * for the surrogate above). */
+int pofd_ensemble_set_surrogate(pofd_ensemble* e, pofd_batch_loglike_fn sfn,
+                                void* sur);
+/* Every exact evaluation of the ensemble is also appended to this
+ * surrogate's training pairs (NULL stops collecting). */
+int pofd_ensemble_collect_pairs(pofd_ensemble* e, pofd_surrogate* s);
+int pofd_ensemble_do_steps_da(pofd_ensemble* e, unsigned nsteps, int record);
+/* Counters since init: [0] proposals, [1] stage-one passes, [2] exact
+ * evaluations (padding included), [3] accepted moves. */
+int pofd_ensemble_da_stats(pofd_ensemble* e, unsigned long long* out4);
+
+/* Goodman's acor on one series x[n] (affineChainSet.cc:884-951); returns
+ * POFD_REJECTED when n < 50 (mean only). */
+int pofd_acor(const float* x, size_t n, double* mean, double* sigma,
+              double* tau);
+
 /* Measured FP64 FMA throughput of a device (TFLOP/s, 2 flops per FMA): the
  * denominator of the FP64-bound kernels' roofline.  No counterpart in the
  * reference (which has no GPU code). */

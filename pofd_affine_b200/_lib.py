@@ -77,6 +77,43 @@ SIGNATURES = {
     "pofd_like2_stage_name": (C.c_char_p, [I]),
     "pofd_pd1_loglike_noalloc": (I, [V, U, D, D, U, D, D, V, V, U, D, D, D, D,
                                      V, V, V]),
+    "pofd_ensemble_create": (I, [V, U, U, D, C.c_ulonglong, PV]),
+    "pofd_ensemble_destroy": (I, [V]),
+    "pofd_ensemble_set_likelihood": (I, [V, V, V]),
+    "pofd_ensemble_use_like1": (I, [V, V]),
+    "pofd_ensemble_use_like2": (I, [V, V]),
+    "pofd_ensemble_set_param_state": (I, [V, U, I]),
+    "pofd_ensemble_set_param_limits": (I, [V, U, C.c_float, C.c_float]),
+    "pofd_ensemble_set_temperature": (I, [V, D]),
+    "pofd_ensemble_init": (I, [V, _fp, V]),
+    "pofd_ensemble_reserve_chain": (I, [V, U]),
+    "pofd_ensemble_clear_chain": (I, [V]),
+    "pofd_ensemble_do_steps": (I, [V, U, I]),
+    "pofd_ensemble_nrecorded": (I, [V, C.POINTER(U)]),
+    "pofd_ensemble_chain": (I, [V, V, V]),
+    "pofd_ensemble_last": (I, [V, V, V]),
+    "pofd_ensemble_naccept": (I, [V, _up]),
+    "pofd_ensemble_acor": (I, [V, _dp]),
+    "pofd_gauss_create": (I, [V, U, _dp, _dp, PV]),
+    "pofd_gauss_destroy": (I, [V]),
+    "pofd_gauss_eval_batch_device": (I, [V, U, V, U, V, V, V]),
+    "pofd_surrogate_create": (I, [V, U, _ip, U, U, U, C.c_ulonglong, PV]),
+    "pofd_surrogate_destroy": (I, [V]),
+    "pofd_surrogate_add_pairs": (I, [V, U, V, U, V, V, V]),
+    "pofd_surrogate_npairs": (I, [V, C.POINTER(U)]),
+    "pofd_surrogate_train": (I, [V, U, U, C.c_float, C.POINTER(C.c_float)]),
+    "pofd_surrogate_predict_device": (I, [V, U, V, U, V, V, V]),
+    "pofd_surrogate_get_params": (I, [V, I, V, C.POINTER(S)]),
+    "pofd_surrogate_set_params": (I, [V, C.POINTER(C.c_void_p)]),
+    "pofd_surrogate_gradients": (I, [V, U, C.POINTER(C.c_void_p),
+                                     C.POINTER(C.c_float)]),
+    "pofd_surrogate_scaling": (I, [V, _dp]),
+    "pofd_bf16_gemm": (I, [I, I, I, V, I, V, I, V, I, V]),
+    "pofd_ensemble_set_surrogate": (I, [V, V, V]),
+    "pofd_ensemble_collect_pairs": (I, [V, V]),
+    "pofd_ensemble_do_steps_da": (I, [V, U, I]),
+    "pofd_ensemble_da_stats": (I, [V, C.POINTER(C.c_ulonglong)]),
+    "pofd_acor": (I, [_fp, S, C.POINTER(D), C.POINTER(D), C.POINTER(D)]),
 }
 
 _lib = None

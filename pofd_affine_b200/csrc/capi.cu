@@ -6,12 +6,16 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/pofd_b200.h"
 #include "engine1d.cuh"
 #include "engine2d.cuh"
+#include "ensemble.cuh"
+#include "surrogate.cuh"
 #include "setup.hh"
 
 namespace {
@@ -59,6 +63,21 @@ struct pofd_beam2 {
 struct pofd_like2 {
   pofd_ctx* ctx = nullptr;
   std::unique_ptr<pofd::Engine2> eng;
+};
+
+struct pofd_gauss {
+  pofd_ctx* ctx = nullptr;
+  std::unique_ptr<pofd::GaussLike> g;
+};
+
+struct pofd_surrogate {
+  pofd_ctx* ctx = nullptr;
+  std::unique_ptr<pofd::Surrogate> s;
+};
+
+struct pofd_ensemble {
+  pofd_ctx* ctx = nullptr;
+  std::unique_ptr<pofd::Ensemble> ens;
 };
 
 struct pofd_pdfactory1 {
@@ -599,5 +618,369 @@ int pofd_like2_profile(pofd_like2* L, unsigned nprop, const float* theta,
 }
 
 const char* pofd_like2_stage_name(int i) { return pofd::Engine2::stage_name(i); }
+
+// ------------------------------------------------------------- ensemble
+static int like1_batch(void* like, unsigned nprop, const float* theta,
+                       unsigned npar, double* logl, int* status, void* stream) {
+  return pofd_like1_eval_batch_device(static_cast<pofd_like1*>(like), nprop, theta, npar, logl,
+                                      status, stream);
+}
+static int like2_batch(void* like, unsigned nprop, const float* theta,
+                       unsigned npar, double* logl, int* status, void* stream) {
+  return pofd_like2_eval_batch_device(static_cast<pofd_like2*>(like), nprop, theta, npar, logl,
+                                      status, stream);
+}
+
+int pofd_ensemble_create(pofd_ctx* ctx, unsigned nwalkers, unsigned nparams,
+                         double scalefac, unsigned long long seed,
+                         pofd_ensemble** out) {
+  return guard([&] {
+    need(ctx && out, "null argument");
+    if (ctx->device >= 0) cudaSetDevice(ctx->device);
+    std::unique_ptr<pofd_ensemble> e(new pofd_ensemble());
+    e->ctx = ctx;
+    e->ens.reset(new pofd::Ensemble(ctx->device, ctx->stream, nwalkers, nparams, scalefac, seed));
+    *out = e.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_destroy(pofd_ensemble* e) {
+  if (e && e->ctx && e->ctx->device >= 0) cudaSetDevice(e->ctx->device);
+  delete e;
+  return POFD_OK;
+}
+
+int pofd_ensemble_set_likelihood(pofd_ensemble* e, pofd_batch_loglike_fn fn, void* like) {
+  return guard([&] {
+    need(e && fn, "null argument");
+    e->ens->set_like(fn, like);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_use_like1(pofd_ensemble* e, pofd_like1* like) {
+  return guard([&] {
+    need(e && like, "null argument");
+    e->ens->set_like(like1_batch, like);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_use_like2(pofd_ensemble* e, pofd_like2* like) {
+  return guard([&] {
+    need(e && like, "null argument");
+    e->ens->set_like(like2_batch, like);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_set_param_state(pofd_ensemble* e, unsigned idx, int state) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->set_param_state(idx, state);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_set_param_limits(pofd_ensemble* e, unsigned idx, float lo, float hi) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->set_limits(idx, lo, hi);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_set_temperature(pofd_ensemble* e, double temp) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->set_temperature(temp);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_init(pofd_ensemble* e, const float* walkers, const double* logl) {
+  return guard([&] {
+    need(e && walkers, "null argument");
+    e->ens->init(walkers, logl);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_reserve_chain(pofd_ensemble* e, unsigned nsteps) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->reserve_chain(nsteps);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_clear_chain(pofd_ensemble* e) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->clear_chain();
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_do_steps(pofd_ensemble* e, unsigned nsteps, int record) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->do_steps(nsteps, record != 0);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_nrecorded(pofd_ensemble* e, unsigned* n) {
+  return guard([&] {
+    need(e && n, "null argument");
+    *n = e->ens->nrecorded();
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_chain(pofd_ensemble* e, float* theta, double* logl) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->chain(theta, logl);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_last(pofd_ensemble* e, float* theta, double* logl) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->last(theta, logl);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_naccept(pofd_ensemble* e, unsigned* naccept) {
+  return guard([&] {
+    need(e && naccept, "null argument");
+    e->ens->naccept(naccept);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_acor(pofd_ensemble* e, double* tau) {
+  return guard([&] {
+    need(e && tau, "null argument");
+    return e->ens->acor(tau) ? POFD_OK : POFD_REJECTED;
+  });
+}
+
+int pofd_acor(const float* x, size_t n, double* mean, double* sigma, double* tau) {
+  return guard([&] {
+    need(x && mean && sigma && tau, "null argument");
+    need(n > 0, "empty series");
+    std::vector<float> v(x, x + n);
+    double m = 0, sg = std::numeric_limits<double>::quiet_NaN(),
+           t = std::numeric_limits<double>::quiet_NaN();
+    const int rc = pofd::acor_series(m, sg, t, v, static_cast<unsigned>(n));
+    *mean = m;
+    *sigma = sg;
+    *tau = t;
+    return rc ? POFD_REJECTED : POFD_OK;
+  });
+}
+
+int pofd_gauss_create(pofd_ctx* ctx, unsigned k, const double* mean, const double* icov,
+                      pofd_gauss** out) {
+  return guard([&] {
+    need(ctx && mean && icov && out, "null argument");
+    std::unique_ptr<pofd_gauss> g(new pofd_gauss());
+    g->ctx = ctx;
+    g->g.reset(new pofd::GaussLike(ctx->device, k, mean, icov));
+    *out = g.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_gauss_destroy(pofd_gauss* g) {
+  if (g && g->ctx && g->ctx->device >= 0) cudaSetDevice(g->ctx->device);
+  delete g;
+  return POFD_OK;
+}
+
+int pofd_gauss_eval_batch_device(void* gv, unsigned nprop, const float* theta, unsigned npar,
+                                 double* logl, int* status, void* stream) {
+  return guard([&] {
+    pofd_gauss* g = static_cast<pofd_gauss*>(gv);
+    need(g && theta && logl && status, "null argument");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g->ctx->stream;
+    g->g->enqueue(nprop, theta, npar, logl, status, st);
+    return POFD_OK;
+  });
+}
+
+// ------------------------------------------------------------ surrogate
+int pofd_surrogate_create(pofd_ctx* ctx, unsigned nparams, const int* input_idx,
+                          unsigned ninputs, unsigned hidden, unsigned capacity,
+                          unsigned long long seed, pofd_surrogate** out) {
+  return guard([&] {
+    need(ctx && input_idx && out, "null argument");
+    if (ctx->device >= 0) cudaSetDevice(ctx->device);
+    std::unique_ptr<pofd_surrogate> s(new pofd_surrogate());
+    s->ctx = ctx;
+    s->s.reset(new pofd::Surrogate(ctx->device, ctx->stream, nparams, input_idx, ninputs, hidden,
+                                   capacity, seed));
+    *out = s.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_destroy(pofd_surrogate* s) {
+  if (s && s->ctx && s->ctx->device >= 0) cudaSetDevice(s->ctx->device);
+  delete s;
+  return POFD_OK;
+}
+
+int pofd_surrogate_add_pairs(pofd_surrogate* s, unsigned n, const float* theta, unsigned npar,
+                             const double* logl, const int* status, void* stream) {
+  return guard([&] {
+    need(s && theta && logl, "null argument");
+    s->s->add_pairs(n, theta, npar, logl, status, static_cast<cudaStream_t>(stream));
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_npairs(pofd_surrogate* s, unsigned* n) {
+  return guard([&] {
+    need(s && n, "null argument");
+    *n = s->s->npairs();
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_train(pofd_surrogate* s, unsigned iters, unsigned batch, float lr,
+                         float* last_loss) {
+  return guard([&] {
+    need(s != nullptr, "null argument");
+    s->s->train(iters, batch, lr, last_loss);
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_predict_device(void* sv, unsigned nprop, const float* theta, unsigned npar,
+                                  double* logl, int* status, void* stream) {
+  return guard([&] {
+    pofd_surrogate* s = static_cast<pofd_surrogate*>(sv);
+    need(s && theta && logl, "null argument");
+    s->s->predict(nprop, theta, npar, logl, status, static_cast<cudaStream_t>(stream));
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_get_params(pofd_surrogate* s, int t, float* out, size_t* size) {
+  return guard([&] {
+    need(s != nullptr, "null argument");
+    need(t >= 0 && t < pofd::Surrogate::kNumTensors, "tensor index out of range");
+    if (size) *size = s->s->tensor_size(t);
+    if (out) {
+      std::vector<std::vector<float>> h;
+      s->s->get_params_host(h);
+      std::memcpy(out, h[t].data(), h[t].size() * sizeof(float));
+    }
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_set_params(pofd_surrogate* s, const float* const* tensors) {
+  return guard([&] {
+    need(s && tensors, "null argument");
+    std::vector<std::vector<float>> h(pofd::Surrogate::kNumTensors);
+    for (int t = 0; t < pofd::Surrogate::kNumTensors; ++t) {
+      need(tensors[t] != nullptr, "null tensor");
+      h[t].assign(tensors[t], tensors[t] + s->s->tensor_size(t));
+    }
+    s->s->set_params_host(h);
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_gradients(pofd_surrogate* s, unsigned n, float* const* grads, float* loss) {
+  return guard([&] {
+    need(s && grads, "null argument");
+    float* dev[pofd::Surrogate::kNumTensors];
+    for (int t = 0; t < pofd::Surrogate::kNumTensors; ++t) dev[t] = nullptr;
+    struct Free {
+      float** d;
+      ~Free() {
+        for (int t = 0; t < pofd::Surrogate::kNumTensors; ++t)
+          if (d[t]) cudaFree(d[t]);
+      }
+    } fr{dev};
+    for (int t = 0; t < pofd::Surrogate::kNumTensors; ++t) {
+      need(grads[t] != nullptr, "null gradient buffer");
+      if (cudaMalloc(&dev[t], s->s->tensor_size(t) * sizeof(float)) != cudaSuccess)
+        throw pofd::Error(POFD_E_NOMEM, "cudaMalloc");
+    }
+    s->s->gradients(n, dev, loss);
+    for (int t = 0; t < pofd::Surrogate::kNumTensors; ++t)
+      if (cudaMemcpy(grads[t], dev[t], s->s->tensor_size(t) * sizeof(float),
+                     cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw pofd::Error(POFD_E_CUDA, "D2H gradients");
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_scaling(pofd_surrogate* s, double* out) {
+  return guard([&] {
+    need(s && out, "null argument");
+    s->s->scaling(out);
+    return POFD_OK;
+  });
+}
+
+int pofd_bf16_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C,
+                   int ldc, void* stream) {
+  return guard([&] {
+    need(A && B && C, "null argument");
+    int* err = nullptr;
+    if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) throw pofd::Error(POFD_E_NOMEM, "cudaMalloc");
+    struct Free { int* p; ~Free() { cudaFree(p); } } fr{err};
+    cudaMemset(err, 0, sizeof(int));
+    pofd::bf16_gemm(M, N, K, A, lda, B, ldb, C, ldc, err, static_cast<cudaStream_t>(stream));
+    int e = 0;
+    if (cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess ||
+        cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw pofd::Error(POFD_E_CUDA, cudaGetErrorString(cudaGetLastError()));
+    if (e) throw pofd::Error(POFD_E_CUDA, "tensor-core wait timed out");
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_set_surrogate(pofd_ensemble* e, pofd_batch_loglike_fn sfn, void* sur) {
+  return guard([&] {
+    need(e && sfn, "null argument");
+    e->ens->set_stage1(sfn, sur);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_collect_pairs(pofd_ensemble* e, pofd_surrogate* s) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->collect_pairs(s ? s->s.get() : nullptr);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_do_steps_da(pofd_ensemble* e, unsigned nsteps, int record) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->do_steps_da(nsteps, record != 0);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_da_stats(pofd_ensemble* e, unsigned long long* out4) {
+  return guard([&] {
+    need(e && out4, "null argument");
+    e->ens->da_stats(out4);
+    return POFD_OK;
+  });
+}
 
 }  // extern "C"

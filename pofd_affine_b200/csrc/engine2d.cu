@@ -382,39 +382,44 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
   }
 }
 
-// Edge integral along band 1 for row 0 (PDFactoryDouble.cc:472-514):
-// Rx[j] = iRxnorm * log-trapezoid over the edge band-1 fluxes of R.
+// Edge rows (band-1 fluxes below the first grid step) against every main and
+// edge column, weighted by the log-trapezoid factors of the band-1 edge
+// integral (PDFactoryDouble.cc:426-514).  One block per (column tile, group
+// of ER edge rows, proposal x beam set); the group partials are summed in
+// k_rfinish2 into Rx (main columns) and the double integral r[0,0] (edge
+// columns).
+constexpr int ER = 8;
 __global__ void __launch_bounds__(NT)
-k_rx2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
-      const int* __restrict__ mstatus, const double* __restrict__ rw,
-      double* __restrict__ redge) {
+k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
+         const int* __restrict__ mstatus, const double* __restrict__ rw,
+         double* __restrict__ epart) {
   extern __shared__ double sm[];
   __shared__ int sh[40];
   __shared__ int s_cnt[2];
-  const int wb = blockIdx.y;
+  const int wb = blockIdx.z;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
   const BSet2Dev& bs = bsets[b];
-  const int T = bs.T;
   double* s_pos = sm;
-  double* s_neg = sm + 3 * T;
+  double* s_neg = sm + 3 * bs.T;
+  const int ncol = n + nedge;
   const int j = blockIdx.x * NT + threadIdx.x;
   double acc = 0.0;
-  for (int i = 0; i < nedge; ++i) {
+  for (int rr = 0; rr < ER; ++rr) {
+    const int i = blockIdx.y * ER + rr;
+    if (i >= nedge) break;
     const int r = n + i;
     const int sgn1 = bs.rowsgn[r];
     stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
               s_pos, s_neg, s_cnt, sh);
-    if (j < n) {
+    if (j < ncol) {
       const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j);
       const double rf = bs.e1[i];
-      if (i == 0) acc = 0.5 * rf * R;
-      else if (i == nedge - 1) acc += 0.5 * rf * R;
-      else acc += rf * R;
+      acc += ((i == 0 || i == nedge - 1) ? 0.5 : 1.0) * rf * R;
     }
     __syncthreads();
   }
-  if (j < n) redge[static_cast<size_t>(wb) * (2 * n + 1) + j] = acc * bs.iRxnorm;
+  if (j < ncol) epart[(static_cast<size_t>(wb) * gridDim.y + blockIdx.y) * ncol + j] = acc;
 }
 
 // Edge integral along band 2 for column 0 (PDFactoryDouble.cc:518-550):
@@ -449,49 +454,14 @@ k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
     redge[static_cast<size_t>(wb) * (2 * n + 1) + n + r] = acc * bs.iRynorm;
 }
 
-// r[0,0]: the double edge integral (PDFactoryDouble.cc:426-467).
-__global__ void __launch_bounds__(NT)
-k_r002(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
-       const int* __restrict__ mstatus, const double* __restrict__ rw,
-       double* __restrict__ redge) {
-  extern __shared__ double sm[];
-  __shared__ int sh[40];
-  __shared__ int s_cnt[2];
-  __shared__ double shr[32];
-  const int wb = blockIdx.x;
-  const int w = wb / B, b = wb - w * B;
-  if (mstatus[w] != 0) return;
-  const BSet2Dev& bs = bsets[b];
-  const int T = bs.T;
-  double* s_pos = sm;
-  double* s_neg = sm + 3 * T;
-  double s = 0.0;
-  for (int i = 0; i < nedge; ++i) {
-    const int r = n + i;
-    const int sgn1 = bs.rowsgn[r];
-    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
-              s_pos, s_neg, s_cnt, sh);
-    double acc = 0.0;
-    for (int jj = threadIdx.x; jj < nedge; jj += NT) {
-      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], n + jj);
-      acc += (jj == 0 || jj == nedge - 1) ? 0.5 * R : R;
-    }
-    acc = dev::block_sum<NT>(acc, shr);
-    const double rf = bs.e1[i];
-    if (i == 0) s = 0.5 * rf * acc;
-    else if (i == nedge - 1) s += 0.5 * rf * acc;
-    else s += rf * acc;
-  }
-  if (threadIdx.x == 0) redge[static_cast<size_t>(wb) * (2 * n + 1) + 2 * n] = s * bs.iR00norm;
-}
-
 // Edge cells into the grid (times dflux1*dflux2), the remaining moment
 // contributions and the shift decisions (PDFactoryDouble.cc:560-585,
 // 1198-1213).
 __global__ void __launch_bounds__(NT)
 k_rfinish2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
-           int edge, int nparts, const int* __restrict__ mstatus,
-           const double* __restrict__ redge, const double* __restrict__ rpart,
+           int edge, int nedge, int ngr, int nparts,
+           const int* __restrict__ mstatus, const double* __restrict__ redge,
+           const double* __restrict__ epart, const double* __restrict__ rpart,
            double* __restrict__ rbuf, double* __restrict__ mom) {
   __shared__ double shr[32];
   const int wb = blockIdx.x;
@@ -501,11 +471,33 @@ k_rfinish2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
   const double fluxfac = bs.dflux1 * bs.dflux2;
   const double* E = redge + static_cast<size_t>(wb) * (2 * n + 1);
   double* R = rbuf + static_cast<size_t>(wb) * n * nc2;
+  const int ncol = n + nedge;
+  const double* ep = epart + static_cast<size_t>(wb) * ngr * ncol;
+  // r[0,0]: trapezoid over the edge columns of the band-1-weighted sums
+  double r00 = 0.0;
+  if (edge) {
+    for (int jj = threadIdx.x; jj < nedge; jj += NT) {
+      double c = 0.0;
+      for (int g = 0; g < ngr; ++g) c += ep[static_cast<size_t>(g) * ncol + n + jj];
+      r00 += (jj == 0 || jj == nedge - 1) ? 0.5 * c : c;
+    }
+    r00 = dev::block_sum<NT>(r00, shr) * bs.iR00norm;
+  }
   double m1 = 0.0, v1 = 0.0, m2 = 0.0, v2 = 0.0;
   // row 0 (row factor 1/2), all columns
   const double cf1r0 = bs.rowflux[0];
   for (int j = threadIdx.x; j < n; j += NT) {
-    const double val = edge ? ((j == 0) ? E[2 * n] : E[j]) * fluxfac : 0.0;
+    double val = 0.0;
+    if (edge) {
+      if (j == 0) {
+        val = r00;
+      } else {
+        double c = 0.0;
+        for (int g = 0; g < ngr; ++g) c += ep[static_cast<size_t>(g) * ncol + j];
+        val = c * bs.iRxnorm;
+      }
+      val *= fluxfac;
+    }
     R[j] = val;
     const double cR = 0.5 * val;
     const double wc = (j == 0 || j == n - 1) ? 0.5 : 1.0;
@@ -1333,7 +1325,7 @@ void Engine2::build_static() {
 
 void Engine2::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.rw, ws_.rbuf,
-                  ws_.rpart, ws_.redge, ws_.mom, ws_.pbuf, ws_.rowpart,
+                  ws_.rpart, ws_.redge, ws_.epart, ws_.mom, ws_.pbuf, ws_.rowpart,
                   ws_.colpart, ws_.pinfo, ws_.gpart, ws_.pdout,
                   ws_.theta_in, ws_.logl, ws_.status};
   for (void* q : ptrs)
@@ -1368,6 +1360,8 @@ void Engine2::reserve(unsigned P) {
   ws_.rbuf = dal<double>(static_cast<size_t>(P) * B_ * n * nc2);
   ws_.rpart = dal<double>(static_cast<size_t>(P) * B_ * gx_ * gy_ * 4);
   ws_.redge = dal<double>(static_cast<size_t>(P) * B_ * (2 * n + 1));
+  const size_t ngr = edge_ ? (nedge_ + ER - 1) / ER : 0;
+  ws_.epart = dal<double>(static_cast<size_t>(P) * B_ * (ngr ? ngr * (n + nedge_) : 1));
   ws_.mom = dal<double>(static_cast<size_t>(P) * B_ * 8);
   ws_.pbuf = dal<double>(static_cast<size_t>(P) * D_ * n * nc2);
   ws_.rowpart = dal<double>(static_cast<size_t>(P) * D_ * n * nct_);
@@ -1380,9 +1374,8 @@ void Engine2::reserve(unsigned P) {
   ck(cudaMemset(ws_.redge, 0, static_cast<size_t>(P) * B_ * (2 * n + 1) * sizeof(double)), "memset");
   const int smem_rows = static_cast<int>(6 * MAXT * sizeof(double));
   ck(cudaFuncSetAttribute(k_rgrid2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
-  ck(cudaFuncSetAttribute(k_rx2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
+  ck(cudaFuncSetAttribute(k_redge2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
   ck(cudaFuncSetAttribute(k_ry2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
-  ck(cudaFuncSetAttribute(k_r002, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
   ck(cudaFuncSetAttribute(k_psplit2, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           static_cast<int>(3 * 8192 * sizeof(double))), "attr");
 }
@@ -1427,15 +1420,17 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   k_rgrid2<<<dim3(gx_, gy_, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, nc2, ws_.mstatus,
                                                          ws_.rw, ws_.rbuf, ws_.rpart);
   mark(3);
+  const int ngr = (ne + ER - 1) / ER;
   if (edge_) {
-    k_rx2<<<dim3(gx_, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.redge);
+    const unsigned gxe = static_cast<unsigned>((n + ne + NT - 1) / NT);
+    k_redge2<<<dim3(gxe, ngr, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus,
+                                                            ws_.rw, ws_.epart);
     k_ry2<<<dim3(n - 1, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.redge);
-    k_r002<<<P * B, NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.redge);
   }
   mark(4);
-  k_rfinish2<<<P * B, NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0,
+  k_rfinish2<<<P * B, NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0, ne, ngr,
                                    static_cast<int>(gx_ * gy_), ws_.mstatus, ws_.redge,
-                                   ws_.rpart, ws_.rbuf, ws_.mom);
+                                   ws_.epart, ws_.rpart, ws_.rbuf, ws_.mom);
   mark(5);
   if (r_only) {
     ck(cudaGetLastError(), "kernel launch");
@@ -1625,7 +1620,7 @@ void Engine2::profile_stages(unsigned nprop, const float* theta, unsigned npar,
 
 const char* Engine2::stage_name(int i) {
   static const char* names[kNumStages] = {
-      "k_model2", "k_rows2", "k_rgrid2", "k_rx2+k_ry2+k_r002", "k_rfinish2",
+      "k_model2", "k_rows2", "k_rgrid2", "k_redge2+k_ry2", "k_rfinish2",
       "cufft_d2z_2d", "k_spectrum2", "cufft_z2d_2d", "k_pscan2", "k_psplit2",
       "k_pgather2", "k_reduce2"};
   return (i >= 0 && i < kNumStages) ? names[i] : "";

@@ -105,7 +105,7 @@ class Engine2 {
   void profile_stages(unsigned nprop, const float* theta, unsigned npar,
                       int reps, double* stage_ms);
   static const char* stage_name(int i);
-  int kernels_per_eval() const { return edge_ ? 13 : 10; }
+  int kernels_per_eval() const { return edge_ ? 11 : 9; }
   unsigned nparams() const {
     return static_cast<unsigned>(knots_.size() + sigk_.size() + offk_.size());
   }
@@ -175,7 +175,8 @@ class Engine2 {
     double* rw = nullptr;       // [P][B][nrows][T][3]
     double* rbuf = nullptr;     // [P][B][n][2nc]
     double* rpart = nullptr;    // [P][B][gy][gx][4]
-    double* redge = nullptr;    // [P][B][2n+1]: Rx (n), Ry (n), r00
+    double* redge = nullptr;    // [P][B][2n+1]: Ry at [n, 2n)
+    double* epart = nullptr;    // [P][B][edge row groups][n + nedge]
     double* mom = nullptr;      // [P][B][8]
     double* pbuf = nullptr;     // [P][D][n][2nc]
     double* rowpart = nullptr;  // [P][D][n][nct]

@@ -1,0 +1,197 @@
+"""Python mirror of the reference's affine-invariant ensemble sampler.
+
+  * affineEnsemble  affineEnsemble (affineEnsemble.h:60-200) over a batched
+                    likelihood of this library (calcLike, calcLikeDouble,
+                    gaussLike): setParamFixed / setParamBonus /
+                    setParamIgnoreAcor, doSteps(nsteps, initsteps),
+                    doBurnIn (fixed burn), getAcor, getAcceptanceFrac, and the
+                    recorded chain.
+  * acor            Goodman's acor (affineChainSet.cc:884-951).
+  * gaussLike       a multivariate Gaussian test likelihood on the device.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import PofdError, check, lib  # noqa: F401
+
+FIXED, ACIGNORE, BONUS = 1, 2, 4  # mcmc_affine (global_settings.h:57)
+
+
+def acor(x):
+    """(mean, sigma, tau, ok) of a series by Goodman's acor; ok is False
+    when the series is shorter than 50 (then only the mean is set)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    m, s, t = C.c_double(), C.c_double(), C.c_double()
+    rc = check(lib().pofd_acor(x, x.size, C.byref(m), C.byref(s),
+                               C.byref(t)))
+    return m.value, s.value, t.value, rc == 0
+
+
+class gaussLike:
+    """log N(theta[:k]; mean, cov) up to a constant, batched on the GPU."""
+
+    def __init__(self, ctx, mean, cov):
+        mean = np.ascontiguousarray(mean, dtype=np.float64)
+        icov = np.ascontiguousarray(np.linalg.inv(np.asarray(cov, np.float64)))
+        h = C.c_void_p()
+        check(lib().pofd_gauss_create(ctx.h, mean.size, mean, icov,
+                                      C.byref(h)))
+        self.h, self.ctx, self.k = h, ctx, mean.size
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pofd_gauss_destroy(self.h)
+            self.h = None
+
+
+class affineEnsemble:
+    """Batched stretch-move ensemble (one process, one GPU)."""
+
+    def __init__(self, ctx, like, nwalkers, nparams, scalefac=2.0, seed=0):
+        h = C.c_void_p()
+        check(lib().pofd_ensemble_create(ctx.h, int(nwalkers), int(nparams),
+                                         float(scalefac), int(seed),
+                                         C.byref(h)))
+        self.h, self.ctx, self.like = h, ctx, like
+        self.nwalkers, self.nparams = int(nwalkers), int(nparams)
+        self.state = np.zeros(self.nparams, dtype=np.int32)
+        self.lo = np.full(self.nparams, -np.inf, np.float32)
+        self.hi = np.full(self.nparams, np.inf, np.float32)
+        self.nsteps_done = 0
+        from .api1d import calcLike
+        from .api2d import calcLikeDouble
+        if isinstance(like, calcLike):
+            check(lib().pofd_ensemble_use_like1(h, like.h))
+        elif isinstance(like, calcLikeDouble):
+            check(lib().pofd_ensemble_use_like2(h, like.h))
+        elif isinstance(like, gaussLike):
+            fn = C.cast(lib().pofd_gauss_eval_batch_device, C.c_void_p)
+            check(lib().pofd_ensemble_set_likelihood(h, fn, like.h))
+        else:
+            raise PofdError(-10, "unsupported likelihood object")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pofd_ensemble_destroy(self.h)
+            self.h = None
+
+    # ---------------------------------------------------------- set-up
+    def _state(self, i, bits):
+        self.state[i] |= bits
+        check(lib().pofd_ensemble_set_param_state(self.h, int(i),
+                                                  int(self.state[i])))
+
+    def setParamFixed(self, i):
+        self._state(i, FIXED | ACIGNORE)
+
+    def setParamIgnoreAcor(self, i):
+        self._state(i, ACIGNORE)
+
+    def setParamBonus(self, i):
+        self._state(i, ACIGNORE | BONUS)
+
+    def setParamLimits(self, i, lo=-np.inf, hi=np.inf):
+        self.lo[i], self.hi[i] = lo, hi
+        check(lib().pofd_ensemble_set_param_limits(self.h, int(i), float(lo),
+                                                   float(hi)))
+
+    def setTemperature(self, t):
+        check(lib().pofd_ensemble_set_temperature(self.h, float(t)))
+
+    def generateInitialPosition(self, theta0, sigma, rng=None,
+                                maxtrials=1000):
+        """Walkers theta0 + sigma * N(0, 1) per free parameter, redrawn
+        until inside the limits (initFileKnots::generateRandomKnotValues);
+        fixed parameters keep theta0, bonus ones are NaN."""
+        rng = np.random.default_rng(rng)
+        theta0 = np.asarray(theta0, np.float32)
+        sigma = np.broadcast_to(np.asarray(sigma, np.float64), theta0.shape)
+        w = np.empty((self.nwalkers, self.nparams), np.float32)
+        for k in range(self.nwalkers):
+            for p in range(self.nparams):
+                if self.state[p] & BONUS:
+                    w[k, p] = np.nan
+                    continue
+                if self.state[p] & FIXED or sigma[p] == 0:
+                    w[k, p] = theta0[p]
+                    continue
+                for _ in range(maxtrials):
+                    v = np.float32(theta0[p] + sigma[p] * rng.standard_normal())
+                    if self.lo[p] <= v <= self.hi[p]:
+                        break
+                else:
+                    raise PofdError(-10, "Couldn't generate initial value")
+                w[k, p] = v
+        return w
+
+    def initChains(self, walkers, logl=None):
+        w = np.ascontiguousarray(walkers, dtype=np.float32)
+        if w.shape != (self.nwalkers, self.nparams):
+            raise PofdError(-10, "walkers must be [nwalkers, nparams]")
+        lp = None
+        if logl is not None:
+            self._l0 = np.ascontiguousarray(logl, dtype=np.float64)
+            lp = self._l0.ctypes.data_as(C.c_void_p)
+        check(lib().pofd_ensemble_init(self.h, w, lp))
+        self.nsteps_done = 0
+
+    # ------------------------------------------------------------ steps
+    def doSteps(self, nsteps, initsteps=0):
+        """initsteps unrecorded steps, then nsteps recorded ones."""
+        if initsteps:
+            check(lib().pofd_ensemble_do_steps(self.h, int(initsteps), 0))
+            self.nsteps_done += int(initsteps)
+        if nsteps:
+            check(lib().pofd_ensemble_do_steps(self.h, int(nsteps), 1))
+            self.nsteps_done += int(nsteps)
+
+    def doBurnIn(self, nburn):
+        """Fixed burn-in (the -f mode): nburn unrecorded steps."""
+        self.doSteps(0, nburn)
+
+    def clearChain(self):
+        check(lib().pofd_ensemble_clear_chain(self.h))
+
+    # ---------------------------------------------------------- results
+    def nRecorded(self):
+        n = C.c_uint()
+        check(lib().pofd_ensemble_nrecorded(self.h, C.byref(n)))
+        return n.value
+
+    def getChain(self):
+        n = self.nRecorded()
+        th = np.empty((n, self.nwalkers, self.nparams), np.float32)
+        ll = np.empty((n, self.nwalkers), np.float64)
+        if n:
+            check(lib().pofd_ensemble_chain(self.h,
+                                            th.ctypes.data_as(C.c_void_p),
+                                            ll.ctypes.data_as(C.c_void_p)))
+        return th, ll
+
+    def getLast(self):
+        th = np.empty((self.nwalkers, self.nparams), np.float32)
+        ll = np.empty(self.nwalkers, np.float64)
+        check(lib().pofd_ensemble_last(self.h, th.ctypes.data_as(C.c_void_p),
+                                       ll.ctypes.data_as(C.c_void_p)))
+        return th, ll
+
+    def getNAccept(self):
+        out = np.empty(self.nwalkers, np.uint32)
+        check(lib().pofd_ensemble_naccept(self.h, out))
+        return out
+
+    def getAcceptanceFrac(self):
+        return self.getNAccept() / max(self.nsteps_done, 1)
+
+    def getAcor(self):
+        """(tau[nparams], ok): NaN for ignored parameters."""
+        tau = np.empty(self.nparams)
+        rc = check(lib().pofd_ensemble_acor(self.h, tau))
+        return tau, rc == 0
+
+    def getESS(self):
+        """nwalkers * nrecorded / max tau (acor over the recorded chain)."""
+        tau, ok = self.getAcor()
+        t = np.nanmax(tau) if np.any(np.isfinite(tau)) else np.nan
+        return self.nwalkers * self.nRecorded() / t, tau, ok

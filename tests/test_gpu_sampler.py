@@ -1,0 +1,128 @@
+"""The batched GPU stretch-move ensemble against the oracle restatement:
+identical chains draw for draw (same counter-based random numbers), acor
+bit for bit, the known posterior of a Gaussian, and the reference's error
+behaviour."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _gauss(k=3, seed=0):
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(k, k))
+    cov = A @ A.T + k * np.eye(k)
+    mu = rng.normal(size=k) * 2
+    return mu, cov
+
+
+def _np_gauss(mu, cov):
+    icov = np.linalg.inv(cov)
+
+    def ll(th):
+        d = th[:, :len(mu)].astype(np.float64) - mu
+        bad = np.isnan(d).any(1)
+        out = -0.5 * np.einsum("ij,jk,ik->i", d, icov, d)
+        return out, np.where(bad, -1, 0)
+    return ll
+
+
+@pytest.mark.parametrize("nw", [16, 15])
+def test_chain_matches_oracle_gauss(gpu_ctx, nw):
+    import sampler_oracle as so
+    from pofd_affine_b200.mcmc import affineEnsemble, gaussLike
+    mu, cov = _gauss(3)
+    npar = 5  # 3 Gaussian parameters, one fixed, one bonus
+    G = gaussLike(gpu_ctx, mu, cov)
+    E = affineEnsemble(gpu_ctx, G, nw, npar, scalefac=2.0, seed=1234)
+    E.setParamFixed(3)
+    E.setParamBonus(4)
+    E.setParamLimits(0, mu[0] - 3 * np.sqrt(cov[0, 0]), np.inf)
+    w = E.generateInitialPosition(np.r_[mu, 7.0, 0.0], np.r_[np.ones(3), 0, 0],
+                                  rng=2)
+    E.initChains(w)
+    E.doSteps(40)
+    ch, cl = E.getChain()
+    oc, ol, on = so.stretch_run(w, np.full(nw, -np.inf), _np_gauss(mu, cov),
+                                40, seed=1234, state=E.state, lo=E.lo,
+                                hi=E.hi)
+    assert np.array_equal(ch, oc, equal_nan=True)
+    assert np.allclose(cl, ol, rtol=1e-13, atol=0)
+    assert np.array_equal(E.getNAccept(), on)
+    assert np.all(np.isnan(ch[..., 4])) and np.all(ch[..., 3] == 7.0)
+
+
+def test_acor_and_posterior_gauss(gpu_ctx):
+    import sampler_oracle as so
+    from pofd_affine_b200.mcmc import affineEnsemble, gaussLike
+    mu, cov = _gauss(4, seed=3)
+    G = gaussLike(gpu_ctx, mu, cov)
+    nw = 32
+    E = affineEnsemble(gpu_ctx, G, nw, 4, seed=9)
+    E.initChains(E.generateInitialPosition(mu, 1.0, rng=4))
+    E.doSteps(2000, initsteps=200)
+    ch, _ = E.getChain()
+    assert ch.shape == (2000, nw, 4)
+    tau, ok = E.getAcor()
+    assert ok
+    for p in range(4):
+        _, _, t, st = so.acor(so.average_series(ch, p))
+        assert st == 0 and t == tau[p]
+    s = ch.reshape(-1, 4).astype(np.float64)
+    sd = np.sqrt(np.diag(cov))
+    ess = nw * 2000 / tau.max()
+    assert np.all(np.abs(s.mean(0) - mu) < 5 * sd / np.sqrt(ess))
+    assert np.all(np.abs(np.diag(np.cov(s.T)) / np.diag(cov) - 1) < 0.15)
+    acc = E.getAcceptanceFrac()
+    assert 0.2 < acc.mean() < 0.9
+
+
+def test_chain_matches_oracle_1d_likelihood(orc, gpu_ctx):
+    """Ten steps of 12 walkers through the 1D P(D) likelihood."""
+    import sampler_oracle as so
+    from pofd_affine_b200 import beam, calcLike, synth
+    from pofd_affine_b200.mcmc import affineEnsemble
+    cfg = synth.config_1d_small(seed=1)
+    n, ni = 2048, 256
+    O = orc.Like1(cfg["knotpos"], n, ni, True, 400)
+    O.add_beamset(cfg["beams"][0], 6.0, 1e-5, True, 120)
+    L = calcLike(gpu_ctx, cfg["knotpos"], n, ni, True, 400)
+    L.addBeamSet(beam(cfg["beams"][0], 6.0, True, 120))
+    O.add_dataset(0, cfg["maps"][0], 0.0025)
+    L.addDataset(0, cfg["maps"][0], 0.0025)
+    O.set_rranges(cfg["theta0"])
+    L.setRRanges(cfg["theta0"])
+    nw, npar = 12, cfg["theta0"].size
+    E = affineEnsemble(gpu_ctx, L, nw, npar, seed=77)
+    E.setParamFixed(npar - 1)
+    w = E.generateInitialPosition(cfg["theta0"], 0.02, rng=5)
+    E.initChains(w)
+    E.doSteps(10)
+    ch, cl = E.getChain()
+    oc, ol, _ = so.stretch_run(w, np.full(nw, -np.inf),
+                               lambda t: O.loglike_batch(t, 4), 10, seed=77,
+                               state=E.state)
+    assert np.array_equal(ch, oc)
+    assert np.max(np.abs(cl - ol)) < 1e-6
+
+
+def test_errors_mirror_reference(gpu_ctx):
+    from pofd_affine_b200 import PofdError
+    from pofd_affine_b200.mcmc import affineEnsemble, gaussLike
+    mu, cov = _gauss(2)
+    G = gaussLike(gpu_ctx, mu, cov)
+    E = affineEnsemble(gpu_ctx, G, 8, 2, seed=1)
+    with pytest.raises(PofdError):
+        E.doSteps(1)  # chains not initialised
+    # walkers outside the limits: no valid step after 40 retries
+    E.setParamLimits(0, 100.0, 101.0)
+    E.initChains(np.zeros((8, 2), np.float32))
+    with pytest.raises(PofdError, match="Unable to generate new step"):
+        E.doSteps(2)
+    # a NaN walker makes the likelihood fail: the run stops
+    E2 = affineEnsemble(gpu_ctx, G, 8, 2, seed=1)
+    w = np.zeros((8, 2), np.float32)
+    w[:, 1] = np.nan
+    E2.initChains(w)
+    with pytest.raises(PofdError):
+        E2.doSteps(1)

@@ -1,0 +1,67 @@
+"""The sampler's host pieces without a GPU: acor of the product library
+against the oracle restatement, bit for bit, and the oracle stretch move
+against the known posterior of a Gaussian."""
+import numpy as np
+import pytest
+
+
+def _ar1(n, rho, seed):
+    rng = np.random.default_rng(seed)
+    x = np.empty(n)
+    x[0] = rng.standard_normal()
+    for i in range(1, n):
+        x[i] = rho * x[i - 1] + np.sqrt(1 - rho * rho) * rng.standard_normal()
+    return x.astype(np.float32)
+
+
+@pytest.mark.parametrize("n,rho", [(30, 0.0), (200, 0.0), (1000, 0.5),
+                                   (4000, 0.9), (5001, 0.97), (80, 0.9),
+                                   (120, 0.95), (300, 0.98)])
+def test_acor_matches_oracle(built_lib, n, rho):
+    import sampler_oracle as so
+    from pofd_affine_b200.mcmc import acor
+    x = _ar1(n, rho, 3)
+    m, s, t, ok = acor(x)
+    om, os_, ot, st = so.acor(x.copy())
+    assert ok == (st == 0)
+    assert m == om
+    if ok:
+        assert s == os_ and t == ot
+    if ok and n >= 4000 and rho <= 0.9:
+        # AR(1): tau = (1 + rho) / (1 - rho)
+        assert abs(t / ((1 + rho) / (1 - rho)) - 1) < 0.35
+
+
+def test_philox_known_answer():
+    """Philox4x32-10 known-answer vectors of the Random123 distribution
+    (kat_vectors: counter/key all zeros, all ones, and the pi digits)."""
+    import sampler_oracle as so
+    assert so.philox4x32_10((0, 0, 0, 0), (0, 0)) == (
+        0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)
+    assert so.philox4x32_10((0xffffffff,) * 4, (0xffffffff,) * 2) == (
+        0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)
+    assert so.philox4x32_10((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344),
+                            (0xa4093822, 0x299f31d0)) == (
+        0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1)
+
+
+def test_oracle_stretch_samples_gaussian():
+    import sampler_oracle as so
+    rng = np.random.default_rng(0)
+    k = 3
+    A = rng.normal(size=(k, k))
+    cov = A @ A.T + k * np.eye(k)
+    mu = np.array([1.0, -2.0, 0.5])
+    icov = np.linalg.inv(cov)
+
+    def ll(th):
+        d = th.astype(np.float64) - mu
+        return -0.5 * np.einsum("ij,jk,ik->i", d, icov, d), np.zeros(len(th), int)
+
+    nw = 16
+    w = (mu + rng.normal(size=(nw, k))).astype(np.float32)
+    ch, _, nacc = so.stretch_run(w, np.full(nw, -np.inf), ll, 600, seed=5)
+    s = ch[100:].reshape(-1, k)
+    assert np.all(np.abs(s.mean(0) - mu) < 0.5 * np.sqrt(np.diag(cov)))
+    assert np.all(np.abs(np.diag(np.cov(s.T)) / np.diag(cov) - 1) < 0.35)
+    assert 0.2 < nacc.sum() / (600 * nw) < 0.9
