@@ -550,6 +550,10 @@ void Ensemble::do_steps(unsigned nsteps, bool record) {
   }
   ck(cudaStreamSynchronize(stream_), "synchronize");
   check_error();
+  const unsigned long long ev = static_cast<unsigned long long>(nsteps) * nw_;
+  stats_[0] += ev;  // every proposal is evaluated exactly
+  stats_[1] += ev;
+  stats_[2] += ev;
 }
 
 void Ensemble::drop_graph() {

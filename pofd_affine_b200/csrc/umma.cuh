@@ -177,6 +177,7 @@ __device__ __forceinline__ uint32_t mainloop(const GemmShape& g, int m0, uint8_t
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  __syncwarp();
   if (threadIdx.x < 32) tmem_alloc(tslot, ncols);
   tc_fence_before();
   __syncthreads();
@@ -223,6 +224,7 @@ __device__ __forceinline__ void release(uint32_t* tslot, int ncols) {
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  __syncwarp();
   if (threadIdx.x < 32) tmem_dealloc(*tslot, static_cast<uint32_t>(ncols));
 }
 

@@ -153,6 +153,32 @@ class affineEnsemble:
     def clearChain(self):
         check(lib().pofd_ensemble_clear_chain(self.h))
 
+    # ------------------------------------------------ delayed acceptance
+    def setSurrogate(self, sur):
+        """First stage of delayed acceptance: a Surrogate."""
+        fn = C.cast(lib().pofd_surrogate_predict_device, C.c_void_p)
+        check(lib().pofd_ensemble_set_surrogate(self.h, fn, sur.h))
+        self.sur = sur
+
+    def collectPairs(self, sur):
+        """Append every exact evaluation to sur's training pairs (None
+        stops)."""
+        check(lib().pofd_ensemble_collect_pairs(self.h,
+                                                sur.h if sur else None))
+        self.collector = sur
+
+    def doStepsDA(self, nsteps, record=True):
+        check(lib().pofd_ensemble_do_steps_da(self.h, int(nsteps),
+                                              1 if record else 0))
+        self.nsteps_done += int(nsteps)
+
+    def daStats(self):
+        """{proposals, stage1_passes, exact_evals, accepted} since init."""
+        o = (C.c_ulonglong * 4)()
+        check(lib().pofd_ensemble_da_stats(self.h, o))
+        return dict(zip(["proposals", "stage1_passes", "exact_evals",
+                         "accepted"], [int(v) for v in o]))
+
     # ---------------------------------------------------------- results
     def nRecorded(self):
         n = C.c_uint()

@@ -1,0 +1,133 @@
+"""The tensor-core surrogate: the tcgen05 GEMM against float64 products of
+the same bf16 operands, the network's forward pass and loss gradients
+against the CPU oracle, training on a known log-density, and the
+delayed-acceptance stretch move (exact posterior, fewer exact evaluations
+per accepted move than the plain method)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_round(a):
+    import mlp_oracle
+    return mlp_oracle.bf16(a)
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 16, 16), (128, 256, 64),
+                                   (300, 192, 80), (256, 384, 256),
+                                   (77, 512, 32), (1024, 256, 1024)])
+def test_bf16_gemm_matches_float64(gpu_ctx, M, N, K):
+    import torch
+    from pofd_affine_b200.surrogate import bf16_gemm
+    rng = np.random.default_rng(M + N + K)
+    a = rng.normal(size=(M, K)).astype(np.float32)
+    b = rng.normal(size=(N, K)).astype(np.float32)
+    A = torch.from_numpy(a).cuda().to(torch.bfloat16).contiguous()
+    B = torch.from_numpy(b).cuda().to(torch.bfloat16).contiguous()
+    Cg = bf16_gemm(A, B).cpu().numpy().astype(np.float64)
+    ref = _bf16_round(a) @ _bf16_round(b).T
+    err = np.max(np.abs(Cg - ref)) / np.max(np.abs(ref))
+    assert err < 1e-5, err
+
+
+def _gauss_pairs(n, k, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(k, k))
+    cov = A @ A.T + k * np.eye(k)
+    mu = rng.normal(size=k)
+    th = (mu + rng.multivariate_normal(np.zeros(k), 2.0 * cov, size=n)).astype(np.float32)
+    d = th.astype(np.float64) - mu
+    ll = -0.5 * np.einsum("ij,jk,ik->i", d, np.linalg.inv(cov), d)
+    return th, ll, mu, cov
+
+
+def test_forward_and_gradients_match_oracle(gpu_ctx):
+    import mlp_oracle
+    from pofd_affine_b200.surrogate import Surrogate
+    k, H, n = 5, 128, 384
+    th, ll, _, _ = _gauss_pairs(n, k, 1)
+    npar = k + 1
+    thp = np.concatenate([th, np.ones((n, 1), np.float32)], 1)
+    S = Surrogate(gpu_ctx, npar, list(range(k)), hidden=H, capacity=4096, seed=3)
+    S.addPairs(thp, ll)
+    assert S.nPairs() == n
+    g, loss = S.gradients(n)  # also fixes the scaling from the pairs
+    sc = S.scaling()
+    params = [p.astype(np.float64) for p in S.getParams()]
+    x = mlp_oracle.standardise(thp, list(range(k)), sc["mu"], sc["isd"])
+    t = ((ll - sc["ymax"]) / sc["ys"]).astype(np.float32).astype(np.float64)
+    og, oloss = mlp_oracle.gradients(params, H, x, t)
+    assert abs(loss - oloss) <= 1e-3 * oloss
+    for name, a, b in zip(["W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4"], g, og):
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        assert rel < 2e-2, (name, rel)
+    # forward: predictions in logL units
+    y, _ = mlp_oracle.forward(params, H, x)
+    pred = S.predict(thp)
+    assert np.max(np.abs(pred - (sc["ymax"] + sc["ys"] * y))) < 2e-3 * sc["ys"]
+
+
+def test_training_fits_a_log_density(gpu_ctx):
+    from pofd_affine_b200.surrogate import Surrogate
+    k = 6
+    th, ll, _, _ = _gauss_pairs(12000, k, 2)
+    thp = np.concatenate([th, np.ones((len(th), 1), np.float32)], 1)
+    S = Surrogate(gpu_ctx, k + 1, list(range(k)), hidden=256, seed=5)
+    S.addPairs(thp[:10000], ll[:10000])
+    before = S.rms(thp[10000:], ll[10000:])
+    S.train(1500, batch=512, lr=1e-3)
+    after = S.rms(thp[10000:], ll[10000:])
+    assert after < 0.1 * before, (before, after)
+    assert after < 0.05 * np.std(ll), (after, np.std(ll))
+
+
+def test_delayed_acceptance_exact_posterior_and_gain(gpu_ctx):
+    """DA keeps the exact posterior (means within 0.1 sigma of the plain
+    run and of the truth) and accepts far more of its exact evaluations."""
+    from pofd_affine_b200.mcmc import affineEnsemble, gaussLike
+    from pofd_affine_b200.surrogate import Surrogate
+    k, nw = 6, 64
+    _, _, mu, cov = _gauss_pairs(10, k, 7)
+    G = gaussLike(gpu_ctx, mu, cov)
+    sd = np.sqrt(np.diag(cov))
+
+    def run(da):
+        E = affineEnsemble(gpu_ctx, G, nw, k, seed=11 + da)
+        E.initChains(E.generateInitialPosition(mu, sd, rng=3))
+        S = None
+        if da:
+            S = Surrogate(gpu_ctx, k, list(range(k)), hidden=256, seed=2)
+            E.collectPairs(S)
+        E.doSteps(0, initsteps=300)  # burn-in, exact pairs collected
+        if da:
+            S.train(2000, batch=512, lr=1e-3)
+            E.collectPairs(None)
+            E.setSurrogate(S)
+            base = E.daStats()
+            E.doStepsDA(3000)
+            st = E.daStats()
+            st = {key: st[key] - base[key] for key in st}
+        else:
+            base = E.daStats()
+            E.doSteps(3000)
+            st = E.daStats()
+            st = {key: st[key] - base[key] for key in st}
+        ch, _ = E.getChain()
+        tau, ok = E.getAcor()
+        return ch.reshape(-1, k).astype(np.float64), st, tau
+
+    sp, stp, taup = run(False)
+    sd_, std_, taud = run(True)
+    for s in (sp, sd_):
+        assert np.all(np.abs(s.mean(0) - mu) < 0.1 * sd)
+    assert np.all(np.abs(sd_.mean(0) - sp.mean(0)) < 0.1 * sd)
+    assert np.all(np.abs(sd_.std(0) / sp.std(0) - 1) < 0.1)
+    acc_plain = stp["accepted"] / stp["exact_evals"]
+    acc_da = std_["accepted"] / std_["exact_evals"]
+    print("DA stats plain", stp, "da", std_, "tau", taup, taud)
+    assert acc_da > 1.5 * acc_plain, (acc_plain, acc_da, std_)
+    # effective samples per exact evaluation
+    ess_p = nw * 3000 / np.nanmax(taup) / stp["exact_evals"]
+    ess_d = nw * 3000 / np.nanmax(taud) / std_["exact_evals"]
+    assert ess_d > ess_p, (ess_p, ess_d)
