@@ -13,7 +13,10 @@ batch (weak scaling, no data-path collective).
     python bench.py [--gpus N] [--steps K] [--warmup W]
     python bench.py --impl reference ...   # the CPU path on host cores
 
-Prints one JSON line (rank 0).
+Prints one JSON line (rank 0).  At N = 1 the line also carries, under
+"workloads" and "mcmc", the 2D plain workload (n = 2048, 64 proposals per
+launch) and the plain vs delayed-acceptance MCMC comparisons (effective
+samples per second) on the 1D and the two-field 2D fits.
 """
 import argparse
 import json
@@ -45,6 +48,10 @@ def args():
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="CPU-baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-2d", action="store_true")
+    p.add_argument("--no-mcmc", action="store_true")
+    p.add_argument("--mcmc-2d", type=int, default=1,
+                   help="include the two-field 2D MCMC comparison")
     return p.parse_args()
 
 
@@ -207,6 +214,168 @@ def read_traffic(stage):
     return None
 
 
+# ------------------------------------------------------------ 2D workload
+BATCH_2D = 64
+
+
+def cpu_baseline_2d(cfg, seconds, nthreads=None):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from pofd_affine_b200 import synth
+    nthreads = nthreads or os.cpu_count() or 1
+    O = pyoracle.Like2(cfg["knotpos"], cfg["sigmapos"], cfg["offsetpos"],
+                       cfg["fftsize"], cfg["nedge"], True, cfg["nbins"])
+    O.add_beamset(cfg["beam1"], cfg["beam2"], cfg["pixsize"], cfg["minval"],
+                  True, cfg["nbeamhist"])
+    for (m1, m2), (s1, s2) in zip(cfg["maps"], cfg["sigmas"]):
+        O.add_dataset(0, m1, m2, s1, s2)
+    O.set_rranges(cfg["theta0"])
+    th = synth.proposals(cfg["theta0"], nthreads, 0.02, rng=98,
+                         fixed_last=False)
+    th[:, -2:] = 1.0
+    done, t0 = 0, time.perf_counter()
+    while True:
+        O.loglike_batch(th, nthreads)
+        done += th.shape[0]
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": done / el, "unit": "evals/s", "cores": nthreads,
+            "kind": "port",
+            "sample": "%d proposals of the 2D workload in %.1f s on %d "
+                      "threads (oracle restatement of the reference CPU path)"
+                      % (done, el, nthreads)}
+
+
+def measure_2d(a, ctx, stream):
+    import torch
+    from pofd_affine_b200 import synth
+    cfg = synth.config_2d()
+    L = synth.build_like2(cfg, ctx)
+    L.reserve(BATCH_2D)
+    npar = cfg["theta0"].size
+    host = []
+    for k in range(2):
+        t = synth.proposals(cfg["theta0"], BATCH_2D, 0.02, rng=300 + k,
+                            fixed_last=False)
+        t[:, -2:] = 1.0
+        host.append(t)
+    dth = [torch.from_numpy(h).cuda() for h in host]
+    dll = torch.empty(BATCH_2D, dtype=torch.float64, device="cuda")
+    dst = torch.empty(BATCH_2D, dtype=torch.int32, device="cuda")
+    sptr = stream.cuda_stream
+    ref, st = L.getLogLikeBatch(host[0])
+    assert np.all(st == 0), st
+    steps = max(3, a.steps // 50)
+    for k in range(max(a.warmup, 3)):
+        L.getLogLikeDevice(BATCH_2D, dth[k % 2].data_ptr(), npar,
+                           dll.data_ptr(), dst.data_ptr(), sptr)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(steps):
+        L.getLogLikeDevice(BATCH_2D, dth[k % 2].data_ptr(), npar,
+                           dll.data_ptr(), dst.data_ptr(), sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t0 = time.perf_counter()
+    for k in range(steps):
+        L.getLogLikeBatch(host[k % 2])
+    e2e_s = time.perf_counter() - t0
+    stages = L.profileStages(host[0], reps=3)
+    out = {"workload": "2D plain method: 8-knot counts 2-500 mJy, log-normal "
+                       "colour (3 sigma + 3 offset knots), FWHM 3.0/4.2 px "
+                       "beams in 100-bin 2D histograms, 1500x1500 map pair, "
+                       "500x500 data bins, n=2048, nedge=256, 64 proposals "
+                       "per launch",
+           "value": BATCH_2D * steps / (ms * 1e-3), "unit": "evals/s",
+           "steps": steps, "ms_per_step": ms / steps,
+           "e2e": {"value": BATCH_2D * steps / e2e_s, "unit": "evals/s",
+                   "h2d_bytes_per_step": BATCH_2D * npar * 4,
+                   "d2h_bytes_per_step": BATCH_2D * 12},
+           "stage_ms": stages, "gpu_launches": L.kernelsPerEval() * steps}
+    if not a.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_2d(cfg, a.cpu_seconds)
+    return out
+
+
+# ---------------------------------------------------------------- MCMC
+def mcmc_1d(ctx):
+    """Plain vs delayed-acceptance stretch move on the 1D plain fit (6
+    knots, n = 4096, 40 walkers, fixed burn 200, 500 recorded steps)."""
+    from pofd_affine_b200 import runner, synth
+    from pofd_affine_b200.mcmc import affineEnsemble
+    from pofd_affine_b200.surrogate import Surrogate
+    cfg = synth.config_1d_small(seed=1)
+    L = synth.build_like1(cfg, ctx)
+    npar = cfg["theta0"].size
+    nk = npar - 1
+
+    def ens(seed):
+        E = affineEnsemble(ctx, L, 40, npar, seed=seed)
+        E.setParamFixed(nk)
+        E.initChains(E.generateInitialPosition(cfg["theta0"], 0.05, rng=seed))
+        return E
+    plain = runner.run_plain(ens(21), 200, 500)
+    ch = plain["chain"].reshape(-1, npar)
+    rng = np.random.default_rng(0)
+    pick = rng.choice(ch.shape[0], 2000, replace=False)
+    hold = (ch[pick], plain["logl"].reshape(-1)[pick])
+    S = Surrogate(ctx, npar, list(range(nk)), hidden=256, seed=7)
+    da = runner.run_da(ens(22), S, 200, 500, holdout=hold)
+    return _mcmc_summary("1D plain fit: 6 knots 2-400 mJy, n=4096, one "
+                         "256x256 map, 40 walkers, burn 200, 500 steps; MLP "
+                         "6 -> 3x256 SiLU -> 1", plain, da, list(range(nk)))
+
+
+def mcmc_2d(ctx):
+    """Plain vs delayed acceptance on the two-field 2D fit (2048^2 and
+    1024^2 grids in one launch, 14 free parameters, 128 walkers)."""
+    from pofd_affine_b200 import runner, synth
+    from pofd_affine_b200.mcmc import affineEnsemble, likeSum
+    from pofd_affine_b200.surrogate import Surrogate
+    a, b = synth.config_2d_two_fields()
+    La, Lb = synth.build_like2(a, ctx), synth.build_like2(b, ctx)
+    S2 = likeSum(ctx, [La, Lb])
+    npar = a["theta0"].size
+    nfree = npar - 2
+
+    def ens(seed):
+        E = affineEnsemble(ctx, S2, 128, npar, seed=seed)
+        E.setParamFixed(npar - 2)
+        E.setParamFixed(npar - 1)
+        sig = np.r_[np.full(8, 0.03), np.full(6, 0.01), 0, 0]
+        E.initChains(E.generateInitialPosition(a["theta0"], sig, rng=seed))
+        return E
+    plain = runner.run_plain(ens(31), 150, 300)
+    ch = plain["chain"].reshape(-1, npar)
+    rng = np.random.default_rng(1)
+    pick = rng.choice(ch.shape[0], 2000, replace=False)
+    hold = (ch[pick], plain["logl"].reshape(-1)[pick])
+    S = Surrogate(ctx, npar, list(range(nfree)), hidden=384, seed=9)
+    da = runner.run_da(ens(32), S, 150, 300, holdout=hold)
+    return _mcmc_summary("2D two-field fit: 1500x1500 pair on 2048^2 + "
+                         "800x600 pair on 1024^2 in one launch, 14 free "
+                         "parameters, 128 walkers, burn 150, 300 steps; MLP "
+                         "14 -> 3x384 SiLU -> 1", plain, da, list(range(nfree)))
+
+
+def _mcmc_summary(name, plain, da, free):
+    from pofd_affine_b200 import runner
+    keep = ("wall_s", "tau_max", "acor_ok", "ess", "ess_per_s", "stats")
+    return {"workload": name,
+            "plain": {k: plain[k] for k in keep},
+            "da": dict({k: da[k] for k in keep},
+                       train_s=da["train_s"], stage1_rate=da["stage1_rate"],
+                       stage2_rate=da["stage2_rate"],
+                       surrogate_rms=da.get("surrogate_rms")),
+            "ess_per_s_ratio": da["ess_per_s"] / plain["ess_per_s"],
+            "posterior_mean_shift_sigma": runner.posterior_agreement(da, plain,
+                                                                     free)}
+
+
 def main():
     a = args()
     from pofd_affine_b200 import synth
@@ -332,6 +501,15 @@ def main():
     hbm_pipe = sum(stage_bytes(s, BATCH, B, D, n) or 0 for s in stages)
     nk = L.kernelsPerEval()
 
+    extra = {}
+    if rank == 0 and world == 1:
+        if not a.no_2d:
+            extra["workloads"] = {"2d": measure_2d(a, ctx, stream)}
+        if not a.no_mcmc:
+            extra["mcmc"] = {"1d": mcmc_1d(ctx)}
+            if a.mcmc_2d:
+                extra["mcmc"]["2d_two_fields"] = mcmc_2d(ctx)
+
     if rank == 0:
         cpu = None
         if not a.no_cpu_baseline and world == 1:
@@ -356,6 +534,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -416,6 +416,23 @@ int pofd_ensemble_do_steps_da(pofd_ensemble* e, unsigned nsteps, int record);
  * evaluations (padding included), [3] accepted moves. */
 int pofd_ensemble_da_stats(pofd_ensemble* e, unsigned long long* out4);
 
+/* Sum of batched likelihoods over the same proposals: fields fitted jointly
+ * with different FFT sizes (the reference's calcLikeDouble takes one
+ * fftsize for all beam sets, calcLikeDouble.h:241), evaluated concurrently
+ * on forked streams and summed; statuses combine as the first failure.
+ * pofd_likesum_eval_batch_device has the pofd_batch_loglike_fn signature.
+ * No counterpart in the reference. */
+typedef struct pofd_likesum pofd_likesum;
+int pofd_likesum_create(pofd_ctx* ctx, pofd_likesum** out);
+int pofd_likesum_destroy(pofd_likesum* ls);
+int pofd_likesum_add(pofd_likesum* ls, pofd_batch_loglike_fn fn, void* like);
+int pofd_likesum_add_like1(pofd_likesum* ls, pofd_like1* like);
+int pofd_likesum_add_like2(pofd_likesum* ls, pofd_like2* like);
+int pofd_likesum_eval_batch_device(void* ls, unsigned nprop,
+                                   const float* theta_dev, unsigned npar,
+                                   double* logl_dev, int* status_dev,
+                                   void* stream);
+
 /* Goodman's acor on one series x[n] (affineChainSet.cc:884-951); returns
  * POFD_REJECTED when n < 50 (mean only). */
 int pofd_acor(const float* x, size_t n, double* mean, double* sigma,

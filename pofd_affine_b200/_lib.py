@@ -113,6 +113,12 @@ SIGNATURES = {
     "pofd_ensemble_collect_pairs": (I, [V, V]),
     "pofd_ensemble_do_steps_da": (I, [V, U, I]),
     "pofd_ensemble_da_stats": (I, [V, C.POINTER(C.c_ulonglong)]),
+    "pofd_likesum_create": (I, [V, PV]),
+    "pofd_likesum_destroy": (I, [V]),
+    "pofd_likesum_add": (I, [V, V, V]),
+    "pofd_likesum_add_like1": (I, [V, V]),
+    "pofd_likesum_add_like2": (I, [V, V]),
+    "pofd_likesum_eval_batch_device": (I, [V, U, V, U, V, V, V]),
     "pofd_acor": (I, [_fp, S, C.POINTER(D), C.POINTER(D), C.POINTER(D)]),
 }
 

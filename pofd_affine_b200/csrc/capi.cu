@@ -75,6 +75,11 @@ struct pofd_surrogate {
   std::unique_ptr<pofd::Surrogate> s;
 };
 
+struct pofd_likesum {
+  pofd_ctx* ctx = nullptr;
+  std::unique_ptr<pofd::LikeSum> ls;
+};
+
 struct pofd_ensemble {
   pofd_ctx* ctx = nullptr;
   std::unique_ptr<pofd::Ensemble> ens;
@@ -979,6 +984,57 @@ int pofd_ensemble_da_stats(pofd_ensemble* e, unsigned long long* out4) {
   return guard([&] {
     need(e && out4, "null argument");
     e->ens->da_stats(out4);
+    return POFD_OK;
+  });
+}
+
+int pofd_likesum_create(pofd_ctx* ctx, pofd_likesum** out) {
+  return guard([&] {
+    need(ctx && out, "null argument");
+    std::unique_ptr<pofd_likesum> l(new pofd_likesum());
+    l->ctx = ctx;
+    l->ls.reset(new pofd::LikeSum(ctx->device, ctx->stream));
+    *out = l.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_likesum_destroy(pofd_likesum* ls) {
+  if (ls && ls->ctx && ls->ctx->device >= 0) cudaSetDevice(ls->ctx->device);
+  delete ls;
+  return POFD_OK;
+}
+
+int pofd_likesum_add(pofd_likesum* ls, pofd_batch_loglike_fn fn, void* like) {
+  return guard([&] {
+    need(ls && fn, "null argument");
+    ls->ls->add(fn, like);
+    return POFD_OK;
+  });
+}
+
+int pofd_likesum_add_like1(pofd_likesum* ls, pofd_like1* like) {
+  return guard([&] {
+    need(ls && like, "null argument");
+    ls->ls->add(like1_batch, like);
+    return POFD_OK;
+  });
+}
+
+int pofd_likesum_add_like2(pofd_likesum* ls, pofd_like2* like) {
+  return guard([&] {
+    need(ls && like, "null argument");
+    ls->ls->add(like2_batch, like);
+    return POFD_OK;
+  });
+}
+
+int pofd_likesum_eval_batch_device(void* lv, unsigned nprop, const float* theta, unsigned npar,
+                                   double* logl, int* status, void* stream) {
+  return guard([&] {
+    pofd_likesum* ls = static_cast<pofd_likesum*>(lv);
+    need(ls && theta && logl && status, "null argument");
+    ls->ls->enqueue(nprop, theta, npar, logl, status, static_cast<cudaStream_t>(stream));
     return POFD_OK;
   });
 }

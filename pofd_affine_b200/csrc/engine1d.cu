@@ -819,8 +819,8 @@ Engine1::~Engine1() {
   cudaSetDevice(device_);
   drop_graphs();
   for (auto& kv : plans_) {
-    if (kv.second.fwd) cufftDestroy(kv.second.fwd);
-    if (kv.second.inv) cufftDestroy(kv.second.inv);
+    if (kv.second.fwd) { fftwork_.forget(kv.second.fwd); cufftDestroy(kv.second.fwd); }
+    if (kv.second.inv) { fftwork_.forget(kv.second.inv); cufftDestroy(kv.second.inv); }
   }
   free_work();
   free_static();
@@ -1165,8 +1165,8 @@ void Engine1::build_static() {
   // shapes changed: old plans/graphs/work space no longer match
   drop_graphs();
   for (auto& kv : plans_) {
-    if (kv.second.fwd) cufftDestroy(kv.second.fwd);
-    if (kv.second.inv) cufftDestroy(kv.second.inv);
+    if (kv.second.fwd) { fftwork_.forget(kv.second.fwd); cufftDestroy(kv.second.fwd); }
+    if (kv.second.inv) { fftwork_.forget(kv.second.inv); cufftDestroy(kv.second.inv); }
   }
   plans_.clear();
   const unsigned P = ws_.P;
@@ -1270,13 +1270,12 @@ void Engine1::ensure_plans(unsigned nprop) {
   int n = static_cast<int>(n_);
   const int nc = n / 2 + 1;
   int inemb[1] = {2 * nc}, onemb[1] = {nc};
-  cufft_check(cufftPlanMany(&pl.fwd, 1, &n, inemb, 1, 2 * nc, onemb, 1, nc,
-                            CUFFT_D2Z, static_cast<int>(nprop * B_)),
-              "cufftPlanMany D2Z");
+  bool grew = fftwork_.make(&pl.fwd, 1, &n, inemb, 2 * nc, onemb, nc, CUFFT_D2Z,
+                            static_cast<int>(nprop * B_));
   int inemb2[1] = {nc}, onemb2[1] = {2 * nc};
-  cufft_check(cufftPlanMany(&pl.inv, 1, &n, inemb2, 1, nc, onemb2, 1, 2 * nc,
-                            CUFFT_Z2D, static_cast<int>(nprop * D_)),
-              "cufftPlanMany Z2D");
+  grew |= fftwork_.make(&pl.inv, 1, &n, inemb2, nc, onemb2, 2 * nc, CUFFT_Z2D,
+                        static_cast<int>(nprop * D_));
+  if (grew) drop_graphs();  // captured transforms used the old work area
   plans_[nprop] = pl;
 }
 

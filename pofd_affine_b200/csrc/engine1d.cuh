@@ -18,6 +18,7 @@
 #include <memory>
 #include <vector>
 
+#include "fftplan.hh"
 #include "setup.hh"
 
 namespace pofd {
@@ -204,6 +205,7 @@ class Engine1 {
                             double* logl, int* status);
   void drop_graphs();
   std::map<unsigned, Plans> plans_;
+  FftWorkArea fftwork_;
 };
 
 }  // namespace pofd

@@ -991,8 +991,8 @@ Engine2::~Engine2() {
   cudaSetDevice(device_);
   drop_graphs();
   for (auto& kv : plans_) {
-    if (kv.second.fwd) cufftDestroy(kv.second.fwd);
-    if (kv.second.inv) cufftDestroy(kv.second.inv);
+    if (kv.second.fwd) { fftwork_.forget(kv.second.fwd); cufftDestroy(kv.second.fwd); }
+    if (kv.second.inv) { fftwork_.forget(kv.second.inv); cufftDestroy(kv.second.inv); }
   }
   free_work();
   free_static();
@@ -1314,8 +1314,8 @@ void Engine2::build_static() {
   static_ok_ = true;
   drop_graphs();
   for (auto& kv : plans_) {
-    if (kv.second.fwd) cufftDestroy(kv.second.fwd);
-    if (kv.second.inv) cufftDestroy(kv.second.inv);
+    if (kv.second.fwd) { fftwork_.forget(kv.second.fwd); cufftDestroy(kv.second.fwd); }
+    if (kv.second.inv) { fftwork_.forget(kv.second.inv); cufftDestroy(kv.second.inv); }
   }
   plans_.clear();
   const unsigned P = ws_.P;
@@ -1387,11 +1387,12 @@ void Engine2::ensure_plans(unsigned nprop) {
   int nn[2] = {static_cast<int>(n_), static_cast<int>(n_)};
   const int nc = static_cast<int>(n_) / 2 + 1;
   int inemb[2] = {nn[0], 2 * nc}, onemb[2] = {nn[0], nc};
-  fk(cufftPlanMany(&pl.fwd, 2, nn, inemb, 1, nn[0] * 2 * nc, onemb, 1, nn[0] * nc,
-                   CUFFT_D2Z, static_cast<int>(nprop * B_)), "cufftPlanMany 2D D2Z");
+  bool grew = fftwork_.make(&pl.fwd, 2, nn, inemb, nn[0] * 2 * nc, onemb, nn[0] * nc,
+                            CUFFT_D2Z, static_cast<int>(nprop * B_));
   int inemb2[2] = {nn[0], nc}, onemb2[2] = {nn[0], 2 * nc};
-  fk(cufftPlanMany(&pl.inv, 2, nn, inemb2, 1, nn[0] * nc, onemb2, 1, nn[0] * 2 * nc,
-                   CUFFT_Z2D, static_cast<int>(nprop * D_)), "cufftPlanMany 2D Z2D");
+  grew |= fftwork_.make(&pl.inv, 2, nn, inemb2, nn[0] * nc, onemb2, nn[0] * 2 * nc, CUFFT_Z2D,
+                        static_cast<int>(nprop * D_));
+  if (grew) drop_graphs();  // captured transforms used the old work area
   plans_[nprop] = pl;
 }
 

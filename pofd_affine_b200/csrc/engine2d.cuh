@@ -18,6 +18,7 @@
 #include <map>
 #include <vector>
 
+#include "fftplan.hh"
 #include "setup.hh"
 
 namespace pofd {
@@ -167,6 +168,7 @@ class Engine2 {
   unsigned nrt_ = 0, nct_ = 0;    // P(D) row / column tiles
   unsigned gchunks_ = 1;          // gather chunks per dataset
   std::map<unsigned, Plans> plans_;
+  FftWorkArea fftwork_;
   struct Work {
     unsigned P = 0;
     double* cnt = nullptr;      // [P][12*KMAX]

@@ -568,13 +568,15 @@ void Ensemble::set_stage1(pofd_batch_loglike_fn fn, void* sur) {
   sur_ = sur;
 }
 
-// Survivor batches are rounded up so that the likelihood sees few distinct
-// batch sizes (each has its own FFT plans and graphs): multiples of 8 up
-// to 64, of 16 up to 256, then of 64.
+// Survivor batches are rounded up so that the likelihood sees a bounded
+// number of batch sizes (each has its own FFT plans and graphs; the plans
+// share one work area): multiples of 2 up to 32, of 4 up to 64, of 8 up to
+// 256, then of 32.
 unsigned Ensemble::bucket(unsigned n) {
-  if (n <= 64) return (n + 7) / 8 * 8;
-  if (n <= 256) return (n + 15) / 16 * 16;
-  return (n + 63) / 64 * 64;
+  if (n <= 32) return (n + 1) / 2 * 2;
+  if (n <= 64) return (n + 3) / 4 * 4;
+  if (n <= 256) return (n + 7) / 8 * 8;
+  return (n + 31) / 32 * 32;
 }
 
 void Ensemble::da_half(int half, double zexp, double invt) {
@@ -801,6 +803,95 @@ void GaussLike::enqueue(unsigned nprop, const float* theta, unsigned npar, doubl
   if (nprop == 0) return;
   k_gauss<<<(nprop + 127) / 128, 128, 0, st>>>(nprop, npar, k_, mean_, icov_, theta, logl, status);
   ck(cudaGetLastError(), "k_gauss");
+}
+
+// ------------------------------------------------------------ LikeSum
+namespace {
+__global__ void k_lsum(unsigned nprop, unsigned k, unsigned cap, const double* __restrict__ l,
+                       const int* __restrict__ s, double* __restrict__ logl,
+                       int* __restrict__ status) {
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nprop) return;
+  double acc = 0.0;
+  int st = POFD_OK;
+  for (unsigned m = 0; m < k; ++m) {
+    const int sm = s[static_cast<size_t>(m) * cap + t];
+    if (st == POFD_OK && sm != POFD_OK) st = sm;
+    acc += l[static_cast<size_t>(m) * cap + t];
+  }
+  logl[t] = acc;
+  status[t] = st;
+}
+}  // namespace
+
+LikeSum::LikeSum(int device, cudaStream_t stream) : device_(device), stream_(stream) {
+  if (device < 0) throw Error(POFD_E_CUDA, "host-only context has no GPU");
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  ck(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "event");
+}
+
+LikeSum::~LikeSum() {
+  cudaSetDevice(device_);
+  for (auto e : done_) cudaEventDestroy(e);
+  for (auto st : streams_) cudaStreamDestroy(st);
+  if (fork_) cudaEventDestroy(fork_);
+  if (l_) cudaFree(l_);
+  if (s_) cudaFree(s_);
+}
+
+void LikeSum::add(pofd_batch_loglike_fn fn, void* like) {
+  if (!fn) throw Error(POFD_E_ARG, "null likelihood");
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  cudaStream_t st;
+  ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+  cudaEvent_t ev;
+  ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+  fn_.push_back(fn);
+  like_.push_back(like);
+  streams_.push_back(st);
+  done_.push_back(ev);
+  if (l_) cudaFree(l_);
+  if (s_) cudaFree(s_);
+  l_ = nullptr;
+  s_ = nullptr;
+  cap_ = 0;
+}
+
+void LikeSum::ensure(unsigned nprop) {
+  if (nprop <= cap_) return;
+  if (l_) cudaFree(l_);
+  if (s_) cudaFree(s_);
+  const size_t k = fn_.size();
+  l_ = dal<double>(k * nprop);
+  s_ = dal<int>(k * nprop);
+  cap_ = nprop;
+}
+
+void LikeSum::enqueue(unsigned nprop, const float* theta, unsigned npar, double* logl,
+                      int* status, cudaStream_t st) {
+  if (fn_.empty()) throw Error(POFD_E_ARG, "empty likelihood sum");
+  if (nprop == 0) return;
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  if (!st) st = stream_;
+  if (nprop > cap_) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    ck(cudaStreamIsCapturing(st, &cs), "cudaStreamIsCapturing");
+    if (cs != cudaStreamCaptureStatusNone)
+      throw Error(POFD_E_ARG, "likelihood sum must run once at this batch size before capture");
+    ck(cudaStreamSynchronize(st), "synchronize");
+    ensure(nprop);
+  }
+  ck(cudaEventRecord(fork_, st), "event record");
+  for (size_t m = 0; m < fn_.size(); ++m) {
+    ck(cudaStreamWaitEvent(streams_[m], fork_, 0), "stream wait");
+    const int rc = fn_[m](like_[m], nprop, theta, npar, l_ + m * cap_, s_ + m * cap_, streams_[m]);
+    if (rc < 0) throw Error(rc, "member likelihood failed");
+    ck(cudaEventRecord(done_[m], streams_[m]), "event record");
+    ck(cudaStreamWaitEvent(st, done_[m], 0), "stream wait");
+  }
+  k_lsum<<<(nprop + 127) / 128, 128, 0, st>>>(nprop, static_cast<unsigned>(fn_.size()), cap_, l_,
+                                             s_, logl, status);
+  ck(cudaGetLastError(), "k_lsum");
 }
 
 }  // namespace pofd

@@ -131,6 +131,33 @@ class GaussLike {
   double* icov_ = nullptr;
 };
 
+// Sum of several batched likelihoods on the same proposals (fields of
+// different FFT sizes fitted jointly): the members run concurrently on
+// forked streams and join into one sum, so a captured step holds all of
+// them in one graph.
+class LikeSum {
+ public:
+  LikeSum(int device, cudaStream_t stream);
+  ~LikeSum();
+  void add(pofd_batch_loglike_fn fn, void* like);
+  void enqueue(unsigned nprop, const float* theta, unsigned npar, double* logl, int* status,
+               cudaStream_t st);
+  size_t size() const { return fn_.size(); }
+
+ private:
+  void ensure(unsigned nprop);
+  int device_;
+  cudaStream_t stream_;
+  std::vector<pofd_batch_loglike_fn> fn_;
+  std::vector<void*> like_;
+  std::vector<cudaStream_t> streams_;
+  std::vector<cudaEvent_t> done_;
+  cudaEvent_t fork_ = nullptr;
+  unsigned cap_ = 0;
+  double* l_ = nullptr;     // [members][cap]
+  int* s_ = nullptr;        // [members][cap]
+};
+
 // Goodman's acor on a series (destroyed); returns 1 when the series is
 // shorter than minfac * maxlag (no estimate), else 0.
 int acor_series(double& mean, double& sigma, double& tau, std::vector<float>& x,

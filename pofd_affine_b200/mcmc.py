@@ -45,6 +45,37 @@ class gaussLike:
             self.h = None
 
 
+class likeSum:
+    """Sum of likelihoods (calcLike / calcLikeDouble / gaussLike) over the
+    same parameters, members evaluated concurrently."""
+
+    def __init__(self, ctx, likes=()):
+        h = C.c_void_p()
+        check(lib().pofd_likesum_create(ctx.h, C.byref(h)))
+        self.h, self.ctx, self.members = h, ctx, []
+        for L in likes:
+            self.add(L)
+
+    def add(self, like):
+        from .api1d import calcLike
+        from .api2d import calcLikeDouble
+        if isinstance(like, calcLike):
+            check(lib().pofd_likesum_add_like1(self.h, like.h))
+        elif isinstance(like, calcLikeDouble):
+            check(lib().pofd_likesum_add_like2(self.h, like.h))
+        elif isinstance(like, gaussLike):
+            fn = C.cast(lib().pofd_gauss_eval_batch_device, C.c_void_p)
+            check(lib().pofd_likesum_add(self.h, fn, like.h))
+        else:
+            raise PofdError(-10, "unsupported likelihood object")
+        self.members.append(like)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pofd_likesum_destroy(self.h)
+            self.h = None
+
+
 class affineEnsemble:
     """Batched stretch-move ensemble (one process, one GPU)."""
 
@@ -67,6 +98,9 @@ class affineEnsemble:
             check(lib().pofd_ensemble_use_like2(h, like.h))
         elif isinstance(like, gaussLike):
             fn = C.cast(lib().pofd_gauss_eval_batch_device, C.c_void_p)
+            check(lib().pofd_ensemble_set_likelihood(h, fn, like.h))
+        elif isinstance(like, likeSum):
+            fn = C.cast(lib().pofd_likesum_eval_batch_device, C.c_void_p)
             check(lib().pofd_ensemble_set_likelihood(h, fn, like.h))
         else:
             raise PofdError(-10, "unsupported likelihood object")

@@ -211,3 +211,22 @@ def build_like2(cfg, ctx):
         L.addDataset(0, m1, m2, s1, s2)
     L.setRRanges(cfg["theta0"])
     return L
+
+
+def config_2d_two_fields(seed=5, scale=1.0):
+    """2D joint fit of two fields with different FFT sizes: the 2D plain
+    configuration's 1500x1500 pair on a 2048^2 grid plus an 800x600 pair
+    (same sources model, noise 2.5 / 2.8 mJy) on a 1024^2 grid; 14 model
+    parameters (8 knots, 3 sigma, 3 offset) plus two fixed sigma
+    multipliers."""
+    a = config_2d(seed=seed, scale=scale)
+    rng = np.random.default_rng(seed + 100)
+    sk, sv, ok, ov = a["sigmapos"], a["sigmavals"], a["offsetpos"], a["offsetvals"]
+    sig_fn = lambda f: np.interp(f, sk, sv)  # noqa: E731
+    off_fn = lambda f: np.interp(f, ok, ov)  # noqa: E731
+    sh = (max(32, int(800 * scale)), max(32, int(600 * scale)))
+    m1, m2 = make_map_pair(sh, 6.0, a["beam1"], a["beam2"], a["knotpos"],
+                           a["knotvals"], sig_fn, off_fn, 0.0025, 0.0028, rng)
+    b = dict(a)
+    b.update(maps=[(m1, m2)], fftsize=1024, nedge=128)
+    return a, b
