@@ -316,6 +316,8 @@ def mcmc_1d(ctx):
     def ens(seed):
         E = affineEnsemble(ctx, L, 40, npar, seed=seed)
         E.setParamFixed(nk)
+        for p in range(nk):  # knot limits of an initialisation file
+            E.setParamLimits(p, cfg["theta0"][p] - 2.0, cfg["theta0"][p] + 2.0)
         E.initChains(E.generateInitialPosition(cfg["theta0"], 0.05, rng=seed))
         return E
     plain = runner.run_plain(ens(21), 200, 500)
@@ -346,6 +348,13 @@ def mcmc_2d(ctx):
         E = affineEnsemble(ctx, S2, 128, npar, seed=seed)
         E.setParamFixed(npar - 2)
         E.setParamFixed(npar - 1)
+        for p in range(8):  # knot limits
+            E.setParamLimits(p, a["theta0"][p] - 2.0, a["theta0"][p] + 2.0)
+        for p in range(8, 11):  # colour sigma
+            E.setParamLimits(p, 0.02, 1.0)
+        for p in range(11, 14):  # colour offset
+            E.setParamLimits(p, -2.0, 1.0)
+        E.setErrorPolicy(True)  # unphysical corners reject instead of stop
         sig = np.r_[np.full(8, 0.03), np.full(6, 0.01), 0, 0]
         E.initChains(E.generateInitialPosition(a["theta0"], sig, rng=seed))
         return E
@@ -364,7 +373,8 @@ def mcmc_2d(ctx):
 
 def _mcmc_summary(name, plain, da, free):
     from pofd_affine_b200 import runner
-    keep = ("wall_s", "tau_max", "acor_ok", "ess", "ess_per_s", "stats")
+    keep = ("wall_s", "tau_max", "acor_ok", "ess", "ess_per_s", "stats",
+            "failures")
     return {"workload": name,
             "plain": {k: plain[k] for k in keep},
             "da": dict({k: da[k] for k in keep},

@@ -391,8 +391,9 @@ int pofd_surrogate_set_params(pofd_surrogate* s, const float* const* tensors);
  * update: grads[8] host buffers of the tensor sizes. */
 int pofd_surrogate_gradients(pofd_surrogate* s, unsigned n,
                              float* const* grads, float* loss);
-/* Input mean[16], 1/sd[16], then the target offset and scale (34 values). */
-int pofd_surrogate_scaling(pofd_surrogate* s, double* out34);
+/* Input mean[16], 1/sd[16], then the target offset (max logL), scale and
+ * floor: targets are max(logL - max, -floor) / scale (35 values). */
+int pofd_surrogate_scaling(pofd_surrogate* s, double* out35);
 /* The tensor-core main loop on its own, on device pointers of the current
  * device: C[M][N] (fp32, ldc) = A[M][K] * B[N][K]^T, A and B bf16 with
  * leading dimensions multiple of 8, N in [16, 512] and K >= 16 multiples of
@@ -412,6 +413,13 @@ int pofd_ensemble_set_surrogate(pofd_ensemble* e, pofd_batch_loglike_fn sfn,
  * surrogate's training pairs (NULL stops collecting). */
 int pofd_ensemble_collect_pairs(pofd_ensemble* e, pofd_surrogate* s);
 int pofd_ensemble_do_steps_da(pofd_ensemble* e, unsigned nsteps, int record);
+/* Failed likelihood evaluations (a P(D) split or unwrap error, a
+ * non-finite logL): reject_failures == 0 (default) stops the run with the
+ * error, as the reference's master does ("Problem encountered in slave",
+ * affineEnsemble.cc:1346-1352); != 0 rejects the step and counts it
+ * (pofd_ensemble_failures). */
+int pofd_ensemble_set_error_policy(pofd_ensemble* e, int reject_failures);
+int pofd_ensemble_failures(pofd_ensemble* e, unsigned long long* n);
 /* Counters since init: [0] proposals, [1] stage-one passes, [2] exact
  * evaluations (padding included), [3] accepted moves. */
 int pofd_ensemble_da_stats(pofd_ensemble* e, unsigned long long* out4);

@@ -119,6 +119,8 @@ SIGNATURES = {
     "pofd_likesum_add_like1": (I, [V, V]),
     "pofd_likesum_add_like2": (I, [V, V]),
     "pofd_likesum_eval_batch_device": (I, [V, U, V, U, V, V, V]),
+    "pofd_ensemble_set_error_policy": (I, [V, I]),
+    "pofd_ensemble_failures": (I, [V, C.POINTER(C.c_ulonglong)]),
     "pofd_acor": (I, [_fp, S, C.POINTER(D), C.POINTER(D), C.POINTER(D)]),
 }
 

@@ -1039,4 +1039,20 @@ int pofd_likesum_eval_batch_device(void* lv, unsigned nprop, const float* theta,
   });
 }
 
+int pofd_ensemble_set_error_policy(pofd_ensemble* e, int reject_failures) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->set_error_policy(reject_failures != 0);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_failures(pofd_ensemble* e, unsigned long long* n) {
+  return guard([&] {
+    need(e && n, "null argument");
+    *n = e->ens->failures();
+    return POFD_OK;
+  });
+}
+
 }  // extern "C"

@@ -138,7 +138,8 @@ __global__ void k_propose(int half, unsigned nw, unsigned np, double scalefac,
 // old step; otherwise accept with min(1, z^(nparams-nfixed-1) e^{dL/T}).
 // The second half also writes the step into the chain.
 __global__ void k_accept(int half, unsigned nw, unsigned np, double zexp,
-                         double invtemp, unsigned long long seed,
+                         double invtemp, unsigned long long seed, int reject_fail,
+                         unsigned long long* __restrict__ nfail,
                          const float* __restrict__ prop,
                          const float* __restrict__ zin,
                          const double* __restrict__ lnew,
@@ -158,10 +159,14 @@ __global__ void k_accept(int half, unsigned nw, unsigned np, double zexp,
     bool take = false;
     if (isnan(z) || s == POFD_REJECTED) {
       take = false;
-    } else if (s != POFD_OK) {
-      if (atomicCAS(err, 0, 2) == 0) { err[1] = static_cast<int>(i); err[2] = s; }
-    } else if (isinf(ln) || isnan(ln)) {
-      if (atomicCAS(err, 0, 3) == 0) err[1] = static_cast<int>(i);
+    } else if (s != POFD_OK || isinf(ln) || isnan(ln)) {
+      if (reject_fail) {
+        atomicAdd(nfail, 1ull);
+      } else if (s != POFD_OK) {
+        if (atomicCAS(err, 0, 2) == 0) { err[1] = static_cast<int>(i); err[2] = s; }
+      } else {
+        if (atomicCAS(err, 0, 3) == 0) err[1] = static_cast<int>(i);
+      }
     } else {
       const double prob = exp(zexp * log(static_cast<double>(z)) + invtemp * (ln - logl[i]));
       if (prob >= 1.0) {
@@ -259,7 +264,8 @@ __global__ void k_pad(int count, int b, unsigned np, float* __restrict__ exprop)
 
 // Stage two: min(1, e^{((L' - L) - (S' - S))/T}) on the exact values.
 __global__ void k_stage2(int half, unsigned nw, unsigned np, double invtemp,
-                         unsigned long long seed, int count, const int* __restrict__ exidx,
+                         unsigned long long seed, int reject_fail,
+                         unsigned long long* __restrict__ nfail, int count, const int* __restrict__ exidx,
                          const float* __restrict__ exprop, const double* __restrict__ exl,
                          const int* __restrict__ exs, const double* __restrict__ spred,
                          float* __restrict__ theta, double* __restrict__ logl,
@@ -273,12 +279,14 @@ __global__ void k_stage2(int half, unsigned nw, unsigned np, double invtemp,
   const int s = exs[q];
   const double ln = exl[q];
   if (s == POFD_REJECTED) return;
-  if (s != POFD_OK) {
-    if (atomicCAS(err, 0, 2) == 0) { err[1] = static_cast<int>(i); err[2] = s; }
-    return;
-  }
-  if (isinf(ln) || isnan(ln)) {
-    if (atomicCAS(err, 0, 3) == 0) err[1] = static_cast<int>(i);
+  if (s != POFD_OK || isinf(ln) || isnan(ln)) {
+    if (reject_fail) {
+      atomicAdd(nfail, 1ull);
+    } else if (s != POFD_OK) {
+      if (atomicCAS(err, 0, 2) == 0) { err[1] = static_cast<int>(i); err[2] = s; }
+    } else {
+      if (atomicCAS(err, 0, 3) == 0) err[1] = static_cast<int>(i);
+    }
     return;
   }
   const double a = exp(invtemp * ((ln - logl[i]) - (spred[t] - scur[i])));
@@ -354,6 +362,8 @@ Ensemble::Ensemble(int device, cudaStream_t stream, unsigned nwalkers,
   exs_ = dal<int>(nh);
   exidx_ = dal<int>(nh);
   dcount_ = dal<int>(1);
+  nfail_ = dal<unsigned long long>(1);
+  ck(cudaMemset(nfail_, 0, sizeof(unsigned long long)), "memset");
   ck(cudaMallocHost(&hcount_, sizeof(int)), "cudaMallocHost");
   ck(cudaMemset(ctr_, 0, 3 * sizeof(unsigned long long)), "memset");
   ck(cudaMemset(err_, 0, 4 * sizeof(int)), "memset");
@@ -365,7 +375,7 @@ Ensemble::~Ensemble() {
   if (graph_) cudaGraphExecDestroy(graph_);
   void* ptrs[] = {theta_, logl_, prop_, z_, lnew_, snew_, nacc_, pstate_, plo_,
                   phi_, ch_theta_, ch_logl_, ctr_, err_, spred_, sst_, scur_,
-                  exprop_, exl_, exs_, exidx_, dcount_};
+                  exprop_, exl_, exs_, exidx_, dcount_, nfail_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (hcount_) cudaFreeHost(hcount_);
@@ -417,6 +427,7 @@ void Ensemble::init(const float* walkers, const double* logl) {
   ck(cudaMemset(nacc_, 0, nw_ * sizeof(unsigned)), "memset");
   ck(cudaMemset(err_, 0, 4 * sizeof(int)), "memset");
   for (auto& v : stats_) v = 0;
+  ck(cudaMemset(nfail_, 0, sizeof(unsigned long long)), "memset");
   init_ = true;
 }
 
@@ -475,7 +486,8 @@ void Ensemble::launch_step(cudaStream_t st) {
     const int rc = fn_(like_, nh, prop_, np_, lnew_, snew_, st);
     if (rc < 0) throw Error(rc, "batched likelihood enqueue failed");
     if (collect_) collect_->add_pairs(nh, prop_, np_, lnew_, snew_, st);
-    k_accept<<<g, ENT, 0, st>>>(half, nw_, np_, zexp, invt, seed_, prop_, z_, lnew_, snew_,
+    k_accept<<<g, ENT, 0, st>>>(half, nw_, np_, zexp, invt, seed_, reject_fail_ ? 1 : 0,
+                                nfail_, prop_, z_, lnew_, snew_,
                                 theta_, logl_, nacc_, ctr_, err_, ch_theta_, ch_logl_, cap_);
     ck(cudaGetLastError(), "k_accept");
   }
@@ -563,6 +575,19 @@ void Ensemble::drop_graph() {
   }
 }
 
+void Ensemble::set_error_policy(bool reject_failures) {
+  reject_fail_ = reject_failures;
+  drop_graph();
+}
+
+unsigned long long Ensemble::failures() const {
+  unsigned long long v = 0;
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  ck(cudaStreamSynchronize(stream_), "synchronize");
+  ck(cudaMemcpy(&v, nfail_, sizeof(v), cudaMemcpyDeviceToHost), "D2H");
+  return v;
+}
+
 void Ensemble::set_stage1(pofd_batch_loglike_fn fn, void* sur) {
   sfn_ = fn;
   sur_ = sur;
@@ -604,7 +629,8 @@ void Ensemble::da_half(int half, double zexp, double invt) {
   stats_[2] += b;
   if (collect_) collect_->add_pairs(count, exprop_, np_, exl_, exs_, stream_);
   k_stage2<<<(count + ENT - 1) / ENT, ENT, 0, stream_>>>(
-      half, nw_, np_, invt, seed_, static_cast<int>(count), exidx_, exprop_, exl_, exs_, spred_,
+      half, nw_, np_, invt, seed_, reject_fail_ ? 1 : 0, nfail_, static_cast<int>(count), exidx_,
+      exprop_, exl_, exs_, spred_,
       theta_, logl_, scur_, nacc_, ctr_, err_);
   ck(cudaGetLastError(), "k_stage2");
 }

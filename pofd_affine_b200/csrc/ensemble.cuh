@@ -51,6 +51,10 @@ class Ensemble {
   void collect_pairs(Surrogate* s) { collect_ = s; drop_graph(); }
   void do_steps_da(unsigned nsteps, bool record);
   void da_stats(unsigned long long* out4) const;
+  // false (default): a failed likelihood evaluation stops the run, as in the
+  // reference; true: it rejects the step and is counted.
+  void set_error_policy(bool reject_failures);
+  unsigned long long failures() const;
   unsigned nrecorded() const;
   void chain(float* theta, double* logl) const;
   void last(float* theta, double* logl) const;
@@ -113,6 +117,8 @@ class Ensemble {
   int* dcount_ = nullptr;     // [1]
   int* hcount_ = nullptr;     // pinned
   unsigned long long stats_[4] = {0, 0, 0, 0};
+  bool reject_fail_ = false;
+  unsigned long long* nfail_ = nullptr;
 };
 
 // A multivariate Gaussian log-density on the first k parameters: a test

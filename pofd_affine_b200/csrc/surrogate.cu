@@ -46,98 +46,118 @@ __device__ __forceinline__ float dsilu(float z) {
 }
 
 // ------------------------------------------------------------ GEMM kernels
+#define UMMA_PROLOGUE                                                         \
+  extern __shared__ __align__(1024) uint8_t smem[];                          \
+  __shared__ umma::Barriers bs;                                               \
+  const int m0 = blockIdx.x * umma::kRows, n0 = blockIdx.y * g.ntile;         \
+  const uint32_t tb = umma::mainloop(g, &tmA, &tmB, m0, n0, smem, bs);        \
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;                 \
+  const int row = m0 + warp * 32 + lane;                                      \
+  const uint32_t tlane = static_cast<uint32_t>(warp * 32) << 16;
+
+__device__ __forceinline__ void st_bf16x16(bf16* dst, const float* v) {
+  __align__(16) bf16 h[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) h[j] = __float2bfloat16_rn(v[j]);
+  reinterpret_cast<uint4*>(dst)[0] = reinterpret_cast<const uint4*>(h)[0];
+  reinterpret_cast<uint4*>(dst)[1] = reinterpret_cast<const uint4*>(h)[1];
+}
+
 // Plain product C = A B^T in FP32 (a checkable entry point of the tensor-core
 // main loop).
-__global__ void __launch_bounds__(NT) k_gemm_f32(umma::GemmShape g, float* __restrict__ C,
+__global__ void __launch_bounds__(NT) k_gemm_f32(const __grid_constant__ CUtensorMap tmA,
+                                                 const __grid_constant__ CUtensorMap tmB,
+                                                 umma::GemmShape g, float* __restrict__ C,
                                                  int ldc) {
-  extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint32_t tslot;
-  __shared__ uint64_t bar;
-  __shared__ int abort_;
-  const int m0 = blockIdx.x * umma::kRows;
-  const uint32_t tb = umma::mainloop(g, m0, smem, &tslot, &bar, &abort_);
+  UMMA_PROLOGUE
   if (tb != 0xFFFFFFFFu) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = m0 + warp * 32 + lane;
-    for (int c0 = 0; c0 < g.N; c0 += 16) {
+    for (int c0 = 0; c0 < g.ntile; c0 += 16) {
       float v[16];
-      umma::tmem_ld16(tb + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
+      umma::tmem_ld16(tb + tlane + c0, v);
       if (row < g.M)
-        for (int j = 0; j < 16; ++j) C[static_cast<size_t>(row) * ldc + c0 + j] = v[j];
+        for (int j = 0; j < 16; ++j) C[static_cast<size_t>(row) * ldc + n0 + c0 + j] = v[j];
     }
   }
-  umma::release(&tslot, umma::tmem_cols(g.N));
+  umma::release(bs, g.ntile);
 }
 
 // Hidden layer forward: z = A W^T + b, h = silu(z); writes h (bf16,
 // [M][ldh]) and, when given, z (fp32 [M][N]) and h^T (bf16 [N][ldt]).  The
-// last hidden layer also forms the network output y = h . w4 + b4 per row.
-__global__ void __launch_bounds__(NT) k_fwd(umma::GemmShape g, const float* __restrict__ bias,
+// last hidden layer also writes this column tile's part of the network
+// output, ypart[tile][row] = h . w4 (+ b4 in tile 0).
+__global__ void __launch_bounds__(NT) k_fwd(const __grid_constant__ CUtensorMap tmA,
+                                            const __grid_constant__ CUtensorMap tmB,
+                                            umma::GemmShape g, const float* __restrict__ bias,
                                             bf16* __restrict__ h, int ldh,
                                             float* __restrict__ z, bf16* __restrict__ ht,
                                             int ldt, const float* __restrict__ w4,
                                             const float* __restrict__ b4,
-                                            float* __restrict__ y) {
-  extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint32_t tslot;
-  __shared__ uint64_t bar;
-  __shared__ int abort_;
-  const int m0 = blockIdx.x * umma::kRows;
-  const uint32_t tb = umma::mainloop(g, m0, smem, &tslot, &bar, &abort_);
+                                            float* __restrict__ ypart) {
+  UMMA_PROLOGUE
   if (tb != 0xFFFFFFFFu) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = m0 + warp * 32 + lane;
     float yacc = 0.0f;
-    for (int c0 = 0; c0 < g.N; c0 += 16) {
-      float v[16];
-      umma::tmem_ld16(tb + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
+    for (int c0 = 0; c0 < g.ntile; c0 += 16) {
+      float v[16], hv[16];
+      umma::tmem_ld16(tb + tlane + c0, v);
+      const int cb = n0 + c0;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        v[j] += bias[cb + j];
+        hv[j] = silu(v[j]);
+      }
       if (row < g.M) {
+        st_bf16x16(h + static_cast<size_t>(row) * ldh + cb, hv);
+        if (z) {
+          float4* zp = reinterpret_cast<float4*>(z + static_cast<size_t>(row) * g.N + cb);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) zp[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        }
+#pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const int c = c0 + j;
-          const float zz = v[j] + bias[c];
-          const float hh = silu(zz);
-          const bf16 hb = __float2bfloat16_rn(hh);
-          h[static_cast<size_t>(row) * ldh + c] = hb;
-          if (z) z[static_cast<size_t>(row) * g.N + c] = zz;
-          if (ht) ht[static_cast<size_t>(c) * ldt + row] = hb;
-          if (w4) yacc += __bfloat162float(hb) * w4[c];
+          const bf16 hb = __float2bfloat16_rn(hv[j]);
+          if (ht) ht[static_cast<size_t>(cb + j) * ldt + row] = hb;
+          if (w4) yacc += __bfloat162float(hb) * w4[cb + j];
         }
       }
     }
-    if (w4 && row < g.M) y[row] = yacc + b4[0];
+    if (w4 && row < g.M)
+      ypart[static_cast<size_t>(blockIdx.y) * g.M + row] = yacc + (blockIdx.y == 0 ? b4[0] : 0.0f);
   }
-  umma::release(&tslot, umma::tmem_cols(g.N));
+  umma::release(bs, g.ntile);
 }
 
 // Backward through a hidden layer: dh = dZ_next W_next (this GEMM, with B =
 // W_next^T), dz = dh * silu'(z); writes dz (bf16 [M][N]) and dz^T (bf16
 // [N][ldt]).
-__global__ void __launch_bounds__(NT) k_bwd_dx(umma::GemmShape g, const float* __restrict__ z,
+__global__ void __launch_bounds__(NT) k_bwd_dx(const __grid_constant__ CUtensorMap tmA,
+                                               const __grid_constant__ CUtensorMap tmB,
+                                               umma::GemmShape g, const float* __restrict__ z,
                                                bf16* __restrict__ dz, bf16* __restrict__ dzt,
                                                int ldt) {
-  extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint32_t tslot;
-  __shared__ uint64_t bar;
-  __shared__ int abort_;
-  const int m0 = blockIdx.x * umma::kRows;
-  const uint32_t tb = umma::mainloop(g, m0, smem, &tslot, &bar, &abort_);
+  UMMA_PROLOGUE
   if (tb != 0xFFFFFFFFu) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = m0 + warp * 32 + lane;
-    for (int c0 = 0; c0 < g.N; c0 += 16) {
+    for (int c0 = 0; c0 < g.ntile; c0 += 16) {
       float v[16];
-      umma::tmem_ld16(tb + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
-      if (row < g.M)
-        for (int j = 0; j < 16; ++j) {
-          const int c = c0 + j;
-          const float d = v[j] * dsilu(z[static_cast<size_t>(row) * g.N + c]);
-          const bf16 db = __float2bfloat16_rn(d);
-          dz[static_cast<size_t>(row) * g.N + c] = db;
-          dzt[static_cast<size_t>(c) * ldt + row] = db;
+      umma::tmem_ld16(tb + tlane + c0, v);
+      const int cb = n0 + c0;
+      if (row < g.M) {
+        const float4* zp = reinterpret_cast<const float4*>(z + static_cast<size_t>(row) * g.N + cb);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 zz = zp[q];
+          v[4 * q] *= dsilu(zz.x);
+          v[4 * q + 1] *= dsilu(zz.y);
+          v[4 * q + 2] *= dsilu(zz.z);
+          v[4 * q + 3] *= dsilu(zz.w);
         }
+        st_bf16x16(dz + static_cast<size_t>(row) * g.N + cb, v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          dzt[static_cast<size_t>(cb + j) * ldt + row] = __float2bfloat16_rn(v[j]);
+      }
     }
   }
-  umma::release(&tslot, umma::tmem_cols(g.N));
+  umma::release(bs, g.ntile);
 }
 
 struct AdamArgs {
@@ -148,44 +168,45 @@ struct AdamArgs {
 // [Nin x M]) followed by the Adam step of W [Nout][Nin]; writes the bf16
 // copies W (row-major) and W^T.  grad_out, when given, receives G instead
 // of the update (gradient checks).
-__global__ void __launch_bounds__(NT) k_wgrad_adam(umma::GemmShape g, AdamArgs ad,
+__global__ void __launch_bounds__(NT) k_wgrad_adam(const __grid_constant__ CUtensorMap tmA,
+                                                   const __grid_constant__ CUtensorMap tmB,
+                                                   umma::GemmShape g, AdamArgs ad,
                                                    float* __restrict__ W, float* __restrict__ m,
                                                    float* __restrict__ v, bf16* __restrict__ Wb,
                                                    int ldwb, bf16* __restrict__ Wt, int ldwt,
                                                    float* __restrict__ grad_out) {
-  extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint32_t tslot;
-  __shared__ uint64_t bar;
-  __shared__ int abort_;
-  const int m0 = blockIdx.x * umma::kRows;
-  const uint32_t tb = umma::mainloop(g, m0, smem, &tslot, &bar, &abort_);
+  UMMA_PROLOGUE
   if (tb != 0xFFFFFFFFu) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = m0 + warp * 32 + lane;
-    for (int c0 = 0; c0 < g.N; c0 += 16) {
+    for (int c0 = 0; c0 < g.ntile; c0 += 16) {
       float gv[16];
-      umma::tmem_ld16(tb + (static_cast<uint32_t>(warp * 32) << 16) + c0, gv);
-      if (row < g.M)
-        for (int j = 0; j < 16; ++j) {
-          const int c = c0 + j;
-          const size_t i = static_cast<size_t>(row) * g.N + c;
-          if (grad_out) {
-            grad_out[i] = gv[j];
-            continue;
-          }
-          const float mm = ad.b1 * m[i] + (1.0f - ad.b1) * gv[j];
-          const float vv = ad.b2 * v[i] + (1.0f - ad.b2) * gv[j] * gv[j];
-          m[i] = mm;
-          v[i] = vv;
-          const float w = W[i] - ad.lr * (mm / ad.bc1) / (sqrtf(vv / ad.bc2) + ad.eps);
-          W[i] = w;
-          const bf16 wb = __float2bfloat16_rn(w);
-          Wb[static_cast<size_t>(row) * ldwb + c] = wb;
-          if (Wt) Wt[static_cast<size_t>(c) * ldwt + row] = wb;
-        }
+      umma::tmem_ld16(tb + tlane + c0, gv);
+      const int cb = n0 + c0;
+      if (row >= g.M) continue;
+      const size_t i0 = static_cast<size_t>(row) * g.N + cb;
+      if (grad_out) {
+        float4* gp = reinterpret_cast<float4*>(grad_out + i0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) gp[q] = make_float4(gv[4 * q], gv[4 * q + 1], gv[4 * q + 2], gv[4 * q + 3]);
+        continue;
+      }
+      float w[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const size_t i = i0 + j;
+        const float mm = ad.b1 * m[i] + (1.0f - ad.b1) * gv[j];
+        const float vv = ad.b2 * v[i] + (1.0f - ad.b2) * gv[j] * gv[j];
+        m[i] = mm;
+        v[i] = vv;
+        w[j] = W[i] - ad.lr * (mm / ad.bc1) / (sqrtf(vv / ad.bc2) + ad.eps);
+        W[i] = w[j];
+      }
+      st_bf16x16(Wb + static_cast<size_t>(row) * ldwb + cb, w);
+      if (Wt)
+        for (int j = 0; j < 16; ++j)
+          Wt[static_cast<size_t>(cb + j) * ldwt + row] = __float2bfloat16_rn(w[j]);
     }
   }
-  umma::release(&tslot, umma::tmem_cols(g.N));
+  umma::release(bs, g.ntile);
 }
 
 // ------------------------------------------------------ elementwise kernels
@@ -209,24 +230,42 @@ __global__ void k_pack_inputs(int M, int Mp, const float* __restrict__ theta, in
   }
 }
 
-// Output layer backward and the loss: dy = 2 (y - t) / M; d(w4) = sum dy h3,
-// d(b4) = sum dy (block partials), dz3 = dy w4 * silu'(z3).
-__global__ void k_out_bwd(int M, int Mp, int H, const float* __restrict__ y,
-                          const float* __restrict__ t, const float* __restrict__ w4,
-                          const float* __restrict__ z3, bf16* __restrict__ dz3,
-                          bf16* __restrict__ dz3t, float* __restrict__ dy_out,
-                          float* __restrict__ loss) {
+// Network output y = sum of the column-tile parts, the loss and
+// dy = 2 (y - t) / M.
+__global__ void k_out_loss(int M, int Mp, int ntiles, const float* __restrict__ ypart,
+                           const float* __restrict__ t, float* __restrict__ y,
+                           float* __restrict__ dy_out, float* __restrict__ loss) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= Mp) return;
-  const float dy = (r < M) ? 2.0f * (y[r] - t[r]) / static_cast<float>(M) : 0.0f;
-  dy_out[r] = dy;
-  if (r < M) atomicAdd(loss, (y[r] - t[r]) * (y[r] - t[r]) / static_cast<float>(M));
-  for (int c = 0; c < H; ++c) {
-    const float d = (r < M) ? dy * w4[c] * dsilu(z3[static_cast<size_t>(r) * H + c]) : 0.0f;
-    const bf16 b = __float2bfloat16_rn(d);
-    dz3[static_cast<size_t>(r) * H + c] = b;
-    dz3t[static_cast<size_t>(c) * Mp + r] = b;
+  float yy = 0.0f;
+  for (int k = 0; k < ntiles; ++k) yy += ypart[static_cast<size_t>(k) * Mp + r];
+  y[r] = yy;
+  const float d = (r < M) ? (yy - t[r]) : 0.0f;
+  dy_out[r] = 2.0f * d / static_cast<float>(M);
+  if (r < M) atomicAdd(loss, d * d / static_cast<float>(M));
+}
+
+// dz3 = dy w4 * silu'(z3), one thread per (16-column chunk, row).
+__global__ void k_out_dz(int Mp, int H, const float* __restrict__ dy,
+                         const float* __restrict__ w4, const float* __restrict__ z3,
+                         bf16* __restrict__ dz3, bf16* __restrict__ dz3t) {
+  const long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= static_cast<long long>(Mp) * (H / 16)) return;
+  const int r = static_cast<int>(e % Mp), c0 = static_cast<int>(e / Mp) * 16;
+  const float d = dy[r];
+  const float4* zp = reinterpret_cast<const float4*>(z3 + static_cast<size_t>(r) * H + c0);
+  float v[16];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float4 zz = zp[q];
+    v[4 * q] = d * w4[c0 + 4 * q] * dsilu(zz.x);
+    v[4 * q + 1] = d * w4[c0 + 4 * q + 1] * dsilu(zz.y);
+    v[4 * q + 2] = d * w4[c0 + 4 * q + 2] * dsilu(zz.z);
+    v[4 * q + 3] = d * w4[c0 + 4 * q + 3] * dsilu(zz.w);
   }
+  st_bf16x16(dz3 + static_cast<size_t>(r) * H + c0, v);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) dz3t[static_cast<size_t>(c0 + j) * Mp + r] = __float2bfloat16_rn(v[j]);
 }
 
 // Gradients of w4 (sum_r dy h3[r]), b4 (sum dy) and the hidden biases
@@ -294,20 +333,25 @@ __global__ void k_pick_rows(int Mb, unsigned n, unsigned long long it,
   rows[r] = static_cast<int>((x >> 32) * static_cast<unsigned long long>(n) >> 32);
 }
 
+// Targets (logL - ymax, floored at -clip) / ys.
 __global__ void k_gather_targets(int M, const int* __restrict__ rows,
-                                 const double* __restrict__ logl, float ymax, float iys,
-                                 float* __restrict__ t) {
+                                 const double* __restrict__ logl, double ymax, double clip,
+                                 double iys, float* __restrict__ t) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= M) return;
-  t[r] = static_cast<float>((logl[rows ? rows[r] : r] - ymax) * iys);
+  const double d = logl[rows ? rows[r] : r] - ymax;
+  t[r] = static_cast<float>((d < -clip ? -clip : d) * iys);
 }
 
 // Network output to log-likelihood units: logL = ymax + ys * y.
-__global__ void k_unscale(int M, const float* __restrict__ y, double ymax, double ys,
-                          double* __restrict__ out, int* __restrict__ status) {
+__global__ void k_unscale(int M, int Mp, int ntiles, const float* __restrict__ ypart,
+                          double ymax, double ys, double* __restrict__ out,
+                          int* __restrict__ status) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= M) return;
-  out[r] = ymax + ys * static_cast<double>(y[r]);
+  float yy = 0.0f;
+  for (int k = 0; k < ntiles; ++k) yy += ypart[static_cast<size_t>(k) * Mp + r];
+  out[r] = ymax + ys * static_cast<double>(yy);
   if (status) status[r] = POFD_OK;
 }
 
@@ -324,6 +368,80 @@ __global__ void k_append_pairs(int n, const float* __restrict__ theta, int npar,
   for (int p = 0; p < npar; ++p) ptheta[static_cast<size_t>(slot) * npar + p] = theta[static_cast<size_t>(r) * npar + p];
   plogl[slot] = logl[r];
   atomicMax(&counters[1], min(slot + 1, cap));
+}
+
+// ----------------------------------------------------------- tensor maps
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encode_fn() {
+  static EncodeFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    ck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q),
+       "cuTensorMapEncodeTiled entry point");
+    if (q != cudaDriverEntryPointSuccess || !p) throw Error(POFD_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<EncodeFn>(p);
+  }
+  return fn;
+}
+
+// A row-major bf16 matrix [rows][K] (leading dimension ld elements) viewed
+// as [K/8][rows][8] so that a {8, box_rows, 8} box lands in the canonical
+// no-swizzle K-major layout; rows and K beyond the matrix read as zero.
+CUtensorMap kmajor_map(const bf16* base, int rows, int K, int ld, int box_rows) {
+  if (reinterpret_cast<uintptr_t>(base) % 16 || ld % 8 || K % 16)
+    throw Error(POFD_E_ARG, "tensor map: base 16-byte aligned, ld multiple of 8, K multiple of 16");
+  CUtensorMap m;
+  const cuuint64_t dims[3] = {8, static_cast<cuuint64_t>(rows), static_cast<cuuint64_t>(K / 8)};
+  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(ld) * 2, 16};
+  // the box is always {8, box_rows, 8}: rows and K groups past the matrix
+  // are zero-filled, so every stage holds exactly stage_bytes() and keeps the
+  // layout the MMA descriptors assume
+  const cuuint32_t box[3] = {8, static_cast<cuuint32_t>(box_rows), 8};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(base),
+                                 dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(POFD_E_CUDA, "cuTensorMapEncodeTiled failed");
+  return m;
+}
+
+struct Gemm {
+  umma::GemmShape g;
+  CUtensorMap a, b;
+  dim3 grid;
+  size_t smem;
+};
+
+// C[M x N] = A[M x K] B[N x K]^T with A (lda) and B (ldb) row-major bf16.
+Gemm plan_gemm(int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb, int* err) {
+  if (M <= 0 || N < 16 || N > umma::kMaxN || N % 16 || K < 16 || K % 16)
+    throw Error(POFD_E_ARG, "gemm: need N in [16, 512] and K >= 16, both multiples of 16");
+  Gemm q;
+  const int nt = umma::pick_ntile(N);
+  q.g = umma::GemmShape{M, N, K, nt, err};
+  q.a = kmajor_map(A, M, K, lda, umma::kRows);
+  q.b = kmajor_map(B, N, K, ldb, nt);
+  q.grid = dim3(static_cast<unsigned>((M + umma::kRows - 1) / umma::kRows),
+                static_cast<unsigned>(N / nt));
+  q.smem = umma::smem_bytes(nt);
+  return q;
+}
+
+void set_gemm_attributes() {
+  static bool done = false;
+  if (done) return;
+  const int sm = static_cast<int>(umma::smem_bytes(umma::kMaxNTile));
+  ck(cudaFuncSetAttribute(k_gemm_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  ck(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  ck(cudaFuncSetAttribute(k_bwd_dx, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  ck(cudaFuncSetAttribute(k_wgrad_adam, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  done = true;
 }
 
 }  // namespace
@@ -364,12 +482,7 @@ Surrogate::Surrogate(int device, cudaStream_t stream, unsigned npar, const int* 
   plogl_ = dal<double>(cap_);
   counters_ = dal<unsigned>(4);
   err_ = dal<int>(1);
-  const int smax = static_cast<int>(umma::smem_bytes(static_cast<int>(H_)));
-  ck(cudaFuncSetAttribute(k_gemm_f32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          static_cast<int>(umma::smem_bytes(umma::kMaxN))), "attr");
-  ck(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smax), "attr");
-  ck(cudaFuncSetAttribute(k_bwd_dx, cudaFuncAttributeMaxDynamicSharedMemorySize, smax), "attr");
-  ck(cudaFuncSetAttribute(k_wgrad_adam, cudaFuncAttributeMaxDynamicSharedMemorySize, smax), "attr");
+  set_gemm_attributes();
   init_weights();
 }
 
@@ -383,7 +496,7 @@ Surrogate::~Surrogate() {
   void* q[] = {idx_, mu_, isd_, w1b_, w2b_, w3b_, w2t_, w3t_, ptheta_, plogl_, counters_, err_,
                ws_.x, ws_.xt, ws_.h[0], ws_.h[1], ws_.h[2], ws_.ht[0], ws_.ht[1], ws_.ht[2],
                ws_.z[0], ws_.z[1], ws_.z[2], ws_.dz[0], ws_.dz[1], ws_.dz[2], ws_.dzt[0],
-               ws_.dzt[1], ws_.dzt[2], ws_.y, ws_.t, ws_.dy, ws_.rows, ws_.loss};
+               ws_.dzt[1], ws_.dzt[2], ws_.y, ws_.ypart, ws_.t, ws_.dy, ws_.rows, ws_.loss};
   for (void* p : q)
     if (p) cudaFree(p);
 }
@@ -457,7 +570,7 @@ void Surrogate::ensure_work(int Mp) {
   if (Mp <= ws_.Mp) return;
   void* q[] = {ws_.x, ws_.xt, ws_.h[0], ws_.h[1], ws_.h[2], ws_.ht[0], ws_.ht[1], ws_.ht[2],
                ws_.z[0], ws_.z[1], ws_.z[2], ws_.dz[0], ws_.dz[1], ws_.dz[2], ws_.dzt[0],
-               ws_.dzt[1], ws_.dzt[2], ws_.y, ws_.t, ws_.dy, ws_.rows, ws_.loss};
+               ws_.dzt[1], ws_.dzt[2], ws_.y, ws_.ypart, ws_.t, ws_.dy, ws_.rows, ws_.loss};
   for (void* p : q)
     if (p) cudaFree(p);
   ws_ = Work{};
@@ -473,6 +586,7 @@ void Surrogate::ensure_work(int Mp) {
     ws_.dzt[l] = dal<bf16>(M * H);
   }
   ws_.y = dal<float>(M);
+  ws_.ypart = dal<float>(M * (umma::kMaxN / 16));
   ws_.t = dal<float>(M);
   ws_.dy = dal<float>(M);
   ws_.rows = dal<int>(M);
@@ -486,19 +600,18 @@ void Surrogate::forward(int M, const float* theta, int npar, const int* rows, bo
   const int Mp = (M + umma::kRows - 1) / umma::kRows * umma::kRows;
   ensure_work(Mp);
   const int H = static_cast<int>(H_);
-  const unsigned gb = static_cast<unsigned>(Mp / umma::kRows);
   k_pack_inputs<<<(Mp + 127) / 128, 128, 0, st>>>(M, Mp, theta, npar, idx_, static_cast<int>(nin_),
                                                   mu_, isd_, rows, ws_.x, train ? ws_.xt : nullptr);
-  const size_t sm = umma::smem_bytes(H);
   const bf16* Ws[3] = {w1b_, w2b_, w3b_};
   const bf16* in = ws_.x;
   int ldin = kInPad;
   for (int l = 0; l < 3; ++l) {
-    umma::GemmShape g{Mp, H, l == 0 ? kInPad : H, in, ldin, Ws[l], l == 0 ? kInPad : H, err_};
+    const int K = (l == 0) ? kInPad : H;
+    const Gemm q = plan_gemm(Mp, H, K, in, ldin, Ws[l], K, err_);
     const bool last = (l == 2);
-    k_fwd<<<gb, NT, sm, st>>>(g, p_[2 * l + 1], ws_.h[l], H, train ? ws_.z[l] : nullptr,
-                              train ? ws_.ht[l] : nullptr, Mp, last ? p_[6] : nullptr,
-                              last ? p_[7] : nullptr, ws_.y);
+    k_fwd<<<q.grid, NT, q.smem, st>>>(q.a, q.b, q.g, p_[2 * l + 1], ws_.h[l], H,
+                                      train ? ws_.z[l] : nullptr, train ? ws_.ht[l] : nullptr, Mp,
+                                      last ? p_[6] : nullptr, last ? p_[7] : nullptr, ws_.ypart);
     in = ws_.h[l];
     ldin = H;
   }
@@ -512,7 +625,10 @@ void Surrogate::predict(unsigned n, const float* theta, unsigned npar, double* o
   ck(cudaSetDevice(device_), "cudaSetDevice");
   if (!st) st = stream_;
   forward(static_cast<int>(n), theta, static_cast<int>(npar), nullptr, false, st);
-  k_unscale<<<(n + 127) / 128, 128, 0, st>>>(static_cast<int>(n), ws_.y, ymax_, ys_, out, status);
+  const int Mp = (static_cast<int>(n) + umma::kRows - 1) / umma::kRows * umma::kRows;
+  const int ntiles = static_cast<int>(H_) / umma::pick_ntile(static_cast<int>(H_));
+  k_unscale<<<(n + 127) / 128, 128, 0, st>>>(static_cast<int>(n), Mp, ntiles, ws_.ypart, ymax_, ys_,
+                                             out, status);
   ck(cudaGetLastError(), "k_unscale");
 }
 
@@ -559,15 +675,22 @@ void Surrogate::refresh_scaling() {
     mu[k] = static_cast<float>(m);
     isd[k] = static_cast<float>(sd > 0 ? 1.0 / sd : 1.0);
   }
-  double mx = -std::numeric_limits<double>::infinity(), s = 0, s2 = 0;
-  for (double v : ll) {
-    mx = std::max(mx, v);
-    s += v;
-  }
+  // target: logL - max, floored at -clip so that far-off burn-in points do
+  // not set the scale; the floor grows with the number of inputs (a
+  // chi-square of nin degrees of freedom sits near -nin/2)
+  double mx = -std::numeric_limits<double>::infinity();
+  for (double v : ll) mx = std::max(mx, v);
+  const double clip = 25.0 + 2.5 * nin_;
+  double s = 0, s2 = 0;
+  for (double v : ll) s += std::max(v - mx, -clip);
   const double m = s / n;
-  for (double v : ll) s2 += (v - m) * (v - m);
+  for (double v : ll) {
+    const double d = std::max(v - mx, -clip) - m;
+    s2 += d * d;
+  }
   const double sd = std::sqrt(s2 / n);
   ymax_ = mx;
+  clip_ = clip;
   ys_ = (sd > 0) ? sd : 1.0;
   ck(cudaMemcpy(mu_, mu.data(), kInPad * sizeof(float), cudaMemcpyHostToDevice), "upload");
   ck(cudaMemcpy(isd_, isd.data(), kInPad * sizeof(float), cudaMemcpyHostToDevice), "upload");
@@ -581,35 +704,38 @@ float Surrogate::iteration(int Mb, const int* rows, float lr, float** grads, cud
   const int Mp = (Mb + umma::kRows - 1) / umma::kRows * umma::kRows;
   const int H = static_cast<int>(H_);
   forward(Mb, ptheta_, static_cast<int>(npar_), rows, true, st);
-  k_gather_targets<<<(Mb + 127) / 128, 128, 0, st>>>(Mb, rows, plogl_, static_cast<float>(ymax_),
-                                                     static_cast<float>(1.0 / ys_), ws_.t);
+  k_gather_targets<<<(Mb + 127) / 128, 128, 0, st>>>(Mb, rows, plogl_, ymax_, clip_, 1.0 / ys_,
+                                                     ws_.t);
   ck(cudaMemsetAsync(ws_.loss, 0, sizeof(float), st), "memset");
-  k_out_bwd<<<(Mp + 127) / 128, 128, 0, st>>>(Mb, Mp, H, ws_.y, ws_.t, p_[6], ws_.z[2], ws_.dz[2],
-                                              ws_.dzt[2], ws_.dy, ws_.loss);
+  const int ntiles = H / umma::pick_ntile(H);
+  k_out_loss<<<(Mp + 127) / 128, 128, 0, st>>>(Mb, Mp, ntiles, ws_.ypart, ws_.t, ws_.y, ws_.dy,
+                                               ws_.loss);
+  {
+    const long long ne = static_cast<long long>(Mp) * (H / 16);
+    k_out_dz<<<static_cast<unsigned>((ne + 127) / 128), 128, 0, st>>>(Mp, H, ws_.dy, p_[6],
+                                                                     ws_.z[2], ws_.dz[2],
+                                                                     ws_.dzt[2]);
+  }
   ++step_;
   AdamArgs ad{lr, 0.9f, 0.999f, 1e-8f, 1.0f - std::pow(0.9f, static_cast<float>(step_)),
               1.0f - std::pow(0.999f, static_cast<float>(step_))};
-  const size_t sm = umma::smem_bytes(H);
-  const unsigned gh = static_cast<unsigned>((H + umma::kRows - 1) / umma::kRows);
-  // layer 3 and 2: dX through W (B = W^T), then the weight gradient
   const bf16* Wt[3] = {nullptr, w2t_, w3t_};
   bf16* Wb[3] = {w1b_, w2b_, w3b_};
   bf16* Wtw[3] = {nullptr, w2t_, w3t_};
   for (int l = 2; l >= 0; --l) {
     if (l > 0) {
       // dh_{l-1} = dz_l W_l: A = dz_l [Mp x H], B = W_l^T [H x H]
-      umma::GemmShape gx{Mp, H, H, ws_.dz[l], H, Wt[l], H, err_};
-      k_bwd_dx<<<static_cast<unsigned>(Mp / umma::kRows), NT, sm, st>>>(gx, ws_.z[l - 1],
-                                                                       ws_.dz[l - 1],
-                                                                       ws_.dzt[l - 1], Mp);
+      const Gemm q = plan_gemm(Mp, H, H, ws_.dz[l], H, Wt[l], H, err_);
+      k_bwd_dx<<<q.grid, NT, q.smem, st>>>(q.a, q.b, q.g, ws_.z[l - 1], ws_.dz[l - 1],
+                                           ws_.dzt[l - 1], Mp);
     }
     // G_l = dz_l^T X_l: A = dz_l^T [H x Mp], B = X_l^T [Nin x Mp]
     const int nin = (l == 0) ? kInPad : H;
     const bf16* XT = (l == 0) ? ws_.xt : ws_.ht[l - 1];
-    umma::GemmShape gw{H, nin, Mp, ws_.dzt[l], Mp, XT, Mp, err_};
-    k_wgrad_adam<<<gh, NT, umma::smem_bytes(nin), st>>>(gw, ad, p_[2 * l], m_[2 * l], v_[2 * l],
-                                                        Wb[l], nin, Wtw[l], H,
-                                                        grads ? grads[2 * l] : nullptr);
+    const Gemm q = plan_gemm(H, nin, Mp, ws_.dzt[l], Mp, XT, Mp, err_);
+    k_wgrad_adam<<<q.grid, NT, q.smem, st>>>(q.a, q.b, q.g, ad, p_[2 * l], m_[2 * l], v_[2 * l],
+                                             Wb[l], nin, Wtw[l], H,
+                                             grads ? grads[2 * l] : nullptr);
   }
   BiasArgs ba{};
   ba.Mp = Mp;
@@ -680,23 +806,16 @@ void Surrogate::scaling(double* out) const {
   }
   out[2 * kInPad] = ymax_;
   out[2 * kInPad + 1] = ys_;
+  out[2 * kInPad + 2] = clip_;
 }
 
 // The tensor-core main loop on its own: C = A B^T (fp32).
 void bf16_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C,
                int ldc, int* err, cudaStream_t st) {
-  if (M <= 0 || N < 16 || N > umma::kMaxN || N % 16 || K < 16 || K % 16)
-    throw Error(POFD_E_ARG, "bf16_gemm: need N in [16, 512] and K >= 16, both multiples of 16");
-  if (lda % 8 || ldb % 8) throw Error(POFD_E_ARG, "bf16_gemm: leading dimensions must be multiples of 8");
-  static bool attr = false;
-  if (!attr) {
-    ck(cudaFuncSetAttribute(k_gemm_f32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(umma::smem_bytes(umma::kMaxN))), "attr");
-    attr = true;
-  }
-  umma::GemmShape g{M, N, K, static_cast<const bf16*>(A), lda, static_cast<const bf16*>(B), ldb, err};
-  const unsigned gb = static_cast<unsigned>((M + umma::kRows - 1) / umma::kRows);
-  k_gemm_f32<<<gb, NT, umma::smem_bytes(N), st>>>(g, C, ldc);
+  set_gemm_attributes();
+  const Gemm q = plan_gemm(M, N, K, static_cast<const bf16*>(A), lda, static_cast<const bf16*>(B),
+                           ldb, err);
+  k_gemm_f32<<<q.grid, NT, q.smem, st>>>(q.a, q.b, q.g, C, ldc);
   ck(cudaGetLastError(), "k_gemm_f32");
 }
 

@@ -36,7 +36,7 @@ class Surrogate {
   void get_params_host(std::vector<std::vector<float>>& host) const;
   void set_params_host(const std::vector<std::vector<float>>& host);
   size_t tensor_size(int t) const { return size_[t]; }
-  void scaling(double* out) const;  // mu[16], 1/sd[16], ymax, ys
+  void scaling(double* out) const;  // mu[16], 1/sd[16], ymax, ys, clip
   void refresh_scaling();
   unsigned hidden() const { return H_; }
   unsigned nin() const { return nin_; }
@@ -57,7 +57,7 @@ class Surrogate {
   uint64_t seed_;
   unsigned step_ = 0;
   bool scaled_ = false;
-  double ymax_ = 0.0, ys_ = 1.0;
+  double ymax_ = 0.0, ys_ = 1.0, clip_ = 1e300;
   int* idx_ = nullptr;
   float* mu_ = nullptr;
   float* isd_ = nullptr;
@@ -79,7 +79,7 @@ class Surrogate {
     float* z[3] = {};
     __nv_bfloat16* dz[3] = {};
     __nv_bfloat16* dzt[3] = {};
-    float *y = nullptr, *t = nullptr, *dy = nullptr, *loss = nullptr;
+    float *y = nullptr, *ypart = nullptr, *t = nullptr, *dy = nullptr, *loss = nullptr;
     int* rows = nullptr;
   } ws_;
 };

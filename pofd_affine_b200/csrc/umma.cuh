@@ -1,22 +1,27 @@
-// umma.cuh -- BF16 tensor-core GEMM on sm_100a (tcgen05 / TMEM) with
+// umma.cuh -- BF16 tensor-core GEMM on sm_100a (TMA + tcgen05 / TMEM) with
 // pluggable epilogues, for the surrogate network.
 //
 //   C[M x N] = A[M x K] * B[N x K]^T      A, B bf16, K-major (row-major with
 //                                          K contiguous), FP32 accumulate
 //
-// One CTA (4 warps) owns a 128-row tile of C and all N <= 512 columns.  K is
-// consumed in 64-wide chunks: the warps stage the A and B chunks in shared
-// memory in the canonical no-swizzle K-major layout (8-row x 16-byte core
-// matrices; the two 16-byte K halves of an MMA sit LBO bytes apart, 8-row
-// groups SBO = 128 bytes apart), one elected thread issues
-// tcgen05.mma.cta_group::1.kind::f16 (M = 128, N <= 256 per instruction,
-// K = 16) into a TMEM accumulator and commits to an mbarrier, and the
-// epilogue reads the accumulator back with tcgen05.ld (warp w owns TMEM
-// lanes 32w..32w+31 = rows of the tile).  Every wait is bounded: on timeout
-// the kernel records an error code and releases its TMEM.
+// One CTA (4 warps) owns a 128 x ntile tile of C (ntile <= 128 divides N).
+// K is consumed in 64-wide chunks through a 3-stage shared-memory ring: one
+// thread (warp 0) issues TMA tile loads (cp.async.bulk.tensor, 3-D tensor
+// maps that view a row-major [rows][K] matrix as [K/8][rows][8], so the
+// copy lands directly in the canonical no-swizzle K-major layout: 8-row x
+// 16-byte core matrices, K halves LBO = rows * 16 bytes apart, 8-row groups
+// SBO = 128 bytes apart), signalling a "full" mbarrier with the byte count;
+// one thread (warp 1) waits on it and issues
+// tcgen05.mma.cta_group::1.kind::f16 (M = 128, N = ntile, K = 16) into a
+// TMEM accumulator, committing to the stage's "empty" mbarrier so the
+// producer can refill it; the last commit releases the epilogue, which reads
+// the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 =
+// rows of the tile).  Every wait is bounded: on timeout the kernel records
+// an error code, stops issuing work and releases its TMEM.
 #ifndef POFD_UMMA_CUH
 #define POFD_UMMA_CUH
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -27,7 +32,9 @@ namespace umma {
 
 constexpr int kRows = 128;      // M tile (TMEM lanes)
 constexpr int kKChunk = 64;     // K per shared-memory stage
-constexpr int kMaxN = 512;      // TMEM columns
+constexpr int kStages = 3;      // shared-memory ring depth
+constexpr int kMaxNTile = 128;  // N per CTA
+constexpr int kMaxN = 512;      // N per GEMM
 constexpr int kThreads = 128;
 constexpr unsigned kSpinLimit = 1u << 24;  // bounded mbarrier wait
 
@@ -95,6 +102,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes),
+               "r"(smem_u32(bar))
+               : "memory");
+}
+
+// 3-D tiled TMA load into this CTA's shared memory, completing on bar.
+__device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* map, int c0, int c1,
+                                          int c2, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
 __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -133,99 +156,120 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 struct GemmShape {
-  int M, N, K;                       // N multiple of 16 (<= 512), K multiple of 16
-  const __nv_bfloat16* A; int lda;   // [M][K]
-  const __nv_bfloat16* B; int ldb;   // [N][K]
-  int* err;                          // error code (0 = ok)
+  int M, N, K;   // N multiple of 16 (<= 512), K multiple of 16
+  int ntile;     // N per CTA (16, 32, 64 or 128; divides N)
+  int* err;      // error code (0 = ok)
 };
 
 __host__ __device__ constexpr int tmem_cols(int n) {
   return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : n <= 256 ? 256 : 512;
 }
 
-// Shared memory bytes of the main loop for N columns.
-__host__ __device__ constexpr size_t smem_bytes(int n) {
-  return static_cast<size_t>(kRows + n) * kKChunk * 2 + 64;
+__host__ __device__ constexpr int pick_ntile(int n) {
+  return (n % 128 == 0) ? 128 : (n % 64 == 0) ? 64 : (n % 32 == 0) ? 32 : 16;
 }
 
-// Stage a [R x kw] bf16 chunk (rows r0.., columns k0..k0+kw) into the
-// canonical layout: 16-byte cell (r, kg) at kg * R * 16 + r * 16.  Rows at or
-// beyond nrows are zero.
-__device__ __forceinline__ void stage_chunk(const __nv_bfloat16* __restrict__ g, int ld,
-                                            int r0, int nrows, int R, int k0, int kw,
-                                            uint8_t* s) {
-  const int kgs = kw >> 3;
-  for (int c = threadIdx.x; c < R * kgs; c += kThreads) {
-    const int r = c % R, kg = c / R;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (r0 + r < nrows)
-      v = *reinterpret_cast<const uint4*>(g + static_cast<size_t>(r0 + r) * ld + k0 + kg * 8);
-    *reinterpret_cast<uint4*>(s + (static_cast<size_t>(kg) * R + r) * 16) = v;
-  }
+__host__ __device__ constexpr size_t stage_bytes(int ntile) {
+  return static_cast<size_t>(kRows + ntile) * kKChunk * 2;
 }
 
-// Main loop: accumulates the CTA's 128 x N tile into TMEM and returns the
-// TMEM base address (or 0xFFFFFFFF after a timeout, err set).  Must be called
-// by all kThreads threads; smem points at smem_bytes(N) dynamic bytes.
-__device__ __forceinline__ uint32_t mainloop(const GemmShape& g, int m0, uint8_t* smem,
-                                             uint32_t* tslot, uint64_t* bar, int* abort) {
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + kRows * kKChunk * 2;
-  const int ncols = tmem_cols(g.N);
+// Dynamic shared memory of the main loop (ring + 1 KB alignment slack).
+__host__ __device__ constexpr size_t smem_bytes(int ntile) {
+  return kStages * stage_bytes(ntile) + 1024;
+}
+
+struct Barriers {
+  uint64_t full[kStages];
+  uint64_t empty[kStages];
+  uint64_t done;
+  uint32_t tslot;
+  int abort;
+};
+
+// Main loop: accumulates the CTA's 128 x ntile tile (rows m0.., columns
+// n0..) into TMEM and returns the TMEM base address, or 0xFFFFFFFF after a
+// timeout (err set).  Called by all kThreads threads.
+__device__ __forceinline__ uint32_t mainloop(const GemmShape& g, const CUtensorMap* tmA,
+                                             const CUtensorMap* tmB, int m0, int n0,
+                                             uint8_t* smem_raw, Barriers& bs) {
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~static_cast<uintptr_t>(1023));
+  const int nt = g.ntile;
+  const size_t sbytes = stage_bytes(nt);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    *abort = 0;
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&bs.full[s], 1);
+      mbar_init(&bs.empty[s], 1);
+    }
+    mbar_init(&bs.done, 1);
+    bs.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
-  if (threadIdx.x < 32) tmem_alloc(tslot, ncols);
+  if (warp == 0) tmem_alloc(&bs.tslot, static_cast<uint32_t>(tmem_cols(nt)));
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tbase = *tslot;
-  const int nchunks = (g.K + kKChunk - 1) / kKChunk;
-  for (int kc = 0; kc < nchunks; ++kc) {
-    const int k0 = kc * kKChunk;
-    const int kw = min(kKChunk, g.K - k0);
-    stage_chunk(g.A, g.lda, m0, g.M, kRows, k0, kw, sA);
-    stage_chunk(g.B, g.ldb, 0, g.N, g.N, k0, kw, sB);
-    fence_async_smem();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      tc_fence_after();
-      for (int s = 0; s < kw / 16; ++s) {
-        const uint32_t a = smem_u32(sA) + static_cast<uint32_t>(2 * s * kRows * 16);
-        const uint64_t ad = smem_desc(a, kRows * 16, 128);
-        for (int n0 = 0; n0 < g.N; n0 += 256) {
-          const int nn = min(256, g.N - n0);
-          const uint32_t b = smem_u32(sB) + static_cast<uint32_t>((2 * s * g.N + n0) * 16);
-          const uint64_t bd = smem_desc(b, static_cast<uint32_t>(g.N) * 16, 128);
-          mma_bf16(tbase + static_cast<uint32_t>(n0), ad, bd, instr_desc(kRows, nn),
-                   (kc > 0 || s > 0) ? 1u : 0u);
-        }
+  const uint32_t tbase = bs.tslot;
+  const int nk = (g.K + kKChunk - 1) / kKChunk;
+  const uint32_t tx = static_cast<uint32_t>(sbytes);
+  if (warp == 0 && lane == 0) {
+    // producer: TMA loads into the ring
+    for (int kc = 0; kc < nk; ++kc) {
+      const int s = kc % kStages;
+      if (kc >= kStages && !mbar_wait(&bs.empty[s], static_cast<uint32_t>((kc / kStages - 1) & 1))) {
+        atomicExch(&bs.abort, 1);
+        break;
       }
-      mma_commit(bar);
+      uint8_t* sa = smem + s * sbytes;
+      mbar_expect_tx(&bs.full[s], tx);
+      tma_load3(sa, tmA, 0, m0, kc * (kKChunk / 8), &bs.full[s]);
+      tma_load3(sa + kRows * kKChunk * 2, tmB, 0, n0, kc * (kKChunk / 8), &bs.full[s]);
     }
-    // all threads wait for the MMAs before the chunk buffers are reused
-    const bool ok = mbar_wait(bar, static_cast<uint32_t>(kc & 1));
-    if (!ok) atomicExch(abort, 1);
-    __syncthreads();
-    if (*abort) break;
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    const uint32_t idesc = instr_desc(kRows, nt);
+    bool ok = true;
+    for (int kc = 0; kc < nk; ++kc) {
+      const int s = kc % kStages;
+      if (!mbar_wait(&bs.full[s], static_cast<uint32_t>((kc / kStages) & 1))) {
+        atomicExch(&bs.abort, 1);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t sa = smem_u32(smem + s * sbytes);
+      const uint32_t sb = sa + static_cast<uint32_t>(kRows * kKChunk * 2);
+      const int kw = min(kKChunk, g.K - kc * kKChunk);
+      for (int q = 0; q < kw / 16; ++q) {
+        const uint64_t ad = smem_desc(sa + static_cast<uint32_t>(2 * q * kRows * 16), kRows * 16, 128);
+        const uint64_t bd = smem_desc(sb + static_cast<uint32_t>(2 * q * nt * 16),
+                                      static_cast<uint32_t>(nt) * 16, 128);
+        mma_bf16(tbase, ad, bd, idesc, (kc > 0 || q > 0) ? 1u : 0u);
+      }
+      mma_commit(&bs.empty[s]);
+    }
+    if (ok) mma_commit(&bs.done);
   }
+  __syncwarp();
+  const bool fin = mbar_wait(&bs.done, 0u);
+  if (!fin) atomicExch(&bs.abort, 1);
   tc_fence_after();
-  if (*abort) {
+  __syncthreads();
+  if (bs.abort) {
     if (threadIdx.x == 0 && g.err) atomicCAS(g.err, 0, 1);
     return 0xFFFFFFFFu;
   }
   return tbase;
 }
 
-__device__ __forceinline__ void release(uint32_t* tslot, int ncols) {
+__device__ __forceinline__ void release(Barriers& bs, int ntile) {
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   __syncwarp();
-  if (threadIdx.x < 32) tmem_dealloc(*tslot, static_cast<uint32_t>(ncols));
+  if (threadIdx.x < 32) tmem_dealloc(bs.tslot, static_cast<uint32_t>(tmem_cols(ntile)));
 }
 
 }  // namespace umma

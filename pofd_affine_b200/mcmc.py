@@ -130,6 +130,17 @@ class affineEnsemble:
         check(lib().pofd_ensemble_set_param_limits(self.h, int(i), float(lo),
                                                    float(hi)))
 
+    def setErrorPolicy(self, reject_failures):
+        """False (default): a failed likelihood evaluation stops the run as
+        in the reference; True: the step is rejected and counted."""
+        check(lib().pofd_ensemble_set_error_policy(self.h,
+                                                   1 if reject_failures else 0))
+
+    def getFailures(self):
+        n = C.c_ulonglong()
+        check(lib().pofd_ensemble_failures(self.h, C.byref(n)))
+        return n.value
+
     def setTemperature(self, t):
         check(lib().pofd_ensemble_set_temperature(self.h, float(t)))
 

@@ -20,6 +20,7 @@ def _summary(E, wall, nsteps):
     tmax = float(np.max(tau[finite])) if np.any(finite) else float("nan")
     ess = E.nwalkers * nsteps / tmax if np.isfinite(tmax) else float("nan")
     return {"wall_s": wall, "tau": [float(t) for t in tau], "tau_max": tmax,
+            "failures": E.getFailures(),
             "acor_ok": bool(ok), "ess": ess, "ess_per_s": ess / wall,
             "chain": ch, "logl": cl}
 

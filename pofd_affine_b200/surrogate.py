@@ -130,6 +130,7 @@ class Surrogate:
         return grads, loss.value
 
     def scaling(self):
-        o = np.empty(34)
+        o = np.empty(35)
         check(lib().pofd_surrogate_scaling(self.h, o))
-        return {"mu": o[:16], "isd": o[16:32], "ymax": o[32], "ys": o[33]}
+        return {"mu": o[:16], "isd": o[16:32], "ymax": o[32], "ys": o[33],
+                "clip": o[34]}

@@ -126,3 +126,26 @@ def test_errors_mirror_reference(gpu_ctx):
     E2.initChains(w)
     with pytest.raises(PofdError):
         E2.doSteps(1)
+
+
+def test_error_policy_reject_counts_failures(gpu_ctx):
+    """A likelihood that fails on every proposal (a bonus parameter feeds it
+    NaN): the default stops the run; the reject policy rejects and counts."""
+    from pofd_affine_b200 import PofdError
+    from pofd_affine_b200.mcmc import affineEnsemble, gaussLike
+    mu, cov = _gauss(3)
+    G = gaussLike(gpu_ctx, mu, cov)
+    w0 = np.tile(mu.astype(np.float32), (8, 1))
+    w0 += np.random.default_rng(0).normal(size=w0.shape).astype(np.float32)
+    E = affineEnsemble(gpu_ctx, G, 8, 3, seed=2)
+    E.setParamBonus(2)
+    E.initChains(w0, logl=np.zeros(8))
+    with pytest.raises(PofdError, match="Problem encountered in likelihood"):
+        E.doSteps(1)
+    E2 = affineEnsemble(gpu_ctx, G, 8, 3, seed=2)
+    E2.setParamBonus(2)
+    E2.setErrorPolicy(True)
+    E2.initChains(w0, logl=np.zeros(8))
+    E2.doSteps(5)
+    assert E2.getFailures() == 8 * 5
+    assert np.all(E2.getNAccept() == 0)

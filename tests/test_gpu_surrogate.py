@@ -56,7 +56,7 @@ def test_forward_and_gradients_match_oracle(gpu_ctx):
     sc = S.scaling()
     params = [p.astype(np.float64) for p in S.getParams()]
     x = mlp_oracle.standardise(thp, list(range(k)), sc["mu"], sc["isd"])
-    t = ((ll - sc["ymax"]) / sc["ys"]).astype(np.float32).astype(np.float64)
+    t = (np.maximum(ll - sc["ymax"], -sc["clip"]) / sc["ys"]).astype(np.float32).astype(np.float64)
     og, oloss = mlp_oracle.gradients(params, H, x, t)
     assert abs(loss - oloss) <= 1e-3 * oloss
     for name, a, b in zip(["W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4"], g, og):
