@@ -326,7 +326,7 @@ def mcmc_1d(ctx):
     pick = rng.choice(ch.shape[0], 2000, replace=False)
     hold = (ch[pick], plain["logl"].reshape(-1)[pick])
     S = Surrogate(ctx, npar, list(range(nk)), hidden=256, seed=7)
-    da = runner.run_da(ens(22), S, 200, 500, holdout=hold)
+    da = runner.run_da(ens(22), S, 200, 500, train_iters=1000, holdout=hold)
     return _mcmc_summary("1D plain fit: 6 knots 2-400 mJy, n=4096, one "
                          "256x256 map, 40 walkers, burn 200, 500 steps; MLP "
                          "6 -> 3x256 SiLU -> 1", plain, da, list(range(nk)))
@@ -364,7 +364,7 @@ def mcmc_2d(ctx):
     pick = rng.choice(ch.shape[0], 2000, replace=False)
     hold = (ch[pick], plain["logl"].reshape(-1)[pick])
     S = Surrogate(ctx, npar, list(range(nfree)), hidden=384, seed=9)
-    da = runner.run_da(ens(32), S, 150, 300, holdout=hold)
+    da = runner.run_da(ens(32), S, 150, 300, train_iters=1000, holdout=hold)
     return _mcmc_summary("2D two-field fit: 1500x1500 pair on 2048^2 + "
                          "800x600 pair on 1024^2 in one launch, 14 free "
                          "parameters, 128 walkers, burn 150, 300 steps; MLP "
@@ -373,6 +373,7 @@ def mcmc_2d(ctx):
 
 def _mcmc_summary(name, plain, da, free):
     from pofd_affine_b200 import runner
+    shift = runner.posterior_agreement(da, plain, free)
     keep = ("wall_s", "tau_max", "acor_ok", "ess", "ess_per_s", "stats",
             "failures")
     return {"workload": name,
@@ -382,8 +383,8 @@ def _mcmc_summary(name, plain, da, free):
                        stage2_rate=da["stage2_rate"],
                        surrogate_rms=da.get("surrogate_rms")),
             "ess_per_s_ratio": da["ess_per_s"] / plain["ess_per_s"],
-            "posterior_mean_shift_sigma": runner.posterior_agreement(da, plain,
-                                                                     free)}
+            "posterior_mean_shift_sigma": shift[0],
+            "posterior_mean_shift_se": shift[1]}
 
 
 def main():

@@ -80,7 +80,11 @@ def run_da(E, S, nburn, nsteps, train_iters=2000, batch=512, lr=1e-3,
 
 
 def posterior_agreement(a, b, free):
-    """max over free parameters of |mean_a - mean_b| / sd_b."""
+    """(max over free parameters of |mean_a - mean_b| / sd_b, the same in
+    units of the standard error of the difference sqrt(var_a / ESS_a +
+    var_b / ESS_b))."""
     ca = a["chain"].reshape(-1, a["chain"].shape[-1])[:, free].astype(np.float64)
     cb = b["chain"].reshape(-1, b["chain"].shape[-1])[:, free].astype(np.float64)
-    return float(np.max(np.abs(ca.mean(0) - cb.mean(0)) / cb.std(0)))
+    d = np.abs(ca.mean(0) - cb.mean(0))
+    se = np.sqrt(ca.var(0) / a["ess"] + cb.var(0) / b["ess"])
+    return float(np.max(d / cb.std(0))), float(np.max(d / se))
