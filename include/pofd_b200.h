@@ -451,6 +451,13 @@ int pofd_acor(const float* x, size_t n, double* mean, double* sigma,
  * reference (which has no GPU code). */
 int pofd_fp64_peak(int device, double* tflops);
 
+/* Self-check of the table-driven exp2 the R builders use (2^x = 2^k T[j]
+ * 2^r, T[j] = 2^(j/64), Taylor series for 2^r): the largest relative
+ * difference from the CUDA library exp2 over n arguments in [lo, hi), hi <
+ * 1023 (below -1022 the table function returns 0; the check then reports
+ * its absolute value).  No counterpart in the reference. */
+int pofd_exp2_check(int device, int n, double lo, double hi, double* max_rel);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,6 +56,7 @@ SIGNATURES = {
     "pofd_like1_profile": (I, [V, U, _fp, U, I, _dp, C.POINTER(I)]),
     "pofd_like1_stage_name": (C.c_char_p, [I]),
     "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
+    "pofd_exp2_check": (I, [I, I, D, D, C.POINTER(D)]),
     "pofd_beam2_create": (I, [_dp, _dp, S, D, D, U, PV]),
     "pofd_beam2_destroy": (I, [V]),
     "pofd_beam2_info": (I, [V, _dp]),

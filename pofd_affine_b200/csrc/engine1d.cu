@@ -176,6 +176,8 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
     s_le[i] = sd.lie[i];
     s_ie[i] = sd.ieta[i];
   }
+  __shared__ dev::Exp2Table e2;
+  e2.load();
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= NI) return;
@@ -191,7 +193,7 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
       const double ieta = s_ie[j];
       const double currarg = af * ieta;
       if (currarg < minknot || currarg >= maxknot) continue;
-      const double cts = exp2(counts_log2(s_lk, s_cs, K, lf + s_le[j]));
+      const double cts = dev::exp2_tab(counts_log2(s_lk, s_cs, K, lf + s_le[j]), e2.t);
       if (cts > 0) workval += s_w[j] * cts * ieta;
     }
   }
@@ -310,9 +312,12 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
          const double* __restrict__ spl, double* __restrict__ rbuf,
          double* __restrict__ rpart) {
   __shared__ double shr[32];
+  __shared__ dev::Exp2Table e2;
   const int wb = blockIdx.y;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
+  e2.load();
+  __syncthreads();
   const BSet1Dev& bs = bsets[b];
   const double dflux = bs.dflux;
   const int wrap = bs.wrapRidx;
@@ -344,7 +349,7 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
       const int j = q[k];
       const double delx = cflux - (neg ? x1 : x0)[j];
       const double v = S[j] + delx * (S[NI + j] + delx * (S[2 * NI + j] + delx * S[3 * NI + j]));
-      r = exp2(v) * dflux;
+      r = dev::exp2_tab(v, e2.t) * dflux;
     }
     R[i] = r;
     // moment weights: 0 at i = 0, 1/2 at the positive edge, 1 elsewhere

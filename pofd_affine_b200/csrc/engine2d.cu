@@ -195,9 +195,12 @@ __global__ void __launch_bounds__(NT)
 k_rows2(const BSet2Dev* __restrict__ bsets, Model2Dev m, int B,
         double ilog2toe, const int* __restrict__ mstatus,
         const double* __restrict__ cnt, double* __restrict__ rw) {
+  __shared__ dev::Exp2Table e2;
   const int wb = blockIdx.y;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
+  e2.load();
+  __syncthreads();
   const BSet2Dev& bs = bsets[b];
   const int T = bs.T;
   const long long t = static_cast<long long>(blockIdx.x) * NT + threadIdx.x;
@@ -220,7 +223,7 @@ k_rows2(const BSet2Dev* __restrict__ bsets, Model2Dev m, int B,
         const double f1prod = f1val * ieta1;
         if (f1prod >= m.minknot && f1prod < m.maxknot) {
           const double* cs = cnt + static_cast<size_t>(w) * 12 * KMAX;
-          const double cts = exp2(spline_at(m.logknots, cs, m.K, log2(f1prod)));
+          const double cts = dev::exp2_tab(spline_at(m.logknots, cs, m.K, log2(f1prod)), e2.t);
           if (cts > 0) {
             const double isigma =
                 1.0 / curve_at(m.sk, cs + 4 * KMAX, m.ns, f1prod, true, m.min_sigma);
@@ -312,7 +315,7 @@ __device__ void stage_row(const BSet2Dev& bs, const double* __restrict__ rwrow,
 __device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
                                        const double* s_pos,
                                        const double* s_neg, int npos,
-                                       int nneg, int j) {
+                                       int nneg, int j, const double* tab) {
   if (sgn1 < 0) return 0.0;
   const double if2 = bs.colinv[j];
   if (if2 == 0) return 0.0;
@@ -324,7 +327,7 @@ __device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
   double wv = 0.0;
   for (int k = 0; k < cnt; ++k) {
     const double tfac = lf2 - L[3 * k + 1];
-    wv += L[3 * k] * exp2(tfac * tfac * L[3 * k + 2]);
+    wv += L[3 * k] * dev::exp2_tab(tfac * tfac * L[3 * k + 2], tab);
   }
   return wv * if2;
 }
@@ -343,6 +346,9 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
   const int wb = blockIdx.z;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
+  __shared__ dev::Exp2Table e2;
+  e2.load();
+  __syncthreads();
   const BSet2Dev& bs = bsets[b];
   const int T = bs.T;
   double* s_pos = sm;
@@ -359,7 +365,7 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
     stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
               s_pos, s_neg, s_cnt, sh);
     if (j >= 1 && j < n) {
-      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j) * fluxfac;
+      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j, e2.t) * fluxfac;
       rbuf[(static_cast<size_t>(wb) * n + r) * nc2 + j] = R;
       const double cf1 = bs.rowflux[r];
       const double cR = (r == n - 1) ? 0.5 * R : R;
@@ -399,6 +405,9 @@ k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   const int wb = blockIdx.z;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
+  __shared__ dev::Exp2Table e2;
+  e2.load();
+  __syncthreads();
   const BSet2Dev& bs = bsets[b];
   double* s_pos = sm;
   double* s_neg = sm + 3 * bs.T;
@@ -413,7 +422,7 @@ k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
     stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
               s_pos, s_neg, s_cnt, sh);
     if (j < ncol) {
-      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j);
+      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j, e2.t);
       const double rf = bs.e1[i];
       acc += ((i == 0 || i == nedge - 1) ? 0.5 : 1.0) * rf * R;
     }
@@ -435,6 +444,9 @@ k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   const int wb = blockIdx.y;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
+  __shared__ dev::Exp2Table e2;
+  e2.load();
+  __syncthreads();
   const BSet2Dev& bs = bsets[b];
   const int T = bs.T;
   const int r = blockIdx.x + 1;  // main rows 1..n-1
@@ -446,7 +458,7 @@ k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
             s_pos, s_neg, s_cnt, sh);
   double acc = 0.0;
   for (int jj = threadIdx.x; jj < nedge; jj += NT) {
-    const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], n + jj);
+    const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], n + jj, e2.t);
     acc += (jj == 0 || jj == nedge - 1) ? 0.5 * R : R;
   }
   acc = dev::block_sum<NT>(acc, shr);
@@ -462,9 +474,12 @@ k_rfinish2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
            int edge, int nedge, int ngr, int nparts,
            const int* __restrict__ mstatus, const double* __restrict__ redge,
            const double* __restrict__ epart, const double* __restrict__ rpart,
-           double* __restrict__ rbuf, double* __restrict__ mom) {
+           double* __restrict__ rbuf, double* __restrict__ fpart) {
+  // Edge cells of row 0 and column 0 (all but r[0,0]) for NT columns/rows
+  // per block, their moment contributions plus a slice of k_rgrid2's
+  // partials; r[0,0] and the final sums are k_rfinal2's.
   __shared__ double shr[32];
-  const int wb = blockIdx.x;
+  const int wb = blockIdx.y;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
   const BSet2Dev& bs = bsets[b];
@@ -473,7 +488,62 @@ k_rfinish2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
   double* R = rbuf + static_cast<size_t>(wb) * n * nc2;
   const int ncol = n + nedge;
   const double* ep = epart + static_cast<size_t>(wb) * ngr * ncol;
-  // r[0,0]: trapezoid over the edge columns of the band-1-weighted sums
+  double m1 = 0.0, v1 = 0.0, m2 = 0.0, v2 = 0.0;
+  const int j = blockIdx.x * NT + threadIdx.x;  // row-0 column / column-0 row
+  if (j >= 1 && j < n) {
+    // row 0 (row factor 1/2)
+    double val = 0.0;
+    if (edge) {
+      double c = 0.0;
+      for (int g = 0; g < ngr; ++g) c += ep[static_cast<size_t>(g) * ncol + j];
+      val = c * bs.iRxnorm * fluxfac;
+    }
+    R[j] = val;
+    const double cf1r0 = bs.rowflux[0];
+    const double cR = 0.5 * val;
+    const double wc = (j == n - 1) ? 0.5 : 1.0;
+    const double cf2 = bs.rflux2[j];
+    const double p1 = wc * cf1r0 * cR, p2 = wc * cf2 * cR;
+    m1 += p1; v1 += cf1r0 * p1; m2 += p2; v2 += cf2 * p2;
+    // column 0 (column factor 1/2), row j
+    const double cv = edge ? E[n + j] * fluxfac : 0.0;
+    R[static_cast<size_t>(j) * nc2] = cv;
+    const double cR2 = (j == n - 1) ? 0.5 * cv : cv;
+    const double cf1 = bs.rowflux[j], cf20 = bs.rflux2[0];
+    const double q1 = 0.5 * cf1 * cR2, q2 = 0.5 * cf20 * cR2;
+    m1 += q1; v1 += cf1 * q1; m2 += q2; v2 += cf20 * q2;
+  }
+  const double* pp = rpart + static_cast<size_t>(wb) * nparts * 4;
+  for (int k = j; k < nparts; k += gridDim.x * NT) {
+    m1 += pp[4 * k]; v1 += pp[4 * k + 1]; m2 += pp[4 * k + 2]; v2 += pp[4 * k + 3];
+  }
+  m1 = dev::block_sum<NT>(m1, shr);
+  v1 = dev::block_sum<NT>(v1, shr);
+  m2 = dev::block_sum<NT>(m2, shr);
+  v2 = dev::block_sum<NT>(v2, shr);
+  if (threadIdx.x == 0) {
+    double* o = fpart + (static_cast<size_t>(wb) * gridDim.x + blockIdx.x) * 4;
+    o[0] = m1; o[1] = v1; o[2] = m2; o[3] = v2;
+  }
+}
+
+// r[0,0] (the double edge integral, PDFactoryDouble.cc:426-467), its cell
+// and moment term, the moment sums and the shift decisions
+// (PDFactoryDouble.cc:560-585, 1198-1213); one block per proposal and beam
+// set.
+__global__ void __launch_bounds__(NT)
+k_rfinal2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2, int edge,
+          int nedge, int ngr, int nfp, const int* __restrict__ mstatus,
+          const double* __restrict__ epart, const double* __restrict__ fpart,
+          double* __restrict__ rbuf, double* __restrict__ mom) {
+  __shared__ double shr[32];
+  const int wb = blockIdx.x;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const BSet2Dev& bs = bsets[b];
+  const double fluxfac = bs.dflux1 * bs.dflux2;
+  const int ncol = n + nedge;
+  const double* ep = epart + static_cast<size_t>(wb) * ngr * ncol;
   double r00 = 0.0;
   if (edge) {
     for (int jj = threadIdx.x; jj < nedge; jj += NT) {
@@ -484,46 +554,21 @@ k_rfinish2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
     r00 = dev::block_sum<NT>(r00, shr) * bs.iR00norm;
   }
   double m1 = 0.0, v1 = 0.0, m2 = 0.0, v2 = 0.0;
-  // row 0 (row factor 1/2), all columns
-  const double cf1r0 = bs.rowflux[0];
-  for (int j = threadIdx.x; j < n; j += NT) {
-    double val = 0.0;
-    if (edge) {
-      if (j == 0) {
-        val = r00;
-      } else {
-        double c = 0.0;
-        for (int g = 0; g < ngr; ++g) c += ep[static_cast<size_t>(g) * ncol + j];
-        val = c * bs.iRxnorm;
-      }
-      val *= fluxfac;
-    }
-    R[j] = val;
-    const double cR = 0.5 * val;
-    const double wc = (j == 0 || j == n - 1) ? 0.5 : 1.0;
-    const double cf2 = bs.rflux2[j];
-    const double p1 = wc * cf1r0 * cR, p2 = wc * cf2 * cR;
-    m1 += p1; v1 += cf1r0 * p1; m2 += p2; v2 += cf2 * p2;
-  }
-  // column 0 (column factor 1/2), rows 1..n-1
-  const double cf20 = bs.rflux2[0];
-  for (int i = 1 + threadIdx.x; i < n; i += NT) {
-    const double val = edge ? E[n + i] * fluxfac : 0.0;
-    R[static_cast<size_t>(i) * nc2] = val;
-    const double cR = (i == n - 1) ? 0.5 * val : val;
-    const double cf1 = bs.rowflux[i];
-    const double p1 = 0.5 * cf1 * cR, p2 = 0.5 * cf20 * cR;
-    m1 += p1; v1 += cf1 * p1; m2 += p2; v2 += cf20 * p2;
-  }
-  const double* pp = rpart + static_cast<size_t>(wb) * nparts * 4;
-  for (int k = threadIdx.x; k < nparts; k += NT) {
-    m1 += pp[4 * k]; v1 += pp[4 * k + 1]; m2 += pp[4 * k + 2]; v2 += pp[4 * k + 3];
+  const double* fp = fpart + static_cast<size_t>(wb) * nfp * 4;
+  for (int k = threadIdx.x; k < nfp; k += NT) {
+    m1 += fp[4 * k]; v1 += fp[4 * k + 1]; m2 += fp[4 * k + 2]; v2 += fp[4 * k + 3];
   }
   m1 = dev::block_sum<NT>(m1, shr);
   v1 = dev::block_sum<NT>(v1, shr);
   m2 = dev::block_sum<NT>(m2, shr);
   v2 = dev::block_sum<NT>(v2, shr);
   if (threadIdx.x == 0) {
+    const double val = edge ? r00 * fluxfac : 0.0;
+    rbuf[static_cast<size_t>(wb) * n * nc2] = val;
+    // cell (0, 0): row factor 1/2, column weight 1/2
+    const double cf1 = bs.rowflux[0], cf2 = bs.rflux2[0];
+    const double p1 = 0.5 * cf1 * 0.5 * val, p2 = 0.5 * cf2 * 0.5 * val;
+    m1 += p1; v1 += cf1 * p1; m2 += p2; v2 += cf2 * p2;
     const double s1 = sqrt(v1), s2 = sqrt(v2);
     const bool d1 = (s1 > bs.dflux1) && (fabs(m1) > bs.dflux1);
     const bool d2 = (s2 > bs.dflux2) && (fabs(m2) > bs.dflux2);
@@ -1325,7 +1370,7 @@ void Engine2::build_static() {
 
 void Engine2::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.rw, ws_.rbuf,
-                  ws_.rpart, ws_.redge, ws_.epart, ws_.mom, ws_.pbuf, ws_.rowpart,
+                  ws_.rpart, ws_.redge, ws_.epart, ws_.fpart, ws_.mom, ws_.pbuf, ws_.rowpart,
                   ws_.colpart, ws_.pinfo, ws_.gpart, ws_.pdout,
                   ws_.theta_in, ws_.logl, ws_.status};
   for (void* q : ptrs)
@@ -1363,6 +1408,7 @@ void Engine2::reserve(unsigned P) {
   const size_t ngr = edge_ ? (nedge_ + ER - 1) / ER : 0;
   ws_.epart = dal<double>(static_cast<size_t>(P) * B_ * (ngr ? ngr * (n + nedge_) : 1));
   ws_.mom = dal<double>(static_cast<size_t>(P) * B_ * 8);
+  ws_.fpart = dal<double>(static_cast<size_t>(P) * B_ * ((n + NT - 1) / NT) * 4);
   ws_.pbuf = dal<double>(static_cast<size_t>(P) * D_ * n * nc2);
   ws_.rowpart = dal<double>(static_cast<size_t>(P) * D_ * n * nct_);
   ws_.colpart = dal<double>(static_cast<size_t>(P) * D_ * nrt_ * n);
@@ -1429,9 +1475,15 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
     k_ry2<<<dim3(n - 1, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.redge);
   }
   mark(4);
-  k_rfinish2<<<P * B, NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0, ne, ngr,
-                                   static_cast<int>(gx_ * gy_), ws_.mstatus, ws_.redge,
-                                   ws_.epart, ws_.rpart, ws_.rbuf, ws_.mom);
+  {
+    const int nfp = (n + NT - 1) / NT;
+    k_rfinish2<<<dim3(nfp, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0, ne, ngr,
+                                                static_cast<int>(gx_ * gy_), ws_.mstatus,
+                                                ws_.redge, ws_.epart, ws_.rpart, ws_.rbuf,
+                                                ws_.fpart);
+    k_rfinal2<<<P * B, NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0, ne, ngr, nfp,
+                                    ws_.mstatus, ws_.epart, ws_.fpart, ws_.rbuf, ws_.mom);
+  }
   mark(5);
   if (r_only) {
     ck(cudaGetLastError(), "kernel launch");
@@ -1621,7 +1673,7 @@ void Engine2::profile_stages(unsigned nprop, const float* theta, unsigned npar,
 
 const char* Engine2::stage_name(int i) {
   static const char* names[kNumStages] = {
-      "k_model2", "k_rows2", "k_rgrid2", "k_redge2+k_ry2", "k_rfinish2",
+      "k_model2", "k_rows2", "k_rgrid2", "k_redge2+k_ry2", "k_rfinish2+k_rfinal2",
       "cufft_d2z_2d", "k_spectrum2", "cufft_z2d_2d", "k_pscan2", "k_psplit2",
       "k_pgather2", "k_reduce2"};
   return (i >= 0 && i < kNumStages) ? names[i] : "";

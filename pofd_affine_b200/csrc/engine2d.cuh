@@ -106,7 +106,7 @@ class Engine2 {
   void profile_stages(unsigned nprop, const float* theta, unsigned npar,
                       int reps, double* stage_ms);
   static const char* stage_name(int i);
-  int kernels_per_eval() const { return edge_ ? 11 : 9; }
+  int kernels_per_eval() const { return edge_ ? 12 : 10; }
   unsigned nparams() const {
     return static_cast<unsigned>(knots_.size() + sigk_.size() + offk_.size());
   }
@@ -180,6 +180,7 @@ class Engine2 {
     double* redge = nullptr;    // [P][B][2n+1]: Ry at [n, 2n)
     double* epart = nullptr;    // [P][B][edge row groups][n + nedge]
     double* mom = nullptr;      // [P][B][8]
+    double* fpart = nullptr;    // [P][B][n/256][4] edge-cell moment partials
     double* pbuf = nullptr;     // [P][D][n][2nc]
     double* rowpart = nullptr;  // [P][D][n][nct]
     double* colpart = nullptr;  // [P][D][nrt][n]

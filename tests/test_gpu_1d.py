@@ -203,3 +203,18 @@ def test_two_beam_sets_sum(orc, gpu_ctx):
     lg, sg = G.getLogLikeBatch(thetas)
     assert list(so) == list(sg)
     assert np.max(np.abs(lo - lg)) < LL_TOL
+
+
+def test_table_exp2_against_library(gpu_ctx):
+    """The R builders' table-driven exp2 stays within 4 ulp (~9e-16) of the
+    CUDA library exp2 over the arguments they see, and is exactly 0 below
+    2^-1022."""
+    import ctypes as C
+    from pofd_affine_b200._lib import lib
+    for lo, hi in ((-1022.0, 0.0), (-60.0, 60.0), (-1.0, 1.0), (0.0, 1022.5)):
+        out = C.c_double()
+        assert lib().pofd_exp2_check(0, 1 << 22, lo, hi, C.byref(out)) == 0
+        assert out.value < 9e-16, (lo, hi, out.value)
+    out = C.c_double()
+    assert lib().pofd_exp2_check(0, 1 << 16, -1100.0, -1022.5, C.byref(out)) == 0
+    assert out.value == 0.0
