@@ -193,6 +193,12 @@ def stage_bytes(stage, P, B, D, n):
     compulsory FP64 read/write of each array it streams)."""
     nc = n // 2 + 1
     return {
+        # own FFT path (n = 2m, m complex per row): passes A and B each read
+        # and write the rows; the spectrum reads Z and writes one row per
+        # dataset
+        "k_fftA1+k_fftB1": 32.0 * n * P * B,
+        "k_spectrum1f": 8.0 * n * P * B + 8.0 * n * P * D,
+        "k_fftA1+k_fftB1_inv": 32.0 * n * P * D,
         "k_rfill1": 8.0 * n * P * B,                         # write R
         "k_spectrum1": 16.0 * nc * P * B + 16.0 * nc * P * D,  # read R~, write per-dataset spectra
         "k_pscan1": 8.0 * n * P * D,                          # read P(D)

@@ -170,12 +170,19 @@ int pofd_like1_kernels_per_eval(const pofd_like1* L, int* nkernels);
 /* Per-stage device time of one launch sequence over nprop proposals
  * (host theta), averaged over reps runs timed with CUDA events between the
  * stages: stage_ms[i] for i < *nstages (at most 16), names from
- * pofd_like1_stage_name(i).  Replaces the reference's -DTIMING clock()
+ * pofd_like1_stage_name(L, i).  Replaces the reference's -DTIMING clock()
  * accumulators (PDFactory.cc:93-126). */
 int pofd_like1_profile(pofd_like1* L, unsigned nprop, const float* theta,
                        unsigned npar, int reps, double* stage_ms,
                        int* nstages);
-const char* pofd_like1_stage_name(int i);
+const char* pofd_like1_stage_name(const pofd_like1* L, int i);
+/* Transform used by the likelihood: mode 0 (default) runs this library's own
+ * FP64 four-step FFT, fused with the R-grid fill and the spectrum, when the
+ * FFT size is a power of two in [4096, 131072], and cuFFT otherwise; mode 1
+ * always uses cuFFT.  pofd_like1_fft_info reports whether the own FFT is in
+ * use.  The reference uses FFTW (PDFactory.cc:293-338). */
+int pofd_like1_set_fft(pofd_like1* L, int mode);
+int pofd_like1_fft_info(pofd_like1* L, int* own);
 
 /* ------------------------------------------------------------- 2D beam
  * Replaces doublebeam::doublebeam(file1, file2, histogram, NBINS, MINVAL)

@@ -54,7 +54,9 @@ SIGNATURES = {
     "pofd_like1_rnodes": (I, [V, I, I, _fp, U, _dp, _dp]),
     "pofd_like1_kernels_per_eval": (I, [V, C.POINTER(I)]),
     "pofd_like1_profile": (I, [V, U, _fp, U, I, _dp, C.POINTER(I)]),
-    "pofd_like1_stage_name": (C.c_char_p, [I]),
+    "pofd_like1_stage_name": (C.c_char_p, [V, I]),
+    "pofd_like1_set_fft": (I, [V, I]),
+    "pofd_like1_fft_info": (I, [V, C.POINTER(I)]),
     "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
     "pofd_exp2_check": (I, [I, I, D, D, C.POINTER(D)]),
     "pofd_beam2_create": (I, [_dp, _dp, S, D, D, U, PV]),

@@ -285,8 +285,17 @@ class calcLike:
         ns = C.c_int()
         check(lib().pofd_like1_profile(self.h, nprop, th.ravel(), npar,
                                        int(reps), ms, C.byref(ns)))
-        return {lib().pofd_like1_stage_name(i).decode(): ms[i]
+        return {lib().pofd_like1_stage_name(self.h, i).decode(): ms[i]
                 for i in range(ns.value)}
+
+    def setFFT(self, mode):
+        """0: own FP64 FFT where the size allows (default), 1: cuFFT."""
+        check(lib().pofd_like1_set_fft(self.h, int(mode)))
+
+    def ownFFT(self):
+        v = C.c_int()
+        check(lib().pofd_like1_fft_info(self.h, C.byref(v)))
+        return bool(v.value)
 
     def kernelsPerEval(self):
         k = C.c_int()

@@ -437,7 +437,26 @@ int pofd_like1_profile(pofd_like1* L, unsigned nprop, const float* theta,
   });
 }
 
-const char* pofd_like1_stage_name(int i) { return pofd::Engine1::stage_name(i); }
+const char* pofd_like1_stage_name(const pofd_like1* L, int i) {
+  return (L && L->eng) ? L->eng->stage_name(i) : "";
+}
+
+int pofd_like1_set_fft(pofd_like1* L, int mode) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_fft_mode(mode);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_fft_info(pofd_like1* L, int* own) {
+  return guard([&] {
+    need(L && own, "null argument");
+    if (L->ctx->device >= 0) L->eng->reserve(1);
+    *own = L->eng->own_fft() ? 1 : 0;
+    return POFD_OK;
+  });
+}
 
 // ------------------------------------------------------------- 2D beam
 int pofd_beam2_create(const double* pix1, const double* pix2, size_t npix,

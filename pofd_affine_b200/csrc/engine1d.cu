@@ -27,6 +27,7 @@
 #include <sstream>
 
 #include "common.cuh"
+#include "fft1d.cuh"
 
 namespace pofd {
 
@@ -468,6 +469,215 @@ k_spectrum1(const BSet1Dev* __restrict__ bsets,
   }
 }
 
+// ------------------------------------------------------------------
+// Own FFT path (power-of-two n = 2m, m = m1 * 256, m1 in [8, 512]): the
+// four-step real transform of fft1d.cuh with the R grid fill fused into the
+// forward pass A, the real-transform split / merge fused into the spectrum
+// kernel, and the inverse written straight into the P(D) rows.
+constexpr int FRB = 16;   // rows per pass-B block
+
+// Pass A: L1*L2-point DFTs down CB = 256/L2 columns of the m1 x 256 view
+// (one DFT per thread in each stage), times W_m^{c b}, stored as rows
+// Y[c][b].  Input rows are complex: for the forward transform the R grid
+// itself, whose real values R_{2j}, R_{2j+1} are z_j.
+template <int L1, int L2, int S>
+__global__ void __launch_bounds__(256, 2)
+k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
+       const double2* __restrict__ in, double2* __restrict__ out,
+       const double2* __restrict__ W) {
+  constexpr int M1 = L1 * L2;
+  constexpr int M2 = 256;
+  constexpr int m = M1 * M2;
+  constexpr int CB = 256 / L2;
+  extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b]
+  const int row = blockIdx.y;
+  if (mstatus[row / nrows_per_w] != 0) return;
+  const int b0 = blockIdx.x * CB;
+  const int t = threadIdx.x;
+  const double2* src = in + static_cast<size_t>(row) * rowsz;
+  double2* dst = out + static_cast<size_t>(row) * rowsz;
+  double2 v[L1];
+  {
+    const int b = t % CB, n2 = t / CB;
+#pragma unroll
+    for (int n1 = 0; n1 < L1; ++n1) v[n1] = src[(L2 * n1 + n2) * M2 + b0 + b];
+    fft::dft<L1, S>(v);
+    if (L2 > 1) {
+#pragma unroll
+      for (int k1 = 0; k1 < L1; ++k1) {
+        if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw<S>(W, (m / M1) * n2 * k1));
+        fs[(n2 * L1 + k1) * CB + b] = v[k1];
+      }
+    } else {
+#pragma unroll
+      for (int k1 = 0; k1 < L1; ++k1) {
+        const int bb = b0 + b;
+        dst[k1 * M2 + bb] = (k1 * bb) ? fft::cmul(v[k1], fft::tw<S>(W, k1 * bb)) : v[k1];
+      }
+    }
+  }
+  if (L2 > 1) {
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < L1 / L2; ++it) {
+      const int e = t + 256 * it;
+      const int b = e % CB, k1 = e / CB;
+      double2 u[L2 > 1 ? L2 : 1];
+#pragma unroll
+      for (int n2 = 0; n2 < L2; ++n2) u[n2] = fs[(n2 * L1 + k1) * CB + b];
+      fft::dft<L2, S>(u);
+#pragma unroll
+      for (int k2 = 0; k2 < L2; ++k2) {
+        const int c = k1 + L1 * k2;
+        const int bb = b0 + b;
+        dst[c * M2 + bb] = (c * bb) ? fft::cmul(u[k2], fft::tw<S>(W, c * bb)) : u[k2];
+      }
+    }
+  }
+}
+
+// Pass B: 256-point DFTs along rows c0..c0+15 of Y (16 x 16 split), stored
+// in natural order Z[c + m1 d].
+template <int S>
+__global__ void __launch_bounds__(256, 2)
+k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
+       const double2* __restrict__ in, double2* __restrict__ out,
+       const double2* __restrict__ W) {
+  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r]
+  const int row = blockIdx.y;
+  if (mstatus[row / nrows_per_w] != 0) return;
+  const int rb = min(FRB, m1);
+  const int c0 = blockIdx.x * rb;
+  const int m = m1 * 256;
+  const int t = threadIdx.x;
+  const double2* src = in + static_cast<size_t>(row) * rowsz;
+  double2* dst = out + static_cast<size_t>(row) * rowsz;
+  if (t < 16 * rb) {
+    const int n2 = t & 15, r = t >> 4;
+    double2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) v[n1] = src[(c0 + r) * 256 + 16 * n1 + n2];
+    fft::dft<16, S>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) {
+      if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw<S>(W, (m / 256) * n2 * k1));
+      fs[(k1 * 16 + n2) * 17 + r] = v[k1];
+    }
+  }
+  __syncthreads();
+  if (t < 16 * rb) {
+    const int r = t % rb, k1 = t / rb;
+    double2 u[16];
+#pragma unroll
+    for (int n2 = 0; n2 < 16; ++n2) u[n2] = fs[(k1 * 16 + n2) * 17 + r];
+    fft::dft<16, S>(u);
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) dst[(c0 + r) + m1 * (k1 + 16 * k2)] = u[k2];
+  }
+}
+
+// The spectrum on bin pairs (q, m - q): the real-transform split X from Z,
+// exp(X - X_0) with the mean shift, the noise factor per dataset (bins whose
+// noise exponent is below -750 for every dataset are exactly 0, as in the
+// reference), and the merge Z' of the inverse real transform, written into
+// each dataset's row.  Wn[k] = e^{-2 pi i k / n}, k in [0, m].
+__device__ __forceinline__ bool spec_all_zero(const BSet1Dev& bs, const DSet1Dev* dsets,
+                                              double sm, double wv, int k) {
+  if (k == 0) return false;
+  for (int dd = 0; dd < bs.nds; ++dd) {
+    const double sigma = sm * dsets[bs.ds_begin + dd].sigma_base;
+    if (!(sigma > 0)) return false;
+    const double sigfac = -0.5 * sigma * sigma;
+    if (!(sigfac * wv * wv < -750.0)) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ double2 spec_p(double2 X, double r0, int k, int m, bool doshift,
+                                          double shiftw) {
+  if (k == 0) return make_double2(1.0, 0.0);
+  const double expfac = exp(X.x - r0);
+  const double ival = doshift ? X.y - shiftw * static_cast<double>(k) : X.y;
+  double s, c;
+  sincos(ival, &s, &c);
+  double2 p = make_double2(expfac * c, expfac * s);
+  if (k == m) p.y = 0.0;
+  return p;
+}
+
+__global__ void __launch_bounds__(NT)
+k_spectrum1f(const BSet1Dev* __restrict__ bsets, const DSet1Dev* __restrict__ dsets, int B,
+             int D, int n, int rowsz, const int* __restrict__ mstatus,
+             const double* __restrict__ sigmult, const double* __restrict__ mom,
+             const double2* __restrict__ zbuf, double2* __restrict__ pbuf,
+             const double2* __restrict__ Wn) {
+  const int wb = blockIdx.y;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const int m = n / 2;
+  const int q = blockIdx.x * NT + threadIdx.x;
+  if (q > m / 2) return;
+  const BSet1Dev& bs = bsets[b];
+  const double iflux = dev::kTwoPi / (static_cast<double>(n) * bs.dflux);
+  const double sm = sigmult[w];
+  const double* mo = mom + static_cast<size_t>(wb) * 4;
+  const bool doshift = mo[3] != 0.0;
+  const double shiftw = mo[2] * iflux;
+  const double2* Z = zbuf + static_cast<size_t>(wb) * rowsz;
+  const int ka = q, kb = (q == 0) ? m : m - q;  // bins of the pair
+  const bool za = spec_all_zero(bs, dsets, sm, iflux * ka, ka);
+  const bool zb = spec_all_zero(bs, dsets, sm, iflux * kb, kb);
+  double2 pa = make_double2(0.0, 0.0), pb = make_double2(0.0, 0.0);
+  if (!(za && zb)) {
+    const double2 z0 = Z[0];
+    const double r0 = z0.x + z0.y;  // X_0
+    double2 Xa, Xb;
+    if (q == 0) {
+      Xa = make_double2(r0, 0.0);
+      Xb = make_double2(z0.x - z0.y, 0.0);  // X_m
+    } else {
+      const double2 a = Z[q], c = Z[m - q];
+      // E_k = (Z_k + conj Z_{m-k}) / 2, O_k = (Z_k - conj Z_{m-k}) / (2i)
+      const double2 Ea = make_double2(0.5 * (a.x + c.x), 0.5 * (a.y - c.y));
+      const double2 Oa = make_double2(0.5 * (a.y + c.y), -0.5 * (a.x - c.x));
+      const double2 Eb = make_double2(Ea.x, -Ea.y);
+      const double2 Ob = make_double2(0.5 * (c.y + a.y), -0.5 * (c.x - a.x));
+      Xa = fft::cadd(Ea, fft::cmul(__ldg(Wn + q), Oa));
+      Xb = fft::cadd(Eb, fft::cmul(__ldg(Wn + m - q), Ob));
+    }
+    if (!za) pa = spec_p(Xa, r0, ka, m, doshift, shiftw);
+    if (!zb) pb = spec_p(Xb, r0, kb, m, doshift, shiftw);
+  }
+  for (int dd = 0; dd < bs.nds; ++dd) {
+    const int d = bs.ds_begin + dd;
+    const double sigma = sm * dsets[d].sigma_base;
+    double2 Pa = pa, Pb = pb;
+    if (sigma > 0) {
+      const double sigfac = -0.5 * sigma * sigma;
+      if (ka > 0) {
+        const double wv = iflux * ka;
+        const double ef = exp(sigfac * wv * wv);
+        Pa = make_double2(ef * pa.x, ef * pa.y);
+      }
+      const double wv = iflux * kb;
+      const double ef = exp(sigfac * wv * wv);
+      Pb = make_double2(ef * pb.x, ef * pb.y);
+    }
+    double2* out = pbuf + static_cast<size_t>(w * D + d) * rowsz;
+    // Z'_k = (P_k + conj P_{m-k}) + i (P_k - conj P_{m-k}) e^{+2 pi i k / n}
+    {
+      const double2 e = make_double2(Pa.x + Pb.x, Pa.y - Pb.y);
+      const double2 o = fft::cmul(make_double2(Pa.x - Pb.x, Pa.y + Pb.y), fft::conj(__ldg(Wn + ka)));
+      out[ka] = make_double2(e.x - o.y, e.y + o.x);
+    }
+    if (q != 0 && kb != ka) {
+      const double2 e = make_double2(Pb.x + Pa.x, Pb.y - Pa.y);
+      const double2 o = fft::cmul(make_double2(Pb.x - Pa.x, Pb.y + Pa.y), fft::conj(__ldg(Wn + kb)));
+      out[kb] = make_double2(e.x - o.y, e.y + o.x);
+    }
+  }
+}
+
 struct SplitParams {
   double sgpos, sgneg, n1sigpos, n1signeg;
   long long botidx, topidx;
@@ -815,6 +1025,41 @@ T* dalloc(size_t n) {
 }  // namespace
 
 // ===================================================================== host
+
+namespace {
+constexpr size_t kFftASmem = 256 * 16 * sizeof(double2);  // CB * m1 = 256 * L1
+
+template <int S>
+void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const int* mstatus,
+                 const double2* in, double2* out, const double2* W) {
+#define POFD_FFTA(L1, L2)                                                              \
+  k_fftA<L1, L2, S><<<dim3(L2, rows), 256, kFftASmem, st>>>(rowsz, nrw, mstatus, in, out, W)
+  switch (m1) {
+    case 8: POFD_FFTA(8, 1); break;
+    case 16: POFD_FFTA(16, 1); break;
+    case 32: POFD_FFTA(16, 2); break;
+    case 64: POFD_FFTA(16, 4); break;
+    case 128: POFD_FFTA(16, 8); break;
+    case 256: POFD_FFTA(16, 16); break;
+    default: throw Error(POFD_E_ARG, "own FFT: unsupported size");
+  }
+#undef POFD_FFTA
+}
+
+template <int S>
+void fftA_attr() {
+  const int sm = static_cast<int>(kFftASmem);
+  cuda_check(cudaFuncSetAttribute(k_fftA<8, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftA<16, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftA<16, 2, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftA<16, 4, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftA<16, 8, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftA<16, 16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+}
+
+constexpr size_t kFftBSmem = 16 * 16 * 17 * sizeof(double2);
+}  // namespace
+
 
 Engine1::Engine1(int device, cudaStream_t stream)
     : device_(device), stream_(stream) {}
@@ -1166,6 +1411,27 @@ void Engine1::build_static() {
   cuda_check(cudaMemcpy(d_dsets_, h_dsets_.data(), D_ * sizeof(DSet1Dev), cudaMemcpyHostToDevice), "upload");
   ntile_ = (n_ + TILE - 1) / TILE;
   nchunk_ = (n_ + CHUNK - 1) / CHUNK;
+  // own FFT: n = 2m, m = m1 * 256 with m1 a power of two in [8, 256]
+  own_fft_ = fft_mode_ == 0 && n_ >= 4096 && n_ <= 131072 && (n_ & (n_ - 1)) == 0;
+  if (own_fft_) {
+    const size_t m = n_ / 2;
+    std::vector<double2> wm(m), wn(m + 1);
+    const long double tau = 6.283185307179586476925286766559005768L;
+    for (size_t t = 0; t < m; ++t) {
+      const long double a = -tau * static_cast<long double>(t) / static_cast<long double>(m);
+      wm[t] = make_double2(static_cast<double>(cosl(a)), static_cast<double>(sinl(a)));
+    }
+    for (size_t k = 0; k <= m; ++k) {
+      const long double a = -tau * static_cast<long double>(k) / static_cast<long double>(n_);
+      wn[k] = make_double2(static_cast<double>(cosl(a)), static_cast<double>(sinl(a)));
+    }
+    d_wm_ = dalloc<double2>(m);
+    static_allocs_.push_back(d_wm_);
+    d_wn_ = dalloc<double2>(m + 1);
+    static_allocs_.push_back(d_wn_);
+    cuda_check(cudaMemcpy(d_wm_, wm.data(), m * sizeof(double2), cudaMemcpyHostToDevice), "upload");
+    cuda_check(cudaMemcpy(d_wn_, wn.data(), (m + 1) * sizeof(double2), cudaMemcpyHostToDevice), "upload");
+  }
   static_ok_ = true;
   // shapes changed: old plans/graphs/work space no longer match
   drop_graphs();
@@ -1209,19 +1475,31 @@ void Engine1::profile_stages(unsigned nprop, const float* theta, unsigned npar,
   for (auto& e : ev) cudaEventDestroy(e);
 }
 
-const char* Engine1::stage_name(int i) {
-  static const char* names[kNumStages] = {
+const char* Engine1::stage_name(int i) const {
+  static const char* lib[kNumStages] = {
       "k_model1+k_rnodes1", "k_rspline1", "k_rfill1", "k_moments1",
       "cufft_d2z", "k_spectrum1", "cufft_z2d", "k_pscan1", "k_pfinish1",
       "k_reduce1"};
-  return (i >= 0 && i < kNumStages) ? names[i] : "";
+  static const char* own[kNumStages] = {
+      "k_model1+k_rnodes1", "k_rspline1", "k_rfill1", "k_moments1",
+      "k_fftA1+k_fftB1", "k_spectrum1f", "k_fftA1+k_fftB1_inv", "k_pscan1", "k_pfinish1",
+      "k_reduce1"};
+  if (i < 0 || i >= kNumStages) return "";
+  return own_fft_ ? own[i] : lib[i];
+}
+
+void Engine1::set_fft_mode(int mode) {
+  if (mode != 0 && mode != 1) throw Error(POFD_E_ARG, "fft mode must be 0 (own) or 1 (cuFFT)");
+  if (mode == fft_mode_) return;
+  fft_mode_ = mode;
+  static_ok_ = false;  // rebuilds tables, plans, graphs and work space
 }
 
 void Engine1::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.nodes, ws_.spl,
                   ws_.rbuf, ws_.rpart, ws_.mom, ws_.pbuf, ws_.ppart,
                   ws_.pmidx, ws_.pinfo, ws_.pdout, ws_.theta_in, ws_.logl,
-                  ws_.status};
+                  ws_.status, ws_.tmp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
@@ -1251,6 +1529,15 @@ void Engine1::reserve(unsigned P) {
   ws_.spl = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * 4 * NI);
   ws_.rbuf = dalloc<double>(static_cast<size_t>(P) * B_ * nc2);
   ws_.rpart = dalloc<double>(static_cast<size_t>(P) * B_ * ntile_ * 2);
+  if (own_fft_) {
+    ws_.tmp = dalloc<double>(static_cast<size_t>(P) * std::max(B_, D_) * nc2);
+    fftA_attr<-1>();
+    fftA_attr<1>();
+    cuda_check(cudaFuncSetAttribute(k_fftB<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(kFftBSmem)), "attr");
+    cuda_check(cudaFuncSetAttribute(k_fftB<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(kFftBSmem)), "attr");
+  }
   ws_.mom = dalloc<double>(static_cast<size_t>(P) * B_ * 4);
   ws_.pbuf = dalloc<double>(static_cast<size_t>(P) * D_ * nc2);
   ws_.ppart = dalloc<double>(static_cast<size_t>(P) * D_ * nchunk_ * 4);
@@ -1270,8 +1557,12 @@ void Engine1::reserve(unsigned P) {
 
 void Engine1::ensure_plans(unsigned nprop) {
   auto it = plans_.find(nprop);
-  if (it != plans_.end() && it->second.fwd) return;
+  if (it != plans_.end() && (it->second.fwd || own_fft_)) return;
   Plans pl;
+  if (own_fft_) {  // the own FFT needs no cuFFT plans; the entry holds graphs
+    plans_[nprop] = pl;
+    return;
+  }
   int n = static_cast<int>(n_);
   const int nc = n / 2 + 1;
   int inemb[1] = {2 * nc}, onemb[1] = {nc};
@@ -1283,6 +1574,7 @@ void Engine1::ensure_plans(unsigned nprop) {
   if (grew) drop_graphs();  // captured transforms used the old work area
   plans_[nprop] = pl;
 }
+
 
 void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                          double* logl, int* status, cudaStream_t st,
@@ -1315,30 +1607,62 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                             ws_.nodes, ws_.spl);
   }
   mark(2);
-  {
-    dim3 grid(ntile_, P * B);
-    k_rfill1<<<grid, NT, 0, st>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
-                                  ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+  if (own_fft_) {
+    const int m = n / 2, m1 = m / 256;
+    const int rowsz = nc;  // double2 per row
+    double2* tmp = reinterpret_cast<double2*>(ws_.tmp);
+    double2* rb = reinterpret_cast<double2*>(ws_.rbuf);
+    double2* pb = reinterpret_cast<double2*>(ws_.pbuf);
+    {
+      dim3 grid(ntile_, P * B);
+      k_rfill1<<<grid, NT, 0, st>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+                                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+    }
+    mark(3);
+    k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, B, n, nc2,
+                                                    static_cast<int>(ntile_), P * B,
+                                                    ws_.mstatus, ws_.rbuf, ws_.rpart, ws_.mom);
+    mark(4);
+    const int rb_rows = m1 < FRB ? m1 : FRB;
+    launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wm_);
+    k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, kFftBSmem, st>>>(m1, rowsz, B, ws_.mstatus, tmp,
+                                                                 rb, d_wm_);
+    mark(5);
+    {
+      dim3 grid((m / 2 + 1 + NT - 1) / NT, P * B);
+      k_spectrum1f<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, rowsz, ws_.mstatus,
+                                        ws_.sigmult, ws_.mom, rb, pb, d_wn_);
+    }
+    mark(6);
+    launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wm_);
+    k_fftB<1><<<dim3(m1 / rb_rows, P * D), 256, kFftBSmem, st>>>(m1, rowsz, D, ws_.mstatus, tmp,
+                                                                pb, d_wm_);
+  } else {
+    {
+      dim3 grid(ntile_, P * B);
+      k_rfill1<<<grid, NT, 0, st>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+                                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+    }
+    mark(3);
+    k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, B, n, nc2,
+                                                    static_cast<int>(ntile_), P * B,
+                                                    ws_.mstatus, ws_.rbuf,
+                                                    ws_.rpart, ws_.mom);
+    mark(4);
+    cufft_check(cufftSetStream(pl.fwd, st), "cufftSetStream");
+    cufft_check(cufftExecD2Z(pl.fwd, ws_.rbuf, reinterpret_cast<cufftDoubleComplex*>(ws_.rbuf)),
+                "cufftExecD2Z");
+    mark(5);
+    {
+      dim3 grid((nc + NT - 1) / NT, P * B);
+      k_spectrum1<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc, ws_.mstatus,
+                                       ws_.sigmult, ws_.mom, ws_.rbuf, ws_.pbuf);
+    }
+    mark(6);
+    cufft_check(cufftSetStream(pl.inv, st), "cufftSetStream");
+    cufft_check(cufftExecZ2D(pl.inv, reinterpret_cast<cufftDoubleComplex*>(ws_.pbuf), ws_.pbuf),
+                "cufftExecZ2D");
   }
-  mark(3);
-  k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, B, n, nc2,
-                                                  static_cast<int>(ntile_), P * B,
-                                                  ws_.mstatus, ws_.rbuf,
-                                                  ws_.rpart, ws_.mom);
-  mark(4);
-  cufft_check(cufftSetStream(pl.fwd, st), "cufftSetStream");
-  cufft_check(cufftExecD2Z(pl.fwd, ws_.rbuf, reinterpret_cast<cufftDoubleComplex*>(ws_.rbuf)),
-              "cufftExecD2Z");
-  mark(5);
-  {
-    dim3 grid((nc + NT - 1) / NT, P * B);
-    k_spectrum1<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc, ws_.mstatus,
-                                     ws_.sigmult, ws_.mom, ws_.rbuf, ws_.pbuf);
-  }
-  mark(6);
-  cufft_check(cufftSetStream(pl.inv, st), "cufftSetStream");
-  cufft_check(cufftExecZ2D(pl.inv, reinterpret_cast<cufftDoubleComplex*>(ws_.pbuf), ws_.pbuf),
-              "cufftExecZ2D");
   mark(7);
   {
     dim3 grid(nchunk_, P * D);

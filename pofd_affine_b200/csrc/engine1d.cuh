@@ -91,6 +91,7 @@ struct Workspace1 {
   double* rpart = nullptr;   // [P][B][ntile][2]
   double* mom = nullptr;     // [P][B][4] mean, var, shift, doshift
   double* pbuf = nullptr;    // [P][D][2*(n/2+1)] spectrum / P(D)
+  double* tmp = nullptr;     // [P][max(B,D)][2*(n/2+1)] own-FFT pass-A rows
   double* ppart = nullptr;   // [P][D][nchunk][4] max, sum, wsum, minval
   int* pmidx = nullptr;      // [P][D][nchunk] argmin index
   PDInfo1* pinfo = nullptr;  // [P][D]
@@ -138,11 +139,15 @@ class Engine1 {
   void rnodes_host(int bs, int side, const float* theta, unsigned npar,
                    double* x_out, double* r_out);
   void rgrid_host(int bs, const float* theta, unsigned npar, double* out);
-  int kernels_per_eval() const { return 9; }
+  int kernels_per_eval() const { return own_fft_ ? 13 : 9; }
   static constexpr int kNumStages = 10;
   void profile_stages(unsigned nprop, const float* theta, unsigned npar,
                       int reps, double* stage_ms);
-  static const char* stage_name(int i);
+  const char* stage_name(int i) const;
+  // 0: own FFT where n allows (power of two in [4096, 131072]), else cuFFT;
+  // 1: cuFFT always.
+  void set_fft_mode(int mode);
+  bool own_fft() const { return own_fft_; }
   unsigned fftsize() const { return n_; }
   unsigned nknots() const { return static_cast<unsigned>(knots_.size()); }
 
@@ -206,6 +211,10 @@ class Engine1 {
   void drop_graphs();
   std::map<unsigned, Plans> plans_;
   FftWorkArea fftwork_;
+  int fft_mode_ = 0;
+  bool own_fft_ = false;
+  double2* d_wm_ = nullptr;  // e^{-2 pi i t / m}, t < m
+  double2* d_wn_ = nullptr;  // e^{-2 pi i k / n}, k <= m
 };
 
 }  // namespace pofd
