@@ -51,6 +51,7 @@ typedef struct pofd_like1 pofd_like1;
 typedef struct pofd_pdfactory1 pofd_pdfactory1;
 typedef struct pofd_beam2 pofd_beam2;
 typedef struct pofd_like2 pofd_like2;
+typedef struct pofd_pdfactory2 pofd_pdfactory2;
 
 /* Message of the last error raised on this thread ("" if none). */
 const char* pofd_last_error(void);
@@ -205,12 +206,14 @@ int pofd_beam2_info(const pofd_beam2* b, double* info17);
  * with nedge steps as PDFactoryDouble::initR (PDFactoryDouble.cc:355-585).
  * Parameter layout: knot values, sigma values, offset values, sigma
  * multiplier band 1, band 2 (calcLikeDouble.cc:1217-1218), bonus slots
- * ignored.  Data are always binned (nbins x nbins). */
+ * ignored.  bin_data != 0 bins each dataset nbins x nbins
+ * (fitsDataDouble.cc:557-608, PDDouble.cc:1103-1222); 0 evaluates the
+ * per-pixel likelihood (PDDouble.cc:994-1051). */
 int pofd_like2_create(pofd_ctx* ctx, unsigned nknots, const double* knotpos,
                       unsigned nsigma, const double* sigmapos,
                       unsigned noffset, const double* offsetpos,
                       unsigned fftsize, unsigned nedge, int edge_integ,
-                      unsigned nbins, pofd_like2** out);
+                      int bin_data, unsigned nbins, pofd_like2** out);
 int pofd_like2_destroy(pofd_like2* L);
 int pofd_like2_add_beamset(pofd_like2* L, const pofd_beam2* beam,
                            double exp_conf1, double exp_conf2);
@@ -277,6 +280,27 @@ int pofd_pd1_loglike_noalloc(const double* pofd_dev, unsigned n, double dflux,
                              unsigned nnz, double bincent0, double bindelta,
                              double like_offset, double like_norm,
                              double* out_dev, int* status_dev, void* stream);
+
+/* ------------------------------------------------------- 2D P(D) factory
+ * PDFactoryDouble (PDFactoryDouble.h:142-148): initPD(n, minflux1,
+ * maxflux1, minflux2, maxflux2, model, beam, setEdge) with the log-normal
+ * colour model given as knot positions plus params (knot log10 values, sigma
+ * values, offset values); getPD(sigma1, sigma2, setLog) writes the n x n
+ * unwrapped, normalised P(D) (row-major, band 1 major) and info4 =
+ * {minflux1, dflux1, minflux2, dflux2}; get_r the R grid (x dflux1 dflux2)
+ * the transform sees.  nedge: edge-integral steps (PDFactoryDouble.h:62). */
+int pofd_pdfactory2_create(pofd_ctx* ctx, unsigned nedge, pofd_pdfactory2** out);
+int pofd_pdfactory2_destroy(pofd_pdfactory2* f);
+int pofd_pdfactory2_initpd(pofd_pdfactory2* f, unsigned n, double minflux1,
+                           double maxflux1, double minflux2, double maxflux2,
+                           unsigned nknots, const double* knotpos,
+                           unsigned nsigma, const double* sigmapos,
+                           unsigned noffset, const double* offsetpos,
+                           const float* params, const pofd_beam2* beam,
+                           int setedge);
+int pofd_pdfactory2_getpd(pofd_pdfactory2* f, double sigma1, double sigma2,
+                          int setlog, double* pd_out, double* info4);
+int pofd_pdfactory2_get_r(pofd_pdfactory2* f, double* rvals_out);
 
 /* ------------------------------------------------------------------ MCMC
  * Batched affine-invariant stretch-move ensemble: replaces affineEnsemble

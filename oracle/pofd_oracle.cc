@@ -1288,6 +1288,45 @@ struct PD2 {
     mean2 += minflux2;
     return {mean1, mean2};
   }
+  // PDDouble::getLogLikeUnbinned, log-stored branch (PDDouble.cc:994-1051):
+  // edge tests are inclusive here, unlike the binned form.
+  double logLikeUnbinned(const std::vector<double>& f1, const std::vector<double>& f2) const {
+    const double maxflux1 = minflux1 + static_cast<double>(n1 - 1) * dflux1;
+    const double maxflux2 = minflux2 + static_cast<double>(n2 - 1) * dflux2;
+    const size_t n2n1 = n2 * n1;
+    const double idflux1 = 1.0 / dflux1, idflux2 = 1.0 / dflux2;
+    double loglike = 0.0;
+    for (size_t i = 0; i < f1.size(); ++i) {
+      const double cflux1 = f1[i], cflux2 = f2[i];
+      const double delt1 = (cflux1 - minflux1) * idflux1;
+      const double delt2 = (cflux2 - minflux2) * idflux2;
+      const int idx1 = static_cast<int>(delt1);
+      const int idx2 = static_cast<int>(delt2);
+      const size_t n2idx1 = n2 * static_cast<size_t>(idx1);
+      double iv;
+      if (cflux1 <= minflux1) {
+        if (cflux2 <= minflux2) iv = pd[0];
+        else if (cflux2 >= maxflux2) iv = pd[n2 - 1];
+        else iv = pd[idx2];
+      } else if (cflux1 >= maxflux1) {
+        if (cflux2 <= minflux2) iv = pd[n2n1 - n1];
+        else if (cflux2 >= maxflux2) iv = pd[n2n1 - 1];
+        else iv = pd[n2n1 - n1 + idx2];
+      } else if (cflux2 <= minflux2) {
+        iv = pd[n2idx1];
+      } else if (cflux2 >= maxflux2) {
+        iv = pd[n2idx1 + n2 - 1];
+      } else {
+        const double t = delt1 - static_cast<double>(idx1);
+        const double u = delt2 - static_cast<double>(idx2);
+        const double omu = 1.0 - u, omt = 1.0 - t;
+        const size_t b = n2idx1 + idx2;
+        iv = omt * (omu * pd[b] + u * pd[b + 1]) + t * (omu * pd[b + n2] + u * pd[b + n2 + 1]);
+      }
+      loglike += iv;
+    }
+    return kLog2toe * loglike;
+  }
   double logLikeBinned(const std::vector<unsigned>& bins, unsigned nb1,
                        unsigned nb2, double bc1, double bc2, double bd1,
                        double bd2) const {
@@ -1831,8 +1870,9 @@ struct Like2 {
     for (size_t i = 0; i < s.data.size(); ++i) {
       s.pdfac.getPD(sm1 * s.sb1[i], sm2 * s.sb2[i], s.pd, true);
       const Data2& d = s.data[i];
-      const double cur = s.pd.logLikeBinned(d.bins, d.nbins1, d.nbins2, d.bc1,
-                                            d.bc2, d.bd1, d.bd2);
+      const double cur = d.binned ? s.pd.logLikeBinned(d.bins, d.nbins1, d.nbins2, d.bc1,
+                                                       d.bc2, d.bd1, d.bd2)
+                                  : s.pd.logLikeUnbinned(d.d1, d.d2);
       LogLike += (cur - s.like_offset[i]) / s.like_norm[i];
     }
     return LogLike;
@@ -2266,13 +2306,12 @@ int orc_like2_add_dataset(void* vL, int bs, const double* d1, const double* d2,
   return guard([&] {
     if (bs < 0 || bs >= static_cast<int>(L->sets.size())) throw OrcError(E_ARG, "bad beam set");
     if (nd <= 0) throw OrcError(E_ARG, "No pixels in data");
-    if (!L->bin_data) throw OrcError(E_ARG, "2D oracle supports binned data only");
     BeamSet2& s = L->sets[bs];
     Data2 d;
     d.d1.assign(d1, d1 + nd);
     d.d2.assign(d2, d2 + nd);
     if (meansub) d.meanSubtract();
-    d.applyBinning(L->nbins, L->nbins);
+    if (L->bin_data) d.applyBinning(L->nbins, L->nbins);
     s.data.push_back(std::move(d));
     s.sb1.push_back(sb1); s.sb2.push_back(sb2);
     s.like_offset.push_back(0.0);

@@ -397,11 +397,12 @@ class Counts2:
 
 class Like2:
     def __init__(self, knots, sigmapos, offsetpos, fftsize, nedge=256,
-                 edge_integ=True, nbins=1000):
+                 edge_integ=True, nbins=1000, bin_data=True):
         k, s, o = f64(knots), f64(sigmapos), f64(offsetpos)
         self.fftsize = fftsize
         self.h = lib().orc_like2_new(len(k), k, len(s), s, len(o), o, fftsize,
-                                     nedge, int(edge_integ), 1, nbins)
+                                     nedge, int(edge_integ), int(bool(bin_data)),
+                                     nbins)
         if not self.h:
             raise OracleError(-10, lib().orc_last_error().decode())
 

@@ -7,6 +7,6 @@ calcLikeDouble).
 """
 from ._lib import PofdError  # noqa: F401
 from .api1d import PD, Context, PDFactory, beam, calcLike  # noqa: F401
-from .api2d import calcLikeDouble, doublebeam  # noqa: F401
+from .api2d import PDFactoryDouble, calcLikeDouble, doublebeam  # noqa: F401
 
 __version__ = "0.1.0"

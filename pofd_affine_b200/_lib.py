@@ -62,7 +62,7 @@ SIGNATURES = {
     "pofd_beam2_create": (I, [_dp, _dp, S, D, D, U, PV]),
     "pofd_beam2_destroy": (I, [V]),
     "pofd_beam2_info": (I, [V, _dp]),
-    "pofd_like2_create": (I, [V, U, _dp, U, _dp, U, _dp, U, U, I, U, PV]),
+    "pofd_like2_create": (I, [V, U, _dp, U, _dp, U, _dp, U, U, I, I, U, PV]),
     "pofd_like2_destroy": (I, [V]),
     "pofd_like2_add_beamset": (I, [V, V, D, D]),
     "pofd_like2_add_dataset": (I, [V, I, _dp, _dp, S, I, D, D, D]),
@@ -124,6 +124,11 @@ SIGNATURES = {
     "pofd_likesum_eval_batch_device": (I, [V, U, V, U, V, V, V]),
     "pofd_ensemble_set_error_policy": (I, [V, I]),
     "pofd_ensemble_failures": (I, [V, C.POINTER(C.c_ulonglong)]),
+    "pofd_pdfactory2_create": (I, [V, U, PV]),
+    "pofd_pdfactory2_destroy": (I, [V]),
+    "pofd_pdfactory2_initpd": (I, [V, U, D, D, D, D, U, _dp, U, _dp, U, _dp, _fp, V, I]),
+    "pofd_pdfactory2_getpd": (I, [V, D, D, I, _dp, _dp]),
+    "pofd_pdfactory2_get_r": (I, [V, _dp]),
     "pofd_acor": (I, [_fp, S, C.POINTER(D), C.POINTER(D), C.POINTER(D)]),
 }
 

@@ -1,5 +1,6 @@
 """Python mirror of the reference's 2D (two-band) interfaces.
 
+  * PDFactoryDouble PDFactoryDouble::initPD / getPD (PDFactoryDouble.h:142-148)
   * doublebeam      doublebeam::doublebeam(file1, file2, histogram, NBINS,
                     MINVAL) (doublebeam.h:81) from two in-memory pixel arrays
   * calcLikeDouble  calcLikeDouble (calcLikeDouble.h:192-347) with the
@@ -50,11 +51,49 @@ class doublebeam:
                 "pixsize": o[16]}
 
 
+class PDFactoryDouble:
+    """2D P(D) factory on the GPU (PDFactoryDouble.h)."""
+
+    def __init__(self, ctx, nedge=256):
+        h = C.c_void_p()
+        check(lib().pofd_pdfactory2_create(ctx.h, int(nedge), C.byref(h)))
+        self.h, self.ctx, self.n = h, ctx, 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pofd_pdfactory2_destroy(self.h)
+            self.h = None
+
+    def initPD(self, n, minflux1, maxflux1, minflux2, maxflux2, knotpos,
+               sigmapos, offsetpos, params, bm, setEdge=True):
+        k, sg, o = _f64(knotpos), _f64(sigmapos), _f64(offsetpos)
+        check(lib().pofd_pdfactory2_initpd(
+            self.h, int(n), float(minflux1), float(maxflux1), float(minflux2),
+            float(maxflux2), k.size, k, sg.size, sg, o.size, o, _f32(params),
+            bm.h, int(bool(setEdge))))
+        self.n = int(n)
+        self._beam = bm
+        return True
+
+    def getPD(self, sigma1, sigma2, setLog=True):
+        out = np.empty(self.n * self.n)
+        info = np.empty(4)
+        check(lib().pofd_pdfactory2_getpd(self.h, float(sigma1), float(sigma2),
+                                          int(setLog), out, info))
+        return out.reshape(self.n, self.n), dict(zip(
+            ["minflux1", "dflux1", "minflux2", "dflux2"], info))
+
+    def getR(self):
+        out = np.empty(self.n * self.n)
+        check(lib().pofd_pdfactory2_get_r(self.h, out))
+        return out.reshape(self.n, self.n)
+
+
 class calcLikeDouble:
     """2D likelihood over beam sets and datasets."""
 
     def __init__(self, ctx, knotpos, sigmapos, offsetpos, fftsize=4096,
-                 nedge=256, edge_integ=True, nbins=1000):
+                 nedge=256, edge_integ=True, nbins=1000, bin_data=True):
         self.ctx = ctx
         k, s, o = _f64(knotpos), _f64(sigmapos), _f64(offsetpos)
         self.nmodel = k.size + s.size + o.size
@@ -62,8 +101,8 @@ class calcLikeDouble:
         h = C.c_void_p()
         check(lib().pofd_like2_create(ctx.h, k.size, k, s.size, s, o.size, o,
                                       self.fftsize, int(nedge),
-                                      int(edge_integ), int(nbins),
-                                      C.byref(h)))
+                                      int(edge_integ), int(bool(bin_data)),
+                                      int(nbins), C.byref(h)))
         self.h = h
         self._beams = []
 
@@ -106,10 +145,10 @@ class calcLikeDouble:
                 "like_norm"]
         info = dict(zip(keys, o))
         nb = int(info["nbins"])
-        bins = np.zeros(nb * nb, dtype=np.uint32)
+        bins = np.zeros(max(nb * nb, 1), dtype=np.uint32)
         check(lib().pofd_like2_dataset_info(self.h, int(beamset), int(ds), o,
                                             _lib.ptr(bins)))
-        info["bins"] = bins.reshape(nb, nb)
+        info["bins"] = bins[:nb * nb].reshape(nb, nb)
         return info
 
     def reserve(self, max_batch):

@@ -60,6 +60,14 @@ struct pofd_beam2 {
   pofd::Beam2 b;
 };
 
+struct pofd_pdfactory2 {
+  pofd_ctx* ctx = nullptr;
+  unsigned nedge = 256;
+  std::unique_ptr<pofd::Engine2> eng;
+  std::vector<float> theta;
+  bool inited = false;
+};
+
 struct pofd_like2 {
   pofd_ctx* ctx = nullptr;
   std::unique_ptr<pofd::Engine2> eng;
@@ -497,7 +505,7 @@ int pofd_like2_create(pofd_ctx* ctx, unsigned nknots, const double* knotpos,
                       unsigned nsigma, const double* sigmapos,
                       unsigned noffset, const double* offsetpos,
                       unsigned fftsize, unsigned nedge, int edge_integ,
-                      unsigned nbins, pofd_like2** out) {
+                      int bin_data, unsigned nbins, pofd_like2** out) {
   return guard([&] {
     need(ctx && knotpos && sigmapos && offsetpos && out, "null argument");
     if (ctx->device >= 0) cudaSetDevice(ctx->device);
@@ -505,7 +513,7 @@ int pofd_like2_create(pofd_ctx* ctx, unsigned nknots, const double* knotpos,
     L->ctx = ctx;
     L->eng.reset(new pofd::Engine2(ctx->device, ctx->stream));
     L->eng->configure(nknots, knotpos, nsigma, sigmapos, noffset, offsetpos,
-                      fftsize, nedge, edge_integ != 0, nbins);
+                      fftsize, nedge, edge_integ != 0, bin_data != 0, nbins);
     *out = L.release();
     return POFD_OK;
   });
@@ -1070,6 +1078,90 @@ int pofd_ensemble_failures(pofd_ensemble* e, unsigned long long* n) {
   return guard([&] {
     need(e && n, "null argument");
     *n = e->ens->failures();
+    return POFD_OK;
+  });
+}
+
+// ------------------------------------------------------ 2D P(D) factory
+int pofd_pdfactory2_create(pofd_ctx* ctx, unsigned nedge, pofd_pdfactory2** out) {
+  return guard([&] {
+    need(ctx && out, "null argument");
+    std::unique_ptr<pofd_pdfactory2> f(new pofd_pdfactory2());
+    f->ctx = ctx;
+    f->nedge = nedge;
+    *out = f.release();
+    return POFD_OK;
+  });
+}
+
+int pofd_pdfactory2_destroy(pofd_pdfactory2* f) {
+  if (f && f->ctx && f->ctx->device >= 0) cudaSetDevice(f->ctx->device);
+  delete f;
+  return POFD_OK;
+}
+
+// PDFactoryDouble::initPD argument checks (PDFactoryDouble.cc:1145-1170),
+// then the engine is configured for one beam set with one noise-only
+// dataset and the given ranges.
+int pofd_pdfactory2_initpd(pofd_pdfactory2* f, unsigned n, double minflux1, double maxflux1,
+                           double minflux2, double maxflux2, unsigned nknots,
+                           const double* knotpos, unsigned nsigma, const double* sigmapos,
+                           unsigned noffset, const double* offsetpos, const float* params,
+                           const pofd_beam2* beam, int setedge) {
+  return guard([&] {
+    need(f && knotpos && sigmapos && offsetpos && params && beam, "null argument");
+    if (n == 0) throw pofd::Error(POFD_E_ARG, "Invalid (zero) n");
+    if (maxflux1 <= 0.0) throw pofd::Error(POFD_E_ARG, "Invalid (non-positive) maxflux1");
+    if (maxflux2 <= 0.0) throw pofd::Error(POFD_E_ARG, "Invalid (non-positive) maxflux2");
+    if (minflux1 == maxflux1) throw pofd::Error(POFD_E_ARG, "Invalid range (0) between min/max flux in band 1");
+    if (minflux2 == maxflux2) throw pofd::Error(POFD_E_ARG, "Invalid range (0) between min/max flux in band 2");
+    const unsigned np = nknots + nsigma + noffset;
+    for (unsigned k = 0; k < np; ++k)
+      if (std::isnan(static_cast<double>(params[k])))
+        throw pofd::Error(POFD_E_INVALID_MODEL, "Invalid model");
+    if (f->ctx->device >= 0) cudaSetDevice(f->ctx->device);
+    f->eng.reset(new pofd::Engine2(f->ctx->device, f->ctx->stream));
+    f->eng->configure(nknots, knotpos, nsigma, sigmapos, noffset, offsetpos, n, f->nedge,
+                      setedge != 0, true, 1);
+    const int bs = f->eng->add_beamset(beam->b, 0.0, 0.0);
+    f->eng->add_virtual_dataset(bs, 1.0, 1.0);
+    f->eng->set_rrange_explicit(bs, minflux1, maxflux1, minflux2, maxflux2);
+    f->eng->reserve(1);
+    f->theta.assign(params, params + np);
+    f->theta.push_back(1.0f);  // sigma multipliers; the noise is the dataset's
+    f->theta.push_back(1.0f);
+    f->inited = true;
+    return POFD_OK;
+  });
+}
+
+int pofd_pdfactory2_getpd(pofd_pdfactory2* f, double sigma1, double sigma2, int setlog,
+                          double* pd_out, double* info4) {
+  return guard([&] {
+    need(f && pd_out, "null argument");
+    if (!f->inited) throw pofd::Error(POFD_E_ARG, "Must call initPD first");
+    if (f->ctx->device >= 0) cudaSetDevice(f->ctx->device);
+    double info[16];
+    f->eng->set_virtual_sigma(0, sigma1, sigma2);
+    const int st = f->eng->pd_host(0, 0, f->theta.data(), static_cast<unsigned>(f->theta.size()),
+                                   setlog != 0, pd_out, info);
+    if (info4) {
+      info4[0] = info[10];
+      info4[1] = info[0];
+      info4[2] = info[11];
+      info4[3] = info[1];
+    }
+    if (st != 0) throw pofd::Error(st, "P(D) unwrap failed (split point or mean)");
+    return POFD_OK;
+  });
+}
+
+int pofd_pdfactory2_get_r(pofd_pdfactory2* f, double* rvals_out) {
+  return guard([&] {
+    need(f && rvals_out, "null argument");
+    if (!f->inited) throw pofd::Error(POFD_E_ARG, "Must call initPD first");
+    if (f->ctx->device >= 0) cudaSetDevice(f->ctx->device);
+    f->eng->rgrid_host(0, f->theta.data(), static_cast<unsigned>(f->theta.size()), rvals_out);
     return POFD_OK;
   });
 }

@@ -930,38 +930,72 @@ k_pgather2(const BSet2Dev* __restrict__ bsets,
     const int s1 = in.s1, s2 = in.s2;
     const double itot = in.itot;
     const int e1 = min(ds.nnz, (blockIdx.x + 1) * GCH);
-    for (int e = blockIdx.x * GCH + threadIdx.x; e < e1; e += NT) {
-      const double cnt = ds.nzcnt[e];
-      const double cflux1 = ds.bc1 + static_cast<double>(ds.nzi1[e]) * ds.bd1;
-      const double cflux2 = ds.bc2 + static_cast<double>(ds.nzi2[e]) * ds.bd2;
-      const int idx1 = static_cast<int>((cflux1 - mf1) * id1);
-      const int idx2 = static_cast<int>((cflux2 - mf2) * id2);
-      double iv;
-      if (cflux1 < mf1) {
-        if (cflux2 < mf2) iv = lq2(p, n, nc2, s1, s2, itot, 0, 0);
-        else if (cflux2 > maxflux2) iv = lq2(p, n, nc2, s1, s2, itot, 0, n - 1);
-        else iv = lq2(p, n, nc2, s1, s2, itot, 0, idx2);
-      } else if (cflux1 > maxflux1) {
-        if (cflux2 < mf2) iv = lq2(p, n, nc2, s1, s2, itot, n - 1, 0);
-        else if (cflux2 > maxflux2) iv = lq2(p, n, nc2, s1, s2, itot, n - 1, n - 1);
-        else iv = lq2(p, n, nc2, s1, s2, itot, n - 1, idx2);
-      } else if (cflux2 < mf2) {
-        iv = lq2(p, n, nc2, s1, s2, itot, idx1, 0);
-      } else if (cflux2 > maxflux2) {
-        iv = lq2(p, n, nc2, s1, s2, itot, idx1, n - 1);
-      } else {
-        double t = (cflux1 - mf1) * id1 - static_cast<double>(idx1);
-        double u = (cflux2 - mf2) * id2 - static_cast<double>(idx2);
-        int i1 = idx1, i2 = idx2;
-        if (i1 > n - 2) { i1 = n - 2; t = 1.0; }
-        if (i2 > n - 2) { i2 = n - 2; u = 1.0; }
-        const double omu = 1.0 - u, omt = 1.0 - t;
-        iv = omt * (omu * lq2(p, n, nc2, s1, s2, itot, i1, i2) +
-                    u * lq2(p, n, nc2, s1, s2, itot, i1, i2 + 1)) +
-             t * (omu * lq2(p, n, nc2, s1, s2, itot, i1 + 1, i2) +
-                  u * lq2(p, n, nc2, s1, s2, itot, i1 + 1, i2 + 1));
+    if (!ds.binned) {
+      // PDDouble::getLogLikeUnbinned (PDDouble.cc:994-1051): per pixel,
+      // inclusive edge tests
+      for (int e = blockIdx.x * GCH + threadIdx.x; e < e1; e += NT) {
+        const double cflux1 = ds.f1[e], cflux2 = ds.f2[e];
+        const double delt1 = (cflux1 - mf1) * id1, delt2 = (cflux2 - mf2) * id2;
+        const int idx1 = static_cast<int>(delt1), idx2 = static_cast<int>(delt2);
+        double iv;
+        if (cflux1 <= mf1) {
+          if (cflux2 <= mf2) iv = lq2(p, n, nc2, s1, s2, itot, 0, 0);
+          else if (cflux2 >= maxflux2) iv = lq2(p, n, nc2, s1, s2, itot, 0, n - 1);
+          else iv = lq2(p, n, nc2, s1, s2, itot, 0, idx2);
+        } else if (cflux1 >= maxflux1) {
+          if (cflux2 <= mf2) iv = lq2(p, n, nc2, s1, s2, itot, n - 1, 0);
+          else if (cflux2 >= maxflux2) iv = lq2(p, n, nc2, s1, s2, itot, n - 1, n - 1);
+          else iv = lq2(p, n, nc2, s1, s2, itot, n - 1, idx2);
+        } else if (cflux2 <= mf2) {
+          iv = lq2(p, n, nc2, s1, s2, itot, idx1, 0);
+        } else if (cflux2 >= maxflux2) {
+          iv = lq2(p, n, nc2, s1, s2, itot, idx1, n - 1);
+        } else {
+          const double t = delt1 - static_cast<double>(idx1);
+          const double u = delt2 - static_cast<double>(idx2);
+          const int i1 = min(idx1, n - 2), i2 = min(idx2, n - 2);
+          const double omu = 1.0 - u, omt = 1.0 - t;
+          iv = omt * (omu * lq2(p, n, nc2, s1, s2, itot, i1, i2) +
+                      u * lq2(p, n, nc2, s1, s2, itot, i1, i2 + 1)) +
+               t * (omu * lq2(p, n, nc2, s1, s2, itot, i1 + 1, i2) +
+                    u * lq2(p, n, nc2, s1, s2, itot, i1 + 1, i2 + 1));
+        }
+        acc += iv;
       }
-      acc += cnt * iv;
+    } else {
+      for (int e = blockIdx.x * GCH + threadIdx.x; e < e1; e += NT) {
+        const double cnt = ds.nzcnt[e];
+        const double cflux1 = ds.bc1 + static_cast<double>(ds.nzi1[e]) * ds.bd1;
+        const double cflux2 = ds.bc2 + static_cast<double>(ds.nzi2[e]) * ds.bd2;
+        const int idx1 = static_cast<int>((cflux1 - mf1) * id1);
+        const int idx2 = static_cast<int>((cflux2 - mf2) * id2);
+        double iv;
+        if (cflux1 < mf1) {
+          if (cflux2 < mf2) iv = lq2(p, n, nc2, s1, s2, itot, 0, 0);
+          else if (cflux2 > maxflux2) iv = lq2(p, n, nc2, s1, s2, itot, 0, n - 1);
+          else iv = lq2(p, n, nc2, s1, s2, itot, 0, idx2);
+        } else if (cflux1 > maxflux1) {
+          if (cflux2 < mf2) iv = lq2(p, n, nc2, s1, s2, itot, n - 1, 0);
+          else if (cflux2 > maxflux2) iv = lq2(p, n, nc2, s1, s2, itot, n - 1, n - 1);
+          else iv = lq2(p, n, nc2, s1, s2, itot, n - 1, idx2);
+        } else if (cflux2 < mf2) {
+          iv = lq2(p, n, nc2, s1, s2, itot, idx1, 0);
+        } else if (cflux2 > maxflux2) {
+          iv = lq2(p, n, nc2, s1, s2, itot, idx1, n - 1);
+        } else {
+          double t = (cflux1 - mf1) * id1 - static_cast<double>(idx1);
+          double u = (cflux2 - mf2) * id2 - static_cast<double>(idx2);
+          int i1 = idx1, i2 = idx2;
+          if (i1 > n - 2) { i1 = n - 2; t = 1.0; }
+          if (i2 > n - 2) { i2 = n - 2; u = 1.0; }
+          const double omu = 1.0 - u, omt = 1.0 - t;
+          iv = omt * (omu * lq2(p, n, nc2, s1, s2, itot, i1, i2) +
+                      u * lq2(p, n, nc2, s1, s2, itot, i1, i2 + 1)) +
+               t * (omu * lq2(p, n, nc2, s1, s2, itot, i1 + 1, i2) +
+                    u * lq2(p, n, nc2, s1, s2, itot, i1 + 1, i2 + 1));
+        }
+        acc += cnt * iv;
+      }
     }
   }
   acc = dev::block_sum<NT>(acc, shr);
@@ -1047,7 +1081,7 @@ void Engine2::configure(unsigned nknots, const double* knotpos,
                         unsigned nsigma, const double* sigmapos,
                         unsigned noffset, const double* offsetpos,
                         unsigned fftsize, unsigned nedge, bool edge_integ,
-                        unsigned nbins) {
+                        bool bin_data, unsigned nbins) {
   auto incr = [](unsigned n, const double* v, const char* what) {
     for (unsigned i = 0; i < n; ++i)
       if (!(v[i] > 0) || (i > 0 && !(v[i] > v[i - 1])))
@@ -1071,6 +1105,7 @@ void Engine2::configure(unsigned nknots, const double* knotpos,
   n_ = fftsize;
   nedge_ = nedge;
   edge_ = edge_integ;
+  bin_data_ = bin_data;
   nbins_ = nbins;
   static_ok_ = false;
 }
@@ -1127,7 +1162,7 @@ void Engine2::add_dataset(int bs, const double* d1, const double* d2,
   d.d1.assign(d1, d1 + nd);
   d.d2.assign(d2, d2 + nd);
   if (meansub) d.meanSubtract();
-  d.applyBinning(nbins_, nbins_);
+  if (bin_data_) d.applyBinning(nbins_, nbins_);
   s.data.push_back(std::move(d));
   s.sb1.push_back(sigma1);
   s.sb2.push_back(sigma2);
@@ -1160,6 +1195,47 @@ void Engine2::set_rranges(const float* theta, unsigned npar) {
     if (s.mdf[3] > s.rr[3] && (hs[0] || hs[2])) s.rr[3] = s.mdf[3];
     s.rr_set = true;
   }
+  static_ok_ = false;
+}
+
+void Engine2::add_virtual_dataset(int bs, double sigma1, double sigma2) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size())) throw Error(POFD_E_ARG, "invalid beam set index");
+  HostSet& s = sets_[bs];
+  Data2 d;
+  d.binned = true;
+  s.data.push_back(std::move(d));
+  s.sb1.push_back(sigma1);
+  s.sb2.push_back(sigma2);
+  s.lo.push_back(0.0);
+  s.ln.push_back(1.0);
+  s.maxsb1 = sigma1;
+  s.maxsb2 = sigma2;
+  static_ok_ = false;
+}
+
+void Engine2::set_virtual_sigma(int bs, double sigma1, double sigma2) {
+  HostSet& s = sets_.at(bs);
+  s.sb1.back() = sigma1;
+  s.sb2.back() = sigma2;
+  s.maxsb1 = sigma1;
+  s.maxsb2 = sigma2;
+  if (!static_ok_) return;
+  const int d = h_bsets_[bs].ds_begin + h_bsets_[bs].nds - 1;
+  h_dsets_[d].sb1 = sigma1;
+  h_dsets_[d].sb2 = sigma2;
+  h_bsets_[bs].maxsb1 = sigma1;
+  h_bsets_[bs].maxsb2 = sigma2;
+  ck(cudaMemcpy(d_dsets_ + d, &h_dsets_[d], sizeof(DSet2Dev), cudaMemcpyHostToDevice), "upload");
+  ck(cudaMemcpy(d_bsets_ + bs, &h_bsets_[bs], sizeof(BSet2Dev), cudaMemcpyHostToDevice), "upload");
+}
+
+void Engine2::set_rrange_explicit(int bs, double min1, double max1, double min2, double max2) {
+  HostSet& s = sets_.at(bs);
+  s.rr[0] = min1;
+  s.rr[1] = max1;
+  s.rr[2] = min2;
+  s.rr[3] = max2;
+  s.rr_set = true;
   static_ok_ = false;
 }
 
@@ -1329,17 +1405,25 @@ void Engine2::build_static() {
       dd.like_norm = s.ln[i];
       std::vector<int> i1, i2;
       std::vector<double> c;
-      for (unsigned a = 0; a < d.nbins1; ++a)
-        for (unsigned bb = 0; bb < d.nbins2; ++bb) {
-          const uint32_t v = d.bins[static_cast<size_t>(a) * d.nbins2 + bb];
-          if (v) { i1.push_back(static_cast<int>(a)); i2.push_back(static_cast<int>(bb)); c.push_back(v); }
-        }
-      dd.nnz = static_cast<int>(c.size());
+      dd.binned = d.binned ? 1 : 0;
+      if (d.binned) {
+        for (unsigned a = 0; a < d.nbins1; ++a)
+          for (unsigned bb = 0; bb < d.nbins2; ++bb) {
+            const uint32_t v = d.bins[static_cast<size_t>(a) * d.nbins2 + bb];
+            if (v) { i1.push_back(static_cast<int>(a)); i2.push_back(static_cast<int>(bb)); c.push_back(v); }
+          }
+        dd.nnz = static_cast<int>(c.size());
+        dd.f1 = dd.f2 = nullptr;
+      } else {
+        dd.nnz = static_cast<int>(d.d1.size());
+        dd.f1 = up(d.d1);
+        dd.f2 = up(d.d2);
+      }
       dd.nzi1 = upi(i1);
       dd.nzi2 = upi(i2);
       dd.nzcnt = up(c);
       dd.bc1 = d.bc1; dd.bc2 = d.bc2; dd.bd1 = d.bd1; dd.bd2 = d.bd2;
-      if (c.size() > maxnnz) maxnnz = static_cast<unsigned>(c.size());
+      if (static_cast<unsigned>(dd.nnz) > maxnnz) maxnnz = static_cast<unsigned>(dd.nnz);
       h_dsets_.push_back(dd);
     }
   }

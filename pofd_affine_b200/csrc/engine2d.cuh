@@ -57,10 +57,13 @@ struct BSet2Dev {
 struct DSet2Dev {
   int bs;
   double sb1, sb2, like_offset, like_norm;
-  int nnz;
+  int binned;
+  int nnz;                // non-zero bins (binned) or pixels (unbinned)
   const int* nzi1;
   const int* nzi2;
   const double* nzcnt;
+  const double* f1;       // unbinned pixel fluxes
+  const double* f2;
   double bc1, bc2, bd1, bd2;
 };
 
@@ -87,12 +90,17 @@ class Engine2 {
   void configure(unsigned nknots, const double* knotpos, unsigned nsigma,
                  const double* sigmapos, unsigned noffset,
                  const double* offsetpos, unsigned fftsize, unsigned nedge,
-                 bool edge_integ, unsigned nbins);
+                 bool edge_integ, bool bin_data, unsigned nbins);
   int add_beamset(const Beam2& bm, double exp_conf1, double exp_conf2);
   void add_dataset(int bs, const double* d1, const double* d2, size_t nd,
                    bool meansub, double sigma1, double sigma2,
                    double like_norm);
   void set_rranges(const float* theta, unsigned npar);
+  // P(D) factory use: a dataset without pixels whose noise is set per call,
+  // and explicit R ranges (PDFactoryDouble::initPD / getPD).
+  void add_virtual_dataset(int bs, double sigma1, double sigma2);
+  void set_virtual_sigma(int bs, double sigma1, double sigma2);
+  void set_rrange_explicit(int bs, double min1, double max1, double min2, double max2);
   void rrange(int bs, double* r4) const;
   void dataset_info(int bs, int ds, double* info10, uint32_t* bins) const;
   void reserve(unsigned max_batch);
@@ -153,7 +161,7 @@ class Engine2 {
   cudaStream_t stream_;
   std::vector<double> knots_, sigk_, offk_;
   unsigned n_ = 0, nedge_ = 256, nbins_ = 1000;
-  bool edge_ = true;
+  bool edge_ = true, bin_data_ = true;
   std::vector<HostSet> sets_;
   bool static_ok_ = false;
   std::vector<void*> static_allocs_;

@@ -18,7 +18,7 @@ def _beam2d(beams, name):
 
 def spec2(seed=0, n=256, nedge=64, edge=True, shape=(96, 96), noise=(0.0025,
           0.003), nbins=120, nh=40, beams_pair=None, ps=6.0, minval=1e-6,
-          ndata=1, nsig=3, noff=3):
+          ndata=1, nsig=3, noff=3, bin_data=True):
     """A small two-band fit of the log-normal colour model."""
     from pofd_affine_b200 import synth
     rng = np.random.default_rng(seed)
@@ -39,15 +39,15 @@ def spec2(seed=0, n=256, nedge=64, edge=True, shape=(96, 96), noise=(0.0025,
     th = np.concatenate([kv, sv, ov, [1.0, 1.0]]).astype(np.float32)
     return dict(kp=kp, sk=sk, ok=ok, b1=b1, b2=b2, maps=maps, noise=noise,
                 th=th, n=n, nedge=nedge, edge=edge, nbins=nbins, nh=nh, ps=ps,
-                minval=minval)
+                minval=minval, bin_data=bin_data)
 
 
 def build2(orc, ctx, s):
     from pofd_affine_b200 import calcLikeDouble, doublebeam
     O = orc.Like2(s["kp"], s["sk"], s["ok"], s["n"], s["nedge"], s["edge"],
-                  s["nbins"])
+                  s["nbins"], s["bin_data"])
     G = calcLikeDouble(ctx, s["kp"], s["sk"], s["ok"], s["n"], s["nedge"],
-                       s["edge"], s["nbins"])
+                       s["edge"], s["nbins"], s["bin_data"])
     O.add_beamset(s["b1"], s["b2"], s["ps"], s["minval"], s["nh"] > 0,
                   s["nh"])
     G.addBeamSet(doublebeam(s["b1"], s["b2"], s["ps"], s["nh"] > 0, s["nh"],
@@ -102,11 +102,21 @@ def test_r_grid_and_pd_match_oracle(orc, gpu_ctx, beams, case):
     assert np.max(np.abs(lg[big] - lo[big])) < 1e-9
 
 
-@pytest.mark.parametrize("case", ["hist", "neg", "noedge", "multi"])
+@pytest.mark.parametrize("case", ["hist", "neg", "noedge", "multi",
+                                  "unbinned", "unbinned_neg"])
 def test_loglike_batch_matches_oracle(orc, gpu_ctx, beams, case):
     from pofd_affine_b200 import synth
-    s = spec2(ndata=3, shape=(64, 64)) if case == "multi" else _case(beams,
-                                                                      case)
+    if case == "multi":
+        s = spec2(ndata=3, shape=(64, 64))
+    elif case == "unbinned":
+        s = spec2(bin_data=False, shape=(40, 50))
+    elif case == "unbinned_neg":
+        s = spec2(bin_data=False, shape=(40, 40),
+                  beams_pair=(_beam2d(beams, "band12_0"),
+                              _beam2d(beams, "band12_1")), ps=8.0,
+                  minval=1e-7, nh=30)
+    else:
+        s = _case(beams, case)
     O, G = build2(orc, gpu_ctx, s)
     th = synth.proposals(s["th"], 10, 0.02, rng=6, fixed_last=False)
     th[:, -2:] = 1.0
@@ -170,3 +180,24 @@ def test_device_pointer_entry_point_2d(orc, gpu_ctx):
     torch.cuda.synchronize()
     assert np.array_equal(dll.cpu().numpy(), ref)
     assert np.all(dst.cpu().numpy() == 0)
+
+
+@pytest.mark.parametrize("edge", [True, False])
+def test_pdfactory2_matches_likelihood(orc, gpu_ctx, edge):
+    """PDFactoryDouble on the likelihood's own ranges gives the likelihood's
+    R grid and P(D), which the oracle's PDFactoryDouble reproduces."""
+    from pofd_affine_b200 import PDFactoryDouble, doublebeam
+    s = spec2(seed=11, edge=edge)
+    O, G = build2(orc, gpu_ctx, s)
+    rr = G.getRRange(0)
+    F = PDFactoryDouble(gpu_ctx, s["nedge"])
+    F.initPD(s["n"], rr[0], rr[1], rr[2], rr[3], s["kp"], s["sk"], s["ok"],
+             s["th"][:-2], doublebeam(s["b1"], s["b2"], s["ps"], True, s["nh"],
+                                      s["minval"]), edge)
+    assert np.array_equal(F.getR(), G.getR(0, s["th"]))
+    pf, inf = F.getPD(s["noise"][0], s["noise"][1], setLog=False)
+    pg, ig = G.getPD(0, 0, s["th"], setLog=False)
+    assert np.max(np.abs(pf - pg)) <= 1e-13 * pg.max()
+    assert inf["minflux1"] == ig["pd_minflux1"] and inf["dflux2"] == ig["dflux2"]
+    po, io = O.pd(0, 0, s["th"], setlog=False)
+    assert np.max(np.abs(pf - po)) <= 1e-10 * po.max()

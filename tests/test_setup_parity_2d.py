@@ -86,6 +86,28 @@ def test_rrange_uses_brent_maxflux(orc, host_ctx):
     assert np.array_equal(O.rrange(0), P.getRRange(0))
 
 
+def test_unbinned_ranges_and_info(orc, host_ctx):
+    """Unbinned data: no bins, R ranges from the raw data extremes."""
+    from pofd_affine_b200 import calcLikeDouble, doublebeam, synth
+    g = synth.gaussian_beam(3.0)
+    rng = np.random.default_rng(9)
+    m1 = rng.normal(0, 0.003, 700) + 0.05 * rng.random(700) ** 9
+    m2 = rng.normal(0, 0.004, 700)
+    O = orc.Like2(KNOTS, SIGK, OFFK, 256, 64, True, 50, False)
+    P = calcLikeDouble(host_ctx, KNOTS, SIGK, OFFK, 256, 64, True, 50, False)
+    O.add_beamset(g, g, 6.0, 1e-6, True, 40)
+    P.addBeamSet(doublebeam(g, g, 6.0, True, 40, 1e-6))
+    O.add_dataset(0, m1, m2, 0.003, 0.004)
+    P.addDataset(0, m1, m2, 0.003, 0.004)
+    O.set_rranges(THETA)
+    P.setRRanges(THETA)
+    assert np.array_equal(O.rrange(0), P.getRRange(0))
+    oi, pi = O.dataset_info(0, 0), P.datasetInfo(0, 0)
+    for k in oi:
+        assert oi[k] == pi[k], k
+    assert pi["nbins"] == 0 and pi["bins"].size == 0
+
+
 def test_invalid_configurations_rejected(host_ctx):
     from pofd_affine_b200 import PofdError, calcLikeDouble
     with pytest.raises(PofdError):
