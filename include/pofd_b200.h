@@ -185,6 +185,29 @@ const char* pofd_like1_stage_name(const pofd_like1* L, int i);
 int pofd_like1_set_fft(pofd_like1* L, int mode);
 int pofd_like1_fft_info(pofd_like1* L, int* own);
 
+/* Priors added once to the summed log-likelihood, in the reference's order
+ * (calcLike.cc:918-952): a Gaussian on the sigma multiplier about 1, on <S>
+ * (CFIRB) and on <S^2> (Poisson), then alpha times the log-slope
+ * regularisation penalty (numberCountsKnotsSpline.cc:540-559).  on = 0
+ * unsets a prior.  Replace calcLike::setSigmaPrior / unsetSigmaPrior,
+ * setCFIRBPrior / unsetCFIRBPrior, setPoissonPrior / unsetPoissonPrior and
+ * setRegularizationAlpha (calcLike.h:251-269, calcLike.cc:839-877); widths
+ * must be positive, means and alpha non-negative. */
+int pofd_like1_set_sigma_prior(pofd_like1* L, int on, double width);
+int pofd_like1_set_cfirb_prior(pofd_like1* L, int on, double mean, double sigma);
+int pofd_like1_set_poisson_prior(pofd_like1* L, int on, double mean, double sigma);
+int pofd_like1_set_regularization(pofd_like1* L, double alpha);
+/* Bonus parameters <S> and <S^2> of the model of each host row, out
+ * [nprop][2]: numberCountsKnotsSpline::getFluxPerArea / getFluxSqPerArea
+ * (numberCountsKnotsSpline.cc:300-343), NaN for an invalid model. */
+int pofd_like1_bonus(pofd_like1* L, unsigned nprop, const float* theta,
+                     unsigned npar, double* out);
+/* calcLike::fillBonusParams (calcLike.cc:958-980) on device rows: writes
+ * <S>, <S^2> into theta_dev[i][nknots + 1], [nknots + 2]; npar must be at
+ * least nknots + 3.  Enqueue only. */
+int pofd_like1_fill_bonus_device(pofd_like1* L, unsigned nprop, float* theta_dev,
+                                 unsigned npar, void* stream);
+
 /* ------------------------------------------------------------- 2D beam
  * Replaces doublebeam::doublebeam(file1, file2, histogram, NBINS, MINVAL)
  * (doublebeam.h:81) with two in-memory pixel arrays of npix values each:
@@ -322,6 +345,11 @@ typedef int (*pofd_batch_loglike_fn)(void* like, unsigned nprop,
                                      const float* theta_dev, unsigned npar,
                                      double* logl_dev, int* status_dev,
                                      void* stream);
+/* Bonus-parameter hook: fills the bonus slots of nprop device rows that were
+ * just evaluated (the slave's fillBonusParams after getLogLike,
+ * affineEnsemble.cc:1490-1493).  Enqueue only, on stream. */
+typedef int (*pofd_batch_bonus_fn)(void* like, unsigned nprop, float* theta_dev,
+                                   unsigned npar, void* stream);
 
 typedef struct pofd_ensemble pofd_ensemble;
 
@@ -334,9 +362,14 @@ int pofd_ensemble_create(pofd_ctx* ctx, unsigned nwalkers, unsigned nparams,
 int pofd_ensemble_destroy(pofd_ensemble* e);
 int pofd_ensemble_set_likelihood(pofd_ensemble* e, pofd_batch_loglike_fn fn,
                                  void* like);
-/* Convenience: the 1D / 2D likelihoods of this library. */
+/* Convenience: the 1D / 2D likelihoods of this library.  With nparams >=
+ * nknots + 3 (1D) or the 2D model's count + 6, the bonus slots after the
+ * sigma multipliers are filled on every evaluation, as pofdMCMC /
+ * pofdMCMCDouble::fillBonusParams do. */
 int pofd_ensemble_use_like1(pofd_ensemble* e, pofd_like1* like);
 int pofd_ensemble_use_like2(pofd_ensemble* e, pofd_like2* like);
+/* Bonus hook for a caller's likelihood (fn NULL: none; bonus slots stay NaN). */
+int pofd_ensemble_set_bonus(pofd_ensemble* e, pofd_batch_bonus_fn fn, void* like);
 /* setParamFixed / setParamIgnoreAcor / setParamBonus
  * (affineEnsemble.h:131-140): state is an OR of POFD_PARAM_*. */
 int pofd_ensemble_set_param_state(pofd_ensemble* e, unsigned idx, int state);

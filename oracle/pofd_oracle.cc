@@ -296,6 +296,23 @@ struct Counts1 {
     }
     return prefac * retval;
   }
+  // numberCountsKnotsSpline::differenceRegularize (numberCountsKnotsSpline.cc:
+  // 540-559): minus alpha times the spread of the log2-log2 slopes.
+  double differenceRegularize(double alpha) const {
+    const size_t nk = knots.size();
+    if (nk < 2) return 0.0;
+    double mean_deriv = 0.0;
+    for (size_t i = 1; i < nk; ++i)
+      mean_deriv += (logknotvals[i] - logknotvals[i - 1]) / (logknots[i] - logknots[i - 1]);
+    mean_deriv /= static_cast<double>(nk - 1);
+    double pen = 0.0;
+    for (size_t i = 1; i < nk; ++i) {
+      const double d = (logknotvals[i] - logknotvals[i - 1]) / (logknots[i] - logknots[i - 1]) -
+                       mean_deriv;
+      pen -= d * d;
+    }
+    return alpha * pen;
+  }
   // Integral of S^alpha dN/dS over the knot range
   // (numberCountsKnotsSpline.cc:300-343 integrates the same function with
   // adaptive GK41 to epsrel 1e-5; here a fixed high-order Gauss-Legendre
@@ -764,6 +781,11 @@ struct Like1 {
   bool bin_data = true;
   Counts1 model;
   std::vector<BeamSet1> sets;
+  // priors and regularisation (calcLike.h:96-116)
+  bool has_sigma_prior = false, has_cfirb_prior = false, has_poisson_prior = false;
+  double sigma_prior_width = 0, cfirb_prior_mean = 0, cfirb_prior_sigma = 0;
+  double poisson_prior_mean = 0, poisson_prior_sigma = 0, regularization_alpha = 0;
+  double mean_flux_per_area = kNaN, mean_fluxsq_per_area = kNaN;
 
   void refreshSet(BeamSet1& s) {
     s.maxsigma_base = s.sigma_base[0];
@@ -829,6 +851,23 @@ struct Like1 {
     const double sigmult = p[nknots];
     double LogLike = 0.0;
     for (auto& s : sets) LogLike += singleLogLike(s, sigmult);
+    // priors, bonus parameters and regularisation (calcLike.cc:918-952)
+    const double half_log_2pi = 0.918938517570495605469;
+    if (has_sigma_prior) {
+      const double val = (sigmult - 1.0) / sigma_prior_width;
+      LogLike -= half_log_2pi + std::log(sigma_prior_width) + 0.5 * val * val;
+    }
+    mean_flux_per_area = model.splineInt(1.0);
+    if (has_cfirb_prior) {
+      const double val = (cfirb_prior_mean - mean_flux_per_area) / cfirb_prior_sigma;
+      LogLike -= half_log_2pi + std::log(cfirb_prior_sigma) + 0.5 * val * val;
+    }
+    mean_fluxsq_per_area = model.splineInt(2.0);
+    if (has_poisson_prior) {
+      const double val = (poisson_prior_mean - mean_fluxsq_per_area) / poisson_prior_sigma;
+      LogLike -= half_log_2pi + std::log(poisson_prior_sigma) + 0.5 * val * val;
+    }
+    if (regularization_alpha > 0.0) LogLike += model.differenceRegularize(regularization_alpha);
     return LogLike;
   }
 };
@@ -2112,6 +2151,28 @@ int orc_like1_dataset_bins(void* vL, int bs, int ds, uint32_t* out) {
   const Data1& d = L->sets.at(bs).data.at(ds);
   std::copy(d.bins.begin(), d.bins.end(), out);
   return 0;
+}
+int orc_like1_set_priors(void* vL, const double* p9) {
+  Like1* L = static_cast<Like1*>(vL);
+  L->pool.clear();
+  L->has_sigma_prior = p9[0] != 0.0;
+  L->sigma_prior_width = p9[1];
+  L->has_cfirb_prior = p9[2] != 0.0;
+  L->cfirb_prior_mean = p9[3];
+  L->cfirb_prior_sigma = p9[4];
+  L->has_poisson_prior = p9[5] != 0.0;
+  L->poisson_prior_mean = p9[6];
+  L->poisson_prior_sigma = p9[7];
+  L->regularization_alpha = p9[8];
+  return 0;
+}
+int orc_like1_bonus(void* vL, const float* theta, int npar, double* out2) {
+  Like1* L = static_cast<Like1*>(vL);
+  return guard([&] {
+    L->model.setParams(theta, npar);
+    out2[0] = L->model.splineInt(1.0);
+    out2[1] = L->model.splineInt(2.0);
+  });
 }
 int orc_like1_eval(void* vL, const float* theta, int npar, double* logl) {
   return guard([&] { *logl = static_cast<Like1*>(vL)->getLogLike(theta, npar); });

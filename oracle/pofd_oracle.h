@@ -141,6 +141,12 @@ int orc_like2_eval_batch(void* L, int nprop, const float* theta, int npar,
                          double* logl, int* status, int nthreads);
 /* dbg: [dflux1, dflux2, mn1, mn2, var1, var2, shift1, shift2, split1,
  *       split2, pd_minflux1, pd_minflux2, sg1pos, sg1neg, sg2pos, sg2neg] */
+/* priors: p9 = {has_sigma_prior, sigma_prior_width, has_cfirb_prior,
+ * cfirb_mean, cfirb_sigma, has_poisson_prior, poisson_mean, poisson_sigma,
+ * regularization_alpha} (calcLike.h:184-195) */
+int orc_like1_set_priors(void* L, const double* p9);
+/* bonus parameters <S>, <S^2> of the model at theta */
+int orc_like1_bonus(void* L, const float* theta, int npar, double* out2);
 int orc_like2_pd(void* L, int beamset, int ds, const float* theta, int npar,
                  int setlog, double* pd_out, double* dbg16,
                  double* rvals_out);

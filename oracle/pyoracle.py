@@ -58,6 +58,8 @@ def lib():
         "orc_like1_dataset_info": (I, [V, I, I, _dp]),
         "orc_like1_dataset_bins": (I, [V, I, I, _up]),
         "orc_like1_eval": (I, [V, _fp, I, _dp]),
+        "orc_like1_set_priors": (I, [V, _dp]),
+        "orc_like1_bonus": (I, [V, _fp, I, _dp]),
         "orc_like1_eval_batch": (I, [V, I, _fp, I, _dp, _ip, I]),
         "orc_like1_pd": (I, [V, I, I, _fp, I, I, _dp, P, P]),
         "orc_like1_rinterp": (I, [V, I, _fp, I, I, _dp, _dp]),
@@ -274,6 +276,27 @@ class Like1:
         out = np.empty(1)
         _chk(lib().orc_like1_eval(self.h, th, len(th), out))
         return out[0]
+
+    def set_priors(self, sigma=None, cfirb=None, poisson=None, alpha=0.0):
+        """sigma: prior width on the sigma multiplier; cfirb, poisson:
+        (mean, sigma) on <S> and <S^2>; alpha: regularisation multiplier
+        (calcLike.h:184-195).  None turns a prior off."""
+        v = np.zeros(9)
+        if sigma is not None:
+            v[0], v[1] = 1.0, sigma
+        if cfirb is not None:
+            v[2], v[3], v[4] = 1.0, cfirb[0], cfirb[1]
+        if poisson is not None:
+            v[5], v[6], v[7] = 1.0, poisson[0], poisson[1]
+        v[8] = alpha
+        _chk(lib().orc_like1_set_priors(self.h, v))
+
+    def bonus(self, theta):
+        """<S> and <S^2> of the model at theta (calcLike.cc:958-980)."""
+        th = f32(theta)
+        out = np.empty(2)
+        _chk(lib().orc_like1_bonus(self.h, th, len(th), out))
+        return out
 
     def loglike_batch(self, thetas, nthreads=1):
         th = f32(thetas)

@@ -57,6 +57,12 @@ SIGNATURES = {
     "pofd_like1_stage_name": (C.c_char_p, [V, I]),
     "pofd_like1_set_fft": (I, [V, I]),
     "pofd_like1_fft_info": (I, [V, C.POINTER(I)]),
+    "pofd_like1_set_sigma_prior": (I, [V, I, D]),
+    "pofd_like1_set_cfirb_prior": (I, [V, I, D, D]),
+    "pofd_like1_set_poisson_prior": (I, [V, I, D, D]),
+    "pofd_like1_set_regularization": (I, [V, D]),
+    "pofd_like1_bonus": (I, [V, U, _fp, U, _dp]),
+    "pofd_like1_fill_bonus_device": (I, [V, U, V, U, V]),
     "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
     "pofd_exp2_check": (I, [I, I, D, D, C.POINTER(D)]),
     "pofd_beam2_create": (I, [_dp, _dp, S, D, D, U, PV]),
@@ -84,6 +90,7 @@ SIGNATURES = {
     "pofd_ensemble_destroy": (I, [V]),
     "pofd_ensemble_set_likelihood": (I, [V, V, V]),
     "pofd_ensemble_use_like1": (I, [V, V]),
+    "pofd_ensemble_set_bonus": (I, [V, V, V]),
     "pofd_ensemble_use_like2": (I, [V, V]),
     "pofd_ensemble_set_param_state": (I, [V, U, I]),
     "pofd_ensemble_set_param_limits": (I, [V, U, C.c_float, C.c_float]),

@@ -288,6 +288,57 @@ class calcLike:
         return {lib().pofd_like1_stage_name(self.h, i).decode(): ms[i]
                 for i in range(ns.value)}
 
+    # priors (calcLike.h:251-269): added once to the summed log-likelihood
+    def setSigmaPrior(self, width):
+        check(lib().pofd_like1_set_sigma_prior(self.h, 1, float(width)))
+
+    def unsetSigmaPrior(self):
+        check(lib().pofd_like1_set_sigma_prior(self.h, 0, 0.0))
+
+    def setCFIRBPrior(self, mean, sigma):
+        check(lib().pofd_like1_set_cfirb_prior(self.h, 1, float(mean),
+                                               float(sigma)))
+
+    def unsetCFIRBPrior(self):
+        check(lib().pofd_like1_set_cfirb_prior(self.h, 0, 0.0, 0.0))
+
+    def setPoissonPrior(self, mean, sigma):
+        check(lib().pofd_like1_set_poisson_prior(self.h, 1, float(mean),
+                                                 float(sigma)))
+
+    def unsetPoissonPrior(self):
+        check(lib().pofd_like1_set_poisson_prior(self.h, 0, 0.0, 0.0))
+
+    def setRegularizationAlpha(self, alpha):
+        check(lib().pofd_like1_set_regularization(self.h, float(alpha)))
+
+    def getBonus(self, thetas):
+        """<S>, <S^2> (numberCountsKnotsSpline::getFluxPerArea /
+        getFluxSqPerArea) of each row: [nprop, 2]."""
+        th = _f32(thetas)
+        if th.ndim == 1:
+            th = th[None, :]
+        th = np.ascontiguousarray(th)
+        out = np.empty((th.shape[0], 2))
+        check(lib().pofd_like1_bonus(self.h, th.shape[0], th.ravel(),
+                                     th.shape[1], out.ravel()))
+        return out
+
+    def fillBonusParams(self, thetas):
+        """calcLike::fillBonusParams on rows with nknots + 3 or more
+        entries: a copy with <S>, <S^2> after the sigma multiplier (float,
+        as the reference's paramSet holds them)."""
+        th = np.array(_f32(thetas), copy=True)
+        one = th.ndim == 1
+        if one:
+            th = th[None, :]
+        k = len(self.knotpos)
+        if th.shape[1] < k + 3:
+            raise PofdError(-10, "Not enough room to fill")
+        b = self.getBonus(th)
+        th[:, k + 1:k + 3] = b.astype(np.float32)
+        return th[0] if one else th
+
     def setFFT(self, mode):
         """0: own FP64 FFT where the size allows (default), 1: cuFFT."""
         check(lib().pofd_like1_set_fft(self.h, int(mode)))

@@ -466,6 +466,60 @@ int pofd_like1_fft_info(pofd_like1* L, int* own) {
   });
 }
 
+int pofd_like1_set_sigma_prior(pofd_like1* L, int on, double width) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_sigma_prior(on != 0, width);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_set_cfirb_prior(pofd_like1* L, int on, double mean, double sigma) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_cfirb_prior(on != 0, mean, sigma);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_set_poisson_prior(pofd_like1* L, int on, double mean, double sigma) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_poisson_prior(on != 0, mean, sigma);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_set_regularization(pofd_like1* L, double alpha) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_regularization(alpha);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_bonus(pofd_like1* L, unsigned nprop, const float* theta, unsigned npar,
+                     double* out) {
+  return guard([&] {
+    need(L && theta && out, "null argument");
+    need(L->ctx->device >= 0, "host-only context has no GPU");
+    cudaSetDevice(L->ctx->device);
+    L->eng->bonus_host(nprop, theta, npar, out);
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_fill_bonus_device(pofd_like1* L, unsigned nprop, float* theta_dev,
+                                 unsigned npar, void* stream) {
+  return guard([&] {
+    need(L && theta_dev, "null argument");
+    need(L->ctx->device >= 0, "host-only context has no GPU");
+    cudaSetDevice(L->ctx->device);
+    L->eng->fill_bonus(nprop, theta_dev, npar, static_cast<cudaStream_t>(stream));
+    return POFD_OK;
+  });
+}
+
 // ------------------------------------------------------------- 2D beam
 int pofd_beam2_create(const double* pix1, const double* pix2, size_t npix,
                       double pixsize, double minval, unsigned nhist,
@@ -657,6 +711,9 @@ static int like1_batch(void* like, unsigned nprop, const float* theta,
   return pofd_like1_eval_batch_device(static_cast<pofd_like1*>(like), nprop, theta, npar, logl,
                                       status, stream);
 }
+static int like1_fill(void* like, unsigned nprop, float* theta, unsigned npar, void* stream) {
+  return pofd_like1_fill_bonus_device(static_cast<pofd_like1*>(like), nprop, theta, npar, stream);
+}
 static int like2_batch(void* like, unsigned nprop, const float* theta,
                        unsigned npar, double* logl, int* status, void* stream) {
   return pofd_like2_eval_batch_device(static_cast<pofd_like2*>(like), nprop, theta, npar, logl,
@@ -695,6 +752,20 @@ int pofd_ensemble_use_like1(pofd_ensemble* e, pofd_like1* like) {
   return guard([&] {
     need(e && like, "null argument");
     e->ens->set_like(like1_batch, like);
+    // bonus slots after the knots and the sigma multiplier are filled when
+    // the parameter vector has room for them (pofdMCMC.cc:354-360)
+    if (e->ens->npar() >= like->eng->nknots() + 3)
+      e->ens->set_bonus(like1_fill, like);
+    else
+      e->ens->set_bonus(nullptr, nullptr);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_set_bonus(pofd_ensemble* e, pofd_batch_bonus_fn fn, void* like) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->set_bonus(fn, like);
     return POFD_OK;
   });
 }

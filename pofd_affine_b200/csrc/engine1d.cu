@@ -977,7 +977,8 @@ k_pfinish1(const BSet1Dev* __restrict__ bsets,
 __global__ void k_reduce1(const BSet1Dev* __restrict__ bsets, int B, int D,
                           int nprop, const int* __restrict__ mstatus,
                           const double* __restrict__ sigmult,
-                          const PDInfo1* __restrict__ pinfo,
+                          const PDInfo1* __restrict__ pinfo, Prior1 pr,
+                          const double* __restrict__ bonus,
                           double* __restrict__ logl, int* __restrict__ status) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= nprop) return;
@@ -1000,8 +1001,117 @@ __global__ void k_reduce1(const BSet1Dev* __restrict__ bsets, int B, int D,
     }
     LogLike += s;
   }
+  // priors, once for all data sets (calcLike.cc:918-952)
+  constexpr double half_log_2pi = 0.918938517570495605469;
+  if (pr.has_sigma) {
+    const double val = (sm - 1.0) / pr.sigma_width;
+    LogLike -= half_log_2pi + pr.log_sigma_width + 0.5 * val * val;
+  }
+  if (pr.has_cfirb) {
+    const double val = (pr.cfirb_mean - bonus[4 * static_cast<size_t>(w)]) / pr.cfirb_sigma;
+    LogLike -= half_log_2pi + pr.log_cfirb_sigma + 0.5 * val * val;
+  }
+  if (pr.has_poisson) {
+    const double val = (pr.poisson_mean - bonus[4 * static_cast<size_t>(w) + 1]) / pr.poisson_sigma;
+    LogLike -= half_log_2pi + pr.log_poisson_sigma + 0.5 * val * val;
+  }
+  if (pr.alpha > 0.0) LogLike += pr.alpha * bonus[4 * static_cast<size_t>(w) + 2];
   status[w] = st;
   logl[w] = (st == 0) ? LogLike : __longlong_as_double(0x7ff8000000000000LL);
+}
+
+// Bonus integrals and the slope penalty of each proposal's knot model, one
+// block per proposal.  <S> and <S^2> are the integrals of S dN/dS and
+// S^2 dN/dS over [S_0, S_{K-1}) (numberCountsKnotsSpline.cc:300-343, the
+// integrand of numberCountsKnotsSpline.cc:646-670), by Gauss-Legendre
+// quadrature in u = log2 S on host-built nodes: the integrand
+// s^{a+1} 2^{spline(u)} is smooth inside each knot interval.  The penalty is
+// minus the sum of squared deviations of the log2-log2 knot slopes from their
+// mean (numberCountsKnotsSpline.cc:540-559), before the factor alpha.
+// out[w][4] = {<S>, <S^2>, penalty, 0}, NaN for an invalid model.  With cnt
+// the spline comes from the model kernel of the same batch; without it the
+// block solves it.  fill_at >= 0 also stores <S>, <S^2> as floats in
+// theta[w][fill_at .. fill_at + 1] (fillBonusParams, calcLike.cc:958-980).
+constexpr int kBonusThreads = 256;
+__global__ void __launch_bounds__(kBonusThreads)
+k_bonus1(Model1Dev m, float* theta, int npar, double logfac,
+         const double* __restrict__ cnt, const int* __restrict__ mstatus,
+         const double* __restrict__ qu, const double* __restrict__ qs,
+         const double* __restrict__ qw, int nper, double* __restrict__ out,
+         int fill_at) {
+  __shared__ double cs[4 * KMAX];
+  __shared__ double lk[KMAX];
+  __shared__ double wk[8 * KMAX];
+  __shared__ double red[2][kBonusThreads / 32];
+  __shared__ int sst;
+  const int w = blockIdx.x;
+  const int K = m.K;
+  const float* th = theta + static_cast<size_t>(w) * npar;
+  for (int i = threadIdx.x; i < K; i += blockDim.x) lk[i] = m.logknots[i];
+  if (threadIdx.x == 0) sst = cnt ? mstatus[w] : model_solve(m, th, logfac, cs, wk);
+  __syncthreads();
+  if (cnt && sst == 0)
+    for (int i = threadIdx.x; i < 4 * (K - 1); i += blockDim.x)
+      cs[i] = cnt[static_cast<size_t>(w) * 4 * KMAX + i];
+  __syncthreads();
+  double s1 = 0.0, s2 = 0.0;
+  if (sst == 0) {
+    const int nq = (K - 1) * nper;
+    for (int j = threadIdx.x; j < nq; j += blockDim.x) {
+      const int k = j / nper;
+      const double d = qu[j] - lk[k];
+      const double* q = cs + 4 * k;
+      const double S = qs[j];
+      const double a = qw[j] * S * S * exp2(q[0] + d * (q[1] + d * (q[2] + d * q[3])));
+      s1 += a;
+      s2 += a * S;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_down_sync(0xffffffffu, s1, o);
+    s2 += __shfl_down_sync(0xffffffffu, s2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = s1;
+    red[1][threadIdx.x >> 5] = s2;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+  double t1 = 0.0, t2 = 0.0, pen = 0.0;
+  for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) {
+    t1 += red[0][i];
+    t2 += red[1][i];
+  }
+  if (sst != 0 || K < 2) {
+    t1 = t2 = qnan;
+    pen = (sst != 0) ? qnan : 0.0;
+  } else {
+    double mean_deriv = 0.0;
+    for (int i = 1; i < K; ++i)
+      mean_deriv += (logfac * static_cast<double>(th[i]) -
+                     logfac * static_cast<double>(th[i - 1])) / (lk[i] - lk[i - 1]);
+    mean_deriv /= static_cast<double>(K - 1);
+    for (int i = 1; i < K; ++i) {
+      const double dl = (logfac * static_cast<double>(th[i]) -
+                         logfac * static_cast<double>(th[i - 1])) / (lk[i] - lk[i - 1]) -
+                        mean_deriv;
+      pen -= dl * dl;
+    }
+  }
+  if (out) {
+    double* o = out + 4 * static_cast<size_t>(w);
+    o[0] = t1;
+    o[1] = t2;
+    o[2] = pen;
+    o[3] = 0.0;
+  }
+  if (fill_at >= 0) {
+    float* tw = theta + static_cast<size_t>(w) * npar;
+    tw[fill_at] = static_cast<float>(t1);
+    tw[fill_at + 1] = static_cast<float>(t2);
+  }
 }
 
 // The unwrapped, normalised (optionally log2) P(D) of one row.
@@ -1263,6 +1373,15 @@ void Engine1::build_static() {
   model_.logknots = up(lk);
   model_.minknot = knots_.front();
   model_.maxknot = knots_.back();
+  {
+    // 64 panels of 20 points per knot interval
+    KnotQuadrature kq;
+    kq.build(lk.data(), static_cast<int>(K), 64, 20);
+    d_qu_ = up(kq.u);
+    d_qs_ = up(kq.s);
+    d_qw_ = up(kq.w);
+    qper_ = kq.nper;
+  }
 
   B_ = static_cast<unsigned>(sets_.size());
   maxterms_ = 1;
@@ -1488,6 +1607,90 @@ const char* Engine1::stage_name(int i) const {
   return own_fft_ ? own[i] : lib[i];
 }
 
+// Prior setters (calcLike.h:251-269, calcLike.cc:839-877).  The prior
+// values are launch arguments of the reduction kernel, so captured graphs
+// are dropped.
+void Engine1::set_sigma_prior(bool on, double width) {
+  if (on && !(width > 0.0)) throw Error(POFD_E_ARG, "Invalid (non-positive) sigma prior width");
+  prior_.has_sigma = on ? 1 : 0;
+  if (on) {
+    prior_.sigma_width = width;
+    prior_.log_sigma_width = std::log(width);
+  }
+  drop_graphs();
+}
+
+void Engine1::set_cfirb_prior(bool on, double mean, double sigma) {
+  if (on) {
+    if (mean < 0.0) throw Error(POFD_E_ARG, "Invalid (negative) CFIRB mean");
+    if (!(sigma > 0.0)) throw Error(POFD_E_ARG, "Invalid (non-positive) CFIRB sigma");
+    prior_.cfirb_mean = mean;
+    prior_.cfirb_sigma = sigma;
+    prior_.log_cfirb_sigma = std::log(sigma);
+  }
+  prior_.has_cfirb = on ? 1 : 0;
+  drop_graphs();
+}
+
+void Engine1::set_poisson_prior(bool on, double mean, double sigma) {
+  if (on) {
+    if (mean < 0.0) throw Error(POFD_E_ARG, "Invalid (negative) Poisson prior mean");
+    if (!(sigma > 0.0)) throw Error(POFD_E_ARG, "Invalid (non-positive) Poisson prior sigma");
+    prior_.poisson_mean = mean;
+    prior_.poisson_sigma = sigma;
+    prior_.log_poisson_sigma = std::log(sigma);
+  }
+  prior_.has_poisson = on ? 1 : 0;
+  drop_graphs();
+}
+
+void Engine1::set_regularization(double alpha) {
+  if (!(alpha >= 0.0)) throw Error(POFD_E_ARG, "Invalid (negative) regularization alpha");
+  prior_.alpha = alpha;
+  drop_graphs();
+}
+
+void Engine1::bonus_host(unsigned nprop, const float* theta, unsigned npar, double* out) {
+  if (nprop == 0) return;
+  if (npar < knots_.size()) throw Error(POFD_E_ARG, "Not enough elements in paramSet");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  const size_t nb = static_cast<size_t>(nprop) * npar * sizeof(float);
+  float* d = nullptr;
+  cuda_check(cudaMalloc(&d, nb), "cudaMalloc");
+  cudaError_t e = cudaMemcpyAsync(d, theta, nb, cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) {
+    k_bonus1<<<nprop, kBonusThreads, 0, stream_>>>(model_, d, static_cast<int>(npar),
+                                                   std::log2(10.0), nullptr, nullptr, d_qu_,
+                                                   d_qs_, d_qw_, qper_, ws_.bonus, -1);
+    e = cudaGetLastError();
+  }
+  std::vector<double> o(static_cast<size_t>(nprop) * 4);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(o.data(), ws_.bonus, o.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                        stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  cudaFree(d);
+  cuda_check(e, "bonus evaluation");
+  for (unsigned i = 0; i < nprop; ++i) {
+    out[2 * i] = o[4 * i];
+    out[2 * i + 1] = o[4 * i + 1];
+  }
+}
+
+void Engine1::fill_bonus(unsigned nprop, float* theta_dev, unsigned npar, cudaStream_t st) {
+  if (nprop == 0) return;
+  const unsigned K = static_cast<unsigned>(knots_.size());
+  if (npar < K + 3) throw Error(POFD_E_ARG, "Not enough room to fill");
+  if (!static_ok_) reserve(std::max(nprop, ws_.P));
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  if (!st) st = stream_;
+  k_bonus1<<<nprop, kBonusThreads, 0, st>>>(model_, theta_dev, static_cast<int>(npar),
+                                            std::log2(10.0), nullptr, nullptr, d_qu_, d_qs_,
+                                            d_qw_, qper_, nullptr, static_cast<int>(K + 1));
+  cuda_check(cudaGetLastError(), "k_bonus1");
+}
+
 void Engine1::set_fft_mode(int mode) {
   if (mode != 0 && mode != 1) throw Error(POFD_E_ARG, "fft mode must be 0 (own) or 1 (cuFFT)");
   if (mode == fft_mode_) return;
@@ -1499,7 +1702,7 @@ void Engine1::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.nodes, ws_.spl,
                   ws_.rbuf, ws_.rpart, ws_.mom, ws_.pbuf, ws_.ppart,
                   ws_.pmidx, ws_.pinfo, ws_.pdout, ws_.theta_in, ws_.logl,
-                  ws_.status, ws_.tmp};
+                  ws_.status, ws_.tmp, ws_.bonus};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
@@ -1525,6 +1728,7 @@ void Engine1::reserve(unsigned P) {
   ws_.cnt = dalloc<double>(static_cast<size_t>(P) * 4 * KMAX);
   ws_.mstatus = dalloc<int>(P);
   ws_.sigmult = dalloc<double>(P);
+  ws_.bonus = dalloc<double>(static_cast<size_t>(P) * 4);
   ws_.nodes = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * NI);
   ws_.spl = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * 4 * NI);
   ws_.rbuf = dalloc<double>(static_cast<size_t>(P) * B_ * nc2);
@@ -1594,6 +1798,10 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
   mark(0);
   k_model1<<<P, 32, 0, st>>>(model_, theta, static_cast<int>(npar), std::log2(10.0),
                              ws_.cnt, ws_.mstatus, ws_.sigmult);
+  if (prior_.needs_bonus())
+    k_bonus1<<<P, kBonusThreads, 0, st>>>(model_, const_cast<float*>(theta), static_cast<int>(npar),
+                                          std::log2(10.0), ws_.cnt, ws_.mstatus, d_qu_, d_qs_,
+                                          d_qw_, qper_, ws_.bonus, -1);
   {
     const size_t smem = (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double);
     dim3 grid((NI + 127) / 128, P * B * 2);
@@ -1678,7 +1886,8 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                    ws_.ppart, ws_.pmidx, ws_.pinfo);
   mark(9);
   k_reduce1<<<(P + 127) / 128, 128, 0, st>>>(d_bsets_, B, D, P, ws_.mstatus,
-                                            ws_.sigmult, ws_.pinfo, logl, status);
+                                            ws_.sigmult, ws_.pinfo, prior_, ws_.bonus, logl,
+                                            status);
   mark(10);
   cuda_check(cudaGetLastError(), "kernel launch");
 }

@@ -68,6 +68,18 @@ struct Model1Dev {
   double minknot, maxknot;
 };
 
+// Priors and regularisation of calcLike (calcLike.h:184-195), applied after
+// the beam-set sum in the reference's order (calcLike.cc:918-952).  The logs
+// of the widths are taken on the host.
+struct Prior1 {
+  int has_sigma = 0, has_cfirb = 0, has_poisson = 0;
+  double sigma_width = 0, log_sigma_width = 0;
+  double cfirb_mean = 0, cfirb_sigma = 0, log_cfirb_sigma = 0;
+  double poisson_mean = 0, poisson_sigma = 0, log_poisson_sigma = 0;
+  double alpha = 0;  // regularisation multiplier, 0 = off
+  bool needs_bonus() const { return has_cfirb || has_poisson || alpha > 0.0; }
+};
+
 // Per-(proposal, dataset) record written by the finishing kernel.
 struct PDInfo1 {
   int status;
@@ -99,6 +111,7 @@ struct Workspace1 {
   float* theta_in = nullptr; // [P][npar] staging for host calls
   double* logl = nullptr;    // [P]
   int* status = nullptr;     // [P]
+  double* bonus = nullptr;   // [P][4] <S>, <S^2>, slope penalty, -
   // pinned host staging
   float* h_theta = nullptr;
   double* h_logl = nullptr;
@@ -139,7 +152,21 @@ class Engine1 {
   void rnodes_host(int bs, int side, const float* theta, unsigned npar,
                    double* x_out, double* r_out);
   void rgrid_host(int bs, const float* theta, unsigned npar, double* out);
-  int kernels_per_eval() const { return own_fft_ ? 13 : 9; }
+  int kernels_per_eval() const {
+    return (own_fft_ ? 13 : 9) + (prior_.needs_bonus() ? 1 : 0);
+  }
+  // priors (calcLike::setSigmaPrior / setCFIRBPrior / setPoissonPrior /
+  // setRegularizationAlpha and their unset forms, calcLike.h:251-269)
+  void set_sigma_prior(bool on, double width);
+  void set_cfirb_prior(bool on, double mean, double sigma);
+  void set_poisson_prior(bool on, double mean, double sigma);
+  void set_regularization(double alpha);
+  const Prior1& priors() const { return prior_; }
+  // <S>, <S^2> of each proposal's model (calcLike::fillBonusParams,
+  // calcLike.cc:958-980): host rows -> out[nprop][2]
+  void bonus_host(unsigned nprop, const float* theta, unsigned npar, double* out);
+  // the same written into theta_dev[i][nknots + 1], [nknots + 2] (device)
+  void fill_bonus(unsigned nprop, float* theta_dev, unsigned npar, cudaStream_t st);
   static constexpr int kNumStages = 10;
   void profile_stages(unsigned nprop, const float* theta, unsigned npar,
                       int reps, double* stage_ms);
@@ -215,6 +242,12 @@ class Engine1 {
   bool own_fft_ = false;
   double2* d_wm_ = nullptr;  // e^{-2 pi i t / m}, t < m
   double2* d_wn_ = nullptr;  // e^{-2 pi i k / n}, k <= m
+  // priors and the knot quadrature of the bonus integrals
+  Prior1 prior_;
+  const double* d_qu_ = nullptr;
+  const double* d_qs_ = nullptr;
+  const double* d_qw_ = nullptr;
+  int qper_ = 0;
 };
 
 }  // namespace pofd

@@ -485,6 +485,8 @@ void Ensemble::launch_step(cudaStream_t st) {
     ck(cudaGetLastError(), "k_propose");
     const int rc = fn_(like_, nh, prop_, np_, lnew_, snew_, st);
     if (rc < 0) throw Error(rc, "batched likelihood enqueue failed");
+    if (bfn_ && bfn_(blike_, nh, prop_, np_, st) < 0)
+      throw Error(POFD_E_ARG, "bonus parameter fill failed");
     if (collect_) collect_->add_pairs(nh, prop_, np_, lnew_, snew_, st);
     k_accept<<<g, ENT, 0, st>>>(half, nw_, np_, zexp, invt, seed_, reject_fail_ ? 1 : 0,
                                 nfail_, prop_, z_, lnew_, snew_,
@@ -626,6 +628,8 @@ void Ensemble::da_half(int half, double zexp, double invt) {
   if (b > count) k_pad<<<b - count, 32, 0, stream_>>>(static_cast<int>(count), static_cast<int>(b), np_, exprop_);
   rc = fn_(like_, b, exprop_, np_, exl_, exs_, stream_);
   if (rc < 0) throw Error(rc, "batched likelihood enqueue failed");
+  if (bfn_ && bfn_(blike_, b, exprop_, np_, stream_) < 0)
+    throw Error(POFD_E_ARG, "bonus parameter fill failed");
   stats_[2] += b;
   if (collect_) collect_->add_pairs(count, exprop_, np_, exl_, exs_, stream_);
   k_stage2<<<(count + ENT - 1) / ENT, ENT, 0, stream_>>>(

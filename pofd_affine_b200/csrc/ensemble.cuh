@@ -48,6 +48,12 @@ class Ensemble {
   void do_steps(unsigned nsteps, bool record);
   // Delayed-acceptance steps with the first-stage evaluator set below.
   void set_stage1(pofd_batch_loglike_fn fn, void* sur);
+  void set_bonus(pofd_batch_bonus_fn fn, void* like) {
+    bfn_ = fn;
+    blike_ = like;
+    drop_graph();
+  }
+  unsigned npar() const { return np_; }
   void collect_pairs(Surrogate* s) { collect_ = s; drop_graph(); }
   void do_steps_da(unsigned nsteps, bool record);
   void da_stats(unsigned long long* out4) const;
@@ -82,6 +88,8 @@ class Ensemble {
   uint64_t seed_;
   pofd_batch_loglike_fn fn_ = nullptr;
   void* like_ = nullptr;
+  pofd_batch_bonus_fn bfn_ = nullptr;
+  void* blike_ = nullptr;
   std::vector<int> state_;
   std::vector<float> lo_, hi_;
   bool params_dirty_ = true, init_ = false;

@@ -598,4 +598,65 @@ void Model2Host::rrange(const Beam2& bm, double* r) const {
   r[0] = min1; r[1] = max1; r[2] = min2; r[3] = max2;
 }
 
+void gauss_legendre(int q, std::vector<double>& x, std::vector<double>& w) {
+  if (q < 1) throw Error(POFD_E_ARG, "quadrature order must be positive");
+  x.assign(q, 0.0);
+  w.assign(q, 0.0);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int i = 0; i < (q + 1) / 2; ++i) {
+    // initial guess (Tricomi) for the i-th largest root, then Newton
+    long double t = std::cos(pi * (i + 0.75L) / (q + 0.5L));
+    long double dp = 1.0L;
+    for (int it = 0; it < 100; ++it) {
+      long double p0 = 1.0L, p1 = t;
+      for (int k = 2; k <= q; ++k) {
+        const long double p2 = ((2 * k - 1) * t * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      // P_q = p1, P_{q-1} = p0; P_q' = q (t P_q - P_{q-1}) / (t^2 - 1)
+      dp = q * (t * p1 - p0) / (t * t - 1.0L);
+      const long double dt = p1 / dp;
+      t -= dt;
+      if (std::fabs(static_cast<double>(dt)) < 1e-19) break;
+    }
+    long double p0 = 1.0L, p1 = t;
+    for (int k = 2; k <= q; ++k) {
+      const long double p2 = ((2 * k - 1) * t * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    dp = (q == 1) ? 1.0L : q * (t * p1 - p0) / (t * t - 1.0L);
+    const long double wt = 2.0L / ((1.0L - t * t) * dp * dp);
+    x[q - 1 - i] = static_cast<double>(t);
+    x[i] = static_cast<double>(-t);
+    w[i] = w[q - 1 - i] = static_cast<double>(wt);
+  }
+}
+
+void KnotQuadrature::build(const double* logknots, int K, int panels, int q) {
+  std::vector<double> gx, gw;
+  gauss_legendre(q, gx, gw);
+  nper = panels * q;
+  const size_t nq = (K > 1) ? static_cast<size_t>(K - 1) * nper : 0;
+  u.assign(nq, 0.0);
+  s.assign(nq, 0.0);
+  w.assign(nq, 0.0);
+  const long double ln2 = 0.693147180559945309417232121458176568L;
+  size_t j = 0;
+  for (int k = 0; k + 1 < K; ++k) {
+    const long double a = logknots[k], b = logknots[k + 1];
+    const long double h = (b - a) / panels;
+    for (int p = 0; p < panels; ++p) {
+      const long double lo = a + p * h;
+      for (int g = 0; g < q; ++g, ++j) {
+        const long double uu = lo + 0.5L * h * (gx[g] + 1.0L);
+        u[j] = static_cast<double>(uu);
+        s[j] = static_cast<double>(std::exp2(uu));
+        w[j] = static_cast<double>(ln2 * 0.5L * h * gw[g]);
+      }
+    }
+  }
+}
+
 }  // namespace pofd

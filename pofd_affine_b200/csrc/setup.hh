@@ -90,6 +90,21 @@ struct RGrid1 {
 // The flux range of a knot model over a beam (numberCountsKnots.cc:345-365).
 std::pair<double, double> rrange_knots(double maxknot, const Beam1& bm);
 
+// Gauss-Legendre rule of order q on [-1, 1], nodes ascending: Newton
+// iterations on the three-term Legendre recurrence, in long double.
+void gauss_legendre(int q, std::vector<double>& x, std::vector<double>& w);
+
+// Quadrature nodes for integrals of S^a dN/dS over [S_0, S_{K-1}] written in
+// u = log2 S (dS = ln2 2^u du): each knot interval [u_k, u_{k+1}] is cut into
+// `panels` equal panels with a q-point Gauss-Legendre rule each.  Node j lies
+// in knot interval j / nper (nper = panels * q); s = 2^u and w = ln2 * h/2 *
+// w_g, so that the integral is sum_j w_j s_j^{a+1} 2^{spline(u_j)}.
+struct KnotQuadrature {
+  std::vector<double> u, s, w;
+  int nper = 0;
+  void build(const double* logknots, int K, int panels, int q);
+};
+
 // ------------------------------------------------------------- 2D beam
 struct Beam2 {
   double pixsize = 0, minval = 0;
