@@ -278,6 +278,27 @@ int pofd_like2_profile(pofd_like2* L, unsigned nprop, const float* theta,
                        int* nstages);
 const char* pofd_like2_stage_name(int i);
 
+/* Priors per band (band 0 or 1), added once to the summed log-likelihood in
+ * the reference's order (calcLikeDouble.cc:1236-1276): Gaussians on the
+ * sigma multipliers about 1, on <S_b> and on <S_b^2>, then alpha times the
+ * band-1 log-slope penalty.  Replace calcLikeDouble::setSigmaPrior1/2,
+ * setCFIRBPrior1/2, setPoissonPrior1/2, their unset forms and
+ * setRegularizationAlpha (calcLikeDouble.h:310-341). */
+int pofd_like2_set_sigma_prior(pofd_like2* L, int band, int on, double width);
+int pofd_like2_set_cfirb_prior(pofd_like2* L, int band, int on, double mean, double sigma);
+int pofd_like2_set_poisson_prior(pofd_like2* L, int band, int on, double mean, double sigma);
+int pofd_like2_set_regularization(pofd_like2* L, double alpha);
+/* <S1>, <S2>, <S1^2>, <S2^2> of each host row, out [nprop][4]
+ * (numberCountsDoubleLogNormal::getFluxPerArea / getFluxSqPerArea,
+ * numberCountsDoubleLogNormal.cc:1549-1665), NaN for an invalid model. */
+int pofd_like2_bonus(pofd_like2* L, unsigned nprop, const float* theta,
+                     unsigned npar, double* out);
+/* calcLikeDouble::fillBonusParams (calcLikeDouble.cc:1283-1310) on device
+ * rows: the four values at theta_dev[i][nmodel + 2 .. nmodel + 5], nmodel =
+ * knots + sigma knots + offset knots; npar >= nmodel + 6.  Enqueue only. */
+int pofd_like2_fill_bonus_device(pofd_like2* L, unsigned nprop, float* theta_dev,
+                                 unsigned npar, void* stream);
+
 /* Allocation-free split / unwrap / normalise / binned log-likelihood of
  * one wrapped 1D P(D) (the inverse-FFT output), for callers that cannot
  * allocate GPU memory when they evaluate: a program whose device memory is

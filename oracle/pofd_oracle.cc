@@ -1026,6 +1026,80 @@ struct Counts2 {
   }
   bool isValid() const { return knots_valid && sigmas_valid && offsets_valid; }
 
+  // Breakpoints of the band-1 integrals in ln S1: the knots, plus the sigma
+  // and offset knots inside the knot range (where the colour curves have
+  // kinks: linear interpolation, clamping).
+  std::vector<double> lnBreaks() const {
+    std::vector<double> b;
+    for (double k : knots) b.push_back(std::log(k));
+    for (const auto* v : {&sigmaknots, &offsetknots})
+      for (double k : *v)
+        if (k > knots.front() && k < knots.back()) b.push_back(std::log(k));
+    std::sort(b.begin(), b.end());
+    b.erase(std::unique(b.begin(), b.end()), b.end());
+    return b;
+  }
+  // numberCountsDoubleLogNormal::splineInt (numberCountsDoubleLogNormal.cc:
+  // 1549-1631) with the integrand of evalPowfNDoubleLogNormal (2424-2512):
+  // S1^(a+b) n1(S1) exp(b mu(S1) + b^2/2 sigma^2(S1)) over [S_0, S_{K-1}),
+  // sigma floored at min_sigma in every branch there.  32 panels of 20-point
+  // Gauss-Legendre per breakpoint interval, in ln S1.
+  double splineInt(double alpha, double beta) const {
+    if (knots.size() < 2 || !isValid()) return kNaN;
+    std::vector<double> gx, gw;
+    gauss_legendre(20, gx, gw);
+    const double power = alpha + beta, c1 = beta, c2 = 0.5 * beta * beta;
+    const auto br = lnBreaks();
+    double tot = 0.0;
+    for (size_t k = 0; k + 1 < br.size(); ++k) {
+      const int npanel = 32;
+      const double h = (br[k + 1] - br[k]) / npanel;
+      for (int p = 0; p < npanel; ++p) {
+        const double lo = br[k] + p * h;
+        for (int g = 0; g < 20; ++g) {
+          const double s1 = std::exp(lo + 0.5 * h * (gx[g] + 1.0));
+          if (s1 < knots.front() || s1 >= knots.back()) continue;
+          double prefac = std::pow(s1, power);
+          if (c1 != 0.0 || c2 != 0.0) {
+            double e = 0.0;
+            if (c1 != 0.0) e = c1 * offsetInner(s1);
+            if (c2 != 0.0) {
+              const size_t ns = sigmaknots.size();
+              double sg;
+              if (ns == 1) sg = sigmavals[0];
+              else if (s1 <= sigmaknots[0]) sg = sigmavals[0];
+              else if (s1 >= sigmaknots[ns - 1]) sg = sigmavals[ns - 1];
+              else sg = (ns == 2) ? linear_interp(sigmaknots, sigmavals, s1) : sigspl.eval(s1);
+              if (sg < min_sigma) sg = min_sigma;
+              e += c2 * sg * sg;
+            }
+            prefac *= std::exp(e);
+          }
+          tot += 0.5 * h * gw[g] * s1 * prefac * std::exp2(spl.eval(std::log2(s1)));
+        }
+      }
+    }
+    return tot;
+  }
+  // differenceRegularize of the band-1 knots (numberCountsDoubleLogNormal.cc:
+  // 2154-2173)
+  double differenceRegularize(double alpha) const {
+    if (!knots_valid) return kNaN;
+    const size_t nk = knots.size();
+    if (nk < 2) return 0.0;
+    double mean_deriv = 0.0;
+    for (size_t i = 1; i < nk; ++i)
+      mean_deriv += (logknotvals[i] - logknotvals[i - 1]) / (logknots[i] - logknots[i - 1]);
+    mean_deriv /= static_cast<double>(nk - 1);
+    double pen = 0.0;
+    for (size_t i = 1; i < nk; ++i) {
+      const double d = (logknotvals[i] - logknotvals[i - 1]) / (logknots[i] - logknots[i - 1]) -
+                       mean_deriv;
+      pen -= d * d;
+    }
+    return alpha * pen;
+  }
+
   double sigmaInner(double f1) const {
     const size_t ns = sigmaknots.size();
     if (ns == 1) return sigmavals[0];
@@ -1850,6 +1924,12 @@ struct Like2 {
   bool edge = true, bin_data = true;
   Counts2 model;
   std::vector<BeamSet2> sets;
+  // priors and regularisation (calcLikeDouble.h:213-232)
+  bool has_sigma_prior[2] = {false, false}, has_cfirb_prior[2] = {false, false};
+  bool has_poisson_prior[2] = {false, false};
+  double sigma_prior_width[2] = {0, 0}, cfirb_prior_mean[2] = {0, 0};
+  double cfirb_prior_sigma[2] = {0, 0}, poisson_prior_mean[2] = {0, 0};
+  double poisson_prior_sigma[2] = {0, 0}, regularization_alpha = 0;
 
   void refreshSet(BeamSet2& s) {
     s.maxsb1 = s.sb1[0]; s.maxsb2 = s.sb2[0];
@@ -1925,6 +2005,27 @@ struct Like2 {
     const double sm1 = p[nm], sm2 = p[nm + 1];
     double LogLike = 0.0;
     for (auto& s : sets) LogLike += singleLogLike(s, sm1, sm2);
+    // priors and regularisation (calcLikeDouble.cc:1236-1276)
+    const double half_log_2pi = 0.918938517570495605469;
+    const double sm[2] = {sm1, sm2};
+    for (int b = 0; b < 2; ++b)
+      if (has_sigma_prior[b]) {
+        const double val = (sm[b] - 1.0) / sigma_prior_width[b];
+        LogLike -= half_log_2pi + std::log(sigma_prior_width[b]) + 0.5 * val * val;
+      }
+    const double mf[2] = {model.splineInt(1.0, 0.0), model.splineInt(0.0, 1.0)};
+    for (int b = 0; b < 2; ++b)
+      if (has_cfirb_prior[b]) {
+        const double val = (cfirb_prior_mean[b] - mf[b]) / cfirb_prior_sigma[b];
+        LogLike -= half_log_2pi + std::log(cfirb_prior_sigma[b]) + 0.5 * val * val;
+      }
+    const double mf2[2] = {model.splineInt(2.0, 0.0), model.splineInt(0.0, 2.0)};
+    for (int b = 0; b < 2; ++b)
+      if (has_poisson_prior[b]) {
+        const double val = (poisson_prior_mean[b] - mf2[b]) / poisson_prior_sigma[b];
+        LogLike -= half_log_2pi + std::log(poisson_prior_sigma[b]) + 0.5 * val * val;
+      }
+    if (regularization_alpha > 0.0) LogLike += model.differenceRegularize(regularization_alpha);
     return LogLike;
   }
 };
@@ -2315,6 +2416,9 @@ int orc_counts2_maxflux(void* vm, double* mm) {
     mm[0] = r.first; mm[1] = r.second;
   });
 }
+int orc_counts2_spline_int(void* vm, double alpha, double beta, double* out) {
+  return guard([&] { *out = static_cast<Counts2*>(vm)->splineInt(alpha, beta); });
+}
 int orc_counts2_rrange(void* vm, void* beam, double* r) {
   return guard([&] {
     const Counts2* m = static_cast<Counts2*>(vm);
@@ -2404,6 +2508,33 @@ int orc_like2_dataset_bins(void* vL, int bs, int ds, uint32_t* out) {
   const Data2& d = L->sets.at(bs).data.at(ds);
   std::copy(d.bins.begin(), d.bins.end(), out);
   return 0;
+}
+int orc_like2_set_priors(void* vL, const double* p17) {
+  Like2* L = static_cast<Like2*>(vL);
+  L->pool.clear();
+  for (int b = 0; b < 2; ++b) {
+    const double* q = p17 + 8 * b;
+    L->has_sigma_prior[b] = q[0] != 0.0;
+    L->sigma_prior_width[b] = q[1];
+    L->has_cfirb_prior[b] = q[2] != 0.0;
+    L->cfirb_prior_mean[b] = q[3];
+    L->cfirb_prior_sigma[b] = q[4];
+    L->has_poisson_prior[b] = q[5] != 0.0;
+    L->poisson_prior_mean[b] = q[6];
+    L->poisson_prior_sigma[b] = q[7];
+  }
+  L->regularization_alpha = p17[16];
+  return 0;
+}
+int orc_like2_bonus(void* vL, const float* theta, int npar, double* out4) {
+  Like2* L = static_cast<Like2*>(vL);
+  return guard([&] {
+    L->model.setParams(theta, npar);
+    out4[0] = L->model.splineInt(1.0, 0.0);
+    out4[1] = L->model.splineInt(0.0, 1.0);
+    out4[2] = L->model.splineInt(2.0, 0.0);
+    out4[3] = L->model.splineInt(0.0, 2.0);
+  });
 }
 int orc_like2_eval(void* vL, const float* theta, int npar, double* logl) {
   return guard([&] { *logl = static_cast<Like2*>(vL)->getLogLike(theta, npar); });

@@ -112,6 +112,8 @@ int orc_counts2_getR(void* m, void* beam, int n1, const double* f1, int n2,
 int orc_counts2_getR_scalar(void* m, void* beam, int n, const double* f1,
                             const double* f2, double* out);
 int orc_counts2_maxflux(void* m, double* mm2);
+/* integral of S1^alpha S2^beta dN/dS1 dS2 (splineInt) */
+int orc_counts2_spline_int(void* m, double alpha, double beta, double* out);
 int orc_counts2_rrange(void* m, void* beam, double* range4);
 int orc_counts2_sigma_offset(void* m, int n, const double* f1, double* sig,
                              double* off);
@@ -137,6 +139,12 @@ int orc_like2_get_rrange(void* L, int beamset, double* range4);
 int orc_like2_dataset_info(void* L, int beamset, int ds, double* info10);
 int orc_like2_dataset_bins(void* L, int beamset, int ds, uint32_t* out);
 int orc_like2_eval(void* L, const float* theta, int npar, double* logl);
+/* priors: p17 = per band b (8 entries at 8b) {has_sigma, width, has_cfirb,
+ * mean, sigma, has_poisson, mean, sigma}, then regularization_alpha
+ * (calcLikeDouble.h:213-232) */
+int orc_like2_set_priors(void* L, const double* p17);
+/* bonus parameters <S1>, <S2>, <S1^2>, <S2^2> of the model at theta */
+int orc_like2_bonus(void* L, const float* theta, int npar, double* out4);
 int orc_like2_eval_batch(void* L, int nprop, const float* theta, int npar,
                          double* logl, int* status, int nthreads);
 /* dbg: [dflux1, dflux2, mn1, mn2, var1, var2, shift1, shift2, split1,

@@ -59,6 +59,8 @@ def lib():
         "orc_like1_dataset_bins": (I, [V, I, I, _up]),
         "orc_like1_eval": (I, [V, _fp, I, _dp]),
         "orc_like1_set_priors": (I, [V, _dp]),
+        "orc_like2_set_priors": (I, [V, _dp]),
+        "orc_like2_bonus": (I, [V, _fp, I, _dp]),
         "orc_like1_bonus": (I, [V, _fp, I, _dp]),
         "orc_like1_eval_batch": (I, [V, I, _fp, I, _dp, _ip, I]),
         "orc_like1_pd": (I, [V, I, I, _fp, I, I, _dp, P, P]),
@@ -71,6 +73,7 @@ def lib():
         "orc_counts2_new": (V, [I, _dp, I, _dp, I, _dp]),
         "orc_counts2_free": (None, [V]),
         "orc_counts2_set": (I, [V, _fp, I]),
+        "orc_counts2_spline_int": (I, [V, D, D, _dp]),
         "orc_counts2_eval": (I, [V, I, _dp, _dp, _dp]),
         "orc_counts2_getR": (I, [V, V, I, _dp, I, _dp, _dp]),
         "orc_counts2_getR_scalar": (I, [V, V, I, _dp, _dp, _dp]),
@@ -405,6 +408,12 @@ class Counts2:
         _chk(lib().orc_counts2_maxflux(self.h, out))
         return out
 
+    def spline_int(self, alpha, beta):
+        out = np.empty(1)
+        _chk(lib().orc_counts2_spline_int(self.h, float(alpha), float(beta),
+                                          out))
+        return out[0]
+
     def rrange(self, beam):
         out = np.empty(4)
         _chk(lib().orc_counts2_rrange(self.h, beam.h, out))
@@ -476,6 +485,29 @@ class Like2:
         out = np.empty(1)
         _chk(lib().orc_like2_eval(self.h, th, len(th), out))
         return out[0]
+
+    def set_priors(self, sigma=(None, None), cfirb=(None, None),
+                   poisson=(None, None), alpha=0.0):
+        """Per band: sigma width, (mean, sigma) on <S_b>, (mean, sigma) on
+        <S_b^2>; None turns a prior off (calcLikeDouble.h:213-232)."""
+        v = np.zeros(17)
+        for b in range(2):
+            q = v[8 * b:8 * b + 8]
+            if sigma[b] is not None:
+                q[0], q[1] = 1.0, sigma[b]
+            if cfirb[b] is not None:
+                q[2], q[3], q[4] = 1.0, cfirb[b][0], cfirb[b][1]
+            if poisson[b] is not None:
+                q[5], q[6], q[7] = 1.0, poisson[b][0], poisson[b][1]
+        v[16] = alpha
+        _chk(lib().orc_like2_set_priors(self.h, v))
+
+    def bonus(self, theta):
+        """<S1>, <S2>, <S1^2>, <S2^2> (calcLikeDouble.cc:1283-1310)."""
+        th = f32(theta)
+        out = np.empty(4)
+        _chk(lib().orc_like2_bonus(self.h, th, len(th), out))
+        return out
 
     def loglike_batch(self, thetas, nthreads=1):
         th = f32(thetas)

@@ -58,6 +58,12 @@ SIGNATURES = {
     "pofd_like1_set_fft": (I, [V, I]),
     "pofd_like1_fft_info": (I, [V, C.POINTER(I)]),
     "pofd_like1_set_sigma_prior": (I, [V, I, D]),
+    "pofd_like2_set_sigma_prior": (I, [V, I, I, D]),
+    "pofd_like2_set_cfirb_prior": (I, [V, I, I, D, D]),
+    "pofd_like2_set_poisson_prior": (I, [V, I, I, D, D]),
+    "pofd_like2_set_regularization": (I, [V, D]),
+    "pofd_like2_bonus": (I, [V, U, _fp, U, _dp]),
+    "pofd_like2_fill_bonus_device": (I, [V, U, V, U, V]),
     "pofd_like1_set_cfirb_prior": (I, [V, I, D, D]),
     "pofd_like1_set_poisson_prior": (I, [V, I, D, D]),
     "pofd_like1_set_regularization": (I, [V, D]),

@@ -171,6 +171,58 @@ class calcLikeDouble:
                                           st))
         return ll, st
 
+    # priors per band (calcLikeDouble.h:310-341); band 0 or 1
+    def setSigmaPrior(self, band, width):
+        check(lib().pofd_like2_set_sigma_prior(self.h, int(band), 1,
+                                               float(width)))
+
+    def unsetSigmaPrior(self, band):
+        check(lib().pofd_like2_set_sigma_prior(self.h, int(band), 0, 0.0))
+
+    def setCFIRBPrior(self, band, mean, sigma):
+        check(lib().pofd_like2_set_cfirb_prior(self.h, int(band), 1,
+                                               float(mean), float(sigma)))
+
+    def unsetCFIRBPrior(self, band):
+        check(lib().pofd_like2_set_cfirb_prior(self.h, int(band), 0, 0.0,
+                                               0.0))
+
+    def setPoissonPrior(self, band, mean, sigma):
+        check(lib().pofd_like2_set_poisson_prior(self.h, int(band), 1,
+                                                 float(mean), float(sigma)))
+
+    def unsetPoissonPrior(self, band):
+        check(lib().pofd_like2_set_poisson_prior(self.h, int(band), 0, 0.0,
+                                                 0.0))
+
+    def setRegularizationAlpha(self, alpha):
+        check(lib().pofd_like2_set_regularization(self.h, float(alpha)))
+
+    def getBonus(self, thetas):
+        """<S1>, <S2>, <S1^2>, <S2^2> of each row: [nprop, 4]."""
+        th = _f32(thetas)
+        if th.ndim == 1:
+            th = th[None, :]
+        th = np.ascontiguousarray(th)
+        out = np.empty((th.shape[0], 4))
+        check(lib().pofd_like2_bonus(self.h, th.shape[0], th.ravel(),
+                                     th.shape[1], out.ravel()))
+        return out
+
+    def fillBonusParams(self, thetas):
+        """calcLikeDouble::fillBonusParams on rows with nmodel + 6 or more
+        entries: a copy with <S1>, <S2>, <S1^2>, <S2^2> after the two sigma
+        multipliers (as floats)."""
+        th = np.array(_f32(thetas), copy=True)
+        one = th.ndim == 1
+        if one:
+            th = th[None, :]
+        k = self.nmodel
+        if th.shape[1] < k + 6:
+            raise PofdError(-10, "Not enough room to fill")
+        th[:, k + 2:k + 6] = self.getBonus(th).astype(np.float32)
+        return th[0] if one else th
+
     def getLogLikeDevice(self, nprop, theta_ptr, npar, logl_ptr, status_ptr,
                          stream=None):
         check(lib().pofd_like2_eval_batch_device(

@@ -691,6 +691,60 @@ int pofd_like2_kernels_per_eval(const pofd_like2* L, int* nk) {
   });
 }
 
+int pofd_like2_set_sigma_prior(pofd_like2* L, int band, int on, double width) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_sigma_prior(band, on != 0, width);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_set_cfirb_prior(pofd_like2* L, int band, int on, double mean, double sigma) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_cfirb_prior(band, on != 0, mean, sigma);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_set_poisson_prior(pofd_like2* L, int band, int on, double mean, double sigma) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_poisson_prior(band, on != 0, mean, sigma);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_set_regularization(pofd_like2* L, double alpha) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_regularization(alpha);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_bonus(pofd_like2* L, unsigned nprop, const float* theta, unsigned npar,
+                     double* out) {
+  return guard([&] {
+    need(L && theta && out, "null argument");
+    need(L->ctx->device >= 0, "host-only context has no GPU");
+    cudaSetDevice(L->ctx->device);
+    L->eng->bonus_host(nprop, theta, npar, out);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_fill_bonus_device(pofd_like2* L, unsigned nprop, float* theta_dev,
+                                 unsigned npar, void* stream) {
+  return guard([&] {
+    need(L && theta_dev, "null argument");
+    need(L->ctx->device >= 0, "host-only context has no GPU");
+    cudaSetDevice(L->ctx->device);
+    L->eng->fill_bonus(nprop, theta_dev, npar, static_cast<cudaStream_t>(stream));
+    return POFD_OK;
+  });
+}
+
 int pofd_like2_profile(pofd_like2* L, unsigned nprop, const float* theta,
                        unsigned npar, int reps, double* stage_ms,
                        int* nstages) {
@@ -713,6 +767,9 @@ static int like1_batch(void* like, unsigned nprop, const float* theta,
 }
 static int like1_fill(void* like, unsigned nprop, float* theta, unsigned npar, void* stream) {
   return pofd_like1_fill_bonus_device(static_cast<pofd_like1*>(like), nprop, theta, npar, stream);
+}
+static int like2_fill(void* like, unsigned nprop, float* theta, unsigned npar, void* stream) {
+  return pofd_like2_fill_bonus_device(static_cast<pofd_like2*>(like), nprop, theta, npar, stream);
 }
 static int like2_batch(void* like, unsigned nprop, const float* theta,
                        unsigned npar, double* logl, int* status, void* stream) {
@@ -774,6 +831,11 @@ int pofd_ensemble_use_like2(pofd_ensemble* e, pofd_like2* like) {
   return guard([&] {
     need(e && like, "null argument");
     e->ens->set_like(like2_batch, like);
+    // bonus slots after the two sigma multipliers (pofdMCMCDouble.cc:408-415)
+    if (e->ens->npar() >= like->eng->nparams() + 6)
+      e->ens->set_bonus(like2_fill, like);
+    else
+      e->ens->set_bonus(nullptr, nullptr);
     return POFD_OK;
   });
 }

@@ -1010,7 +1010,8 @@ __global__ void k_reduce2(const BSet2Dev* __restrict__ bsets,
                           const int* __restrict__ mstatus,
                           const double* __restrict__ sigmult,
                           const PDInfo2* __restrict__ pinfo,
-                          const double* __restrict__ gpart,
+                          const double* __restrict__ gpart, Prior2 pr,
+                          const double* __restrict__ bonus,
                           double* __restrict__ logl, int* __restrict__ status) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= nprop) return;
@@ -1041,8 +1042,119 @@ __global__ void k_reduce2(const BSet2Dev* __restrict__ bsets,
     }
     LogLike += s;
   }
+  // priors, once for all data sets (calcLikeDouble.cc:1236-1276)
+  constexpr double half_log_2pi = 0.918938517570495605469;
+  const double sm[2] = {sm1, sm2};
+  const double* bn = bonus + 8 * static_cast<size_t>(w);
+  for (int b = 0; b < 2; ++b)
+    if (pr.has_sigma[b]) {
+      const double val = (sm[b] - 1.0) / pr.sigma_width[b];
+      LogLike -= half_log_2pi + pr.log_sigma_width[b] + 0.5 * val * val;
+    }
+  for (int b = 0; b < 2; ++b)
+    if (pr.has_cfirb[b]) {
+      const double val = (pr.cfirb_mean[b] - bn[b]) / pr.cfirb_sigma[b];
+      LogLike -= half_log_2pi + pr.log_cfirb_sigma[b] + 0.5 * val * val;
+    }
+  for (int b = 0; b < 2; ++b)
+    if (pr.has_poisson[b]) {
+      const double val = (pr.poisson_mean[b] - bn[2 + b]) / pr.poisson_sigma[b];
+      LogLike -= half_log_2pi + pr.log_poisson_sigma[b] + 0.5 * val * val;
+    }
+  if (pr.alpha > 0.0) LogLike += pr.alpha * bn[4];
   status[w] = st;
   logl[w] = (st == 0) ? LogLike : qnan;
+}
+
+// Bonus integrals and the band-1 slope penalty of each proposal's model,
+// one block per proposal.  numberCountsDoubleLogNormal::splineInt(a, b)
+// (numberCountsDoubleLogNormal.cc:1549-1631) integrates
+// S1^(a+b) n1(S1) exp(b mu(S1) + b^2/2 sigma^2(S1)) over [S_0, S_{K-1})
+// (the integrand of numberCountsDoubleLogNormal.cc:2424-2512, sigma floored
+// at min_sigma in every branch there); here by Gauss-Legendre quadrature in
+// u = log2 S1 on host-built nodes that also break at the colour-curve
+// knots.  out[w][8] = {<S1>, <S2>, <S1^2>, <S2^2>, penalty, 0, 0, 0}, NaN for
+// an invalid model; the penalty is differenceRegularize of the band-1 knots
+// (numberCountsDoubleLogNormal.cc:2154-2173) before the factor alpha.
+// fill_at >= 0 stores the four integrals as floats at theta[w][fill_at..].
+constexpr int kBonus2Threads = 256;
+__global__ void __launch_bounds__(kBonus2Threads)
+k_bonus2(Model2Dev m, float* theta, int npar, double logfac,
+         const double* __restrict__ cnt, const int* __restrict__ mstatus,
+         const double* __restrict__ qu, const double* __restrict__ qs,
+         const double* __restrict__ qw, const int* __restrict__ qk, int nq,
+         double* __restrict__ out, int fill_at) {
+  __shared__ double cs[12 * KMAX];
+  __shared__ double lk[KMAX], sk[KMAX], okn[KMAX];
+  __shared__ double red[4][kBonus2Threads / 32];
+  const int w = blockIdx.x;
+  const int K = m.K;
+  const int st = mstatus[w];
+  for (int i = threadIdx.x; i < K; i += blockDim.x) lk[i] = m.logknots[i];
+  for (int i = threadIdx.x; i < m.ns; i += blockDim.x) sk[i] = m.sk[i];
+  for (int i = threadIdx.x; i < m.no; i += blockDim.x) okn[i] = m.ok[i];
+  for (int i = threadIdx.x; i < 12 * KMAX; i += blockDim.x)
+    cs[i] = cnt[static_cast<size_t>(w) * 12 * KMAX + i];
+  __syncthreads();
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  if (st == 0) {
+    for (int j = threadIdx.x; j < nq; j += blockDim.x) {
+      const int k = qk[j];
+      const double d = qu[j] - lk[k];
+      const double* q = cs + 4 * k;
+      const double S = qs[j];
+      const double base = qw[j] * S * S * exp2(q[0] + d * (q[1] + d * (q[2] + d * q[3])));
+      const double mu = curve_at(okn, cs + 8 * KMAX, m.no, S, false, 0.0);
+      double sg = curve_at(sk, cs + 4 * KMAX, m.ns, S, false, 0.0);
+      if (sg < m.min_sigma) sg = m.min_sigma;
+      a[0] += base;
+      a[1] += base * exp(mu + 0.5 * sg * sg);
+      a[2] += base * S;
+      a[3] += base * S * exp(2.0 * mu + 2.0 * sg * sg);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a[c] += __shfl_down_sync(0xffffffffu, a[c], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int c = 0; c < 4; ++c) red[c][threadIdx.x >> 5] = a[c];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+  double t[4] = {0.0, 0.0, 0.0, 0.0}, pen = 0.0;
+  for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i)
+    for (int c = 0; c < 4; ++c) t[c] += red[c][i];
+  const float* th = theta + static_cast<size_t>(w) * npar;
+  if (st != 0) {
+    for (int c = 0; c < 4; ++c) t[c] = qnan;
+    pen = qnan;
+  } else {
+    double mean_deriv = 0.0;
+    for (int i = 1; i < K; ++i)
+      mean_deriv += (logfac * static_cast<double>(th[i]) -
+                     logfac * static_cast<double>(th[i - 1])) / (lk[i] - lk[i - 1]);
+    mean_deriv /= static_cast<double>(K - 1);
+    for (int i = 1; i < K; ++i) {
+      const double dl = (logfac * static_cast<double>(th[i]) -
+                         logfac * static_cast<double>(th[i - 1])) / (lk[i] - lk[i - 1]) -
+                        mean_deriv;
+      pen -= dl * dl;
+    }
+  }
+  if (out) {
+    double* o = out + 8 * static_cast<size_t>(w);
+    o[0] = t[0];
+    o[1] = t[1];
+    o[2] = t[2];
+    o[3] = t[3];
+    o[4] = pen;
+    o[5] = o[6] = o[7] = 0.0;
+  }
+  if (fill_at >= 0) {
+    float* tw = theta + static_cast<size_t>(w) * npar;
+    for (int c = 0; c < 4; ++c) tw[fill_at + c] = static_cast<float>(t[c]);
+  }
 }
 
 // The unwrapped, normalised (optionally log2) 2D P(D) of one row.
@@ -1300,6 +1412,26 @@ void Engine2::build_static() {
   model_.minknot = knots_.front();
   model_.maxknot = knots_.back();
   model_.min_sigma = 0.0;
+  {
+    // bonus integrals: 32 panels of 20 points per interval between the
+    // knots and the colour-curve knots inside the knot range
+    std::vector<double> extra;
+    for (double v : sigk_) extra.push_back(std::log2(v));
+    for (double v : offk_) extra.push_back(std::log2(v));
+    KnotQuadrature kq;
+    kq.build_breaks(lk.data(), static_cast<int>(knots_.size()), extra, 32, 20);
+    d_qu_ = up(kq.u);
+    d_qs_ = up(kq.s);
+    d_qw_ = up(kq.w);
+    int* qk = nullptr;
+    ck(cudaMalloc(&qk, (kq.kidx.size() + 1) * sizeof(int)), "cudaMalloc");
+    static_allocs_.push_back(qk);
+    if (!kq.kidx.empty())
+      ck(cudaMemcpy(qk, kq.kidx.data(), kq.kidx.size() * sizeof(int), cudaMemcpyHostToDevice),
+         "upload");
+    d_qk_ = qk;
+    nq_ = static_cast<int>(kq.u.size());
+  }
 
   const unsigned n = n_;
   B_ = static_cast<unsigned>(sets_.size());
@@ -1456,7 +1588,8 @@ void Engine2::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.rw, ws_.rbuf,
                   ws_.rpart, ws_.redge, ws_.epart, ws_.fpart, ws_.mom, ws_.pbuf, ws_.rowpart,
                   ws_.colpart, ws_.pinfo, ws_.gpart, ws_.pdout,
-                  ws_.theta_in, ws_.logl, ws_.status};
+                  ws_.theta_in, ws_.logl, ws_.status, ws_.bonus, ws_.bcnt,
+                  ws_.bstatus, ws_.bsig};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
@@ -1485,6 +1618,10 @@ void Engine2::reserve(unsigned P) {
   ws_.cnt = dal<double>(static_cast<size_t>(P) * 12 * KMAX);
   ws_.mstatus = dal<int>(P);
   ws_.sigmult = dal<double>(2 * static_cast<size_t>(P));
+  ws_.bonus = dal<double>(8 * static_cast<size_t>(P));
+  ws_.bcnt = dal<double>(static_cast<size_t>(P) * 12 * KMAX);
+  ws_.bstatus = dal<int>(P);
+  ws_.bsig = dal<double>(2 * static_cast<size_t>(P));
   ws_.rw = dal<double>(static_cast<size_t>(P) * B_ * nrows * Tmax_ * 3);
   ws_.rbuf = dal<double>(static_cast<size_t>(P) * B_ * n * nc2);
   ws_.rpart = dal<double>(static_cast<size_t>(P) * B_ * gx_ * gy_ * 4);
@@ -1540,6 +1677,10 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   mark(0);
   k_model2<<<P, 32, 0, st>>>(model_, theta, static_cast<int>(npar), std::log2(10.0),
                              ws_.cnt, ws_.mstatus, ws_.sigmult);
+  if (prior_.needs_bonus())
+    k_bonus2<<<P, kBonus2Threads, 0, st>>>(model_, const_cast<float*>(theta), static_cast<int>(npar),
+                                           std::log2(10.0), ws_.cnt, ws_.mstatus, d_qu_, d_qs_,
+                                           d_qw_, d_qk_, nq_, ws_.bonus, -1);
   mark(1);
   {
     const size_t nrows = static_cast<size_t>(n + ne);
@@ -1599,7 +1740,7 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   k_reduce2<<<(P + 127) / 128, 128, 0, st>>>(d_bsets_, d_dsets_, B, D, P,
                                             static_cast<int>(gchunks_), std::log(2.0),
                                             ws_.mstatus, ws_.sigmult, ws_.pinfo,
-                                            ws_.gpart, logl, status);
+                                            ws_.gpart, prior_, ws_.bonus, logl, status);
   mark(12);
   ck(cudaGetLastError(), "kernel launch");
 }
@@ -1688,6 +1829,101 @@ void Engine2::eval_host(unsigned nprop, const float* theta, unsigned npar,
   ck(cudaStreamSynchronize(stream_), "synchronize");
   std::memcpy(logl, ws_.h_logl, nprop * sizeof(double));
   std::memcpy(status, ws_.h_status, nprop * sizeof(int));
+}
+
+// Prior setters (calcLikeDouble.h:310-341); prior values are launch
+// arguments of the reduction kernel, so captured graphs are dropped.
+void Engine2::set_sigma_prior(int band, bool on, double width) {
+  if (band != 0 && band != 1) throw Error(POFD_E_ARG, "band must be 0 or 1");
+  if (on && !(width > 0.0)) throw Error(POFD_E_ARG, "Invalid (non-positive) sigma prior width");
+  prior_.has_sigma[band] = on ? 1 : 0;
+  if (on) {
+    prior_.sigma_width[band] = width;
+    prior_.log_sigma_width[band] = std::log(width);
+  }
+  drop_graphs();
+}
+
+void Engine2::set_cfirb_prior(int band, bool on, double mean, double sigma) {
+  if (band != 0 && band != 1) throw Error(POFD_E_ARG, "band must be 0 or 1");
+  if (on) {
+    if (mean < 0.0) throw Error(POFD_E_ARG, "Invalid (negative) CFIRB mean");
+    if (!(sigma > 0.0)) throw Error(POFD_E_ARG, "Invalid (non-positive) CFIRB sigma");
+    prior_.cfirb_mean[band] = mean;
+    prior_.cfirb_sigma[band] = sigma;
+    prior_.log_cfirb_sigma[band] = std::log(sigma);
+  }
+  prior_.has_cfirb[band] = on ? 1 : 0;
+  drop_graphs();
+}
+
+void Engine2::set_poisson_prior(int band, bool on, double mean, double sigma) {
+  if (band != 0 && band != 1) throw Error(POFD_E_ARG, "band must be 0 or 1");
+  if (on) {
+    if (mean < 0.0) throw Error(POFD_E_ARG, "Invalid (negative) Poisson prior mean");
+    if (!(sigma > 0.0)) throw Error(POFD_E_ARG, "Invalid (non-positive) Poisson prior sigma");
+    prior_.poisson_mean[band] = mean;
+    prior_.poisson_sigma[band] = sigma;
+    prior_.log_poisson_sigma[band] = std::log(sigma);
+  }
+  prior_.has_poisson[band] = on ? 1 : 0;
+  drop_graphs();
+}
+
+void Engine2::set_regularization(double alpha) {
+  if (!(alpha >= 0.0)) throw Error(POFD_E_ARG, "Invalid (negative) regularization alpha");
+  prior_.alpha = alpha;
+  drop_graphs();
+}
+
+// Model set-up into the bonus scratch, then the integrals (fill_at < 0:
+// into ws_.bonus).
+void Engine2::bonus_launch(unsigned nprop, float* theta_dev, unsigned npar, int fill_at,
+                           cudaStream_t st) {
+  const int P = static_cast<int>(nprop);
+  k_model2<<<P, 32, 0, st>>>(model_, theta_dev, static_cast<int>(npar), std::log2(10.0),
+                             ws_.bcnt, ws_.bstatus, ws_.bsig);
+  k_bonus2<<<P, kBonus2Threads, 0, st>>>(model_, theta_dev, static_cast<int>(npar),
+                                         std::log2(10.0), ws_.bcnt, ws_.bstatus, d_qu_, d_qs_,
+                                         d_qw_, d_qk_, nq_, fill_at < 0 ? ws_.bonus : nullptr,
+                                         fill_at);
+  ck(cudaGetLastError(), "k_bonus2");
+}
+
+void Engine2::bonus_host(unsigned nprop, const float* theta, unsigned npar, double* out) {
+  if (nprop == 0) return;
+  if (npar < nparams() + 2) throw Error(POFD_E_ARG, "Not enough elements in params");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  const size_t nb = static_cast<size_t>(nprop) * npar * sizeof(float);
+  float* d = nullptr;
+  ck(cudaMalloc(&d, nb), "cudaMalloc");
+  std::vector<double> o(static_cast<size_t>(nprop) * 8);
+  cudaError_t e = cudaMemcpyAsync(d, theta, nb, cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) {
+    try {
+      bonus_launch(nprop, d, npar, -1, stream_);
+    } catch (...) {
+      cudaFree(d);
+      throw;
+    }
+    e = cudaMemcpyAsync(o.data(), ws_.bonus, o.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                        stream_);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  cudaFree(d);
+  ck(e, "bonus evaluation");
+  for (unsigned i = 0; i < nprop; ++i)
+    for (int c = 0; c < 4; ++c) out[4 * i + c] = o[8 * i + c];
+}
+
+void Engine2::fill_bonus(unsigned nprop, float* theta_dev, unsigned npar, cudaStream_t st) {
+  if (nprop == 0) return;
+  const unsigned nm = nparams();
+  if (npar < nm + 6) throw Error(POFD_E_ARG, "Not enough room to fill");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  bonus_launch(nprop, theta_dev, npar, static_cast<int>(nm + 2), st ? st : stream_);
 }
 
 int Engine2::pd_host(int bs, int ds, const float* theta, unsigned npar,

@@ -75,6 +75,20 @@ struct Model2Dev {
   double minknot, maxknot, min_sigma;
 };
 
+// Priors and regularisation of calcLikeDouble (calcLikeDouble.h:213-232),
+// per band, applied after the beam-set sum in the reference's order
+// (calcLikeDouble.cc:1236-1276); logs of the widths taken on the host.
+struct Prior2 {
+  int has_sigma[2] = {0, 0}, has_cfirb[2] = {0, 0}, has_poisson[2] = {0, 0};
+  double sigma_width[2] = {0, 0}, log_sigma_width[2] = {0, 0};
+  double cfirb_mean[2] = {0, 0}, cfirb_sigma[2] = {0, 0}, log_cfirb_sigma[2] = {0, 0};
+  double poisson_mean[2] = {0, 0}, poisson_sigma[2] = {0, 0}, log_poisson_sigma[2] = {0, 0};
+  double alpha = 0;
+  bool needs_bonus() const {
+    return has_cfirb[0] || has_cfirb[1] || has_poisson[0] || has_poisson[1] || alpha > 0.0;
+  }
+};
+
 struct PDInfo2 {
   int status, s1, s2, pad;
   double itot, minflux1, minflux2, sg1pos, sg1neg, sg2pos, sg2neg, pad2;
@@ -114,7 +128,19 @@ class Engine2 {
   void profile_stages(unsigned nprop, const float* theta, unsigned npar,
                       int reps, double* stage_ms);
   static const char* stage_name(int i);
-  int kernels_per_eval() const { return edge_ ? 12 : 10; }
+  int kernels_per_eval() const { return (edge_ ? 12 : 10) + (prior_.needs_bonus() ? 1 : 0); }
+  // priors per band (calcLikeDouble::setSigmaPrior1/2, setCFIRBPrior1/2,
+  // setPoissonPrior1/2 and unset forms, setRegularizationAlpha,
+  // calcLikeDouble.h:310-341)
+  void set_sigma_prior(int band, bool on, double width);
+  void set_cfirb_prior(int band, bool on, double mean, double sigma);
+  void set_poisson_prior(int band, bool on, double mean, double sigma);
+  void set_regularization(double alpha);
+  // <S1>, <S2>, <S1^2>, <S2^2> per host row -> out[nprop][4]
+  void bonus_host(unsigned nprop, const float* theta, unsigned npar, double* out);
+  // fillBonusParams (calcLikeDouble.cc:1283-1310) on device rows: the four
+  // values at theta_dev[i][nparams() + 2 .. + 5]
+  void fill_bonus(unsigned nprop, float* theta_dev, unsigned npar, cudaStream_t st);
   unsigned nparams() const {
     return static_cast<unsigned>(knots_.size() + sigk_.size() + offk_.size());
   }
@@ -146,6 +172,8 @@ class Engine2 {
     bool warmed = false, no_graph = false;
   };
   void refresh_set(HostSet& s);
+  void bonus_launch(unsigned nprop, float* theta_dev, unsigned npar, int fill_at,
+                    cudaStream_t st);
   void build_static();
   void free_static();
   void free_work();
@@ -177,6 +205,12 @@ class Engine2 {
   unsigned gchunks_ = 1;          // gather chunks per dataset
   std::map<unsigned, Plans> plans_;
   FftWorkArea fftwork_;
+  Prior2 prior_;
+  const double* d_qu_ = nullptr;
+  const double* d_qs_ = nullptr;
+  const double* d_qw_ = nullptr;
+  const int* d_qk_ = nullptr;
+  int nq_ = 0;
   struct Work {
     unsigned P = 0;
     double* cnt = nullptr;      // [P][12*KMAX]
@@ -195,6 +229,10 @@ class Engine2 {
     PDInfo2* pinfo = nullptr;   // [P][D]
     double* gpart = nullptr;    // [P][D][gchunks]
     double* pdout = nullptr;    // [n*n]
+    double* bonus = nullptr;    // [P][8] <S1>, <S2>, <S1^2>, <S2^2>, penalty
+    double* bcnt = nullptr;     // [P][12*KMAX] model scratch of fill_bonus
+    int* bstatus = nullptr;     // [P]
+    double* bsig = nullptr;     // [P][2]
     float* theta_in = nullptr;
     double* logl = nullptr;
     int* status = nullptr;

@@ -635,25 +635,38 @@ void gauss_legendre(int q, std::vector<double>& x, std::vector<double>& w) {
 }
 
 void KnotQuadrature::build(const double* logknots, int K, int panels, int q) {
+  build_breaks(logknots, K, {}, panels, q);
+}
+
+void KnotQuadrature::build_breaks(const double* logknots, int K, std::vector<double> extra,
+                                  int panels, int q) {
   std::vector<double> gx, gw;
   gauss_legendre(q, gx, gw);
   nper = panels * q;
-  const size_t nq = (K > 1) ? static_cast<size_t>(K - 1) * nper : 0;
-  u.assign(nq, 0.0);
-  s.assign(nq, 0.0);
-  w.assign(nq, 0.0);
+  u.clear();
+  s.clear();
+  w.clear();
+  kidx.clear();
+  if (K < 2) return;
+  std::vector<double> br(logknots, logknots + K);
+  for (double e : extra)
+    if (e > logknots[0] && e < logknots[K - 1]) br.push_back(e);
+  std::sort(br.begin(), br.end());
+  br.erase(std::unique(br.begin(), br.end()), br.end());
   const long double ln2 = 0.693147180559945309417232121458176568L;
-  size_t j = 0;
-  for (int k = 0; k + 1 < K; ++k) {
-    const long double a = logknots[k], b = logknots[k + 1];
+  int k = 0;
+  for (size_t i = 0; i + 1 < br.size(); ++i) {
+    while (k + 2 < K && br[i] >= logknots[k + 1]) ++k;
+    const long double a = br[i], b = br[i + 1];
     const long double h = (b - a) / panels;
     for (int p = 0; p < panels; ++p) {
       const long double lo = a + p * h;
-      for (int g = 0; g < q; ++g, ++j) {
+      for (int g = 0; g < q; ++g) {
         const long double uu = lo + 0.5L * h * (gx[g] + 1.0L);
-        u[j] = static_cast<double>(uu);
-        s[j] = static_cast<double>(std::exp2(uu));
-        w[j] = static_cast<double>(ln2 * 0.5L * h * gw[g]);
+        u.push_back(static_cast<double>(uu));
+        s.push_back(static_cast<double>(std::exp2(uu)));
+        w.push_back(static_cast<double>(ln2 * 0.5L * h * gw[g]));
+        kidx.push_back(k);
       }
     }
   }

@@ -101,8 +101,14 @@ void gauss_legendre(int q, std::vector<double>& x, std::vector<double>& w);
 // w_g, so that the integral is sum_j w_j s_j^{a+1} 2^{spline(u_j)}.
 struct KnotQuadrature {
   std::vector<double> u, s, w;
+  std::vector<int> kidx;  // knot interval of each node
   int nper = 0;
   void build(const double* logknots, int K, int panels, int q);
+  // The same with extra breakpoints (log2 S, strictly inside the knot range)
+  // splitting the knot intervals, for integrands with kinks there; nper is
+  // then the nodes per sub-interval and kidx the only interval map.
+  void build_breaks(const double* logknots, int K, std::vector<double> extra, int panels,
+                    int q);
 };
 
 // ------------------------------------------------------------- 2D beam

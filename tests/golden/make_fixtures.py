@@ -125,6 +125,12 @@ def main(refroot):
             "rrange_upper1": [0.039119421, 1e-4],
             "rrange_upper2": [0.0671758809, 1e-4],
         },
+        "integrals2": {
+            "cite": "model_test.cc:681-702 (the model2 model)",
+            "ns": [57266.8, 10.0],
+            "flux_per_area1": [152.262, 0.1],
+            "flux_per_area2": [148.585, 0.1],
+        },
         "counts2": {
             "cite": "model_test.cc:646-677",
             "f1": [0.003, 0.011, 0.011, 0.03],
