@@ -484,12 +484,15 @@ template <int L1, int L2, int S>
 __global__ void __launch_bounds__(256, 2)
 k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
        const double2* __restrict__ in, double2* __restrict__ out,
-       const double2* __restrict__ W) {
+       const double2* __restrict__ WH, const double2* __restrict__ WL) {
   constexpr int M1 = L1 * L2;
   constexpr int M2 = 256;
   constexpr int m = M1 * M2;
   constexpr int CB = 256 / L2;
-  extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b]
+  constexpr int NH = m / 128;
+  extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L
+  double2* Hs = fs + 256 * L1;
+  const double2* Ls = Hs + NH;
   const int row = blockIdx.y;
   if (mstatus[row / nrows_per_w] != 0) return;
   const int b0 = blockIdx.x * CB;
@@ -501,18 +504,20 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
     const int b = t % CB, n2 = t / CB;
 #pragma unroll
     for (int n1 = 0; n1 < L1; ++n1) v[n1] = src[(L2 * n1 + n2) * M2 + b0 + b];
+    fft::load_tw2(Hs, WH, WL, NH, t, 256);
+    __syncthreads();
     fft::dft<L1, S>(v);
     if (L2 > 1) {
 #pragma unroll
       for (int k1 = 0; k1 < L1; ++k1) {
-        if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw<S>(W, (m / M1) * n2 * k1));
+        if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, (m / M1) * n2 * k1));
         fs[(n2 * L1 + k1) * CB + b] = v[k1];
       }
     } else {
 #pragma unroll
       for (int k1 = 0; k1 < L1; ++k1) {
         const int bb = b0 + b;
-        dst[k1 * M2 + bb] = (k1 * bb) ? fft::cmul(v[k1], fft::tw<S>(W, k1 * bb)) : v[k1];
+        dst[k1 * M2 + bb] = (k1 * bb) ? fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, k1 * bb)) : v[k1];
       }
     }
   }
@@ -530,7 +535,7 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
       for (int k2 = 0; k2 < L2; ++k2) {
         const int c = k1 + L1 * k2;
         const int bb = b0 + b;
-        dst[c * M2 + bb] = (c * bb) ? fft::cmul(u[k2], fft::tw<S>(W, c * bb)) : u[k2];
+        dst[c * M2 + bb] = (c * bb) ? fft::cmul(u[k2], fft::tw2<S>(Hs, Ls, c * bb)) : u[k2];
       }
     }
   }
@@ -542,8 +547,10 @@ template <int S>
 __global__ void __launch_bounds__(256, 2)
 k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
        const double2* __restrict__ in, double2* __restrict__ out,
-       const double2* __restrict__ W) {
-  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r]
+       const double2* __restrict__ WH, const double2* __restrict__ WL) {
+  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then H, L
+  double2* Hs = fs + 16 * 16 * 17;
+  const double2* Ls = Hs + 2 * m1;
   const int row = blockIdx.y;
   if (mstatus[row / nrows_per_w] != 0) return;
   const int rb = min(FRB, m1);
@@ -552,15 +559,20 @@ k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
   const int t = threadIdx.x;
   const double2* src = in + static_cast<size_t>(row) * rowsz;
   double2* dst = out + static_cast<size_t>(row) * rowsz;
+  double2 v[16];
   if (t < 16 * rb) {
     const int n2 = t & 15, r = t >> 4;
-    double2 v[16];
 #pragma unroll
     for (int n1 = 0; n1 < 16; ++n1) v[n1] = src[(c0 + r) * 256 + 16 * n1 + n2];
+  }
+  fft::load_tw2(Hs, WH, WL, 2 * m1, t, 256);
+  __syncthreads();
+  if (t < 16 * rb) {
+    const int n2 = t & 15, r = t >> 4;
     fft::dft<16, S>(v);
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) {
-      if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw<S>(W, (m / 256) * n2 * k1));
+      if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, (m / 256) * n2 * k1));
       fs[(k1 * 16 + n2) * 17 + r] = v[k1];
     }
   }
@@ -1137,13 +1149,19 @@ T* dalloc(size_t n) {
 // ===================================================================== host
 
 namespace {
-constexpr size_t kFftASmem = 256 * 16 * sizeof(double2);  // CB * m1 = 256 * L1
+// exchange (256 L1 entries) plus the twiddle tables: H has m / 128 = 2 m1
+// entries, L 128
+constexpr size_t kFftASmemMax = (256 * 16 + 2 * 256 + 128) * sizeof(double2);
+inline size_t fftA_smem(int m1) {
+  return (256 * static_cast<size_t>(m1 < 16 ? m1 : 16) + 2 * m1 + 128) * sizeof(double2);
+}
 
 template <int S>
 void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const int* mstatus,
-                 const double2* in, double2* out, const double2* W) {
+                 const double2* in, double2* out, const double2* WH, const double2* WL) {
 #define POFD_FFTA(L1, L2)                                                              \
-  k_fftA<L1, L2, S><<<dim3(L2, rows), 256, kFftASmem, st>>>(rowsz, nrw, mstatus, in, out, W)
+  k_fftA<L1, L2, S><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(rowsz, nrw, mstatus, in, out, \
+                                                                WH, WL)
   switch (m1) {
     case 8: POFD_FFTA(8, 1); break;
     case 16: POFD_FFTA(16, 1); break;
@@ -1158,7 +1176,7 @@ void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const in
 
 template <int S>
 void fftA_attr() {
-  const int sm = static_cast<int>(kFftASmem);
+  const int sm = static_cast<int>(kFftASmemMax);
   cuda_check(cudaFuncSetAttribute(k_fftA<8, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
   cuda_check(cudaFuncSetAttribute(k_fftA<16, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
   cuda_check(cudaFuncSetAttribute(k_fftA<16, 2, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
@@ -1167,7 +1185,10 @@ void fftA_attr() {
   cuda_check(cudaFuncSetAttribute(k_fftA<16, 16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
 }
 
-constexpr size_t kFftBSmem = 16 * 16 * 17 * sizeof(double2);
+constexpr size_t kFftBSmemMax = (16 * 16 * 17 + 2 * 256 + 128) * sizeof(double2);
+inline size_t fftB_smem(int m1) {
+  return (16 * 16 * 17 + 2 * static_cast<size_t>(m1) + 128) * sizeof(double2);
+}
 }  // namespace
 
 
@@ -1534,21 +1555,28 @@ void Engine1::build_static() {
   own_fft_ = fft_mode_ == 0 && n_ >= 4096 && n_ <= 131072 && (n_ & (n_ - 1)) == 0;
   if (own_fft_) {
     const size_t m = n_ / 2;
-    std::vector<double2> wm(m), wn(m + 1);
+    std::vector<double2> wh(m / 128), wl(128), wn(m + 1);
     const long double tau = 6.283185307179586476925286766559005768L;
-    for (size_t t = 0; t < m; ++t) {
-      const long double a = -tau * static_cast<long double>(t) / static_cast<long double>(m);
-      wm[t] = make_double2(static_cast<double>(cosl(a)), static_cast<double>(sinl(a)));
+    for (size_t j = 0; j < m / 128; ++j) {
+      const long double a = -tau * static_cast<long double>(128 * j) / static_cast<long double>(m);
+      wh[j] = make_double2(static_cast<double>(cosl(a)), static_cast<double>(sinl(a)));
+    }
+    for (size_t i = 0; i < 128; ++i) {
+      const long double a = -tau * static_cast<long double>(i) / static_cast<long double>(m);
+      wl[i] = make_double2(static_cast<double>(cosl(a)), static_cast<double>(sinl(a)));
     }
     for (size_t k = 0; k <= m; ++k) {
       const long double a = -tau * static_cast<long double>(k) / static_cast<long double>(n_);
       wn[k] = make_double2(static_cast<double>(cosl(a)), static_cast<double>(sinl(a)));
     }
-    d_wm_ = dalloc<double2>(m);
-    static_allocs_.push_back(d_wm_);
+    d_wh_ = dalloc<double2>(m / 128);
+    static_allocs_.push_back(d_wh_);
+    d_wl_ = dalloc<double2>(128);
+    static_allocs_.push_back(d_wl_);
     d_wn_ = dalloc<double2>(m + 1);
     static_allocs_.push_back(d_wn_);
-    cuda_check(cudaMemcpy(d_wm_, wm.data(), m * sizeof(double2), cudaMemcpyHostToDevice), "upload");
+    cuda_check(cudaMemcpy(d_wh_, wh.data(), wh.size() * sizeof(double2), cudaMemcpyHostToDevice), "upload");
+    cuda_check(cudaMemcpy(d_wl_, wl.data(), wl.size() * sizeof(double2), cudaMemcpyHostToDevice), "upload");
     cuda_check(cudaMemcpy(d_wn_, wn.data(), (m + 1) * sizeof(double2), cudaMemcpyHostToDevice), "upload");
   }
   static_ok_ = true;
@@ -1738,9 +1766,9 @@ void Engine1::reserve(unsigned P) {
     fftA_attr<-1>();
     fftA_attr<1>();
     cuda_check(cudaFuncSetAttribute(k_fftB<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(kFftBSmem)), "attr");
+                                    static_cast<int>(kFftBSmemMax)), "attr");
     cuda_check(cudaFuncSetAttribute(k_fftB<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(kFftBSmem)), "attr");
+                                    static_cast<int>(kFftBSmemMax)), "attr");
   }
   ws_.mom = dalloc<double>(static_cast<size_t>(P) * B_ * 4);
   ws_.pbuf = dalloc<double>(static_cast<size_t>(P) * D_ * nc2);
@@ -1832,9 +1860,9 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                                     ws_.mstatus, ws_.rbuf, ws_.rpart, ws_.mom);
     mark(4);
     const int rb_rows = m1 < FRB ? m1 : FRB;
-    launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wm_);
-    k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, kFftBSmem, st>>>(m1, rowsz, B, ws_.mstatus, tmp,
-                                                                 rb, d_wm_);
+    launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_);
+    k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, fftB_smem(m1), st>>>(
+        m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_);
     mark(5);
     {
       dim3 grid((m / 2 + 1 + NT - 1) / NT, P * B);
@@ -1842,9 +1870,9 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                         ws_.sigmult, ws_.mom, rb, pb, d_wn_);
     }
     mark(6);
-    launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wm_);
-    k_fftB<1><<<dim3(m1 / rb_rows, P * D), 256, kFftBSmem, st>>>(m1, rowsz, D, ws_.mstatus, tmp,
-                                                                pb, d_wm_);
+    launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_);
+    k_fftB<1><<<dim3(m1 / rb_rows, P * D), 256, fftB_smem(m1), st>>>(
+        m1, rowsz, D, ws_.mstatus, tmp, pb, d_wh_, d_wl_);
   } else {
     {
       dim3 grid(ntile_, P * B);

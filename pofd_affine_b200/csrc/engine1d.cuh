@@ -240,7 +240,8 @@ class Engine1 {
   FftWorkArea fftwork_;
   int fft_mode_ = 0;
   bool own_fft_ = false;
-  double2* d_wm_ = nullptr;  // e^{-2 pi i t / m}, t < m
+  double2* d_wh_ = nullptr;  // e^{-2 pi i 128 j / m}, j < m / 128
+  double2* d_wl_ = nullptr;  // e^{-2 pi i i / m}, i < 128
   double2* d_wn_ = nullptr;  // e^{-2 pi i k / n}, k <= m
   // priors and the knot quadrature of the bonus integrals
   Prior1 prior_;

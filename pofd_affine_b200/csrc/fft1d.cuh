@@ -15,7 +15,7 @@
 // partial results meet in shared memory for the L2-point register DFTs.
 // The register DFTs are radix-2 decimation in time on at most 16 points with
 // exact constant twiddles; all other twiddles come from tables built on the
-// host in long double.
+// host in long double and are read from shared memory (fft::tw2).
 #ifndef POFD_FFT1D_CUH
 #define POFD_FFT1D_CUH
 
@@ -84,11 +84,28 @@ __device__ __forceinline__ void dft(double2* v) {
   }
 }
 
-// Twiddle e^{S 2 pi i t / m} from the forward table W[t] = e^{-2 pi i t/m}.
+// Twiddle e^{S 2 pi i t / m}, t < m, from two shared-memory tables:
+// H[j] = e^{-2 pi i 128 j / m} (m / 128 entries) and L[i] = e^{-2 pi i i / m}
+// (128 entries), W^t = H[t >> 7] L[t & 127] -- exact (one table entry) when
+// t is a multiple of 128, else one complex product of two correctly rounded
+// values.
 template <int S>
-__device__ __forceinline__ double2 tw(const double2* __restrict__ W, int t) {
-  const double2 w = __ldg(W + t);
+__device__ __forceinline__ double2 tw2(const double2* H, const double2* L, int t) {
+  const double2 h = H[t >> 7];
+  const int lo = t & 127;
+  const double2 w = lo ? cmul(h, L[lo]) : h;
   return (S < 0) ? w : make_double2(w.x, -w.y);
+}
+
+// Loads the two twiddle tables (nh = m / 128 entries of H, then 128 of L)
+// into shared memory; the caller synchronises before use.
+__device__ __forceinline__ void load_tw2(double2* Hs, const double2* __restrict__ WH,
+                                         const double2* __restrict__ WL, int nh, int t,
+                                         int nthreads) {
+  for (int i = t; i < nh + 128; i += nthreads) {
+    if (i < nh) Hs[i] = __ldg(WH + i);
+    else Hs[i] = __ldg(WL + (i - nh));
+  }
 }
 
 }  // namespace fft
