@@ -101,9 +101,16 @@ struct pofd_pdfactory1 {
   bool inited = false;
 };
 
+namespace pofd {
+// Lets entry points outside this file (the allocation-free one) report a
+// message through pofd_last_error().
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace pofd
+
 extern "C" {
 
 const char* pofd_last_error(void) { return g_err.c_str(); }
+
 const char* pofd_version(void) { return "pofd_b200 0.1.0 (reference pofd_affine 0.5.1)"; }
 
 // ------------------------------------------------------------- context

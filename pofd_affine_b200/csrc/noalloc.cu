@@ -265,27 +265,44 @@ k_na_pfinish(const double* __restrict__ p, int n, double dflux,
 
 }  // namespace
 
+namespace pofd {
+void set_last_error(const char* msg);  // capi.cu
+}
+
 extern "C" int pofd_pd1_loglike_noalloc(
     const double* pofd_dev, unsigned n, double dflux, double minflux_R,
     unsigned wrapRidx, double var_noi, double sigma, const int* nzidx_dev,
     const double* nzcnt_dev, unsigned nnz, double bincent0, double bindelta,
     double like_offset, double like_norm, double* out_dev, int* status_dev,
     void* stream) {
-  if (!pofd_dev || !out_dev || !status_dev || (nnz > 0 && (!nzidx_dev || !nzcnt_dev)))
+  if (!pofd_dev || !out_dev || !status_dev || (nnz > 0 && (!nzidx_dev || !nzcnt_dev))) {
+    pofd::set_last_error("pofd_pd1_loglike_noalloc: null device pointer");
     return POFD_E_ARG;
-  if (n < 2 || n > kMaxN) return POFD_E_ARG;  // n beyond the fixed scratch
-  if (!(dflux > 0) || wrapRidx < 1 || wrapRidx >= n) return POFD_E_ARG;
+  }
+  if (n < 2 || n > kMaxN) {
+    // n beyond the fixed scratch (64 chunks of 4096 values)
+    pofd::set_last_error("pofd_pd1_loglike_noalloc: n must be in [2, 262144]");
+    return POFD_E_ARG;
+  }
+  if (!(dflux > 0) || wrapRidx < 1 || wrapRidx >= n) {
+    pofd::set_last_error("pofd_pd1_loglike_noalloc: need dflux > 0 and 1 <= wrapRidx < n");
+    return POFD_E_ARG;
+  }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    pofd::set_last_error("pofd_pd1_loglike_noalloc: no usable current device");
     return POFD_E_CUDA;
+  }
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mtx);
     if (!g_scratch_addr[dev]) {
       // set-up, once per device, with that device current
       void* ptr = nullptr;
-      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
+      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+        pofd::set_last_error("pofd_pd1_loglike_noalloc: scratch address lookup failed");
         return POFD_E_CUDA;
+      }
       g_scratch_addr[dev] = static_cast<double*>(ptr);
     }
     scratch = g_scratch_addr[dev];

@@ -99,3 +99,4 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(gpu_ctx):
                                         1e-6, 1e-3, dummy, dummy, 1, 0.0, 1.0,
                                         0.0, 1.0, dummy, dummy, None)
     assert rc == -10
+    assert b"262144" in lib().pofd_last_error()
