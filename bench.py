@@ -188,17 +188,64 @@ def reference_arm(a, cfg):
 
 
 # ---------------------------------------------------------------- roofline
-def stage_bytes(stage, P, B, D, n):
+def noise_cuts(L, cfg, theta):
+    """Per beam set and dataset, the own-FFT path's noise cut-off (bins k
+    with min(k, m - k) > kc carry exp(-sigma^2 w_k^2 / 2) < e^-760, i.e.
+    exactly 0; the same formula as the library's noise_cut), with the grid
+    step of each beam set from the library and sigma = the dataset's noise
+    (the proposals keep the sigma multiplier at 1)."""
+    n = cfg["fftsize"]
+    m = n // 2
+    sets = []
+    for b in range(len(cfg["beams"])):
+        dflux = L.getPD(b, 0, theta, setLog=False)[1]["dflux"]
+        iflux = 2 * np.pi / (n * dflux)
+        kcs = []
+        for d, bi in enumerate(cfg["map_beam"]):
+            if bi != b:
+                continue
+            x = np.sqrt(1520.0) / (cfg["sigmas"][d] * iflux)
+            kcs.append(m if x >= m else int(np.ceil(x)) + 1)
+        sets.append(kcs)
+    return sets
+
+
+def stage_bytes(stage, P, B, D, n, cuts=None):
     """Algorithmic HBM bytes per launch of an HBM-bound stage (one
-    compulsory FP64 read/write of each array it streams)."""
+    compulsory FP64 read/write of each array it streams).  With the noise
+    cut-offs of the own-FFT path (noise_cuts), the bins that path skips:
+    forward pass B writes only bins with min(k, m - k) <= kc of the beam
+    set (the widest of its datasets), the spectrum reads only those pairs
+    and writes, per dataset, only the 256-bin rows the inverse pass A reads,
+    and pass A reads only those rows."""
     nc = n // 2 + 1
+    m = n // 2
+    row = 16.0 * m  # one complex row of m points
+    fwd = 4.0 * row * P * B
+    spec = 8.0 * n * P * B + 8.0 * n * P * D
+    inv = 4.0 * row * P * D
+    if cuts is not None:
+        k = np.arange(m)
+        kmin = np.minimum(k, m - k)
+        a = np.arange(m // 256)
+        rmin = np.minimum(256 * a, m - 256 * a - 255)
+        fwd = inv = spec = 0.0
+        for kcs in cuts:
+            kset = max(kcs) if kcs else m
+            f = float(np.mean(kmin <= kset))
+            fwd += P * row * (3.0 + f)
+            spec += P * 32.0 * (min(kset, m // 2) + 1)
+            for kc in kcs:
+                g = float(np.mean(rmin <= kc))
+                spec += P * row * g
+                inv += P * row * (3.0 + g)
     return {
         # own FFT path (n = 2m, m complex per row): passes A and B each read
         # and write the rows; the spectrum reads Z and writes one row per
         # dataset
-        "k_fftA1+k_fftB1": 32.0 * n * P * B,
-        "k_spectrum1f": 8.0 * n * P * B + 8.0 * n * P * D,
-        "k_fftA1+k_fftB1_inv": 32.0 * n * P * D,
+        "k_fftA1+k_fftB1": fwd,
+        "k_spectrum1f": spec,
+        "k_fftA1+k_fftB1_inv": inv,
         "k_rfill1": 8.0 * n * P * B,                         # write R
         "k_spectrum1": 16.0 * nc * P * B + 16.0 * nc * P * D,  # read R~, write per-dataset spectra
         "k_pscan1": 8.0 * n * P * D,                          # read P(D)
@@ -497,7 +544,8 @@ def main():
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     hbm_peak = hb.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in hb else "fallback"
-    nbytes = stage_bytes(dom, BATCH, B, D, n)
+    cuts = noise_cuts(L, cfg, cfg["theta0"]) if L.ownFFT() else None
+    nbytes = stage_bytes(dom, BATCH, B, D, n, cuts)
     if nbytes is not None:
         ach = nbytes / (own[dom] * 1e-3) / 1e9
         traffic = read_traffic(dom)
@@ -515,7 +563,7 @@ def main():
                 "peak_source": "measured (pofd_fp64_peak DFMA loop)",
                 "achieved": None, "frac": None,
                 "traffic": read_traffic(dom)}
-    hbm_pipe = sum(stage_bytes(s, BATCH, B, D, n) or 0 for s in stages)
+    hbm_pipe = sum(stage_bytes(s, BATCH, B, D, n, cuts) or 0 for s in stages)
     nk = L.kernelsPerEval()
 
     extra = {}

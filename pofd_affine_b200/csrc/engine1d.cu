@@ -372,17 +372,51 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
 
 // Moments, sigma estimate and the shift decision (PDFactory.cc:660-679,
 // 1067-1076), one thread per (proposal, beam set).
-__global__ void k_moments1(const BSet1Dev* __restrict__ bsets, int B, int n,
+// Noise cut-off of the half-length spectrum (own-FFT path): with noise sigma
+// the factor exp(-sigma^2 w_k^2 / 2) is below e^-760 -- exactly 0 in double
+// precision, whose exp underflows below -745.2 -- for every bin k with
+// min(k, m - k) > kc, kc = ceil(sqrt(1520) / (sigma * 2 pi / (n dflux))) + 1.
+// Returns m (no bin is cut) without noise.
+__device__ __forceinline__ int noise_cut(double sigma, double dflux, int n) {
+  const int m = n / 2;
+  if (!(sigma > 0.0)) return m;
+  const double iflux = dev::kTwoPi / (static_cast<double>(n) * dflux);
+  const double x = sqrt(1520.0) / (sigma * iflux);
+  return (x >= static_cast<double>(m)) ? m : static_cast<int>(ceil(x)) + 1;
+}
+
+// Rows of 256 bins (row a: bins [256 a, 256 a + 256) of the m1 x 256 view)
+// whose bins all lie beyond the cut-off.
+__device__ __forceinline__ bool row_cut(int a, int m, int kc) {
+  return min(256 * a, m - 256 * a - 255) > kc;
+}
+
+__global__ void k_moments1(const BSet1Dev* __restrict__ bsets,
+                           const DSet1Dev* __restrict__ dsets, int B, int D, int n,
                            int nc2, int ntile, int nrow,
                            const int* __restrict__ mstatus,
+                           const double* __restrict__ sigmult,
                            const double* __restrict__ rbuf,
                            const double* __restrict__ rpart,
-                           double* __restrict__ mom) {
+                           double* __restrict__ mom, int* __restrict__ kcut_set,
+                           int* __restrict__ kcut_ds) {
   const int wb = blockIdx.x * blockDim.x + threadIdx.x;
   if (wb >= nrow) return;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
   const BSet1Dev& bs = bsets[b];
+  if (kcut_set) {
+    // bins the spectrum kernel reads: the widest cut-off of the set's
+    // datasets; per dataset for the inverse transform's input
+    int kmax = 0;
+    for (int dd = 0; dd < bs.nds; ++dd) {
+      const int d = bs.ds_begin + dd;
+      const int kc = noise_cut(sigmult[w] * dsets[d].sigma_base, bs.dflux, n);
+      kcut_ds[static_cast<size_t>(w) * D + d] = kc;
+      kmax = max(kmax, kc);
+    }
+    kcut_set[wb] = (bs.nds > 0) ? kmax : n / 2;
+  }
   double mn = 0.0, var = 0.0;
   const double* p = rpart + static_cast<size_t>(wb) * ntile * 2;
   for (int t = 0; t < ntile; ++t) {
@@ -484,7 +518,8 @@ template <int L1, int L2, int S>
 __global__ void __launch_bounds__(256, 2)
 k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
        const double2* __restrict__ in, double2* __restrict__ out,
-       const double2* __restrict__ WH, const double2* __restrict__ WL) {
+       const double2* __restrict__ WH, const double2* __restrict__ WL,
+       const int* __restrict__ kcut) {
   constexpr int M1 = L1 * L2;
   constexpr int M2 = 256;
   constexpr int m = M1 * M2;
@@ -502,8 +537,13 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
   double2 v[L1];
   {
     const int b = t % CB, n2 = t / CB;
+    // inverse input: rows beyond the noise cut-off are zero and not read
+    const int kc = kcut ? kcut[row] : m;
 #pragma unroll
-    for (int n1 = 0; n1 < L1; ++n1) v[n1] = src[(L2 * n1 + n2) * M2 + b0 + b];
+    for (int n1 = 0; n1 < L1; ++n1) {
+      const int a = L2 * n1 + n2;
+      v[n1] = row_cut(a, m, kc) ? make_double2(0.0, 0.0) : src[a * M2 + b0 + b];
+    }
     fft::load_tw2(Hs, WH, WL, NH, t, 256);
     __syncthreads();
     fft::dft<L1, S>(v);
@@ -547,7 +587,8 @@ template <int S>
 __global__ void __launch_bounds__(256, 2)
 k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
        const double2* __restrict__ in, double2* __restrict__ out,
-       const double2* __restrict__ WH, const double2* __restrict__ WL) {
+       const double2* __restrict__ WH, const double2* __restrict__ WL,
+       const int* __restrict__ kcut) {
   extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then H, L
   double2* Hs = fs + 16 * 16 * 17;
   const double2* Ls = Hs + 2 * m1;
@@ -559,6 +600,7 @@ k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
   const int t = threadIdx.x;
   const double2* src = in + static_cast<size_t>(row) * rowsz;
   double2* dst = out + static_cast<size_t>(row) * rowsz;
+  const int kc = kcut ? kcut[row] : m;
   double2 v[16];
   if (t < 16 * rb) {
     const int n2 = t & 15, r = t >> 4;
@@ -584,7 +626,11 @@ k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
     for (int n2 = 0; n2 < 16; ++n2) u[n2] = fs[(k1 * 16 + n2) * 17 + r];
     fft::dft<16, S>(u);
 #pragma unroll
-    for (int k2 = 0; k2 < 16; ++k2) dst[(c0 + r) + m1 * (k1 + 16 * k2)] = u[k2];
+    for (int k2 = 0; k2 < 16; ++k2) {
+      // bins beyond the noise cut-off are never read (forward transform)
+      const int k = (c0 + r) + m1 * (k1 + 16 * k2);
+      if (min(k, m - k) <= kc) dst[k] = u[k2];
+    }
   }
 }
 
@@ -622,13 +668,12 @@ k_spectrum1f(const BSet1Dev* __restrict__ bsets, const DSet1Dev* __restrict__ ds
              int D, int n, int rowsz, const int* __restrict__ mstatus,
              const double* __restrict__ sigmult, const double* __restrict__ mom,
              const double2* __restrict__ zbuf, double2* __restrict__ pbuf,
-             const double2* __restrict__ Wn) {
+             const double2* __restrict__ Wn, const int* __restrict__ kcut_set,
+             const int* __restrict__ kcut_ds) {
   const int wb = blockIdx.y;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
   const int m = n / 2;
-  const int q = blockIdx.x * NT + threadIdx.x;
-  if (q > m / 2) return;
   const BSet1Dev& bs = bsets[b];
   const double iflux = dev::kTwoPi / (static_cast<double>(n) * bs.dflux);
   const double sm = sigmult[w];
@@ -636,56 +681,64 @@ k_spectrum1f(const BSet1Dev* __restrict__ bsets, const DSet1Dev* __restrict__ ds
   const bool doshift = mo[3] != 0.0;
   const double shiftw = mo[2] * iflux;
   const double2* Z = zbuf + static_cast<size_t>(wb) * rowsz;
-  const int ka = q, kb = (q == 0) ? m : m - q;  // bins of the pair
-  const bool za = spec_all_zero(bs, dsets, sm, iflux * ka, ka);
-  const bool zb = spec_all_zero(bs, dsets, sm, iflux * kb, kb);
-  double2 pa = make_double2(0.0, 0.0), pb = make_double2(0.0, 0.0);
-  if (!(za && zb)) {
-    const double2 z0 = Z[0];
-    const double r0 = z0.x + z0.y;  // X_0
-    double2 Xa, Xb;
-    if (q == 0) {
-      Xa = make_double2(r0, 0.0);
-      Xb = make_double2(z0.x - z0.y, 0.0);  // X_m
-    } else {
-      const double2 a = Z[q], c = Z[m - q];
-      // E_k = (Z_k + conj Z_{m-k}) / 2, O_k = (Z_k - conj Z_{m-k}) / (2i)
-      const double2 Ea = make_double2(0.5 * (a.x + c.x), 0.5 * (a.y - c.y));
-      const double2 Oa = make_double2(0.5 * (a.y + c.y), -0.5 * (a.x - c.x));
-      const double2 Eb = make_double2(Ea.x, -Ea.y);
-      const double2 Ob = make_double2(0.5 * (c.y + a.y), -0.5 * (c.x - a.x));
-      Xa = fft::cadd(Ea, fft::cmul(__ldg(Wn + q), Oa));
-      Xb = fft::cadd(Eb, fft::cmul(__ldg(Wn + m - q), Ob));
-    }
-    if (!za) pa = spec_p(Xa, r0, ka, m, doshift, shiftw);
-    if (!zb) pb = spec_p(Xb, r0, kb, m, doshift, shiftw);
-  }
-  for (int dd = 0; dd < bs.nds; ++dd) {
-    const int d = bs.ds_begin + dd;
-    const double sigma = sm * dsets[d].sigma_base;
-    double2 Pa = pa, Pb = pb;
-    if (sigma > 0) {
-      const double sigfac = -0.5 * sigma * sigma;
-      if (ka > 0) {
-        const double wv = iflux * ka;
-        const double ef = exp(sigfac * wv * wv);
-        Pa = make_double2(ef * pa.x, ef * pa.y);
+  // pairs up to the widest cut-off of the set plus one row of 256 bins cover
+  // every bin of a row the inverse transform reads (at either end)
+  const int qmax = min(m / 2, kcut_set[wb] + 256);
+  for (int q = blockIdx.x * NT + threadIdx.x; q <= qmax; q += gridDim.x * NT) {
+    const int ka = q, kb = (q == 0) ? m : m - q;  // bins of the pair
+    const bool za = spec_all_zero(bs, dsets, sm, iflux * ka, ka);
+    const bool zb = spec_all_zero(bs, dsets, sm, iflux * kb, kb);
+    double2 pa = make_double2(0.0, 0.0), pb = make_double2(0.0, 0.0);
+    if (!(za && zb)) {
+      const double2 z0 = Z[0];
+      const double r0 = z0.x + z0.y;  // X_0
+      double2 Xa, Xb;
+      if (q == 0) {
+        Xa = make_double2(r0, 0.0);
+        Xb = make_double2(z0.x - z0.y, 0.0);  // X_m
+      } else {
+        const double2 a = Z[q], c = Z[m - q];
+        // E_k = (Z_k + conj Z_{m-k}) / 2, O_k = (Z_k - conj Z_{m-k}) / (2i)
+        const double2 Ea = make_double2(0.5 * (a.x + c.x), 0.5 * (a.y - c.y));
+        const double2 Oa = make_double2(0.5 * (a.y + c.y), -0.5 * (a.x - c.x));
+        const double2 Eb = make_double2(Ea.x, -Ea.y);
+        const double2 Ob = make_double2(0.5 * (c.y + a.y), -0.5 * (c.x - a.x));
+        Xa = fft::cadd(Ea, fft::cmul(__ldg(Wn + q), Oa));
+        Xb = fft::cadd(Eb, fft::cmul(__ldg(Wn + m - q), Ob));
       }
-      const double wv = iflux * kb;
-      const double ef = exp(sigfac * wv * wv);
-      Pb = make_double2(ef * pb.x, ef * pb.y);
+      if (!za) pa = spec_p(Xa, r0, ka, m, doshift, shiftw);
+      if (!zb) pb = spec_p(Xb, r0, kb, m, doshift, shiftw);
     }
-    double2* out = pbuf + static_cast<size_t>(w * D + d) * rowsz;
-    // Z'_k = (P_k + conj P_{m-k}) + i (P_k - conj P_{m-k}) e^{+2 pi i k / n}
-    {
-      const double2 e = make_double2(Pa.x + Pb.x, Pa.y - Pb.y);
-      const double2 o = fft::cmul(make_double2(Pa.x - Pb.x, Pa.y + Pb.y), fft::conj(__ldg(Wn + ka)));
-      out[ka] = make_double2(e.x - o.y, e.y + o.x);
-    }
-    if (q != 0 && kb != ka) {
-      const double2 e = make_double2(Pb.x + Pa.x, Pb.y - Pa.y);
-      const double2 o = fft::cmul(make_double2(Pb.x - Pa.x, Pb.y + Pa.y), fft::conj(__ldg(Wn + kb)));
-      out[kb] = make_double2(e.x - o.y, e.y + o.x);
+    for (int dd = 0; dd < bs.nds; ++dd) {
+      const int d = bs.ds_begin + dd;
+      const double sigma = sm * dsets[d].sigma_base;
+      double2 Pa = pa, Pb = pb;
+      if (sigma > 0) {
+        const double sigfac = -0.5 * sigma * sigma;
+        if (ka > 0) {
+          const double wv = iflux * ka;
+          const double ef = exp(sigfac * wv * wv);
+          Pa = make_double2(ef * pa.x, ef * pa.y);
+        }
+        const double wv = iflux * kb;
+        const double ef = exp(sigfac * wv * wv);
+        Pb = make_double2(ef * pb.x, ef * pb.y);
+      }
+      double2* out = pbuf + static_cast<size_t>(w * D + d) * rowsz;
+      // rows the inverse transform does not read (every bin beyond the noise
+      // cut-off, hence zero) are not written
+      const int kc = kcut_ds[static_cast<size_t>(w) * D + d];
+      // Z'_k = (P_k + conj P_{m-k}) + i (P_k - conj P_{m-k}) e^{+2 pi i k / n}
+      if (!row_cut(ka >> 8, m, kc)) {
+        const double2 e = make_double2(Pa.x + Pb.x, Pa.y - Pb.y);
+        const double2 o = fft::cmul(make_double2(Pa.x - Pb.x, Pa.y + Pb.y), fft::conj(__ldg(Wn + ka)));
+        out[ka] = make_double2(e.x - o.y, e.y + o.x);
+      }
+      if (q != 0 && kb != ka && !row_cut(kb >> 8, m, kc)) {
+        const double2 e = make_double2(Pb.x + Pa.x, Pb.y - Pa.y);
+        const double2 o = fft::cmul(make_double2(Pb.x - Pa.x, Pb.y + Pa.y), fft::conj(__ldg(Wn + kb)));
+        out[kb] = make_double2(e.x - o.y, e.y + o.x);
+      }
     }
   }
 }
@@ -1158,10 +1211,11 @@ inline size_t fftA_smem(int m1) {
 
 template <int S>
 void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const int* mstatus,
-                 const double2* in, double2* out, const double2* WH, const double2* WL) {
+                 const double2* in, double2* out, const double2* WH, const double2* WL,
+                 const int* kcut) {
 #define POFD_FFTA(L1, L2)                                                              \
   k_fftA<L1, L2, S><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(rowsz, nrw, mstatus, in, out, \
-                                                                WH, WL)
+                                                                WH, WL, kcut)
   switch (m1) {
     case 8: POFD_FFTA(8, 1); break;
     case 16: POFD_FFTA(16, 1); break;
@@ -1730,7 +1784,7 @@ void Engine1::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.nodes, ws_.spl,
                   ws_.rbuf, ws_.rpart, ws_.mom, ws_.pbuf, ws_.ppart,
                   ws_.pmidx, ws_.pinfo, ws_.pdout, ws_.theta_in, ws_.logl,
-                  ws_.status, ws_.tmp, ws_.bonus};
+                  ws_.status, ws_.tmp, ws_.bonus, ws_.kcut_set, ws_.kcut_ds};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
@@ -1771,6 +1825,8 @@ void Engine1::reserve(unsigned P) {
                                     static_cast<int>(kFftBSmemMax)), "attr");
   }
   ws_.mom = dalloc<double>(static_cast<size_t>(P) * B_ * 4);
+  ws_.kcut_set = dalloc<int>(static_cast<size_t>(P) * B_);
+  ws_.kcut_ds = dalloc<int>(static_cast<size_t>(P) * D_);
   ws_.pbuf = dalloc<double>(static_cast<size_t>(P) * D_ * nc2);
   ws_.ppart = dalloc<double>(static_cast<size_t>(P) * D_ * nchunk_ * 4);
   ws_.pmidx = dalloc<int>(static_cast<size_t>(P) * D_ * nchunk_);
@@ -1855,24 +1911,27 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                     ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
-    k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, B, n, nc2,
+    k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
                                                     static_cast<int>(ntile_), P * B,
-                                                    ws_.mstatus, ws_.rbuf, ws_.rpart, ws_.mom);
+                                                    ws_.mstatus, ws_.sigmult, ws_.rbuf, ws_.rpart,
+                                                    ws_.mom, ws_.kcut_set, ws_.kcut_ds);
     mark(4);
     const int rb_rows = m1 < FRB ? m1 : FRB;
-    launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_);
+    launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
     k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, fftB_smem(m1), st>>>(
-        m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_);
+        m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_, ws_.kcut_set);
     mark(5);
     {
-      dim3 grid((m / 2 + 1 + NT - 1) / NT, P * B);
+      // a few blocks per row loop over the pairs up to the row's cut-off
+      dim3 grid(std::min((m / 2 + 1 + NT - 1) / NT, 8), P * B);
       k_spectrum1f<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, rowsz, ws_.mstatus,
-                                        ws_.sigmult, ws_.mom, rb, pb, d_wn_);
+                                        ws_.sigmult, ws_.mom, rb, pb, d_wn_, ws_.kcut_set,
+                                        ws_.kcut_ds);
     }
     mark(6);
-    launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_);
+    launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_, ws_.kcut_ds);
     k_fftB<1><<<dim3(m1 / rb_rows, P * D), 256, fftB_smem(m1), st>>>(
-        m1, rowsz, D, ws_.mstatus, tmp, pb, d_wh_, d_wl_);
+        m1, rowsz, D, ws_.mstatus, tmp, pb, d_wh_, d_wl_, nullptr);
   } else {
     {
       dim3 grid(ntile_, P * B);
@@ -1880,10 +1939,10 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                     ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
-    k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, B, n, nc2,
+    k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
                                                     static_cast<int>(ntile_), P * B,
-                                                    ws_.mstatus, ws_.rbuf,
-                                                    ws_.rpart, ws_.mom);
+                                                    ws_.mstatus, ws_.sigmult, ws_.rbuf,
+                                                    ws_.rpart, ws_.mom, nullptr, nullptr);
     mark(4);
     cufft_check(cufftSetStream(pl.fwd, st), "cufftSetStream");
     cufft_check(cufftExecD2Z(pl.fwd, ws_.rbuf, reinterpret_cast<cufftDoubleComplex*>(ws_.rbuf)),

@@ -102,6 +102,8 @@ struct Workspace1 {
   double* rbuf = nullptr;    // [P][B][2*(n/2+1)] R grid / spectrum
   double* rpart = nullptr;   // [P][B][ntile][2]
   double* mom = nullptr;     // [P][B][4] mean, var, shift, doshift
+  int* kcut_set = nullptr;   // [P][B] noise cut-off of the forward spectrum
+  int* kcut_ds = nullptr;    // [P][D] noise cut-off of each dataset's spectrum
   double* pbuf = nullptr;    // [P][D][2*(n/2+1)] spectrum / P(D)
   double* tmp = nullptr;     // [P][max(B,D)][2*(n/2+1)] own-FFT pass-A rows
   double* ppart = nullptr;   // [P][D][nchunk][4] max, sum, wsum, minval
