@@ -49,6 +49,8 @@ def args():
                    help="CPU-baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-2d", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the default launch shapes (skip the autotuner)")
     p.add_argument("--no-mcmc", action="store_true")
     p.add_argument("--mcmc-2d", type=int, default=1,
                    help="include the two-field 2D MCMC comparison")
@@ -472,6 +474,8 @@ def main():
     nbatches = 4  # distinct resident proposal batches, cycled
     host = [synth.proposals(cfg["theta0"], BATCH, 0.02, rng=100 * rank + k)
             for k in range(nbatches)]
+    # launch shapes chosen by the library's autotuner on this workload
+    tuning = L.autotune(host[0], reps=10) if not a.no_autotune else L.getTuning()
     dth = [torch.from_numpy(h).cuda() for h in host]
     dll = [torch.empty(BATCH, dtype=torch.float64, device="cuda")
            for _ in range(nbatches)]
@@ -587,6 +591,7 @@ def main():
             "data": "synthetic (seeded maps of the workload's shapes)",
             "config": {"workload": WORKLOAD, "proposals_per_step": BATCH,
                        "fftsize": n, "beam_sets": B, "datasets": D,
+                       "autotune": tuning,
                        "l2": "working set per step ~400 MB > 126 MB L2 "
                              "(no flush needed)"},
             "e2e": {"value": e2e, "unit": "evals/s",

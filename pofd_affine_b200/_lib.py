@@ -58,6 +58,9 @@ SIGNATURES = {
     "pofd_like1_set_fft": (I, [V, I]),
     "pofd_like1_fft_info": (I, [V, C.POINTER(I)]),
     "pofd_like1_set_sigma_prior": (I, [V, I, D]),
+    "pofd_like1_autotune": (I, [V, U, _fp, U, I, V]),
+    "pofd_like1_get_tuning": (I, [V, _ip]),
+    "pofd_like1_set_tuning": (I, [V, _ip]),
     "pofd_like2_set_sigma_prior": (I, [V, I, I, D]),
     "pofd_like2_set_cfirb_prior": (I, [V, I, I, D, D]),
     "pofd_like2_set_poisson_prior": (I, [V, I, I, D, D]),

@@ -339,6 +339,34 @@ class calcLike:
         th[:, k + 1:k + 3] = b.astype(np.float32)
         return th[0] if one else th
 
+    TUNING_KEYS = ("own_fft", "rfill_per", "rnodes_threads", "spec_blocks")
+
+    def autotune(self, thetas, reps=20):
+        """Choose the launch shapes by timing the graph-captured launch
+        sequence on these rows; returns the chosen knobs with the best and
+        the untuned time per launch (ms)."""
+        th = np.ascontiguousarray(_f32(thetas))
+        if th.ndim != 2:
+            raise PofdError(-10, "thetas must be [nprop, npar]")
+        out = np.zeros(6)
+        check(lib().pofd_like1_autotune(self.h, th.shape[0], th.ravel(),
+                                        th.shape[1], int(reps),
+                                        out.ctypes.data_as(C.c_void_p)))
+        d = {k: int(v) for k, v in zip(self.TUNING_KEYS, out[:4])}
+        d["ms"], d["untuned_ms"] = float(out[4]), float(out[5])
+        return d
+
+    def getTuning(self):
+        k = np.zeros(4, dtype=np.int32)
+        check(lib().pofd_like1_get_tuning(self.h, k))
+        return {n: int(v) for n, v in zip(self.TUNING_KEYS, k)}
+
+    def setTuning(self, **knobs):
+        cur = self.getTuning()
+        cur.update(knobs)
+        k = np.array([cur[n] for n in self.TUNING_KEYS], dtype=np.int32)
+        check(lib().pofd_like1_set_tuning(self.h, k))
+
     def setFFT(self, mode):
         """0: own FP64 FFT where the size allows (default), 1: cuFFT."""
         check(lib().pofd_like1_set_fft(self.h, int(mode)))

@@ -34,7 +34,7 @@ namespace pofd {
 namespace {
 
 constexpr int NT = 256;           // threads per block for the streaming kernels
-constexpr int TILE = NT * 8;      // R grid points per block
+constexpr int kMaxTilesPer = 4;   // smallest R-fill tile: NT * 4 grid points
 constexpr int CHUNK = NT * 16;    // P(D) elements per reduction block
 constexpr int KMAX = Engine1::KMAX;
 constexpr int MAXTERMS = 4096;    // beam terms held in shared memory
@@ -307,6 +307,7 @@ k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
 // sums of the first and second flux moments (PDFactory.cc:634-665).  The
 // node interval of every grid point is parameter-independent and comes from
 // a host-built table (gidx, -1 outside the covered ranges).
+template <int PER>
 __global__ void __launch_bounds__(NT)
 k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
          int nc2, int ntile, const int* __restrict__ mstatus,
@@ -329,8 +330,7 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
   const double off0 = bs.side[0].grid_off, off1 = bs.side[1].grid_off;
   const double* __restrict__ x0 = bs.side[0].x;
   const double* __restrict__ x1 = bs.side[1].x;
-  constexpr int PER = TILE / NT;
-  const int base = blockIdx.x * TILE + threadIdx.x;
+  const int base = blockIdx.x * (NT * PER) + threadIdx.x;
   int q[PER];
 #pragma unroll
   for (int k = 0; k < PER; ++k) {
@@ -367,6 +367,17 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
     double* o = rpart + (static_cast<size_t>(wb) * ntile + blockIdx.x) * 2;
     o[0] = mn;
     o[1] = var;
+  }
+}
+
+// R-fill launch with PER grid points per thread (an autotuned knob).
+void launch_rfill(int per, dim3 grid, cudaStream_t st, const BSet1Dev* bsets, int B, int n,
+                  int NI, int nc2, int ntile, const int* mstatus, const double* spl,
+                  double* rbuf, double* rpart) {
+  switch (per) {
+    case 4: k_rfill1<4><<<grid, NT, 0, st>>>(bsets, B, n, NI, nc2, ntile, mstatus, spl, rbuf, rpart); break;
+    case 16: k_rfill1<16><<<grid, NT, 0, st>>>(bsets, B, n, NI, nc2, ntile, mstatus, spl, rbuf, rpart); break;
+    default: k_rfill1<8><<<grid, NT, 0, st>>>(bsets, B, n, NI, nc2, ntile, mstatus, spl, rbuf, rpart); break;
   }
 }
 
@@ -1603,7 +1614,7 @@ void Engine1::build_static() {
   d_dsets_ = dalloc<DSet1Dev>(D_);
   static_allocs_.push_back(d_dsets_);
   cuda_check(cudaMemcpy(d_dsets_, h_dsets_.data(), D_ * sizeof(DSet1Dev), cudaMemcpyHostToDevice), "upload");
-  ntile_ = (n_ + TILE - 1) / TILE;
+  ntile_ = (n_ + NT * tune_.rfill_per - 1) / (NT * tune_.rfill_per);
   nchunk_ = (n_ + CHUNK - 1) / CHUNK;
   // own FFT: n = 2m, m = m1 * 256 with m1 a power of two in [8, 256]
   own_fft_ = fft_mode_ == 0 && n_ >= 4096 && n_ <= 131072 && (n_ & (n_ - 1)) == 0;
@@ -1674,6 +1685,95 @@ void Engine1::profile_stages(unsigned nprop, const float* theta, unsigned npar,
     }
   }
   for (auto& e : ev) cudaEventDestroy(e);
+}
+
+// Mean time of one launch sequence for these rows, as the caller's graph
+// replays it (the first evaluation stages the rows and captures the graph).
+double Engine1::time_sequence(unsigned nprop, const float* theta, unsigned npar, int reps) {
+  std::vector<double> ll(nprop);
+  std::vector<int> st(nprop);
+  eval_host(nprop, theta, npar, ll.data(), st.data());
+  enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);  // warm
+  cudaEvent_t e0, e1;
+  cuda_check(cudaEventCreate(&e0), "event create");
+  cuda_check(cudaEventCreate(&e1), "event create");
+  cuda_check(cudaEventRecord(e0, stream_), "event record");
+  for (int r = 0; r < reps; ++r) enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);
+  cuda_check(cudaEventRecord(e1, stream_), "event record");
+  cuda_check(cudaEventSynchronize(e1), "event sync");
+  float ms = 0.f;
+  cuda_check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return static_cast<double>(ms) / reps;
+}
+
+void Engine1::set_tuning(const Tune1& t) {
+  if (t.rfill_per != 4 && t.rfill_per != 8 && t.rfill_per != 16)
+    throw Error(POFD_E_ARG, "rfill_per must be 4, 8 or 16");
+  if (t.rnodes_threads != 64 && t.rnodes_threads != 128 && t.rnodes_threads != 256)
+    throw Error(POFD_E_ARG, "rnodes_threads must be 64, 128 or 256");
+  if (t.spec_blocks < 1 || t.spec_blocks > 64) throw Error(POFD_E_ARG, "spec_blocks must be in [1, 64]");
+  const bool fft_changed = (t.own_fft != 0) != (tune_.own_fft != 0);
+  tune_ = t;
+  tune_.own_fft = t.own_fft ? 1 : 0;
+  if (fft_changed) set_fft_mode(tune_.own_fft ? 0 : 1);  // rebuilds tables, plans, work space
+  if (static_ok_) ntile_ = (n_ + NT * tune_.rfill_per - 1) / (NT * tune_.rfill_per);
+  drop_graphs();
+}
+
+// Coordinate descent over the knobs, one pass, each candidate timed on the
+// captured graph of the whole sequence.  The FFT choice is tried only where
+// the own FFT supports the size.
+void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out6) {
+  if (nprop == 0 || reps < 1) throw Error(POFD_E_ARG, "autotune needs rows and reps >= 1");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  const double t_untuned = time_sequence(nprop, theta, npar, reps);
+  Tune1 best = tune_;
+  double best_ms = t_untuned;
+  auto trial = [&](const Tune1& t) {
+    set_tuning(t);
+    const double ms = time_sequence(nprop, theta, npar, reps);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  };
+  const bool own_possible = n_ >= 4096 && n_ <= 131072 && (n_ & (n_ - 1)) == 0;
+  if (own_possible) {
+    Tune1 t = best;
+    t.own_fft = best.own_fft ? 0 : 1;
+    trial(t);
+  }
+  for (int per : {4, 8, 16}) {
+    if (per == best.rfill_per) continue;
+    Tune1 t = best;
+    t.rfill_per = per;
+    trial(t);
+  }
+  for (int th : {64, 128, 256}) {
+    if (th == best.rnodes_threads) continue;
+    Tune1 t = best;
+    t.rnodes_threads = th;
+    trial(t);
+  }
+  if (best.own_fft && own_possible) {
+    for (int sb : {2, 4, 8, 16, 32}) {
+      if (sb == best.spec_blocks) continue;
+      Tune1 t = best;
+      t.spec_blocks = sb;
+      trial(t);
+    }
+  }
+  set_tuning(best);
+  if (out6) {
+    out6[0] = best.own_fft;
+    out6[1] = best.rfill_per;
+    out6[2] = best.rnodes_threads;
+    out6[3] = best.spec_blocks;
+    out6[4] = best_ms;
+    out6[5] = t_untuned;
+  }
 }
 
 const char* Engine1::stage_name(int i) const {
@@ -1775,6 +1875,7 @@ void Engine1::fill_bonus(unsigned nprop, float* theta_dev, unsigned npar, cudaSt
 
 void Engine1::set_fft_mode(int mode) {
   if (mode != 0 && mode != 1) throw Error(POFD_E_ARG, "fft mode must be 0 (own) or 1 (cuFFT)");
+  tune_.own_fft = (mode == 0) ? 1 : 0;
   if (mode == fft_mode_) return;
   fft_mode_ = mode;
   static_ok_ = false;  // rebuilds tables, plans, graphs and work space
@@ -1814,7 +1915,9 @@ void Engine1::reserve(unsigned P) {
   ws_.nodes = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * NI);
   ws_.spl = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * 4 * NI);
   ws_.rbuf = dalloc<double>(static_cast<size_t>(P) * B_ * nc2);
-  ws_.rpart = dalloc<double>(static_cast<size_t>(P) * B_ * ntile_ * 2);
+  // room for the smallest tile the autotuner may pick
+  ws_.rpart = dalloc<double>(static_cast<size_t>(P) * B_ *
+                             ((n_ + NT * kMaxTilesPer - 1) / (NT * kMaxTilesPer)) * 2);
   if (own_fft_) {
     ws_.tmp = dalloc<double>(static_cast<size_t>(P) * std::max(B_, D_) * nc2);
     fftA_attr<-1>();
@@ -1888,9 +1991,10 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                           d_qw_, qper_, ws_.bonus, -1);
   {
     const size_t smem = (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double);
-    dim3 grid((NI + 127) / 128, P * B * 2);
-    k_rnodes1<<<grid, 128, smem, st>>>(d_bsets_, model_, B, NI, maxterms_,
-                                       ws_.cnt, ws_.mstatus, ws_.nodes);
+    const int th = tune_.rnodes_threads;
+    dim3 grid((NI + th - 1) / th, P * B * 2);
+    k_rnodes1<<<grid, th, smem, st>>>(d_bsets_, model_, B, NI, maxterms_,
+                                      ws_.cnt, ws_.mstatus, ws_.nodes);
   }
   mark(1);
   {
@@ -1907,8 +2011,8 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
     double2* pb = reinterpret_cast<double2*>(ws_.pbuf);
     {
       dim3 grid(ntile_, P * B);
-      k_rfill1<<<grid, NT, 0, st>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
-                                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+      launch_rfill(tune_.rfill_per, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+                   ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
     k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
@@ -1923,7 +2027,7 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
     mark(5);
     {
       // a few blocks per row loop over the pairs up to the row's cut-off
-      dim3 grid(std::min((m / 2 + 1 + NT - 1) / NT, 8), P * B);
+      dim3 grid(std::min((m / 2 + 1 + NT - 1) / NT, tune_.spec_blocks), P * B);
       k_spectrum1f<<<grid, NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, rowsz, ws_.mstatus,
                                         ws_.sigmult, ws_.mom, rb, pb, d_wn_, ws_.kcut_set,
                                         ws_.kcut_ds);
@@ -1935,8 +2039,8 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
   } else {
     {
       dim3 grid(ntile_, P * B);
-      k_rfill1<<<grid, NT, 0, st>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
-                                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+      launch_rfill(tune_.rfill_per, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+                   ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
     k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
@@ -2135,8 +2239,8 @@ void Engine1::rgrid_host(int bs, const float* theta, unsigned npar, double* out)
       d_bsets_, model_, B, NI, maxterms_, ws_.cnt, ws_.mstatus, ws_.nodes);
   k_rspline1<<<B * 2, NT, (2 * static_cast<size_t>(NI) + 2 * NT) * sizeof(double), stream_>>>(
       d_bsets_, B, NI, ws_.mstatus, ws_.nodes, ws_.spl);
-  k_rfill1<<<dim3(ntile_, B), NT, 0, stream_>>>(d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
-                                                ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+  launch_rfill(tune_.rfill_per, dim3(ntile_, B), stream_, d_bsets_, B, n, NI, nc2,
+               static_cast<int>(ntile_), ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
   cuda_check(cudaGetLastError(), "rgrid kernels");
   cuda_check(cudaMemcpyAsync(out, ws_.rbuf + static_cast<size_t>(bs) * nc2, n_ * sizeof(double),
                              cudaMemcpyDeviceToHost, stream_), "D2H R grid");

@@ -121,6 +121,16 @@ struct Workspace1 {
   unsigned h_npar = 0;
 };
 
+// Launch-shape knobs chosen by Engine1::autotune (none changes what is
+// computed; the R-fill tile changes the grouping of the R moment partial sums
+// and the FFT choice the rounding of the transform).
+struct Tune1 {
+  int own_fft = 1;          // own FP64 FFT where the size allows (else cuFFT)
+  int rfill_per = 8;        // R grid points per thread of k_rfill1 (4, 8, 16)
+  int rnodes_threads = 128; // threads per block of k_rnodes1 (64, 128, 256)
+  int spec_blocks = 8;      // blocks per row of k_spectrum1f (2 ... 32)
+};
+
 class Engine1 {
  public:
   static constexpr int KMAX = 64;
@@ -164,6 +174,13 @@ class Engine1 {
   void set_poisson_prior(bool on, double mean, double sigma);
   void set_regularization(double alpha);
   const Prior1& priors() const { return prior_; }
+  // Times the full launch sequence (graph replays, CUDA events) for the
+  // candidate values of each knob in turn on nprop host rows and keeps the
+  // fastest; out (optional) receives {own_fft, rfill_per, rnodes_threads,
+  // spec_blocks, best ms per launch, untuned ms per launch}.
+  void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out6);
+  const Tune1& tuning() const { return tune_; }
+  void set_tuning(const Tune1& t);
   // <S>, <S^2> of each proposal's model (calcLike::fillBonusParams,
   // calcLike.cc:958-980): host rows -> out[nprop][2]
   void bonus_host(unsigned nprop, const float* theta, unsigned npar, double* out);
@@ -245,6 +262,8 @@ class Engine1 {
   double2* d_wh_ = nullptr;  // e^{-2 pi i 128 j / m}, j < m / 128
   double2* d_wl_ = nullptr;  // e^{-2 pi i i / m}, i < 128
   double2* d_wn_ = nullptr;  // e^{-2 pi i k / n}, k <= m
+  double time_sequence(unsigned nprop, const float* theta, unsigned npar, int reps);
+  Tune1 tune_;
   // priors and the knot quadrature of the bonus integrals
   Prior1 prior_;
   const double* d_qu_ = nullptr;
