@@ -451,17 +451,10 @@ def main():
         return
 
     import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(local)
+    from pofd_affine_b200.ranks import Ranks
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rk = Ranks("nccl")
+    rank, world, local = rk.rank, rk.world, rk.local
     from pofd_affine_b200 import Context, build
     build.build()
     from pofd_affine_b200._lib import lib
@@ -472,7 +465,7 @@ def main():
     L.reserve(BATCH)
     npar = cfg["theta0"].size
     nbatches = 4  # distinct resident proposal batches, cycled
-    host = [synth.proposals(cfg["theta0"], BATCH, 0.02, rng=100 * rank + k)
+    host = [synth.proposals(cfg["theta0"], BATCH, 0.02, rng=rk.proposal_seed(k))
             for k in range(nbatches)]
     # launch shapes chosen by the library's autotuner on this workload
     tuning = L.autotune(host[0], reps=10) if not a.no_autotune else L.getTuning()
@@ -502,8 +495,7 @@ def main():
     for k in range(max(a.warmup, 3)):
         step(k)
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    rk.barrier()
     clk = ClockSampler(local)
     clk.start()
     time.sleep(0.3)
@@ -516,28 +508,19 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * BATCH * a.steps / (ms * 1e-3)
+    ms = rk.max_over_ranks(e0.elapsed_time(e1))
+    value = rk.throughput(BATCH * a.steps, ms * 1e-3)
 
     # end to end through the public API with host buffers
     L.getLogLikeBatch(host[1])
-    if dist:
-        dist.barrier()
+    rk.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for k in range(a.steps):
         L.getLogLikeBatch(host[k % nbatches])
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * BATCH * a.steps / e2e_s
+    e2e_s = rk.max_over_ranks(time.perf_counter() - t0)
+    e2e = rk.throughput(BATCH * a.steps, e2e_s)
 
     # per-stage device times of the same launch sequence (CUDA events)
     stages = L.profileStages(host[0], reps=5)
@@ -606,9 +589,7 @@ def main():
         }
         line.update(extra)
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rk.close()
 
 
 if __name__ == "__main__":
