@@ -511,6 +511,10 @@ int pofd_ensemble_set_surrogate(pofd_ensemble* e, pofd_batch_loglike_fn sfn,
 /* Every exact evaluation of the ensemble is also appended to this
  * surrogate's training pairs (NULL stops collecting). */
 int pofd_ensemble_collect_pairs(pofd_ensemble* e, pofd_surrogate* s);
+/* Set-up before delayed-acceptance steps: one exact evaluation of every
+ * survivor batch size on the buffers the steps use, so that plans and
+ * captured graphs are made outside the sampling loop (no counterpart). */
+int pofd_ensemble_prepare_da(pofd_ensemble* e);
 int pofd_ensemble_do_steps_da(pofd_ensemble* e, unsigned nsteps, int record);
 /* Failed likelihood evaluations (a P(D) split or unwrap error, a
  * non-finite logL): reject_failures == 0 (default) stops the run with the

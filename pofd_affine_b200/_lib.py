@@ -99,6 +99,7 @@ SIGNATURES = {
     "pofd_ensemble_destroy": (I, [V]),
     "pofd_ensemble_set_likelihood": (I, [V, V, V]),
     "pofd_ensemble_use_like1": (I, [V, V]),
+    "pofd_ensemble_prepare_da": (I, [V]),
     "pofd_ensemble_set_bonus": (I, [V, V, V]),
     "pofd_ensemble_use_like2": (I, [V, V]),
     "pofd_ensemble_set_param_state": (I, [V, U, I]),

@@ -1175,6 +1175,14 @@ int pofd_ensemble_collect_pairs(pofd_ensemble* e, pofd_surrogate* s) {
   });
 }
 
+int pofd_ensemble_prepare_da(pofd_ensemble* e) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->prepare_da();
+    return POFD_OK;
+  });
+}
+
 int pofd_ensemble_do_steps_da(pofd_ensemble* e, unsigned nsteps, int record) {
   return guard([&] {
     need(e != nullptr, "null argument");

@@ -639,6 +639,37 @@ void Ensemble::da_half(int half, double zexp, double invt) {
   ck(cudaGetLastError(), "k_stage2");
 }
 
+// Set-up for delayed acceptance: one exact evaluation of every batch size
+// the survivor buckets can take, on the buffers the steps use, so that the
+// likelihood's transform plans and captured graphs exist before sampling
+// (the reference likewise plans its FFTs at set-up).
+void Ensemble::prepare_da() {
+  if (!init_) throw Error(POFD_E_ARG, "Chains not initialised");
+  if (!fn_) throw Error(POFD_E_ARG, "No likelihood set");
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  const unsigned nmax = nw_ - nw_ / 2;
+  unsigned last = 0;
+  for (unsigned c = 1; c <= nmax; ++c) {
+    const unsigned b = std::min(bucket(c), nmax);
+    if (b == last) continue;
+    last = b;
+    ck(cudaMemcpyAsync(exprop_, theta_, static_cast<size_t>(b) * np_ * sizeof(float),
+                       cudaMemcpyDeviceToDevice, stream_), "copy walkers");
+    const int rc = fn_(like_, b, exprop_, np_, exl_, exs_, stream_);
+    if (rc < 0) throw Error(rc, "batched likelihood enqueue failed");
+    ck(cudaStreamSynchronize(stream_), "synchronize");
+  }
+  if (nw_ / 2 != nmax) {
+    // the first half's size, if it differs
+    const unsigned b = std::min(bucket(nw_ / 2), nmax);
+    ck(cudaMemcpyAsync(exprop_, theta_, static_cast<size_t>(b) * np_ * sizeof(float),
+                       cudaMemcpyDeviceToDevice, stream_), "copy walkers");
+    const int rc = fn_(like_, b, exprop_, np_, exl_, exs_, stream_);
+    if (rc < 0) throw Error(rc, "batched likelihood enqueue failed");
+    ck(cudaStreamSynchronize(stream_), "synchronize");
+  }
+}
+
 void Ensemble::do_steps_da(unsigned nsteps, bool record) {
   if (!init_) throw Error(POFD_E_ARG, "Chains not initialised");
   if (!fn_) throw Error(POFD_E_ARG, "No likelihood set");

@@ -56,6 +56,7 @@ class Ensemble {
   unsigned npar() const { return np_; }
   void collect_pairs(Surrogate* s) { collect_ = s; drop_graph(); }
   void do_steps_da(unsigned nsteps, bool record);
+  void prepare_da();
   void da_stats(unsigned long long* out4) const;
   // false (default): a failed likelihood evaluation stops the run, as in the
   // reference; true: it rejects the step and is counted.

@@ -662,16 +662,31 @@ void Surrogate::refresh_scaling() {
   ck(cudaMemcpy(ll.data(), plogl_, n * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
   std::vector<int> idx(kInPad, 0);
   ck(cudaMemcpy(idx.data(), idx_, kInPad * sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+  // inputs standardised over the pairs whose target is not clipped (the
+  // region the sampler explores once burnt in), when there are enough of
+  // them; far-off burn-in points then sit at large |x| instead of setting
+  // the scale
+  double lmax = -std::numeric_limits<double>::infinity();
+  for (double v : ll) lmax = std::max(lmax, v);
+  const double clip0 = 25.0 + 2.5 * nin_;
+  std::vector<unsigned> use;
+  for (unsigned i = 0; i < n; ++i)
+    if (ll[i] - lmax > -clip0) use.push_back(i);
+  if (use.size() < std::max<size_t>(2 * nin_, 64)) {
+    use.resize(n);
+    for (unsigned i = 0; i < n; ++i) use[i] = i;
+  }
+  const double nu = static_cast<double>(use.size());
   std::vector<float> mu(kInPad, 0.0f), isd(kInPad, 1.0f);
   for (unsigned k = 0; k < nin_; ++k) {
     double s = 0, s2 = 0;
-    for (unsigned i = 0; i < n; ++i) s += th[static_cast<size_t>(i) * npar_ + idx[k]];
-    const double m = s / n;
-    for (unsigned i = 0; i < n; ++i) {
+    for (unsigned i : use) s += th[static_cast<size_t>(i) * npar_ + idx[k]];
+    const double m = s / nu;
+    for (unsigned i : use) {
       const double d = th[static_cast<size_t>(i) * npar_ + idx[k]] - m;
       s2 += d * d;
     }
-    const double sd = std::sqrt(s2 / n);
+    const double sd = std::sqrt(s2 / nu);
     mu[k] = static_cast<float>(m);
     isd[k] = static_cast<float>(sd > 0 ? 1.0 / sd : 1.0);
   }

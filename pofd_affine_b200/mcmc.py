@@ -182,6 +182,10 @@ class affineEnsemble:
         self.nsteps_done = 0
 
     # ------------------------------------------------------------ steps
+    def sync(self):
+        """Wait for the ensemble's queued work (reads the record counter)."""
+        self.nRecorded()
+
     def doSteps(self, nsteps, initsteps=0):
         """initsteps unrecorded steps, then nsteps recorded ones."""
         if initsteps:
@@ -211,6 +215,11 @@ class affineEnsemble:
         check(lib().pofd_ensemble_collect_pairs(self.h,
                                                 sur.h if sur else None))
         self.collector = sur
+
+    def prepareDA(self):
+        """One exact evaluation of every survivor batch size (plans and
+        graphs made before sampling)."""
+        check(lib().pofd_ensemble_prepare_da(self.h))
 
     def doStepsDA(self, nsteps, record=True):
         check(lib().pofd_ensemble_do_steps_da(self.h, int(nsteps),
