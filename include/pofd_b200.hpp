@@ -151,6 +151,41 @@ class Like1 {
     check(pofd_like1_eval_batch(h_, nprop, p, npar, logl, status),
           "calcLike::getLogLikeBatch");
   }
+  // priors (calcLike.h:251-269)
+  void setSigmaPrior(double width) {
+    check(pofd_like1_set_sigma_prior(h_, 1, width), "calcLike::setSigmaPrior");
+  }
+  void unsetSigmaPrior() {
+    check(pofd_like1_set_sigma_prior(h_, 0, 0.0), "calcLike::unsetSigmaPrior");
+  }
+  void setCFIRBPrior(double mean, double sigma) {
+    check(pofd_like1_set_cfirb_prior(h_, 1, mean, sigma), "calcLike::setCFIRBPrior");
+  }
+  void unsetCFIRBPrior() {
+    check(pofd_like1_set_cfirb_prior(h_, 0, 0.0, 0.0), "calcLike::unsetCFIRBPrior");
+  }
+  void setPoissonPrior(double mean, double sigma) {
+    check(pofd_like1_set_poisson_prior(h_, 1, mean, sigma), "calcLike::setPoissonPrior");
+  }
+  void unsetPoissonPrior() {
+    check(pofd_like1_set_poisson_prior(h_, 0, 0.0, 0.0), "calcLike::unsetPoissonPrior");
+  }
+  void setRegularizationAlpha(double alpha) {
+    check(pofd_like1_set_regularization(h_, alpha), "calcLike::setRegularizationAlpha");
+  }
+  // calcLike::fillBonusParams (calcLike.cc:958-980) on host rows of npar >=
+  // nknots + 3 entries: <S>, <S^2> written after the sigma multiplier
+  void fillBonusParams(unsigned nknots, float* p, unsigned npar) {
+    if (npar < nknots + 3) throw std::runtime_error("calcLike::fillBonusParams: Not enough room to fill");
+    double b[2];
+    check(pofd_like1_bonus(h_, 1, p, npar, b), "calcLike::fillBonusParams");
+    p[nknots + 1] = static_cast<float>(b[0]);
+    p[nknots + 2] = static_cast<float>(b[1]);
+  }
+  // launch-shape autotuner on nprop representative rows (no counterpart)
+  void autotune(unsigned nprop, const float* p, unsigned npar, int reps = 20) {
+    check(pofd_like1_autotune(h_, nprop, p, npar, reps, nullptr), "calcLike::autotune");
+  }
   pofd_like1* get() const { return h_; }
 
  private:
