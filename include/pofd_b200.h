@@ -189,15 +189,16 @@ int pofd_like1_fft_info(pofd_like1* L, int* own);
  * GPU and no counterpart): times the whole graph-captured launch sequence on
  * nprop host rows (reps replays per candidate, CUDA events) for each knob in
  * turn -- own FFT vs cuFFT, R-fill points per thread {4, 8, 16}, R-node
- * threads per block {64, 128, 256}, spectrum blocks per row {2 ... 32} --
- * and keeps the fastest.  out6 (optional) = {own_fft, rfill_per,
- * rnodes_threads, spec_blocks, best ms, untuned ms}.  get/set_tuning read or
- * impose the four knobs (e.g. a tuning saved from an earlier run).  Results
+ * threads per block {64, 128, 256}, persistent prefetching FFT passes or
+ * not, spectrum blocks per row {2 ... 32} -- and keeps the fastest.  out7
+ * (optional) = {own_fft, rfill_per, rnodes_threads, spec_blocks,
+ * fft_persist, best ms, untuned ms}.  get/set_tuning read or impose the five
+ * knobs in that order (e.g. a tuning saved from an earlier run).  Results
  * change only by rounding (reduction grouping, FFT implementation). */
 int pofd_like1_autotune(pofd_like1* L, unsigned nprop, const float* theta,
-                        unsigned npar, int reps, double* out6);
-int pofd_like1_get_tuning(const pofd_like1* L, int* knobs4);
-int pofd_like1_set_tuning(pofd_like1* L, const int* knobs4);
+                        unsigned npar, int reps, double* out7);
+int pofd_like1_get_tuning(const pofd_like1* L, int* knobs5);
+int pofd_like1_set_tuning(pofd_like1* L, const int* knobs5);
 
 /* Priors added once to the summed log-likelihood, in the reference's order
  * (calcLike.cc:918-952): a Gaussian on the sigma multiplier about 1, on <S>

@@ -592,6 +592,142 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
   }
 }
 
+// Persistent forms of passes A and B (m1 >= 16): a grid of about two
+// blocks per SM walks the tiles (row, column block) / (row, row block); as
+// soon as a tile's inputs have gone through the first register DFT into the
+// shared-memory exchange, the next tile's loads are issued into the same
+// registers, so they are in flight while the second stage and the stores of
+// the current tile run.  Same arithmetic as k_fftA / k_fftB; rows of failed
+// proposals are transformed on zeros and not stored.
+template <int L2, int S>
+__device__ __forceinline__ void fftAP_load(double2* v, int tile, const double2* __restrict__ in,
+                                           int rowsz, int nrows_per_w,
+                                           const int* __restrict__ mstatus,
+                                           const int* __restrict__ kcut, int b, int n2) {
+  constexpr int M1 = 16 * L2, m = M1 * 256, CB = 256 / L2;
+  const int row = tile / L2, b0 = (tile % L2) * CB;
+  const double2* src = in + static_cast<size_t>(row) * rowsz;
+  const int kc = kcut ? kcut[row] : m;
+  const bool skip = mstatus[row / nrows_per_w] != 0;
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) {
+    const int a = L2 * n1 + n2;
+    v[n1] = (skip || row_cut(a, m, kc)) ? make_double2(0.0, 0.0) : src[a * 256 + b0 + b];
+  }
+}
+
+template <int L2, int S>
+__global__ void __launch_bounds__(256, 2)
+k_fftAP(int rows, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
+        const double2* __restrict__ in, double2* __restrict__ out,
+        const double2* __restrict__ WH, const double2* __restrict__ WL,
+        const int* __restrict__ kcut) {
+  constexpr int L1 = 16, M1 = L1 * L2, M2 = 256, m = M1 * M2, CB = 256 / L2, NH = m / 128;
+  extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L
+  double2* Hs = fs + 256 * L1;
+  const double2* Ls = Hs + NH;
+  const int t = threadIdx.x;
+  const int b = t % CB, n2 = t / CB;
+  const int ntiles = rows * L2;
+  int tile = blockIdx.x;
+  double2 v[L1];
+  fft::load_tw2(Hs, WH, WL, NH, t, 256);
+  if (tile < ntiles) fftAP_load<L2, S>(v, tile, in, rowsz, nrows_per_w, mstatus, kcut, b, n2);
+  __syncthreads();
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int row = tile / L2, b0 = (tile % L2) * CB;
+    const bool skip = mstatus[row / nrows_per_w] != 0;
+    double2* dst = out + static_cast<size_t>(row) * rowsz;
+    fft::dft<L1, S>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < L1; ++k1) {
+      if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, (m / M1) * n2 * k1));
+      fs[(n2 * L1 + k1) * CB + b] = v[k1];
+    }
+    const int next = tile + static_cast<int>(gridDim.x);
+    if (next < ntiles) fftAP_load<L2, S>(v, next, in, rowsz, nrows_per_w, mstatus, kcut, b, n2);
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < L1 / L2; ++it) {
+      const int e = t + 256 * it;
+      const int bb = e % CB, k1 = e / CB;
+      double2 u[L2];
+#pragma unroll
+      for (int q = 0; q < L2; ++q) u[q] = fs[(q * L1 + k1) * CB + bb];
+      fft::dft<L2, S>(u);
+      if (!skip) {
+#pragma unroll
+        for (int k2 = 0; k2 < L2; ++k2) {
+          const int c = k1 + L1 * k2;
+          const int gb = b0 + bb;
+          dst[c * M2 + gb] = (c * gb) ? fft::cmul(u[k2], fft::tw2<S>(Hs, Ls, c * gb)) : u[k2];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256, 2)
+k_fftBP(int m1, int rows, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
+        const double2* __restrict__ in, double2* __restrict__ out,
+        const double2* __restrict__ WH, const double2* __restrict__ WL,
+        const int* __restrict__ kcut) {
+  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then H, L
+  double2* Hs = fs + 16 * 16 * 17;
+  const double2* Ls = Hs + 2 * m1;
+  const int m = m1 * 256;
+  const int tpr = m1 / 16;  // row blocks per row
+  const int ntiles = rows * tpr;
+  const int t = threadIdx.x;
+  const int n2 = t & 15, r = t >> 4;
+  int tile = blockIdx.x;
+  double2 v[16];
+  auto load = [&](int tl) {
+    const int row = tl / tpr, c0 = (tl % tpr) * 16;
+    const double2* src = in + static_cast<size_t>(row) * rowsz;
+    const bool skip = mstatus[row / nrows_per_w] != 0;
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1)
+      v[n1] = skip ? make_double2(0.0, 0.0) : src[(c0 + r) * 256 + 16 * n1 + n2];
+  };
+  fft::load_tw2(Hs, WH, WL, 2 * m1, t, 256);
+  if (tile < ntiles) load(tile);
+  __syncthreads();
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int row = tile / tpr, c0 = (tile % tpr) * 16;
+    const bool skip = mstatus[row / nrows_per_w] != 0;
+    double2* dst = out + static_cast<size_t>(row) * rowsz;
+    const int kc = kcut ? kcut[row] : m;
+    fft::dft<16, S>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) {
+      if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, (m / 256) * n2 * k1));
+      fs[(k1 * 16 + n2) * 17 + r] = v[k1];
+    }
+    const int next = tile + static_cast<int>(gridDim.x);
+    if (next < ntiles) load(next);
+    __syncthreads();
+    {
+      const int rr = t & 15, k1 = t >> 4;
+      double2 u[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) u[q] = fs[(k1 * 16 + q) * 17 + rr];
+      fft::dft<16, S>(u);
+      if (!skip) {
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) {
+          // bins beyond the noise cut-off are never read (forward transform)
+          const int k = (c0 + rr) + m1 * (k1 + 16 * k2);
+          if (min(k, m - k) <= kc) dst[k] = u[k2];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Pass B: 256-point DFTs along rows c0..c0+15 of Y (16 x 16 split), stored
 // in natural order Z[c + m1 d].
 template <int S>
@@ -1251,6 +1387,36 @@ void fftA_attr() {
 }
 
 constexpr size_t kFftBSmemMax = (16 * 16 * 17 + 2 * 256 + 128) * sizeof(double2);
+
+template <int S>
+void launch_fftAP(int m1, int rows, int grid, cudaStream_t st, int rowsz, int nrw,
+                  const int* mstatus, const double2* in, double2* out, const double2* WH,
+                  const double2* WL, const int* kcut) {
+  const size_t sm = fftA_smem(m1);
+#define POFD_FFTAP(L2)                                                                     \
+  k_fftAP<L2, S><<<grid, 256, sm, st>>>(rows, rowsz, nrw, mstatus, in, out, WH, WL, kcut)
+  switch (m1) {
+    case 16: POFD_FFTAP(1); break;
+    case 32: POFD_FFTAP(2); break;
+    case 64: POFD_FFTAP(4); break;
+    case 128: POFD_FFTAP(8); break;
+    case 256: POFD_FFTAP(16); break;
+    default: throw Error(POFD_E_ARG, "persistent FFT pass: unsupported size");
+  }
+#undef POFD_FFTAP
+}
+
+template <int S>
+void fftAP_attr() {
+  const int sm = static_cast<int>(kFftASmemMax);
+  cuda_check(cudaFuncSetAttribute(k_fftAP<1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAP<2, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAP<4, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAP<8, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAP<16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftBP<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(kFftBSmemMax)), "attr");
+}
 inline size_t fftB_smem(int m1) {
   return (16 * 16 * 17 + 2 * static_cast<size_t>(m1) + 128) * sizeof(double2);
 }
@@ -1469,6 +1635,8 @@ void Engine1::build_static() {
     qper_ = kq.nper;
   }
 
+  cuda_check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_),
+             "SM count");
   B_ = static_cast<unsigned>(sets_.size());
   maxterms_ = 1;
   h_bsets_.assign(B_, BSet1Dev{});
@@ -1714,6 +1882,7 @@ void Engine1::set_tuning(const Tune1& t) {
   if (t.rnodes_threads != 64 && t.rnodes_threads != 128 && t.rnodes_threads != 256)
     throw Error(POFD_E_ARG, "rnodes_threads must be 64, 128 or 256");
   if (t.spec_blocks < 1 || t.spec_blocks > 64) throw Error(POFD_E_ARG, "spec_blocks must be in [1, 64]");
+  if (t.fft_persist != 0 && t.fft_persist != 1) throw Error(POFD_E_ARG, "fft_persist must be 0 or 1");
   const bool fft_changed = (t.own_fft != 0) != (tune_.own_fft != 0);
   tune_ = t;
   tune_.own_fft = t.own_fft ? 1 : 0;
@@ -1725,7 +1894,7 @@ void Engine1::set_tuning(const Tune1& t) {
 // Coordinate descent over the knobs, one pass, each candidate timed on the
 // captured graph of the whole sequence.  The FFT choice is tried only where
 // the own FFT supports the size.
-void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out6) {
+void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7) {
   if (nprop == 0 || reps < 1) throw Error(POFD_E_ARG, "autotune needs rows and reps >= 1");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
   const double t_untuned = time_sequence(nprop, theta, npar, reps);
@@ -1757,6 +1926,11 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     t.rnodes_threads = th;
     trial(t);
   }
+  if (best.own_fft && own_possible && n_ / 512 >= 16) {
+    Tune1 t = best;
+    t.fft_persist = best.fft_persist ? 0 : 1;
+    trial(t);
+  }
   if (best.own_fft && own_possible) {
     for (int sb : {2, 4, 8, 16, 32}) {
       if (sb == best.spec_blocks) continue;
@@ -1766,13 +1940,14 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     }
   }
   set_tuning(best);
-  if (out6) {
-    out6[0] = best.own_fft;
-    out6[1] = best.rfill_per;
-    out6[2] = best.rnodes_threads;
-    out6[3] = best.spec_blocks;
-    out6[4] = best_ms;
-    out6[5] = t_untuned;
+  if (out7) {
+    out7[0] = best.own_fft;
+    out7[1] = best.rfill_per;
+    out7[2] = best.rnodes_threads;
+    out7[3] = best.spec_blocks;
+    out7[4] = best.fft_persist;
+    out7[5] = best_ms;
+    out7[6] = t_untuned;
   }
 }
 
@@ -1922,6 +2097,10 @@ void Engine1::reserve(unsigned P) {
     ws_.tmp = dalloc<double>(static_cast<size_t>(P) * std::max(B_, D_) * nc2);
     fftA_attr<-1>();
     fftA_attr<1>();
+    if (n_ / 512 >= 16) {
+      fftAP_attr<-1>();
+      fftAP_attr<1>();
+    }
     cuda_check(cudaFuncSetAttribute(k_fftB<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kFftBSmemMax)), "attr");
     cuda_check(cudaFuncSetAttribute(k_fftB<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2021,9 +2200,17 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                                     ws_.mom, ws_.kcut_set, ws_.kcut_ds);
     mark(4);
     const int rb_rows = m1 < FRB ? m1 : FRB;
-    launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
-    k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, fftB_smem(m1), st>>>(
-        m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_, ws_.kcut_set);
+    const bool persist = tune_.fft_persist && m1 >= 16;
+    const int gA = std::min(P * B * (m1 / 16 > 0 ? m1 / 16 : 1), 2 * sm_count_);
+    if (persist) {
+      launch_fftAP<-1>(m1, P * B, gA, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
+      k_fftBP<-1><<<gA, 256, fftB_smem(m1), st>>>(m1, P * B, rowsz, B, ws_.mstatus, tmp, rb,
+                                                  d_wh_, d_wl_, ws_.kcut_set);
+    } else {
+      launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
+      k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, fftB_smem(m1), st>>>(
+          m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_, ws_.kcut_set);
+    }
     mark(5);
     {
       // a few blocks per row loop over the pairs up to the row's cut-off
@@ -2033,9 +2220,17 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                         ws_.kcut_ds);
     }
     mark(6);
-    launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_, ws_.kcut_ds);
-    k_fftB<1><<<dim3(m1 / rb_rows, P * D), 256, fftB_smem(m1), st>>>(
-        m1, rowsz, D, ws_.mstatus, tmp, pb, d_wh_, d_wl_, nullptr);
+    if (persist) {
+      const int gI = std::min(P * D * (m1 / 16), 2 * sm_count_);
+      launch_fftAP<1>(m1, P * D, gI, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_,
+                      ws_.kcut_ds);
+      k_fftBP<1><<<gI, 256, fftB_smem(m1), st>>>(m1, P * D, rowsz, D, ws_.mstatus, tmp, pb,
+                                                 d_wh_, d_wl_, nullptr);
+    } else {
+      launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_, ws_.kcut_ds);
+      k_fftB<1><<<dim3(m1 / rb_rows, P * D), 256, fftB_smem(m1), st>>>(
+          m1, rowsz, D, ws_.mstatus, tmp, pb, d_wh_, d_wl_, nullptr);
+    }
   } else {
     {
       dim3 grid(ntile_, P * B);

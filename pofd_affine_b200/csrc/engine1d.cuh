@@ -129,6 +129,7 @@ struct Tune1 {
   int rfill_per = 8;        // R grid points per thread of k_rfill1 (4, 8, 16)
   int rnodes_threads = 128; // threads per block of k_rnodes1 (64, 128, 256)
   int spec_blocks = 8;      // blocks per row of k_spectrum1f (2 ... 32)
+  int fft_persist = 0;      // persistent, prefetching FFT passes (m1 >= 16)
 };
 
 class Engine1 {
@@ -177,8 +178,8 @@ class Engine1 {
   // Times the full launch sequence (graph replays, CUDA events) for the
   // candidate values of each knob in turn on nprop host rows and keeps the
   // fastest; out (optional) receives {own_fft, rfill_per, rnodes_threads,
-  // spec_blocks, best ms per launch, untuned ms per launch}.
-  void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out6);
+  // spec_blocks, fft_persist, best ms per launch, untuned ms per launch}.
+  void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7);
   const Tune1& tuning() const { return tune_; }
   void set_tuning(const Tune1& t);
   // <S>, <S^2> of each proposal's model (calcLike::fillBonusParams,
@@ -259,6 +260,7 @@ class Engine1 {
   FftWorkArea fftwork_;
   int fft_mode_ = 0;
   bool own_fft_ = false;
+  int sm_count_ = 148;
   double2* d_wh_ = nullptr;  // e^{-2 pi i 128 j / m}, j < m / 128
   double2* d_wl_ = nullptr;  // e^{-2 pi i i / m}, i < 128
   double2* d_wn_ = nullptr;  // e^{-2 pi i k / n}, k <= m
