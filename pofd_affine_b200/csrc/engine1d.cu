@@ -940,27 +940,34 @@ k_pscan1(const BSet1Dev* __restrict__ bsets, const DSet1Dev* __restrict__ dsets,
   const SplitParams sp = split_params(bs, var, sigmult[w] * ds.sigma_base);
   const double* p = pbuf + static_cast<size_t>(wd) * nc2;
   const int base = blockIdx.x * CHUNK;
-  constexpr int PER = CHUNK / NT;
-  double v[PER];
+  constexpr int PER2 = CHUNK / NT / 2;  // double2 loads per thread
+  double2 v[PER2];
 #pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const int i = base + k * NT + threadIdx.x;
-    v[k] = (i < n) ? p[i] : -1.0;
+  for (int k = 0; k < PER2; ++k) {
+    const int i = base + 2 * (k * NT + threadIdx.x);
+    v[k] = (i < n) ? *reinterpret_cast<const double2*>(p + i) : make_double2(-1.0, -1.0);
   }
   double mx = 0.0, sum = 0.0, wsum = 0.0, mnv = 1.0e308;
   int mni = 0x7fffffff;
   bool any = false;
 #pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const int li = k * NT + threadIdx.x;
+  for (int k = 0; k < PER2; ++k) {
+    const int li = 2 * (k * NT + threadIdx.x);
     const int i = base + li;
     if (i >= n) break;
-    const double x = clip0(v[k]);
-    if (!any || x > mx) mx = x;
+    const double xa = clip0(v[k].x);
+    if (!any || xa > mx) mx = xa;
     any = true;
-    sum += x;
-    wsum += static_cast<double>(li) * x;
-    if (i >= sp.botidx && i <= sp.topidx) dev::argmin_merge(mnv, mni, x, i);
+    sum += xa;
+    wsum += static_cast<double>(li) * xa;
+    if (i >= sp.botidx && i <= sp.topidx) dev::argmin_merge(mnv, mni, xa, i);
+    if (i + 1 < n) {  // odd n: the row's last pair has one element
+      const double xb = clip0(v[k].y);
+      if (xb > mx) mx = xb;
+      sum += xb;
+      wsum += static_cast<double>(li + 1) * xb;
+      if (i + 1 >= sp.botidx && i + 1 <= sp.topidx) dev::argmin_merge(mnv, mni, xb, i + 1);
+    }
   }
   if (!any) mx = -1.0e308;
   mx = dev::block_max<NT>(mx, shd);
