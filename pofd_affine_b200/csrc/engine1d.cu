@@ -116,15 +116,6 @@ __device__ int model_solve(const Model1Dev& m, const float* __restrict__ th,
   return POFD_OK;
 }
 
-__device__ __forceinline__ double counts_log2(const double* __restrict__ lk,
-                                              const double* __restrict__ cs,
-                                              int K, double u) {
-  const int k = dev::bsearch_lo(lk, u, 0, K - 1);
-  const double delx = u - lk[k];
-  const double* q = cs + 4 * k;
-  return q[0] + delx * (q[1] + delx * (q[2] + delx * q[3]));
-}
-
 // Knot spline of every proposal: one block per proposal, thread 0 solving
 // in shared memory.  Publishes the model status and the sigma multiplier.
 __global__ void k_model1(Model1Dev m, const float* __restrict__ theta,
@@ -184,18 +175,21 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
   if (i >= NI) return;
   const double f = sd.x[i];
   const double lf = sd.lxa[i];
-  const double minknot = m.minknot, maxknot = m.maxknot;
   double workval = 0.0;
   const bool posb = (f > 0 && bs.haspos && f <= bs.rr_hi);
   const bool negb = !posb && (bs.hasneg && f < 0 && f >= bs.rr_lo);
   if (posb || negb) {
-    const double af = posb ? f : -f;
+    // the knot interval and the range test of every term at this node come
+    // from the host-built table (the reference searches them per call)
+    const unsigned char* __restrict__ kt = sd.kidx + i;
     for (int j = 0; j < nt; ++j) {
-      const double ieta = s_ie[j];
-      const double currarg = af * ieta;
-      if (currarg < minknot || currarg >= maxknot) continue;
-      const double cts = dev::exp2_tab(counts_log2(s_lk, s_cs, K, lf + s_le[j]), e2.t);
-      if (cts > 0) workval += s_w[j] * cts * ieta;
+      const int k = kt[static_cast<size_t>(j) * NI];
+      if (k == 255) continue;
+      const double delx = (lf + s_le[j]) - s_lk[k];
+      const double* q = s_cs + 4 * k;
+      const double cts =
+          dev::exp2_tab(q[0] + delx * (q[1] + delx * (q[2] + delx * q[3])), e2.t);
+      if (cts > 0) workval += s_w[j] * cts * s_ie[j];
     }
   }
   nodes[static_cast<size_t>(row) * NI + i] = bs.prefac * workval;
@@ -1711,6 +1705,32 @@ void Engine1::build_static() {
       for (size_t j = 0; j < tie.size(); ++j) lie[j] = std::log2(tie[j]);
       sd.lxa = up(lxa);
       sd.lie = up(lie);
+      {
+        // knot interval of every (term, node): parameter independent, as
+        // the range test on |x| / eta and log2|x| + log2(1/eta) are
+        const size_t nt = tie.size();
+        std::vector<double> lk(knots_.size());
+        for (size_t k = 0; k < knots_.size(); ++k) lk[k] = std::log2(knots_[k]);
+        const int K = static_cast<int>(knots_.size());
+        std::vector<unsigned char> kt(nt * NI, 255);
+        for (size_t j = 0; j < nt; ++j)
+          for (unsigned i = 0; i < NI; ++i) {
+            const double currarg = std::fabs(sys.x[i]) * tie[j];
+            if (currarg < knots_.front() || currarg >= knots_.back()) continue;
+            const double u = lxa[i] + lie[j];
+            int ilo = 0, ihi = K - 1;
+            while (ihi > ilo + 1) {
+              const int mid = (ihi + ilo) >> 1;
+              if (lk[mid] > u) ihi = mid; else ilo = mid;
+            }
+            kt[j * NI + i] = static_cast<unsigned char>(ilo);
+          }
+        unsigned char* d = nullptr;
+        cuda_check(cudaMalloc(&d, kt.size() + 16), "cudaMalloc");
+        static_allocs_.push_back(d);
+        cuda_check(cudaMemcpy(d, kt.data(), kt.size(), cudaMemcpyHostToDevice), "upload");
+        sd.kidx = d;
+      }
       sd.nodes = 1;
       sd.nterms = static_cast<int>(tie.size());
       if (sd.nterms > maxterms_) maxterms_ = sd.nterms;

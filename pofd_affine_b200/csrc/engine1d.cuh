@@ -35,6 +35,8 @@ struct Side1Dev {
   const double* gamma;  // LDL^T sub-diagonal ratio (ninterp-2)
   const double* lxa;    // log2|x| of the nodes
   const double* lie;    // log2 of the inverse beam terms
+  const unsigned char* kidx;  // [nterms][ninterp] knot interval of term j at
+                              // node i (255: outside the knot range)
   int grid_lo, grid_hi; // inclusive grid index range filled from this side
   double grid_off;      // grid flux = i*dflux + grid_off
 };
