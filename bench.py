@@ -241,11 +241,21 @@ def stage_bytes(stage, P, B, D, n, cuts=None):
                 g = float(np.mean(rmin <= kc))
                 spec += P * row * g
                 inv += P * row * (3.0 + g)
+    # forward pass B alone (pass A fused with the R fill): reads the rows,
+    # writes the bins inside the cut-off
+    fwdB = 2.0 * row * P * B
+    if cuts is not None:
+        fwdB = 0.0
+        for kcs in cuts:
+            kset = max(kcs) if kcs else m
+            fwdB += P * row * (1.0 + float(np.mean(kmin <= kset)))
     return {
         # own FFT path (n = 2m, m complex per row): passes A and B each read
         # and write the rows; the spectrum reads Z and writes one row per
         # dataset
         "k_fftA1+k_fftB1": fwd,
+        "k_fftAR1": row * P * B,                              # write pass A rows
+        "k_fftB1": fwdB,
         "k_spectrum1f": spec,
         "k_fftA1+k_fftB1_inv": inv,
         "k_rfill1": 8.0 * n * P * B,                         # write R
@@ -254,6 +264,23 @@ def stage_bytes(stage, P, B, D, n, cuts=None):
         "cufft_d2z": 8.0 * n * P * B + 16.0 * nc * P * B,
         "cufft_z2d": 16.0 * nc * P * D + 8.0 * n * P * D,
     }.get(stage)
+
+
+def stage_flops(stage, P, B, n):
+    """Algorithmic FP64 flops per launch of the FP64-bound R-grid stages.
+    An R grid point costs 35 (grid flux and interval offset 3, the cubic 6,
+    the table exp2 21, the dflux scale 1, the two moment terms 4); every
+    grid point is counted (the R range, hence the grid, is set to the span
+    the spline covers).  A complex element of the fused forward pass A adds
+    5 log2(m1) (its m1-point DFT) + 12 (the inter-stage and outgoing
+    twiddle products)."""
+    m = n // 2
+    rpts = 35.0 * n * P * B
+    if stage == "k_rfill1":
+        return rpts
+    if stage == "k_fftAR1":
+        return rpts + (5.0 * np.log2(m // 256) + 12.0) * m * P * B
+    return None
 
 
 def read_traffic(stage):
@@ -514,7 +541,19 @@ def main():
     peak_src = "measured" if "hbm_gbs" in hb else "fallback"
     cuts = noise_cuts(L, cfg, cfg["theta0"]) if L.ownFFT() else None
     nbytes = stage_bytes(dom, BATCH, B, D, n, cuts)
-    if nbytes is not None:
+    nflops = stage_flops(dom, BATCH, B, n)
+    if nflops is not None:
+        # FP64-bound R grid fill (fused with the forward pass A): algorithmic
+        # FP64 flops against the measured FP64 FMA peak
+        pk = C.c_double()
+        lib().pofd_fp64_peak(local, C.byref(pk))
+        ach = nflops / (own[dom] * 1e-3) / 1e12
+        roof = {"bound": "fp64", "kernel": dom, "ms_per_launch": own[dom],
+                "achieved": ach, "peak": pk.value, "unit": "TFLOP/s",
+                "frac": ach / pk.value,
+                "peak_source": "measured (pofd_fp64_peak DFMA loop)",
+                "algorithmic_flops": nflops, "traffic": read_traffic(dom)}
+    elif nbytes is not None:
         ach = nbytes / (own[dom] * 1e-3) / 1e9
         traffic = read_traffic(dom)
         roof = {"bound": "hbm", "kernel": dom, "achieved": ach,

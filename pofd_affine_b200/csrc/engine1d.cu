@@ -297,10 +297,50 @@ k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
 }
 
 // The wrapped R grid: 2^spline(flux) * dflux inside each side's covered
-// index range, zero elsewhere (PDFactory.cc:556-613), plus block partial
-// sums of the first and second flux moments (PDFactory.cc:634-665).  The
-// node interval of every grid point is parameter-independent and comes from
-// a host-built table (gidx, -1 outside the covered ranges).
+// index range, zero elsewhere (PDFactory.cc:556-613), plus the first and
+// second flux moments (PDFactory.cc:634-665).  The node interval of every
+// grid point is parameter-independent and comes from a host-built table
+// (gidx, -1 outside the covered ranges).
+struct GridFill1 {
+  double dflux, minflux_R, off0, off1;
+  int wrap, NI;
+  const double* __restrict__ x0;
+  const double* __restrict__ x1;
+  const double* __restrict__ S0;   // this row's node spline [2][4][NI]
+  const double* __restrict__ e2;   // exp2 table in shared memory
+
+  __device__ __forceinline__ GridFill1(const BSet1Dev& bs, const double* spl_row, int ni,
+                                       const double* tab)
+      : dflux(bs.dflux), minflux_R(bs.minflux_R), off0(bs.side[0].grid_off),
+        off1(bs.side[1].grid_off), wrap(bs.wrapRidx), NI(ni), x0(bs.side[0].x),
+        x1(bs.side[1].x), S0(spl_row), e2(tab) {}
+
+  // R at grid index i (di = i as a double) with node interval q (< 0: not
+  // covered), and its moment terms added to mn, var: weight 0 at i = 0 (its
+  // flux is 0), 1/2 at the positive edge, 1 elsewhere
+  __device__ __forceinline__ double point(int i, double di, int q, double& mn,
+                                          double& var) const {
+    const bool neg = i > wrap;
+    const double pd = __dmul_rn(di, dflux);
+    double r = 0.0;
+    if (q >= 0) {
+      const double cflux = __dadd_rn(pd, neg ? off1 : off0);
+      const double* S = S0 + (neg ? 4 * NI : 0);
+      const double delx = cflux - (neg ? x1 : x0)[q];
+      const double v = S[q] + delx * (S[NI + q] + delx * (S[2 * NI + q] + delx * S[3 * NI + q]));
+      r = dev::exp2_tab(v, e2) * dflux;
+    }
+    const double cf = neg ? static_cast<double>(i - wrap - 1) * dflux + minflux_R : pd;
+    double prod = cf * r;
+    if (i == wrap) prod *= 0.5;
+    mn += prod;
+    var += cf * prod;
+    return r;
+  }
+};
+
+// The R grid materialised (cuFFT path, and the own path when the fill is
+// not fused into the forward pass A), with block partial moment sums.
 template <int PER>
 __global__ void __launch_bounds__(NT)
 k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
@@ -315,15 +355,9 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
   e2.load();
   __syncthreads();
   const BSet1Dev& bs = bsets[b];
-  const double dflux = bs.dflux;
-  const int wrap = bs.wrapRidx;
-  const double minflux_R = bs.minflux_R;
+  const GridFill1 rg(bs, spl + static_cast<size_t>(wb) * 2 * 4 * NI, NI, e2.t);
   const int* __restrict__ gidx = bs.gidx;
   double* R = rbuf + static_cast<size_t>(wb) * nc2;
-  const double* S0 = spl + static_cast<size_t>(wb) * 2 * 4 * NI;
-  const double off0 = bs.side[0].grid_off, off1 = bs.side[1].grid_off;
-  const double* __restrict__ x0 = bs.side[0].x;
-  const double* __restrict__ x1 = bs.side[1].x;
   const int base = blockIdx.x * (NT * PER) + threadIdx.x;
   int q[PER];
 #pragma unroll
@@ -336,24 +370,7 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
   for (int k = 0; k < PER; ++k) {
     const int i = base + k * NT;
     if (q[k] == -2) break;
-    const bool neg = i > wrap;
-    double r = 0.0;
-    if (q[k] >= 0) {
-      const double cflux = __dadd_rn(__dmul_rn(static_cast<double>(i), dflux), neg ? off1 : off0);
-      const double* S = S0 + (neg ? 4 * NI : 0);
-      const int j = q[k];
-      const double delx = cflux - (neg ? x1 : x0)[j];
-      const double v = S[j] + delx * (S[NI + j] + delx * (S[2 * NI + j] + delx * S[3 * NI + j]));
-      r = dev::exp2_tab(v, e2.t) * dflux;
-    }
-    R[i] = r;
-    // moment weights: 0 at i = 0, 1/2 at the positive edge, 1 elsewhere
-    const double cf = neg ? static_cast<double>(i - wrap - 1) * dflux + minflux_R
-                          : static_cast<double>(i) * dflux;
-    const double wt = (i == 0) ? 0.0 : ((i == wrap) ? 0.5 : 1.0);
-    const double prod = wt * cf * r;
-    mn += prod;
-    var += cf * prod;
+    R[i] = rg.point(i, static_cast<double>(i), q[k], mn, var);
   }
   mn = dev::block_sum<NT>(mn, shr);
   var = dev::block_sum<NT>(var, shr);
@@ -530,9 +547,10 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
   constexpr int m = M1 * M2;
   constexpr int CB = 256 / L2;
   constexpr int NH = m / 128;
-  extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L
+  extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L, T
   double2* Hs = fs + 256 * L1;
   const double2* Ls = Hs + NH;
+  double2* Ts = Hs + NH + 128;  // inter-stage twiddles W_m^{(m / M1) n2 k1}
   const int row = blockIdx.y;
   if (mstatus[row / nrows_per_w] != 0) return;
   const int b0 = blockIdx.x * CB;
@@ -550,12 +568,13 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
       v[n1] = row_cut(a, m, kc) ? make_double2(0.0, 0.0) : src[a * M2 + b0 + b];
     }
     fft::load_tw2(Hs, WH, WL, NH, t, 256);
+    if (L2 > 1 && t < L1 * L2) Ts[t] = fft::tw2<S>(WH, WL, (m / M1) * (t / L1) * (t % L1));
     __syncthreads();
     fft::dft<L1, S>(v);
     if (L2 > 1) {
 #pragma unroll
       for (int k1 = 0; k1 < L1; ++k1) {
-        if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, (m / M1) * n2 * k1));
+        if (n2 * k1) v[k1] = fft::cmul(v[k1], Ts[n2 * L1 + k1]);
         fs[(n2 * L1 + k1) * CB + b] = v[k1];
       }
     } else {
@@ -583,6 +602,104 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
         dst[c * M2 + bb] = (c * bb) ? fft::cmul(u[k2], fft::tw2<S>(Hs, Ls, c * bb)) : u[k2];
       }
     }
+  }
+}
+
+// Forward pass A with the R grid fill fused in: each thread evaluates the
+// R values of its inputs z_j = R_{2j} + i R_{2j+1} (GridFill1::point, as
+// k_rfill1 does) straight into the registers of its first DFT, so the R grid
+// is neither written to nor read back from memory.  Block partial moment
+// sums go to rpart[row][blockIdx.x] (L2 tiles per row); R at grid index
+// wrap - 1, which k_moments1 needs for its edge term, is stored at its place
+// in rbuf -- pass B overwrites rbuf with the spectrum only after
+// k_moments1 has read it.
+template <int L1, int L2>
+__global__ void __launch_bounds__(256, 2)
+k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
+        const int* __restrict__ mstatus, const double* __restrict__ spl,
+        double* __restrict__ rbuf, double* __restrict__ rpart,
+        double2* __restrict__ out, const double2* __restrict__ WH,
+        const double2* __restrict__ WL) {
+  constexpr int M1 = L1 * L2;
+  constexpr int M2 = 256;
+  constexpr int m = M1 * M2;
+  constexpr int CB = 256 / L2;
+  constexpr int NH = m / 128;
+  extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L
+  __shared__ dev::Exp2Table e2;
+  __shared__ double shr[32];
+  double2* Hs = fs + 256 * L1;
+  const double2* Ls = Hs + NH;
+  double2* Ts = Hs + NH + 128;  // inter-stage twiddles W_m^{(m / M1) n2 k1}
+  const int row = blockIdx.y;
+  const int w = row / B, bset = row - w * B;
+  if (mstatus[w] != 0) return;
+  const int b0 = blockIdx.x * CB;
+  const int t = threadIdx.x;
+  e2.load();
+  fft::load_tw2(Hs, WH, WL, NH, t, 256);
+  if (L2 > 1 && t < L1 * L2) Ts[t] = fft::tw2<-1>(WH, WL, (m / M1) * (t / L1) * (t % L1));
+  __syncthreads();
+  const BSet1Dev& bs = bsets[bset];
+  const GridFill1 rg(bs, spl + static_cast<size_t>(row) * 2 * 4 * NI, NI, e2.t);
+  const int* __restrict__ gidx = bs.gidx;
+  const int iw = bs.wrapRidx - 1;
+  double* Rrow = rbuf + static_cast<size_t>(row) * 2 * rowsz;
+  double2* dst = out + static_cast<size_t>(row) * rowsz;
+  double mn = 0.0, var = 0.0;
+  double2 v[L1];
+  {
+    const int b = t % CB, n2 = t / CB;
+#pragma unroll
+    for (int n1 = 0; n1 < L1; ++n1) {
+      const int i = 2 * ((L2 * n1 + n2) * M2 + b0 + b);
+      const int2 q = __ldg(reinterpret_cast<const int2*>(gidx + i));
+      const double di = static_cast<double>(i);
+      const double r0 = rg.point(i, di, q.x, mn, var);
+      const double r1 = rg.point(i + 1, di + 1.0, q.y, mn, var);
+      if (i == iw) Rrow[i] = r0;
+      if (i + 1 == iw) Rrow[i + 1] = r1;
+      v[n1] = make_double2(r0, r1);
+    }
+    fft::dft<L1, -1>(v);
+    if (L2 > 1) {
+#pragma unroll
+      for (int k1 = 0; k1 < L1; ++k1) {
+        if (n2 * k1) v[k1] = fft::cmul(v[k1], Ts[n2 * L1 + k1]);
+        fs[(n2 * L1 + k1) * CB + b] = v[k1];
+      }
+    } else {
+#pragma unroll
+      for (int k1 = 0; k1 < L1; ++k1) {
+        const int bb = b0 + b;
+        dst[k1 * M2 + bb] = (k1 * bb) ? fft::cmul(v[k1], fft::tw2<-1>(Hs, Ls, k1 * bb)) : v[k1];
+      }
+    }
+  }
+  if (L2 > 1) {
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < L1 / L2; ++it) {
+      const int e = t + 256 * it;
+      const int b = e % CB, k1 = e / CB;
+      double2 u[L2 > 1 ? L2 : 1];
+#pragma unroll
+      for (int n2 = 0; n2 < L2; ++n2) u[n2] = fs[(n2 * L1 + k1) * CB + b];
+      fft::dft<L2, -1>(u);
+#pragma unroll
+      for (int k2 = 0; k2 < L2; ++k2) {
+        const int c = k1 + L1 * k2;
+        const int bb = b0 + b;
+        dst[c * M2 + bb] = (c * bb) ? fft::cmul(u[k2], fft::tw2<-1>(Hs, Ls, c * bb)) : u[k2];
+      }
+    }
+  }
+  mn = dev::block_sum<256>(mn, shr);
+  var = dev::block_sum<256>(var, shr);
+  if (t == 0) {
+    double* o = rpart + (static_cast<size_t>(row) * L2 + blockIdx.x) * 2;
+    o[0] = mn;
+    o[1] = var;
   }
 }
 
@@ -722,6 +839,155 @@ k_fftBP(int m1, int rows, int rowsz, int nrows_per_w, const int* __restrict__ ms
   }
 }
 
+// Pass B fed by bulk copies: a persistent grid (one CTA per SM) walks the
+// tiles (row, rb = min(16, m1) rows c) -- each a contiguous rb * 4 KB run of
+// Y -- through a two-stage shared-memory ring.  Thread 0 issues
+// cp.async.bulk (no multicast) for tile i + 2 as soon as every thread has
+// read tile i out of its stage, so the copy of the next tiles is in flight
+// while a tile is transformed; completion is counted in bytes on the stage's
+// mbarrier.  Same arithmetic as k_fftB.  Every wait is bounded: on a timeout
+// the CTA records kErrTimeout in *err, waits (bounded) for its copies in
+// flight and returns.  Rows of failed proposals are transformed and not
+// stored.
+constexpr int kBTStages = 2;
+constexpr unsigned kBTSpin = 1u << 22;
+constexpr int kErrTimeout = 1;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ bool bt_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_addr(bar);
+  for (unsigned it = 0; it < kBTSpin; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void bt_load(void* dst, const void* src, uint32_t bytes,
+                                        uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes),
+               "r"(smem_addr(bar))
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes),
+      "r"(smem_addr(bar))
+      : "memory");
+}
+
+inline size_t fftBT_smem(int m1) {
+  return (static_cast<size_t>(kBTStages) * FRB * 256 + 16 * 16 * 17 + 2 * m1 + 128 + 256) *
+             sizeof(double2) +
+         kBTStages * sizeof(uint64_t);
+}
+
+template <int S>
+__global__ void __launch_bounds__(256, 1)
+k_fftBT(int m1, int rows, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
+        const double2* __restrict__ in, double2* __restrict__ out,
+        const double2* __restrict__ WH, const double2* __restrict__ WL,
+        const int* __restrict__ kcut, int* __restrict__ err) {
+  extern __shared__ __align__(128) double2 smb[];
+  double2* stage = smb;                           // [kBTStages][FRB * 256]
+  double2* fs = stage + kBTStages * FRB * 256;    // [(k1 * 16 + n2) * 17 + r]
+  double2* Hs = fs + 16 * 16 * 17;
+  const double2* Ls = Hs + 2 * m1;
+  double2* Ts = Hs + 2 * m1 + 128;  // inter-stage twiddles W_256^{n2 k1} (symmetric)
+  uint64_t* full = reinterpret_cast<uint64_t*>(Ts + 256);
+  const int rb = min(FRB, m1);
+  const int tpr = m1 / rb;  // tiles per row
+  const int ntiles = rows * tpr;
+  const int m = m1 * 256;
+  const int t = threadIdx.x;
+  const uint32_t bytes = static_cast<uint32_t>(rb) * 256 * sizeof(double2);
+  auto src_of = [&](int tl) {
+    return in + static_cast<size_t>(tl / tpr) * rowsz + (tl % tpr) * rb * 256;
+  };
+  if (t == 0) {
+    for (int s = 0; s < kBTStages; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[s])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fft::load_tw2(Hs, WH, WL, 2 * m1, t, 256);
+  Ts[t] = fft::tw2<S>(WH, WL, (m / 256) * (t >> 4) * (t & 15));
+  __syncthreads();
+  if (t == 0) {
+    for (int s = 0; s < kBTStages; ++s) {
+      const int tl = blockIdx.x + s * static_cast<int>(gridDim.x);
+      if (tl < ntiles) bt_load(stage + s * FRB * 256, src_of(tl), bytes, &full[s]);
+    }
+  }
+  int it = 0;
+  bool aborted = false;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int s = it % kBTStages;
+    const bool ok = bt_wait(&full[s], static_cast<uint32_t>((it / kBTStages) & 1));
+    // also orders the previous tile's exchange reads before this tile's writes
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+    const int row = tile / tpr, c0 = (tile % tpr) * rb;
+    const double2* st = stage + s * FRB * 256;
+    if (t < 16 * rb) {
+      const int n2 = t & 15, r = t >> 4;
+      double2 v[16];
+#pragma unroll
+      for (int n1 = 0; n1 < 16; ++n1) v[n1] = st[r * 256 + 16 * n1 + n2];
+      fft::dft<16, S>(v);
+#pragma unroll
+      for (int k1 = 0; k1 < 16; ++k1) {
+        if (n2 * k1) v[k1] = fft::cmul(v[k1], Ts[k1 * 16 + n2]);
+        fs[(k1 * 16 + n2) * 17 + r] = v[k1];
+      }
+    }
+    __syncthreads();  // stage s read out, exchange written
+    if (t == 0) {
+      const int nx = tile + kBTStages * static_cast<int>(gridDim.x);
+      if (nx < ntiles) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        bt_load(stage + s * FRB * 256, src_of(nx), bytes, &full[s]);
+      }
+    }
+    if (t < 16 * rb && mstatus[row / nrows_per_w] == 0) {
+      const int r = t % rb, k1 = t / rb;
+      double2* dst = out + static_cast<size_t>(row) * rowsz;
+      const int kc = kcut ? kcut[row] : m;
+      double2 u[16];
+#pragma unroll
+      for (int n2 = 0; n2 < 16; ++n2) u[n2] = fs[(k1 * 16 + n2) * 17 + r];
+      fft::dft<16, S>(u);
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) {
+        // bins beyond the noise cut-off are never read (forward transform)
+        const int k = (c0 + r) + m1 * (k1 + 16 * k2);
+        if (min(k, m - k) <= kc) dst[k] = u[k2];
+      }
+    }
+  }
+  if (aborted && t == 0) {
+    if (err) atomicCAS(err, 0, kErrTimeout);
+    // let the copies in flight land before the CTA's shared memory goes
+    // away: iterations up to it + 1 had their copies issued; the last one
+    // into stage s completes that stage's phase (last / kBTStages)
+    const int nit = (ntiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
+                    static_cast<int>(gridDim.x);
+    const int hi = min(it + kBTStages - 1, nit - 1);
+    for (int s = 0; s < kBTStages; ++s) {
+      const int last = hi - ((hi - s) % kBTStages + kBTStages) % kBTStages;
+      if (last >= 0) bt_wait(&full[s], static_cast<uint32_t>((last / kBTStages) & 1));
+    }
+  }
+}
+
 // Pass B: 256-point DFTs along rows c0..c0+15 of Y (16 x 16 split), stored
 // in natural order Z[c + m1 d].
 template <int S>
@@ -730,9 +996,10 @@ k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
        const double2* __restrict__ in, double2* __restrict__ out,
        const double2* __restrict__ WH, const double2* __restrict__ WL,
        const int* __restrict__ kcut) {
-  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then H, L
+  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then H, L, T
   double2* Hs = fs + 16 * 16 * 17;
   const double2* Ls = Hs + 2 * m1;
+  double2* Ts = Hs + 2 * m1 + 128;  // inter-stage twiddles W_256^{n2 k1} (symmetric)
   const int row = blockIdx.y;
   if (mstatus[row / nrows_per_w] != 0) return;
   const int rb = min(FRB, m1);
@@ -749,13 +1016,14 @@ k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
     for (int n1 = 0; n1 < 16; ++n1) v[n1] = src[(c0 + r) * 256 + 16 * n1 + n2];
   }
   fft::load_tw2(Hs, WH, WL, 2 * m1, t, 256);
+  Ts[t] = fft::tw2<S>(WH, WL, (m / 256) * (t >> 4) * (t & 15));
   __syncthreads();
   if (t < 16 * rb) {
     const int n2 = t & 15, r = t >> 4;
     fft::dft<16, S>(v);
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) {
-      if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, (m / 256) * n2 * k1));
+      if (n2 * k1) v[k1] = fft::cmul(v[k1], Ts[k1 * 16 + n2]);
       fs[(k1 * 16 + n2) * 17 + r] = v[k1];
     }
   }
@@ -1191,10 +1459,16 @@ __global__ void k_reduce1(const BSet1Dev* __restrict__ bsets, int B, int D,
                           int nprop, const int* __restrict__ mstatus,
                           const double* __restrict__ sigmult,
                           const PDInfo1* __restrict__ pinfo, Prior1 pr,
-                          const double* __restrict__ bonus,
+                          const double* __restrict__ bonus, const int* __restrict__ err,
                           double* __restrict__ logl, int* __restrict__ status) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= nprop) return;
+  if (err && *err != 0) {
+    // a bounded wait of the FFT passes timed out: no result is valid
+    logl[w] = __longlong_as_double(0x7ff8000000000000LL);
+    status[w] = POFD_E_CUDA;
+    return;
+  }
   if (mstatus[w] != 0) {
     logl[w] = __longlong_as_double(0x7ff8000000000000LL);
     status[w] = mstatus[w];
@@ -1351,10 +1625,10 @@ T* dalloc(size_t n) {
 
 namespace {
 // exchange (256 L1 entries) plus the twiddle tables: H has m / 128 = 2 m1
-// entries, L 128
-constexpr size_t kFftASmemMax = (256 * 16 + 2 * 256 + 128) * sizeof(double2);
+// entries, L 128, the inter-stage table 256
+constexpr size_t kFftASmemMax = (256 * 16 + 2 * 256 + 128 + 256) * sizeof(double2);
 inline size_t fftA_smem(int m1) {
-  return (256 * static_cast<size_t>(m1 < 16 ? m1 : 16) + 2 * m1 + 128) * sizeof(double2);
+  return (256 * static_cast<size_t>(m1 < 16 ? m1 : 16) + 2 * m1 + 128 + 256) * sizeof(double2);
 }
 
 template <int S>
@@ -1376,6 +1650,37 @@ void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const in
 #undef POFD_FFTA
 }
 
+// Fused R fill + forward pass A; returns the tiles per row (partial
+// moment sums per row in rpart).
+int launch_fftAR(int m1, int rows, cudaStream_t st, const BSet1Dev* bsets, int B, int NI,
+                 int rowsz, const int* mstatus, const double* spl, double* rbuf, double* rpart,
+                 double2* out, const double2* WH, const double2* WL) {
+#define POFD_FFTAR(L1, L2)                                                                 \
+  k_fftAR<L1, L2><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(bsets, B, NI, rowsz, mstatus, \
+                                                              spl, rbuf, rpart, out, WH, WL); \
+  return L2
+  switch (m1) {
+    case 8: POFD_FFTAR(8, 1);
+    case 16: POFD_FFTAR(16, 1);
+    case 32: POFD_FFTAR(16, 2);
+    case 64: POFD_FFTAR(16, 4);
+    case 128: POFD_FFTAR(16, 8);
+    case 256: POFD_FFTAR(16, 16);
+    default: throw Error(POFD_E_ARG, "own FFT: unsupported size");
+  }
+#undef POFD_FFTAR
+}
+
+void fftAR_attr() {
+  const int sm = static_cast<int>(kFftASmemMax);
+  cuda_check(cudaFuncSetAttribute(k_fftAR<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+}
+
 template <int S>
 void fftA_attr() {
   const int sm = static_cast<int>(kFftASmemMax);
@@ -1387,7 +1692,7 @@ void fftA_attr() {
   cuda_check(cudaFuncSetAttribute(k_fftA<16, 16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
 }
 
-constexpr size_t kFftBSmemMax = (16 * 16 * 17 + 2 * 256 + 128) * sizeof(double2);
+constexpr size_t kFftBSmemMax = (16 * 16 * 17 + 2 * 256 + 128 + 256) * sizeof(double2);
 
 template <int S>
 void launch_fftAP(int m1, int rows, int grid, cudaStream_t st, int rowsz, int nrw,
@@ -1419,7 +1724,7 @@ void fftAP_attr() {
                                   static_cast<int>(kFftBSmemMax)), "attr");
 }
 inline size_t fftB_smem(int m1) {
-  return (16 * 16 * 17 + 2 * static_cast<size_t>(m1) + 128) * sizeof(double2);
+  return (16 * 16 * 17 + 2 * static_cast<size_t>(m1) + 128 + 256) * sizeof(double2);
 }
 }  // namespace
 
@@ -1909,7 +2214,8 @@ void Engine1::set_tuning(const Tune1& t) {
   if (t.rnodes_threads != 64 && t.rnodes_threads != 128 && t.rnodes_threads != 256)
     throw Error(POFD_E_ARG, "rnodes_threads must be 64, 128 or 256");
   if (t.spec_blocks < 1 || t.spec_blocks > 64) throw Error(POFD_E_ARG, "spec_blocks must be in [1, 64]");
-  if (t.fft_persist != 0 && t.fft_persist != 1) throw Error(POFD_E_ARG, "fft_persist must be 0 or 1");
+  if (t.fft_persist < 0 || t.fft_persist > 2) throw Error(POFD_E_ARG, "fft_persist must be 0, 1 or 2");
+  if (t.rfill_fused != 0 && t.rfill_fused != 1) throw Error(POFD_E_ARG, "rfill_fused must be 0 or 1");
   const bool fft_changed = (t.own_fft != 0) != (tune_.own_fft != 0);
   tune_ = t;
   tune_.own_fft = t.own_fft ? 1 : 0;
@@ -1921,7 +2227,7 @@ void Engine1::set_tuning(const Tune1& t) {
 // Coordinate descent over the knobs, one pass, each candidate timed on the
 // captured graph of the whole sequence.  The FFT choice is tried only where
 // the own FFT supports the size.
-void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7) {
+void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out8) {
   if (nprop == 0 || reps < 1) throw Error(POFD_E_ARG, "autotune needs rows and reps >= 1");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
   const double t_untuned = time_sequence(nprop, theta, npar, reps);
@@ -1953,10 +2259,18 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     t.rnodes_threads = th;
     trial(t);
   }
-  if (best.own_fft && own_possible && n_ / 512 >= 16) {
+  if (best.own_fft && own_possible) {
     Tune1 t = best;
-    t.fft_persist = best.fft_persist ? 0 : 1;
+    t.rfill_fused = best.rfill_fused ? 0 : 1;
     trial(t);
+  }
+  if (best.own_fft && own_possible) {
+    for (int fp : {0, 1, 2}) {
+      if (fp == best.fft_persist || (fp == 1 && n_ / 512 < 16)) continue;
+      Tune1 t = best;
+      t.fft_persist = fp;
+      trial(t);
+    }
   }
   if (best.own_fft && own_possible) {
     for (int sb : {2, 4, 8, 16, 32}) {
@@ -1967,14 +2281,15 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     }
   }
   set_tuning(best);
-  if (out7) {
-    out7[0] = best.own_fft;
-    out7[1] = best.rfill_per;
-    out7[2] = best.rnodes_threads;
-    out7[3] = best.spec_blocks;
-    out7[4] = best.fft_persist;
-    out7[5] = best_ms;
-    out7[6] = t_untuned;
+  if (out8) {
+    out8[0] = best.own_fft;
+    out8[1] = best.rfill_per;
+    out8[2] = best.rnodes_threads;
+    out8[3] = best.spec_blocks;
+    out8[4] = best.fft_persist;
+    out8[5] = best.rfill_fused;
+    out8[6] = best_ms;
+    out8[7] = t_untuned;
   }
 }
 
@@ -1987,8 +2302,13 @@ const char* Engine1::stage_name(int i) const {
       "k_model1+k_rnodes1", "k_rspline1", "k_rfill1", "k_moments1",
       "k_fftA1+k_fftB1", "k_spectrum1f", "k_fftA1+k_fftB1_inv", "k_pscan1", "k_pfinish1",
       "k_reduce1"};
+  static const char* fused[kNumStages] = {
+      "k_model1+k_rnodes1", "k_rspline1", "k_fftAR1", "k_moments1",
+      "k_fftB1", "k_spectrum1f", "k_fftA1+k_fftB1_inv", "k_pscan1", "k_pfinish1",
+      "k_reduce1"};
   if (i < 0 || i >= kNumStages) return "";
-  return own_fft_ ? own[i] : lib[i];
+  if (!own_fft_) return lib[i];
+  return fused_fill() ? fused[i] : own[i];
 }
 
 // Prior setters (calcLike.h:251-269, calcLike.cc:839-877).  The prior
@@ -2087,7 +2407,8 @@ void Engine1::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.nodes, ws_.spl,
                   ws_.rbuf, ws_.rpart, ws_.mom, ws_.pbuf, ws_.ppart,
                   ws_.pmidx, ws_.pinfo, ws_.pdout, ws_.theta_in, ws_.logl,
-                  ws_.status, ws_.tmp, ws_.bonus, ws_.kcut_set, ws_.kcut_ds};
+                  ws_.status, ws_.tmp, ws_.bonus, ws_.kcut_set, ws_.kcut_ds,
+                  ws_.err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
@@ -2124,6 +2445,7 @@ void Engine1::reserve(unsigned P) {
     ws_.tmp = dalloc<double>(static_cast<size_t>(P) * std::max(B_, D_) * nc2);
     fftA_attr<-1>();
     fftA_attr<1>();
+    fftAR_attr();
     if (n_ / 512 >= 16) {
       fftAP_attr<-1>();
       fftAP_attr<1>();
@@ -2132,8 +2454,15 @@ void Engine1::reserve(unsigned P) {
                                     static_cast<int>(kFftBSmemMax)), "attr");
     cuda_check(cudaFuncSetAttribute(k_fftB<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kFftBSmemMax)), "attr");
+    const int bt = static_cast<int>(fftBT_smem(static_cast<int>(n_ / 512)));
+    cuda_check(cudaFuncSetAttribute(k_fftBT<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt),
+               "attr");
+    cuda_check(cudaFuncSetAttribute(k_fftBT<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt),
+               "attr");
   }
   ws_.mom = dalloc<double>(static_cast<size_t>(P) * B_ * 4);
+  ws_.err = dalloc<int>(1);
+  cuda_check(cudaMemset(ws_.err, 0, sizeof(int)), "cudaMemset");
   ws_.kcut_set = dalloc<int>(static_cast<size_t>(P) * B_);
   ws_.kcut_ds = dalloc<int>(static_cast<size_t>(P) * D_);
   ws_.pbuf = dalloc<double>(static_cast<size_t>(P) * D_ * nc2);
@@ -2215,21 +2544,39 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
     double2* tmp = reinterpret_cast<double2*>(ws_.tmp);
     double2* rb = reinterpret_cast<double2*>(ws_.rbuf);
     double2* pb = reinterpret_cast<double2*>(ws_.pbuf);
-    {
+    const bool fused = fused_fill();
+    int ntile = static_cast<int>(ntile_);
+    if (fused) {
+      // R fill inside the forward pass A: the grid goes straight into tmp
+      ntile = launch_fftAR(m1, P * B, st, d_bsets_, B, NI, rowsz, ws_.mstatus, ws_.spl,
+                           ws_.rbuf, ws_.rpart, tmp, d_wh_, d_wl_);
+    } else {
       dim3 grid(ntile_, P * B);
       launch_rfill(tune_.rfill_per, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
     k_moments1<<<(P * B + 127) / 128, 128, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc2,
-                                                    static_cast<int>(ntile_), P * B,
+                                                    ntile, P * B,
                                                     ws_.mstatus, ws_.sigmult, ws_.rbuf, ws_.rpart,
                                                     ws_.mom, ws_.kcut_set, ws_.kcut_ds);
     mark(4);
     const int rb_rows = m1 < FRB ? m1 : FRB;
-    const bool persist = tune_.fft_persist && m1 >= 16;
+    const bool persist = tune_.fft_persist == 1 && m1 >= 16;
+    const bool bulkB = tune_.fft_persist == 2;
     const int gA = std::min(P * B * (m1 / 16 > 0 ? m1 / 16 : 1), 2 * sm_count_);
-    if (persist) {
+    if (bulkB) {
+      // cleared once per sequence, before the first pass that may set it
+      cuda_check(cudaMemsetAsync(ws_.err, 0, sizeof(int), st), "cudaMemsetAsync");
+      if (!fused)
+        launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
+      const int gB = std::min(P * B * (m1 / rb_rows), sm_count_);
+      k_fftBT<-1><<<gB, 256, fftBT_smem(m1), st>>>(m1, P * B, rowsz, B, ws_.mstatus, tmp, rb,
+                                                   d_wh_, d_wl_, ws_.kcut_set, ws_.err);
+    } else if (fused) {
+      k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, fftB_smem(m1), st>>>(
+          m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_, ws_.kcut_set);
+    } else if (persist) {
       launch_fftAP<-1>(m1, P * B, gA, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
       k_fftBP<-1><<<gA, 256, fftB_smem(m1), st>>>(m1, P * B, rowsz, B, ws_.mstatus, tmp, rb,
                                                   d_wh_, d_wl_, ws_.kcut_set);
@@ -2247,7 +2594,12 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                         ws_.kcut_ds);
     }
     mark(6);
-    if (persist) {
+    if (bulkB) {
+      launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_, ws_.kcut_ds);
+      const int gB = std::min(P * D * (m1 / rb_rows), sm_count_);
+      k_fftBT<1><<<gB, 256, fftBT_smem(m1), st>>>(m1, P * D, rowsz, D, ws_.mstatus, tmp, pb,
+                                                  d_wh_, d_wl_, nullptr, ws_.err);
+    } else if (persist) {
       const int gI = std::min(P * D * (m1 / 16), 2 * sm_count_);
       launch_fftAP<1>(m1, P * D, gI, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_,
                       ws_.kcut_ds);
@@ -2299,8 +2651,9 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                    ws_.ppart, ws_.pmidx, ws_.pinfo);
   mark(9);
   k_reduce1<<<(P + 127) / 128, 128, 0, st>>>(d_bsets_, B, D, P, ws_.mstatus,
-                                            ws_.sigmult, ws_.pinfo, prior_, ws_.bonus, logl,
-                                            status);
+                                            ws_.sigmult, ws_.pinfo, prior_, ws_.bonus,
+                                            own_fft_ && tune_.fft_persist == 2 ? ws_.err : nullptr,
+                                            logl, status);
   mark(10);
   cuda_check(cudaGetLastError(), "kernel launch");
 }

@@ -31,6 +31,22 @@ def test_own_fft_matches_cufft(orc, gpu_ctx, n):
     assert list(so) == list(sc)
     ok = so == 0
     assert np.max(np.abs(lo[ok] - lc[ok])) < 1e-7
+    # the R grid fill fused into the forward pass A (default) against the
+    # materialised grid: the same values, moments grouped differently
+    assert L.getTuning()["rfill_fused"] == 1
+    L.setTuning(rfill_fused=0)
+    lu, su = L.getLogLikeBatch(th)
+    L.setTuning(rfill_fused=1)
+    assert list(su) == list(so)
+    assert np.max(np.abs(lu[ok] - lo[ok])) < 1e-7
+    # pass B fed by bulk copies through a shared-memory ring: same arithmetic
+    L.setTuning(fft_persist=2)
+    lb, sb = L.getLogLikeBatch(th)
+    pb, ib = L.getPD(1, 0, th[0], setLog=False)
+    L.setTuning(fft_persist=0)
+    assert list(sb) == list(so)
+    assert np.max(np.abs(lb[ok] - lo[ok])) < 1e-9
+    assert np.max(np.abs(pb - po)) <= 1e-13 * po.max()
     # where the P(D) tail lies at the transform's rounding floor (large n),
     # the first bin below the reference's split threshold is set by rounding
     # and can differ between any two FFTs; the unwrapped arrays are then the
