@@ -884,7 +884,7 @@ __device__ __forceinline__ void bt_load(void* dst, const void* src, uint32_t byt
 }
 
 inline size_t fftBT_smem(int m1) {
-  return (static_cast<size_t>(kBTStages) * FRB * 256 + 16 * 16 * 17 + 2 * m1 + 128 + 256) *
+  return (static_cast<size_t>(kBTStages) * FRB * 256 + 16 * 16 * 17 + 256) *
              sizeof(double2) +
          kBTStages * sizeof(uint64_t);
 }
@@ -898,9 +898,7 @@ k_fftBT(int m1, int rows, int rowsz, int nrows_per_w, const int* __restrict__ ms
   extern __shared__ __align__(128) double2 smb[];
   double2* stage = smb;                           // [kBTStages][FRB * 256]
   double2* fs = stage + kBTStages * FRB * 256;    // [(k1 * 16 + n2) * 17 + r]
-  double2* Hs = fs + 16 * 16 * 17;
-  const double2* Ls = Hs + 2 * m1;
-  double2* Ts = Hs + 2 * m1 + 128;  // inter-stage twiddles W_256^{n2 k1} (symmetric)
+  double2* Ts = fs + 16 * 16 * 17;  // inter-stage twiddles W_256^{n2 k1} (symmetric)
   uint64_t* full = reinterpret_cast<uint64_t*>(Ts + 256);
   const int rb = min(FRB, m1);
   const int tpr = m1 / rb;  // tiles per row
@@ -916,7 +914,6 @@ k_fftBT(int m1, int rows, int rowsz, int nrows_per_w, const int* __restrict__ ms
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[s])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  fft::load_tw2(Hs, WH, WL, 2 * m1, t, 256);
   Ts[t] = fft::tw2<S>(WH, WL, (m / 256) * (t >> 4) * (t & 15));
   __syncthreads();
   if (t == 0) {
@@ -996,10 +993,8 @@ k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
        const double2* __restrict__ in, double2* __restrict__ out,
        const double2* __restrict__ WH, const double2* __restrict__ WL,
        const int* __restrict__ kcut) {
-  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then H, L, T
-  double2* Hs = fs + 16 * 16 * 17;
-  const double2* Ls = Hs + 2 * m1;
-  double2* Ts = Hs + 2 * m1 + 128;  // inter-stage twiddles W_256^{n2 k1} (symmetric)
+  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then T
+  double2* Ts = fs + 16 * 16 * 17;  // inter-stage twiddles W_256^{n2 k1} (symmetric)
   const int row = blockIdx.y;
   if (mstatus[row / nrows_per_w] != 0) return;
   const int rb = min(FRB, m1);
@@ -1015,7 +1010,6 @@ k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
 #pragma unroll
     for (int n1 = 0; n1 < 16; ++n1) v[n1] = src[(c0 + r) * 256 + 16 * n1 + n2];
   }
-  fft::load_tw2(Hs, WH, WL, 2 * m1, t, 256);
   Ts[t] = fft::tw2<S>(WH, WL, (m / 256) * (t >> 4) * (t & 15));
   __syncthreads();
   if (t < 16 * rb) {
@@ -1232,17 +1226,50 @@ k_pscan1(const BSet1Dev* __restrict__ bsets, const DSet1Dev* __restrict__ dsets,
     }
   }
   if (!any) mx = -1.0e308;
-  mx = dev::block_max<NT>(mx, shd);
-  sum = dev::block_sum<NT>(sum, shd);
-  wsum = dev::block_sum<NT>(wsum, shd);
-  dev::block_argmin<NT>(mnv, mni, shd, shi);
-  if (threadIdx.x == 0) {
-    double* o = ppart + (static_cast<size_t>(wd) * nchunk + blockIdx.x) * 4;
-    o[0] = mx;
-    o[1] = sum;
-    o[2] = wsum;
-    o[3] = mnv;
-    pmidx[static_cast<size_t>(wd) * nchunk + blockIdx.x] = mni;
+  // the four block reductions in one shared-memory round, each with the
+  // butterfly trees of dev::block_max / block_sum / block_argmin (the same
+  // results, one barrier instead of a dozen)
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = dev::dmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+    const double v2 = __shfl_xor_sync(0xffffffffu, mnv, o);
+    const int i2 = __shfl_xor_sync(0xffffffffu, mni, o);
+    dev::argmin_merge(mnv, mni, v2, i2);
+  }
+  const int wp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    shd[wp] = mx;
+    shd[8 + wp] = sum;
+    shd[16 + wp] = wsum;
+    shd[24 + wp] = mnv;
+    shi[wp] = mni;
+  }
+  __syncthreads();
+  if (wp == 0) {
+    static_assert(NT / 32 <= 8, "one shared slot per warp");
+    const bool in = l < NT / 32;
+    mx = in ? shd[l] : -1.0e308;
+    sum = in ? shd[8 + l] : 0.0;
+    wsum = in ? shd[16 + l] : 0.0;
+    mnv = in ? shd[24 + l] : 1.0e308;
+    mni = in ? shi[l] : 0x7fffffff;
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = dev::dmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+      const double v2 = __shfl_xor_sync(0xffffffffu, mnv, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, mni, o);
+      dev::argmin_merge(mnv, mni, v2, i2);
+    }
+    if (l == 0) {
+      double* o = ppart + (static_cast<size_t>(wd) * nchunk + blockIdx.x) * 4;
+      o[0] = mx;
+      o[1] = sum;
+      o[2] = wsum;
+      o[3] = mnv;
+      pmidx[static_cast<size_t>(wd) * nchunk + blockIdx.x] = mni;
+    }
   }
 }
 
@@ -1692,7 +1719,8 @@ void fftA_attr() {
   cuda_check(cudaFuncSetAttribute(k_fftA<16, 16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
 }
 
-constexpr size_t kFftBSmemMax = (16 * 16 * 17 + 2 * 256 + 128 + 256) * sizeof(double2);
+constexpr size_t kFftBSmemMax = (16 * 16 * 17 + 256) * sizeof(double2);
+constexpr size_t kFftBPSmemMax = (16 * 16 * 17 + 2 * 256 + 128) * sizeof(double2);
 
 template <int S>
 void launch_fftAP(int m1, int rows, int grid, cudaStream_t st, int rowsz, int nrw,
@@ -1721,10 +1749,14 @@ void fftAP_attr() {
   cuda_check(cudaFuncSetAttribute(k_fftAP<8, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
   cuda_check(cudaFuncSetAttribute(k_fftAP<16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
   cuda_check(cudaFuncSetAttribute(k_fftBP<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(kFftBSmemMax)), "attr");
+                                  static_cast<int>(kFftBPSmemMax)), "attr");
 }
-inline size_t fftB_smem(int m1) {
-  return (16 * 16 * 17 + 2 * static_cast<size_t>(m1) + 128 + 256) * sizeof(double2);
+// pass B: the exchange and the inter-stage table (its twiddles are W_256
+// powers only)
+inline size_t fftB_smem(int) { return kFftBSmemMax; }
+// persistent pass B: exchange plus the H and L tables
+inline size_t fftBP_smem(int m1) {
+  return (16 * 16 * 17 + 2 * static_cast<size_t>(m1) + 128) * sizeof(double2);
 }
 }  // namespace
 
@@ -2578,7 +2610,7 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
           m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_, ws_.kcut_set);
     } else if (persist) {
       launch_fftAP<-1>(m1, P * B, gA, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
-      k_fftBP<-1><<<gA, 256, fftB_smem(m1), st>>>(m1, P * B, rowsz, B, ws_.mstatus, tmp, rb,
+      k_fftBP<-1><<<gA, 256, fftBP_smem(m1), st>>>(m1, P * B, rowsz, B, ws_.mstatus, tmp, rb,
                                                   d_wh_, d_wl_, ws_.kcut_set);
     } else {
       launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
@@ -2603,7 +2635,7 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
       const int gI = std::min(P * D * (m1 / 16), 2 * sm_count_);
       launch_fftAP<1>(m1, P * D, gI, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_,
                       ws_.kcut_ds);
-      k_fftBP<1><<<gI, 256, fftB_smem(m1), st>>>(m1, P * D, rowsz, D, ws_.mstatus, tmp, pb,
+      k_fftBP<1><<<gI, 256, fftBP_smem(m1), st>>>(m1, P * D, rowsz, D, ws_.mstatus, tmp, pb,
                                                  d_wh_, d_wl_, nullptr);
     } else {
       launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_, ws_.kcut_ds);
