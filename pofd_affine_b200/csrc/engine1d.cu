@@ -2193,6 +2193,8 @@ void Engine1::drop_graphs() {
   for (auto& kv : plans_) {
     for (auto& g : kv.second.graphs) cudaGraphExecDestroy(g.second);
     kv.second.graphs.clear();
+    if (kv.second.host_graph) cudaGraphExecDestroy(kv.second.host_graph);
+    kv.second.host_graph = nullptr;
   }
 }
 
@@ -2439,13 +2441,12 @@ void Engine1::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.nodes, ws_.spl,
                   ws_.rbuf, ws_.rpart, ws_.mom, ws_.pbuf, ws_.ppart,
                   ws_.pmidx, ws_.pinfo, ws_.pdout, ws_.theta_in, ws_.logl,
-                  ws_.status, ws_.tmp, ws_.bonus, ws_.kcut_set, ws_.kcut_ds,
+                  ws_.tmp, ws_.bonus, ws_.kcut_set, ws_.kcut_ds,
                   ws_.err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
-  if (ws_.h_logl) cudaFreeHost(ws_.h_logl);
-  if (ws_.h_status) cudaFreeHost(ws_.h_status);
+  if (ws_.h_logl) cudaFreeHost(ws_.h_logl);  // h_status lies in the same block
   ws_ = Workspace1{};
 }
 
@@ -2502,8 +2503,9 @@ void Engine1::reserve(unsigned P) {
   ws_.pmidx = dalloc<int>(static_cast<size_t>(P) * D_ * nchunk_);
   ws_.pinfo = dalloc<PDInfo1>(static_cast<size_t>(P) * D_);
   ws_.pdout = dalloc<double>(n_);
-  ws_.logl = dalloc<double>(P);
-  ws_.status = dalloc<int>(P);
+  // logL [P] then status [P] in one allocation: one download per call
+  ws_.logl = dalloc<double>(P + (P + 1) / 2);
+  ws_.status = reinterpret_cast<int*>(ws_.logl + P);
   cuda_check(cudaFuncSetAttribute(k_rnodes1, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>((KMAX + 4 * KMAX + 3 * MAXTERMS) * sizeof(double))),
              "smem attribute");
@@ -2750,6 +2752,44 @@ cudaGraphExec_t Engine1::graph_for(unsigned nprop, const float* theta,
   return ge;
 }
 
+// The upload of theta, the launch sequence and the download of logL and
+// status, captured together for each batch size after its first (eager) use.
+cudaGraphExec_t Engine1::host_graph_for(unsigned nprop, unsigned npar) {
+  Plans& pl = plans_.at(nprop);
+  if (pl.no_graph || !pl.warmed) return nullptr;
+  if (pl.host_graph && pl.host_npar == npar) return pl.host_graph;
+  if (pl.host_graph) {
+    cudaGraphExecDestroy(pl.host_graph);
+    pl.host_graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    bool threw = false;
+    try {
+      cuda_check(cudaMemcpyAsync(ws_.theta_in, ws_.h_theta,
+                                 static_cast<size_t>(nprop) * npar * sizeof(float),
+                                 cudaMemcpyHostToDevice, stream_), "H2D theta");
+      launch_all(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_, nullptr);
+      cuda_check(cudaMemcpyAsync(ws_.h_logl, ws_.logl,
+                                 ws_.P * sizeof(double) + nprop * sizeof(int),
+                                 cudaMemcpyDeviceToHost, stream_), "D2H results");
+    } catch (...) {
+      threw = true;
+    }
+    const cudaError_t ec = cudaStreamEndCapture(stream_, &g);
+    if (threw || ec != cudaSuccess || !g || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+      ge = nullptr;
+    if (g) cudaGraphDestroy(g);
+  }
+  cudaGetLastError();
+  if (ge) {
+    pl.host_graph = ge;
+    pl.host_npar = npar;
+  }
+  return ge;
+}
+
 void Engine1::eval_host(unsigned nprop, const float* theta, unsigned npar,
                         double* logl, int* status) {
   if (nprop == 0) return;
@@ -2765,18 +2805,24 @@ void Engine1::eval_host(unsigned nprop, const float* theta, unsigned npar,
     drop_graphs();
   }
   if (!ws_.h_logl) {
-    cuda_check(cudaMallocHost(&ws_.h_logl, ws_.P * sizeof(double)), "cudaMallocHost");
-    cuda_check(cudaMallocHost(&ws_.h_status, ws_.P * sizeof(int)), "cudaMallocHost");
+    // logL [P] then status [P], as on the device
+    cuda_check(cudaMallocHost(&ws_.h_logl, ws_.P * (sizeof(double) + sizeof(int))),
+               "cudaMallocHost");
+    ws_.h_status = reinterpret_cast<int*>(ws_.h_logl + ws_.P);
   }
   std::memcpy(ws_.h_theta, theta, static_cast<size_t>(nprop) * npar * sizeof(float));
-  cuda_check(cudaMemcpyAsync(ws_.theta_in, ws_.h_theta,
-                             static_cast<size_t>(nprop) * npar * sizeof(float),
-                             cudaMemcpyHostToDevice, stream_), "H2D theta");
-  enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);
-  cuda_check(cudaMemcpyAsync(ws_.h_logl, ws_.logl, nprop * sizeof(double),
-                             cudaMemcpyDeviceToHost, stream_), "D2H logl");
-  cuda_check(cudaMemcpyAsync(ws_.h_status, ws_.status, nprop * sizeof(int),
-                             cudaMemcpyDeviceToHost, stream_), "D2H status");
+  ensure_plans(nprop);
+  cudaGraphExec_t g = host_graph_for(nprop, npar);
+  if (g) {
+    cuda_check(cudaGraphLaunch(g, stream_), "graph launch");
+  } else {
+    cuda_check(cudaMemcpyAsync(ws_.theta_in, ws_.h_theta,
+                               static_cast<size_t>(nprop) * npar * sizeof(float),
+                               cudaMemcpyHostToDevice, stream_), "H2D theta");
+    enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);
+    cuda_check(cudaMemcpyAsync(ws_.h_logl, ws_.logl, ws_.P * sizeof(double) + nprop * sizeof(int),
+                               cudaMemcpyDeviceToHost, stream_), "D2H results");
+  }
   cuda_check(cudaStreamSynchronize(stream_), "synchronize");
   std::memcpy(logl, ws_.h_logl, nprop * sizeof(double));
   std::memcpy(status, ws_.h_status, nprop * sizeof(int));

@@ -264,9 +264,14 @@ class Engine1 {
     std::vector<std::pair<GraphKey, cudaGraphExec_t>> graphs;
     bool warmed = false;
     bool no_graph = false;
+    // eval_host's graph: theta upload, the launch sequence and the result
+    // download in one launch (for host_npar parameters per row)
+    cudaGraphExec_t host_graph = nullptr;
+    unsigned host_npar = 0;
   };
   cudaGraphExec_t graph_for(unsigned nprop, const float* theta, unsigned npar,
                             double* logl, int* status);
+  cudaGraphExec_t host_graph_for(unsigned nprop, unsigned npar);
   void drop_graphs();
   std::map<unsigned, Plans> plans_;
   FftWorkArea fftwork_;
