@@ -194,6 +194,98 @@ __device__ __forceinline__ void block_affine_rscan(double& a, double& b,
   }
 }
 
+// Warp-shuffle forms of the two scans for NT threads (a multiple of 32,
+// at most 1024): a register scan inside each warp, one warp scanning the
+// warp totals, and each warp composed with the total of the warps before it
+// (after it, for the reverse scan).  Shared scratch of 2 * 32 doubles, two
+// barriers.  Besides the inclusive map of the thread, returns the b of the
+// neighbour's inclusive map (the previous thread's, 0 for thread 0; the
+// next thread's, 0 for the last), i.e. the value the neighbour's composed
+// map takes at z = 0.
+template <int NT>
+__device__ __forceinline__ double block_affine_scan_w(double& a, double& b, double* sh) {
+  const int t = threadIdx.x, l = t & 31, w = t >> 5;
+  constexpr int NW = NT / 32;
+  for (int off = 1; off < 32; off <<= 1) {
+    const double pa = __shfl_up_sync(0xffffffffu, a, off);
+    const double pb = __shfl_up_sync(0xffffffffu, b, off);
+    if (l >= off) {
+      b = a * pb + b;
+      a = a * pa;
+    }
+  }
+  if (l == 31) {
+    sh[w] = a;
+    sh[32 + w] = b;
+  }
+  __syncthreads();
+  if (w == 0) {
+    double wa = (l < NW) ? sh[l] : 1.0, wb = (l < NW) ? sh[32 + l] : 0.0;
+    for (int off = 1; off < 32; off <<= 1) {
+      const double pa = __shfl_up_sync(0xffffffffu, wa, off);
+      const double pb = __shfl_up_sync(0xffffffffu, wb, off);
+      if (l >= off) {
+        wb = wa * pb + wb;
+        wa = wa * pa;
+      }
+    }
+    if (l < NW) {
+      sh[l] = wa;
+      sh[32 + l] = wb;
+    }
+  }
+  __syncthreads();
+  const double pb0 = (w > 0) ? sh[32 + w - 1] : 0.0;
+  if (w > 0) {
+    b = a * pb0 + b;
+    a = a * sh[w - 1];
+  }
+  const double nb = __shfl_up_sync(0xffffffffu, b, 1);
+  return (l > 0) ? nb : pb0;
+}
+
+template <int NT>
+__device__ __forceinline__ double block_affine_rscan_w(double& a, double& b, double* sh) {
+  const int t = threadIdx.x, l = t & 31, w = t >> 5;
+  constexpr int NW = NT / 32;
+  for (int off = 1; off < 32; off <<= 1) {
+    const double pa = __shfl_down_sync(0xffffffffu, a, off);
+    const double pb = __shfl_down_sync(0xffffffffu, b, off);
+    if (l + off < 32) {
+      b = a * pb + b;
+      a = a * pa;
+    }
+  }
+  if (l == 0) {
+    sh[w] = a;
+    sh[32 + w] = b;
+  }
+  __syncthreads();
+  if (w == 0) {
+    double wa = (l < NW) ? sh[l] : 1.0, wb = (l < NW) ? sh[32 + l] : 0.0;
+    for (int off = 1; off < 32; off <<= 1) {
+      const double pa = __shfl_down_sync(0xffffffffu, wa, off);
+      const double pb = __shfl_down_sync(0xffffffffu, wb, off);
+      if (l + off < NW) {
+        wb = wa * pb + wb;
+        wa = wa * pa;
+      }
+    }
+    if (l < NW) {
+      sh[l] = wa;
+      sh[32 + l] = wb;
+    }
+  }
+  __syncthreads();
+  const double nb0 = (w + 1 < NW) ? sh[32 + w + 1] : 0.0;
+  if (w + 1 < NW) {
+    b = a * nb0 + b;
+    a = a * sh[w + 1];
+  }
+  const double nb = __shfl_down_sync(0xffffffffu, b, 1);
+  return (l < 31) ? nb : nb0;
+}
+
 // Largest i in [lo, hi-1] with x[i] <= v (x increasing): the bisection of
 // the interpolation library the reference uses, clamped to [lo, hi-1].
 __device__ __forceinline__ int bsearch_lo(const double* __restrict__ x,

@@ -36,6 +36,7 @@ namespace {
 constexpr int NT = 256;           // threads per block for the streaming kernels
 constexpr int kMaxTilesPer = 4;   // smallest R-fill tile: NT * 4 grid points
 constexpr int CHUNK = NT * 16;    // P(D) elements per reduction block
+constexpr int kSplineThreads = 1024;  // threads per node-spline block
 constexpr int KMAX = Engine1::KMAX;
 constexpr int MAXTERMS = 4096;    // beam terms held in shared memory
 
@@ -199,7 +200,8 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
 // the tridiagonal system, forward and back substitution against the
 // precomputed LDL^T factors as two block-wide affine-map scans, then the
 // per-interval (y, b, c, d) (PDFactory.cc:466-474, 522).
-__global__ void __launch_bounds__(NT)
+template <int RT>
+__global__ void __launch_bounds__(RT)
 k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
            const int* __restrict__ mstatus, const double* __restrict__ nodes,
            double* __restrict__ spl) {
@@ -212,15 +214,15 @@ k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
   if (!sd.nodes || mstatus[w] != 0) return;
   double* y = sm;             // NI
   double* c = y + NI;         // NI (full second-derivative/2 array)
-  double* scr = c + NI;       // 2*NT
+  double* scr = c + NI;       // 64
   const double* R = nodes + static_cast<size_t>(row) * NI;
-  for (int i = threadIdx.x; i < NI; i += NT) {
+  for (int i = threadIdx.x; i < NI; i += RT) {
     const double v = R[i];
     y[i] = (v > 0) ? log2(v) : dev::kSmallLogVal;
   }
   __syncthreads();
   const int N = NI - 2;
-  const int E = (N + NT - 1) / NT;
+  const int E = (N + RT - 1) / RT;
   const int s0 = threadIdx.x * E;
   const int s1 = min(s0 + E, N);
   const double* ih = sd.ih;
@@ -235,16 +237,8 @@ k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
     Bv = a * Bv + gi;
     A = a * A;
   }
-  dev::block_affine_scan<NT>(A, Bv, scr);
-  double zin = 0.0;
-  {
-    // exclusive prefix: inclusive result of the previous thread
-    __syncthreads();
-    scr[threadIdx.x] = Bv;
-    __syncthreads();
-    zin = (threadIdx.x > 0) ? scr[threadIdx.x - 1] : 0.0;
-    __syncthreads();
-  }
+  // exclusive prefix: the previous thread's composed map at z = 0
+  const double zin = dev::block_affine_scan_w<RT>(A, Bv, scr);
   {
     double z = zin;
     for (int i = s0; i < s1; ++i) {
@@ -262,15 +256,7 @@ k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
     Bv = a * Bv + c[1 + i];
     A = a * A;
   }
-  dev::block_affine_rscan<NT>(A, Bv, scr);
-  double cin = 0.0;
-  {
-    __syncthreads();
-    scr[threadIdx.x] = Bv;
-    __syncthreads();
-    cin = (threadIdx.x + 1 < NT) ? scr[threadIdx.x + 1] : 0.0;
-    __syncthreads();
-  }
+  const double cin = dev::block_affine_rscan_w<RT>(A, Bv, scr);
   {
     double cn = cin;
     for (int i = s1 - 1; i >= s0; --i) {
@@ -286,7 +272,7 @@ k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
   __syncthreads();
   double* out = spl + static_cast<size_t>(row) * 4 * NI;
   const double* x = sd.x;
-  for (int i = threadIdx.x; i < NI - 1; i += NT) {
+  for (int i = threadIdx.x; i < NI - 1; i += RT) {
     const double dx = x[i + 1] - x[i];
     const double dy = y[i + 1] - y[i];
     out[i] = y[i];
@@ -2509,8 +2495,9 @@ void Engine1::reserve(unsigned P) {
   cuda_check(cudaFuncSetAttribute(k_rnodes1, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>((KMAX + 4 * KMAX + 3 * MAXTERMS) * sizeof(double))),
              "smem attribute");
-  cuda_check(cudaFuncSetAttribute(k_rspline1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>((2 * 8192 + 2 * NT) * sizeof(double))),
+  cuda_check(cudaFuncSetAttribute(k_rspline1<kSplineThreads>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>((2 * 8192 + 64) * sizeof(double))),
              "smem attribute");
   cuda_check(cudaMemset(ws_.nodes, 0, static_cast<size_t>(P) * B_ * 2 * NI * sizeof(double)), "memset");
 }
@@ -2567,8 +2554,8 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
   }
   mark(1);
   {
-    const size_t smem = (2 * static_cast<size_t>(NI) + 2 * NT) * sizeof(double);
-    k_rspline1<<<P * B * 2, NT, smem, st>>>(d_bsets_, B, NI, ws_.mstatus,
+    const size_t smem = (2 * static_cast<size_t>(NI) + 64) * sizeof(double);
+    k_rspline1<kSplineThreads><<<P * B * 2, kSplineThreads, smem, st>>>(d_bsets_, B, NI, ws_.mstatus,
                                             ws_.nodes, ws_.spl);
   }
   mark(2);
@@ -2890,7 +2877,7 @@ void Engine1::rgrid_host(int bs, const float* theta, unsigned npar, double* out)
   k_rnodes1<<<dim3((NI + 127) / 128, B * 2), 128,
               (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double), stream_>>>(
       d_bsets_, model_, B, NI, maxterms_, ws_.cnt, ws_.mstatus, ws_.nodes);
-  k_rspline1<<<B * 2, NT, (2 * static_cast<size_t>(NI) + 2 * NT) * sizeof(double), stream_>>>(
+  k_rspline1<kSplineThreads><<<B * 2, kSplineThreads, (2 * static_cast<size_t>(NI) + 64) * sizeof(double), stream_>>>(
       d_bsets_, B, NI, ws_.mstatus, ws_.nodes, ws_.spl);
   launch_rfill(tune_.rfill_per, dim3(ntile_, B), stream_, d_bsets_, B, n, NI, nc2,
                static_cast<int>(ntile_), ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
