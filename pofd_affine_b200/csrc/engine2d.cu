@@ -579,10 +579,14 @@ k_rfinal2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2, int edge,
   }
 }
 
-__device__ __forceinline__ double2 pval2(const double2* Rt, int nc, int n,
-                                         int i1, int i2, double r0,
-                                         const double* mo, double sf1,
-                                         double sf2) {
+// Exponent a = Re R~ - R~00 and phase (cos, sin) of the shifted imaginary
+// part at bin (i1, i2).
+struct PVal2 {
+  double a, c, s;
+};
+__device__ __forceinline__ PVal2 pval2(const double2* Rt, int nc, int n, int i1, int i2,
+                                       double r0, const double* mo, double sf1,
+                                       double sf2) {
   const double2 v = Rt[static_cast<size_t>(i1) * nc + i2];
   double ival = v.y;
   if (mo[6] != 0.0) {
@@ -591,18 +595,57 @@ __device__ __forceinline__ double2 pval2(const double2* Rt, int nc, int n,
     ival = ival - sp1;
   }
   if (mo[7] != 0.0) ival = ival - sf2 * static_cast<double>(i2);
-  const double e = exp(v.x - r0);
-  double s, c;
-  sincos(ival, &s, &c);
-  return make_double2(e * c, e * s);
+  PVal2 r;
+  r.a = v.x - r0;
+  sincos(ival, &r.s, &r.c);
+  return r;
+}
+
+// The self-conjugate columns (i2 = 0 and n/2, two of nc): the Hermitian
+// part p = (p(i1) + conj p(n - i1)) / 2, or the real part where the row is
+// its own mirror, times each dataset's noise factor.
+__device__ __forceinline__ void spectrum2_selfconj(const BSet2Dev& bs, const DSet2Dev* dsets,
+                                                int n, int nc, int i1, int i2,
+                                                const double2* Rt, double r0, const double* mo,
+                                                double sf1, double sf2, double sm1, double sm2,
+                                                double iflux1, double iflux2, double didx1,
+                                                double didx2, double2* out, size_t dstride) {
+  const PVal2 pv = pval2(Rt, nc, n, i1, i2, r0, mo, sf1, sf2);
+  // (a mirror at the origin would need i1 = 0 and i2 = 0: the origin itself)
+  const int j1 = (n - i1) % n;
+  const bool self = (j1 == i1);
+  PVal2 qv{0.0, 1.0, 0.0};
+  if (!self) qv = pval2(Rt, nc, n, j1, i2, r0, mo, sf1, sf2);
+  for (int dd = 0; dd < bs.nds; ++dd) {
+    const int d = bs.ds_begin + dd;
+    const DSet2Dev& ds = dsets[d];
+    const double s1 = sm1 * ds.sb1, s2 = sm2 * ds.sb2;
+    double nz = 0.0;
+    if (s1 > 0 || s2 > 0) {
+      const double sf1n = -0.5 * s1 * s1 * iflux1 * iflux1;
+      const double sf2n = -0.5 * s2 * s2 * iflux2 * iflux2;
+      nz = sf1n * didx1 * didx1 + sf2n * didx2 * didx2;
+    }
+    const double ep = exp(pv.a + nz);
+    double2 o;
+    if (self) {
+      o = make_double2(ep * pv.c, 0.0);
+    } else {
+      const double eq = exp(qv.a + nz);
+      o = make_double2(0.5 * (ep * pv.c + eq * qv.c), 0.5 * (ep * pv.s - eq * qv.s));
+    }
+    out[static_cast<size_t>(d) * dstride] = o;
+  }
 }
 
 // exp(R~ - R~00) with the shifts, the Hermitian part of the self-conjugate
 // columns (0 and n/2), then one noise product per dataset
-// (PDFactoryDouble.cc:1241-1342, 1383-1437).  Bins where every dataset's
-// noise exponent is below -750 are exactly 0 in the reference and are
-// written as 0 directly.
-__global__ void __launch_bounds__(NT)
+// (PDFactoryDouble.cc:1241-1342, 1383-1437).  The noise exponent of a
+// dataset is added to the exponent of exp(R~ - R~00) -- one exp per bin and
+// dataset for the reference's two, the same product rounded once.  Bins
+// where every dataset's noise exponent is below -750 are exactly 0 in the
+// reference and are written as 0 directly.
+__global__ void __launch_bounds__(NT, 5)
 k_spectrum2(const BSet2Dev* __restrict__ bsets,
             const DSet2Dev* __restrict__ dsets, int B, int D, int n, int nc,
             const int* __restrict__ mstatus, const double* __restrict__ sigmult,
@@ -629,50 +672,39 @@ k_spectrum2(const BSet2Dev* __restrict__ bsets,
     const double sf2 = -0.5 * s2 * s2 * iflux2 * iflux2;
     if (!(sf1 * didx1 * didx1 + sf2 * didx2 * didx2 < -750.0)) all_zero = false;
   }
+  double2* out0 = reinterpret_cast<double2*>(pbuf) + static_cast<size_t>(w) * D * n * nc;
   if (all_zero) {
     for (int dd = 0; dd < bs.nds; ++dd)
-      reinterpret_cast<double2*>(pbuf + (static_cast<size_t>(w) * D + bs.ds_begin + dd) * n * 2 * nc)[e] =
-          make_double2(0.0, 0.0);
+      out0[static_cast<size_t>(bs.ds_begin + dd) * n * nc + e] = make_double2(0.0, 0.0);
     return;
   }
   const double2* Rt = reinterpret_cast<const double2*>(rbuf + static_cast<size_t>(wb) * n * 2 * nc);
   const double* mo = mom + static_cast<size_t>(wb) * 8;
   const double r0 = Rt[0].x;
   const double sf1 = mo[4] * iflux1, sf2 = mo[5] * iflux2;
-  double2 p;
   if (i1 == 0 && i2 == 0) {
-    p = make_double2(1.0, 0.0);
-  } else {
-    p = pval2(Rt, nc, n, i1, i2, r0, mo, sf1, sf2);
-    if (i2 == 0 || ((n & 1) == 0 && i2 == n / 2)) {
-      const int j1 = (n - i1) % n;
-      if (j1 == i1) {
-        p.y = 0.0;
-      } else {
-        double2 q;
-        if (j1 == 0 && i2 == 0) q = make_double2(1.0, 0.0);
-        else q = pval2(Rt, nc, n, j1, i2, r0, mo, sf1, sf2);
-        p = make_double2(0.5 * (p.x + q.x), 0.5 * (p.y - q.y));
-      }
-    }
+    for (int dd = 0; dd < bs.nds; ++dd)
+      out0[static_cast<size_t>(bs.ds_begin + dd) * n * nc + e] = make_double2(1.0, 0.0);
+    return;
   }
+  if (i2 == 0 || ((n & 1) == 0 && i2 == n / 2)) {
+    spectrum2_selfconj(bs, dsets, n, nc, i1, i2, Rt, r0, mo, sf1, sf2, sm1, sm2, iflux1,
+                       iflux2, didx1, didx2, out0 + e, static_cast<size_t>(n) * nc);
+    return;
+  }
+  const PVal2 pv = pval2(Rt, nc, n, i1, i2, r0, mo, sf1, sf2);
   for (int dd = 0; dd < bs.nds; ++dd) {
     const int d = bs.ds_begin + dd;
     const DSet2Dev& ds = dsets[d];
     const double s1 = sm1 * ds.sb1, s2 = sm2 * ds.sb2;
-    double2 o = p;
+    double nz = 0.0;
     if (s1 > 0 || s2 > 0) {
-      if (i1 == 0 && i2 == 0) {
-        o = make_double2(1.0, 0.0);
-      } else {
-        const double sf1n = -0.5 * s1 * s1 * iflux1 * iflux1;
-        const double sf2n = -0.5 * s2 * s2 * iflux2 * iflux2;
-        const double sp1 = sf1n * didx1 * didx1;
-        const double ef = exp(sp1 + sf2n * didx2 * didx2);
-        o = make_double2(ef * p.x, ef * p.y);
-      }
+      const double sf1n = -0.5 * s1 * s1 * iflux1 * iflux1;
+      const double sf2n = -0.5 * s2 * s2 * iflux2 * iflux2;
+      nz = sf1n * didx1 * didx1 + sf2n * didx2 * didx2;
     }
-    reinterpret_cast<double2*>(pbuf + (static_cast<size_t>(w) * D + d) * n * 2 * nc)[e] = o;
+    const double ep = exp(pv.a + nz);
+    out0[static_cast<size_t>(d) * n * nc + e] = make_double2(ep * pv.c, ep * pv.s);
   }
 }
 
