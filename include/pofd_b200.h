@@ -295,6 +295,19 @@ int pofd_like2_profile(pofd_like2* L, unsigned nprop, const float* theta,
                        unsigned npar, int reps, double* stage_ms,
                        int* nstages);
 const char* pofd_like2_stage_name(int i);
+/* Stage names of the FFT mode in use (they differ from the above in
+ * mode 1). */
+const char* pofd_like2_stage_name_now(const pofd_like2* L, int i);
+
+/* FFT of the 2D likelihood (the project's own choice; the reference plans
+ * FFTW 2D transforms, PDFactoryDouble.cc:727-768): mode 1 (default) runs
+ * batched 1D cuFFT transforms along the rows and this library's kernel that
+ * transforms the columns, applies exp/shift/noise per bin and transforms the
+ * columns back, where n is a power of two in [512, 4096] (else mode 0);
+ * mode 0 runs batched 2D cuFFT transforms with the spectrum kernel between
+ * them.  fft_info reports whether the fused column path is in use. */
+int pofd_like2_set_fft(pofd_like2* L, int mode);
+int pofd_like2_fft_info(const pofd_like2* L, int* fused);
 
 /* Priors per band (band 0 or 1), added once to the summed log-likelihood in
  * the reference's order (calcLikeDouble.cc:1236-1276): Gaussians on the

@@ -93,6 +93,9 @@ SIGNATURES = {
     "pofd_like2_kernels_per_eval": (I, [V, C.POINTER(I)]),
     "pofd_like2_profile": (I, [V, U, _fp, U, I, _dp, C.POINTER(I)]),
     "pofd_like2_stage_name": (C.c_char_p, [I]),
+    "pofd_like2_stage_name_now": (C.c_char_p, [V, I]),
+    "pofd_like2_set_fft": (I, [V, I]),
+    "pofd_like2_fft_info": (I, [V, C.POINTER(I)]),
     "pofd_pd1_loglike_noalloc": (I, [V, U, D, D, U, D, D, V, V, U, D, D, D, D,
                                      V, V, V]),
     "pofd_ensemble_create": (I, [V, U, U, D, C.c_ulonglong, PV]),

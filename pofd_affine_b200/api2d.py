@@ -256,8 +256,21 @@ class calcLikeDouble:
         ns = C.c_int()
         check(lib().pofd_like2_profile(self.h, nprop, th.ravel(), npar,
                                        int(reps), ms, C.byref(ns)))
-        return {lib().pofd_like2_stage_name(i).decode(): ms[i]
+        return {lib().pofd_like2_stage_name_now(self.h, i).decode(): ms[i]
                 for i in range(ns.value)}
+
+    def setFFT(self, mode):
+        """1: 1D cuFFT row transforms around the library's fused column
+        transform + spectrum kernel (default, n a power of two in
+        [512, 4096]); 0: 2D cuFFT transforms with the spectrum kernel between
+        them."""
+        check(lib().pofd_like2_set_fft(self.h, int(mode)))
+
+    def fusedColumns(self):
+        """True when the fused column path is the one in use."""
+        k = C.c_int()
+        check(lib().pofd_like2_fft_info(self.h, C.byref(k)))
+        return bool(k.value)
 
     def kernelsPerEval(self):
         k = C.c_int()

@@ -806,6 +806,26 @@ int pofd_like2_profile(pofd_like2* L, unsigned nprop, const float* theta,
 
 const char* pofd_like2_stage_name(int i) { return pofd::Engine2::stage_name(i); }
 
+const char* pofd_like2_stage_name_now(const pofd_like2* L, int i) {
+  return (L && L->eng) ? L->eng->stage_name_now(i) : "";
+}
+
+int pofd_like2_set_fft(pofd_like2* L, int mode) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_fft_mode(mode);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_fft_info(const pofd_like2* L, int* fused) {
+  return guard([&] {
+    need(L && fused, "null argument");
+    *fused = L->eng->colspec() ? 1 : 0;
+    return POFD_OK;
+  });
+}
+
 // ------------------------------------------------------------- ensemble
 static int like1_batch(void* like, unsigned nprop, const float* theta,
                        unsigned npar, double* logl, int* status, void* stream) {

@@ -27,6 +27,7 @@
 #include <sstream>
 
 #include "common.cuh"
+#include "fft1d.cuh"
 
 namespace pofd {
 
@@ -1109,6 +1110,278 @@ __global__ void k_reduce2(const BSet2Dev* __restrict__ bsets,
 // an invalid model; the penalty is differenceRegularize of the band-1 knots
 // (numberCountsDoubleLogNormal.cc:2154-2173) before the factor alpha.
 // fill_at >= 0 stores the four integrals as floats at theta[w][fill_at..].
+// ------------------------------------------------------------------
+// Column transforms fused with the spectrum (FFT mode 1).  After batched 1D
+// row transforms of the R grid (cuFFT D2Z on its n rows), the row-
+// transformed grid Y[i1][i2] (n x nc, row stride nc) goes down its columns
+// here: each block takes C = 256 / M adjacent columns (M = n / 16 threads
+// per column) into shared memory, runs the forward n-point DFT of every
+// column, forms per bin exp(R~ - R~00) with the shifts and one dataset's
+// noise (the work of k_spectrum2, same formulas), runs the inverse column
+// DFT and writes the columns of that dataset's half spectrum, which batched
+// 1D Z2D row transforms then take to the P(D).  So the spectrum costs no
+// HBM round trip of its own and the column passes of both 2D transforms
+// read and write the grid once.
+//
+// Column DFT, n = 16 M, M = 16 M3 (n in [512, 4096]): with n = n1 M + u,
+// u = m M3 + s and k = k1 + 16 (k2 + 16 k3),
+//   stage 1: 16-point register DFTs over n1, times W_n^{u k1};
+//   stage 2: 16-point register DFTs over m, times W_M^{s k2};
+//   stage 3: M3-point register DFTs over s.
+// The forward output stays in the stage-3 slots, position
+// (16 k1 + k2)(M3 + 1) + k3 (a padded stride, free of bank conflicts); the
+// spectrum works slot by slot, and the inverse runs the transposed stages
+// in reverse order (M3-point DFTs over k3, twiddle W_M^{-s k2}, 16-point
+// DFTs over k2, twiddle W_n^{-u k1}, 16-point DFTs over k1), which read
+// those slots and end in natural order.  Twiddles W_n^j, j < n, come from
+// two shared tables H[j >> 5] L[j & 31] built on the host in long double.
+constexpr int CS_THREADS = 256;
+
+__host__ __device__ constexpr int cs_m3(int n) { return n / 256; }
+__host__ __device__ constexpr int cs_slots(int n) { return 256 * (n / 256 + 1); }
+inline size_t colspec_smem(int n) {
+  const int C = CS_THREADS / (n / 16);
+  return (static_cast<size_t>(C) * cs_slots(n) + n / 32 + 32) * sizeof(double2);
+}
+
+template <int S>
+__device__ __forceinline__ double2 cs_tw(const double2* H, const double2* L, int j) {
+  const double2 h = H[j >> 5];
+  const int lo = j & 31;
+  const double2 w = lo ? fft::cmul(h, L[lo]) : h;
+  return (S < 0) ? w : make_double2(w.x, -w.y);
+}
+
+// forward column DFT of the C columns in buf (natural order in, stage-3
+// slots out)
+template <int N>
+__device__ __forceinline__ void cs_forward(double2* buf, const double2* H, const double2* L,
+                                           int c, int u) {
+  constexpr int M = N / 16, M3 = N / 256, SL = cs_slots(N), PP = 16 / M3;
+  double2* b = buf + c * SL;
+  double2 v[16];
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) v[n1] = b[n1 * M + u];
+  fft::dft<16, -1>(v);
+#pragma unroll
+  for (int k1 = 1; k1 < 16; ++k1)
+    if (u) v[k1] = fft::cmul(v[k1], cs_tw<-1>(H, L, u * k1));
+  __syncthreads();
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1) b[k1 * M + u] = v[k1];
+  __syncthreads();
+  {
+    const int k1 = u / M3, s = u % M3;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = b[k1 * M + m * M3 + s];
+    fft::dft<16, -1>(v);
+#pragma unroll
+    for (int k2 = 1; k2 < 16; ++k2)
+      if (s) v[k2] = fft::cmul(v[k2], cs_tw<-1>(H, L, 16 * s * k2));
+    __syncthreads();
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) b[(k1 * 16 + k2) * (M3 + 1) + s] = v[k2];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int pp = 0; pp < PP; ++pp) {
+    const int pr = pp * M + u;
+    double2 z[M3];
+#pragma unroll
+    for (int s2 = 0; s2 < M3; ++s2) z[s2] = b[pr * (M3 + 1) + s2];
+    fft::dft<M3, -1>(z);
+#pragma unroll
+    for (int k3 = 0; k3 < M3; ++k3) b[pr * (M3 + 1) + k3] = z[k3];
+  }
+  __syncthreads();
+}
+
+// inverse column DFT: stage-3 slots in, natural order out (into b[i1])
+template <int N>
+__device__ __forceinline__ void cs_inverse(double2* buf, const double2* H, const double2* L,
+                                           int c, int u) {
+  constexpr int M = N / 16, M3 = N / 256, SL = cs_slots(N), PP = 16 / M3;
+  double2* b = buf + c * SL;
+#pragma unroll
+  for (int pp = 0; pp < PP; ++pp) {
+    const int pr = pp * M + u;
+    const int k2 = pr & 15;
+    double2 z[M3];
+#pragma unroll
+    for (int k3 = 0; k3 < M3; ++k3) z[k3] = b[pr * (M3 + 1) + k3];
+    fft::dft<M3, 1>(z);
+#pragma unroll
+    for (int s2 = 0; s2 < M3; ++s2)
+      b[pr * (M3 + 1) + s2] = (s2 * k2) ? fft::cmul(z[s2], cs_tw<1>(H, L, 16 * s2 * k2)) : z[s2];
+  }
+  __syncthreads();
+  double2 v[16];
+  {
+    const int k1 = u / M3, s = u % M3;
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) v[k2] = b[(k1 * 16 + k2) * (M3 + 1) + s];
+    fft::dft<16, 1>(v);
+    __syncthreads();
+    // Z_{k1}[m M3 + s], times W_n^{-u' k1} for u' = m M3 + s
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int up = m * M3 + s;
+      b[k1 * M + up] = (up * k1) ? fft::cmul(v[m], cs_tw<1>(H, L, up * k1)) : v[m];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1) v[k1] = b[k1 * M + u];
+  fft::dft<16, 1>(v);
+  __syncthreads();
+#pragma unroll
+  for (int n1 = 0; n1 < 16; ++n1) b[n1 * M + u] = v[n1];
+  __syncthreads();
+}
+
+// Sum of the row-transformed grid's column 0 over the rows: R~00 (the DC
+// bin of the 2D transform), one block per (proposal, beam set).
+__global__ void __launch_bounds__(NT)
+k_r0sum2(int n, int nc, const int* __restrict__ mstatus, int B,
+         const double* __restrict__ rbuf, double* __restrict__ r0) {
+  __shared__ double shr[32];
+  const int wb = blockIdx.x;
+  if (mstatus[wb / B] != 0) return;
+  const double2* Y = reinterpret_cast<const double2*>(rbuf) + static_cast<size_t>(wb) * n * nc;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += NT) acc += Y[static_cast<size_t>(i) * nc].x;
+  acc = dev::block_sum<NT>(acc, shr);
+  if (threadIdx.x == 0) r0[wb] = acc;
+}
+
+template <int N>
+__global__ void __launch_bounds__(CS_THREADS, 2)
+k_colspec2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dsets, int B,
+           int D, const int* __restrict__ mstatus, const double* __restrict__ sigmult,
+           const double* __restrict__ mom, const double* __restrict__ r0buf,
+           const double* __restrict__ rbuf, double* __restrict__ pbuf,
+           const double2* __restrict__ WH, const double2* __restrict__ WL) {
+  constexpr int M = N / 16, M3 = N / 256, SL = cs_slots(N);
+  constexpr int C = CS_THREADS / M;
+  constexpr int nc = N / 2 + 1;
+  extern __shared__ double2 csm[];
+  double2* buf = csm;                 // [C][SL]
+  double2* Hs = csm + C * SL;         // N / 32
+  double2* Ls = Hs + N / 32;          // 32
+  const int wb = blockIdx.y;
+  const int w = wb / B, bsi = wb - w * B;
+  if (mstatus[w] != 0) return;
+  const int t = threadIdx.x;
+  for (int i = t; i < N / 32 + 32; i += CS_THREADS)
+    Hs[i] = (i < N / 32) ? WH[i] : WL[i - N / 32];
+  const int c0 = blockIdx.x * C;      // first column of the block
+  const int c = t / M, u = t % M;
+  const BSet2Dev& bs = bsets[bsi];
+  const double2* Y = reinterpret_cast<const double2*>(rbuf) + static_cast<size_t>(wb) * N * nc;
+  const double iflux1 = dev::kTwoPi / (static_cast<double>(N) * bs.dflux1);
+  const double iflux2 = dev::kTwoPi / (static_cast<double>(N) * bs.dflux2);
+  const double sm1 = sigmult[2 * w], sm2 = sigmult[2 * w + 1];
+  const double* mo = mom + static_cast<size_t>(wb) * 8;
+  const double r0 = r0buf[wb];
+  const double sf1 = mo[4] * iflux1, sf2 = mo[5] * iflux2;
+  const bool sh1 = mo[6] != 0.0, sh2 = mo[7] != 0.0;
+  for (int dd = 0; dd < bs.nds; ++dd) {
+    const int d = bs.ds_begin + dd;
+    const DSet2Dev& ds = dsets[d];
+    // load the C columns (a warp covers 32 / C rows of C adjacent columns)
+    for (int e = t; e < C * N; e += CS_THREADS) {
+      const int i1 = e / C, cc = e % C;
+      const int i2 = c0 + cc;
+      buf[cc * SL + i1] = (i2 < nc) ? Y[static_cast<size_t>(i1) * nc + i2] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    cs_forward<N>(buf, Hs, Ls, c, u);
+    // spectrum, slot by slot and in place; the self-conjugate columns
+    // (i2 = 0 and n/2) go by mirror pairs (i1, n - i1), each pair owned by
+    // one thread: their Hermitian parts are conjugates of each other
+    const double s1 = sm1 * ds.sb1, s2 = sm2 * ds.sb2;
+    const bool noisy = (s1 > 0 || s2 > 0);
+    const double sf1n = -0.5 * s1 * s1 * iflux1 * iflux1;
+    const double sf2n = -0.5 * s2 * s2 * iflux2 * iflux2;
+#pragma unroll 1
+    for (int q = t; q < C * SL; q += CS_THREADS) {
+      const int cc = q / SL, pos = q % SL;
+      const int pr = pos / (M3 + 1), k3 = pos % (M3 + 1);
+      const int i2 = c0 + cc;
+      if (k3 == M3 || i2 >= nc || i2 == 0 || i2 == N / 2) continue;
+      const int i1 = (pr >> 4) + 16 * ((pr & 15) + 16 * k3);
+      const double didx1 = (i1 < nc) ? static_cast<double>(i1) : static_cast<double>(N - i1);
+      const double didx2 = static_cast<double>(i2);
+      const double nz = noisy ? sf1n * didx1 * didx1 + sf2n * didx2 * didx2 : 0.0;
+      if (noisy && nz < -750.0) {  // exactly 0 in the reference
+        buf[q] = make_double2(0.0, 0.0);
+        continue;
+      }
+      const double2 X = buf[q];
+      double ival = X.y;
+      if (sh1) ival -= (i1 < nc) ? sf1 * static_cast<double>(i1) : -sf1 * static_cast<double>(N - i1);
+      if (sh2) ival -= sf2 * static_cast<double>(i2);
+      double sn, cs;
+      sincos(ival, &sn, &cs);
+      const double ep = exp((X.x - r0) + nz);
+      buf[q] = make_double2(ep * cs, ep * sn);
+    }
+    for (int cc = 0; cc < C; ++cc) {
+      const int i2 = c0 + cc;
+      if (i2 != 0 && i2 != N / 2) continue;
+      double2* b = buf + cc * SL;
+      const double didx2 = static_cast<double>(i2);
+#pragma unroll 1
+      for (int i1 = t; i1 <= N / 2; i1 += CS_THREADS) {
+        const int j1 = (N - i1) % N;
+        const int si = ((i1 & 15) * 16 + ((i1 >> 4) & 15)) * (M3 + 1) + (i1 >> 8);
+        const int sj = ((j1 & 15) * 16 + ((j1 >> 4) & 15)) * (M3 + 1) + (j1 >> 8);
+        if (i1 == 0 && i2 == 0) {
+          b[si] = make_double2(1.0, 0.0);
+          continue;
+        }
+        const double didx1 = static_cast<double>(i1);
+        const double nz = noisy ? sf1n * didx1 * didx1 + sf2n * didx2 * didx2 : 0.0;
+        if (noisy && nz < -750.0) {
+          b[si] = make_double2(0.0, 0.0);
+          if (j1 != i1) b[sj] = make_double2(0.0, 0.0);
+          continue;
+        }
+        const double2 X = b[si];
+        double ival = X.y;
+        if (sh1) ival -= sf1 * static_cast<double>(i1);
+        if (sh2) ival -= sf2 * didx2;
+        double sn, cs;
+        sincos(ival, &sn, &cs);
+        const double ep = exp((X.x - r0) + nz);
+        if (j1 == i1) {
+          b[si] = make_double2(ep * cs, 0.0);
+        } else {
+          const double2 Xq = b[sj];
+          double iq = Xq.y;
+          if (sh1) iq -= -sf1 * static_cast<double>(N - j1);
+          if (sh2) iq -= sf2 * didx2;
+          double sq, cq;
+          sincos(iq, &sq, &cq);
+          const double eq = exp((Xq.x - r0) + nz);
+          const double2 o = make_double2(0.5 * (ep * cs + eq * cq), 0.5 * (ep * sn - eq * sq));
+          b[si] = o;
+          b[sj] = make_double2(o.x, -o.y);
+        }
+      }
+    }
+    __syncthreads();
+    cs_inverse<N>(buf, Hs, Ls, c, u);
+    double2* Pd = reinterpret_cast<double2*>(pbuf) + (static_cast<size_t>(w) * D + d) * N * nc;
+    for (int e = t; e < C * N; e += CS_THREADS) {
+      const int i1 = e / C, cc = e % C;
+      const int i2 = c0 + cc;
+      if (i2 < nc) Pd[static_cast<size_t>(i1) * nc + i2] = buf[cc * SL + i1];
+    }
+    __syncthreads();
+  }
+}
+
 constexpr int kBonus2Threads = 256;
 __global__ void __launch_bounds__(kBonus2Threads)
 k_bonus2(Model2Dev m, float* theta, int npar, double logfac,
@@ -1406,6 +1679,9 @@ void Engine2::free_static() {
   static_allocs_.clear();
   d_bsets_ = nullptr;
   d_dsets_ = nullptr;
+  d_cwh_ = nullptr;
+  d_cwl_ = nullptr;
+  colspec_ = false;
   static_ok_ = false;
 }
 
@@ -1605,12 +1881,8 @@ void Engine2::build_static() {
   nct_ = (n + NT - 1) / NT;
   gchunks_ = (maxnnz + GCH - 1) / GCH;
   static_ok_ = true;
-  drop_graphs();
-  for (auto& kv : plans_) {
-    if (kv.second.fwd) { fftwork_.forget(kv.second.fwd); cufftDestroy(kv.second.fwd); }
-    if (kv.second.inv) { fftwork_.forget(kv.second.inv); cufftDestroy(kv.second.inv); }
-  }
-  plans_.clear();
+  drop_plans();
+  setup_colspec();
   const unsigned P = ws_.P;
   free_work();
   if (P) reserve(P);
@@ -1621,7 +1893,7 @@ void Engine2::free_work() {
                   ws_.rpart, ws_.redge, ws_.epart, ws_.fpart, ws_.mom, ws_.pbuf, ws_.rowpart,
                   ws_.colpart, ws_.pinfo, ws_.gpart, ws_.pdout,
                   ws_.theta_in, ws_.logl, ws_.status, ws_.bonus, ws_.bcnt,
-                  ws_.bstatus, ws_.bsig};
+                  ws_.bstatus, ws_.bsig, ws_.r0};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
@@ -1661,6 +1933,7 @@ void Engine2::reserve(unsigned P) {
   const size_t ngr = edge_ ? (nedge_ + ER - 1) / ER : 0;
   ws_.epart = dal<double>(static_cast<size_t>(P) * B_ * (ngr ? ngr * (n + nedge_) : 1));
   ws_.mom = dal<double>(static_cast<size_t>(P) * B_ * 8);
+  ws_.r0 = dal<double>(static_cast<size_t>(P) * B_);
   ws_.fpart = dal<double>(static_cast<size_t>(P) * B_ * ((n + NT - 1) / NT) * 4);
   ws_.pbuf = dal<double>(static_cast<size_t>(P) * D_ * n * nc2);
   ws_.rowpart = dal<double>(static_cast<size_t>(P) * D_ * n * nct_);
@@ -1679,12 +1952,77 @@ void Engine2::reserve(unsigned P) {
                           static_cast<int>(3 * 8192 * sizeof(double))), "attr");
 }
 
+// Twiddle tables and kernel attributes of FFT mode 1 where the size allows.
+void Engine2::setup_colspec() {
+  const unsigned n = n_;
+  colspec_ = fft_mode_ == 1 && (n == 512 || n == 1024 || n == 2048 || n == 4096);
+  if (!colspec_) return;
+  if (!d_cwh_) {
+    std::vector<double2> wh(n / 32), wl(32);
+    const long double tau = 6.283185307179586476925286766559005768L;
+    for (unsigned h = 0; h < n / 32; ++h) {
+      const long double a = -tau * static_cast<long double>(32 * h) / static_cast<long double>(n);
+      wh[h] = make_double2(static_cast<double>(cosl(a)), static_cast<double>(sinl(a)));
+    }
+    for (unsigned l = 0; l < 32; ++l) {
+      const long double a = -tau * static_cast<long double>(l) / static_cast<long double>(n);
+      wl[l] = make_double2(static_cast<double>(cosl(a)), static_cast<double>(sinl(a)));
+    }
+    d_cwh_ = dal<double2>(wh.size());
+    d_cwl_ = dal<double2>(wl.size());
+    static_allocs_.push_back(d_cwh_);
+    static_allocs_.push_back(d_cwl_);
+    ck(cudaMemcpy(d_cwh_, wh.data(), wh.size() * sizeof(double2), cudaMemcpyHostToDevice), "upload");
+    ck(cudaMemcpy(d_cwl_, wl.data(), wl.size() * sizeof(double2), cudaMemcpyHostToDevice), "upload");
+  }
+  const int sm = static_cast<int>(colspec_smem(static_cast<int>(n)));
+  switch (n) {
+    case 512: ck(cudaFuncSetAttribute(k_colspec2<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr"); break;
+    case 1024: ck(cudaFuncSetAttribute(k_colspec2<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr"); break;
+    case 2048: ck(cudaFuncSetAttribute(k_colspec2<2048>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr"); break;
+    default: ck(cudaFuncSetAttribute(k_colspec2<4096>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr"); break;
+  }
+}
+
+void Engine2::drop_plans() {
+  drop_graphs();
+  for (auto& kv : plans_) {
+    if (kv.second.fwd) { fftwork_.forget(kv.second.fwd); cufftDestroy(kv.second.fwd); }
+    if (kv.second.inv) { fftwork_.forget(kv.second.inv); cufftDestroy(kv.second.inv); }
+  }
+  plans_.clear();
+}
+
+void Engine2::set_fft_mode(int mode) {
+  if (mode != 0 && mode != 1) throw Error(POFD_E_ARG, "2D FFT mode must be 0 or 1");
+  if (mode == fft_mode_) return;
+  fft_mode_ = mode;
+  if (device_ >= 0) ck(cudaSetDevice(device_), "cudaSetDevice");
+  drop_plans();
+  if (static_ok_) setup_colspec();
+  else colspec_ = false;
+}
+
 void Engine2::ensure_plans(unsigned nprop) {
   auto it = plans_.find(nprop);
   if (it != plans_.end() && it->second.fwd) return;
   Plans pl;
   int nn[2] = {static_cast<int>(n_), static_cast<int>(n_)};
   const int nc = static_cast<int>(n_) / 2 + 1;
+  if (colspec_) {
+    // 1D row transforms of every (proposal, beam set) or (proposal, dataset)
+    // grid: n rows each, padded real rows of 2 nc doubles / nc complex
+    int n1[1] = {nn[0]};
+    int ie[1] = {2 * nc}, oe[1] = {nc};
+    bool grew = fftwork_.make(&pl.fwd, 1, n1, ie, 2 * nc, oe, nc, CUFFT_D2Z,
+                              static_cast<int>(nprop * B_ * n_));
+    int ie2[1] = {nc}, oe2[1] = {2 * nc};
+    grew |= fftwork_.make(&pl.inv, 1, n1, ie2, nc, oe2, 2 * nc, CUFFT_Z2D,
+                          static_cast<int>(nprop * D_ * n_));
+    if (grew) drop_graphs();
+    plans_[nprop] = pl;
+    return;
+  }
   int inemb[2] = {nn[0], 2 * nc}, onemb[2] = {nn[0], nc};
   bool grew = fftwork_.make(&pl.fwd, 2, nn, inemb, nn[0] * 2 * nc, onemb, nn[0] * nc,
                             CUFFT_D2Z, static_cast<int>(nprop * B_));
@@ -1747,16 +2085,35 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
     return;
   }
   fk(cufftSetStream(pl.fwd, st), "cufftSetStream");
-  fk(cufftExecD2Z(pl.fwd, ws_.rbuf, reinterpret_cast<cufftDoubleComplex*>(ws_.rbuf)), "cufftExecD2Z 2D");
+  fk(cufftExecD2Z(pl.fwd, ws_.rbuf, reinterpret_cast<cufftDoubleComplex*>(ws_.rbuf)),
+     colspec_ ? "cufftExecD2Z rows" : "cufftExecD2Z 2D");
   mark(6);
-  {
+  if (colspec_) {
+    k_r0sum2<<<P * B, NT, 0, st>>>(n, nc, ws_.mstatus, B, ws_.rbuf, ws_.r0);
+    const int C = CS_THREADS / (n / 16);
+    const dim3 g((nc + C - 1) / C, P * B);
+    const size_t sm = colspec_smem(n);
+#define POFD_CS(NN)                                                                        \
+  k_colspec2<NN><<<g, CS_THREADS, sm, st>>>(d_bsets_, d_dsets_, B, D, ws_.mstatus,          \
+                                             ws_.sigmult, ws_.mom, ws_.r0, ws_.rbuf, ws_.pbuf, \
+                                             d_cwh_, d_cwl_)
+    switch (n) {
+      case 512: POFD_CS(512); break;
+      case 1024: POFD_CS(1024); break;
+      case 2048: POFD_CS(2048); break;
+      case 4096: POFD_CS(4096); break;
+      default: throw Error(POFD_E_ARG, "column transform: unsupported size");
+    }
+#undef POFD_CS
+  } else {
     const unsigned gs = static_cast<unsigned>((static_cast<size_t>(n) * nc + NT - 1) / NT);
     k_spectrum2<<<dim3(gs, P * B), NT, 0, st>>>(d_bsets_, d_dsets_, B, D, n, nc, ws_.mstatus,
                                                 ws_.sigmult, ws_.mom, ws_.rbuf, ws_.pbuf);
   }
   mark(7);
   fk(cufftSetStream(pl.inv, st), "cufftSetStream");
-  fk(cufftExecZ2D(pl.inv, reinterpret_cast<cufftDoubleComplex*>(ws_.pbuf), ws_.pbuf), "cufftExecZ2D 2D");
+  fk(cufftExecZ2D(pl.inv, reinterpret_cast<cufftDoubleComplex*>(ws_.pbuf), ws_.pbuf),
+     colspec_ ? "cufftExecZ2D rows" : "cufftExecZ2D 2D");
   mark(8);
   k_pscan2<<<dim3(nct_, nrt_, P * D), NT, 0, st>>>(D, n, nc2, ws_.mstatus, ws_.pbuf,
                                                     ws_.rowpart, ws_.colpart);
@@ -2028,6 +2385,15 @@ const char* Engine2::stage_name(int i) {
       "k_model2", "k_rows2", "k_rgrid2", "k_redge2+k_ry2", "k_rfinish2+k_rfinal2",
       "cufft_d2z_2d", "k_spectrum2", "cufft_z2d_2d", "k_pscan2", "k_psplit2",
       "k_pgather2", "k_reduce2"};
+  return (i >= 0 && i < kNumStages) ? names[i] : "";
+}
+
+const char* Engine2::stage_name_now(int i) const {
+  static const char* names[kNumStages] = {
+      "k_model2", "k_rows2", "k_rgrid2", "k_redge2+k_ry2", "k_rfinish2+k_rfinal2",
+      "cufft_d2z_rows", "k_r0sum2+k_colspec2", "cufft_z2d_rows", "k_pscan2", "k_psplit2",
+      "k_pgather2", "k_reduce2"};
+  if (!colspec_) return stage_name(i);
   return (i >= 0 && i < kNumStages) ? names[i] : "";
 }
 

@@ -128,7 +128,22 @@ class Engine2 {
   void profile_stages(unsigned nprop, const float* theta, unsigned npar,
                       int reps, double* stage_ms);
   static const char* stage_name(int i);
-  int kernels_per_eval() const { return (edge_ ? 12 : 10) + (prior_.needs_bonus() ? 1 : 0); }
+  // the stage names of the FFT mode in use
+  const char* stage_name_now(int i) const;
+  int kernels_per_eval() const {
+    return (edge_ ? 12 : 10) + (colspec_ ? 1 : 0) + (prior_.needs_bonus() ? 1 : 0);
+  }
+  // 0: batched 2D cuFFT transforms with k_spectrum2 between them; 1: batched
+  // 1D cuFFT row transforms around this library's fused column-transform +
+  // spectrum kernel (k_colspec2), where n is a power of two in [512, 4096]
+  // (mode 0 otherwise).
+  void set_fft_mode(int mode);
+  int fft_mode() const { return fft_mode_; }
+  // the fused column path is (or, before the first evaluation, will be) used
+  bool colspec() const {
+    if (static_ok_) return colspec_;
+    return fft_mode_ == 1 && (n_ == 512 || n_ == 1024 || n_ == 2048 || n_ == 4096);
+  }
   // priors per band (calcLikeDouble::setSigmaPrior1/2, setCFIRBPrior1/2,
   // setPoissonPrior1/2 and unset forms, setRegularizationAlpha,
   // calcLikeDouble.h:310-341)
@@ -205,6 +220,12 @@ class Engine2 {
   unsigned gchunks_ = 1;          // gather chunks per dataset
   std::map<unsigned, Plans> plans_;
   FftWorkArea fftwork_;
+  void setup_colspec();
+  void drop_plans();
+  int fft_mode_ = 1;
+  bool colspec_ = false;
+  double2* d_cwh_ = nullptr;  // e^{-2 pi i 32 h / n}, h < n / 32
+  double2* d_cwl_ = nullptr;  // e^{-2 pi i l / n}, l < 32
   Prior2 prior_;
   const double* d_qu_ = nullptr;
   const double* d_qs_ = nullptr;
@@ -222,6 +243,7 @@ class Engine2 {
     double* redge = nullptr;    // [P][B][2n+1]: Ry at [n, 2n)
     double* epart = nullptr;    // [P][B][edge row groups][n + nedge]
     double* mom = nullptr;      // [P][B][8]
+    double* r0 = nullptr;       // [P][B] R~00 (FFT mode 1)
     double* fpart = nullptr;    // [P][B][n/256][4] edge-cell moment partials
     double* pbuf = nullptr;     // [P][D][n][2nc]
     double* rowpart = nullptr;  // [P][D][n][nct]
