@@ -1303,7 +1303,7 @@ k_colspec2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dset
     const bool noisy = (s1 > 0 || s2 > 0);
     const double sf1n = -0.5 * s1 * s1 * iflux1 * iflux1;
     const double sf2n = -0.5 * s2 * s2 * iflux2 * iflux2;
-#pragma unroll 1
+#pragma unroll 4
     for (int q = t; q < C * SL; q += CS_THREADS) {
       const int cc = q / SL, pos = q % SL;
       const int pr = pos / (M3 + 1), k3 = pos % (M3 + 1);
