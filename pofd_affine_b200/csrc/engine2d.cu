@@ -325,12 +325,21 @@ __device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
   const double* L = fs ? s_neg : s_pos;
   const int cnt = fs ? nneg : npos;
   const double lf2 = bs.collog[j];
-  double wv = 0.0;
-  for (int k = 0; k < cnt; ++k) {
-    const double tfac = lf2 - L[3 * k + 1];
-    wv += L[3 * k] * dev::exp2_tab(tfac * tfac * L[3 * k + 2], tab);
+  // two partial sums over alternate terms: independent exp2 chains overlap
+  double wa = 0.0, wb = 0.0;
+  int k = 0;
+#pragma unroll 2
+  for (; k + 1 < cnt; k += 2) {
+    const double ta = lf2 - L[3 * k + 1];
+    const double tb = lf2 - L[3 * k + 4];
+    wa += L[3 * k] * dev::exp2_tab(ta * ta * L[3 * k + 2], tab);
+    wb += L[3 * k + 3] * dev::exp2_tab(tb * tb * L[3 * k + 5], tab);
   }
-  return wv * if2;
+  if (k < cnt) {
+    const double ta = lf2 - L[3 * k + 1];
+    wa += L[3 * k] * dev::exp2_tab(ta * ta * L[3 * k + 2], tab);
+  }
+  return (wa + wb) * if2;
 }
 
 // Main R grid, rows 1..n-1 x columns 1..n-1 (row 0 and column 0 are the
