@@ -9,6 +9,9 @@
 //   double L = like.getLogLike(theta, npar, pars_invalid);   // calcLike.h:275
 //   like.getLogLikeBatch(nprop, thetas, npar, logl, status); // batched
 //
+// The 2D likelihood likewise: Beam2 (doublebeam) and Like2 (calcLikeDouble,
+// priors per band, fillBonusParams).
+//
 // Errors are thrown as pofd_b200::Exception carrying the status code and the
 // library's message, in the place where the reference throws affineExcept.
 #ifndef POFD_B200_HPP
@@ -190,6 +193,112 @@ class Like1 {
 
  private:
   pofd_like1* h_ = nullptr;
+};
+
+// doublebeam::doublebeam(file1, file2, histogram, NBINS, MINVAL)
+// (doublebeam.h:81) from two pixel arrays of npix values each.
+class Beam2 {
+ public:
+  Beam2(const double* pix1, const double* pix2, size_t npix, double pixsize,
+        bool histogram = false, unsigned nbins = 150, double minval = 1e-6) {
+    check(pofd_beam2_create(pix1, pix2, npix, pixsize, minval,
+                            histogram ? nbins : 0u, &h_),
+          "doublebeam::doublebeam");
+  }
+  ~Beam2() { pofd_beam2_destroy(h_); }
+  Beam2(const Beam2&) = delete;
+  Beam2& operator=(const Beam2&) = delete;
+  const pofd_beam2* get() const { return h_; }
+
+ private:
+  pofd_beam2* h_ = nullptr;
+};
+
+// calcLikeDouble (calcLikeDouble.h:192-347) with the log-normal colour model.
+class Like2 {
+ public:
+  Like2(Context& ctx, unsigned nknots, const double* knotpos, unsigned nsigma,
+        const double* sigmapos, unsigned noffset, const double* offsetpos,
+        unsigned fftsize = 4096, unsigned nedge = 256, bool edge_integ = true,
+        bool bin_data = true, unsigned nbins = 1000) {
+    check(pofd_like2_create(ctx.get(), nknots, knotpos, nsigma, sigmapos, noffset,
+                            offsetpos, fftsize, nedge, edge_integ ? 1 : 0,
+                            bin_data ? 1 : 0, nbins, &h_),
+          "calcLikeDouble::calcLikeDouble");
+  }
+  ~Like2() { pofd_like2_destroy(h_); }
+  Like2(const Like2&) = delete;
+  Like2& operator=(const Like2&) = delete;
+  int addBeamSet(const Beam2& bm, double exp_conf1 = 0.0, double exp_conf2 = 0.0) {
+    return check(pofd_like2_add_beamset(h_, bm.get(), exp_conf1, exp_conf2),
+                 "calcLikeDouble::readDataFromFiles");
+  }
+  void addDataset(int beamset, const double* data1, const double* data2, size_t ndata,
+                  double sigma_base1, double sigma_base2, double like_norm = 1.0,
+                  bool meansub = true) {
+    check(pofd_like2_add_dataset(h_, beamset, data1, data2, ndata, meansub ? 1 : 0,
+                                 sigma_base1, sigma_base2, like_norm),
+          "calcLikeDouble::readDataFromFiles");
+  }
+  void setRRanges(const float* p, unsigned npar) {
+    check(pofd_like2_set_rranges(h_, p, npar), "calcLikeDouble::setRRanges");
+  }
+  void reserve(unsigned max_batch) {
+    check(pofd_like2_reserve(h_, max_batch), "calcLikeDouble::reserve");
+  }
+  double getLogLike(const float* p, unsigned npar, bool& pars_invalid) {
+    double ll = 0.0;
+    int inv = 0;
+    check(pofd_like2_loglike(h_, p, npar, &ll, &inv), "calcLikeDouble::getLogLike");
+    pars_invalid = inv != 0;
+    return ll;
+  }
+  void getLogLikeBatch(unsigned nprop, const float* p, unsigned npar, double* logl,
+                       int* status) {
+    check(pofd_like2_eval_batch(h_, nprop, p, npar, logl, status),
+          "calcLikeDouble::getLogLikeBatch");
+  }
+  // priors per band 0/1 (calcLikeDouble.h:310-341)
+  void setSigmaPrior(int band, double width) {
+    check(pofd_like2_set_sigma_prior(h_, band, 1, width), "calcLikeDouble::setSigmaPrior");
+  }
+  void unsetSigmaPrior(int band) {
+    check(pofd_like2_set_sigma_prior(h_, band, 0, 0.0), "calcLikeDouble::unsetSigmaPrior");
+  }
+  void setCFIRBPrior(int band, double mean, double sigma) {
+    check(pofd_like2_set_cfirb_prior(h_, band, 1, mean, sigma), "calcLikeDouble::setCFIRBPrior");
+  }
+  void unsetCFIRBPrior(int band) {
+    check(pofd_like2_set_cfirb_prior(h_, band, 0, 0.0, 0.0), "calcLikeDouble::unsetCFIRBPrior");
+  }
+  void setPoissonPrior(int band, double mean, double sigma) {
+    check(pofd_like2_set_poisson_prior(h_, band, 1, mean, sigma),
+          "calcLikeDouble::setPoissonPrior");
+  }
+  void unsetPoissonPrior(int band) {
+    check(pofd_like2_set_poisson_prior(h_, band, 0, 0.0, 0.0),
+          "calcLikeDouble::unsetPoissonPrior");
+  }
+  void setRegularizationAlpha(double alpha) {
+    check(pofd_like2_set_regularization(h_, alpha), "calcLikeDouble::setRegularizationAlpha");
+  }
+  // calcLikeDouble::fillBonusParams (calcLikeDouble.cc:1283-1310) on a host
+  // row: <S1>, <S2>, <S1^2>, <S2^2> after the two sigma multipliers
+  // (nmodel = knots + sigma knots + offset knots; npar >= nmodel + 6)
+  void fillBonusParams(unsigned nmodel, float* p, unsigned npar) {
+    if (npar < nmodel + 6)
+      throw std::runtime_error("calcLikeDouble::fillBonusParams: Not enough room to fill");
+    double b[4];
+    check(pofd_like2_bonus(h_, 1, p, npar, b), "calcLikeDouble::fillBonusParams");
+    for (int i = 0; i < 4; ++i) p[nmodel + 2 + i] = static_cast<float>(b[i]);
+  }
+  // 1: row cuFFT + fused column kernel (default where the size allows),
+  // 0: 2D cuFFT (no counterpart: the reference's FFTW plans are internal)
+  void setFFT(int mode) { check(pofd_like2_set_fft(h_, mode), "calcLikeDouble::setFFT"); }
+  pofd_like2* get() const { return h_; }
+
+ private:
+  pofd_like2* h_ = nullptr;
 };
 
 }  // namespace pofd_b200

@@ -44,6 +44,26 @@ int main() {
     std::printf("beam %d\n", e.code());
   }
   std::printf("loglike %d\n", code);
+  // the 2D classes: set-up on the host, evaluation needs a GPU
+  std::vector<double> beam2(27 * 27);
+  for (size_t i = 0; i < beam2.size(); ++i) beam2[i] = std::pow(beam[i], 0.6);
+  pofd_b200::Beam2 bm2(beam.data(), beam2.data(), beam.size(), 6.0, true, 40, 1e-6);
+  double sk[2] = {0.003, 0.3}, ok[1] = {0.01};
+  pofd_b200::Like2 like2(ctx, 5, knots, 2, sk, 1, ok, 256, 64, true, true, 100);
+  int bs2 = like2.addBeamSet(bm2);
+  std::vector<double> d2(1000);
+  for (int i = 0; i < 1000; ++i) d2[i] = 0.0025 * std::cos(0.41 * i);
+  like2.addDataset(bs2, data.data(), d2.data(), data.size(), 0.002, 0.0025);
+  float th2[10] = {6.5f, 5.2f, 3.4f, 1.9f, 0.1f, 0.2f, 0.25f, -0.3f, 1.0f, 1.0f};
+  int code2 = 0;
+  try {
+    like2.setRRanges(th2, 10);
+    bool inv = false;
+    like2.getLogLike(th2, 10, inv);
+  } catch (const pofd_b200::Exception& e) {
+    code2 = e.code();
+  }
+  std::printf("loglike2 %d\n", code2);
   return 0;
 }
 """
@@ -62,3 +82,4 @@ def test_cpp_shim_compiles_links_and_throws(built_lib, tmp_path):
                          check=True).stdout
     assert "beam -10" in out
     assert "loglike -11" in out
+    assert "loglike2 -11" in out
