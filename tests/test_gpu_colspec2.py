@@ -74,3 +74,22 @@ def test_fused_columns_not_used_for_other_sizes(orc, gpu_ctx):
     ll, st = G.getLogLikeBatch(s["th"][None, :])
     lo, _ = O.loglike_batch(s["th"][None, :])
     assert np.abs(ll[0] - lo[0]) < LL_TOL
+
+
+def test_fused_columns_largest_size(orc, gpu_ctx):
+    """n = 4096 (one column per block) against the 2D-transform path."""
+    s = spec2(n=4096, nedge=256, shape=(48, 48))
+    O, G = build2(orc, gpu_ctx, s)
+    th = _batch(s, nprop=2, seed=5)
+    assert G.fusedColumns()
+    lf, sf = G.getLogLikeBatch(th)
+    pf, inf = G.getPD(0, 0, th[0], setLog=False)
+    G.setFFT(0)
+    l0, s0 = G.getLogLikeBatch(th)
+    p0, in0 = G.getPD(0, 0, th[0], setLog=False)
+    assert list(sf) == list(s0)
+    ok = sf == 0
+    assert ok.any()
+    assert np.max(np.abs(lf[ok] - l0[ok])) < 1e-7
+    assert (inf["split1"], inf["split2"]) == (in0["split1"], in0["split2"])
+    assert np.max(np.abs(pf - p0)) <= P_TOL * p0.max()
