@@ -70,6 +70,27 @@ int pofd_ctx_destroy(pofd_ctx* ctx);
 int pofd_ctx_stream(pofd_ctx* ctx, void** stream_out);
 int pofd_ctx_synchronize(pofd_ctx* ctx);
 
+/* ------------------------------------------------------------ FITS input
+ * The FITS images the reference's drivers read (no GPU needed).  Both use
+ * the two-call pattern: with out == NULL only the sizes are returned.
+ *
+ * pofd_fits_read_data replaces fitsData::readData(file, ignore_mask,
+ * meansub) (fitsData.cc:56-316): the image of an "image"/"IMAGE" extension,
+ * else of the primary HDU (a "file.fits[k]" suffix selects HDU k), minus the
+ * pixels a "mask"/"MASK" extension marks non-zero, in file order; *n = the
+ * pixels kept; errors as the reference ("All data masked", mask extent
+ * mismatch, not 2D).  The values feed pofd_like1_add_dataset (meansub = 0
+ * there if done here) or, one map per band, pofd_like2_add_dataset.
+ *
+ * pofd_fits_read_beam replaces beam::readFile (beam.cc:295-395) and each
+ * band of doublebeam's: the primary HDU (or HDU k), its PIXSIZE (else
+ * PIXSCALE) keyword, nx * ny pixels in file order; the values feed
+ * pofd_beam1_create / pofd_beam2_create. */
+int pofd_fits_read_data(const char* path, int ignore_mask, int meansub, double* out,
+                        size_t cap, size_t* n);
+int pofd_fits_read_beam(const char* path, double* out, size_t cap, size_t* nx, size_t* ny,
+                        double* pixsize);
+
 /* ------------------------------------------------------------- 1D beam
  * Replaces beam::beam(filename, histogram, NBINS, MINVAL) (beam.h:69) with
  * an in-memory pixel array: beam::readFile's selection and sorting

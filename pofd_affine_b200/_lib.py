@@ -29,6 +29,9 @@ SIGNATURES = {
     "pofd_ctx_destroy": (I, [V]),
     "pofd_ctx_stream": (I, [V, PV]),
     "pofd_ctx_synchronize": (I, [V]),
+    "pofd_fits_read_data": (I, [C.c_char_p, I, I, V, S, C.POINTER(S)]),
+    "pofd_fits_read_beam": (I, [C.c_char_p, V, S, C.POINTER(S), C.POINTER(S),
+                                C.POINTER(D)]),
     "pofd_beam1_create": (I, [_dp, S, D, D, U, PV]),
     "pofd_beam1_destroy": (I, [V]),
     "pofd_beam1_info": (I, [V, _dp]),

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUTDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUTDIR, "libpofd_b200.so")
-SOURCES = ["setup.cc", "engine1d.cu", "engine2d.cu", "ensemble.cu", "surrogate.cu", "capi.cu", "peaks.cu",
+SOURCES = ["setup.cc", "fits.cc", "engine1d.cu", "engine2d.cu", "ensemble.cu", "surrogate.cu", "capi.cu", "peaks.cu",
            "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

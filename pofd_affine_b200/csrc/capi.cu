@@ -15,6 +15,7 @@
 #include "engine1d.cuh"
 #include "engine2d.cuh"
 #include "ensemble.cuh"
+#include "fits.hh"
 #include "surrogate.cuh"
 #include "setup.hh"
 
@@ -173,6 +174,36 @@ int pofd_ctx_synchronize(pofd_ctx* ctx) {
 }
 
 // ------------------------------------------------------------- 1D beam
+int pofd_fits_read_data(const char* path, int ignore_mask, int meansub, double* out,
+                        size_t cap, size_t* n) {
+  return guard([&] {
+    need(path && n, "null argument");
+    const std::vector<double> d = pofd::fits_read_data(path, ignore_mask != 0, meansub != 0);
+    *n = d.size();
+    if (out) {
+      need(cap >= d.size(), "output buffer too small");
+      std::memcpy(out, d.data(), d.size() * sizeof(double));
+    }
+    return POFD_OK;
+  });
+}
+
+int pofd_fits_read_beam(const char* path, double* out, size_t cap, size_t* nx, size_t* ny,
+                        double* pixsize) {
+  return guard([&] {
+    need(path && nx && ny && pixsize, "null argument");
+    const pofd::FitsBeam b = pofd::fits_read_beam(path);
+    *nx = static_cast<size_t>(b.nx);
+    *ny = static_cast<size_t>(b.ny);
+    *pixsize = b.pixsize;
+    if (out) {
+      need(cap >= b.pix.size(), "output buffer too small");
+      std::memcpy(out, b.pix.data(), b.pix.size() * sizeof(double));
+    }
+    return POFD_OK;
+  });
+}
+
 int pofd_beam1_create(const double* pix, size_t npix, double pixsize,
                       double minval, unsigned nhist, pofd_beam1** out) {
   return guard([&] {
