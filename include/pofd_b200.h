@@ -90,6 +90,12 @@ int pofd_fits_read_data(const char* path, int ignore_mask, int meansub, double* 
                         size_t cap, size_t* n);
 int pofd_fits_read_beam(const char* path, double* out, size_t cap, size_t* nx, size_t* ny,
                         double* pixsize);
+/* fitsDataDouble::readData (fitsDataDouble.cc:304-430): the two bands' maps
+ * (same pixel count, else an error); with a mask in both files a pixel is
+ * dropped where the two mask values share a set bit (mask1 & mask2 != 0),
+ * with one mask where it is non-zero; meansub per band. */
+int pofd_fits_read_data2(const char* path1, const char* path2, int ignore_mask, int meansub,
+                         double* out1, double* out2, size_t cap, size_t* n);
 
 /* ------------------------------------------------------------- 1D beam
  * Replaces beam::beam(filename, histogram, NBINS, MINVAL) (beam.h:69) with

@@ -32,6 +32,8 @@ SIGNATURES = {
     "pofd_fits_read_data": (I, [C.c_char_p, I, I, V, S, C.POINTER(S)]),
     "pofd_fits_read_beam": (I, [C.c_char_p, V, S, C.POINTER(S), C.POINTER(S),
                                 C.POINTER(D)]),
+    "pofd_fits_read_data2": (I, [C.c_char_p, C.c_char_p, I, I, V, V, S,
+                                 C.POINTER(S)]),
     "pofd_beam1_create": (I, [_dp, S, D, D, U, PV]),
     "pofd_beam1_destroy": (I, [V]),
     "pofd_beam1_info": (I, [V, _dp]),

@@ -204,6 +204,33 @@ class calcLike:
                 index[id(b)] = self.addBeamSet(b, exp_conf)
             self.addDataset(index[id(b)], d, s, ln, meansub)
 
+    def readDataFromFiles(self, datafiles, beamfiles, sigmas, like_norms,
+                          ignore_mask=False, meansub=False, minbeamval=1e-5,
+                          histogram=False, nbeamhist=120, exp_conf=0.0):
+        """calcLike::readDataFromFiles (calcLike.cc:688-758): the datasets
+        grouped into beam sets by beam file, the groups in the order of their
+        file names (the reference keys a std::map by them), each group's
+        datasets in input order; FITS files read as fitsData::readData and
+        beam::readFile.  Returns the beam set index of each dataset."""
+        from . import fitsio
+        n = len(datafiles)
+        if n == 0:
+            raise PofdError(-10, "No datafiles")
+        if not (n == len(beamfiles) == len(sigmas) == len(like_norms)):
+            raise PofdError(-10, "datafiles, beamfiles, sigmas, like_norms "
+                                 "not same length")
+        sets = {}
+        for bf in sorted(set(beamfiles)):
+            pix, ps = fitsio.readBeam(bf)
+            sets[bf] = self.addBeamSet(beam(pix, ps, histogram, nbeamhist,
+                                            minbeamval), exp_conf)
+        for df, bf, s_, ln in sorted(zip(datafiles, beamfiles, sigmas,
+                                         like_norms),
+                                     key=lambda r: sets[r[1]]):
+            self.addDataset(sets[bf], fitsio.readData(df, ignore_mask),
+                            s_, ln, meansub)
+        return [sets[bf] for bf in beamfiles]
+
     def setRRanges(self, p):
         th = _f32(p)
         check(lib().pofd_like1_set_rranges(self.h, th, th.size))

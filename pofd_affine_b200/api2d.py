@@ -127,6 +127,45 @@ class calcLikeDouble:
                                            int(meansub), float(sigma1),
                                            float(sigma2), float(like_norm)))
 
+    def readDataFromFiles(self, datafiles1, datafiles2, beamfiles1, beamfiles2,
+                          sigmas1, sigmas2, like_norms, ignore_mask=False,
+                          meansub=False, minbeamval=1e-6, histogram=False,
+                          nbeamhist=150, exp_conf1=0.0, exp_conf2=0.0):
+        """calcLikeDouble::readDataFromFiles (calcLikeDouble.cc:932-1030):
+        datasets grouped into beam sets by the pair of beam files (key
+        "file1:file2", groups in key order as the reference's std::map),
+        each group's datasets in input order; the two bands' maps read as
+        fitsDataDouble::readData, the beams as doublebeam's.  Returns the
+        beam set index of each dataset."""
+        from . import fitsio
+        n = len(datafiles1)
+        if n != len(datafiles2):
+            raise PofdError(-10, "Datafiles1 and datafile2 not same length")
+        if n == 0:
+            raise PofdError(-10, "No datafiles")
+        if not (n == len(beamfiles1) == len(beamfiles2) == len(sigmas1)
+                == len(sigmas2) == len(like_norms)):
+            raise PofdError(-10, "datafiles, beamfiles, sigmas, like_norms "
+                                 "not same length")
+        keys = [b1 + ":" + b2 for b1, b2 in zip(beamfiles1, beamfiles2)]
+        sets = {}
+        for k in sorted(set(keys)):
+            i = keys.index(k)
+            p1, ps1 = fitsio.readBeam(beamfiles1[i])
+            p2, ps2 = fitsio.readBeam(beamfiles2[i])
+            if abs((ps1 - ps2) / ps1) > 1e-5:  # doublebeam.cc:263-270
+                raise PofdError(-10, "Pixel scale in %s doesn't match that of %s"
+                                % (beamfiles2[i], beamfiles1[i]))
+            sets[k] = self.addBeamSet(doublebeam(p1, p2, ps1, histogram,
+                                                 nbeamhist, minbeamval),
+                                      exp_conf1, exp_conf2)
+        order = sorted(range(n), key=lambda i: sets[keys[i]])
+        for i in order:
+            d1, d2 = fitsio.readData2(datafiles1[i], datafiles2[i], ignore_mask)
+            self.addDataset(sets[keys[i]], d1, d2, sigmas1[i], sigmas2[i],
+                            like_norms[i], meansub)
+        return [sets[k] for k in keys]
+
     def setRRanges(self, p):
         th = _f32(p)
         check(lib().pofd_like2_set_rranges(self.h, th, th.size))

@@ -188,6 +188,23 @@ int pofd_fits_read_data(const char* path, int ignore_mask, int meansub, double* 
   });
 }
 
+int pofd_fits_read_data2(const char* path1, const char* path2, int ignore_mask, int meansub,
+                         double* out1, double* out2, size_t cap, size_t* n) {
+  return guard([&] {
+    need(path1 && path2 && n, "null argument");
+    std::vector<double> a, b;
+    pofd::fits_read_data2(path1, path2, ignore_mask != 0, meansub != 0, &a, &b);
+    *n = a.size();
+    if (out1 || out2) {
+      need(out1 && out2, "null argument");
+      need(cap >= a.size(), "output buffer too small");
+      std::memcpy(out1, a.data(), a.size() * sizeof(double));
+      std::memcpy(out2, b.data(), b.size() * sizeof(double));
+    }
+    return POFD_OK;
+  });
+}
+
 int pofd_fits_read_beam(const char* path, double* out, size_t cap, size_t* nx, size_t* ny,
                         double* pixsize) {
   return guard([&] {

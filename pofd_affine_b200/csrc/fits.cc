@@ -1,7 +1,8 @@
 // fits.cc -- reading the FITS images the reference's drivers take: the data
 // maps with their optional mask (fitsData::readData, fitsData.cc:56-316;
-// fitsDataDouble reads one such map per band) and the beam maps with their
-// pixel size (beam::readFile, beam.cc:295-395; doublebeam reads two).
+// fitsDataDouble::readData reads one map per band and masks them jointly,
+// fitsDataDouble.cc:304-430) and the beam maps with their pixel size
+// (beam::readFile, beam.cc:295-395; doublebeam reads two).
 //
 // A FITS file is a sequence of header-data units (HDUs): a header of
 // 80-character "KEYWORD = value" cards in 2880-byte blocks ending at END,
@@ -198,12 +199,22 @@ std::vector<double> pixels(const std::string& path, const std::string& buf, cons
 
 }  // namespace
 
-std::vector<double> fits_read_data(const std::string& spec, bool ignore_mask, bool meansub) {
+namespace {
+
+struct ImageMask {
+  std::vector<double> data;
+  std::vector<unsigned int> mask;  // empty: no mask (or ignored)
+};
+
+// The image of a data file and, unless ignored, its mask extension
+// (fitsData.cc:94-275, fitsDataDouble.cc:94-295): the selected HDU, else an
+// "image"/"IMAGE" extension, else the primary; the mask from a
+// "mask"/"MASK" extension, read as unsigned integers.
+ImageMask read_image_mask(const std::string& spec, bool ignore_mask) {
   const auto sel = split_selector(spec);
   const std::string& path = sel.first;
   const std::string buf = read_file(path);
   const std::vector<Hdu> hdus = scan(path, buf);
-  // the image: the selected HDU, else an "image" extension, else the primary
   int ih = sel.second;
   if (ih < 0) {
     ih = find_ext(hdus, "image");
@@ -212,25 +223,38 @@ std::vector<double> fits_read_data(const std::string& spec, bool ignore_mask, bo
   }
   if (ih >= static_cast<int>(hdus.size())) throw Error(POFD_E_ARG, "No HDU " + std::to_string(ih) + " in " + path);
   long nx = 0, ny = 0;
-  std::vector<double> data = pixels(path, buf, hdus[ih], &nx, &ny, "Image");
-  if (data.empty()) throw Error(POFD_E_ARG, "Image in " + path + " is empty");
+  ImageMask im;
+  im.data = pixels(path, buf, hdus[ih], &nx, &ny, "Image");
+  if (im.data.empty()) throw Error(POFD_E_ARG, "Image in " + path + " is empty");
   if (!ignore_mask) {
-    int im = find_ext(hdus, "mask");
-    if (im < 0) im = find_ext(hdus, "MASK");
-    if (im >= 0) {
+    int mh = find_ext(hdus, "mask");
+    if (mh < 0) mh = find_ext(hdus, "MASK");
+    if (mh >= 0) {
       long mx = 0, my = 0;
-      const std::vector<double> mask = pixels(path, buf, hdus[im], &mx, &my, "Mask");
-      if (mask.empty()) throw Error(POFD_E_ARG, "Mask present zero extent");
+      const std::vector<double> m = pixels(path, buf, hdus[mh], &mx, &my, "Mask");
+      if (m.empty()) throw Error(POFD_E_ARG, "Mask present zero extent");
       if (mx != nx) throw Error(POFD_E_ARG, "Mask does not match image extent along first dimension");
       if (my != ny) throw Error(POFD_E_ARG, "Mask does not match image extent along second dimension");
-      // keep the pixels whose mask value (read as an unsigned integer) is 0
-      std::vector<double> kept;
-      kept.reserve(data.size());
-      for (size_t i = 0; i < data.size(); ++i)
-        if (static_cast<unsigned int>(mask[i]) == 0u) kept.push_back(data[i]);
-      if (kept.empty()) throw Error(POFD_E_ARG, "All data masked");
-      data.swap(kept);
+      im.mask.resize(m.size());
+      for (size_t i = 0; i < m.size(); ++i) im.mask[i] = static_cast<unsigned int>(m[i]);
     }
+  }
+  return im;
+}
+
+}  // namespace
+
+std::vector<double> fits_read_data(const std::string& spec, bool ignore_mask, bool meansub) {
+  ImageMask im = read_image_mask(spec, ignore_mask);
+  std::vector<double> data;
+  if (im.mask.empty()) {
+    data.swap(im.data);
+  } else {
+    // keep the pixels whose mask is 0, in file order (fitsData.cc:286-312)
+    data.reserve(im.data.size());
+    for (size_t i = 0; i < im.data.size(); ++i)
+      if (im.mask[i] == 0u) data.push_back(im.data[i]);
+    if (data.empty()) throw Error(POFD_E_ARG, "All data masked");
   }
   if (meansub) {
     Data1 d;
@@ -239,6 +263,36 @@ std::vector<double> fits_read_data(const std::string& spec, bool ignore_mask, bo
     data.swap(d.data);
   }
   return data;
+}
+
+void fits_read_data2(const std::string& spec1, const std::string& spec2, bool ignore_mask,
+                     bool meansub, std::vector<double>* out1, std::vector<double>* out2) {
+  ImageMask a = read_image_mask(spec1, ignore_mask);
+  ImageMask b = read_image_mask(spec2, ignore_mask);
+  if (a.data.size() != b.data.size())
+    throw Error(POFD_E_ARG, "Data from file1 and file2 not the same size");
+  const size_t n = a.data.size();
+  Data2 d;
+  if (a.mask.empty() && b.mask.empty()) {
+    d.d1.swap(a.data);
+    d.d2.swap(b.data);
+  } else {
+    // fitsDataDouble.cc:338-395: with both masks a pixel is dropped only
+    // where the two mask values share a set bit (mask1 & mask2); with one,
+    // where that mask is non-zero
+    const bool both = !a.mask.empty() && !b.mask.empty();
+    for (size_t i = 0; i < n; ++i) {
+      const unsigned int m = both ? (a.mask[i] & b.mask[i]) : (a.mask.empty() ? b.mask[i] : a.mask[i]);
+      if (m == 0u) {
+        d.d1.push_back(a.data[i]);
+        d.d2.push_back(b.data[i]);
+      }
+    }
+    if (d.d1.empty()) throw Error(POFD_E_ARG, "All data masked");
+  }
+  if (meansub) d.meanSubtract();
+  out1->swap(d.d1);
+  out2->swap(d.d2);
 }
 
 FitsBeam fits_read_beam(const std::string& spec) {

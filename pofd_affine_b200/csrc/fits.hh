@@ -15,6 +15,11 @@ namespace pofd {
 // ignore_mask), in file order, mean-subtracted on request.
 std::vector<double> fits_read_data(const std::string& spec, bool ignore_mask, bool meansub);
 
+// fitsDataDouble::readData (fitsDataDouble.cc:304-430): the two bands'
+// images read as above, the same number of pixels in each, masked jointly.
+void fits_read_data2(const std::string& spec1, const std::string& spec2, bool ignore_mask,
+                     bool meansub, std::vector<double>* out1, std::vector<double>* out2);
+
 struct FitsBeam {
   std::vector<double> pix;  // file order, first axis fastest
   long nx = 0, ny = 0;

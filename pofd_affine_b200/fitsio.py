@@ -26,6 +26,23 @@ def readData(path, ignore_mask=False, meansub=False):
     return out
 
 
+def readData2(path1, path2, ignore_mask=False, meansub=False):
+    """The two bands' maps as fitsDataDouble::readData reads them
+    (fitsDataDouble.cc:304-430): with masks in both files a pixel is dropped
+    where the two mask values share a set bit, with one mask where it is
+    non-zero."""
+    n = C.c_size_t()
+    a, b = str(path1).encode(), str(path2).encode()
+    check(lib().pofd_fits_read_data2(a, b, int(ignore_mask), int(meansub), None,
+                                     None, 0, C.byref(n)))
+    o1, o2 = np.empty(n.value), np.empty(n.value)
+    check(lib().pofd_fits_read_data2(a, b, int(ignore_mask), int(meansub),
+                                     o1.ctypes.data_as(C.c_void_p),
+                                     o2.ctypes.data_as(C.c_void_p), o1.size,
+                                     C.byref(n)))
+    return o1, o2
+
+
 def readBeam(path):
     """(pixels [ny][nx], pixsize in arcsec)."""
     nx, ny, ps = C.c_size_t(), C.c_size_t(), C.c_double()

@@ -153,3 +153,101 @@ def test_reference_beam_files_match_fixtures():
         assert np.array_equal(b.ravel(), g[name])
         assert list(b.shape[::-1]) == list(g[name + "_dims"])
         assert ps == float(g[name + "_pixsize"])
+
+
+def test_two_band_masks_as_the_reference(tmp_path):
+    """fitsDataDouble.cc:338-395: both masked -> dropped where mask1 & mask2
+    share a bit; one mask -> dropped where it is non-zero."""
+    from pofd_affine_b200 import PofdError, fitsio
+    rng = np.random.default_rng(4)
+    a, b = rng.normal(size=(5, 6)), rng.normal(size=(5, 6))
+    m1 = rng.integers(0, 4, size=a.shape).astype(np.int32)
+    m2 = rng.integers(0, 4, size=a.shape).astype(np.int32)
+    f1 = _write(tmp_path / "1.fits", _hdu(a, -64, True), _hdu(m1, 32, False, "MASK"))
+    f2 = _write(tmp_path / "2.fits", _hdu(b, -64, True), _hdu(m2, 32, False, "MASK"))
+    f2n = _write(tmp_path / "2n.fits", _hdu(b, -64, True))
+    d1, d2 = fitsio.readData2(f1, f2)
+    keep = (m1 & m2).ravel() == 0
+    assert np.array_equal(d1, a.ravel()[keep]) and np.array_equal(d2, b.ravel()[keep])
+    d1, d2 = fitsio.readData2(f1, f2n)
+    keep = m1.ravel() == 0
+    assert np.array_equal(d1, a.ravel()[keep]) and np.array_equal(d2, b.ravel()[keep])
+    d1, d2 = fitsio.readData2(f1, f2, meansub=True)
+    k = (m1 & m2).ravel() == 0
+    for d, x in ((d1, a.ravel()[k]), (d2, b.ravel()[k])):
+        m = x[0]
+        for v in x[1:]:
+            m += v
+        assert np.array_equal(d, x - m / x.size)
+    small = _write(tmp_path / "s.fits", _hdu(np.ones((2, 2)), -64, True))
+    with pytest.raises(PofdError, match="not the same size"):
+        fitsio.readData2(f1, small)
+
+
+def test_read_data_from_files_groups_like_the_reference(tmp_path):
+    """calcLike::readDataFromFiles: beam sets keyed by beam file in name
+    order, datasets in input order inside a set (host-only context)."""
+    from pofd_affine_b200 import Context, calcLike, synth
+    ctx = Context(-1)
+    bm = synth.gaussian_beam(3.0)
+    bz = _write(tmp_path / "z_beam.fits", _hdu(bm, -64, True, keys=[("PIXSIZE", 6.0)]))
+    ba = _write(tmp_path / "a_beam.fits", _hdu(bm ** 1.2, -64, True,
+                                               keys=[("PIXSIZE", 6.0)]))
+    rng = np.random.default_rng(0)
+    maps = [rng.normal(0, 0.002, (40, 40)) for _ in range(3)]
+    files = [_write(tmp_path / ("m%d.fits" % i), _hdu(m, -64, True))
+             for i, m in enumerate(maps)]
+    kp, kv = synth.knot_model(6, 0.002, 0.4, rng=rng)
+    L = calcLike(ctx, kp, 4096, 256, True, 100)
+    idx = L.readDataFromFiles(files, [bz, ba, bz], [0.002, 0.003, 0.004],
+                              [1.0, 1.0, 1.0], meansub=True)
+    assert idx == [1, 0, 1]  # a_beam sorts first
+    info = L.datasetInfo(1, 1)
+    assert info["sigma_base"] == 0.004  # second dataset of the z_beam set
+
+
+@pytest.mark.gpu
+def test_likelihood_from_files_equals_from_arrays(gpu_ctx, tmp_path):
+    from pofd_affine_b200 import beam, calcLike, calcLikeDouble, doublebeam, synth
+    rng = np.random.default_rng(6)
+    kp, kv = synth.knot_model(6, 0.002, 0.4, rng=rng)
+    bm = synth.gaussian_beam(3.0)
+    img = synth.make_map((96, 96), 6.0, bm, kp, kv, 0.002, rng)
+    bf = _write(tmp_path / "b.fits", _hdu(bm, -64, True, keys=[("PIXSIZE", 6.0)]))
+    df = _write(tmp_path / "d.fits", _hdu(img, -64, True))
+    th = np.concatenate([kv, [1.0]]).astype(np.float32)
+    A = calcLike(gpu_ctx, kp, 4096, 512, True, 300)
+    A.readDataFromFiles([df], [bf], [0.002], [1.0], meansub=True, histogram=True)
+    A.setRRanges(th)
+    B = calcLike(gpu_ctx, kp, 4096, 512, True, 300)
+    B.addBeamSet(beam(bm, 6.0, True, 120, 1e-5))
+    B.addDataset(0, img, 0.002, 1.0, True)
+    B.setRRanges(th)
+    la, sa = A.getLogLikeBatch(th[None, :])
+    lb, sb = B.getLogLikeBatch(th[None, :])
+    assert sa[0] == 0 and la[0] == lb[0]
+    # 2D
+    b1, b2 = synth.gaussian_beam(3.0), synth.gaussian_beam(3.0) ** 0.6
+    sk = np.logspace(np.log10(0.003), np.log10(0.3), 2)
+    ok = np.array([0.01])
+    sv = np.array([0.2, 0.25], np.float32)
+    ov = np.array([np.log(0.7)], np.float32)
+    m1, m2 = synth.make_map_pair((64, 64), 6.0, b1, b2, kp, kv,
+                                 lambda f: np.interp(f, sk, sv),
+                                 lambda f: 0 * f + ov[0], 0.0025, 0.003, rng)
+    f1 = _write(tmp_path / "m1.fits", _hdu(m1, -64, True))
+    f2 = _write(tmp_path / "m2.fits", _hdu(m2, -64, True))
+    g1 = _write(tmp_path / "b1.fits", _hdu(b1, -64, True, keys=[("PIXSIZE", 6.0)]))
+    g2 = _write(tmp_path / "b2.fits", _hdu(b2, -64, True, keys=[("PIXSIZE", 6.0)]))
+    th2 = np.concatenate([kv, sv, ov, [1.0, 1.0]]).astype(np.float32)
+    C2 = calcLikeDouble(gpu_ctx, kp, sk, ok, 256, 64, True, 100, True)
+    C2.readDataFromFiles([f1], [f2], [g1], [g2], [0.0025], [0.003], [1.0],
+                         meansub=True, histogram=True, nbeamhist=40)
+    C2.setRRanges(th2)
+    D2 = calcLikeDouble(gpu_ctx, kp, sk, ok, 256, 64, True, 100, True)
+    D2.addBeamSet(doublebeam(b1, b2, 6.0, True, 40, 1e-6))
+    D2.addDataset(0, m1, m2, 0.0025, 0.003, 1.0, True)
+    D2.setRRanges(th2)
+    lc, sc = C2.getLogLikeBatch(th2[None, :])
+    ld, sd = D2.getLogLikeBatch(th2[None, :])
+    assert sc[0] == 0 and lc[0] == ld[0]
