@@ -17,6 +17,8 @@
 #ifndef POFD_B200_HPP
 #define POFD_B200_HPP
 
+#include <cmath>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -38,6 +40,38 @@ class Exception : public std::runtime_error {
 inline int check(int st, const char* method) {
   if (st < 0) throw Exception(st, method);
   return st;
+}
+
+// FITS reading through the library (fitsData::readData, beam::readFile).
+inline std::vector<double> readFitsData(const std::string& path, bool ignore_mask,
+                                        bool meansub) {
+  size_t n = 0;
+  check(pofd_fits_read_data(path.c_str(), ignore_mask, meansub, nullptr, 0, &n),
+        "fitsData::readData");
+  std::vector<double> d(n);
+  check(pofd_fits_read_data(path.c_str(), ignore_mask, meansub, d.data(), n, &n),
+        "fitsData::readData");
+  return d;
+}
+inline void readFitsData2(const std::string& p1, const std::string& p2, bool ignore_mask,
+                          bool meansub, std::vector<double>& d1, std::vector<double>& d2) {
+  size_t n = 0;
+  check(pofd_fits_read_data2(p1.c_str(), p2.c_str(), ignore_mask, meansub, nullptr, nullptr,
+                             0, &n),
+        "fitsDataDouble::readData");
+  d1.resize(n);
+  d2.resize(n);
+  check(pofd_fits_read_data2(p1.c_str(), p2.c_str(), ignore_mask, meansub, d1.data(),
+                             d2.data(), n, &n),
+        "fitsDataDouble::readData");
+}
+inline std::vector<double> readFitsBeam(const std::string& path, double& pixsize) {
+  size_t nx = 0, ny = 0;
+  check(pofd_fits_read_beam(path.c_str(), nullptr, 0, &nx, &ny, &pixsize), "beam::readFile");
+  std::vector<double> b(nx * ny);
+  check(pofd_fits_read_beam(path.c_str(), b.data(), b.size(), &nx, &ny, &pixsize),
+        "beam::readFile");
+  return b;
 }
 
 class Context {
@@ -135,6 +169,33 @@ class Like1 {
     check(pofd_like1_add_dataset(h_, beamset, data, ndata, meansub ? 1 : 0,
                                  sigma_base, like_norm),
           "calcLike::readDataFromFiles");
+  }
+  // calcLike::readDataFromFiles (calcLike.h:218-223, calcLike.cc:688-758):
+  // datasets grouped by beam file, the groups in file-name order (the
+  // reference's std::map), each group's datasets in input order
+  void readDataFromFiles(const std::vector<std::string>& datafiles,
+                         const std::vector<std::string>& beamfiles,
+                         const std::vector<double>& sigmas,
+                         const std::vector<double>& like_norms, bool IGNOREMASK = false,
+                         bool MEANSUB = false, double MINBEAMVAL = 1e-5,
+                         bool HISTOGRAMBEAMS = false, unsigned int NBEAMHIST = 120,
+                         double EXPCONF = 0.0) {
+    const size_t n = datafiles.size();
+    if (n == 0) throw std::runtime_error("calcLike::readDataFromFiles: No datafiles");
+    if (n != beamfiles.size() || n != sigmas.size() || n != like_norms.size())
+      throw std::runtime_error("calcLike::readDataFromFiles: inputs not same length");
+    std::map<std::string, std::vector<size_t>> groups;
+    for (size_t i = 0; i < n; ++i) groups[beamfiles[i]].push_back(i);
+    for (const auto& g : groups) {
+      double ps = 0.0;
+      const std::vector<double> pix = readFitsBeam(g.first, ps);
+      Beam1 bm(pix.data(), pix.size(), ps, HISTOGRAMBEAMS, NBEAMHIST, MINBEAMVAL);
+      const int bs = addBeamSet(bm, EXPCONF);
+      for (size_t i : g.second) {
+        const std::vector<double> d = readFitsData(datafiles[i], IGNOREMASK, false);
+        addDataset(bs, d.data(), d.size(), sigmas[i], like_norms[i], MEANSUB);
+      }
+    }
   }
   void setRRanges(const float* p, unsigned npar) {
     check(pofd_like1_set_rranges(h_, p, npar), "calcLike::setRRanges");
@@ -239,6 +300,46 @@ class Like2 {
     check(pofd_like2_add_dataset(h_, beamset, data1, data2, ndata, meansub ? 1 : 0,
                                  sigma_base1, sigma_base2, like_norm),
           "calcLikeDouble::readDataFromFiles");
+  }
+  // calcLikeDouble::readDataFromFiles (calcLikeDouble.cc:932-1030): groups
+  // keyed by "beamfile1:beamfile2" in key order, datasets in input order
+  void readDataFromFiles(const std::vector<std::string>& datafiles1,
+                         const std::vector<std::string>& datafiles2,
+                         const std::vector<std::string>& beamfiles1,
+                         const std::vector<std::string>& beamfiles2,
+                         const std::vector<double>& sigmas1, const std::vector<double>& sigmas2,
+                         const std::vector<double>& like_norms, bool IGNOREMASK = false,
+                         bool MEANSUB = false, double MINBEAMVAL = 1e-6, bool HISTOGRAM = false,
+                         unsigned int NBEAMHIST = 150, double EXPCONF1 = 0.0,
+                         double EXPCONF2 = 0.0) {
+    const size_t n = datafiles1.size();
+    if (n != datafiles2.size())
+      throw std::runtime_error("calcLikeDouble::readDataFromFiles: Datafiles1 and datafile2 not same length");
+    if (n == 0) throw std::runtime_error("calcLikeDouble::readDataFromFiles: No datafiles");
+    if (n != beamfiles1.size() || n != beamfiles2.size() || n != sigmas1.size() ||
+        n != sigmas2.size() || n != like_norms.size())
+      throw std::runtime_error("calcLikeDouble::readDataFromFiles: inputs not same length");
+    std::map<std::string, std::vector<size_t>> groups;
+    for (size_t i = 0; i < n; ++i) groups[beamfiles1[i] + ":" + beamfiles2[i]].push_back(i);
+    for (const auto& g : groups) {
+      const size_t i0 = g.second.front();
+      double ps1 = 0.0, ps2 = 0.0;
+      const std::vector<double> p1 = readFitsBeam(beamfiles1[i0], ps1);
+      const std::vector<double> p2 = readFitsBeam(beamfiles2[i0], ps2);
+      if (std::abs((ps1 - ps2) / ps1) > 1e-5)  // doublebeam.cc:263-270
+        throw std::runtime_error("doublebeam::readFiles: Pixel scale in " + beamfiles2[i0] +
+                                 " doesn't match that of " + beamfiles1[i0]);
+      if (p1.size() != p2.size())
+        throw std::runtime_error("doublebeam::readFiles: beam sizes differ");
+      Beam2 bm(p1.data(), p2.data(), p1.size(), ps1, HISTOGRAM, NBEAMHIST, MINBEAMVAL);
+      const int bs = addBeamSet(bm, EXPCONF1, EXPCONF2);
+      for (size_t i : g.second) {
+        std::vector<double> d1, d2;
+        readFitsData2(datafiles1[i], datafiles2[i], IGNOREMASK, false, d1, d2);
+        addDataset(bs, d1.data(), d2.data(), d1.size(), sigmas1[i], sigmas2[i], like_norms[i],
+                   MEANSUB);
+      }
+    }
   }
   void setRRanges(const float* p, unsigned npar) {
     check(pofd_like2_set_rranges(h_, p, npar), "calcLikeDouble::setRRanges");

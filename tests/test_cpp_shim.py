@@ -83,3 +83,68 @@ def test_cpp_shim_compiles_links_and_throws(built_lib, tmp_path):
     assert "beam -10" in out
     assert "loglike -11" in out
     assert "loglike2 -11" in out
+
+
+PROG_FILES = r"""
+#include <cstdio>
+#include <string>
+#include <vector>
+#include "pofd_b200.hpp"
+int main(int argc, char** argv) {
+  const std::string dir = argv[1];
+  pofd_b200::Context ctx(-1);
+  double knots[5] = {0.002, 0.005, 0.02, 0.08, 0.3};
+  pofd_b200::Like1 like(ctx, 5, knots, 2048, 256, true, 100);
+  like.readDataFromFiles({dir + "/d0.fits", dir + "/d1.fits", dir + "/d2.fits"},
+                         {dir + "/z_beam.fits", dir + "/a_beam.fits", dir + "/z_beam.fits"},
+                         {0.002, 0.003, 0.004}, {1.0, 1.0, 1.0}, false, true, 1e-5, true, 120);
+  double info[9];
+  pofd_like1_dataset_info(like.get(), 1, 1, info, nullptr);
+  std::printf("set1ds1 ndata %g sigma %g\n", info[0], info[5]);
+  pofd_like1_dataset_info(like.get(), 0, 0, info, nullptr);
+  std::printf("set0ds0 ndata %g sigma %g\n", info[0], info[5]);
+  double sk[2] = {0.003, 0.3}, ok[1] = {0.01};
+  pofd_b200::Like2 like2(ctx, 5, knots, 2, sk, 1, ok, 256, 64, true, true, 50);
+  like2.readDataFromFiles({dir + "/d0.fits"}, {dir + "/d1.fits"}, {dir + "/z_beam.fits"},
+                          {dir + "/a_beam.fits"}, {0.002}, {0.003}, {1.0}, false, true, 1e-6,
+                          true, 40);
+  double info10[10];
+  pofd_like2_dataset_info(like2.get(), 0, 0, info10, nullptr);
+  std::printf("like2 ndata %g sigma2 %g\n", info10[0], info10[8]);
+  return 0;
+}
+"""
+
+
+def test_cpp_shim_reads_data_from_files(built_lib, tmp_path):
+    """readDataFromFiles with the reference's signature and grouping: the
+    a_beam group comes first (file-name order), the z_beam group holds the
+    first and third datasets in input order; the masked map loses its
+    masked pixels."""
+    from test_fits_input import _hdu, _write
+    from pofd_affine_b200 import synth
+    bm = synth.gaussian_beam(3.0)
+    _write(tmp_path / "z_beam.fits", _hdu(bm, -64, True, keys=[("PIXSIZE", 6.0)]))
+    _write(tmp_path / "a_beam.fits", _hdu(bm ** 1.2, -64, True, keys=[("PIXSIZE", 6.0)]))
+    rng = np.random.default_rng(3)
+    for i in range(3):
+        m = rng.normal(0, 0.002, (30, 30))
+        if i == 2:
+            mask = np.zeros((30, 30), np.int32)
+            mask[:5] = 1
+            _write(tmp_path / ("d%d.fits" % i), _hdu(m, -64, True),
+                   _hdu(mask, 32, False, "MASK"))
+        else:
+            _write(tmp_path / ("d%d.fits" % i), _hdu(m, -64, True))
+    src = tmp_path / "files.cc"
+    src.write_text(PROG_FILES)
+    exe = tmp_path / "files"
+    libdir = os.path.dirname(built_lib)
+    subprocess.check_call(["g++", "-std=c++17", "-O1", str(src), "-I",
+                           os.path.join(ROOT, "include"), "-L", libdir,
+                           "-lpofd_b200", "-Wl,-rpath," + libdir, "-o", str(exe)])
+    out = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True,
+                         check=True).stdout
+    assert "set1ds1 ndata 750 sigma 0.004" in out
+    assert "set0ds0 ndata 900 sigma 0.003" in out
+    assert "like2 ndata 900 sigma2 0.003" in out
