@@ -14,7 +14,7 @@
 // Layout in HBM (P proposals, B beam sets, D datasets, n FFT size, NI
 // interpolation nodes, nc = n/2+1):
 //   nodes [P][B][2][NI]        R at the nodes (pos/neg side)
-//   spl   [P][B][2][4][NI]     node spline y, b, c, d per interval
+//   spl   [P][B][2][NI][4]     node spline (y, b, c, d) per interval
 //   rbuf  [P][B][2*nc]         R grid (x dflux), then its D2Z spectrum in place
 //   pbuf  [P][D][2*nc]         per-dataset spectrum, then its Z2D P(D) in place
 //   ppart/pmidx [P][D][nchunk] chunk reductions of the P(D)
@@ -270,15 +270,14 @@ k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
     c[NI - 1] = 0.0;
   }
   __syncthreads();
-  double* out = spl + static_cast<size_t>(row) * 4 * NI;
+  // one 32-byte record (y, b, c, d) per interval
+  double2* out = reinterpret_cast<double2*>(spl + static_cast<size_t>(row) * 4 * NI);
   const double* x = sd.x;
   for (int i = threadIdx.x; i < NI - 1; i += RT) {
     const double dx = x[i + 1] - x[i];
     const double dy = y[i + 1] - y[i];
-    out[i] = y[i];
-    out[NI + i] = (dy / dx) - dx * (c[i + 1] + 2.0 * c[i]) / 3.0;
-    out[2 * NI + i] = c[i];
-    out[3 * NI + i] = (c[i + 1] - c[i]) / (3.0 * dx);
+    out[2 * i] = make_double2(y[i], (dy / dx) - dx * (c[i + 1] + 2.0 * c[i]) / 3.0);
+    out[2 * i + 1] = make_double2(c[i], (c[i + 1] - c[i]) / (3.0 * dx));
   }
 }
 
@@ -292,7 +291,7 @@ struct GridFill1 {
   int wrap, NI;
   const double* __restrict__ x0;
   const double* __restrict__ x1;
-  const double* __restrict__ S0;   // this row's node spline [2][4][NI]
+  const double* __restrict__ S0;   // this row's node spline [2][NI][4]
   const double* __restrict__ e2;   // exp2 table in shared memory
 
   __device__ __forceinline__ GridFill1(const BSet1Dev& bs, const double* spl_row, int ni,
@@ -311,9 +310,10 @@ struct GridFill1 {
     double r = 0.0;
     if (q >= 0) {
       const double cflux = __dadd_rn(pd, neg ? off1 : off0);
-      const double* S = S0 + (neg ? 4 * NI : 0);
+      const double2* S = reinterpret_cast<const double2*>(S0 + (neg ? 4 * NI : 0)) + 2 * q;
+      const double2 yb = S[0], cd = S[1];
       const double delx = cflux - (neg ? x1 : x0)[q];
-      const double v = S[q] + delx * (S[NI + q] + delx * (S[2 * NI + q] + delx * S[3 * NI + q]));
+      const double v = yb.x + delx * (yb.y + delx * (cd.x + delx * cd.y));
       r = dev::exp2_tab(v, e2) * dflux;
     }
     const double cf = neg ? static_cast<double>(i - wrap - 1) * dflux + minflux_R : pd;

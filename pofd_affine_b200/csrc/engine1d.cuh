@@ -100,7 +100,7 @@ struct Workspace1 {
   int* mstatus = nullptr;    // [P] model status
   double* sigmult = nullptr; // [P]
   double* nodes = nullptr;   // [P][B][2][NI] R at nodes -> log2 R
-  double* spl = nullptr;     // [P][B][2][4][NI] spline y,b,c,d per interval
+  double* spl = nullptr;     // [P][B][2][NI][4] spline (y,b,c,d) per interval
   double* rbuf = nullptr;    // [P][B][2*(n/2+1)] R grid / spectrum
   double* rpart = nullptr;   // [P][B][ntile][2]
   double* mom = nullptr;     // [P][B][4] mean, var, shift, doshift
