@@ -570,6 +570,19 @@ def main():
                 "peak_source": "measured (pofd_fp64_peak DFMA loop)",
                 "achieved": None, "frac": None,
                 "traffic": read_traffic(dom)}
+    # the longest HBM-bound stage beside it (the dominant one is FP64 bound)
+    hbm_stages = {k: v for k, v in own.items()
+                  if stage_flops(k, BATCH, B, n) is None
+                  and stage_bytes(k, BATCH, B, D, n, cuts) is not None}
+    roof_hbm = None
+    if hbm_stages:
+        hs = max(hbm_stages, key=hbm_stages.get)
+        hb_bytes = stage_bytes(hs, BATCH, B, D, n, cuts)
+        ach_h = hb_bytes / (own[hs] * 1e-3) / 1e9
+        roof_hbm = {"bound": "hbm", "kernel": hs, "achieved": ach_h,
+                    "peak": hbm_peak, "unit": "GB/s", "frac": ach_h / hbm_peak,
+                    "algorithmic_bytes": hb_bytes, "ms_per_launch": own[hs],
+                    "peak_source": peak_src}
     hbm_pipe = sum(stage_bytes(s, BATCH, B, D, n, cuts) or 0 for s in stages)
     nk = L.kernelsPerEval()
 
@@ -601,6 +614,7 @@ def main():
                     "h2d_bytes_per_step": BATCH * npar * 4,
                     "d2h_bytes_per_step": BATCH * (8 + 4)},
             "roofline": roof,
+            "roofline_hbm_stage": roof_hbm,
             "stage_ms": stages,
             "pipeline_hbm_bytes_per_step": hbm_pipe,
             "gpu_launches": nk * a.steps,
