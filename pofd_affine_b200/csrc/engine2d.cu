@@ -1146,7 +1146,6 @@ __global__ void k_reduce2(const BSet2Dev* __restrict__ bsets,
 // two shared tables H[j >> 5] L[j & 31] built on the host in long double.
 constexpr int CS_THREADS = 256;
 
-__host__ __device__ constexpr int cs_m3(int n) { return n / 256; }
 __host__ __device__ constexpr int cs_slots(int n) { return 256 * (n / 256 + 1); }
 inline size_t colspec_smem(int n) {
   const int C = CS_THREADS / (n / 16);
