@@ -476,6 +476,19 @@ int pofd_ensemble_last(pofd_ensemble* e, float* theta, double* logl);
 /* Accepted steps per walker (getAcceptanceFrac numerator,
  * affineEnsemble.h:157). */
 int pofd_ensemble_naccept(pofd_ensemble* e, unsigned* naccept);
+/* Checkpoint / resume (no counterpart: the reference writes its chain once
+ * at the end and cannot restart, pofd_affine_mcmc.cc:313-316).  Every
+ * random draw is keyed by (seed; step, walker, draw), so the generator's
+ * position is one step counter.  A run re-created with the same seed,
+ * initialised from pofd_ensemble_last's walkers and log-likelihoods and
+ * given the saved counter (and acceptance counts) continues the random
+ * stream of the uninterrupted run: the plain stretch-move chains are
+ * identical.  (Delayed acceptance also needs its first-stage model
+ * restored by the caller.) */
+int pofd_ensemble_get_counter(pofd_ensemble* e, unsigned long long* step,
+                              unsigned long long* seed);
+int pofd_ensemble_set_counter(pofd_ensemble* e, unsigned long long step);
+int pofd_ensemble_set_naccept(pofd_ensemble* e, const unsigned* naccept);
 /* getAcor (affineEnsemble.h:155, affineChainSet.cc:824-1030): tau[nparams]
  * over the recorded chain, NaN for ACIGNORE parameters; returns POFD_OK, or
  * POFD_REJECTED when some parameter's series was too short (< 50). */

@@ -34,6 +34,10 @@ SIGNATURES = {
                                 C.POINTER(D)]),
     "pofd_fits_read_data2": (I, [C.c_char_p, C.c_char_p, I, I, V, V, S,
                                  C.POINTER(S)]),
+    "pofd_ensemble_get_counter": (I, [V, C.POINTER(C.c_ulonglong),
+                                      C.POINTER(C.c_ulonglong)]),
+    "pofd_ensemble_set_counter": (I, [V, C.c_ulonglong]),
+    "pofd_ensemble_set_naccept": (I, [V, _up]),
     "pofd_beam1_create": (I, [_dp, S, D, D, U, PV]),
     "pofd_beam1_destroy": (I, [V]),
     "pofd_beam1_info": (I, [V, _dp]),

@@ -1035,6 +1035,32 @@ int pofd_ensemble_last(pofd_ensemble* e, float* theta, double* logl) {
   });
 }
 
+int pofd_ensemble_get_counter(pofd_ensemble* e, unsigned long long* step,
+                              unsigned long long* seed) {
+  return guard([&] {
+    need(e && step && seed, "null argument");
+    *step = e->ens->step_counter();
+    *seed = e->ens->seed();
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_set_counter(pofd_ensemble* e, unsigned long long step) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->set_step_counter(step);
+    return POFD_OK;
+  });
+}
+
+int pofd_ensemble_set_naccept(pofd_ensemble* e, const unsigned* naccept) {
+  return guard([&] {
+    need(e && naccept, "null argument");
+    e->ens->set_naccept(naccept);
+    return POFD_OK;
+  });
+}
+
 int pofd_ensemble_naccept(pofd_ensemble* e, unsigned* naccept) {
   return guard([&] {
     need(e && naccept, "null argument");

@@ -460,6 +460,26 @@ void Ensemble::clear_chain() {
   ck(cudaStreamSynchronize(stream_), "synchronize");
 }
 
+unsigned long long Ensemble::step_counter() const {
+  unsigned long long c = 0;
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  ck(cudaMemcpyAsync(&c, ctr_, sizeof(c), cudaMemcpyDeviceToHost, stream_), "D2H");
+  ck(cudaStreamSynchronize(stream_), "synchronize");
+  return c;
+}
+
+void Ensemble::set_step_counter(unsigned long long step) {
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  ck(cudaMemcpyAsync(ctr_, &step, sizeof(step), cudaMemcpyHostToDevice, stream_), "H2D");
+  ck(cudaStreamSynchronize(stream_), "synchronize");
+}
+
+void Ensemble::set_naccept(const unsigned* in) {
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  ck(cudaMemcpyAsync(nacc_, in, nw_ * sizeof(unsigned), cudaMemcpyHostToDevice, stream_), "H2D");
+  ck(cudaStreamSynchronize(stream_), "synchronize");
+}
+
 unsigned Ensemble::nrecorded() const {
   unsigned long long c[3];
   ck(cudaSetDevice(device_), "cudaSetDevice");

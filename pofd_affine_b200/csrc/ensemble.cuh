@@ -66,6 +66,12 @@ class Ensemble {
   void chain(float* theta, double* logl) const;
   void last(float* theta, double* logl) const;
   void naccept(unsigned* out) const;
+  // checkpoint / resume: the generator's step counter (draws are keyed by
+  // (seed; step, walker, draw)), the seed, and the accepted-step counts
+  unsigned long long step_counter() const;
+  void set_step_counter(unsigned long long step);
+  void set_naccept(const unsigned* in);
+  uint64_t seed() const { return seed_; }
   // Acor of every parameter over the recorded chain (NaN where ignored or
   // the chain is too short); returns 1 if every non-ignored parameter
   // succeeded.

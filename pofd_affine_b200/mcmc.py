@@ -261,6 +261,40 @@ class affineEnsemble:
         check(lib().pofd_ensemble_naccept(self.h, out))
         return out
 
+    def checkpoint(self, path):
+        """Write the sampler's resumable state to path (.npz): the current
+        walkers and log-likelihoods, the generator's step counter and seed,
+        the accepted-step counts and the steps taken.  The recorded chain is
+        not part of it (read it with getChain before)."""
+        th, ll = self.getLast()
+        step, seed = C.c_ulonglong(), C.c_ulonglong()
+        check(lib().pofd_ensemble_get_counter(self.h, C.byref(step),
+                                              C.byref(seed)))
+        np.savez(path, walkers=th, logl=ll, step=np.uint64(step.value),
+                 seed=np.uint64(seed.value), naccept=self.getNAccept(),
+                 nsteps_done=np.int64(self.nsteps_done),
+                 shape=np.array([self.nwalkers, self.nparams]))
+
+    def resume(self, path):
+        """Continue from a checkpoint written by checkpoint(): same walker
+        count, parameter count and seed required.  Parameter states, limits,
+        the likelihood and the temperature are the caller's to set as
+        before.  The plain stretch-move chain then continues exactly as the
+        uninterrupted run would."""
+        z = np.load(path)
+        if list(z["shape"]) != [self.nwalkers, self.nparams]:
+            raise PofdError(-10, "checkpoint is for another ensemble shape")
+        step, seed = C.c_ulonglong(), C.c_ulonglong()
+        check(lib().pofd_ensemble_get_counter(self.h, C.byref(step),
+                                              C.byref(seed)))
+        if int(z["seed"]) != seed.value:
+            raise PofdError(-10, "checkpoint was written with another seed")
+        self.initChains(z["walkers"], z["logl"])
+        check(lib().pofd_ensemble_set_counter(self.h, int(z["step"])))
+        check(lib().pofd_ensemble_set_naccept(
+            self.h, np.ascontiguousarray(z["naccept"], np.uint32)))
+        self.nsteps_done = int(z["nsteps_done"])
+
     def getAcceptanceFrac(self):
         return self.getNAccept() / max(self.nsteps_done, 1)
 

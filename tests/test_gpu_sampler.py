@@ -149,3 +149,40 @@ def test_error_policy_reject_counts_failures(gpu_ctx):
     E2.doSteps(5)
     assert E2.getFailures() == 8 * 5
     assert np.all(E2.getNAccept() == 0)
+
+
+def test_checkpoint_resume_continues_the_chain_exactly(gpu_ctx, tmp_path):
+    """8 steps in one run equal 4 steps, a checkpoint to a file, a new
+    ensemble (same seed) resumed from it and 4 more steps: walkers,
+    log-likelihoods and acceptance counts bit for bit."""
+    from pofd_affine_b200.mcmc import affineEnsemble, gaussLike
+    mu, cov = _gauss(4, seed=3)
+    G = gaussLike(gpu_ctx, mu, cov)
+
+    def make():
+        E = affineEnsemble(gpu_ctx, G, 24, 4, scalefac=2.0, seed=4321)
+        E.setParamLimits(1, mu[1] - 4 * np.sqrt(cov[1, 1]), np.inf)
+        return E
+
+    rng = np.random.default_rng(0)
+    w0 = (mu + rng.normal(size=(24, 4))).astype(np.float32)
+    A = make()
+    A.initChains(w0)
+    A.doSteps(8)
+    ta, la = A.getLast()
+    B = make()
+    B.initChains(w0)
+    B.doSteps(4)
+    path = str(tmp_path / "ck.npz")
+    B.checkpoint(path)
+    C2 = make()
+    C2.resume(path)
+    C2.doSteps(4)
+    tc, lc = C2.getLast()
+    assert np.array_equal(ta, tc)
+    assert np.array_equal(la, lc)
+    assert np.array_equal(A.getNAccept(), C2.getNAccept())
+    D = affineEnsemble(gpu_ctx, G, 24, 4, seed=1)
+    from pofd_affine_b200 import PofdError
+    with pytest.raises(PofdError, match="seed"):
+        D.resume(path)
