@@ -5,7 +5,20 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace pofd {
+
+// A named NVTX range for the life of the object: host entry points show up
+// as ranges in a timeline profiler (NVTX v3 is header-only; without a tool
+// attached the calls return at once).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 namespace dev {
 
 constexpr double kTwoPi = 6.283185307179586476925286766559005768394;

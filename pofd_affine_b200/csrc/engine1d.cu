@@ -2248,6 +2248,7 @@ void Engine1::set_tuning(const Tune1& t) {
 // captured graph of the whole sequence.  The FFT choice is tried only where
 // the own FFT supports the size.
 void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out8) {
+  NvtxRange nvtx_range("pofd like1 autotune");
   if (nprop == 0 || reps < 1) throw Error(POFD_E_ARG, "autotune needs rows and reps >= 1");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
   const double t_untuned = time_sequence(nprop, theta, npar, reps);
@@ -2684,6 +2685,7 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
 // itself being captured, the launches are recorded into the caller's graph.
 void Engine1::enqueue(unsigned nprop, const float* theta_dev, unsigned npar,
                       double* logl_dev, int* status_dev, cudaStream_t st) {
+  NvtxRange nvtx_range("pofd like1 enqueue");
   if (nprop == 0) return;
   if (npar < knots_.size() + 1) throw Error(POFD_E_ARG, "Not enough elements in paramSet");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
@@ -2779,6 +2781,7 @@ cudaGraphExec_t Engine1::host_graph_for(unsigned nprop, unsigned npar) {
 
 void Engine1::eval_host(unsigned nprop, const float* theta, unsigned npar,
                         double* logl, int* status) {
+  NvtxRange nvtx_range("pofd like1 eval_batch");
   if (nprop == 0) return;
   if (npar < knots_.size() + 1) throw Error(POFD_E_ARG, "Not enough elements in paramSet");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));

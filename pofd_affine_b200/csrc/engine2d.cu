@@ -2182,6 +2182,7 @@ cudaGraphExec_t Engine2::graph_for(unsigned nprop, const float* theta,
 
 void Engine2::enqueue(unsigned nprop, const float* theta_dev, unsigned npar,
                       double* logl_dev, int* status_dev, cudaStream_t st) {
+  NvtxRange nvtx_range("pofd like2 enqueue");
   if (nprop == 0) return;
   if (npar < nparams() + 2) throw Error(POFD_E_ARG, "Not enough elements in params");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
@@ -2201,6 +2202,7 @@ void Engine2::enqueue(unsigned nprop, const float* theta_dev, unsigned npar,
 
 void Engine2::eval_host(unsigned nprop, const float* theta, unsigned npar,
                         double* logl, int* status) {
+  NvtxRange nvtx_range("pofd like2 eval_batch");
   if (nprop == 0) return;
   if (npar < nparams() + 2) throw Error(POFD_E_ARG, "Not enough elements in params");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));

@@ -6,6 +6,7 @@
 #include <limits>
 #include <sstream>
 
+#include "common.cuh"
 #include "setup.hh"
 #include "surrogate.cuh"
 
@@ -537,6 +538,7 @@ void Ensemble::check_error() {
 }
 
 void Ensemble::do_steps(unsigned nsteps, bool record) {
+  NvtxRange nvtx_range("pofd ensemble do_steps");
   if (!init_) throw Error(POFD_E_ARG, "Chains not initialised");
   if (!fn_) throw Error(POFD_E_ARG, "No likelihood set");
   if (nsteps == 0) return;
@@ -691,6 +693,7 @@ void Ensemble::prepare_da() {
 }
 
 void Ensemble::do_steps_da(unsigned nsteps, bool record) {
+  NvtxRange nvtx_range("pofd ensemble do_steps_da");
   if (!init_) throw Error(POFD_E_ARG, "Chains not initialised");
   if (!fn_) throw Error(POFD_E_ARG, "No likelihood set");
   if (!sfn_) throw Error(POFD_E_ARG, "No first-stage evaluator set");
