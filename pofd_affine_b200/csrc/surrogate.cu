@@ -418,12 +418,30 @@ struct Gemm {
   size_t smem;
 };
 
+// N tile of a GEMM: the widest of 128, 64, 32 dividing N that still gives at
+// least one CTA per SM, else 16.  The surrogate's GEMMs are small (a few
+// hundred rows); narrower tiles spread them -- and the fused epilogues, the
+// Adam update of the weight gradient above all -- over more SMs.
+int ntile_for(int M, int N) {
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
+      nsm = 148;
+  }
+  const int rt = (M + umma::kRows - 1) / umma::kRows;
+  for (int nt : {128, 64, 32})
+    if (N % nt == 0 && rt * (N / nt) >= nsm) return nt;
+  return 16;
+}
+
 // C[M x N] = A[M x K] B[N x K]^T with A (lda) and B (ldb) row-major bf16.
 Gemm plan_gemm(int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb, int* err) {
   if (M <= 0 || N < 16 || N > umma::kMaxN || N % 16 || K < 16 || K % 16)
     throw Error(POFD_E_ARG, "gemm: need N in [16, 512] and K >= 16, both multiples of 16");
   Gemm q;
-  const int nt = umma::pick_ntile(N);
+  const int nt = ntile_for(M, N);
   q.g = umma::GemmShape{M, N, K, nt, err};
   q.a = kmajor_map(A, M, K, lda, umma::kRows);
   q.b = kmajor_map(B, N, K, ldb, nt);
@@ -626,7 +644,7 @@ void Surrogate::predict(unsigned n, const float* theta, unsigned npar, double* o
   if (!st) st = stream_;
   forward(static_cast<int>(n), theta, static_cast<int>(npar), nullptr, false, st);
   const int Mp = (static_cast<int>(n) + umma::kRows - 1) / umma::kRows * umma::kRows;
-  const int ntiles = static_cast<int>(H_) / umma::pick_ntile(static_cast<int>(H_));
+  const int ntiles = static_cast<int>(H_) / ntile_for(Mp, static_cast<int>(H_));
   k_unscale<<<(n + 127) / 128, 128, 0, st>>>(static_cast<int>(n), Mp, ntiles, ws_.ypart, ymax_, ys_,
                                              out, status);
   ck(cudaGetLastError(), "k_unscale");
@@ -722,7 +740,7 @@ float Surrogate::iteration(int Mb, const int* rows, float lr, float** grads, cud
   k_gather_targets<<<(Mb + 127) / 128, 128, 0, st>>>(Mb, rows, plogl_, ymax_, clip_, 1.0 / ys_,
                                                      ws_.t);
   ck(cudaMemsetAsync(ws_.loss, 0, sizeof(float), st), "memset");
-  const int ntiles = H / umma::pick_ntile(H);
+  const int ntiles = H / ntile_for(Mp, H);
   k_out_loss<<<(Mp + 127) / 128, 128, 0, st>>>(Mb, Mp, ntiles, ws_.ypart, ws_.t, ws_.y, ws_.dy,
                                                ws_.loss);
   {
