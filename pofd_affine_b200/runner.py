@@ -147,7 +147,7 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=150, plain_control=False,
     several hundred log-likelihood units below it), a 1e-3 ball around it
     and npre plain steps.  Each run then burns nburn steps and records
     nsteps.  With plain_control a second plain run (another seed) gives the
-    plain-vs-plain agreement the DA-vs-plain agreement is judged against."""
+    plain-vs-plain agreement the DA-vs-plain agreement is compared with."""
     from . import synth
     from .mcmc import affineEnsemble, likeSum
     from .surrogate import Surrogate
