@@ -57,7 +57,9 @@ SIGNATURES = {
     "pofd_like1_dataset_info": (I, [V, I, I, _dp, V]),
     "pofd_like1_reserve": (I, [V, U]),
     "pofd_like1_loglike": (I, [V, _fp, U, C.POINTER(D), C.POINTER(I)]),
-    "pofd_like1_eval_batch": (I, [V, U, _fp, U, _dp, _ip]),
+    # the batch calls take raw pointers: the arrays are made contiguous and
+    # typed by the caller, and ndpointer's checks cost microseconds per call
+    "pofd_like1_eval_batch": (I, [V, U, V, U, V, V]),
     "pofd_like1_eval_batch_device": (I, [V, U, V, U, V, V, V]),
     "pofd_like1_pd": (I, [V, I, I, _fp, U, I, _dp, V]),
     "pofd_like1_rnodes": (I, [V, I, I, _fp, U, _dp, _dp]),
@@ -95,7 +97,7 @@ SIGNATURES = {
     "pofd_like2_dataset_info": (I, [V, I, I, _dp, V]),
     "pofd_like2_reserve": (I, [V, U]),
     "pofd_like2_loglike": (I, [V, _fp, U, C.POINTER(D), C.POINTER(I)]),
-    "pofd_like2_eval_batch": (I, [V, U, _fp, U, _dp, _ip]),
+    "pofd_like2_eval_batch": (I, [V, U, V, U, V, V]),
     "pofd_like2_eval_batch_device": (I, [V, U, V, U, V, V, V]),
     "pofd_like2_pd": (I, [V, I, I, _fp, U, I, _dp, V]),
     "pofd_like2_get_r": (I, [V, I, _fp, U, _dp]),

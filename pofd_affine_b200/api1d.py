@@ -274,8 +274,8 @@ class calcLike:
         nprop, npar = th.shape
         ll = np.empty(nprop)
         st = np.empty(nprop, dtype=np.int32)
-        check(lib().pofd_like1_eval_batch(self.h, nprop, th.ravel(), npar, ll,
-                                          st))
+        check(lib().pofd_like1_eval_batch(self.h, nprop, th.ctypes.data, npar,
+                                          ll.ctypes.data, st.ctypes.data))
         return ll, st
 
     def getLogLikeDevice(self, nprop, theta_ptr, npar, logl_ptr, status_ptr,

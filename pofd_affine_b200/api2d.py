@@ -203,11 +203,13 @@ class calcLikeDouble:
 
     def getLogLikeBatch(self, thetas):
         th = _f32(thetas)
+        if th.ndim != 2:
+            raise PofdError(-10, "thetas must be [nprop, npar]")
         nprop, npar = th.shape
         ll = np.empty(nprop)
         st = np.empty(nprop, dtype=np.int32)
-        check(lib().pofd_like2_eval_batch(self.h, nprop, th.ravel(), npar, ll,
-                                          st))
+        check(lib().pofd_like2_eval_batch(self.h, nprop, th.ctypes.data, npar,
+                                          ll.ctypes.data, st.ctypes.data))
         return ll, st
 
     # priors per band (calcLikeDouble.h:310-341); band 0 or 1
