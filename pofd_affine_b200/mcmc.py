@@ -295,6 +295,17 @@ class affineEnsemble:
             self.h, np.ascontiguousarray(z["naccept"], np.uint32)))
         self.nsteps_done = int(z["nsteps_done"])
 
+    def writeChain(self, path, param_names=None, **metadata):
+        """The recorded chain with its likelihoods, the parameter states,
+        the acceptance fractions and acor lengths, in the reference's output
+        layout (affineEnsemble::writeToHDF5), as .npz (stats.writeChain)."""
+        from .stats import writeChain
+        th, ll = self.getChain()
+        tau = self.getAcor()[0] if self.nRecorded() > 1 else np.full(self.nparams, np.nan)
+        writeChain(path, th, ll, param_names=param_names, param_states=self.state,
+                   acceptance=self.getAcceptanceFrac(), acor=tau,
+                   nsteps_done=self.nsteps_done, **metadata)
+
     def getAcceptanceFrac(self):
         return self.getNAccept() / max(self.nsteps_done, 1)
 

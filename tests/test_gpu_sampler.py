@@ -182,6 +182,14 @@ def test_checkpoint_resume_continues_the_chain_exactly(gpu_ctx, tmp_path):
     assert np.array_equal(ta, tc)
     assert np.array_equal(la, lc)
     assert np.array_equal(A.getNAccept(), C2.getNAccept())
+    # the recorded chain written in the reference's layout and read back
+    from pofd_affine_b200 import stats
+    A.writeChain(str(tmp_path / "chain.npz"), param_names=["a", "b", "c", "d"])
+    back = stats.readChain(str(tmp_path / "chain.npz"))
+    th, ll = A.getChain()
+    assert np.array_equal(back["chain"], th) and np.array_equal(back["likelihood"], ll)
+    assert np.allclose(back["acceptance"], A.getAcceptanceFrac())
+    assert list(back["param_names"]) == ["a", "b", "c", "d"]
     D = affineEnsemble(gpu_ctx, G, 24, 4, seed=1)
     from pofd_affine_b200 import PofdError
     with pytest.raises(PofdError, match="seed"):
