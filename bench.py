@@ -116,13 +116,17 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------- CPU baseline
-def cpu_baseline(cfg, seconds, nthreads=None):
-    """The oracle port of the reference path (calcLike::getLogLike per
-    proposal) on the host cores, thread farm over proposals."""
+CPU_FFT = ("radix-4 Stockham real FFT (oracle/fastfft.cc, AVX2/FMA clone "
+           "when the CPU has it), the counterpart of the reference's "
+           "FFTW_MEASURE plans")
+
+
+def _oracle1(cfg):
+    """The oracle's calcLike for the 1D workload, with the fast transforms
+    of the timed CPU baseline switched on."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    from pofd_affine_b200 import synth
-    nthreads = nthreads or os.cpu_count() or 1
+    pyoracle.set_fast_fft(True)
     O = pyoracle.Like1(cfg["knotpos"], cfg["fftsize"], cfg["ninterp"], True,
                        cfg["nbins"])
     for b in cfg["beams"]:
@@ -130,7 +134,42 @@ def cpu_baseline(cfg, seconds, nthreads=None):
     for m, bi, s in zip(cfg["maps"], cfg["map_beam"], cfg["sigmas"]):
         O.add_dataset(bi, m, s)
     O.set_rranges(cfg["theta0"])
+    return O
+
+
+def cpu_fft_share(O, cfg, th, reps=4):
+    """Share of one single-threaded CPU evaluation spent in the real
+    transforms: one forward per beam set and one inverse per dataset, timed
+    alone, against the evaluation."""
+    import pyoracle
+    n = cfg["fftsize"]
+    x = np.random.default_rng(0).normal(size=n)
+    X = np.fft.rfft(x)
+    nb, nd = len(cfg["beams"]), len(cfg["maps"])
+    O.loglike_batch(th[:1], 1)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.loglike_batch(th[:1], 1)
+    t_eval = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for _ in range(nb):
+            pyoracle.rfft(x)
+        for _ in range(nd):
+            pyoracle.irfft(X, n)
+    t_fft = (time.perf_counter() - t0) / reps
+    return {"eval_ms_1thread": 1e3 * t_eval, "fft_ms": 1e3 * t_fft,
+            "fft_share": t_fft / t_eval}
+
+
+def cpu_baseline(cfg, seconds, nthreads=None):
+    """The oracle port of the reference path (calcLike::getLogLike per
+    proposal) on the host cores, thread farm over proposals."""
+    from pofd_affine_b200 import synth
+    nthreads = nthreads or os.cpu_count() or 1
+    O = _oracle1(cfg)
     th = synth.proposals(cfg["theta0"], 4 * nthreads, 0.02, rng=99)
+    share = cpu_fft_share(O, cfg, th)
     O.loglike_batch(th[:nthreads], nthreads)  # builds the thread copies
     done, t0 = 0, time.perf_counter()
     while True:
@@ -140,11 +179,11 @@ def cpu_baseline(cfg, seconds, nthreads=None):
         if el >= seconds:
             break
     return {"value": done / el, "unit": "evals/s", "cores": nthreads,
-            "kind": "port",
+            "kind": "port", "fft": CPU_FFT, "fft_share_1thread": share,
             "sample": "%d proposals of the workload in %.1f s on %d threads "
-                      "(oracle restatement of the reference CPU path; the "
-                      "reference needs GSL/FFTW/cfitsio/HDF5/MPI, absent "
-                      "here)" % (done, el, nthreads)}
+                      "(oracle restatement of the reference CPU path with a "
+                      "%s; the reference needs GSL/FFTW/cfitsio/HDF5/MPI, "
+                      "absent here)" % (done, el, nthreads, CPU_FFT)}
 
 
 def reference_arm(a, cfg):
@@ -152,16 +191,8 @@ def reference_arm(a, cfg):
     if rank != 0:
         return
     cpu = os.cpu_count() or 1
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle
     from pofd_affine_b200 import synth
-    O = pyoracle.Like1(cfg["knotpos"], cfg["fftsize"], cfg["ninterp"], True,
-                       cfg["nbins"])
-    for b in cfg["beams"]:
-        O.add_beamset(b, cfg["pixsize"], 1e-5, True, cfg["nbeamhist"])
-    for m, bi, s in zip(cfg["maps"], cfg["map_beam"], cfg["sigmas"]):
-        O.add_dataset(bi, m, s)
-    O.set_rranges(cfg["theta0"])
+    O = _oracle1(cfg)
     per_step = 2 * cpu  # bounded sample per step
     th = synth.proposals(cfg["theta0"], per_step, 0.02, rng=99)
     for _ in range(a.warmup):
@@ -180,10 +211,11 @@ def reference_arm(a, cfg):
                        "proposals_per_step": per_step},
             "cpu_baseline": {"value": v, "unit": "evals/s", "cores": cpu,
                              "kind": "port",
+                             "fft": CPU_FFT,
                              "sample": "%d proposals per step, %d steps, %d "
                                        "threads (oracle restatement of the "
-                                       "reference CPU path)"
-                                       % (per_step, a.steps, cpu)},
+                                       "reference CPU path, %s)"
+                                       % (per_step, a.steps, cpu, CPU_FFT)},
             "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -304,6 +336,7 @@ def cpu_baseline_2d(cfg, seconds, nthreads=None):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from pofd_affine_b200 import synth
+    pyoracle.set_fast_fft(True)
     nthreads = nthreads or os.cpu_count() or 1
     O = pyoracle.Like2(cfg["knotpos"], cfg["sigmapos"], cfg["offsetpos"],
                        cfg["fftsize"], cfg["nedge"], True, cfg["nbins"])
@@ -324,9 +357,10 @@ def cpu_baseline_2d(cfg, seconds, nthreads=None):
             break
     return {"value": done / el, "unit": "evals/s", "cores": nthreads,
             "kind": "port",
+            "fft": CPU_FFT,
             "sample": "%d proposals of the 2D workload in %.1f s on %d "
-                      "threads (oracle restatement of the reference CPU path)"
-                      % (done, el, nthreads)}
+                      "threads (oracle restatement of the reference CPU path, "
+                      "%s)" % (done, el, nthreads, CPU_FFT)}
 
 
 def measure_2d(a, ctx, stream):

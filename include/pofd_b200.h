@@ -336,6 +336,15 @@ const char* pofd_like2_stage_name_now(const pofd_like2* L, int i);
 int pofd_like2_set_fft(pofd_like2* L, int mode);
 int pofd_like2_fft_info(const pofd_like2* L, int* fused);
 
+/* Summation order of the 2D normalisation and means (PDDouble::getIntegral,
+ * normalize and getMeans, PDDouble.cc:142-208, 355-447).  0 (default): tree
+ * sums, exact to ~1e-16 relative.  1: one sequential chain each in the
+ * reference's row-major order with every operation rounded separately, so
+ * the result carries the reference's own rounding (a few 1e-12 relative at
+ * n = 2048, ~1e-5 in a log-likelihood over 2.25 M pixels).  Mode 1 is slow
+ * (a 2 n^2-long dependent chain per dataset) and meant for parity checks. */
+int pofd_like2_set_reference_sums(pofd_like2* L, int on);
+
 /* Priors per band (band 0 or 1), added once to the summed log-likelihood in
  * the reference's order (calcLikeDouble.cc:1236-1276): Gaussians on the
  * sigma multipliers about 1, on <S_b> and on <S_b^2>, then alpha times the
@@ -373,8 +382,12 @@ int pofd_like2_fill_bonus_device(pofd_like2* L, unsigned nprop, float* theta_dev
  * cudaStream_t; NULL = the legacy default stream) of the current device; the
  * call returns after enqueueing.  Its scratch is a fixed static device array
  * shared by all calls (one per GPU, held until exit): calls that overlap on
- * the GPU race, so serialise them.  The first call on a device looks the
- * array up with cudaGetSymbolAddress; make it before any stream capture. */
+ * the GPU race, so serialise them.  Each call made outside stream capture
+ * looks the array's device address up with cudaGetSymbolAddress (so a
+ * device reset, which moves the array, is harmless); a call made while its
+ * stream is capturing uses the address of the last uncaptured call on that
+ * device, so make one call before any stream capture, and none across a
+ * device reset inside a capture. */
 int pofd_pd1_loglike_noalloc(const double* pofd_dev, unsigned n, double dflux,
                              double minflux_R, unsigned wrapRidx,
                              double var_noi, double sigma,
@@ -528,6 +541,10 @@ int pofd_surrogate_add_pairs(pofd_surrogate* s, unsigned n,
                              const double* logl_dev, const int* status_dev,
                              void* stream);
 int pofd_surrogate_npairs(pofd_surrogate* s, unsigned* n);
+/* The first n training pairs held, in buffer order, into host arrays
+ * theta_out [n][nparams] and logl_out [n] (either may be NULL). */
+int pofd_surrogate_get_pairs(pofd_surrogate* s, unsigned n, float* theta_out,
+                             double* logl_out);
 /* iters Adam steps (lr, beta 0.9/0.999) on minibatches of batch pairs drawn
  * with replacement; the scaling is refreshed from the pairs first. */
 int pofd_surrogate_train(pofd_surrogate* s, unsigned iters, unsigned batch,

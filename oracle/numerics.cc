@@ -2,8 +2,11 @@
 // TEST INFRASTRUCTURE ONLY (see pofd_oracle.h and numerics.hh).
 #include "numerics.hh"
 
+#include <atomic>
 #include <map>
 #include <mutex>
+
+#include "fastfft.hh"
 
 namespace orc {
 
@@ -88,7 +91,15 @@ void cfft_strided(cplx* a, size_t n, size_t stride, int sign,
   for (size_t i = 0; i < n; ++i) a[i * stride] = work[i];
 }
 
+namespace {
+std::atomic<bool> g_fast_fft{false};
+}
+
+void set_fast_fft(bool on) { g_fast_fft.store(on); }
+bool fast_fft() { return g_fast_fft.load(); }
+
 void rfft(size_t n, const double* in, cplx* out) {
+  if (fast_fft() && fastfft_supported(n)) return rfft_fast(n, in, out);
   std::vector<cplx> a(n);
   for (size_t i = 0; i < n; ++i) a[i] = cplx(in[i], 0.0);
   fft_any(a.data(), n, -1);
@@ -96,6 +107,7 @@ void rfft(size_t n, const double* in, cplx* out) {
 }
 
 void irfft(size_t n, const cplx* in, double* out) {
+  if (fast_fft() && fastfft_supported(n)) return irfft_fast(n, in, out);
   const size_t nc = n / 2 + 1;
   std::vector<cplx> a(n);
   a[0] = cplx(in[0].real(), 0.0);
@@ -109,6 +121,7 @@ void irfft(size_t n, const cplx* in, double* out) {
 }
 
 void rfft2(size_t n, const double* in, cplx* out) {
+  if (fast_fft() && fastfft_supported(n)) return rfft2_fast(n, in, out);
   const size_t nc = n / 2 + 1;
   std::vector<cplx> row(n), work;
   for (size_t i = 0; i < n; ++i) {
@@ -120,6 +133,7 @@ void rfft2(size_t n, const double* in, cplx* out) {
 }
 
 void irfft2(size_t n, const cplx* in, double* out) {
+  if (fast_fft() && fastfft_supported(n)) return irfft2_fast(n, in, out);
   const size_t nc = n / 2 + 1;
   std::vector<cplx> a(in, in + n * nc), work;
   // Hermitian projection of the self-conjugate columns.

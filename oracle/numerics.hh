@@ -131,6 +131,11 @@ void cfft(std::vector<cplx>& a, int sign);
 void cfft_strided(cplx* a, size_t n, size_t stride, int sign,
                   std::vector<cplx>& work);
 // Real forward: out has n/2+1 entries.
+// Process-wide switch (default off): route the real transforms below to
+// the fast radix-4 ones of fastfft.hh for powers of two >= 8.  For the
+// timed CPU baseline; the parity checks keep the radix-2 transforms.
+void set_fast_fft(bool on);
+bool fast_fft();
 void rfft(size_t n, const double* in, cplx* out);
 // Real inverse (c2r), unnormalised.  The DC and (even n) Nyquist bins are
 // taken by their real parts, which is how an FFTW-style c2r treats them.

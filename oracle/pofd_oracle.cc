@@ -2093,6 +2093,10 @@ int orc_cspline_eval(int n, const double* x, const double* y, int m,
   });
 }
 
+int orc_set_fast_fft(int on) {
+  set_fast_fft(on != 0);
+  return 0;
+}
 int orc_rfft(int n, const double* in, double* out_c) {
   return guard([&] { rfft(n, in, reinterpret_cast<cplx*>(out_c)); });
 }

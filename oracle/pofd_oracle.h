@@ -31,6 +31,10 @@ const char* orc_last_error(void);
 /* ---- numerics building blocks (for self-tests) ---- */
 int orc_cspline_eval(int n, const double* x, const double* y, int m,
                      const double* xq, double* out);
+/* Transforms of the oracle: 0 (default) radix-2, the parity form; 1 the
+ * fast radix-4 real transforms (fastfft.hh) for powers of two >= 8, used by
+ * the timed CPU baseline.  Process-wide. */
+int orc_set_fast_fft(int on);
 int orc_rfft(int n, const double* in, double* out_c /* 2*(n/2+1) */);
 int orc_irfft(int n, const double* in_c, double* out);
 int orc_rfft2(int n, const double* in, double* out_c /* 2*n*(n/2+1) */);

@@ -37,6 +37,7 @@ def lib():
     sigs = {
         "orc_last_error": (C.c_char_p, []),
         "orc_cspline_eval": (I, [I, _dp, _dp, I, _dp, _dp]),
+        "orc_set_fast_fft": (I, [I]),
         "orc_rfft": (I, [I, _dp, _dp]),
         "orc_irfft": (I, [I, _dp, _dp]),
         "orc_rfft2": (I, [I, _dp, _dp]),
@@ -130,6 +131,13 @@ def cspline_eval(x, y, xq):
     out = np.empty_like(xq)
     _chk(lib().orc_cspline_eval(len(x), x, y, len(xq), xq, out))
     return out
+
+
+def set_fast_fft(on):
+    """Route the oracle's real transforms (powers of two >= 8) to the fast
+    radix-4 transforms (oracle/fastfft.hh) -- for the timed CPU baseline --
+    or back to the radix-2 parity form.  Process-wide."""
+    _chk(lib().orc_set_fast_fft(1 if on else 0))
 
 
 def rfft(a):

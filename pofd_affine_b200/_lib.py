@@ -106,6 +106,7 @@ SIGNATURES = {
     "pofd_like2_stage_name": (C.c_char_p, [I]),
     "pofd_like2_stage_name_now": (C.c_char_p, [V, I]),
     "pofd_like2_set_fft": (I, [V, I]),
+    "pofd_like2_set_reference_sums": (I, [V, I]),
     "pofd_like2_fft_info": (I, [V, C.POINTER(I)]),
     "pofd_pd1_loglike_noalloc": (I, [V, U, D, D, U, D, D, V, V, U, D, D, D, D,
                                      V, V, V]),
@@ -135,6 +136,7 @@ SIGNATURES = {
     "pofd_surrogate_destroy": (I, [V]),
     "pofd_surrogate_add_pairs": (I, [V, U, V, U, V, V, V]),
     "pofd_surrogate_npairs": (I, [V, C.POINTER(U)]),
+    "pofd_surrogate_get_pairs": (I, [V, U, V, V]),
     "pofd_surrogate_train": (I, [V, U, U, C.c_float, C.POINTER(C.c_float)]),
     "pofd_surrogate_predict_device": (I, [V, U, V, U, V, V, V]),
     "pofd_surrogate_get_params": (I, [V, I, V, C.POINTER(S)]),

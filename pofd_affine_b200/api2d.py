@@ -307,6 +307,12 @@ class calcLikeDouble:
         them."""
         check(lib().pofd_like2_set_fft(self.h, int(mode)))
 
+    def setReferenceSums(self, on):
+        """Sum the P(D) integral and means in the reference's sequential
+        row-major order (PDDouble.cc:142-208, 355-447) instead of the
+        default tree sums; slow, for parity checks."""
+        check(lib().pofd_like2_set_reference_sums(self.h, 1 if on else 0))
+
     def fusedColumns(self):
         """True when the fused column path is the one in use."""
         k = C.c_int()

@@ -866,6 +866,14 @@ int pofd_like2_set_fft(pofd_like2* L, int mode) {
   });
 }
 
+int pofd_like2_set_reference_sums(pofd_like2* L, int on) {
+  return guard([&] {
+    need(L != nullptr, "null argument");
+    L->eng->set_reference_sums(on != 0);
+    return POFD_OK;
+  });
+}
+
 int pofd_like2_fft_info(const pofd_like2* L, int* fused) {
   return guard([&] {
     need(L && fused, "null argument");
@@ -1155,6 +1163,15 @@ int pofd_surrogate_npairs(pofd_surrogate* s, unsigned* n) {
   return guard([&] {
     need(s && n, "null argument");
     *n = s->s->npairs();
+    return POFD_OK;
+  });
+}
+
+int pofd_surrogate_get_pairs(pofd_surrogate* s, unsigned n, float* theta_out,
+                             double* logl_out) {
+  return guard([&] {
+    need(s != nullptr, "null argument");
+    s->s->pairs_host(n, theta_out, logl_out);
     return POFD_OK;
   });
 }

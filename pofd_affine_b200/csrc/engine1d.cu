@@ -323,6 +323,88 @@ struct GridFill1 {
     var += cf * prod;
     return r;
   }
+
+  // R at the 16 consecutive grid indices i0 .. i0 + 15 (i0 a multiple of
+  // 16) into out[0..7] as complex pairs (R_i0 + i R_i0+1, ...), with their
+  // moment terms; R at index iw is also stored to Rrow.  When all 16 points
+  // lie in one node interval of one side, the cubic exponent v(t) of point
+  // i0 + t has constant third differences, so 2^v follows from three running
+  // products: R(t+1) = R(t) E1(t), E1(t+1) = E1(t) E2(t), E2(t+1) = E2(t) E3
+  // with E1(0) = 2^(v(1) - v(0)), E2(0) = 2^(second difference), E3 =
+  // 2^(third difference), the differences taken analytically from the
+  // cubic -- four exp2 per segment instead of sixteen, and no per-point
+  // cubic or table lookup.  The running products add at most ~16^3/6
+  // roundings (< 1e-13 relative) to each value.  Other segments (interval or
+  // side changes, uncovered points) evaluate every point directly.
+  __device__ __forceinline__ void segment16(int i0, const int* __restrict__ gidx, double2* out,
+                                            double& mn, double& var, int iw,
+                                            double* Rrow) const {
+    int q[16];
+    {
+      const int4* g4 = reinterpret_cast<const int4*>(gidx + i0);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int4 g = __ldg(g4 + k);
+        q[4 * k] = g.x;
+        q[4 * k + 1] = g.y;
+        q[4 * k + 2] = g.z;
+        q[4 * k + 3] = g.w;
+      }
+    }
+    bool uni = q[0] >= 0 && (i0 > wrap) == (i0 + 15 > wrap);
+#pragma unroll
+    for (int k = 1; k < 16; ++k) uni = uni && (q[k] == q[0]);
+    if (uni) {
+      const bool neg = i0 > wrap;
+      const double2* S = reinterpret_cast<const double2*>(S0 + (neg ? 4 * NI : 0)) + 2 * q[0];
+      const double2 yb = S[0], cd = S[1];
+      const double h = dflux;
+      const double d0 = __dadd_rn(__dmul_rn(static_cast<double>(i0), dflux), neg ? off1 : off0) -
+                        (neg ? x1 : x0)[q[0]];
+      const double v0 = yb.x + d0 * (yb.y + d0 * (cd.x + d0 * cd.y));
+      const double D1 = h * (yb.y + cd.x * (2.0 * d0 + h) + cd.y * (3.0 * d0 * (d0 + h) + h * h));
+      const double D2 = h * h * (2.0 * cd.x + 6.0 * cd.y * (d0 + h));
+      const double D3 = 6.0 * cd.y * h * h * h;
+      // (exponents far outside the P(D) range go point by point, as does a
+      // segment whose values would leave the double range)
+      if (fabs(v0) < 500.0 && fabs(D1) < 16.0 && fabs(D2) < 4.0 && fabs(D3) < 2.0) {
+        double R = dev::exp2_tab(v0, e2) * dflux;
+        double E1 = dev::exp2_tab(D1, e2), E2 = dev::exp2_tab(D2, e2);
+        const double E3 = dev::exp2_tab(D3, e2);
+        double rv[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          rv[k] = R;
+          R *= E1;
+          E1 *= E2;
+          E2 *= E3;
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int i = i0 + k;
+          const double cf = neg ? static_cast<double>(i - wrap - 1) * dflux + minflux_R
+                                : __dmul_rn(static_cast<double>(i), dflux);
+          double prod = cf * rv[k];
+          if (i == wrap) prod *= 0.5;
+          mn += prod;
+          var += cf * prod;
+          if (i == iw) Rrow[i] = rv[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) out[k] = make_double2(rv[2 * k], rv[2 * k + 1]);
+        return;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = i0 + 2 * k;
+      const double r0 = point(i, static_cast<double>(i), q[2 * k], mn, var);
+      const double r1 = point(i + 1, static_cast<double>(i + 1), q[2 * k + 1], mn, var);
+      if (i == iw) Rrow[i] = r0;
+      if (i + 1 == iw) Rrow[i + 1] = r1;
+      out[k] = make_double2(r0, r1);
+    }
+  }
 };
 
 // The R grid materialised (cuFFT path, and the own path when the fill is
@@ -599,7 +681,18 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
 // wrap - 1, which k_moments1 needs for its edge term, is stored at its place
 // in rbuf -- pass B overwrites rbuf with the spectrum only after
 // k_moments1 has read it.
+//
+// INC: the block first evaluates its whole tile (M1 rows of 2 CB
+// consecutive grid points) in segments of 16 points with
+// GridFill1::segment16 into a padded shared-memory tile (row stride CB + 1
+// complex values, bank-conflict free for both the segment writes and the
+// column reads), then reads its DFT inputs from there.
 template <int L1, int L2>
+__host__ __device__ constexpr int fftAR_tile() {
+  return (L1 * L2) * (256 / L2 + 1) > 256 * L1 ? (L1 * L2) * (256 / L2 + 1) : 256 * L1;
+}
+
+template <int L1, int L2, bool INC>
 __global__ void __launch_bounds__(256, 2)
 k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
         const int* __restrict__ mstatus, const double* __restrict__ spl,
@@ -611,10 +704,11 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
   constexpr int m = M1 * M2;
   constexpr int CB = 256 / L2;
   constexpr int NH = m / 128;
+  constexpr int CBP = CB + 1;  // padded tile row (INC)
   extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L
   __shared__ dev::Exp2Table e2;
   __shared__ double shr[32];
-  double2* Hs = fs + 256 * L1;
+  double2* Hs = fs + (INC ? fftAR_tile<L1, L2>() : 256 * L1);
   const double2* Ls = Hs + NH;
   double2* Ts = Hs + NH + 128;  // inter-stage twiddles W_m^{(m / M1) n2 k1}
   const int row = blockIdx.y;
@@ -634,18 +728,37 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
   double2* dst = out + static_cast<size_t>(row) * rowsz;
   double mn = 0.0, var = 0.0;
   double2 v[L1];
+  if (INC) {
+    // the tile in segments of 16 grid points (8 complex inputs): row a of
+    // the m1 x 256 view holds grid indices 2 (a 256 + b0) .. + 2 CB - 1
+    constexpr int SPR = CB / 8;  // segments per tile row
+    for (int sgi = t; sgi < M1 * SPR; sgi += 256) {
+      const int a = sgi % M1, g = sgi / M1;
+      double2 o[8];
+      rg.segment16(2 * (a * M2 + b0) + 16 * g, gidx, o, mn, var, iw, Rrow);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) fs[a * CBP + 8 * g + k] = o[k];
+    }
+    __syncthreads();
+  }
   {
     const int b = t % CB, n2 = t / CB;
+    if (INC) {
 #pragma unroll
-    for (int n1 = 0; n1 < L1; ++n1) {
-      const int i = 2 * ((L2 * n1 + n2) * M2 + b0 + b);
-      const int2 q = __ldg(reinterpret_cast<const int2*>(gidx + i));
-      const double di = static_cast<double>(i);
-      const double r0 = rg.point(i, di, q.x, mn, var);
-      const double r1 = rg.point(i + 1, di + 1.0, q.y, mn, var);
-      if (i == iw) Rrow[i] = r0;
-      if (i + 1 == iw) Rrow[i + 1] = r1;
-      v[n1] = make_double2(r0, r1);
+      for (int n1 = 0; n1 < L1; ++n1) v[n1] = fs[(L2 * n1 + n2) * CBP + b];
+      __syncthreads();  // the tile is overwritten by the exchange below
+    } else {
+#pragma unroll
+      for (int n1 = 0; n1 < L1; ++n1) {
+        const int i = 2 * ((L2 * n1 + n2) * M2 + b0 + b);
+        const int2 q = __ldg(reinterpret_cast<const int2*>(gidx + i));
+        const double di = static_cast<double>(i);
+        const double r0 = rg.point(i, di, q.x, mn, var);
+        const double r1 = rg.point(i + 1, di + 1.0, q.y, mn, var);
+        if (i == iw) Rrow[i] = r0;
+        if (i + 1 == iw) Rrow[i + 1] = r1;
+        v[n1] = make_double2(r0, r1);
+      }
     }
     fft::dft<L1, -1>(v);
     if (L2 > 1) {
@@ -1663,14 +1776,28 @@ void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const in
 #undef POFD_FFTA
 }
 
-// Fused R fill + forward pass A; returns the tiles per row (partial
-// moment sums per row in rpart).
+// Shared memory of the incremental fused fill: the padded tile replaces
+// the exchange area where it is larger.
+inline size_t fftAR_inc_smem(int m1) {
+  const size_t l1 = m1 < 16 ? m1 : 16, l2 = m1 < 16 ? 1 : m1 / 16;
+  const size_t tile = std::max(static_cast<size_t>(m1) * (256 / l2 + 1), 256 * l1);
+  return (tile + 2 * m1 + 128 + 256) * sizeof(double2);
+}
+// largest at m1 = 256 (tile 256 x 17)
+constexpr size_t kFftARIncSmemMax = (256 * 17 + 2 * 256 + 128 + 256) * sizeof(double2);
+
+// Fused R fill + forward pass A (inc: segment-wise running products);
+// returns the tiles per row (partial moment sums per row in rpart).
 int launch_fftAR(int m1, int rows, cudaStream_t st, const BSet1Dev* bsets, int B, int NI,
                  int rowsz, const int* mstatus, const double* spl, double* rbuf, double* rpart,
-                 double2* out, const double2* WH, const double2* WL) {
-#define POFD_FFTAR(L1, L2)                                                                 \
-  k_fftAR<L1, L2><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(bsets, B, NI, rowsz, mstatus, \
-                                                              spl, rbuf, rpart, out, WH, WL); \
+                 double2* out, const double2* WH, const double2* WL, bool inc) {
+#define POFD_FFTAR(L1, L2)                                                                  \
+  if (inc)                                                                                  \
+    k_fftAR<L1, L2, true><<<dim3(L2, rows), 256, fftAR_inc_smem(m1), st>>>(                 \
+        bsets, B, NI, rowsz, mstatus, spl, rbuf, rpart, out, WH, WL);                       \
+  else                                                                                      \
+    k_fftAR<L1, L2, false><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(                     \
+        bsets, B, NI, rowsz, mstatus, spl, rbuf, rpart, out, WH, WL);                       \
   return L2
   switch (m1) {
     case 8: POFD_FFTAR(8, 1);
@@ -1684,14 +1811,19 @@ int launch_fftAR(int m1, int rows, cudaStream_t st, const BSet1Dev* bsets, int B
 #undef POFD_FFTAR
 }
 
+template <bool INC>
+void fftAR_attr_one() {
+  const int sm = static_cast<int>(INC ? std::max(kFftARIncSmemMax, kFftASmemMax) : kFftASmemMax);
+  cuda_check(cudaFuncSetAttribute(k_fftAR<8, 1, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 1, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 4, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 8, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 16, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+}
 void fftAR_attr() {
-  const int sm = static_cast<int>(kFftASmemMax);
-  cuda_check(cudaFuncSetAttribute(k_fftAR<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  fftAR_attr_one<false>();
+  fftAR_attr_one<true>();
 }
 
 template <int S>
@@ -2235,7 +2367,7 @@ void Engine1::set_tuning(const Tune1& t) {
     throw Error(POFD_E_ARG, "rnodes_threads must be 64, 128 or 256");
   if (t.spec_blocks < 1 || t.spec_blocks > 64) throw Error(POFD_E_ARG, "spec_blocks must be in [1, 64]");
   if (t.fft_persist < 0 || t.fft_persist > 2) throw Error(POFD_E_ARG, "fft_persist must be 0, 1 or 2");
-  if (t.rfill_fused != 0 && t.rfill_fused != 1) throw Error(POFD_E_ARG, "rfill_fused must be 0 or 1");
+  if (t.rfill_fused < 0 || t.rfill_fused > 2) throw Error(POFD_E_ARG, "rfill_fused must be 0, 1 or 2");
   const bool fft_changed = (t.own_fft != 0) != (tune_.own_fft != 0);
   tune_ = t;
   tune_.own_fft = t.own_fft ? 1 : 0;
@@ -2281,9 +2413,12 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     trial(t);
   }
   if (best.own_fft && own_possible) {
-    Tune1 t = best;
-    t.rfill_fused = best.rfill_fused ? 0 : 1;
-    trial(t);
+    for (int rf : {0, 1, 2}) {
+      if (rf == best.rfill_fused) continue;
+      Tune1 t = best;
+      t.rfill_fused = rf;
+      trial(t);
+    }
   }
   if (best.own_fft && own_possible) {
     for (int fp : {0, 1, 2}) {
@@ -2571,7 +2706,7 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
     if (fused) {
       // R fill inside the forward pass A: the grid goes straight into tmp
       ntile = launch_fftAR(m1, P * B, st, d_bsets_, B, NI, rowsz, ws_.mstatus, ws_.spl,
-                           ws_.rbuf, ws_.rpart, tmp, d_wh_, d_wl_);
+                           ws_.rbuf, ws_.rpart, tmp, d_wh_, d_wl_, tune_.rfill_fused == 2);
     } else {
       dim3 grid(ntile_, P * B);
       launch_rfill(tune_.rfill_per, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),

@@ -135,8 +135,10 @@ struct Tune1 {
   int fft_persist = 0;      // 0: plain FFT passes; 1: persistent passes that
                             // prefetch into registers (m1 >= 16); 2: pass B
                             // fed by bulk copies through a shared-memory ring
-  int rfill_fused = 1;      // R grid fill inside the forward pass A (own FFT,
-                            // not with fft_persist = 1)
+  int rfill_fused = 2;      // R grid fill inside the forward pass A (own FFT,
+                            // not with fft_persist = 1): 0 no, 1 one exp2
+                            // per grid point, 2 running products over
+                            // segments of 16 points in one node interval
 };
 
 class Engine1 {

@@ -936,6 +936,120 @@ k_psplit2(const BSet2Dev* __restrict__ bsets,
   }
 }
 
+// Reference-order sums (opt-in): PDDouble::getIntegral, normalize and
+// getMeans (PDDouble.cc:142-208, 355-447) as one sequential chain each over
+// the rotated, clipped P(D) in row-major order, every product and sum
+// rounded separately (no fused multiply-add), as the reference's host build
+// evaluates them.  Overwrites itot and the two minflux values k_psplit2 left
+// in pinfo; the split indices are kept.  One block per (proposal, dataset):
+// the block stages one rotated row in shared memory and thread 0 walks it.
+// The tree sums of k_psplit2 are exact to ~1e-16 relative; the sequential
+// chain is not (its rounding grows with n^2), and at n = 2048 the
+// difference moves a log-likelihood over millions of pixels by ~1e-5.  Slow
+// (a 2n^2-long dependent chain per dataset): for parity checks, not for
+// sampling.
+__global__ void __launch_bounds__(NT)
+k_pseq2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dsets,
+        int D, int n, int nc2, const int* __restrict__ mstatus,
+        const double* __restrict__ pbuf, PDInfo2* __restrict__ pinfo) {
+  extern __shared__ double row[];
+  __shared__ double s_itot;
+  const int wd = blockIdx.x;
+  const int w = wd / D, d = wd - w * D;
+  if (mstatus[w] != 0) return;
+  PDInfo2& info = pinfo[wd];
+  if (info.status != 0) return;
+  const BSet2Dev& bs = bsets[dsets[d].bs];
+  const double d1 = bs.dflux1, d2 = bs.dflux2;
+  const int s1 = info.s1, s2 = info.s2;
+  const double* p = pbuf + static_cast<size_t>(wd) * n * nc2;
+  auto stage = [&](int a) {
+    int i = a + s1;
+    if (i >= n) i -= n;
+    const double* r = p + static_cast<size_t>(i) * nc2;
+    for (int b = threadIdx.x; b < n; b += NT) {
+      int j = b + s2;
+      if (j >= n) j -= n;
+      row[b] = clip0(r[j]);
+    }
+  };
+  // getIntegral
+  double tot = 0.0;
+  for (int a = 0; a < n; ++a) {
+    __syncthreads();
+    stage(a);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (a == 0) {
+        tot = __dmul_rn(0.5, row[0]);
+        for (int j = 1; j < n - 1; ++j) tot = __dadd_rn(tot, row[j]);
+        tot = __dadd_rn(tot, __dmul_rn(0.5, row[n - 1]));
+        tot = __dmul_rn(tot, 0.5);
+      } else if (a < n - 1) {
+        tot = __dadd_rn(tot, __dmul_rn(0.5, row[0]));
+        for (int j = 1; j < n - 1; ++j) tot = __dadd_rn(tot, row[j]);
+        tot = __dadd_rn(tot, __dmul_rn(0.5, row[n - 1]));
+      } else {
+        tot = __dadd_rn(tot, __dmul_rn(0.25, row[0]));
+        for (int j = 1; j < n - 1; ++j) tot = __dadd_rn(tot, __dmul_rn(0.5, row[j]));
+        tot = __dadd_rn(tot, __dmul_rn(0.25, row[n - 1]));
+      }
+    }
+  }
+  if (threadIdx.x == 0) s_itot = 1.0 / __dmul_rn(__dmul_rn(tot, d1), d2);
+  __syncthreads();
+  const double itot = s_itot;
+  // getMeans on the normalised array (each element stored as p * itot)
+  double mean1 = 0.0, mean2 = 0.0;
+  const double nm1 = static_cast<double>(n - 1);
+  for (int a = 0; a < n; ++a) {
+    __syncthreads();
+    stage(a);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (a == 0) {
+        for (int j = 1; j < n - 1; ++j)
+          mean2 = __dadd_rn(mean2, __dmul_rn(static_cast<double>(j), __dmul_rn(row[j], itot)));
+        mean2 = __dadd_rn(mean2, __dmul_rn(__dmul_rn(0.5, nm1), __dmul_rn(row[n - 1], itot)));
+        mean2 = __dmul_rn(mean2, 0.5);
+      } else if (a < n - 1) {
+        double xsum = __dmul_rn(0.5, __dmul_rn(row[0], itot));
+        for (int j = 1; j < n - 1; ++j) {
+          const double pv = __dmul_rn(row[j], itot);
+          xsum = __dadd_rn(xsum, pv);
+          mean2 = __dadd_rn(mean2, __dmul_rn(static_cast<double>(j), pv));
+        }
+        const double pl = __dmul_rn(row[n - 1], itot);
+        xsum = __dadd_rn(xsum, __dmul_rn(0.5, pl));
+        mean1 = __dadd_rn(mean1, __dmul_rn(xsum, static_cast<double>(a)));
+        mean2 = __dadd_rn(mean2, __dmul_rn(__dmul_rn(0.5, nm1), pl));
+      } else {
+        double xsum = __dmul_rn(0.5, __dmul_rn(row[0], itot));
+        for (int j = 1; j < n - 1; ++j) {
+          const double pv = __dmul_rn(row[j], itot);
+          xsum = __dadd_rn(xsum, pv);
+          mean2 = __dadd_rn(mean2, __dmul_rn(__dmul_rn(0.5, static_cast<double>(j)), pv));
+        }
+        const double pl = __dmul_rn(row[n - 1], itot);
+        xsum = __dadd_rn(xsum, __dmul_rn(0.5, pl));
+        mean1 = __dadd_rn(mean1, __dmul_rn(__dmul_rn(0.5, xsum), nm1));
+        mean2 = __dadd_rn(mean2, __dmul_rn(__dmul_rn(0.25, nm1), pl));
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    mean1 = __dmul_rn(mean1, __dmul_rn(__dmul_rn(d1, d1), d2));
+    mean2 = __dmul_rn(mean2, __dmul_rn(__dmul_rn(d1, d2), d2));
+    if (isinf(mean1) || isnan(mean1) || isinf(mean2) || isnan(mean2)) {
+      info.status = POFD_E_UNSHIFT;
+    } else {
+      info.itot = itot;
+      info.minflux1 = -mean1;
+      info.minflux2 = -mean2;
+    }
+  }
+}
+
 __device__ __forceinline__ double lq2(const double* __restrict__ p, int n,
                                       int nc2, int s1, int s2, double itot,
                                       int a, int b) {
@@ -2011,6 +2125,12 @@ void Engine2::set_fft_mode(int mode) {
   else colspec_ = false;
 }
 
+void Engine2::set_reference_sums(bool on) {
+  if (on == refsum_) return;
+  refsum_ = on;
+  drop_graphs();
+}
+
 void Engine2::ensure_plans(unsigned nprop) {
   auto it = plans_.find(nprop);
   if (it != plans_.end() && it->second.fwd) return;
@@ -2129,6 +2249,9 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   k_psplit2<<<P * D, SNT, 3 * static_cast<size_t>(n) * sizeof(double), st>>>(
       d_bsets_, d_dsets_, B, D, n, nc2, static_cast<int>(nct_), static_cast<int>(nrt_),
       ws_.mstatus, ws_.sigmult, ws_.mom, ws_.pbuf, ws_.rowpart, ws_.colpart, ws_.pinfo);
+  if (refsum_)
+    k_pseq2<<<P * D, NT, static_cast<size_t>(n) * sizeof(double), st>>>(
+        d_bsets_, d_dsets_, D, n, nc2, ws_.mstatus, ws_.pbuf, ws_.pinfo);
   mark(10);
   k_pgather2<<<dim3(gchunks_, P * D), NT, 0, st>>>(d_bsets_, d_dsets_, D, n, nc2,
                                                     static_cast<int>(gchunks_), ws_.mstatus,

@@ -131,8 +131,15 @@ class Engine2 {
   // the stage names of the FFT mode in use
   const char* stage_name_now(int i) const;
   int kernels_per_eval() const {
-    return (edge_ ? 12 : 10) + (colspec_ ? 1 : 0) + (prior_.needs_bonus() ? 1 : 0);
+    return (edge_ ? 12 : 10) + (colspec_ ? 1 : 0) + (prior_.needs_bonus() ? 1 : 0) +
+           (refsum_ ? 1 : 0);
   }
+  // Reference-order normalisation and means (k_pseq2 after the split
+  // search): the P(D) integral and the two means summed in one sequential
+  // chain in the reference's order instead of the default tree sums.  For
+  // parity checks only (a 2n^2-long dependent chain per dataset).
+  void set_reference_sums(bool on);
+  bool reference_sums() const { return refsum_; }
   // 0: batched 2D cuFFT transforms with k_spectrum2 between them; 1: batched
   // 1D cuFFT row transforms around this library's fused column-transform +
   // spectrum kernel (k_colspec2), where n is a power of two in [512, 4096]
@@ -224,6 +231,7 @@ class Engine2 {
   void drop_plans();
   int fft_mode_ = 1;
   bool colspec_ = false;
+  bool refsum_ = false;
   double2* d_cwh_ = nullptr;  // e^{-2 pi i 32 h / n}, h < n / 32
   double2* d_cwl_ = nullptr;  // e^{-2 pi i l / n}, l < 32
   Prior2 prior_;

@@ -766,41 +766,60 @@ void Ensemble::naccept(unsigned* out) const {
   ck(cudaMemcpy(out, nacc_, nw_ * sizeof(unsigned), cudaMemcpyDeviceToHost), "D2H naccept");
 }
 
-// affineChainSet::acor (affineChainSet.cc:884-951): Goodman's acor with
-// taumax 2, winmult 5, maxlag 10, minfac 5.
+// Integrated autocorrelation time of one series by Goodman's acor method
+// (affineChainSet::acor, affineChainSet.cc:884-951; Goodman's published
+// acor: autocovariances to lag 10, tau = (C0 + 2 sum C_s) / C0, and while
+// tau is long against that window the series is summed in adjacent pairs
+// and the estimate repeated on the half-length series, the result scaled
+// back up level by level).  Written as a descent through the levels
+// followed by the scale-back, with the operation order of the recursive
+// form so that tau is bitwise the same: the series is float (products of
+// two elements rounded to float, then accumulated in double), the mean is
+// a double sum in index order, and a level too short for the lag window
+// leaves the previous level's sigma in place.  Returns 1 when the series
+// is too short for the window at the top level.
 int acor_series(double& mean, double& sigma, double& tau, std::vector<float>& X,
                 unsigned L) {
-  constexpr unsigned taumax = 2, winmult = 5, maxlag = taumax * winmult, minfac = 5;
-  const double invL = 1.0 / static_cast<double>(L);
-  mean = X[0];
-  for (unsigned i = 1; i < L; ++i) mean += X[i];
-  mean *= invL;
-  for (unsigned i = 0; i < L; ++i) X[i] -= mean;
-  if (L < minfac * maxlag) return 1;
-  double C[maxlag + 1];
-  for (unsigned s = 0; s <= maxlag; ++s) C[s] = 0.0;
-  const unsigned iMax = L - maxlag;
-  const double invImax = 1.0 / static_cast<double>(iMax);
-  for (unsigned i = 0; i < iMax; ++i)
-    for (unsigned s = 0; s <= maxlag; ++s) C[s] += X[i] * X[i + s];
-  for (unsigned s = 0; s <= maxlag; ++s) C[s] *= invImax;
-  double D = C[0];
-  for (unsigned s = 1; s <= maxlag; ++s) D += 2 * C[s];
-  sigma = std::sqrt(D * invL);
-  tau = D / C[0];
-  if (tau * winmult < maxlag) return 0;
-  const unsigned Lh = L / 2;
-  double newMean;
-  unsigned j1 = 0, j2 = 1;
-  for (unsigned i = 0; i < Lh; ++i) {
-    X[i] = X[j1] + X[j2];
-    j1 += 2;
-    j2 += 2;
+  constexpr unsigned kWin = 5;              // window multiple of tau
+  constexpr unsigned kLag = 2 * kWin;       // largest lag (tau up to 2)
+  constexpr unsigned kMinLen = 5 * kLag;    // shortest series analysed
+  struct Scale {
+    double c0;
+    unsigned len;
+  };
+  std::vector<Scale> descent;
+  unsigned len = L;
+  for (unsigned level = 0;; ++level) {
+    double m = X[0];
+    for (unsigned i = 1; i < len; ++i) m += X[i];
+    m *= 1.0 / static_cast<double>(len);
+    if (level == 0) mean = m;
+    for (unsigned i = 0; i < len; ++i) X[i] -= m;
+    if (len < kMinLen) {
+      if (level == 0) return 1;
+      break;  // the level above keeps its sigma
+    }
+    double cov[kLag + 1] = {};
+    const unsigned span = len - kLag;
+    for (unsigned i = 0; i < span; ++i)
+      for (unsigned lag = 0; lag <= kLag; ++lag) cov[lag] += X[i] * X[i + lag];
+    const double ispan = 1.0 / static_cast<double>(span);
+    for (unsigned lag = 0; lag <= kLag; ++lag) cov[lag] *= ispan;
+    double d = cov[0];
+    for (unsigned lag = 1; lag <= kLag; ++lag) d += 2 * cov[lag];
+    sigma = std::sqrt(d * (1.0 / static_cast<double>(len)));
+    tau = d / cov[0];
+    if (tau * kWin < kLag) break;
+    descent.push_back({cov[0], len});
+    const unsigned half = len / 2;
+    for (unsigned i = 0; i < half; ++i) X[i] = X[2 * i] + X[2 * i + 1];
+    len = half;
   }
-  acor_series(newMean, sigma, tau, X, Lh);
-  D = 0.25 * sigma * sigma * static_cast<double>(L);
-  tau = D / C[0];
-  sigma = std::sqrt(D * invL);
+  for (auto it = descent.rbegin(); it != descent.rend(); ++it) {
+    const double d = 0.25 * sigma * sigma * static_cast<double>(it->len);
+    tau = d / it->c0;
+    sigma = std::sqrt(d * (1.0 / static_cast<double>(it->len)));
+  }
   return 0;
 }
 

@@ -112,19 +112,37 @@ std::vector<Hdu> scan(const std::string& path, const std::string& buf) {
       throw Error(POFD_E_ARG, path + " is not a FITS file");
     h.bitpix = static_cast<int>(key_long(h, "BITPIX", 0, true, path));
     const long naxis = key_long(h, "NAXIS", 0, true, path);
-    long prod = naxis > 0 ? 1 : 0;
+    // FITS standard 4.4.1: 0 <= NAXIS <= 999, NAXISn >= 0, PCOUNT >= 0,
+    // GCOUNT >= 1; the data size is |BITPIX|/8 * GCOUNT * (PCOUNT + prod
+    // NAXISn), computed with overflow checks so that a corrupt header ends
+    // in an error instead of a wrapped size
+    if (naxis < 0 || naxis > 999) throw Error(POFD_E_ARG, "Invalid NAXIS in " + path);
+    auto bad_size = [&]() { return Error(POFD_E_ARG, "Invalid data size in FITS header of " + path); };
+    size_t prod = naxis > 0 ? 1 : 0;
     for (long a = 1; a <= naxis; ++a) {
       const long na = key_long(h, "NAXIS" + std::to_string(a), 0, true, path);
+      if (na < 0) throw Error(POFD_E_ARG, "Negative NAXIS" + std::to_string(a) + " in " + path);
       h.naxes.push_back(na);
-      prod *= na;
+      if (__builtin_mul_overflow(prod, static_cast<size_t>(na), &prod)) throw bad_size();
     }
     const long pcount = key_long(h, "PCOUNT", 0, false, path);
     const long gcount = key_long(h, "GCOUNT", 1, false, path);
+    if (pcount < 0) throw Error(POFD_E_ARG, "Negative PCOUNT in " + path);
+    if (gcount < 1) throw Error(POFD_E_ARG, "GCOUNT below 1 in " + path);
+    size_t elems = 0, bytes = 0, padded = 0, next = 0;
+    if (__builtin_add_overflow(prod, static_cast<size_t>(pcount), &elems) ||
+        __builtin_mul_overflow(elems, static_cast<size_t>(gcount), &elems) ||
+        __builtin_mul_overflow(elems, static_cast<size_t>(std::abs(h.bitpix) / 8), &bytes) ||
+        __builtin_add_overflow(bytes, kBlock - 1, &padded) ||
+        __builtin_add_overflow(p, padded / kBlock * kBlock, &next))
+      throw bad_size();
     h.data_off = p;
-    h.data_bytes = static_cast<size_t>(std::abs(h.bitpix) / 8) *
-                   static_cast<size_t>(gcount) * static_cast<size_t>(pcount + prod);
+    h.data_bytes = bytes;
     hdus.push_back(h);
-    pos = p + (h.data_bytes + kBlock - 1) / kBlock * kBlock;
+    // the next header starts after this one's data, inside the file; a data
+    // block that runs past the end is caught where the data is read
+    if (next <= pos) throw bad_size();
+    pos = next;
   }
   if (hdus.empty()) throw Error(POFD_E_ARG, path + " is not a FITS file");
   return hdus;

@@ -293,11 +293,20 @@ extern "C" int pofd_pd1_loglike_noalloc(
     pofd::set_last_error("pofd_pd1_loglike_noalloc: no usable current device");
     return POFD_E_CUDA;
   }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    pofd::set_last_error("pofd_pd1_loglike_noalloc: stream query failed");
+    return POFD_E_CUDA;
+  }
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mtx);
-    if (!g_scratch_addr[dev]) {
-      // set-up, once per device, with that device current
+    // Outside stream capture the address is looked up on every call (with
+    // the device current): a device reset reloads the module and moves the
+    // array, and a stored address would then be stale.  Inside a capture
+    // the address from the last uncaptured call on this device is used.
+    if (cs == cudaStreamCaptureStatusNone || !g_scratch_addr[dev]) {
       void* ptr = nullptr;
       if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
         pofd::set_last_error("pofd_pd1_loglike_noalloc: scratch address lookup failed");
@@ -308,7 +317,6 @@ extern "C" int pofd_pd1_loglike_noalloc(
     scratch = g_scratch_addr[dev];
   }
   const int nchunk = static_cast<int>((n + kChunk - 1) / kChunk);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   k_na_pscan<<<nchunk, kNT, 0, st>>>(pofd_dev, static_cast<int>(n), dflux,
                                      minflux_R, static_cast<int>(wrapRidx),
                                      var_noi, sigma, scratch);

@@ -669,6 +669,15 @@ unsigned Surrogate::npairs() const {
   return c[1];
 }
 
+void Surrogate::pairs_host(unsigned n, float* theta, double* logl) const {
+  if (n > npairs()) throw Error(POFD_E_ARG, "more pairs asked for than are held");
+  if (n == 0) return;
+  if (theta)
+    ck(cudaMemcpy(theta, ptheta_, static_cast<size_t>(n) * npar_ * sizeof(float),
+                  cudaMemcpyDeviceToHost), "D2H pairs");
+  if (logl) ck(cudaMemcpy(logl, plogl_, n * sizeof(double), cudaMemcpyDeviceToHost), "D2H pairs");
+}
+
 // Standardisation of the inputs (mean, 1/sd of the free parameters) and of
 // the target (running max, sd of logL) from the pairs held.
 void Surrogate::refresh_scaling() {

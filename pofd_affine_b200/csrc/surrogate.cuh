@@ -25,6 +25,8 @@ class Surrogate {
   void add_pairs(unsigned n, const float* theta, unsigned npar, const double* logl,
                  const int* status, cudaStream_t st);
   unsigned npairs() const;
+  // The first n pairs held (buffer order) into host theta [n][npar], logl [n].
+  void pairs_host(unsigned n, float* theta, double* logl) const;
   // iters Adam steps on random minibatches of the pairs held.
   void train(unsigned iters, unsigned batch, float lr, float* last_loss);
   // Predicted logL of n device rows (batched-likelihood signature).

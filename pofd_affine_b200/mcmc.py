@@ -7,6 +7,8 @@
                     doBurnIn (fixed burn), getAcor, getAcceptanceFrac, and the
                     recorded chain.
   * acor            Goodman's acor (affineChainSet.cc:884-951).
+  * integrated_time the integrated autocorrelation time with Sokal's
+                    automatic window (no counterpart in the reference).
   * gaussLike       a multivariate Gaussian test likelihood on the device.
 """
 import ctypes as C
@@ -26,6 +28,51 @@ def acor(x):
     rc = check(lib().pofd_acor(x, x.size, C.byref(m), C.byref(s),
                                C.byref(t)))
     return m.value, s.value, t.value, rc == 0
+
+
+def _autocorr_1d(x):
+    """Normalised autocorrelation function of a series (FFT, zero-padded to
+    at least twice its length so that the circular correlation is the
+    linear one)."""
+    x = np.asarray(x, dtype=np.float64)
+    n = x.size
+    m = 1
+    while m < 2 * n:
+        m *= 2
+    f = np.fft.rfft(x - x.mean(), n=m)
+    acf = np.fft.irfft(f * np.conjugate(f), n=m)[:n]
+    return acf / acf[0] if acf[0] > 0 else np.zeros(n)
+
+
+def integrated_time(chain, c=5.0):
+    """Integrated autocorrelation time per parameter of an ensemble chain
+    [nsteps][nwalkers][nparams] with Sokal's automatic window: the
+    autocorrelation function is averaged over the walkers (Goodman & Weare
+    2010), tau(M) = 1 + 2 sum_{t=1..M} rho(t), and M is the first window
+    with M >= c tau(M) (Sokal 1997, sec. 3; c = 5 as in emcee).  Unlike
+    acor's fixed 10-lag window this estimate does not saturate for long
+    correlation times.  Returns (tau [nparams], window [nparams],
+    converged [nparams]): converged is False when no window up to the chain
+    length satisfies the rule (tau is then a lower bound)."""
+    ch = np.asarray(chain, dtype=np.float64)
+    nsteps, nwalkers, npar = ch.shape
+    tau = np.full(npar, np.nan)
+    win = np.zeros(npar, dtype=int)
+    conv = np.zeros(npar, dtype=bool)
+    for p in range(npar):
+        if np.all(ch[:, :, p] == ch[0, 0, p]):
+            continue  # a fixed parameter
+        rho = np.mean([_autocorr_1d(ch[:, k, p]) for k in range(nwalkers)],
+                      axis=0)
+        taus = 2.0 * np.cumsum(rho) - 1.0
+        ok = np.arange(taus.size) >= c * taus
+        if np.any(ok):
+            m = int(np.argmax(ok))
+            conv[p] = True
+        else:
+            m = taus.size - 1
+        tau[p], win[p] = taus[m], m
+    return tau, win, conv
 
 
 class gaussLike:
@@ -320,3 +367,15 @@ class affineEnsemble:
         tau, ok = self.getAcor()
         t = np.nanmax(tau) if np.any(np.isfinite(tau)) else np.nan
         return self.nwalkers * self.nRecorded() / t, tau, ok
+
+    def getIntegratedTime(self, c=5.0):
+        """integrated_time of the recorded chain over the parameters that
+        are neither fixed nor ignored for acor: (tau [nparams] with NaN for
+        the others, converged)."""
+        ch, _ = self.getChain()
+        tau, _, conv = integrated_time(ch, c)
+        for p in range(self.nparams):
+            if self.state[p] & (FIXED | ACIGNORE):
+                tau[p] = np.nan
+                conv[p] = True
+        return tau, bool(np.all(conv))

@@ -128,9 +128,16 @@ def setupFluxes(minval, maxval, n, logspace=True):
     return (lo + (hi - lo) / (n - 1) * i).astype(np.float32)
 
 
-def _band_range(knotpos):
+def _band_range(knotpos, double_knots=False):
     """The reference's flux range of a counts curve: the first knot to just
-    below the last (the counts are 0 at the last knot), in float."""
+    below the last (the counts are 0 at the last knot), passed on as float.
+    The two-band model holds its knots as float and pulls the top in float
+    arithmetic (numberCountsDoubleLogNormalStats.cc:212-214); the 1D model
+    holds double knots and pulls the top in double before the conversion
+    (numberCountsKnotsSplineStats.cc:156-159): double_knots=True."""
+    if double_knots:
+        lo, hi = float(knotpos[0]), float(knotpos[-1])
+        return np.float32(lo), np.float32(hi - 1e-4 * (hi - lo))
     lo, hi = np.float32(knotpos[0]), np.float32(knotpos[-1])
     d = np.float32(hi - lo)
     return lo, np.float32(float(hi) - 1e-4 * float(d))
@@ -164,7 +171,8 @@ def numberCountsStats(chain, logl, knotpos, nflux=1024, thin=5, logspace=True):
     flat, lflat, best, samples, nsamp = _read_walker_major(chain, logl, thin)
     pmean, pmed, psnake = accumulateStats(samples.T)
     K = len(knotpos)
-    flux = setupFluxes(*_band_range(knotpos), nflux, logspace).astype(np.float64)
+    flux = setupFluxes(*_band_range(knotpos, double_knots=True), nflux,
+                       logspace).astype(np.float64)
     working = np.empty((nflux, nsamp), np.float32)
     for i, p in enumerate(samples):
         with np.errstate(divide="ignore"):

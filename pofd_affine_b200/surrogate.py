@@ -79,6 +79,17 @@ class Surrogate:
         check(lib().pofd_surrogate_npairs(self.h, C.byref(n)))
         return n.value
 
+    def getPairs(self, n=None):
+        """The training pairs held (buffer order): (theta [n][nparams]
+        float32, logl [n] float64)."""
+        n = self.nPairs() if n is None else int(n)
+        th = np.empty((n, self.nparams), np.float32)
+        ll = np.empty(n, np.float64)
+        check(lib().pofd_surrogate_get_pairs(self.h, n,
+                                             th.ctypes.data_as(C.c_void_p),
+                                             ll.ctypes.data_as(C.c_void_p)))
+        return th, ll
+
     # ---------------------------------------------------------- training
     def train(self, iters, batch=1024, lr=1e-3):
         loss = C.c_float()

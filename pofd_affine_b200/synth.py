@@ -113,12 +113,13 @@ def make_map_pair(shape, pixsize, beam1, beam2, knotpos, log10vals,
 
 
 # ------------------------------------------------------------ configurations
-def config_1d_small(seed=1):
+def config_1d_small(seed=1, norm_scale=1.0):
     """1D plain fit: 6 knots over 2-400 mJy, FWHM 3 px beam at 6", 120-bin
     beam histogram, n = 4096, one 256x256 map at 2.5 mJy noise, 1000 data
-    bins."""
+    bins.  norm_scale multiplies the counts (100 makes the map confusion
+    dominated: the split search then takes its jitter branch)."""
     rng = np.random.default_rng(seed)
-    kp, kv = knot_model(6, 0.002, 0.400, rng=rng)
+    kp, kv = knot_model(6, 0.002, 0.400, norm=1e4 * norm_scale, rng=rng)
     bm = gaussian_beam(3.0)
     img = make_map((256, 256), 6.0, bm, kp, kv, 0.0025, rng)
     return dict(knotpos=kp, knotvals=kv, fftsize=4096, ninterp=2048,

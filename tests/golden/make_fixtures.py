@@ -3,7 +3,7 @@
 Run in a container where the reference tree is mounted (it is not needed at
 test time):
 
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py <reference checkout>   (or POFD_REFERENCE_DIR)
 
 Writes, next to this script:
   * beams.npz -- the reference's test beams (test/testdata/band1_beam.fits,
@@ -182,4 +182,7 @@ def main(refroot):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("POFD_REFERENCE_DIR")
+    if not src:
+        sys.exit("usage: make_fixtures.py <reference checkout> (or set POFD_REFERENCE_DIR)")
+    main(src)

@@ -14,7 +14,10 @@ import os
 import numpy as np
 import pytest
 
-REFDATA = "/root/reference/test/testdata"
+# the reference's own test FITS files (test/testdata in its tree), when a
+# checkout is named by POFD_REFERENCE_DIR; skipped otherwise
+REFDATA = os.path.join(os.environ.get("POFD_REFERENCE_DIR", ""), "test", "testdata") \
+    if os.environ.get("POFD_REFERENCE_DIR") else ""
 
 
 def _card(key, value=None, comment=""):
@@ -141,7 +144,8 @@ def test_reference_errors(tmp_path):
         fitsio.readData(str(junk))
 
 
-@pytest.mark.skipif(not os.path.isdir(REFDATA), reason="reference test data absent")
+@pytest.mark.skipif(not REFDATA or not os.path.isdir(REFDATA),
+                    reason="POFD_REFERENCE_DIR not set or its test data absent")
 def test_reference_beam_files_match_fixtures():
     from pofd_affine_b200 import fitsio
     here = os.path.dirname(os.path.abspath(__file__))

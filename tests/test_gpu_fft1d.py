@@ -31,14 +31,20 @@ def test_own_fft_matches_cufft(orc, gpu_ctx, n):
     assert list(so) == list(sc)
     ok = so == 0
     assert np.max(np.abs(lo[ok] - lc[ok])) < 1e-7
-    # the R grid fill fused into the forward pass A (default) against the
-    # materialised grid: the same values, moments grouped differently
-    assert L.getTuning()["rfill_fused"] == 1
-    L.setTuning(rfill_fused=0)
-    lu, su = L.getLogLikeBatch(th)
-    L.setTuning(rfill_fused=1)
-    assert list(su) == list(so)
-    assert np.max(np.abs(lu[ok] - lo[ok])) < 1e-7
+    # the R grid fill fused into the forward pass A by running products over
+    # 16-point segments (default) against the fill with one exp2 per point,
+    # fused and materialised: values within ~1e-13 relative, moments grouped
+    # differently
+    assert L.getTuning()["rfill_fused"] == 2
+    for rf in (0, 1):
+        L.setTuning(rfill_fused=rf)
+        lu, su = L.getLogLikeBatch(th)
+        pu, iu = L.getPD(1, 0, th[0], setLog=False)
+        assert list(su) == list(so)
+        assert np.max(np.abs(lu[ok] - lo[ok])) < 1e-7
+        du = int(io["splitidx"] - iu["splitidx"])
+        assert np.max(np.abs(np.roll(po, du) - pu)) <= 1e-10 * pu.max()
+    L.setTuning(rfill_fused=2)
     # pass B fed by bulk copies through a shared-memory ring: same arithmetic
     L.setTuning(fft_persist=2)
     lb, sb = L.getLogLikeBatch(th)

@@ -87,9 +87,18 @@ int main(int argc, char** argv) {
   fits_read_data2(dir + "/m.fits", dir + "/m.fits", false, false, &x1, &x2);
   int errors = 0;
   for (const char* f : {"/trunc_head.fits", "/trunc_data.fits", "/junk.fits", "/nofile.fits",
-                        "/cube.fits"}) {
+                        "/cube.fits", "/negaxis.fits", "/bigaxis.fits", "/negpcount.fits",
+                        "/gcount0.fits"}) {
     try {
       fits_read_data(dir + f, false, false);
+    } catch (const Error&) {
+      ++errors;
+    }
+  }
+  // beams with corrupt axis sizes are rejected as well
+  for (const char* f : {"/negaxis.fits", "/bigaxis.fits"}) {
+    try {
+      fits_read_beam(dir + f);
     } catch (const Error&) {
       ++errors;
     }
@@ -98,6 +107,18 @@ int main(int argc, char** argv) {
   return 0;
 }
 """
+
+
+def _raw_header(cards, nbytes_data=2880):
+    """A primary HDU written card by card (no validation): 80-character
+    cards, END, padded to 2880-byte blocks, then nbytes_data of zeros."""
+    txt = "".join(c.ljust(80)[:80] for c in cards + ["END"])
+    txt = txt.ljust((len(txt) + 2879) // 2880 * 2880)
+    return txt.encode("ascii") + b"\0" * nbytes_data
+
+
+def _card(key, val):
+    return "%-8s= %20s" % (key, val)
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no host compiler")
@@ -113,6 +134,15 @@ def test_setup_and_fits_under_asan_ubsan(tmp_path):
     (tmp_path / "trunc_data.fits").write_bytes(raw[:2880 + 1000])
     (tmp_path / "junk.fits").write_bytes(b"\x00\xff" * 3000)
     _write(tmp_path / "cube.fits", _hdu(np.ones((2, 3, 4)), -64, True))
+    base = [_card("SIMPLE", "T"), _card("BITPIX", -64), _card("NAXIS", 2)]
+    (tmp_path / "negaxis.fits").write_bytes(_raw_header(
+        base + [_card("NAXIS1", -1), _card("NAXIS2", -1)]))
+    (tmp_path / "bigaxis.fits").write_bytes(_raw_header(
+        base + [_card("NAXIS1", 2 ** 32), _card("NAXIS2", 2 ** 32)]))
+    (tmp_path / "negpcount.fits").write_bytes(_raw_header(
+        base + [_card("NAXIS1", 4), _card("NAXIS2", 4), _card("PCOUNT", -100)]))
+    (tmp_path / "gcount0.fits").write_bytes(_raw_header(
+        base + [_card("NAXIS1", 4), _card("NAXIS2", 4), _card("GCOUNT", 0)]))
     src = tmp_path / "drv.cc"
     src.write_text(DRIVER)
     exe = tmp_path / "drv"
@@ -126,7 +156,7 @@ def test_setup_and_fits_under_asan_ubsan(tmp_path):
     r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True,
                        env=env, timeout=300)
     assert r.returncode == 0, r.stderr[-4000:]
-    assert "errors 5" in r.stdout
+    assert "errors 11" in r.stdout
     assert "fits 510 9 9 510" in r.stdout  # 600 pixels, 3 rows of 30 masked
 
 
@@ -163,7 +193,12 @@ int main() {
     std::vector<double> lls(4);
     std::vector<int> sts(4);
     orc_like1_eval_batch(L, 4, ths.data(), 6, lls.data(), sts.data(), 2);
-    std::printf("oracle binned %d status %d finite %d\n", binned, st, std::isfinite(ll) ? 1 : 0);
+    orc_set_fast_fft(1);
+    double llf = 0.0;
+    const int stf = orc_like1_eval(L, th, 6, &llf);
+    orc_set_fast_fft(0);
+    std::printf("oracle binned %d status %d finite %d fast %d %d\n", binned, st,
+                std::isfinite(ll) ? 1 : 0, stf, std::fabs(llf - ll) < 1e-6 ? 1 : 0);
     orc_like1_free(L);
   }
   return 0;
@@ -181,11 +216,12 @@ def test_oracle_under_asan_ubsan(tmp_path):
              "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
              "-fno-omit-frame-pointer"]
     subprocess.check_call(["g++"] + flags + [str(src), os.path.join(odir, "pofd_oracle.cc"),
-                                             os.path.join(odir, "numerics.cc"), "-I", odir,
+                                             os.path.join(odir, "numerics.cc"),
+                                             os.path.join(odir, "fastfft.cc"), "-I", odir,
                                              "-o", str(exe)])
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1:abort_on_error=1",
                UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1")
     r = subprocess.run([str(exe)], capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0, r.stderr[-4000:]
-    assert "oracle binned 0 status 0 finite 1" in r.stdout
-    assert "oracle binned 1 status 0 finite 1" in r.stdout
+    assert "oracle binned 0 status 0 finite 1 fast 0 1" in r.stdout
+    assert "oracle binned 1 status 0 finite 1 fast 0 1" in r.stdout

@@ -181,3 +181,52 @@ def test_like_batch_threads_match_serial(orc, beams):
     assert st1[3] == -1 and np.isnan(ll1[3])
     ok = st1 == 0
     assert np.array_equal(ll1[ok], ll4[ok])
+
+
+@pytest.mark.parametrize("n", [8, 32, 256, 4096, 65536])
+def test_fast_real_fft_against_numpy(orc, n):
+    """The timed CPU baseline's radix-4 real transforms (oracle/fastfft.cc)
+    against numpy's, forward and unnormalised inverse, 1D and 2D."""
+    rng = np.random.default_rng(n)
+    x = rng.normal(size=n)
+    X = np.fft.rfft(x)
+    Y = X * np.exp(0.1j * rng.normal(size=X.size))
+    orc.set_fast_fft(True)
+    try:
+        f = orc.rfft(x)
+        y = orc.irfft(Y, n)
+        if n <= 256:
+            x2 = rng.normal(size=(n, n))
+            X2 = np.fft.rfft2(x2)
+            Y2 = X2 * np.exp(0.1j * rng.normal(size=X2.shape))
+            f2 = orc.rfft2(x2)
+            y2 = orc.irfft2(Y2, n)
+    finally:
+        orc.set_fast_fft(False)
+    assert np.max(np.abs(f - X)) < 1e-14 * np.abs(X).max()
+    yr = np.fft.irfft(Y, n) * n
+    assert np.max(np.abs(y - yr)) < 1e-14 * np.abs(yr).max()
+    if n <= 256:
+        assert np.max(np.abs(f2 - X2)) < 1e-14 * np.abs(X2).max()
+        y2r = np.fft.irfft2(Y2, (n, n)) * n * n
+        assert np.max(np.abs(y2 - y2r)) < 1e-14 * np.abs(y2r).max()
+
+
+def test_fast_fft_likelihood_agrees(orc):
+    """The oracle's log-likelihood with the fast transforms (the timed CPU
+    baseline) against the radix-2 parity form."""
+    from pofd_affine_b200 import synth
+    cfg = synth.config_1d_small(seed=3)
+    O = orc.Like1(cfg["knotpos"], 8192, 512, True, 500)
+    O.add_beamset(cfg["beams"][0], 6.0, 1e-5, True, 120)
+    O.add_dataset(0, cfg["maps"][0], cfg["sigmas"][0])
+    O.set_rranges(cfg["theta0"])
+    th = synth.proposals(cfg["theta0"], 4, 0.02, rng=5)
+    l0, s0 = O.loglike_batch(th, 2)
+    orc.set_fast_fft(True)
+    try:
+        l1, s1 = O.loglike_batch(th, 2)
+    finally:
+        orc.set_fast_fft(False)
+    assert list(s0) == list(s1)
+    assert np.max(np.abs(l1 - l0)) < 1e-6

@@ -65,3 +65,23 @@ def test_oracle_stretch_samples_gaussian():
     assert np.all(np.abs(s.mean(0) - mu) < 0.5 * np.sqrt(np.diag(cov)))
     assert np.all(np.abs(np.diag(np.cov(s.T)) / np.diag(cov) - 1) < 0.35)
     assert 0.2 < nacc.sum() / (600 * nw) < 0.9
+
+
+@pytest.mark.parametrize("rho", [0.5, 0.9, 0.97])
+def test_integrated_time_on_ar1_ensembles(rho):
+    """Sokal-window integrated time against the exact tau = (1 + rho) /
+    (1 - rho) of AR(1) walkers, within 10 % on chains of > 100 tau."""
+    from pofd_affine_b200.mcmc import integrated_time
+    rng = np.random.default_rng(int(rho * 100))
+    nsteps, nw = 8000, 32
+    x = np.empty((nsteps, nw, 2))
+    e = rng.normal(size=(nsteps, nw, 2))
+    x[0] = e[0] / np.sqrt(1 - rho * rho)
+    for t in range(1, nsteps):
+        x[t] = rho * x[t - 1] + e[t]
+    x[:, :, 1] = 3.0  # a fixed parameter
+    tau, win, conv = integrated_time(x)
+    exact = (1 + rho) / (1 - rho)
+    assert conv[0] and abs(tau[0] / exact - 1) < 0.1, (tau[0], exact)
+    assert np.isnan(tau[1])
+    assert win[0] >= 5 * tau[0]

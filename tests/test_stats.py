@@ -176,3 +176,24 @@ def test_double_lognormal_stats_on_a_synthetic_chain(golden):
     for c in (r["band1"], r["sigma"], r["offset"], rr["sigma"]):
         lo, hi = c["snake"][2, :, 0], c["snake"][2, :, 1]
         assert np.all(lo <= c["median"]) and np.all(c["median"] <= hi)
+
+
+def test_band_range_rounding_rules():
+    """The top of the flux grid: pulled in by 1e-4 of the range in double
+    for the 1D model's double knots, then converted to float
+    (numberCountsKnotsSplineStats.cc:156-159); in float arithmetic for the
+    two-band model's float knots (numberCountsDoubleLogNormalStats.cc:212-214).
+    The two rules differ by a float ulp on a good share of knot pairs."""
+    from pofd_affine_b200 import stats
+    rng = np.random.default_rng(5)
+    differ = 0
+    for _ in range(2000):
+        k = np.sort(rng.uniform(1e-4, 1.0, 2))
+        lo1, hi1 = stats._band_range(k, double_knots=True)
+        assert lo1 == np.float32(k[0])
+        assert hi1 == np.float32(k[1] - 1e-4 * (k[1] - k[0]))
+        lo2, hi2 = stats._band_range(k)
+        f0, f1 = np.float32(k[0]), np.float32(k[1])
+        assert hi2 == np.float32(float(f1) - 1e-4 * float(np.float32(f1 - f0)))
+        differ += hi1 != hi2
+    assert differ > 0

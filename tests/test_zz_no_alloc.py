@@ -38,32 +38,59 @@ def _wrapped_pd(rv, info, sigma):
     return np.fft.irfft(p, n) * n
 
 
-def test_noalloc_matches_regular_entry_point(orc, gpu_ctx):
+def _jitter_branch(raw, info, sigma):
+    """True when the reference's split search (PDFactory.cc:756-921) finds
+    no monotonic descent before the minimum and takes its jitter-estimate
+    branch on this wrapped P(D)."""
+    dflux = info["dflux"]
+    sgpos = np.sqrt(info["var_noi"] + sigma * sigma)
+    sgneg = sigma if 9 * sigma * sigma > info["var_noi"] else sgpos
+    bot = int(2.5 * sgpos / dflux)
+    mfr, wr = info["minflux_R"], int(info["wrapRidx"])
+    top = wr if 2.5 * sgpos > abs(mfr) else int(-(2.5 * sgneg + mfr) / dflux
+                                                 + wr + 1)
+    p = np.where(raw > 0, raw, 0.0)
+    mi = bot + int(np.argmin(p[bot:top + 1]))
+    return mi > 17 and not np.all(np.diff(p[mi - 17:mi + 1]) < 0)
+
+
+# (knots, knot range, FWHM px, beam histogram bins, noise, map, n, nodes,
+# data bins): a noise-dominated P(D) whose split is the first minimum, and
+# the 65536-point P(D) of the batched workload's first beam set, which
+# reaches the rounding floor and takes the jitter branch
+CASES = {
+    "monotone": (6, 0.002, 0.4, 3.0, 120, 0.002, (128, 128), 8192, 512, 500),
+    "jitter": (10, 0.001, 0.8, 3.0, 150, 0.002, (400, 400), 65536, 2048, 1000),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_noalloc_matches_regular_entry_point(orc, gpu_ctx, case):
     import torch
     from pofd_affine_b200 import beam, calcLike, synth
     from pofd_affine_b200._lib import lib
 
+    nk, smin, smax, fwhm, nh, sigma, shape, n, ni, nb = CASES[case]
     rng = np.random.default_rng(21)
-    kp, kv = synth.knot_model(6, 0.002, 0.4, rng=rng)
-    bm = synth.gaussian_beam(3.0)
-    sigma = 0.002
-    img = synth.make_map((128, 128), 6.0, bm, kp, kv, sigma, rng)
+    kp, kv = synth.knot_model(nk, smin, smax, rng=rng)
+    bm = synth.gaussian_beam(fwhm)
+    img = synth.make_map(shape, 6.0, bm, kp, kv, sigma, rng)
     th = np.concatenate([kv, [1.0]]).astype(np.float32)
-    n, ni, nb = 8192, 512, 500
 
     G = calcLike(gpu_ctx, kp, n, ni, True, nb)
-    G.addBeamSet(beam(bm, 6.0, True, 120))
+    G.addBeamSet(beam(bm, 6.0, True, nh))
     G.addDataset(0, img, sigma)
     G.setRRanges(th)
     ref, st = G.getLogLikeBatch(th[None, :])
     assert st[0] == 0
 
     O = orc.Like1(kp, n, ni, True, nb)
-    O.add_beamset(bm, 6.0, 1e-5, True, 120)
+    O.add_beamset(bm, 6.0, 1e-5, True, nh)
     O.add_dataset(0, img, sigma)
     O.set_rranges(th)
     _, info, rv = O.pd(0, 0, th, setlog=False, want_r=True)
     raw = _wrapped_pd(rv, info, sigma)
+    assert _jitter_branch(raw, info, sigma) == (case == "jitter")
 
     di = G.datasetInfo(0, 0)
     nz = np.nonzero(di["bins"])[0]
