@@ -54,7 +54,50 @@ def args():
     p.add_argument("--no-mcmc", action="store_true")
     p.add_argument("--mcmc-2d", type=int, default=1,
                    help="include the two-field 2D MCMC comparison")
+    p.add_argument("--profile-case", choices=["1d", "2d", "surrogate"],
+                   help="run a small fixed workload for a profiler and exit "
+                        "(--batch proposals or pairs, --reps repetitions)")
+    p.add_argument("--batch", type=int, default=8)
+    p.add_argument("--reps", type=int, default=2)
     return p.parse_args()
+
+
+# ------------------------------------------------------- profiler workloads
+def profile_case(a):
+    """Small fixed workloads to run under a profiler (one GPU, a few hundred
+    MB on the device, a handful of launches per kernel).  1d: the 1D batched
+    configuration (n = 65536, three beam sets and maps); 2d: the 2D plain
+    configuration (n = 2048, 1500 x 1500 map pair); both run `reps`
+    likelihood batches of `batch` proposals.  surrogate: `reps` Adam steps of
+    the H = 256 network on minibatches of `batch` pairs."""
+    from pofd_affine_b200 import Context, synth
+    ctx = Context(0)
+    if a.profile_case == "surrogate":
+        from pofd_affine_b200.surrogate import Surrogate
+        rng = np.random.default_rng(0)
+        th = rng.normal(size=(8192, 7)).astype(np.float32)
+        ll = -0.5 * (th[:, :6] ** 2).sum(1)
+        S = Surrogate(ctx, 7, list(range(6)), hidden=256, seed=1)
+        S.addPairs(th, ll)
+        for _ in range(a.reps):
+            S.train(1, a.batch)
+        print("surrogate: %d Adam steps of batch %d" % (a.reps, a.batch))
+        return
+    if a.profile_case == "1d":
+        cfg = synth.config_1d_batched(seed=2)
+        L = synth.build_like1(cfg, ctx)
+        th = synth.proposals(cfg["theta0"], a.batch, 0.02, rng=1)
+    else:
+        cfg = synth.config_2d()
+        L = synth.build_like2(cfg, ctx)
+        th = synth.proposals(cfg["theta0"], a.batch, 0.02, rng=1,
+                             fixed_last=False)
+        th[:, -2:] = 1.0
+    L.reserve(a.batch)
+    for _ in range(a.reps):
+        ll, st = L.getLogLikeBatch(th)
+    print("%s: %d batches of %d, status %s" % (a.profile_case, a.reps,
+                                               a.batch, sorted(set(st.tolist()))))
 
 
 # --------------------------------------------------------------- clocks
@@ -486,6 +529,9 @@ def _mcmc_summary(name, plain, da, free):
 
 def main():
     a = args()
+    if a.profile_case:
+        profile_case(a)
+        return
     from pofd_affine_b200 import synth
     cfg = synth.config_1d_batched(seed=2)
     if a.impl == "reference":
@@ -499,7 +545,7 @@ def main():
     rank, world, local = rk.rank, rk.world, rk.local
     from pofd_affine_b200 import Context, build
     build.build()
-    from pofd_affine_b200._lib import lib
+    from pofd_affine_b200._lib import support_lib
     import ctypes as C
 
     ctx = Context(local)
@@ -580,7 +626,7 @@ def main():
         # FP64-bound R grid fill (fused with the forward pass A): algorithmic
         # FP64 flops against the measured FP64 FMA peak
         pk = C.c_double()
-        lib().pofd_fp64_peak(local, C.byref(pk))
+        support_lib().pofd_fp64_peak(local, C.byref(pk))
         ach = nflops / (own[dom] * 1e-3) / 1e12
         roof = {"bound": "fp64", "kernel": dom, "ms_per_launch": own[dom],
                 "achieved": ach, "peak": pk.value, "unit": "TFLOP/s",
@@ -598,7 +644,7 @@ def main():
         # FP64-bound R builder: FP64 flops of the R terms against the
         # measured FP64 FMA peak
         pk = C.c_double()
-        lib().pofd_fp64_peak(local, C.byref(pk))
+        support_lib().pofd_fp64_peak(local, C.byref(pk))
         roof = {"bound": "fp64", "kernel": dom, "ms_per_launch": own[dom],
                 "peak": pk.value, "unit": "TFLOP/s",
                 "peak_source": "measured (pofd_fp64_peak DFMA loop)",

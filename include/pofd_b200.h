@@ -506,19 +506,6 @@ int pofd_ensemble_set_naccept(pofd_ensemble* e, const unsigned* naccept);
  * over the recorded chain, NaN for ACIGNORE parameters; returns POFD_OK, or
  * POFD_REJECTED when some parameter's series was too short (< 50). */
 int pofd_ensemble_acor(pofd_ensemble* e, double* tau);
-/* A multivariate Gaussian test likelihood, log N(theta[0:k]; mean, icov^-1)
- * up to a constant, batched on the device with the pofd_batch_loglike_fn
- * signature (pofd_gauss_eval_batch_device): a target with a known
- * posterior for checking the sampler and the surrogate.  No counterpart in
- * the reference. */
-typedef struct pofd_gauss pofd_gauss;
-int pofd_gauss_create(pofd_ctx* ctx, unsigned k, const double* mean,
-                      const double* icov, pofd_gauss** out);
-int pofd_gauss_destroy(pofd_gauss* g);
-int pofd_gauss_eval_batch_device(void* g, unsigned nprop,
-                                 const float* theta_dev, unsigned npar,
-                                 double* logl_dev, int* status_dev,
-                                 void* stream);
 
 /* ------------------------------------------------------------- surrogate
  * An MLP surrogate of the log-likelihood (inputs: the listed parameters,
@@ -623,17 +610,6 @@ int pofd_likesum_eval_batch_device(void* ls, unsigned nprop,
 int pofd_acor(const float* x, size_t n, double* mean, double* sigma,
               double* tau);
 
-/* Measured FP64 FMA throughput of a device (TFLOP/s, 2 flops per FMA): the
- * denominator of the FP64-bound kernels' roofline.  No counterpart in the
- * reference (which has no GPU code). */
-int pofd_fp64_peak(int device, double* tflops);
-
-/* Self-check of the table-driven exp2 the R builders use (2^x = 2^k T[j]
- * 2^r, T[j] = 2^(j/64), Taylor series for 2^r): the largest relative
- * difference from the CUDA library exp2 over n arguments in [lo, hi), hi <
- * 1023 (below -1022 the table function returns 0; the check then reports
- * its absolute value).  No counterpart in the reference. */
-int pofd_exp2_check(int device, int n, double lo, double hi, double* max_rel);
 
 #ifdef __cplusplus
 }

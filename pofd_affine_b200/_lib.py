@@ -12,6 +12,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "_lib", "libpofd_b200.so")
 HEADER = os.path.join(HERE, "..", "include", "pofd_b200.h")
+SUPPORT_LIBPATH = os.path.join(HERE, "_lib", "libpofd_b200_support.so")
+SUPPORT_HEADER = os.path.join(HERE, "..", "include", "pofd_b200_support.h")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -83,8 +85,6 @@ SIGNATURES = {
     "pofd_like1_set_regularization": (I, [V, D]),
     "pofd_like1_bonus": (I, [V, U, _fp, U, _dp]),
     "pofd_like1_fill_bonus_device": (I, [V, U, V, U, V]),
-    "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
-    "pofd_exp2_check": (I, [I, I, D, D, C.POINTER(D)]),
     "pofd_beam2_create": (I, [_dp, _dp, S, D, D, U, PV]),
     "pofd_beam2_destroy": (I, [V]),
     "pofd_beam2_info": (I, [V, _dp]),
@@ -129,9 +129,6 @@ SIGNATURES = {
     "pofd_ensemble_last": (I, [V, V, V]),
     "pofd_ensemble_naccept": (I, [V, _up]),
     "pofd_ensemble_acor": (I, [V, _dp]),
-    "pofd_gauss_create": (I, [V, U, _dp, _dp, PV]),
-    "pofd_gauss_destroy": (I, [V]),
-    "pofd_gauss_eval_batch_device": (I, [V, U, V, U, V, V, V]),
     "pofd_surrogate_create": (I, [V, U, _ip, U, U, U, C.c_ulonglong, PV]),
     "pofd_surrogate_destroy": (I, [V]),
     "pofd_surrogate_add_pairs": (I, [V, U, V, U, V, V, V]),
@@ -165,7 +162,18 @@ SIGNATURES = {
     "pofd_acor": (I, [_fp, S, C.POINTER(D), C.POINTER(D), C.POINTER(D)]),
 }
 
+# libpofd_b200_support.so (include/pofd_b200_support.h): measurement and
+# test helpers outside the likelihood's ABI
+SUPPORT_SIGNATURES = {
+    "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
+    "pofd_exp2_check": (I, [I, I, D, D, C.POINTER(D)]),
+    "pofd_gauss_create": (I, [I, U, _dp, _dp, PV]),
+    "pofd_gauss_destroy": (I, [V]),
+    "pofd_gauss_eval_batch_device": (I, [V, U, V, U, V, V, V]),
+}
+
 _lib = None
+_support = None
 
 
 class PofdError(RuntimeError):
@@ -193,16 +201,35 @@ def lib():
     return L
 
 
+def support_lib():
+    """The measurement / test helper library (FP64 peak, exp2 self-check,
+    Gaussian test target)."""
+    global _support
+    if _support is not None:
+        return _support
+    if not os.path.exists(SUPPORT_LIBPATH):
+        raise RuntimeError(
+            "libpofd_b200_support.so is not built (%s); run python -m "
+            "pofd_affine_b200.build" % SUPPORT_LIBPATH)
+    L = C.CDLL(SUPPORT_LIBPATH)
+    for name, (res, args) in SUPPORT_SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _support = L
+    return L
+
+
 def check(st):
     if st < 0:
         raise PofdError(st, lib().pofd_last_error().decode())
     return st
 
 
-def declared_functions():
-    """Function names declared in include/pofd_b200.h."""
+def declared_functions(header=HEADER):
+    """Function names declared in a header (default include/pofd_b200.h)."""
     import re
-    txt = open(HEADER).read()
+    txt = open(header).read()
     return sorted(set(re.findall(r"\b(pofd_[a-z0-9_]+)\s*\(", txt)))
 
 

@@ -14,8 +14,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUTDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUTDIR, "libpofd_b200.so")
-SOURCES = ["setup.cc", "fits.cc", "engine1d.cu", "engine2d.cu", "ensemble.cu", "surrogate.cu", "capi.cu", "peaks.cu",
+SOURCES = ["setup.cc", "fits.cc", "engine1d.cu", "engine2d.cu", "ensemble.cu", "surrogate.cu", "capi.cu",
            "noalloc.cu"]
+# measurement and test helpers, kept out of the likelihood's ABI
+SUPPORT_LIB = os.path.join(OUTDIR, "libpofd_b200_support.so")
+SUPPORT_SOURCES = [os.path.join("support", "support.cu")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -26,12 +29,15 @@ def nvcc_path():
 
 
 def _stale():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(SUPPORT_LIB):
         return True
-    t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
-    deps.append(os.path.join(HERE, "..", "include", "pofd_b200.h"))
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    t = min(os.path.getmtime(LIB), os.path.getmtime(SUPPORT_LIB))
+    deps = [os.path.join(d, f) for d in (CSRC, os.path.join(CSRC, "support"))
+            for f in os.listdir(d)]
+    deps += [os.path.join(HERE, "..", "include", h)
+             for h in ("pofd_b200.h", "pofd_b200_support.h")]
+    return any(os.path.getmtime(d) > t for d in deps
+               if os.path.isfile(d))
 
 
 def build(force=False, verbose_ptxas=False):
@@ -58,6 +64,16 @@ def build(force=False, verbose_ptxas=False):
     subprocess.check_call([nvcc] + ARCH + ["-shared", "-o", tmp] + objs +
                           ["-lcufft", "-lcudart"])
     os.replace(tmp, LIB)
+    sobjs = []
+    for src in SUPPORT_SOURCES:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        subprocess.check_call([nvcc] + common + ["-c", os.path.join(CSRC, src),
+                                                 "-o", obj])
+        sobjs.append(obj)
+    tmp = SUPPORT_LIB + ".tmp"
+    subprocess.check_call([nvcc] + ARCH + ["-shared", "-o", tmp] + sobjs +
+                          ["-lcudart"])
+    os.replace(tmp, SUPPORT_LIB)
     return LIB
 
 

@@ -74,11 +74,6 @@ struct pofd_like2 {
   std::unique_ptr<pofd::Engine2> eng;
 };
 
-struct pofd_gauss {
-  pofd_ctx* ctx = nullptr;
-  std::unique_ptr<pofd::GaussLike> g;
-};
-
 struct pofd_surrogate {
   pofd_ctx* ctx = nullptr;
   std::unique_ptr<pofd::Surrogate> s;
@@ -1096,35 +1091,6 @@ int pofd_acor(const float* x, size_t n, double* mean, double* sigma, double* tau
     *sigma = sg;
     *tau = t;
     return rc ? POFD_REJECTED : POFD_OK;
-  });
-}
-
-int pofd_gauss_create(pofd_ctx* ctx, unsigned k, const double* mean, const double* icov,
-                      pofd_gauss** out) {
-  return guard([&] {
-    need(ctx && mean && icov && out, "null argument");
-    std::unique_ptr<pofd_gauss> g(new pofd_gauss());
-    g->ctx = ctx;
-    g->g.reset(new pofd::GaussLike(ctx->device, k, mean, icov));
-    *out = g.release();
-    return POFD_OK;
-  });
-}
-
-int pofd_gauss_destroy(pofd_gauss* g) {
-  if (g && g->ctx && g->ctx->device >= 0) cudaSetDevice(g->ctx->device);
-  delete g;
-  return POFD_OK;
-}
-
-int pofd_gauss_eval_batch_device(void* gv, unsigned nprop, const float* theta, unsigned npar,
-                                 double* logl, int* status, void* stream) {
-  return guard([&] {
-    pofd_gauss* g = static_cast<pofd_gauss*>(gv);
-    need(g && theta && logl && status, "null argument");
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g->ctx->stream;
-    g->g->enqueue(nprop, theta, npar, logl, status, st);
-    return POFD_OK;
   });
 }
 

@@ -853,61 +853,6 @@ int Ensemble::acor(double* tau) const {
   return succ;
 }
 
-// ---------------------------------------------------------------- Gaussian
-namespace {
-// log N(theta; mean, cov) up to a constant: -(1/2) d^T icov d, one thread per
-// proposal; a NaN parameter gives POFD_E_INVALID_MODEL.
-__global__ void k_gauss(unsigned nprop, unsigned npar, unsigned k,
-                        const double* __restrict__ mean,
-                        const double* __restrict__ icov,
-                        const float* __restrict__ theta,
-                        double* __restrict__ logl, int* __restrict__ status) {
-  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nprop) return;
-  const float* x = theta + static_cast<size_t>(t) * npar;
-  double d[Ensemble::kMaxParams];
-  int st = POFD_OK;
-  for (unsigned p = 0; p < k; ++p) {
-    d[p] = static_cast<double>(x[p]) - mean[p];
-    if (isnan(d[p])) st = POFD_E_INVALID_MODEL;
-  }
-  double q = 0.0;
-  for (unsigned a = 0; a < k; ++a) {
-    double r = 0.0;
-    for (unsigned b = 0; b < k; ++b) r += icov[a * k + b] * d[b];
-    q += d[a] * r;
-  }
-  logl[t] = (st == POFD_OK) ? -0.5 * q : __longlong_as_double(0x7ff8000000000000LL);
-  status[t] = st;
-}
-}  // namespace
-
-GaussLike::GaussLike(int device, unsigned k, const double* mean, const double* icov)
-    : device_(device), k_(k) {
-  if (device < 0) throw Error(POFD_E_CUDA, "host-only context has no GPU");
-  if (k == 0 || k > Ensemble::kMaxParams) throw Error(POFD_E_ARG, "dimension must be in [1, 64]");
-  ck(cudaSetDevice(device_), "cudaSetDevice");
-  mean_ = dal<double>(k);
-  icov_ = dal<double>(static_cast<size_t>(k) * k);
-  ck(cudaMemcpy(mean_, mean, k * sizeof(double), cudaMemcpyHostToDevice), "upload");
-  ck(cudaMemcpy(icov_, icov, static_cast<size_t>(k) * k * sizeof(double), cudaMemcpyHostToDevice),
-     "upload");
-}
-
-GaussLike::~GaussLike() {
-  cudaSetDevice(device_);
-  cudaFree(mean_);
-  cudaFree(icov_);
-}
-
-void GaussLike::enqueue(unsigned nprop, const float* theta, unsigned npar, double* logl,
-                        int* status, cudaStream_t st) const {
-  if (npar < k_) throw Error(POFD_E_ARG, "Not enough elements in params");
-  if (nprop == 0) return;
-  k_gauss<<<(nprop + 127) / 128, 128, 0, st>>>(nprop, npar, k_, mean_, icov_, theta, logl, status);
-  ck(cudaGetLastError(), "k_gauss");
-}
-
 // ------------------------------------------------------------ LikeSum
 namespace {
 __global__ void k_lsum(unsigned nprop, unsigned k, unsigned cap, const double* __restrict__ l,

@@ -136,22 +136,6 @@ class Ensemble {
   unsigned long long* nfail_ = nullptr;
 };
 
-// A multivariate Gaussian log-density on the first k parameters: a test
-// target for the sampler and the surrogate (known posterior).
-class GaussLike {
- public:
-  GaussLike(int device, unsigned k, const double* mean, const double* icov);
-  ~GaussLike();
-  void enqueue(unsigned nprop, const float* theta, unsigned npar, double* logl,
-               int* status, cudaStream_t st) const;
-
- private:
-  int device_;
-  unsigned k_;
-  double* mean_ = nullptr;
-  double* icov_ = nullptr;
-};
-
 // Sum of several batched likelihoods on the same proposals (fields of
 // different FFT sizes fitted jointly): the members run concurrently on
 // forked streams and join into one sum, so a captured step holds all of

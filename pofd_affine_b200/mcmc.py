@@ -15,7 +15,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import PofdError, check, lib  # noqa: F401
+from ._lib import PofdError, check, lib, support_lib  # noqa: F401
 
 FIXED, ACIGNORE, BONUS = 1, 2, 4  # mcmc_affine (global_settings.h:57)
 
@@ -79,16 +79,18 @@ class gaussLike:
     """log N(theta[:k]; mean, cov) up to a constant, batched on the GPU."""
 
     def __init__(self, ctx, mean, cov):
+        from ._lib import support_lib
         mean = np.ascontiguousarray(mean, dtype=np.float64)
         icov = np.ascontiguousarray(np.linalg.inv(np.asarray(cov, np.float64)))
         h = C.c_void_p()
-        check(lib().pofd_gauss_create(ctx.h, mean.size, mean, icov,
-                                      C.byref(h)))
+        check(support_lib().pofd_gauss_create(ctx.device, mean.size, mean,
+                                              icov, C.byref(h)))
         self.h, self.ctx, self.k = h, ctx, mean.size
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_gauss_destroy(self.h)
+            from ._lib import support_lib
+            support_lib().pofd_gauss_destroy(self.h)
             self.h = None
 
 
@@ -111,7 +113,7 @@ class likeSum:
         elif isinstance(like, calcLikeDouble):
             check(lib().pofd_likesum_add_like2(self.h, like.h))
         elif isinstance(like, gaussLike):
-            fn = C.cast(lib().pofd_gauss_eval_batch_device, C.c_void_p)
+            fn = C.cast(support_lib().pofd_gauss_eval_batch_device, C.c_void_p)
             check(lib().pofd_likesum_add(self.h, fn, like.h))
         else:
             raise PofdError(-10, "unsupported likelihood object")
@@ -144,7 +146,7 @@ class affineEnsemble:
         elif isinstance(like, calcLikeDouble):
             check(lib().pofd_ensemble_use_like2(h, like.h))
         elif isinstance(like, gaussLike):
-            fn = C.cast(lib().pofd_gauss_eval_batch_device, C.c_void_p)
+            fn = C.cast(support_lib().pofd_gauss_eval_batch_device, C.c_void_p)
             check(lib().pofd_ensemble_set_likelihood(h, fn, like.h))
         elif isinstance(like, likeSum):
             fn = C.cast(lib().pofd_likesum_eval_batch_device, C.c_void_p)

@@ -18,6 +18,21 @@ def test_every_declared_symbol_is_exported(built_lib):
     assert set(decl) <= set(_lib.SIGNATURES), set(decl) - set(_lib.SIGNATURES)
 
 
+def test_support_library_exports_its_header(built_lib):
+    """The measurement and test helpers live in libpofd_b200_support.so,
+    declared in include/pofd_b200_support.h, and none of them in the
+    likelihood's ABI."""
+    from pofd_affine_b200 import _lib
+    raw = C.CDLL(_lib.SUPPORT_LIBPATH)
+    decl = _lib.declared_functions(_lib.SUPPORT_HEADER)
+    assert set(decl) == set(_lib.SUPPORT_SIGNATURES)
+    missing = [n for n in decl if not hasattr(raw, n)]
+    assert not missing, missing
+    main = C.CDLL(built_lib)
+    assert not [n for n in decl if hasattr(main, n)]
+    assert not set(decl) & set(_lib.declared_functions())
+
+
 def test_version_and_no_error(built_lib):
     from pofd_affine_b200._lib import lib
     assert b"pofd_affine 0.5.1" in lib().pofd_version()
