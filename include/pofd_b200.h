@@ -216,19 +216,18 @@ int pofd_like1_fft_info(pofd_like1* L, int* own);
  * GPU and no counterpart): times the whole graph-captured launch sequence on
  * nprop host rows (reps replays per candidate, CUDA events) for each knob in
  * turn -- own FFT vs cuFFT, R-fill points per thread {4, 8, 16}, R-node
- * threads per block {64, 128, 256}, R grid fill fused into the forward FFT
- * pass or not, FFT pass feeding (fft_persist 0: plain passes, 1: persistent
- * passes prefetching into registers, 2: pass B fed by bulk copies through a
- * shared-memory ring), spectrum blocks per row {2 ... 32} -- and keeps the
- * fastest.  out8 (optional) = {own_fft,
- * rfill_per, rnodes_threads, spec_blocks, fft_persist, rfill_fused, best ms,
- * untuned ms}.  get/set_tuning read or impose the six knobs in that order
- * (e.g. a tuning saved from an earlier run).  Results change only by
- * rounding (reduction grouping, FFT implementation). */
+ * threads per block {64, 128, 256}, the R grid fill (0: materialised, 1:
+ * inside the forward FFT pass A with one exp2 per grid point, 2: inside it
+ * by running products over 16-point segments), spectrum blocks per row
+ * {2 ... 32} -- and keeps the fastest.  out7 (optional) = {own_fft,
+ * rfill_per, rnodes_threads, spec_blocks, rfill_fused, best ms, untuned ms}.
+ * get/set_tuning read or impose the five knobs in that order (e.g. a tuning
+ * saved from an earlier run).  Results change only by rounding (reduction
+ * grouping, FFT implementation, exponential evaluation). */
 int pofd_like1_autotune(pofd_like1* L, unsigned nprop, const float* theta,
-                        unsigned npar, int reps, double* out8);
-int pofd_like1_get_tuning(const pofd_like1* L, int* knobs6);
-int pofd_like1_set_tuning(pofd_like1* L, const int* knobs6);
+                        unsigned npar, int reps, double* out7);
+int pofd_like1_get_tuning(const pofd_like1* L, int* knobs5);
+int pofd_like1_set_tuning(pofd_like1* L, const int* knobs5);
 
 /* Priors added once to the summed log-likelihood, in the reference's order
  * (calcLike.cc:918-952): a Gaussian on the sigma multiplier about 1, on <S>

@@ -802,288 +802,6 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
   }
 }
 
-// Persistent forms of passes A and B (m1 >= 16): a grid of about two
-// blocks per SM walks the tiles (row, column block) / (row, row block); as
-// soon as a tile's inputs have gone through the first register DFT into the
-// shared-memory exchange, the next tile's loads are issued into the same
-// registers, so they are in flight while the second stage and the stores of
-// the current tile run.  Same arithmetic as k_fftA / k_fftB; rows of failed
-// proposals are transformed on zeros and not stored.
-template <int L2, int S>
-__device__ __forceinline__ void fftAP_load(double2* v, int tile, const double2* __restrict__ in,
-                                           int rowsz, int nrows_per_w,
-                                           const int* __restrict__ mstatus,
-                                           const int* __restrict__ kcut, int b, int n2) {
-  constexpr int M1 = 16 * L2, m = M1 * 256, CB = 256 / L2;
-  const int row = tile / L2, b0 = (tile % L2) * CB;
-  const double2* src = in + static_cast<size_t>(row) * rowsz;
-  const int kc = kcut ? kcut[row] : m;
-  const bool skip = mstatus[row / nrows_per_w] != 0;
-#pragma unroll
-  for (int n1 = 0; n1 < 16; ++n1) {
-    const int a = L2 * n1 + n2;
-    v[n1] = (skip || row_cut(a, m, kc)) ? make_double2(0.0, 0.0) : src[a * 256 + b0 + b];
-  }
-}
-
-template <int L2, int S>
-__global__ void __launch_bounds__(256, 2)
-k_fftAP(int rows, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
-        const double2* __restrict__ in, double2* __restrict__ out,
-        const double2* __restrict__ WH, const double2* __restrict__ WL,
-        const int* __restrict__ kcut) {
-  constexpr int L1 = 16, M1 = L1 * L2, M2 = 256, m = M1 * M2, CB = 256 / L2, NH = m / 128;
-  extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L
-  double2* Hs = fs + 256 * L1;
-  const double2* Ls = Hs + NH;
-  const int t = threadIdx.x;
-  const int b = t % CB, n2 = t / CB;
-  const int ntiles = rows * L2;
-  int tile = blockIdx.x;
-  double2 v[L1];
-  fft::load_tw2(Hs, WH, WL, NH, t, 256);
-  if (tile < ntiles) fftAP_load<L2, S>(v, tile, in, rowsz, nrows_per_w, mstatus, kcut, b, n2);
-  __syncthreads();
-  for (; tile < ntiles; tile += gridDim.x) {
-    const int row = tile / L2, b0 = (tile % L2) * CB;
-    const bool skip = mstatus[row / nrows_per_w] != 0;
-    double2* dst = out + static_cast<size_t>(row) * rowsz;
-    fft::dft<L1, S>(v);
-#pragma unroll
-    for (int k1 = 0; k1 < L1; ++k1) {
-      if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, (m / M1) * n2 * k1));
-      fs[(n2 * L1 + k1) * CB + b] = v[k1];
-    }
-    const int next = tile + static_cast<int>(gridDim.x);
-    if (next < ntiles) fftAP_load<L2, S>(v, next, in, rowsz, nrows_per_w, mstatus, kcut, b, n2);
-    __syncthreads();
-#pragma unroll
-    for (int it = 0; it < L1 / L2; ++it) {
-      const int e = t + 256 * it;
-      const int bb = e % CB, k1 = e / CB;
-      double2 u[L2];
-#pragma unroll
-      for (int q = 0; q < L2; ++q) u[q] = fs[(q * L1 + k1) * CB + bb];
-      fft::dft<L2, S>(u);
-      if (!skip) {
-#pragma unroll
-        for (int k2 = 0; k2 < L2; ++k2) {
-          const int c = k1 + L1 * k2;
-          const int gb = b0 + bb;
-          dst[c * M2 + gb] = (c * gb) ? fft::cmul(u[k2], fft::tw2<S>(Hs, Ls, c * gb)) : u[k2];
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
-template <int S>
-__global__ void __launch_bounds__(256, 2)
-k_fftBP(int m1, int rows, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
-        const double2* __restrict__ in, double2* __restrict__ out,
-        const double2* __restrict__ WH, const double2* __restrict__ WL,
-        const int* __restrict__ kcut) {
-  extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then H, L
-  double2* Hs = fs + 16 * 16 * 17;
-  const double2* Ls = Hs + 2 * m1;
-  const int m = m1 * 256;
-  const int tpr = m1 / 16;  // row blocks per row
-  const int ntiles = rows * tpr;
-  const int t = threadIdx.x;
-  const int n2 = t & 15, r = t >> 4;
-  int tile = blockIdx.x;
-  double2 v[16];
-  auto load = [&](int tl) {
-    const int row = tl / tpr, c0 = (tl % tpr) * 16;
-    const double2* src = in + static_cast<size_t>(row) * rowsz;
-    const bool skip = mstatus[row / nrows_per_w] != 0;
-#pragma unroll
-    for (int n1 = 0; n1 < 16; ++n1)
-      v[n1] = skip ? make_double2(0.0, 0.0) : src[(c0 + r) * 256 + 16 * n1 + n2];
-  };
-  fft::load_tw2(Hs, WH, WL, 2 * m1, t, 256);
-  if (tile < ntiles) load(tile);
-  __syncthreads();
-  for (; tile < ntiles; tile += gridDim.x) {
-    const int row = tile / tpr, c0 = (tile % tpr) * 16;
-    const bool skip = mstatus[row / nrows_per_w] != 0;
-    double2* dst = out + static_cast<size_t>(row) * rowsz;
-    const int kc = kcut ? kcut[row] : m;
-    fft::dft<16, S>(v);
-#pragma unroll
-    for (int k1 = 0; k1 < 16; ++k1) {
-      if (n2 * k1) v[k1] = fft::cmul(v[k1], fft::tw2<S>(Hs, Ls, (m / 256) * n2 * k1));
-      fs[(k1 * 16 + n2) * 17 + r] = v[k1];
-    }
-    const int next = tile + static_cast<int>(gridDim.x);
-    if (next < ntiles) load(next);
-    __syncthreads();
-    {
-      const int rr = t & 15, k1 = t >> 4;
-      double2 u[16];
-#pragma unroll
-      for (int q = 0; q < 16; ++q) u[q] = fs[(k1 * 16 + q) * 17 + rr];
-      fft::dft<16, S>(u);
-      if (!skip) {
-#pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2) {
-          // bins beyond the noise cut-off are never read (forward transform)
-          const int k = (c0 + rr) + m1 * (k1 + 16 * k2);
-          if (min(k, m - k) <= kc) dst[k] = u[k2];
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Pass B fed by bulk copies: a persistent grid (one CTA per SM) walks the
-// tiles (row, rb = min(16, m1) rows c) -- each a contiguous rb * 4 KB run of
-// Y -- through a two-stage shared-memory ring.  Thread 0 issues
-// cp.async.bulk (no multicast) for tile i + 2 as soon as every thread has
-// read tile i out of its stage, so the copy of the next tiles is in flight
-// while a tile is transformed; completion is counted in bytes on the stage's
-// mbarrier.  Same arithmetic as k_fftB.  Every wait is bounded: on a timeout
-// the CTA records kErrTimeout in *err, waits (bounded) for its copies in
-// flight and returns.  Rows of failed proposals are transformed and not
-// stored.
-constexpr int kBTStages = 2;
-constexpr unsigned kBTSpin = 1u << 22;
-constexpr int kErrTimeout = 1;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ bool bt_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_addr(bar);
-  for (unsigned it = 0; it < kBTSpin; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-__device__ __forceinline__ void bt_load(void* dst, const void* src, uint32_t bytes,
-                                        uint64_t* bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes),
-               "r"(smem_addr(bar))
-               : "memory");
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-      ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes),
-      "r"(smem_addr(bar))
-      : "memory");
-}
-
-inline size_t fftBT_smem(int m1) {
-  return (static_cast<size_t>(kBTStages) * FRB * 256 + 16 * 16 * 17 + 256) *
-             sizeof(double2) +
-         kBTStages * sizeof(uint64_t);
-}
-
-template <int S>
-__global__ void __launch_bounds__(256, 1)
-k_fftBT(int m1, int rows, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
-        const double2* __restrict__ in, double2* __restrict__ out,
-        const double2* __restrict__ WH, const double2* __restrict__ WL,
-        const int* __restrict__ kcut, int* __restrict__ err) {
-  extern __shared__ __align__(128) double2 smb[];
-  double2* stage = smb;                           // [kBTStages][FRB * 256]
-  double2* fs = stage + kBTStages * FRB * 256;    // [(k1 * 16 + n2) * 17 + r]
-  double2* Ts = fs + 16 * 16 * 17;  // inter-stage twiddles W_256^{n2 k1} (symmetric)
-  uint64_t* full = reinterpret_cast<uint64_t*>(Ts + 256);
-  const int rb = min(FRB, m1);
-  const int tpr = m1 / rb;  // tiles per row
-  const int ntiles = rows * tpr;
-  const int m = m1 * 256;
-  const int t = threadIdx.x;
-  const uint32_t bytes = static_cast<uint32_t>(rb) * 256 * sizeof(double2);
-  auto src_of = [&](int tl) {
-    return in + static_cast<size_t>(tl / tpr) * rowsz + (tl % tpr) * rb * 256;
-  };
-  if (t == 0) {
-    for (int s = 0; s < kBTStages; ++s)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[s])) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  Ts[t] = fft::tw2<S>(WH, WL, (m / 256) * (t >> 4) * (t & 15));
-  __syncthreads();
-  if (t == 0) {
-    for (int s = 0; s < kBTStages; ++s) {
-      const int tl = blockIdx.x + s * static_cast<int>(gridDim.x);
-      if (tl < ntiles) bt_load(stage + s * FRB * 256, src_of(tl), bytes, &full[s]);
-    }
-  }
-  int it = 0;
-  bool aborted = false;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-    const int s = it % kBTStages;
-    const bool ok = bt_wait(&full[s], static_cast<uint32_t>((it / kBTStages) & 1));
-    // also orders the previous tile's exchange reads before this tile's writes
-    if (__syncthreads_or(!ok)) {
-      aborted = true;
-      break;
-    }
-    const int row = tile / tpr, c0 = (tile % tpr) * rb;
-    const double2* st = stage + s * FRB * 256;
-    if (t < 16 * rb) {
-      const int n2 = t & 15, r = t >> 4;
-      double2 v[16];
-#pragma unroll
-      for (int n1 = 0; n1 < 16; ++n1) v[n1] = st[r * 256 + 16 * n1 + n2];
-      fft::dft<16, S>(v);
-#pragma unroll
-      for (int k1 = 0; k1 < 16; ++k1) {
-        if (n2 * k1) v[k1] = fft::cmul(v[k1], Ts[k1 * 16 + n2]);
-        fs[(k1 * 16 + n2) * 17 + r] = v[k1];
-      }
-    }
-    __syncthreads();  // stage s read out, exchange written
-    if (t == 0) {
-      const int nx = tile + kBTStages * static_cast<int>(gridDim.x);
-      if (nx < ntiles) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        bt_load(stage + s * FRB * 256, src_of(nx), bytes, &full[s]);
-      }
-    }
-    if (t < 16 * rb && mstatus[row / nrows_per_w] == 0) {
-      const int r = t % rb, k1 = t / rb;
-      double2* dst = out + static_cast<size_t>(row) * rowsz;
-      const int kc = kcut ? kcut[row] : m;
-      double2 u[16];
-#pragma unroll
-      for (int n2 = 0; n2 < 16; ++n2) u[n2] = fs[(k1 * 16 + n2) * 17 + r];
-      fft::dft<16, S>(u);
-#pragma unroll
-      for (int k2 = 0; k2 < 16; ++k2) {
-        // bins beyond the noise cut-off are never read (forward transform)
-        const int k = (c0 + r) + m1 * (k1 + 16 * k2);
-        if (min(k, m - k) <= kc) dst[k] = u[k2];
-      }
-    }
-  }
-  if (aborted && t == 0) {
-    if (err) atomicCAS(err, 0, kErrTimeout);
-    // let the copies in flight land before the CTA's shared memory goes
-    // away: iterations up to it + 1 had their copies issued; the last one
-    // into stage s completes that stage's phase (last / kBTStages)
-    const int nit = (ntiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
-                    static_cast<int>(gridDim.x);
-    const int hi = min(it + kBTStages - 1, nit - 1);
-    for (int s = 0; s < kBTStages; ++s) {
-      const int last = hi - ((hi - s) % kBTStages + kBTStages) % kBTStages;
-      if (last >= 0) bt_wait(&full[s], static_cast<uint32_t>((last / kBTStages) & 1));
-    }
-  }
-}
-
 // Pass B: 256-point DFTs along rows c0..c0+15 of Y (16 x 16 split), stored
 // in natural order Z[c + m1 d].
 template <int S>
@@ -1585,16 +1303,10 @@ __global__ void k_reduce1(const BSet1Dev* __restrict__ bsets, int B, int D,
                           int nprop, const int* __restrict__ mstatus,
                           const double* __restrict__ sigmult,
                           const PDInfo1* __restrict__ pinfo, Prior1 pr,
-                          const double* __restrict__ bonus, const int* __restrict__ err,
+                          const double* __restrict__ bonus,
                           double* __restrict__ logl, int* __restrict__ status) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= nprop) return;
-  if (err && *err != 0) {
-    // a bounded wait of the FFT passes timed out: no result is valid
-    logl[w] = __longlong_as_double(0x7ff8000000000000LL);
-    status[w] = POFD_E_CUDA;
-    return;
-  }
   if (mstatus[w] != 0) {
     logl[w] = __longlong_as_double(0x7ff8000000000000LL);
     status[w] = mstatus[w];
@@ -1838,44 +1550,10 @@ void fftA_attr() {
 }
 
 constexpr size_t kFftBSmemMax = (16 * 16 * 17 + 256) * sizeof(double2);
-constexpr size_t kFftBPSmemMax = (16 * 16 * 17 + 2 * 256 + 128) * sizeof(double2);
 
-template <int S>
-void launch_fftAP(int m1, int rows, int grid, cudaStream_t st, int rowsz, int nrw,
-                  const int* mstatus, const double2* in, double2* out, const double2* WH,
-                  const double2* WL, const int* kcut) {
-  const size_t sm = fftA_smem(m1);
-#define POFD_FFTAP(L2)                                                                     \
-  k_fftAP<L2, S><<<grid, 256, sm, st>>>(rows, rowsz, nrw, mstatus, in, out, WH, WL, kcut)
-  switch (m1) {
-    case 16: POFD_FFTAP(1); break;
-    case 32: POFD_FFTAP(2); break;
-    case 64: POFD_FFTAP(4); break;
-    case 128: POFD_FFTAP(8); break;
-    case 256: POFD_FFTAP(16); break;
-    default: throw Error(POFD_E_ARG, "persistent FFT pass: unsupported size");
-  }
-#undef POFD_FFTAP
-}
-
-template <int S>
-void fftAP_attr() {
-  const int sm = static_cast<int>(kFftASmemMax);
-  cuda_check(cudaFuncSetAttribute(k_fftAP<1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAP<2, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAP<4, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAP<8, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAP<16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftBP<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(kFftBPSmemMax)), "attr");
-}
 // pass B: the exchange and the inter-stage table (its twiddles are W_256
 // powers only)
 inline size_t fftB_smem(int) { return kFftBSmemMax; }
-// persistent pass B: exchange plus the H and L tables
-inline size_t fftBP_smem(int m1) {
-  return (16 * 16 * 17 + 2 * static_cast<size_t>(m1) + 128) * sizeof(double2);
-}
 }  // namespace
 
 
@@ -2366,7 +2044,6 @@ void Engine1::set_tuning(const Tune1& t) {
   if (t.rnodes_threads != 64 && t.rnodes_threads != 128 && t.rnodes_threads != 256)
     throw Error(POFD_E_ARG, "rnodes_threads must be 64, 128 or 256");
   if (t.spec_blocks < 1 || t.spec_blocks > 64) throw Error(POFD_E_ARG, "spec_blocks must be in [1, 64]");
-  if (t.fft_persist < 0 || t.fft_persist > 2) throw Error(POFD_E_ARG, "fft_persist must be 0, 1 or 2");
   if (t.rfill_fused < 0 || t.rfill_fused > 2) throw Error(POFD_E_ARG, "rfill_fused must be 0, 1 or 2");
   const bool fft_changed = (t.own_fft != 0) != (tune_.own_fft != 0);
   tune_ = t;
@@ -2379,7 +2056,7 @@ void Engine1::set_tuning(const Tune1& t) {
 // Coordinate descent over the knobs, one pass, each candidate timed on the
 // captured graph of the whole sequence.  The FFT choice is tried only where
 // the own FFT supports the size.
-void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out8) {
+void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7) {
   NvtxRange nvtx_range("pofd like1 autotune");
   if (nprop == 0 || reps < 1) throw Error(POFD_E_ARG, "autotune needs rows and reps >= 1");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
@@ -2421,14 +2098,6 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     }
   }
   if (best.own_fft && own_possible) {
-    for (int fp : {0, 1, 2}) {
-      if (fp == best.fft_persist || (fp == 1 && n_ / 512 < 16)) continue;
-      Tune1 t = best;
-      t.fft_persist = fp;
-      trial(t);
-    }
-  }
-  if (best.own_fft && own_possible) {
     for (int sb : {2, 4, 8, 16, 32}) {
       if (sb == best.spec_blocks) continue;
       Tune1 t = best;
@@ -2437,15 +2106,14 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     }
   }
   set_tuning(best);
-  if (out8) {
-    out8[0] = best.own_fft;
-    out8[1] = best.rfill_per;
-    out8[2] = best.rnodes_threads;
-    out8[3] = best.spec_blocks;
-    out8[4] = best.fft_persist;
-    out8[5] = best.rfill_fused;
-    out8[6] = best_ms;
-    out8[7] = t_untuned;
+  if (out7) {
+    out7[0] = best.own_fft;
+    out7[1] = best.rfill_per;
+    out7[2] = best.rnodes_threads;
+    out7[3] = best.spec_blocks;
+    out7[4] = best.rfill_fused;
+    out7[5] = best_ms;
+    out7[6] = t_untuned;
   }
 }
 
@@ -2563,8 +2231,7 @@ void Engine1::free_work() {
   void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.nodes, ws_.spl,
                   ws_.rbuf, ws_.rpart, ws_.mom, ws_.pbuf, ws_.ppart,
                   ws_.pmidx, ws_.pinfo, ws_.pdout, ws_.theta_in, ws_.logl,
-                  ws_.tmp, ws_.bonus, ws_.kcut_set, ws_.kcut_ds,
-                  ws_.err};
+                  ws_.tmp, ws_.bonus, ws_.kcut_set, ws_.kcut_ds};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ws_.h_theta) cudaFreeHost(ws_.h_theta);
@@ -2601,23 +2268,12 @@ void Engine1::reserve(unsigned P) {
     fftA_attr<-1>();
     fftA_attr<1>();
     fftAR_attr();
-    if (n_ / 512 >= 16) {
-      fftAP_attr<-1>();
-      fftAP_attr<1>();
-    }
     cuda_check(cudaFuncSetAttribute(k_fftB<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kFftBSmemMax)), "attr");
     cuda_check(cudaFuncSetAttribute(k_fftB<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kFftBSmemMax)), "attr");
-    const int bt = static_cast<int>(fftBT_smem(static_cast<int>(n_ / 512)));
-    cuda_check(cudaFuncSetAttribute(k_fftBT<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt),
-               "attr");
-    cuda_check(cudaFuncSetAttribute(k_fftBT<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bt),
-               "attr");
   }
   ws_.mom = dalloc<double>(static_cast<size_t>(P) * B_ * 4);
-  ws_.err = dalloc<int>(1);
-  cuda_check(cudaMemset(ws_.err, 0, sizeof(int)), "cudaMemset");
   ws_.kcut_set = dalloc<int>(static_cast<size_t>(P) * B_);
   ws_.kcut_ds = dalloc<int>(static_cast<size_t>(P) * D_);
   ws_.pbuf = dalloc<double>(static_cast<size_t>(P) * D_ * nc2);
@@ -2719,29 +2375,10 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                                     ws_.mom, ws_.kcut_set, ws_.kcut_ds);
     mark(4);
     const int rb_rows = m1 < FRB ? m1 : FRB;
-    const bool persist = tune_.fft_persist == 1 && m1 >= 16;
-    const bool bulkB = tune_.fft_persist == 2;
-    const int gA = std::min(P * B * (m1 / 16 > 0 ? m1 / 16 : 1), 2 * sm_count_);
-    if (bulkB) {
-      // cleared once per sequence, before the first pass that may set it
-      cuda_check(cudaMemsetAsync(ws_.err, 0, sizeof(int), st), "cudaMemsetAsync");
-      if (!fused)
-        launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
-      const int gB = std::min(P * B * (m1 / rb_rows), sm_count_);
-      k_fftBT<-1><<<gB, 256, fftBT_smem(m1), st>>>(m1, P * B, rowsz, B, ws_.mstatus, tmp, rb,
-                                                   d_wh_, d_wl_, ws_.kcut_set, ws_.err);
-    } else if (fused) {
-      k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, fftB_smem(m1), st>>>(
-          m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_, ws_.kcut_set);
-    } else if (persist) {
-      launch_fftAP<-1>(m1, P * B, gA, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
-      k_fftBP<-1><<<gA, 256, fftBP_smem(m1), st>>>(m1, P * B, rowsz, B, ws_.mstatus, tmp, rb,
-                                                  d_wh_, d_wl_, ws_.kcut_set);
-    } else {
+    if (!fused)
       launch_fftA<-1>(m1, P * B, st, rowsz, B, ws_.mstatus, rb, tmp, d_wh_, d_wl_, nullptr);
-      k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, fftB_smem(m1), st>>>(
-          m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_, ws_.kcut_set);
-    }
+    k_fftB<-1><<<dim3(m1 / rb_rows, P * B), 256, fftB_smem(m1), st>>>(
+        m1, rowsz, B, ws_.mstatus, tmp, rb, d_wh_, d_wl_, ws_.kcut_set);
     mark(5);
     {
       // a few blocks per row loop over the pairs up to the row's cut-off
@@ -2751,22 +2388,9 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                         ws_.kcut_ds);
     }
     mark(6);
-    if (bulkB) {
-      launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_, ws_.kcut_ds);
-      const int gB = std::min(P * D * (m1 / rb_rows), sm_count_);
-      k_fftBT<1><<<gB, 256, fftBT_smem(m1), st>>>(m1, P * D, rowsz, D, ws_.mstatus, tmp, pb,
-                                                  d_wh_, d_wl_, nullptr, ws_.err);
-    } else if (persist) {
-      const int gI = std::min(P * D * (m1 / 16), 2 * sm_count_);
-      launch_fftAP<1>(m1, P * D, gI, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_,
-                      ws_.kcut_ds);
-      k_fftBP<1><<<gI, 256, fftBP_smem(m1), st>>>(m1, P * D, rowsz, D, ws_.mstatus, tmp, pb,
-                                                 d_wh_, d_wl_, nullptr);
-    } else {
-      launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_, ws_.kcut_ds);
-      k_fftB<1><<<dim3(m1 / rb_rows, P * D), 256, fftB_smem(m1), st>>>(
-          m1, rowsz, D, ws_.mstatus, tmp, pb, d_wh_, d_wl_, nullptr);
-    }
+    launch_fftA<1>(m1, P * D, st, rowsz, D, ws_.mstatus, pb, tmp, d_wh_, d_wl_, ws_.kcut_ds);
+    k_fftB<1><<<dim3(m1 / rb_rows, P * D), 256, fftB_smem(m1), st>>>(
+        m1, rowsz, D, ws_.mstatus, tmp, pb, d_wh_, d_wl_, nullptr);
   } else {
     {
       dim3 grid(ntile_, P * B);
@@ -2809,7 +2433,6 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
   mark(9);
   k_reduce1<<<(P + 127) / 128, 128, 0, st>>>(d_bsets_, B, D, P, ws_.mstatus,
                                             ws_.sigmult, ws_.pinfo, prior_, ws_.bonus,
-                                            own_fft_ && tune_.fft_persist == 2 ? ws_.err : nullptr,
                                             logl, status);
   mark(10);
   cuda_check(cudaGetLastError(), "kernel launch");

@@ -106,7 +106,6 @@ struct Workspace1 {
   double* mom = nullptr;     // [P][B][4] mean, var, shift, doshift
   int* kcut_set = nullptr;   // [P][B] noise cut-off of the forward spectrum
   int* kcut_ds = nullptr;    // [P][D] noise cut-off of each dataset's spectrum
-  int* err = nullptr;        // [1] device error word (bounded waits that timed out)
   double* pbuf = nullptr;    // [P][D][2*(n/2+1)] spectrum / P(D)
   double* tmp = nullptr;     // [P][max(B,D)][2*(n/2+1)] own-FFT pass-A rows
   double* ppart = nullptr;   // [P][D][nchunk][4] max, sum, wsum, minval
@@ -132,11 +131,8 @@ struct Tune1 {
   int rfill_per = 8;        // R grid points per thread of k_rfill1 (4, 8, 16)
   int rnodes_threads = 128; // threads per block of k_rnodes1 (64, 128, 256)
   int spec_blocks = 8;      // blocks per row of k_spectrum1f (2 ... 32)
-  int fft_persist = 0;      // 0: plain FFT passes; 1: persistent passes that
-                            // prefetch into registers (m1 >= 16); 2: pass B
-                            // fed by bulk copies through a shared-memory ring
-  int rfill_fused = 2;      // R grid fill inside the forward pass A (own FFT,
-                            // not with fft_persist = 1): 0 no, 1 one exp2
+  int rfill_fused = 2;      // R grid fill inside the forward pass A (own
+                            // FFT): 0 no, 1 one exp2
                             // per grid point, 2 running products over
                             // segments of 16 points in one node interval
 };
@@ -179,7 +175,7 @@ class Engine1 {
   }
   // the R grid fill runs inside the forward FFT pass A (own FFT, plain passes)
   bool fused_fill() const {
-    return own_fft_ && tune_.rfill_fused && !(tune_.fft_persist == 1 && n_ / 512 >= 16);
+    return own_fft_ && tune_.rfill_fused;
   }
   // priors (calcLike::setSigmaPrior / setCFIRBPrior / setPoissonPrior /
   // setRegularizationAlpha and their unset forms, calcLike.h:251-269)
@@ -191,9 +187,9 @@ class Engine1 {
   // Times the full launch sequence (graph replays, CUDA events) for the
   // candidate values of each knob in turn on nprop host rows and keeps the
   // fastest; out (optional) receives {own_fft, rfill_per, rnodes_threads,
-  // spec_blocks, fft_persist, rfill_fused, best ms per launch, untuned ms per
+  // spec_blocks, rfill_fused, best ms per launch, untuned ms per
   // launch}.
-  void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out8);
+  void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7);
   const Tune1& tuning() const { return tune_; }
   void set_tuning(const Tune1& t);
   // <S>, <S^2> of each proposal's model (calcLike::fillBonusParams,
