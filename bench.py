@@ -54,6 +54,8 @@ def args():
     p.add_argument("--no-mcmc", action="store_true")
     p.add_argument("--mcmc-2d", type=int, default=1,
                    help="include the two-field 2D MCMC comparison")
+    p.add_argument("--mcmc-steps", type=int, default=1000,
+                   help="recorded steps of each 2D MCMC run")
     p.add_argument("--profile-case", choices=["1d", "2d", "surrogate"],
                    help="run a small fixed workload for a profiler and exit "
                         "(--batch proposals or pairs, --reps repetitions)")
@@ -461,10 +463,32 @@ def measure_2d(a, ctx, stream):
 
 
 # ---------------------------------------------------------------- MCMC
+def _device_ms(fn, reps=50):
+    """Mean device time of fn() (which enqueues on torch's current stream)
+    by CUDA events, after one warm call."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def mcmc_1d(ctx):
     """Plain vs delayed-acceptance stretch move on the 1D plain fit (6
-    knots, n = 4096, 40 walkers, fixed burn 200, 500 recorded steps)."""
+    knots, n = 4096, 40 walkers, fixed burn 200, 500 recorded steps), with
+    the cost of one half-ensemble's exact likelihood and of its surrogate
+    screening (the 1D exact step is latency-bound, so the screening cannot
+    save much)."""
+    import ctypes as C
+    import torch
     from pofd_affine_b200 import runner, synth
+    from pofd_affine_b200._lib import lib
     from pofd_affine_b200.mcmc import affineEnsemble
     from pofd_affine_b200.surrogate import Surrogate
     cfg = synth.config_1d_small(seed=1)
@@ -486,38 +510,51 @@ def mcmc_1d(ctx):
     hold = (ch[pick], plain["logl"].reshape(-1)[pick])
     S = Surrogate(ctx, npar, list(range(nk)), hidden=256, seed=7)
     da = runner.run_da(ens(22), S, 200, 500, train_iters=1000, holdout=hold)
-    return _mcmc_summary("1D plain fit: 6 knots 2-400 mJy, n=4096, one "
-                         "256x256 map, 40 walkers, burn 200, 500 steps; MLP "
-                         "6 -> 3x256 SiLU -> 1", plain, da, list(range(nk)))
+    out = _mcmc_summary("1D plain fit: 6 knots 2-400 mJy, n=4096, one "
+                        "256x256 map, 40 walkers, burn 200, 500 steps; MLP "
+                        "6 -> 3x256 SiLU -> 1", plain, da, list(range(nk)))
+    # one half-ensemble (20 proposals): exact likelihood vs surrogate
+    th = torch.from_numpy(np.ascontiguousarray(ch[:20])).cuda()
+    ll = torch.empty(20, dtype=torch.float64, device="cuda")
+    st = torch.empty(20, dtype=torch.int32, device="cuda")
+    sp = torch.cuda.current_stream().cuda_stream
+    exact_ms = _device_ms(lambda: L.getLogLikeDevice(
+        20, th.data_ptr(), npar, ll.data_ptr(), st.data_ptr(), sp))
+    sur_ms = _device_ms(lambda: lib().pofd_surrogate_predict_device(
+        S.h, 20, C.c_void_p(th.data_ptr()), npar, C.c_void_p(ll.data_ptr()),
+        C.c_void_p(st.data_ptr()), C.c_void_p(sp)))
+    out["half_step_ms"] = {"exact_20": exact_ms, "surrogate_20": sur_ms}
+    return out
 
 
-def mcmc_2d(ctx):
+def mcmc_2d(ctx, nsteps=1000):
     """Plain vs delayed acceptance on the two-field 2D fit (2048^2 and
     1024^2 grids in one launch, 14 free parameters, 128 walkers), from a
-    shared equilibrated start (runner.compare_two_fields_2d)."""
+    shared equilibrated start, with a plain-vs-plain control
+    (runner.compare_two_fields_2d, runner.summarise)."""
     from pofd_affine_b200 import runner
-    r = runner.compare_two_fields_2d(ctx, 300, 400)
-    out = _mcmc_summary("2D two-field fit: 1500x1500 pair on 2048^2 + "
-                        "800x600 pair on 1024^2 in one launch, 14 free "
-                        "parameters, 128 walkers, shared start (Powell "
-                        "maximum + 400 plain steps, untimed), then burn 150, "
-                        "300 steps; MLP 14 -> 3x384 SiLU -> 1", r["plain"],
-                        r["da"], list(range(14)))
-    out["start_loglike"] = r["start_loglike"]
+    r = runner.compare_two_fields_2d(ctx, nsteps, 400, plain_control=True)
+    out = runner.summarise(r)
+    out["workload"] = ("2D two-field fit: 1500x1500 pair on 2048^2 + 800x600 "
+                       "pair on 1024^2 in one launch, 14 free parameters, "
+                       "128 walkers, shared start (Powell maximum + 400 plain "
+                       "steps, untimed), burn %d steps (20k exact pairs), %d "
+                       "recorded steps; DA: MLP 14 -> 3x384 SiLU -> 1 trained "
+                       "on the burn-in pairs, retrained every 5k exact "
+                       "evaluations, stretch a = %g (plain a = 2)"
+                       % (-(-runner.DA_PAIRS // 128), nsteps,
+                          runner.DA_SCALE_2D))
     return out
 
 
 def _mcmc_summary(name, plain, da, free):
     from pofd_affine_b200 import runner
     shift = runner.posterior_agreement(da, plain, free)
-    keep = ("wall_s", "burn_s", "tau_max", "acor_ok", "ess", "ess_per_s",
-            "ess_per_s_after_burn", "stats", "failures")
+    keep = runner.SUMMARY_KEYS + ("stats",)
     return {"workload": name,
             "plain": {k: plain[k] for k in keep},
             "da": dict({k: da[k] for k in keep},
-                       train_s=da["train_s"], stage1_rate=da["stage1_rate"],
-                       stage2_rate=da["stage2_rate"],
-                       surrogate_rms=da.get("surrogate_rms")),
+                       **{k: da[k] for k in runner.DA_KEYS if k in da}),
             "ess_per_s_ratio": da["ess_per_s"] / plain["ess_per_s"],
             # both methods share the burn-in; after it, DA's time includes
             # its training
@@ -673,7 +710,7 @@ def main():
         if not a.no_mcmc:
             extra["mcmc"] = {"1d": mcmc_1d(ctx)}
             if a.mcmc_2d:
-                extra["mcmc"]["2d_two_fields"] = mcmc_2d(ctx)
+                extra["mcmc"]["2d_two_fields"] = mcmc_2d(ctx, a.mcmc_steps)
 
     if rank == 0:
         cpu = None

@@ -550,9 +550,13 @@ int pofd_surrogate_set_params(pofd_surrogate* s, const float* const* tensors);
  * update: grads[8] host buffers of the tensor sizes. */
 int pofd_surrogate_gradients(pofd_surrogate* s, unsigned n,
                              float* const* grads, float* loss);
-/* Input mean[16], 1/sd[16], then the target offset (max logL), scale and
- * floor: targets are max(logL - max, -floor) / scale (35 values). */
-int pofd_surrogate_scaling(pofd_surrogate* s, double* out35);
+/* The input transform and target scaling fixed at the last training:
+ * mean[16], W[16][16] (row-major; network inputs x = W (theta_free - mean),
+ * W the inverse Cholesky factor of the inputs' covariance, or diagonal 1/sd
+ * when that covariance is singular), the target offset (max logL), scale
+ * and floor (targets are max(logL - max, -floor) / scale), and 1 when W is
+ * the full whitening (276 values). */
+int pofd_surrogate_scaling(pofd_surrogate* s, double* out276);
 /* The tensor-core main loop on its own, on device pointers of the current
  * device: C[M][N] (fp32, ldc) = A[M][K] * B[N][K]^T, A and B bf16 with
  * leading dimensions multiple of 8, N in [16, 512] and K >= 16 multiples of
@@ -568,6 +572,12 @@ int pofd_bf16_gemm(int M, int N, int K, const void* A, int lda, const void* B,
  * for the surrogate above). */
 int pofd_ensemble_set_surrogate(pofd_ensemble* e, pofd_batch_loglike_fn sfn,
                                 void* sur);
+/* Stretch parameter a (> 1) of the delayed-acceptance steps; 0 (default)
+ * uses the plain steps' scalefac.  A rejected first-stage proposal costs a
+ * surrogate evaluation only, so a wider stretch than the plain optimum
+ * (a = 2) gives more effective samples per exact evaluation; the target
+ * stays exact for any a.  No counterpart in the reference. */
+int pofd_ensemble_set_da_scale(pofd_ensemble* e, double a);
 /* Every exact evaluation of the ensemble is also appended to this
  * surrogate's training pairs (NULL stops collecting). */
 int pofd_ensemble_collect_pairs(pofd_ensemble* e, pofd_surrogate* s);

@@ -36,10 +36,14 @@ def unpack(params, H):
     return W1, params[1], W2, params[3], W3, params[5], params[6], params[7][0]
 
 
-def standardise(theta, idx, mu, isd):
+def standardise(theta, idx, mu, W):
+    """Network inputs x = W (theta[idx] - mu) in float32 (the product's
+    k_pack_inputs), W the 16 x 16 input transform."""
     x = np.zeros((theta.shape[0], IN_PAD), np.float32)
+    d = np.zeros((theta.shape[0], IN_PAD), np.float32)
     for k, p in enumerate(idx):
-        x[:, k] = (theta[:, p].astype(np.float32) - np.float32(mu[k])) * np.float32(isd[k])
+        d[:, k] = theta[:, p].astype(np.float32) - np.float32(mu[k])
+    x[:, :] = d @ np.asarray(W, np.float32).T
     return x
 
 

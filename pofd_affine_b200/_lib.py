@@ -144,6 +144,7 @@ SIGNATURES = {
     "pofd_bf16_gemm": (I, [I, I, I, V, I, V, I, V, I, V]),
     "pofd_ensemble_set_surrogate": (I, [V, V, V]),
     "pofd_ensemble_collect_pairs": (I, [V, V]),
+    "pofd_ensemble_set_da_scale": (I, [V, D]),
     "pofd_ensemble_do_steps_da": (I, [V, U, I]),
     "pofd_ensemble_da_stats": (I, [V, C.POINTER(C.c_ulonglong)]),
     "pofd_likesum_create": (I, [V, PV]),

@@ -1246,6 +1246,14 @@ int pofd_ensemble_set_surrogate(pofd_ensemble* e, pofd_batch_loglike_fn sfn, voi
   });
 }
 
+int pofd_ensemble_set_da_scale(pofd_ensemble* e, double a) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->set_da_scale(a);
+    return POFD_OK;
+  });
+}
+
 int pofd_ensemble_collect_pairs(pofd_ensemble* e, pofd_surrogate* s) {
   return guard([&] {
     need(e != nullptr, "null argument");

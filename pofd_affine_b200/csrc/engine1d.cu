@@ -684,12 +684,19 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
 //
 // INC: the block first evaluates its whole tile (M1 rows of 2 CB
 // consecutive grid points) in segments of 16 points with
-// GridFill1::segment16 into a padded shared-memory tile (row stride CB + 1
-// complex values, bank-conflict free for both the segment writes and the
-// column reads), then reads its DFT inputs from there.
+// GridFill1::segment16 into a shared-memory tile, then reads its DFT
+// inputs from there.  Adjacent lanes take adjacent segments of one row, so
+// their interval-table and spline loads share cache lines.  The tile rows
+// are padded to CB + 4 complex values (consecutive rows 16 banks apart) and
+// the 8 values of segment g are rotated by g within their 8 slots, so that
+// neither the segment stores (lane = (row, segment)) nor the column reads
+// (lane = column) conflict on banks.
 template <int L1, int L2>
 __host__ __device__ constexpr int fftAR_tile() {
-  return (L1 * L2) * (256 / L2 + 1) > 256 * L1 ? (L1 * L2) * (256 / L2 + 1) : 256 * L1;
+  return (L1 * L2) * (256 / L2 + 4) > 256 * L1 ? (L1 * L2) * (256 / L2 + 4) : 256 * L1;
+}
+__device__ __forceinline__ int fftAR_slot(int b) {
+  return (b & ~7) | (((b & 7) + (b >> 3)) & 7);
 }
 
 template <int L1, int L2, bool INC>
@@ -704,7 +711,7 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
   constexpr int m = M1 * M2;
   constexpr int CB = 256 / L2;
   constexpr int NH = m / 128;
-  constexpr int CBP = CB + 1;  // padded tile row (INC)
+  constexpr int CBP = CB + 4;  // padded tile row (INC)
   extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L
   __shared__ dev::Exp2Table e2;
   __shared__ double shr[32];
@@ -733,19 +740,20 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
     // the m1 x 256 view holds grid indices 2 (a 256 + b0) .. + 2 CB - 1
     constexpr int SPR = CB / 8;  // segments per tile row
     for (int sgi = t; sgi < M1 * SPR; sgi += 256) {
-      const int a = sgi % M1, g = sgi / M1;
+      const int a = sgi / SPR, g = sgi % SPR;
       double2 o[8];
       rg.segment16(2 * (a * M2 + b0) + 16 * g, gidx, o, mn, var, iw, Rrow);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) fs[a * CBP + 8 * g + k] = o[k];
+      for (int k = 0; k < 8; ++k) fs[a * CBP + 8 * g + ((k + g) & 7)] = o[k];
     }
     __syncthreads();
   }
   {
     const int b = t % CB, n2 = t / CB;
     if (INC) {
+      const int sb = fftAR_slot(b);
 #pragma unroll
-      for (int n1 = 0; n1 < L1; ++n1) v[n1] = fs[(L2 * n1 + n2) * CBP + b];
+      for (int n1 = 0; n1 < L1; ++n1) v[n1] = fs[(L2 * n1 + n2) * CBP + sb];
       __syncthreads();  // the tile is overwritten by the exchange below
     } else {
 #pragma unroll
@@ -1492,11 +1500,11 @@ void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const in
 // the exchange area where it is larger.
 inline size_t fftAR_inc_smem(int m1) {
   const size_t l1 = m1 < 16 ? m1 : 16, l2 = m1 < 16 ? 1 : m1 / 16;
-  const size_t tile = std::max(static_cast<size_t>(m1) * (256 / l2 + 1), 256 * l1);
+  const size_t tile = std::max(static_cast<size_t>(m1) * (256 / l2 + 4), 256 * l1);
   return (tile + 2 * m1 + 128 + 256) * sizeof(double2);
 }
-// largest at m1 = 256 (tile 256 x 17)
-constexpr size_t kFftARIncSmemMax = (256 * 17 + 2 * 256 + 128 + 256) * sizeof(double2);
+// largest at m1 = 256 (tile 256 x 20)
+constexpr size_t kFftARIncSmemMax = (256 * 20 + 2 * 256 + 128 + 256) * sizeof(double2);
 
 // Fused R fill + forward pass A (inc: segment-wise running products);
 // returns the tiles per row (partial moment sums per row in rpart).

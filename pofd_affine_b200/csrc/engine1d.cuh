@@ -131,7 +131,7 @@ struct Tune1 {
   int rfill_per = 8;        // R grid points per thread of k_rfill1 (4, 8, 16)
   int rnodes_threads = 128; // threads per block of k_rnodes1 (64, 128, 256)
   int spec_blocks = 8;      // blocks per row of k_spectrum1f (2 ... 32)
-  int rfill_fused = 2;      // R grid fill inside the forward pass A (own
+  int rfill_fused = 1;      // R grid fill inside the forward pass A (own
                             // FFT): 0 no, 1 one exp2
                             // per grid point, 2 running products over
                             // segments of 16 points in one node interval

@@ -617,6 +617,16 @@ void Ensemble::set_stage1(pofd_batch_loglike_fn fn, void* sur) {
   sur_ = sur;
 }
 
+// A wider stretch than the plain steps' pays under delayed acceptance: a
+// rejected proposal then costs one surrogate evaluation instead of an exact
+// one, so larger moves with a lower pass rate give more effective samples
+// per exact evaluation.  Any a > 1 leaves the target exact (the stretch
+// move's z^(d-1) factor is in the first-stage ratio).
+void Ensemble::set_da_scale(double a) {
+  if (!(a > 1.0) && a != 0.0) throw Error(POFD_E_ARG, "stretch parameter must be > 1 (or 0)");
+  da_scale_ = a;
+}
+
 // Survivor batches are rounded up so that the likelihood sees a bounded
 // number of batch sizes (each has its own FFT plans and graphs; the plans
 // share one work area): multiples of 2 up to 32, of 4 up to 64, of 8 up to
@@ -631,7 +641,8 @@ unsigned Ensemble::bucket(unsigned n) {
 void Ensemble::da_half(int half, double zexp, double invt) {
   const unsigned nh0 = nw_ / 2, nh = half ? nw_ - nh0 : nh0;
   const unsigned g = (nh + ENT - 1) / ENT;
-  k_propose<<<g, ENT, 0, stream_>>>(half, nw_, np_, scalefac_, seed_, pstate_, plo_, phi_, theta_,
+  const double a = (da_scale_ > 1.0) ? da_scale_ : scalefac_;
+  k_propose<<<g, ENT, 0, stream_>>>(half, nw_, np_, a, seed_, pstate_, plo_, phi_, theta_,
                                     prop_, z_, ctr_, err_);
   ck(cudaGetLastError(), "k_propose");
   int rc = sfn_(sur_, nh, prop_, np_, spred_, sst_, stream_);

@@ -48,6 +48,9 @@ class Ensemble {
   void do_steps(unsigned nsteps, bool record);
   // Delayed-acceptance steps with the first-stage evaluator set below.
   void set_stage1(pofd_batch_loglike_fn fn, void* sur);
+  // stretch parameter of the delayed-acceptance steps (default: the plain
+  // steps' scalefac)
+  void set_da_scale(double a);
   void set_bonus(pofd_batch_bonus_fn fn, void* like) {
     bfn_ = fn;
     blike_ = like;
@@ -92,6 +95,7 @@ class Ensemble {
   cudaStream_t stream_;
   unsigned nw_, np_;
   double scalefac_, temp_ = 1.0;
+  double da_scale_ = 0.0;  // 0: use scalefac_
   uint64_t seed_;
   pofd_batch_loglike_fn fn_ = nullptr;
   void* like_ = nullptr;

@@ -210,20 +210,26 @@ __global__ void __launch_bounds__(NT) k_wgrad_adam(const __grid_constant__ CUten
 }
 
 // ------------------------------------------------------ elementwise kernels
-// Standardised, zero-padded bf16 inputs x [Mp][16] and x^T [16][Mp] from
-// theta rows (free parameters only); rows >= M are zero.
+// Whitened, zero-padded bf16 inputs x [Mp][16] and x^T [16][Mp] from theta
+// rows (free parameters only): x = W (theta_free - mu), W [16][16] row-major
+// (lower triangular); rows >= M are zero.
 __global__ void k_pack_inputs(int M, int Mp, const float* __restrict__ theta, int npar,
                               const int* __restrict__ idx, int nin,
-                              const float* __restrict__ mu, const float* __restrict__ isd,
+                              const float* __restrict__ mu, const float* __restrict__ wm,
                               const int* __restrict__ rows, bf16* __restrict__ x,
                               bf16* __restrict__ xt) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= Mp) return;
   const int src = (r < M) ? (rows ? rows[r] : r) : -1;
+  float d[Surrogate::kInPad];
+#pragma unroll
+  for (int j = 0; j < Surrogate::kInPad; ++j)
+    d[j] = (src >= 0 && j < nin) ? theta[static_cast<size_t>(src) * npar + idx[j]] - mu[j] : 0.0f;
+#pragma unroll
   for (int k = 0; k < Surrogate::kInPad; ++k) {
     float v = 0.0f;
-    if (src >= 0 && k < nin)
-      v = (theta[static_cast<size_t>(src) * npar + idx[k]] - mu[k]) * isd[k];
+#pragma unroll
+    for (int j = 0; j < Surrogate::kInPad; ++j) v = fmaf(wm[k * Surrogate::kInPad + j], d[j], v);
     const bf16 b = __float2bfloat16_rn(v);
     x[static_cast<size_t>(r) * Surrogate::kInPad + k] = b;
     if (xt) xt[static_cast<size_t>(k) * Mp + r] = b;
@@ -480,9 +486,10 @@ Surrogate::Surrogate(int device, cudaStream_t stream, unsigned npar, const int* 
   idx_ = dal<int>(kInPad);
   ck(cudaMemcpy(idx_, free_idx, nin * sizeof(int), cudaMemcpyHostToDevice), "upload");
   mu_ = dal<float>(kInPad);
-  isd_ = dal<float>(kInPad);
-  std::vector<float> one(kInPad, 1.0f);
-  ck(cudaMemcpy(isd_, one.data(), kInPad * sizeof(float), cudaMemcpyHostToDevice), "upload");
+  wm_ = dal<float>(kInPad * kInPad);
+  std::vector<float> eye(kInPad * kInPad, 0.0f);
+  for (int k = 0; k < kInPad; ++k) eye[k * kInPad + k] = 1.0f;
+  ck(cudaMemcpy(wm_, eye.data(), eye.size() * sizeof(float), cudaMemcpyHostToDevice), "upload");
   const size_t H = H_;
   const size_t sz[kNumTensors] = {H * kInPad, H, H * H, H, H * H, H, H, 1};
   for (int t = 0; t < kNumTensors; ++t) {
@@ -511,7 +518,7 @@ Surrogate::~Surrogate() {
     cudaFree(m_[t]);
     cudaFree(v_[t]);
   }
-  void* q[] = {idx_, mu_, isd_, w1b_, w2b_, w3b_, w2t_, w3t_, ptheta_, plogl_, counters_, err_,
+  void* q[] = {idx_, mu_, wm_, w1b_, w2b_, w3b_, w2t_, w3t_, ptheta_, plogl_, counters_, err_,
                ws_.x, ws_.xt, ws_.h[0], ws_.h[1], ws_.h[2], ws_.ht[0], ws_.ht[1], ws_.ht[2],
                ws_.z[0], ws_.z[1], ws_.z[2], ws_.dz[0], ws_.dz[1], ws_.dz[2], ws_.dzt[0],
                ws_.dzt[1], ws_.dzt[2], ws_.y, ws_.ypart, ws_.t, ws_.dy, ws_.rows, ws_.loss};
@@ -619,7 +626,7 @@ void Surrogate::forward(int M, const float* theta, int npar, const int* rows, bo
   ensure_work(Mp);
   const int H = static_cast<int>(H_);
   k_pack_inputs<<<(Mp + 127) / 128, 128, 0, st>>>(M, Mp, theta, npar, idx_, static_cast<int>(nin_),
-                                                  mu_, isd_, rows, ws_.x, train ? ws_.xt : nullptr);
+                                                  mu_, wm_, rows, ws_.x, train ? ws_.xt : nullptr);
   const bf16* Ws[3] = {w1b_, w2b_, w3b_};
   const bf16* in = ws_.x;
   int ldin = kInPad;
@@ -703,20 +710,64 @@ void Surrogate::refresh_scaling() {
     use.resize(n);
     for (unsigned i = 0; i < n; ++i) use[i] = i;
   }
+  // Whitening: mean and covariance of the inputs over those pairs, W = L^-1
+  // with L L^T the covariance (Cholesky), so that the network sees
+  // decorrelated unit-variance inputs (the knot values of a P(D) posterior
+  // are strongly correlated).  A covariance that is not positive definite
+  // falls back to the diagonal (1/sd) scaling.
   const double nu = static_cast<double>(use.size());
-  std::vector<float> mu(kInPad, 0.0f), isd(kInPad, 1.0f);
-  for (unsigned k = 0; k < nin_; ++k) {
-    double s = 0, s2 = 0;
+  const unsigned K = nin_;
+  std::vector<double> mean_in(K, 0.0), cov(K * K, 0.0);
+  for (unsigned k = 0; k < K; ++k) {
+    double s = 0;
     for (unsigned i : use) s += th[static_cast<size_t>(i) * npar_ + idx[k]];
-    const double m = s / nu;
-    for (unsigned i : use) {
-      const double d = th[static_cast<size_t>(i) * npar_ + idx[k]] - m;
-      s2 += d * d;
-    }
-    const double sd = std::sqrt(s2 / nu);
-    mu[k] = static_cast<float>(m);
-    isd[k] = static_cast<float>(sd > 0 ? 1.0 / sd : 1.0);
+    mean_in[k] = s / nu;
   }
+  for (unsigned i : use) {
+    double d[kInPad];
+    for (unsigned k = 0; k < K; ++k) d[k] = th[static_cast<size_t>(i) * npar_ + idx[k]] - mean_in[k];
+    for (unsigned a = 0; a < K; ++a)
+      for (unsigned b = 0; b <= a; ++b) cov[a * K + b] += d[a] * d[b];
+  }
+  for (unsigned a = 0; a < K; ++a)
+    for (unsigned b = 0; b <= a; ++b) cov[a * K + b] /= nu;
+  std::vector<double> L(K * K, 0.0), Winv(K * K, 0.0);
+  bool chol = true;
+  for (unsigned a = 0; a < K && chol; ++a) {
+    for (unsigned b = 0; b <= a; ++b) {
+      double v = cov[a * K + b];
+      for (unsigned c = 0; c < b; ++c) v -= L[a * K + c] * L[b * K + c];
+      if (a == b) {
+        if (!(v > 1e-12 * std::fabs(cov[a * K + a])) || !(v > 0)) {
+          chol = false;
+          break;
+        }
+        L[a * K + a] = std::sqrt(v);
+      } else {
+        L[a * K + b] = v / L[b * K + b];
+      }
+    }
+  }
+  if (chol) {
+    // inverse of the lower-triangular factor, column by column
+    for (unsigned c = 0; c < K; ++c)
+      for (unsigned a = c; a < K; ++a) {
+        double v = (a == c) ? 1.0 : 0.0;
+        for (unsigned b = c; b < a; ++b) v -= L[a * K + b] * Winv[b * K + c];
+        Winv[a * K + c] = v / L[a * K + a];
+      }
+  } else {
+    for (unsigned k = 0; k < K; ++k) {
+      const double sd = std::sqrt(std::max(cov[k * K + k], 0.0));
+      Winv[k * K + k] = sd > 0 ? 1.0 / sd : 1.0;
+    }
+  }
+  std::vector<float> mu(kInPad, 0.0f), wm(kInPad * kInPad, 0.0f);
+  for (unsigned a = 0; a < K; ++a) {
+    mu[a] = static_cast<float>(mean_in[a]);
+    for (unsigned b = 0; b < K; ++b) wm[a * kInPad + b] = static_cast<float>(Winv[a * K + b]);
+  }
+  whitened_ = chol;
   // target: logL - max, floored at -clip so that far-off burn-in points do
   // not set the scale; the floor grows with the number of inputs (a
   // chi-square of nin degrees of freedom sits near -nin/2)
@@ -735,7 +786,7 @@ void Surrogate::refresh_scaling() {
   clip_ = clip;
   ys_ = (sd > 0) ? sd : 1.0;
   ck(cudaMemcpy(mu_, mu.data(), kInPad * sizeof(float), cudaMemcpyHostToDevice), "upload");
-  ck(cudaMemcpy(isd_, isd.data(), kInPad * sizeof(float), cudaMemcpyHostToDevice), "upload");
+  ck(cudaMemcpy(wm_, wm.data(), wm.size() * sizeof(float), cudaMemcpyHostToDevice), "upload");
   scaled_ = true;
 }
 
@@ -839,16 +890,16 @@ void Surrogate::check_err() {
 }
 
 void Surrogate::scaling(double* out) const {
-  std::vector<float> mu(kInPad), isd(kInPad);
+  std::vector<float> mu(kInPad), wm(kInPad * kInPad);
   ck(cudaMemcpy(mu.data(), mu_, kInPad * sizeof(float), cudaMemcpyDeviceToHost), "D2H");
-  ck(cudaMemcpy(isd.data(), isd_, kInPad * sizeof(float), cudaMemcpyDeviceToHost), "D2H");
-  for (int k = 0; k < kInPad; ++k) {
-    out[k] = mu[k];
-    out[kInPad + k] = isd[k];
-  }
-  out[2 * kInPad] = ymax_;
-  out[2 * kInPad + 1] = ys_;
-  out[2 * kInPad + 2] = clip_;
+  ck(cudaMemcpy(wm.data(), wm_, wm.size() * sizeof(float), cudaMemcpyDeviceToHost), "D2H");
+  for (int k = 0; k < kInPad; ++k) out[k] = mu[k];
+  for (int k = 0; k < kInPad * kInPad; ++k) out[kInPad + k] = wm[k];
+  const int o = kInPad + kInPad * kInPad;
+  out[o] = ymax_;
+  out[o + 1] = ys_;
+  out[o + 2] = clip_;
+  out[o + 3] = whitened_ ? 1.0 : 0.0;
 }
 
 // The tensor-core main loop on its own: C = A B^T (fp32).

@@ -38,7 +38,8 @@ class Surrogate {
   void get_params_host(std::vector<std::vector<float>>& host) const;
   void set_params_host(const std::vector<std::vector<float>>& host);
   size_t tensor_size(int t) const { return size_[t]; }
-  void scaling(double* out) const;  // mu[16], 1/sd[16], ymax, ys, clip
+  // mu[16], W[16][16], ymax, ys, clip, whitened (276 values)
+  void scaling(double* out) const;
   void refresh_scaling();
   unsigned hidden() const { return H_; }
   unsigned nin() const { return nin_; }
@@ -62,7 +63,8 @@ class Surrogate {
   double ymax_ = 0.0, ys_ = 1.0, clip_ = 1e300;
   int* idx_ = nullptr;
   float* mu_ = nullptr;
-  float* isd_ = nullptr;
+  float* wm_ = nullptr;    // input whitening W [16][16]
+  bool whitened_ = false;
   float* p_[kNumTensors] = {};
   float* m_[kNumTensors] = {};
   float* v_[kNumTensors] = {};

@@ -258,6 +258,11 @@ class affineEnsemble:
         check(lib().pofd_ensemble_set_surrogate(self.h, fn, sur.h))
         self.sur = sur
 
+    def setDAScale(self, a):
+        """Stretch parameter of the delayed-acceptance steps (0: the plain
+        steps' scalefac)."""
+        check(lib().pofd_ensemble_set_da_scale(self.h, float(a)))
+
     def collectPairs(self, sur):
         """Append every exact evaluation to sur's training pairs (None
         stops)."""

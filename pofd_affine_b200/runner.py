@@ -1,7 +1,8 @@
 """Fixed-burn MCMC runs of the plain and the delayed-acceptance stretch move
 (the single-process counterpart of pofd_affine_mcmc's fixed-burn mode,
 pofdMCMC / affineEnsemble::doBurnIn with a fixed burn, then doSteps), with
-effective samples per second measured by acor.
+effective samples per second from the integrated autocorrelation time
+(Sokal's automatic window; the reference's acor reported beside it).
 
   * run_plain(E, nburn, nsteps)
   * run_da(E, S, nburn, nsteps, ...)   burn-in pairs train the surrogate,
@@ -14,14 +15,32 @@ import numpy as np
 
 
 def _summary(E, wall, nsteps):
+    """Effective samples of the recorded chain: the integrated
+    autocorrelation time with Sokal's automatic window (mcmc.integrated_time)
+    sets ESS = nwalkers nsteps / max tau; the reference's acor (fixed 10-lag
+    window, which saturates on long correlation times) is reported beside
+    it."""
+    from .mcmc import integrated_time
     ch, cl = E.getChain()
     tau, ok = E.getAcor()
     finite = np.isfinite(tau)
     tmax = float(np.max(tau[finite])) if np.any(finite) else float("nan")
-    ess = E.nwalkers * nsteps / tmax if np.isfinite(tmax) else float("nan")
-    return {"wall_s": wall, "tau": [float(t) for t in tau], "tau_max": tmax,
+    ti, win, conv = integrated_time(ch)
+    for p in range(E.nparams):
+        if E.state[p] & 3:  # fixed or ignored
+            ti[p] = np.nan
+            conv[p] = True
+    fi = np.isfinite(ti)
+    timax = float(np.max(ti[fi])) if np.any(fi) else float("nan")
+    ess = E.nwalkers * nsteps / timax if np.isfinite(timax) else float("nan")
+    ess_acor = E.nwalkers * nsteps / tmax if np.isfinite(tmax) else float("nan")
+    return {"wall_s": wall, "tau_acor": [float(t) for t in tau],
+            "tau_acor_max": tmax, "acor_ok": bool(ok),
+            "tau": [float(t) for t in ti], "tau_max": timax,
+            "tau_converged": bool(np.all(conv)),
+            "steps_per_tau": nsteps / timax if np.isfinite(timax) else float("nan"),
             "failures": E.getFailures(),
-            "acor_ok": bool(ok), "ess": ess, "ess_per_s": ess / wall,
+            "ess": ess, "ess_per_s": ess / wall, "ess_acor": ess_acor,
             "chain": ch, "logl": cl}
 
 
@@ -44,27 +63,34 @@ def run_plain(E, nburn, nsteps):
 
 
 def run_da(E, S, nburn, nsteps, train_iters=2000, batch=512, lr=1e-3,
-           refresh=5000, refresh_iters=300, chunk=25, holdout=None):
+           refresh=5000, refresh_iters=400, chunk=25, holdout=None,
+           da_scale=0.0):
     """Burn-in with exact evaluations collected as training pairs, train,
-    then delayed-acceptance steps in chunks, retraining after every
-    `refresh` new exact evaluations.  The timed region includes the
-    training.  holdout (theta, logl) gives the surrogate RMS error.  The
-    likelihood's plans and graphs for every survivor batch size are made
-    before the timed region (prepareDA), as the plain run's are by its
-    first step."""
+    then delayed-acceptance steps in chunks, retraining on all pairs held
+    after every `refresh` new exact evaluations.  The timed region includes
+    the training.  da_scale: stretch parameter of the delayed-acceptance
+    steps (0: the plain one).  The surrogate RMS error is reported on
+    holdout (theta, logl) pairs when given, and on the exact pairs the run
+    evaluated after its last training (never trained on).  The likelihood's
+    plans and graphs for every survivor batch size are made before the timed
+    region (prepareDA), as the plain run's are by its first step."""
     E.prepareDA()
+    E.setDAScale(da_scale)
     t0 = time.perf_counter()
     E.collectPairs(S)
     E.doSteps(0, nburn)
     E.sync()
     t1 = time.perf_counter()
     t_burn = t1 - t0
+    npairs_burn = S.nPairs()
     S.train(train_iters, batch, lr)
     t_train = time.perf_counter() - t1
+    trained_on = npairs_burn
     E.setSurrogate(S)
     base = E.daStats()
     last = base["exact_evals"]
     done = 0
+    nrefresh = 0
     while done < nsteps:
         k = min(chunk, nsteps - done)
         E.doStepsDA(k)
@@ -72,9 +98,11 @@ def run_da(E, S, nburn, nsteps, train_iters=2000, batch=512, lr=1e-3,
         st = E.daStats()
         if st["exact_evals"] - last >= refresh and done < nsteps:
             t1 = time.perf_counter()
+            trained_on = S.nPairs()
             S.train(refresh_iters, batch, lr)
             t_train += time.perf_counter() - t1
             last = st["exact_evals"]
+            nrefresh += 1
     wall = time.perf_counter() - t0
     E.collectPairs(None)
     st = E.daStats()
@@ -82,6 +110,9 @@ def run_da(E, S, nburn, nsteps, train_iters=2000, batch=512, lr=1e-3,
     out["stats"] = {k: st[k] - base[k] for k in st}
     out["train_s"] = t_train
     out["burn_s"] = t_burn
+    out["training_pairs_burn"] = npairs_burn
+    out["refreshes"] = nrefresh
+    out["da_scale"] = da_scale
     # after the common burn-in; the training stays in
     out["ess_per_s_after_burn"] = out["ess"] / (wall - t_burn)
     s = out["stats"]
@@ -89,6 +120,12 @@ def run_da(E, S, nburn, nsteps, train_iters=2000, batch=512, lr=1e-3,
     out["stage2_rate"] = s["accepted"] / max(s["stage1_passes"], 1)
     if holdout is not None:
         out["surrogate_rms"] = S.rms(*holdout)
+    th, ll = S.getPairs()
+    if th.shape[0] - trained_on >= 100:
+        th, ll = th[trained_on:], ll[trained_on:]
+        ok = np.isfinite(ll)
+        out["surrogate_rms_untrained_pairs"] = S.rms(th[ok], ll[ok])
+        out["untrained_pairs"] = int(ok.sum())
     return out
 
 
@@ -127,17 +164,26 @@ def find_start(loglike, x0, rounds=4, maxfev=2000, bounds=None):
 
 def posterior_agreement(a, b, free):
     """(max over free parameters of |mean_a - mean_b| / sd_b, the same in
-    units of the standard error of the difference sqrt(var_a / ESS_a +
-    var_b / ESS_b))."""
+    units of the standard error of the difference sqrt(var_a / ESS_a,p +
+    var_b / ESS_b,p), ESS_p = nwalkers nsteps / tau_p with each parameter's
+    own integrated autocorrelation time)."""
     ca = a["chain"].reshape(-1, a["chain"].shape[-1])[:, free].astype(np.float64)
     cb = b["chain"].reshape(-1, b["chain"].shape[-1])[:, free].astype(np.float64)
     d = np.abs(ca.mean(0) - cb.mean(0))
-    se = np.sqrt(ca.var(0) / a["ess"] + cb.var(0) / b["ess"])
+    ta = np.asarray(a["tau"], np.float64)[free]
+    tb = np.asarray(b["tau"], np.float64)[free]
+    ea, eb = ca.shape[0] / ta, cb.shape[0] / tb
+    se = np.sqrt(ca.var(0) / ea + cb.var(0) / eb)
     return float(np.max(d / cb.std(0))), float(np.max(d / se))
 
 
-def compare_two_fields_2d(ctx, nsteps, npre, nburn=150, plain_control=False,
-                          train_iters=1000):
+DA_PAIRS = 20000       # exact burn-in pairs the surrogate first trains on
+DA_REFRESH = 5000      # retrain after this many new exact evaluations
+DA_SCALE_2D = 5.0      # stretch parameter of the delayed-acceptance steps
+
+
+def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
+                          train_iters=2000, da_scale=DA_SCALE_2D):
     """Plain vs delayed acceptance on the two-field 2D fit (a 1500x1500 pair
     on a 2048^2 grid and an 800x600 pair on a 1024^2 grid in one summed
     likelihood, 14 free parameters, 128 walkers).
@@ -145,13 +191,19 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=150, plain_control=False,
     Both methods start from the same walkers, made untimed: a bounded Powell
     maximum of the likelihood (the synthetic maps' generating parameters lie
     several hundred log-likelihood units below it), a 1e-3 ball around it
-    and npre plain steps.  Each run then burns nburn steps and records
-    nsteps.  With plain_control a second plain run (another seed) gives the
-    plain-vs-plain agreement the DA-vs-plain agreement is compared with."""
+    and npre plain steps.  Each run then burns nburn steps (default: enough
+    for 20k exact pairs, on which the surrogate first trains) and records
+    nsteps; the surrogate is retrained every 5k new exact evaluations, and
+    the delayed-acceptance steps use the stretch parameter da_scale (the
+    plain steps the reference's 2).  With plain_control a second plain run
+    (another seed) gives the plain-vs-plain agreement the DA-vs-plain
+    agreement is compared with."""
     from . import synth
     from .mcmc import affineEnsemble, likeSum
     from .surrogate import Surrogate
     a, b = synth.config_2d_two_fields()
+    if nburn is None:
+        nburn = -(-DA_PAIRS // 128)
     La, Lb = synth.build_like2(a, ctx), synth.build_like2(b, ctx)
     S2 = likeSum(ctx, [La, Lb])
     npar = a["theta0"].size
@@ -192,7 +244,7 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=150, plain_control=False,
     hold = (ch[pick], plain["logl"].reshape(-1)[pick])
     S = Surrogate(ctx, npar, list(range(nfree)), hidden=384, seed=9)
     da = run_da(ens(32, start), S, nburn, nsteps, train_iters=train_iters,
-                holdout=hold)
+                refresh=DA_REFRESH, holdout=hold, da_scale=da_scale)
     free = list(range(nfree))
     out = {"plain": plain, "da": da, "start_loglike": lopt,
            "agreement": posterior_agreement(da, plain, free)}
@@ -200,6 +252,37 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=150, plain_control=False,
         plain2 = run_plain(ens(41, start), nburn, nsteps)
         out["plain_control"] = plain2
         out["agreement_plain_control"] = posterior_agreement(plain2, plain, free)
+    return out
+
+
+SUMMARY_KEYS = ("wall_s", "burn_s", "tau_max", "tau_acor_max", "tau_converged",
+                "steps_per_tau", "ess", "ess_per_s", "ess_per_s_after_burn",
+                "failures")
+DA_KEYS = ("train_s", "training_pairs_burn", "refreshes", "da_scale",
+           "surrogate_rms", "surrogate_rms_untrained_pairs", "untrained_pairs",
+           "stage1_rate", "stage2_rate", "stats")
+
+
+def summarise(r):
+    """The comparison of compare_two_fields_2d as plain numbers: both runs'
+    wall times, autocorrelation times and effective samples per second, the
+    ratios over the whole run and after the common burn-in, and the
+    posterior-mean agreements (in sigma and in standard errors) of DA vs
+    plain and, when run, of plain vs plain."""
+    def pick(run, keys):
+        return {k: run[k] for k in keys if k in run}
+    out = {"plain": pick(r["plain"], SUMMARY_KEYS + ("stats",)),
+           "da": pick(r["da"], SUMMARY_KEYS + DA_KEYS),
+           "ess_per_s_ratio": r["da"]["ess_per_s"] / r["plain"]["ess_per_s"],
+           "ess_per_s_ratio_after_burn": (r["da"]["ess_per_s_after_burn"] /
+                                          r["plain"]["ess_per_s_after_burn"]),
+           "posterior_mean_shift_sigma": r["agreement"][0],
+           "posterior_mean_shift_se": r["agreement"][1],
+           "start_loglike": r["start_loglike"]}
+    if "plain_control" in r:
+        out["plain_control"] = pick(r["plain_control"], SUMMARY_KEYS)
+        out["plain_vs_plain_shift_sigma"] = r["agreement_plain_control"][0]
+        out["plain_vs_plain_shift_se"] = r["agreement_plain_control"][1]
     return out
 
 
@@ -212,21 +295,13 @@ def _main(argv=None):
     p.add_argument("case", choices=["two-fields-2d"])
     p.add_argument("--steps", type=int, default=1500)
     p.add_argument("--pre", type=int, default=1000)
-    p.add_argument("--burn", type=int, default=150)
+    p.add_argument("--burn", type=int, default=None)
+    p.add_argument("--da-scale", type=float, default=DA_SCALE_2D)
     a = p.parse_args(argv)
-    r = compare_two_fields_2d(Context(0), a.steps, a.pre, a.burn, plain_control=True)
-    keep = ("wall_s", "burn_s", "tau_max", "ess", "ess_per_s", "ess_per_s_after_burn")
-    summ = {"steps": a.steps, "pre": a.pre, "burn": a.burn,
-            "start_loglike": r["start_loglike"],
-            "plain": {k: r["plain"][k] for k in keep},
-            "plain_control": {k: r["plain_control"][k] for k in keep},
-            "da": {k: r["da"][k] for k in keep + ("train_s", "surrogate_rms",
-                                                  "stage1_rate", "stage2_rate")},
-            "da_vs_plain_shift_sigma_se": r["agreement"],
-            "plain_vs_plain_shift_sigma_se": r["agreement_plain_control"],
-            "ess_per_s_ratio": r["da"]["ess_per_s"] / r["plain"]["ess_per_s"],
-            "ess_per_s_ratio_after_burn": (r["da"]["ess_per_s_after_burn"] /
-                                           r["plain"]["ess_per_s_after_burn"])}
+    r = compare_two_fields_2d(Context(0), a.steps, a.pre, a.burn, plain_control=True,
+                              da_scale=a.da_scale)
+    summ = summarise(r)
+    summ.update(steps=a.steps, pre=a.pre, burn=a.burn)
     print(json.dumps(summ))
 
 

@@ -141,7 +141,9 @@ class Surrogate:
         return grads, loss.value
 
     def scaling(self):
-        o = np.empty(35)
+        """Input transform x = W (theta_free - mu) and target scaling of the
+        last training."""
+        o = np.empty(276)
         check(lib().pofd_surrogate_scaling(self.h, o))
-        return {"mu": o[:16], "isd": o[16:32], "ymax": o[32], "ys": o[33],
-                "clip": o[34]}
+        return {"mu": o[:16], "W": o[16:272].reshape(16, 16), "ymax": o[272],
+                "ys": o[273], "clip": o[274], "whitened": bool(o[275])}
