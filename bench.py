@@ -408,6 +408,48 @@ def cpu_baseline_2d(cfg, seconds, nthreads=None):
                       "%s)" % (done, el, nthreads, CPU_FFT)}
 
 
+def roofline_2d(L, cfg, thetas, stages, P):
+    """Rooflines of the two dominant 2D kernels from the stage times.
+    k_rgrid2 (FP64): every active colour term of every main-grid row is
+    evaluated once per column, 25 flops each (the table exp2 21, the
+    squared offset 3, the weighted add 1); the active terms per proposal
+    are counted by the library for the first proposal and taken for all.
+    k_colspec2 (HBM): per proposal it reads the row-transformed R spectrum
+    and writes one column-transformed spectrum per dataset, 16 n (n/2+1)
+    bytes each."""
+    import ctypes as C
+    from pofd_affine_b200._lib import support_lib
+    n = cfg["fftsize"]
+    nc = n // 2 + 1
+    main, edge = L.activeTerms(thetas[0])
+    pk = C.c_double()
+    support_lib().pofd_fp64_peak(0, C.byref(pk))
+    hb = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = hb.get("hbm_gbs", 6650.0)
+    out = {"active_terms_per_proposal": {"main_rows": main, "edge_rows": edge}}
+    ms = stages.get("k_rgrid2")
+    if ms:
+        flops = 25.0 * main * (n - 1) * P
+        ach = flops / (ms * 1e-3) / 1e12
+        out["roofline_rgrid2"] = {
+            "bound": "fp64", "kernel": "k_rgrid2", "ms_per_launch": ms,
+            "algorithmic_flops": flops, "achieved": ach, "peak": pk.value,
+            "unit": "TFLOP/s", "frac": ach / pk.value,
+            "peak_source": "measured (pofd_fp64_peak DFMA loop)"}
+    ms = stages.get("k_r0sum2+k_colspec2")
+    if ms:
+        nds = len(cfg["maps"])
+        nbytes = 16.0 * n * nc * (1 + nds) * P
+        ach = nbytes / (ms * 1e-3) / 1e9
+        out["roofline_colspec2"] = {
+            "bound": "hbm", "kernel": "k_r0sum2+k_colspec2", "ms_per_launch": ms,
+            "algorithmic_bytes": nbytes, "achieved": ach, "peak": hbm_peak,
+            "unit": "GB/s", "frac": ach / hbm_peak,
+            "peak_source": "measured" if "hbm_gbs" in hb else "fallback"}
+    return out
+
+
 def measure_2d(a, ctx, stream):
     import torch
     from pofd_affine_b200 import synth
@@ -446,6 +488,7 @@ def measure_2d(a, ctx, stream):
         L.getLogLikeBatch(host[k % 2])
     e2e_s = time.perf_counter() - t0
     stages = L.profileStages(host[0], reps=3)
+    roof = roofline_2d(L, cfg, host[0], stages, BATCH_2D)
     out = {"workload": "2D plain method: 8-knot counts 2-500 mJy, log-normal "
                        "colour (3 sigma + 3 offset knots), FWHM 3.0/4.2 px "
                        "beams in 100-bin 2D histograms, 1500x1500 map pair, "
@@ -457,6 +500,7 @@ def measure_2d(a, ctx, stream):
                    "h2d_bytes_per_step": BATCH_2D * npar * 4,
                    "d2h_bytes_per_step": BATCH_2D * 12},
            "stage_ms": stages, "gpu_launches": L.kernelsPerEval() * steps}
+    out.update(roof)
     if not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_2d(cfg, a.cpu_seconds)
     return out

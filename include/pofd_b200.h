@@ -343,6 +343,13 @@ int pofd_like2_fft_info(const pofd_like2* L, int* fused);
  * n = 2048, ~1e-5 in a log-likelihood over 2.25 M pixels).  Mode 1 is slow
  * (a 2 n^2-long dependent chain per dataset) and meant for parity checks. */
 int pofd_like2_set_reference_sums(pofd_like2* L, int on);
+/* Work count of the 2D R builders for one proposal theta: out2[0] = the
+ * active colour terms (numberCountsDoubleLogNormal.cc:1883-1963, c0 != 0)
+ * summed over the main grid rows 1 .. n-1, out2[1] over the edge rows, all
+ * beam sets; each term is evaluated once per column.  For roofline
+ * accounting; no counterpart in the reference. */
+int pofd_like2_active_terms(pofd_like2* L, const float* theta, unsigned npar,
+                            long long* out2);
 
 /* Priors per band (band 0 or 1), added once to the summed log-likelihood in
  * the reference's order (calcLikeDouble.cc:1236-1276): Gaussians on the

@@ -313,6 +313,15 @@ class calcLikeDouble:
         default tree sums; slow, for parity checks."""
         check(lib().pofd_like2_set_reference_sums(self.h, 1 if on else 0))
 
+    def activeTerms(self, p):
+        """(main-row, edge-row) active colour terms of one proposal's R
+        grid, summed over rows and beam sets (the R builders' work per
+        column)."""
+        th = _f32(p)
+        out = (C.c_longlong * 2)()
+        check(lib().pofd_like2_active_terms(self.h, th, th.size, out))
+        return int(out[0]), int(out[1])
+
     def fusedColumns(self):
         """True when the fused column path is the one in use."""
         k = C.c_int()

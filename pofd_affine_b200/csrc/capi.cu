@@ -771,6 +771,17 @@ int pofd_like2_get_r(pofd_like2* L, int beamset, const float* theta,
   });
 }
 
+int pofd_like2_active_terms(pofd_like2* L, const float* theta, unsigned npar,
+                            long long* out2) {
+  return guard([&] {
+    need(L && theta && out2, "null argument");
+    need(L->ctx->device >= 0, "host-only context has no GPU");
+    cudaSetDevice(L->ctx->device);
+    L->eng->active_terms(theta, npar, out2);
+    return POFD_OK;
+  });
+}
+
 int pofd_like2_kernels_per_eval(const pofd_like2* L, int* nk) {
   return guard([&] {
     need(L && nk, "null argument");

@@ -27,35 +27,34 @@ constexpr double kSmallLogVal = -30.0;
 // ------------------------------------------------------------------ exp2
 // Table-driven 2^x after Tang ("Table-driven implementation of the
 // exponential function in IEEE floating-point arithmetic", ACM TOMS 15,
-// 1989): x = k + j/64 + r with j in [0, 64), |r| <= 1/128;
-// 2^x = 2^k * T[j] * 2^r, T[j] = 2^(j/64) from a 64-entry table built at
-// block start, 2^r from its Taylor series sum_{m<=6} (r ln 2)^m / m!
-// (truncation < 3e-20 relative), 2^k by adding k to the exponent field.
-// Arguments below -1022 give exactly 0 (results under 2^-1022 never change
-// the sums they enter); arguments must be below 1023.
+// 1989): x = k + j/256 + r with j in [0, 256), |r| <= 1/512;
+// 2^x = 2^k * T[j] * 2^r, T[j] = 2^(j/256) from a 256-entry table built at
+// block start, 2^r from its Taylor series sum_{m<=4} (r ln 2)^m / m!
+// (truncation < 4e-17 relative: (ln 2 / 512)^5 / 5!), 2^k by adding k to
+// the exponent field.  Arguments below -1022 give exactly 0 (results under
+// 2^-1022 never change the sums they enter); arguments must be below 1023.
 struct Exp2Table {
-  double t[64];
+  double t[256];
   __device__ __forceinline__ void load() {
-    for (int j = threadIdx.x; j < 64; j += blockDim.x) t[j] = exp2(static_cast<double>(j) / 64.0);
+    for (int j = threadIdx.x; j < 256; j += blockDim.x) t[j] = exp2(static_cast<double>(j) / 256.0);
   }
 };
 
 __device__ __forceinline__ double exp2_tab(double x, const double* __restrict__ tab) {
-  // n = round(64 x) via the 1.5 * 2^52 shifter; its low word holds n
+  // n = round(256 x) via the 1.5 * 2^52 shifter; its low word holds n
   const double sh = 6755399441055744.0;
-  const double t = fma(x, 64.0, sh);
+  const double t = fma(x, 256.0, sh);
   const double nd = t - sh;
   const int n = __double2loint(t);
-  const double r = fma(nd, -0.015625, x);
-  double p = 1.5403530393381609e-04;
-  p = fma(p, r, 1.3333558146428443e-03);
-  p = fma(p, r, 9.6181291076284772e-03);
+  const double r = fma(nd, -0.00390625, x);
+  // (ln 2)^m / m!, m = 4 .. 1
+  double p = 9.6181291076284772e-03;
   p = fma(p, r, 5.5504108664821580e-02);
   p = fma(p, r, 2.4022650695910071e-01);
   p = fma(p, r, 6.9314718055994531e-01);
   p = fma(p, r, 1.0);
-  const double v = p * tab[n & 63];
-  const int k = n >> 6;
+  const double v = p * tab[n & 255];
+  const int k = n >> 8;
   const double s = __hiloint2double(__double2hiint(v) + (k << 20), __double2loint(v));
   return (x < -1022.0) ? 0.0 : s;
 }

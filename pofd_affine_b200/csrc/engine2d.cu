@@ -38,7 +38,7 @@ constexpr int RB = 4;        // R-grid rows per block
 constexpr int RTILE = 32;    // P(D) rows per scan block
 constexpr int GCH = 1024;    // data bins per gather block
 constexpr int KMAX = Engine2::KMAX;
-constexpr int MAXT = 2048;   // colour terms per row slot held in shared memory
+constexpr int MAXT = 2048;   // colour terms per row slot (a sanity limit on raw beams)
 constexpr int SNT = 1024;    // threads of the split kernel
 
 void ck(cudaError_t e, const char* what) {
@@ -188,14 +188,46 @@ __device__ __forceinline__ double curve_at(const double* x, const double* s,
   return val;
 }
 
-// Per-row colour terms (numberCountsDoubleLogNormal.cc:1883-1963), one thread
-// per (row, term slot): c0 = weight * counts / sigma * prefac (0 marks a
-// term to skip), c1 = log f1 + offset - log(beam1/beam2), c2 = -1/(2 ln2
-// sigma^2).
+// One colour term of a row (numberCountsDoubleLogNormal.cc:1883-1963):
+// c0 = weight * counts / sigma * prefac (0: the term is skipped), c1 =
+// log f1 + offset - log(beam1/beam2), c2 = -1/(2 ln2 sigma^2).
+__device__ __forceinline__ double3 row_term(const BSet2Dev& bs, const Model2Dev& m,
+                                            const double* __restrict__ cs, int r, int sgn,
+                                            int j, double ilog2toe, const double* tab) {
+  double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+  const Sign2Dev& sg = bs.sg[sgn];
+  const double f1val = fabs(bs.rowflux[r]);
+  if (f1val < sg.maxf1) {
+    const double ieta1 = sg.ieta1[j];
+    const double f1prod = f1val * ieta1;
+    if (f1prod >= m.minknot && f1prod < m.maxknot) {
+      const double cts = dev::exp2_tab(spline_at(m.logknots, cs, m.K, log2(f1prod)), tab);
+      if (cts > 0) {
+        const double isigma =
+            1.0 / curve_at(m.sk, cs + 4 * KMAX, m.ns, f1prod, true, m.min_sigma);
+        if (sg.ishist) c0 = sg.w[j] * ieta1 * isigma * cts * bs.prefac;
+        else c0 = cts * ieta1 * isigma * bs.prefac;
+        c1 = bs.rowlog[r] + curve_at(m.ok, cs + 8 * KMAX, m.no, f1prod, false, 0.0) -
+             sg.logratio[j];
+        c2 = -0.5 * isigma * isigma * ilog2toe;
+      }
+    }
+  }
+  return make_double3(c0, c1, c2);
+}
+
+// Per-row colour terms, one warp per row: the row's terms of the positive
+// band-2 sign component, then those of the negative one, each list with
+// its zero terms dropped and its order kept, written as (c0, c1, c2)
+// triples at rw[row][0 .. npos + nneg); rcnt[row] = (npos, nneg).  The R
+// grid kernels read these lists directly (the same values for every lane
+// of a warp), with no per-block staging.
+constexpr int ROWS_PER_BLOCK = NT / 32;
 __global__ void __launch_bounds__(NT)
 k_rows2(const BSet2Dev* __restrict__ bsets, Model2Dev m, int B,
         double ilog2toe, const int* __restrict__ mstatus,
-        const double* __restrict__ cnt, double* __restrict__ rw) {
+        const double* __restrict__ cnt, double* __restrict__ rw,
+        int2* __restrict__ rcnt) {
   __shared__ dev::Exp2Table e2;
   const int wb = blockIdx.y;
   const int w = wb / B, b = wb - w * B;
@@ -203,141 +235,69 @@ k_rows2(const BSet2Dev* __restrict__ bsets, Model2Dev m, int B,
   e2.load();
   __syncthreads();
   const BSet2Dev& bs = bsets[b];
-  const int T = bs.T;
-  const long long t = static_cast<long long>(blockIdx.x) * NT + threadIdx.x;
-  if (t >= static_cast<long long>(bs.nrows) * T) return;
-  const int r = static_cast<int>(t / T), k = static_cast<int>(t - static_cast<long long>(r) * T);
-  double* out = rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3 + 3 * k;
+  const int r = blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= bs.nrows) return;
+  double* out = rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3;
   const int sgn1 = bs.rowsgn[r];
-  double c0 = 0.0, c1 = 0.0, c2 = 0.0;
-  if (sgn1 >= 0) {
-    const int np = bs.hassign[sgn1] ? bs.sg[sgn1].nt : 0;
-    const int nn = bs.hassign[sgn1 + 1] ? bs.sg[sgn1 + 1].nt : 0;
-    int sgn = -1, j = 0;
-    if (k < np) { sgn = sgn1; j = k; }
-    else if (k < np + nn) { sgn = sgn1 + 1; j = k - np; }
-    if (sgn >= 0) {
-      const Sign2Dev& sg = bs.sg[sgn];
-      const double f1val = fabs(bs.rowflux[r]);
-      if (f1val < sg.maxf1) {
-        const double ieta1 = sg.ieta1[j];
-        const double f1prod = f1val * ieta1;
-        if (f1prod >= m.minknot && f1prod < m.maxknot) {
-          const double* cs = cnt + static_cast<size_t>(w) * 12 * KMAX;
-          const double cts = dev::exp2_tab(spline_at(m.logknots, cs, m.K, log2(f1prod)), e2.t);
-          if (cts > 0) {
-            const double isigma =
-                1.0 / curve_at(m.sk, cs + 4 * KMAX, m.ns, f1prod, true, m.min_sigma);
-            if (sg.ishist) c0 = sg.w[j] * ieta1 * isigma * cts * bs.prefac;
-            else c0 = cts * ieta1 * isigma * bs.prefac;
-            c1 = bs.rowlog[r] + curve_at(m.ok, cs + 8 * KMAX, m.no, f1prod, false, 0.0) -
-                 sg.logratio[j];
-            c2 = -0.5 * isigma * isigma * ilog2toe;
-          }
-        }
-      }
-    }
-  }
-  out[0] = c0;
-  out[1] = c1;
-  out[2] = c2;
-}
-
-// Stable block-wide compaction count: exclusive position of this thread's
-// set flag among the block's set flags, and the total.
-__device__ __forceinline__ int block_excl_count(bool flag, int& total, int* sh) {
-  const unsigned ballot = __ballot_sync(0xffffffffu, flag);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  const int within = __popc(ballot & ((1u << lane) - 1u));
-  if (lane == 0) sh[warp] = __popc(ballot);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int i = 0; i < nw; ++i) {
-      const int c = sh[i];
-      sh[i] = acc;
-      acc += c;
-    }
-    sh[nw] = acc;
-  }
-  __syncthreads();
-  const int pos = sh[warp] + within;
-  total = sh[nw];
-  __syncthreads();
-  return pos;
-}
-
-// Stage one row's non-zero terms in shared memory, positive-f2 and
-// negative-f2 lists separately, in the reference's order.
-__device__ void stage_row(const BSet2Dev& bs, const double* __restrict__ rwrow,
-                          int sgn1, double* s_pos, double* s_neg, int* s_cnt,
-                          int* sh) {
   int np = 0, nn = 0;
   if (sgn1 >= 0) {
     np = bs.hassign[sgn1] ? bs.sg[sgn1].nt : 0;
     nn = bs.hassign[sgn1 + 1] ? bs.sg[sgn1 + 1].nt : 0;
   }
-  int bp = 0, bn = 0;
-  for (int k0 = 0; k0 < np + nn; k0 += blockDim.x) {
-    const int k = k0 + threadIdx.x;
-    const bool valid = k < np + nn;
-    double c0 = 0.0, c1 = 0.0, c2 = 0.0;
-    if (valid) {
-      c0 = rwrow[3 * k];
-      c1 = rwrow[3 * k + 1];
-      c2 = rwrow[3 * k + 2];
+  const double* cs = cnt + static_cast<size_t>(w) * 12 * KMAX;
+  int npos = 0, nneg = 0;
+  for (int half = 0; half < 2; ++half) {
+    const int k0 = half ? np : 0, k1 = half ? np + nn : np;
+    const int sgn = sgn1 + half;
+    int put = half ? npos : 0;
+    for (int kb = k0; kb < k1; kb += 32) {
+      const int k = kb + lane;
+      double3 t = make_double3(0.0, 0.0, 0.0);
+      if (k < k1) t = row_term(bs, m, cs, r, sgn, k - k0, ilog2toe, e2.t);
+      const bool keep = (k < k1) && t.x != 0.0;
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        double* q = out + 3 * (put + __popc(bal & ((1u << lane) - 1u)));
+        q[0] = t.x;
+        q[1] = t.y;
+        q[2] = t.z;
+      }
+      put += __popc(bal);
     }
-    const bool fp = valid && k < np && c0 != 0.0;
-    const bool fn = valid && k >= np && c0 != 0.0;
-    int tp, tn;
-    const int ip = block_excl_count(fp, tp, sh);
-    const int in = block_excl_count(fn, tn, sh);
-    if (fp) {
-      double* q = s_pos + 3 * (bp + ip);
-      q[0] = c0; q[1] = c1; q[2] = c2;
-    }
-    if (fn) {
-      double* q = s_neg + 3 * (bn + in);
-      q[0] = c0; q[1] = c1; q[2] = c2;
-    }
-    bp += tp;
-    bn += tn;
+    if (half) nneg = put - npos;
+    else npos = put;
   }
-  if (threadIdx.x == 0) {
-    s_cnt[0] = bp;
-    s_cnt[1] = bn;
-  }
-  __syncthreads();
+  if (lane == 0) rcnt[static_cast<size_t>(wb) * bs.nrows + r] = make_int2(npos, nneg);
 }
 
-// R(f1 row, f2 column j) from a staged row (numberCountsDoubleLogNormal.cc:
-// 1972-2002): (sum_k c0 2^{(log|f2| - c1)^2 c2}) / |f2|.
+// R(f1 row, f2 column j) from a row's compacted term lists
+// (numberCountsDoubleLogNormal.cc:1972-2002): (sum_k c0 2^{(log|f2| - c1)^2
+// c2}) / |f2|, over the list of column j's band-2 sign.
 __device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
-                                       const double* s_pos,
-                                       const double* s_neg, int npos,
-                                       int nneg, int j, const double* tab) {
+                                       const double* __restrict__ row, int2 nt, int j,
+                                       const double* tab) {
   if (sgn1 < 0) return 0.0;
   const double if2 = bs.colinv[j];
   if (if2 == 0) return 0.0;
   const int fs = bs.colsgn[j];
   if (!bs.hassign[sgn1 + fs]) return 0.0;
-  const double* L = fs ? s_neg : s_pos;
-  const int cnt = fs ? nneg : npos;
+  const double* L = fs ? row + 3 * nt.x : row;
+  const int cnt = fs ? nt.y : nt.x;
   const double lf2 = bs.collog[j];
   // two partial sums over alternate terms: independent exp2 chains overlap
   double wa = 0.0, wb = 0.0;
   int k = 0;
 #pragma unroll 2
   for (; k + 1 < cnt; k += 2) {
-    const double ta = lf2 - L[3 * k + 1];
-    const double tb = lf2 - L[3 * k + 4];
-    wa += L[3 * k] * dev::exp2_tab(ta * ta * L[3 * k + 2], tab);
-    wb += L[3 * k + 3] * dev::exp2_tab(tb * tb * L[3 * k + 5], tab);
+    const double ta = lf2 - __ldg(L + 3 * k + 1);
+    const double tb = lf2 - __ldg(L + 3 * k + 4);
+    wa += __ldg(L + 3 * k) * dev::exp2_tab(ta * ta * __ldg(L + 3 * k + 2), tab);
+    wb += __ldg(L + 3 * k + 3) * dev::exp2_tab(tb * tb * __ldg(L + 3 * k + 5), tab);
   }
   if (k < cnt) {
-    const double ta = lf2 - L[3 * k + 1];
-    wa += L[3 * k] * dev::exp2_tab(ta * ta * L[3 * k + 2], tab);
+    const double ta = lf2 - __ldg(L + 3 * k + 1);
+    wa += __ldg(L + 3 * k) * dev::exp2_tab(ta * ta * __ldg(L + 3 * k + 2), tab);
   }
   return (wa + wb) * if2;
 }
@@ -348,10 +308,8 @@ __device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
 __global__ void __launch_bounds__(NT)
 k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
          const int* __restrict__ mstatus, const double* __restrict__ rw,
-         double* __restrict__ rbuf, double* __restrict__ rpart) {
-  extern __shared__ double sm[];
-  __shared__ int sh[40];
-  __shared__ int s_cnt[2];
+         const int2* __restrict__ rcnt, double* __restrict__ rbuf,
+         double* __restrict__ rpart) {
   __shared__ double shr[32];
   const int wb = blockIdx.z;
   const int w = wb / B, b = wb - w * B;
@@ -360,9 +318,6 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
   e2.load();
   __syncthreads();
   const BSet2Dev& bs = bsets[b];
-  const int T = bs.T;
-  double* s_pos = sm;
-  double* s_neg = sm + 3 * T;
   const int j = blockIdx.x * NT + threadIdx.x;
   const double fluxfac = bs.dflux1 * bs.dflux2;
   const double cf2 = (j < n) ? bs.rflux2[j] : 0.0;
@@ -372,10 +327,9 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
     const int r = 1 + blockIdx.y * RB + rr;
     if (r >= n) break;
     const int sgn1 = bs.rowsgn[r];
-    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
-              s_pos, s_neg, s_cnt, sh);
+    const size_t ri = static_cast<size_t>(wb) * bs.nrows + r;
     if (j >= 1 && j < n) {
-      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j, e2.t) * fluxfac;
+      const double R = r_at(bs, sgn1, rw + ri * bs.Ts * 3, rcnt[ri], j, e2.t) * fluxfac;
       rbuf[(static_cast<size_t>(wb) * n + r) * nc2 + j] = R;
       const double cf1 = bs.rowflux[r];
       const double cR = (r == n - 1) ? 0.5 * R : R;
@@ -386,7 +340,6 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
       m2 += p2;
       v2 += cf2 * p2;
     }
-    __syncthreads();
   }
   m1 = dev::block_sum<NT>(m1, shr);
   v1 = dev::block_sum<NT>(v1, shr);
@@ -408,10 +361,7 @@ constexpr int ER = 8;
 __global__ void __launch_bounds__(NT)
 k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
          const int* __restrict__ mstatus, const double* __restrict__ rw,
-         double* __restrict__ epart) {
-  extern __shared__ double sm[];
-  __shared__ int sh[40];
-  __shared__ int s_cnt[2];
+         const int2* __restrict__ rcnt, double* __restrict__ epart) {
   const int wb = blockIdx.z;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
@@ -419,8 +369,6 @@ k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   e2.load();
   __syncthreads();
   const BSet2Dev& bs = bsets[b];
-  double* s_pos = sm;
-  double* s_neg = sm + 3 * bs.T;
   const int ncol = n + nedge;
   const int j = blockIdx.x * NT + threadIdx.x;
   double acc = 0.0;
@@ -429,14 +377,12 @@ k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
     if (i >= nedge) break;
     const int r = n + i;
     const int sgn1 = bs.rowsgn[r];
-    stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
-              s_pos, s_neg, s_cnt, sh);
+    const size_t ri = static_cast<size_t>(wb) * bs.nrows + r;
     if (j < ncol) {
-      const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], j, e2.t);
+      const double R = r_at(bs, sgn1, rw + ri * bs.Ts * 3, rcnt[ri], j, e2.t);
       const double rf = bs.e1[i];
       acc += ((i == 0 || i == nedge - 1) ? 0.5 : 1.0) * rf * R;
     }
-    __syncthreads();
   }
   if (j < ncol) epart[(static_cast<size_t>(wb) * gridDim.y + blockIdx.y) * ncol + j] = acc;
 }
@@ -446,10 +392,7 @@ k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
 __global__ void __launch_bounds__(NT)
 k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
       const int* __restrict__ mstatus, const double* __restrict__ rw,
-      double* __restrict__ redge) {
-  extern __shared__ double sm[];
-  __shared__ int sh[40];
-  __shared__ int s_cnt[2];
+      const int2* __restrict__ rcnt, double* __restrict__ redge) {
   __shared__ double shr[32];
   const int wb = blockIdx.y;
   const int w = wb / B, b = wb - w * B;
@@ -458,17 +401,15 @@ k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   e2.load();
   __syncthreads();
   const BSet2Dev& bs = bsets[b];
-  const int T = bs.T;
   const int r = blockIdx.x + 1;  // main rows 1..n-1
   if (r >= n) return;
-  double* s_pos = sm;
-  double* s_neg = sm + 3 * T;
   const int sgn1 = bs.rowsgn[r];
-  stage_row(bs, rw + (static_cast<size_t>(wb) * bs.nrows + r) * bs.Ts * 3, sgn1,
-            s_pos, s_neg, s_cnt, sh);
+  const size_t ri = static_cast<size_t>(wb) * bs.nrows + r;
+  const double* row = rw + ri * bs.Ts * 3;
+  const int2 nt = rcnt[ri];
   double acc = 0.0;
   for (int jj = threadIdx.x; jj < nedge; jj += NT) {
-    const double R = r_at(bs, sgn1, s_pos, s_neg, s_cnt[0], s_cnt[1], n + jj, e2.t);
+    const double R = r_at(bs, sgn1, row, nt, n + jj, e2.t);
     acc += (jj == 0 || jj == nedge - 1) ? 0.5 * R : R;
   }
   acc = dev::block_sum<NT>(acc, shr);
@@ -2011,7 +1952,7 @@ void Engine2::build_static() {
 }
 
 void Engine2::free_work() {
-  void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.rw, ws_.rbuf,
+  void* ptrs[] = {ws_.cnt, ws_.mstatus, ws_.sigmult, ws_.rw, ws_.rcnt, ws_.rbuf,
                   ws_.rpart, ws_.redge, ws_.epart, ws_.fpart, ws_.mom, ws_.pbuf, ws_.rowpart,
                   ws_.colpart, ws_.pinfo, ws_.gpart, ws_.pdout,
                   ws_.theta_in, ws_.logl, ws_.status, ws_.bonus, ws_.bcnt,
@@ -2049,6 +1990,7 @@ void Engine2::reserve(unsigned P) {
   ws_.bstatus = dal<int>(P);
   ws_.bsig = dal<double>(2 * static_cast<size_t>(P));
   ws_.rw = dal<double>(static_cast<size_t>(P) * B_ * nrows * Tmax_ * 3);
+  ws_.rcnt = dal<int2>(static_cast<size_t>(P) * B_ * nrows);
   ws_.rbuf = dal<double>(static_cast<size_t>(P) * B_ * n * nc2);
   ws_.rpart = dal<double>(static_cast<size_t>(P) * B_ * gx_ * gy_ * 4);
   ws_.redge = dal<double>(static_cast<size_t>(P) * B_ * (2 * n + 1));
@@ -2066,10 +2008,6 @@ void Engine2::reserve(unsigned P) {
   ws_.logl = dal<double>(P);
   ws_.status = dal<int>(P);
   ck(cudaMemset(ws_.redge, 0, static_cast<size_t>(P) * B_ * (2 * n + 1) * sizeof(double)), "memset");
-  const int smem_rows = static_cast<int>(6 * MAXT * sizeof(double));
-  ck(cudaFuncSetAttribute(k_rgrid2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
-  ck(cudaFuncSetAttribute(k_redge2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
-  ck(cudaFuncSetAttribute(k_ry2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows), "attr");
   ck(cudaFuncSetAttribute(k_psplit2, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           static_cast<int>(3 * 8192 * sizeof(double))), "attr");
 }
@@ -2170,7 +2108,6 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   const int n = static_cast<int>(n_), nc = n / 2 + 1, nc2 = 2 * nc;
   const int P = static_cast<int>(nprop), B = static_cast<int>(B_), D = static_cast<int>(D_);
   const int ne = edge_ ? static_cast<int>(nedge_) : 0;
-  const size_t smem_rows = 6 * static_cast<size_t>(Tmax_) * sizeof(double);
   Plans& pl = plans_.at(nprop);
   mark(0);
   k_model2<<<P, 32, 0, st>>>(model_, theta, static_cast<int>(npar), std::log2(10.0),
@@ -2181,21 +2118,22 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                            d_qw_, d_qk_, nq_, ws_.bonus, -1);
   mark(1);
   {
-    const size_t nrows = static_cast<size_t>(n + ne);
-    const unsigned gxr = static_cast<unsigned>((nrows * Tmax_ + NT - 1) / NT);
+    const unsigned nrows = static_cast<unsigned>(n + ne);
+    const unsigned gxr = (nrows + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK;
     k_rows2<<<dim3(gxr, P * B), NT, 0, st>>>(d_bsets_, model_, B, 1.0 / std::log(2.),
-                                             ws_.mstatus, ws_.cnt, ws_.rw);
+                                             ws_.mstatus, ws_.cnt, ws_.rw, ws_.rcnt);
   }
   mark(2);
-  k_rgrid2<<<dim3(gx_, gy_, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, nc2, ws_.mstatus,
-                                                         ws_.rw, ws_.rbuf, ws_.rpart);
+  k_rgrid2<<<dim3(gx_, gy_, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
+                                                 ws_.rcnt, ws_.rbuf, ws_.rpart);
   mark(3);
   const int ngr = (ne + ER - 1) / ER;
   if (edge_) {
     const unsigned gxe = static_cast<unsigned>((n + ne + NT - 1) / NT);
-    k_redge2<<<dim3(gxe, ngr, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus,
-                                                            ws_.rw, ws_.epart);
-    k_ry2<<<dim3(n - 1, P * B), NT, smem_rows, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.redge);
+    k_redge2<<<dim3(gxe, ngr, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw,
+                                                    ws_.rcnt, ws_.epart);
+    k_ry2<<<dim3(n - 1, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.rcnt,
+                                             ws_.redge);
   }
   mark(4);
   {
@@ -2477,6 +2415,21 @@ int Engine2::pd_host(int bs, int ds, const float* theta, unsigned npar,
   ck(cudaMemcpyAsync(pd_out, ws_.pdout, n * n * sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H pd");
   ck(cudaStreamSynchronize(stream_), "synchronize");
   return 0;
+}
+
+void Engine2::active_terms(const float* theta, unsigned npar, long long* out2) {
+  double ll;
+  int st;
+  eval_host(1, theta, npar, &ll, &st);
+  out2[0] = out2[1] = 0;
+  for (unsigned b = 0; b < B_; ++b) {
+    const BSet2Dev& bs = h_bsets_[b];
+    std::vector<int2> rc(bs.nrows);
+    ck(cudaMemcpy(rc.data(), ws_.rcnt + static_cast<size_t>(b) * bs.nrows,
+                  rc.size() * sizeof(int2), cudaMemcpyDeviceToHost), "D2H row counts");
+    for (int r = 1; r < bs.nrows; ++r)
+      out2[r < static_cast<int>(n_) ? 0 : 1] += rc[r].x + rc[r].y;
+  }
 }
 
 void Engine2::rgrid_host(int bs, const float* theta, unsigned npar, double* out) {

@@ -125,6 +125,10 @@ class Engine2 {
   int pd_host(int bs, int ds, const float* theta, unsigned npar, bool setlog,
               double* pd_out, double* info16);
   void rgrid_host(int bs, const float* theta, unsigned npar, double* out);
+  // Active colour terms (c0 != 0) of one proposal's R grid rows, summed over
+  // the main rows 1 .. n-1 (out[0]) and the edge rows (out[1]) of every beam
+  // set: the R builders' algorithmic work is these times the columns.
+  void active_terms(const float* theta, unsigned npar, long long* out2);
   void profile_stages(unsigned nprop, const float* theta, unsigned npar,
                       int reps, double* stage_ms);
   static const char* stage_name(int i);
@@ -245,7 +249,8 @@ class Engine2 {
     double* cnt = nullptr;      // [P][12*KMAX]
     int* mstatus = nullptr;
     double* sigmult = nullptr;  // [P][2]
-    double* rw = nullptr;       // [P][B][nrows][T][3]
+    double* rw = nullptr;       // [P][B][nrows][T][3] compacted row terms
+    int2* rcnt = nullptr;       // [P][B][nrows] (positive, negative) term counts
     double* rbuf = nullptr;     // [P][B][n][2nc]
     double* rpart = nullptr;    // [P][B][gy][gx][4]
     double* redge = nullptr;    // [P][B][2n+1]: Ry at [n, 2n)

@@ -51,13 +51,23 @@ def _compare(orc, gpu_ctx, cfg, nprop, seed, sigmult_rows=()):
     assert ok.sum() >= nprop - 1
     err = float(np.max(np.abs(lg[ok] - lo[ok])))
     assert err < LL_TOL, err
-    # P(D) of every beam set for one proposal with a sigma multiplier
+    # P(D) of every beam set for one proposal with a sigma multiplier.  Where
+    # the split search takes its jitter branch (the P(D) tail reaches the
+    # transform's rounding floor, as at n = 65536), the first bin below the
+    # jitter estimate is set by rounding noise and can differ between any
+    # two FFTs; the unwrapped arrays are then the same wrapped P(D) rotated
+    # differently, and the bins between the two splits are at the noise
+    # floor (the log-likelihood above is unaffected).
     k = sigmult_rows[0][0] if sigmult_rows else 0
     for b in range(len(cfg["beams"])):
         pg, ig = G.getPD(b, 0, th[k], setLog=False)
         po, io = O.pd(b, 0, th[k], setlog=False)
-        assert int(ig["splitidx"]) == int(io["splitidx"])
-        assert np.max(np.abs(pg - po)) <= P_TOL * po.max()
+        ds = int(ig["splitidx"]) - int(io["splitidx"])
+        if ds:
+            assert abs(ds) < 0.01 * pg.size
+            tail = pg[-ds:] if ds > 0 else pg[:-ds]
+            assert np.max(tail) < 1e-9 * pg.max()
+        assert np.max(np.abs(np.roll(po, -ds) - pg)) <= P_TOL * po.max()
     return err
 
 
