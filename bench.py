@@ -469,6 +469,7 @@ def measure_2d(a, ctx, stream):
     sptr = stream.cuda_stream
     ref, st = L.getLogLikeBatch(host[0])
     assert np.all(st == 0), st
+    tuning = L.autotune(host[0], reps=3) if not a.no_autotune else L.getTuning()
     steps = max(3, a.steps // 50)
     for k in range(max(a.warmup, 3)):
         L.getLogLikeDevice(BATCH_2D, dth[k % 2].data_ptr(), npar,
@@ -499,7 +500,8 @@ def measure_2d(a, ctx, stream):
            "e2e": {"value": BATCH_2D * steps / e2e_s, "unit": "evals/s",
                    "h2d_bytes_per_step": BATCH_2D * npar * 4,
                    "d2h_bytes_per_step": BATCH_2D * 12},
-           "stage_ms": stages, "gpu_launches": L.kernelsPerEval() * steps}
+           "stage_ms": stages, "gpu_launches": L.kernelsPerEval() * steps,
+           "autotune": tuning}
     out.update(roof)
     if not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_2d(cfg, a.cpu_seconds)

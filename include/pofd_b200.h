@@ -343,6 +343,18 @@ int pofd_like2_fft_info(const pofd_like2* L, int* fused);
  * n = 2048, ~1e-5 in a log-likelihood over 2.25 M pixels).  Mode 1 is slow
  * (a 2 n^2-long dependent chain per dataset) and meant for parity checks. */
 int pofd_like2_set_reference_sums(pofd_like2* L, int on);
+/* Autotuner of the 2D launch shapes (the project's own; no counterpart in
+ * the reference): times the whole graph-captured launch sequence on nprop
+ * host rows (reps replays per candidate, CUDA events) for each knob in turn
+ * -- FFT mode (see pofd_like2_set_fft), R-grid rows per block {2, 4, 8},
+ * band-1 edge rows per group {4, 8, 16} -- and keeps the fastest.  out5
+ * (optional) = {fft_mode, rgrid_rows, edge_rows, best ms, untuned ms}.
+ * get/set_tuning read or impose the three knobs in that order.  Results
+ * change only by rounding (reduction grouping, FFT implementation). */
+int pofd_like2_autotune(pofd_like2* L, unsigned nprop, const float* theta,
+                        unsigned npar, int reps, double* out5);
+int pofd_like2_get_tuning(const pofd_like2* L, int* knobs3);
+int pofd_like2_set_tuning(pofd_like2* L, const int* knobs3);
 /* Work count of the 2D R builders for one proposal theta: out2[0] = the
  * active colour terms (numberCountsDoubleLogNormal.cc:1883-1963, c0 != 0)
  * summed over the main grid rows 1 .. n-1, out2[1] over the edge rows, all

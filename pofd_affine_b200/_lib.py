@@ -108,6 +108,9 @@ SIGNATURES = {
     "pofd_like2_set_fft": (I, [V, I]),
     "pofd_like2_set_reference_sums": (I, [V, I]),
     "pofd_like2_active_terms": (I, [V, _fp, U, C.POINTER(C.c_longlong)]),
+    "pofd_like2_autotune": (I, [V, U, _fp, U, I, V]),
+    "pofd_like2_get_tuning": (I, [V, _ip]),
+    "pofd_like2_set_tuning": (I, [V, _ip]),
     "pofd_like2_fft_info": (I, [V, C.POINTER(I)]),
     "pofd_pd1_loglike_noalloc": (I, [V, U, D, D, U, D, D, V, V, U, D, D, D, D,
                                      V, V, V]),

@@ -313,6 +313,34 @@ class calcLikeDouble:
         default tree sums; slow, for parity checks."""
         check(lib().pofd_like2_set_reference_sums(self.h, 1 if on else 0))
 
+    TUNING_KEYS = ("fft_mode", "rgrid_rows", "edge_rows")
+
+    def autotune(self, thetas, reps=5):
+        """Choose the launch shapes by timing the graph-captured launch
+        sequence on these rows; returns the chosen knobs with the best and
+        the untuned time per launch (ms)."""
+        th = np.ascontiguousarray(_f32(thetas))
+        if th.ndim != 2:
+            raise PofdError(-10, "thetas must be [nprop, npar]")
+        out = np.zeros(5)
+        check(lib().pofd_like2_autotune(self.h, th.shape[0], th.ravel(),
+                                        th.shape[1], int(reps),
+                                        out.ctypes.data_as(C.c_void_p)))
+        d = {k: int(v) for k, v in zip(self.TUNING_KEYS, out[:3])}
+        d["ms"], d["untuned_ms"] = float(out[3]), float(out[4])
+        return d
+
+    def getTuning(self):
+        k = np.zeros(len(self.TUNING_KEYS), dtype=np.int32)
+        check(lib().pofd_like2_get_tuning(self.h, k))
+        return {n: int(v) for n, v in zip(self.TUNING_KEYS, k)}
+
+    def setTuning(self, **knobs):
+        cur = self.getTuning()
+        cur.update(knobs)
+        k = np.array([cur[n] for n in self.TUNING_KEYS], dtype=np.int32)
+        check(lib().pofd_like2_set_tuning(self.h, k))
+
     def activeTerms(self, p):
         """(main-row, edge-row) active colour terms of one proposal's R
         grid, summed over rows and beam sets (the R builders' work per

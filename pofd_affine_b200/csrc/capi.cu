@@ -771,6 +771,41 @@ int pofd_like2_get_r(pofd_like2* L, int beamset, const float* theta,
   });
 }
 
+int pofd_like2_autotune(pofd_like2* L, unsigned nprop, const float* theta, unsigned npar,
+                        int reps, double* out5) {
+  return guard([&] {
+    need(L && theta, "null argument");
+    need(L->ctx->device >= 0, "host-only context has no GPU");
+    cudaSetDevice(L->ctx->device);
+    L->eng->autotune(nprop, theta, npar, reps, out5);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_get_tuning(const pofd_like2* L, int* knobs3) {
+  return guard([&] {
+    need(L && knobs3, "null argument");
+    const pofd::Tune2 t = L->eng->tuning();
+    knobs3[0] = t.fft_mode;
+    knobs3[1] = t.rgrid_rows;
+    knobs3[2] = t.edge_rows;
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_set_tuning(pofd_like2* L, const int* knobs3) {
+  return guard([&] {
+    need(L && knobs3, "null argument");
+    pofd::Tune2 t;
+    t.fft_mode = knobs3[0];
+    t.rgrid_rows = knobs3[1];
+    t.edge_rows = knobs3[2];
+    if (L->ctx->device >= 0) cudaSetDevice(L->ctx->device);
+    L->eng->set_tuning(t);
+    return POFD_OK;
+  });
+}
+
 int pofd_like2_active_terms(pofd_like2* L, const float* theta, unsigned npar,
                             long long* out2) {
   return guard([&] {

@@ -34,7 +34,7 @@ namespace pofd {
 namespace {
 
 constexpr int NT = 256;
-constexpr int RB = 4;        // R-grid rows per block
+constexpr int RB_MIN = 2;    // fewest R-grid rows per block (sizes the partials)
 constexpr int RTILE = 32;    // P(D) rows per scan block
 constexpr int GCH = 1024;    // data bins per gather block
 constexpr int KMAX = Engine2::KMAX;
@@ -305,6 +305,7 @@ __device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
 // Main R grid, rows 1..n-1 x columns 1..n-1 (row 0 and column 0 are the
 // edge cells), times dflux1*dflux2, with block partial sums of the
 // trapezoid moments of getRStats (PDFactoryDouble.cc:593-722).
+template <int RB>
 __global__ void __launch_bounds__(NT)
 k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
          const int* __restrict__ mstatus, const double* __restrict__ rw,
@@ -357,7 +358,8 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
 // of ER edge rows, proposal x beam set); the group partials are summed in
 // k_rfinish2 into Rx (main columns) and the double integral r[0,0] (edge
 // columns).
-constexpr int ER = 8;
+constexpr int ER_MIN = 4;    // fewest edge rows per group (sizes the partials)
+template <int ER>
 __global__ void __launch_bounds__(NT)
 k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
          const int* __restrict__ mstatus, const double* __restrict__ rw,
@@ -1939,7 +1941,7 @@ void Engine2::build_static() {
   static_allocs_.push_back(d_dsets_);
   ck(cudaMemcpy(d_dsets_, h_dsets_.data(), D_ * sizeof(DSet2Dev), cudaMemcpyHostToDevice), "upload");
   gx_ = (n + NT - 1) / NT;
-  gy_ = (n - 1 + RB - 1) / RB;
+  gy_ = (n - 1 + RB_MIN - 1) / RB_MIN;  // the most row groups any tuning uses
   nrt_ = (n + RTILE - 1) / RTILE;
   nct_ = (n + NT - 1) / NT;
   gchunks_ = (maxnnz + GCH - 1) / GCH;
@@ -1994,7 +1996,7 @@ void Engine2::reserve(unsigned P) {
   ws_.rbuf = dal<double>(static_cast<size_t>(P) * B_ * n * nc2);
   ws_.rpart = dal<double>(static_cast<size_t>(P) * B_ * gx_ * gy_ * 4);
   ws_.redge = dal<double>(static_cast<size_t>(P) * B_ * (2 * n + 1));
-  const size_t ngr = edge_ ? (nedge_ + ER - 1) / ER : 0;
+  const size_t ngr = edge_ ? (nedge_ + ER_MIN - 1) / ER_MIN : 0;
   ws_.epart = dal<double>(static_cast<size_t>(P) * B_ * (ngr ? ngr * (n + nedge_) : 1));
   ws_.mom = dal<double>(static_cast<size_t>(P) * B_ * 8);
   ws_.r0 = dal<double>(static_cast<size_t>(P) * B_);
@@ -2063,6 +2065,84 @@ void Engine2::set_fft_mode(int mode) {
   else colspec_ = false;
 }
 
+double Engine2::time_sequence(unsigned nprop, const float* theta, unsigned npar, int reps) {
+  std::vector<double> ll(nprop);
+  std::vector<int> st(nprop);
+  eval_host(nprop, theta, npar, ll.data(), st.data());
+  enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);  // capture or warm
+  enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);
+  cudaEvent_t e0, e1;
+  ck(cudaEventCreate(&e0), "event create");
+  ck(cudaEventCreate(&e1), "event create");
+  ck(cudaEventRecord(e0, stream_), "event record");
+  for (int r = 0; r < reps; ++r) enqueue(nprop, ws_.theta_in, npar, ws_.logl, ws_.status, stream_);
+  ck(cudaEventRecord(e1, stream_), "event record");
+  ck(cudaEventSynchronize(e1), "event sync");
+  float ms = 0.f;
+  ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return static_cast<double>(ms) / reps;
+}
+
+void Engine2::set_tuning(const Tune2& t) {
+  if (t.fft_mode != 0 && t.fft_mode != 1) throw Error(POFD_E_ARG, "fft_mode must be 0 or 1");
+  if (t.rgrid_rows != 2 && t.rgrid_rows != 4 && t.rgrid_rows != 8)
+    throw Error(POFD_E_ARG, "rgrid_rows must be 2, 4 or 8");
+  if (t.edge_rows != 4 && t.edge_rows != 8 && t.edge_rows != 16)
+    throw Error(POFD_E_ARG, "edge_rows must be 4, 8 or 16");
+  set_fft_mode(t.fft_mode);
+  tune_ = t;
+  drop_graphs();
+}
+
+// Coordinate descent over the knobs, one pass, each candidate timed on the
+// captured graph of the whole sequence.
+void Engine2::autotune(unsigned nprop, const float* theta, unsigned npar, int reps,
+                       double* out5) {
+  NvtxRange nvtx_range("pofd like2 autotune");
+  if (nprop == 0 || reps < 1) throw Error(POFD_E_ARG, "autotune needs rows and reps >= 1");
+  if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
+  const double t_untuned = time_sequence(nprop, theta, npar, reps);
+  Tune2 best = tuning();
+  double best_ms = t_untuned;
+  auto trial = [&](const Tune2& t) {
+    set_tuning(t);
+    const double ms = time_sequence(nprop, theta, npar, reps);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  };
+  {
+    Tune2 t = best;
+    t.fft_mode = best.fft_mode ? 0 : 1;
+    trial(t);
+  }
+  for (int rb : {2, 4, 8}) {
+    if (rb == best.rgrid_rows) continue;
+    Tune2 t = best;
+    t.rgrid_rows = rb;
+    trial(t);
+  }
+  if (edge_) {
+    for (int er : {4, 8, 16}) {
+      if (er == best.edge_rows) continue;
+      Tune2 t = best;
+      t.edge_rows = er;
+      trial(t);
+    }
+  }
+  set_tuning(best);
+  if (out5) {
+    out5[0] = best.fft_mode;
+    out5[1] = best.rgrid_rows;
+    out5[2] = best.edge_rows;
+    out5[3] = best_ms;
+    out5[4] = t_untuned;
+  }
+}
+
 void Engine2::set_reference_sums(bool on) {
   if (on == refsum_) return;
   refsum_ = on;
@@ -2124,14 +2204,39 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                              ws_.mstatus, ws_.cnt, ws_.rw, ws_.rcnt);
   }
   mark(2);
-  k_rgrid2<<<dim3(gx_, gy_, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
-                                                 ws_.rcnt, ws_.rbuf, ws_.rpart);
+  const int rb = tune_.rgrid_rows;
+  const unsigned gy = static_cast<unsigned>((n - 1 + rb - 1) / rb);
+  switch (rb) {
+    case 2:
+      k_rgrid2<2><<<dim3(gx_, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
+                                                       ws_.rcnt, ws_.rbuf, ws_.rpart);
+      break;
+    case 8:
+      k_rgrid2<8><<<dim3(gx_, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
+                                                       ws_.rcnt, ws_.rbuf, ws_.rpart);
+      break;
+    default:
+      k_rgrid2<4><<<dim3(gx_, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
+                                                       ws_.rcnt, ws_.rbuf, ws_.rpart);
+  }
   mark(3);
-  const int ngr = (ne + ER - 1) / ER;
+  const int er = tune_.edge_rows;
+  const int ngr = (ne + er - 1) / er;
   if (edge_) {
     const unsigned gxe = static_cast<unsigned>((n + ne + NT - 1) / NT);
-    k_redge2<<<dim3(gxe, ngr, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw,
-                                                    ws_.rcnt, ws_.epart);
+    switch (er) {
+      case 4:
+        k_redge2<4><<<dim3(gxe, ngr, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw,
+                                                          ws_.rcnt, ws_.epart);
+        break;
+      case 16:
+        k_redge2<16><<<dim3(gxe, ngr, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw,
+                                                           ws_.rcnt, ws_.epart);
+        break;
+      default:
+        k_redge2<8><<<dim3(gxe, ngr, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw,
+                                                          ws_.rcnt, ws_.epart);
+    }
     k_ry2<<<dim3(n - 1, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.rcnt,
                                              ws_.redge);
   }
@@ -2139,7 +2244,7 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   {
     const int nfp = (n + NT - 1) / NT;
     k_rfinish2<<<dim3(nfp, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0, ne, ngr,
-                                                static_cast<int>(gx_ * gy_), ws_.mstatus,
+                                                static_cast<int>(gx_ * gy), ws_.mstatus,
                                                 ws_.redge, ws_.epart, ws_.rpart, ws_.rbuf,
                                                 ws_.fpart);
     k_rfinal2<<<P * B, NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0, ne, ngr, nfp,

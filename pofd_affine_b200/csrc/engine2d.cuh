@@ -94,6 +94,14 @@ struct PDInfo2 {
   double itot, minflux1, minflux2, sg1pos, sg1neg, sg2pos, sg2neg, pad2;
 };
 
+// Launch-shape knobs of the 2D sequence chosen by Engine2::autotune (none
+// changes what is computed; the FFT mode changes the transform's rounding).
+struct Tune2 {
+  int fft_mode = 1;     // see set_fft_mode
+  int rgrid_rows = 4;   // R-grid rows per block of k_rgrid2 (2, 4, 8)
+  int edge_rows = 8;    // band-1 edge rows per group of k_redge2 (4, 8, 16)
+};
+
 class Engine2 {
  public:
   static constexpr int KMAX = 64;
@@ -143,6 +151,17 @@ class Engine2 {
   // chain in the reference's order instead of the default tree sums.  For
   // parity checks only (a 2n^2-long dependent chain per dataset).
   void set_reference_sums(bool on);
+  // Times the whole launch sequence (graph replays, CUDA events) for each
+  // candidate of each knob in turn on nprop host rows and keeps the
+  // fastest; out5 (optional) = {fft_mode, rgrid_rows, edge_rows, best ms per
+  // launch, untuned ms per launch}.
+  void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out5);
+  Tune2 tuning() const {
+    Tune2 t = tune_;
+    t.fft_mode = fft_mode_;
+    return t;
+  }
+  void set_tuning(const Tune2& t);
   bool reference_sums() const { return refsum_; }
   // 0: batched 2D cuFFT transforms with k_spectrum2 between them; 1: batched
   // 1D cuFFT row transforms around this library's fused column-transform +
@@ -236,6 +255,8 @@ class Engine2 {
   int fft_mode_ = 1;
   bool colspec_ = false;
   bool refsum_ = false;
+  Tune2 tune_;
+  double time_sequence(unsigned nprop, const float* theta, unsigned npar, int reps);
   double2* d_cwh_ = nullptr;  // e^{-2 pi i 32 h / n}, h < n / 32
   double2* d_cwl_ = nullptr;  // e^{-2 pi i l / n}, l < 32
   Prior2 prior_;
