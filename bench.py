@@ -54,7 +54,7 @@ def args():
     p.add_argument("--no-mcmc", action="store_true")
     p.add_argument("--mcmc-2d", type=int, default=1,
                    help="include the two-field 2D MCMC comparison")
-    p.add_argument("--mcmc-steps", type=int, default=1000,
+    p.add_argument("--mcmc-steps", type=int, default=1500,
                    help="recorded steps of each 2D MCMC run")
     p.add_argument("--profile-case", choices=["1d", "2d", "surrogate"],
                    help="run a small fixed workload for a profiler and exit "
@@ -573,18 +573,19 @@ def mcmc_1d(ctx):
     return out
 
 
-def mcmc_2d(ctx, nsteps=1000):
+def mcmc_2d(ctx, nsteps=1500):
     """Plain vs delayed acceptance on the two-field 2D fit (2048^2 and
     1024^2 grids in one launch, 14 free parameters, 128 walkers), from a
     shared equilibrated start, with a plain-vs-plain control
     (runner.compare_two_fields_2d, runner.summarise)."""
     from pofd_affine_b200 import runner
-    r = runner.compare_two_fields_2d(ctx, nsteps, 400, plain_control=True)
+    r = runner.compare_two_fields_2d(ctx, nsteps, 300, plain_control=True)
     out = runner.summarise(r)
     out["workload"] = ("2D two-field fit: 1500x1500 pair on 2048^2 + 800x600 "
                        "pair on 1024^2 in one launch, 14 free parameters, "
-                       "128 walkers, shared start (Powell maximum + 400 plain "
-                       "steps, untimed), burn %d steps (20k exact pairs), %d "
+                       "128 walkers, shared start (Powell maximum, walkers "
+                       "from its Laplace approximation, 300 plain steps, "
+                       "untimed), burn %d steps (20k exact pairs), %d "
                        "recorded steps; DA: MLP 14 -> 3x384 SiLU -> 1 trained "
                        "on the burn-in pairs, retrained every 5k exact "
                        "evaluations, stretch a = %g (plain a = 2)"

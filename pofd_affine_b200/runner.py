@@ -162,6 +162,49 @@ def find_start(loglike, x0, rounds=4, maxfev=2000, bounds=None):
     return x, -best
 
 
+def laplace_covariance(loglike_batch, x0, h, bounds=None):
+    """Covariance of the Laplace approximation at a likelihood maximum x0:
+    the inverse of minus the Hessian of the log-likelihood by central
+    differences with steps h (per parameter), all 1 + 2k + 2k(k-1)
+    evaluations in one batch (loglike_batch(X [m][k]) -> logL [m], None
+    entries for rejected points).  A Hessian that is not negative definite
+    is made so by flipping its negative eigenvalues' signs."""
+    x0 = np.asarray(x0, np.float64)
+    h = np.broadcast_to(np.asarray(h, np.float64), x0.shape)
+    k = x0.size
+    pts = [x0]
+    for i in range(k):
+        for si in (1, -1):
+            e = x0.copy()
+            e[i] += si * h[i]
+            pts.append(e)
+    pairs = [(i, j) for i in range(k) for j in range(i + 1, k)]
+    for i, j in pairs:
+        for si, sj in ((1, 1), (1, -1), (-1, 1), (-1, -1)):
+            e = x0.copy()
+            e[i] += si * h[i]
+            e[j] += sj * h[j]
+            pts.append(e)
+    X = np.array(pts)
+    if bounds is not None:
+        lo = np.array([b[0] for b in bounds])
+        hi = np.array([b[1] for b in bounds])
+        X = np.clip(X, lo, hi)
+    L = np.asarray(loglike_batch(X), np.float64)
+    f0 = L[0]
+    H = np.empty((k, k))
+    for i in range(k):
+        H[i, i] = (L[1 + 2 * i] - 2 * f0 + L[2 + 2 * i]) / (h[i] * h[i])
+    off = 1 + 2 * k
+    for q, (i, j) in enumerate(pairs):
+        a, b, c, d = L[off + 4 * q:off + 4 * q + 4]
+        H[i, j] = H[j, i] = (a - b - c + d) / (4 * h[i] * h[j])
+    w, V = np.linalg.eigh(-0.5 * (H + H.T))
+    w = np.abs(w)
+    w[w < 1e-12 * w.max()] = 1e-12 * w.max()
+    return (V / w) @ V.T
+
+
 def posterior_agreement(a, b, free):
     """(max over free parameters of |mean_a - mean_b| / sd_b, the same in
     units of the standard error of the difference sqrt(var_a / ESS_a,p +
@@ -190,8 +233,9 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
 
     Both methods start from the same walkers, made untimed: a bounded Powell
     maximum of the likelihood (the synthetic maps' generating parameters lie
-    several hundred log-likelihood units below it), a 1e-3 ball around it
-    and npre plain steps.  Each run then burns nburn steps (default: enough
+    several hundred log-likelihood units below it), walkers drawn from the
+    Laplace approximation there (finite-difference Hessian) and npre plain
+    steps.  Each run then burns nburn steps (default: enough
     for 20k exact pairs, on which the surrogate first trains) and records
     nsteps; the surrogate is retrained every 5k new exact evaluations, and
     the delayed-acceptance steps use the stretch parameter da_scale (the
@@ -221,6 +265,14 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
     x0 = a["theta0"].copy()
     x0[:nfree] = xopt
 
+    def loglike_batch(X):
+        t = np.repeat(a["theta0"][None, :].astype(np.float64), X.shape[0], 0)
+        t[:, :nfree] = X
+        t = t.astype(np.float32)
+        (la, sa), (lb, sb) = La.getLogLikeBatch(t), Lb.getLogLikeBatch(t)
+        return np.where((sa == 0) & (sb == 0), la + lb, -np.inf)
+    cov = laplace_covariance(loglike_batch, xopt, 1e-3, bounds=lims)
+
     def ens(seed, start=None):
         E = affineEnsemble(ctx, S2, 128, npar, seed=seed)
         E.setParamFixed(npar - 2)
@@ -229,8 +281,19 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
             E.setParamLimits(p, lo, hi)
         E.setErrorPolicy(True)  # unphysical corners reject instead of stop
         if start is None:
-            sig = np.r_[np.full(nfree, 1e-3), 0, 0]
-            E.initChains(E.generateInitialPosition(x0, sig, rng=seed))
+            # walkers drawn from the Laplace approximation at the maximum,
+            # inside the limits
+            rng = np.random.default_rng(seed)
+            lo = np.array([l for l, _ in lims])
+            hi = np.array([h for _, h in lims])
+            w = np.repeat(x0[None, :].astype(np.float64), 128, 0)
+            k = 0
+            while k < 128:
+                d = rng.multivariate_normal(xopt, cov)
+                if np.all(d > lo) and np.all(d < hi):
+                    w[k, :nfree] = d
+                    k += 1
+            E.initChains(w.astype(np.float32))
         else:
             E.initChains(*start)
         return E
@@ -287,14 +350,14 @@ def summarise(r):
 
 
 def _main(argv=None):
-    """python -m pofd_affine_b200.runner two-fields-2d --steps 1500 --pre 1000"""
+    """python -m pofd_affine_b200.runner two-fields-2d --steps 3000 --pre 300"""
     import argparse
     import json
     from . import Context
     p = argparse.ArgumentParser()
     p.add_argument("case", choices=["two-fields-2d"])
-    p.add_argument("--steps", type=int, default=1500)
-    p.add_argument("--pre", type=int, default=1000)
+    p.add_argument("--steps", type=int, default=3000)
+    p.add_argument("--pre", type=int, default=300)
     p.add_argument("--burn", type=int, default=None)
     p.add_argument("--da-scale", type=float, default=DA_SCALE_2D)
     a = p.parse_args(argv)
