@@ -168,6 +168,12 @@ int pofd_like1_add_dataset(pofd_like1* L, int beamset, const double* data,
 int pofd_like1_set_rranges(pofd_like1* L, const float* theta, unsigned npar);
 /* range2 = {minRFlux, maxRFlux} of a beam set. */
 int pofd_like1_get_rrange(const pofd_like1* L, int beamset, double* range2);
+/* The R grid (times dflux) of one beam set for one proposal theta, out[n],
+ * as the forward transform sees it (PDFactory::initR, PDFactory.cc:541-620),
+ * built by the R fill the tuning selects (materialised forms; the fused
+ * form evaluates the same points one exp2 each). */
+int pofd_like1_get_r(pofd_like1* L, int beamset, const float* theta,
+                     unsigned npar, double* out);
 /* info9 = {ndata, nbins, bincent0, bindelta, like_offset, sigma_base,
  *  like_norm, minDataFlux, maxDataFlux}; bins (may be NULL) gets nbins
  *  counts. */
@@ -216,11 +222,12 @@ int pofd_like1_fft_info(pofd_like1* L, int* own);
  * GPU and no counterpart): times the whole graph-captured launch sequence on
  * nprop host rows (reps replays per candidate, CUDA events) for each knob in
  * turn -- own FFT vs cuFFT, R-fill points per thread {4, 8, 16}, R-node
- * threads per block {64, 128, 256}, the R grid fill (0: materialised, 1:
- * inside the forward FFT pass A with one exp2 per grid point, 2: inside it
- * by running products over 16-point segments), spectrum blocks per row
- * {2 ... 32} -- and keeps the fastest.  out7 (optional) = {own_fft,
- * rfill_per, rnodes_threads, spec_blocks, rfill_fused, best ms, untuned ms}.
+ * threads per block {64, 128, 256}, the R grid fill (rfill_mode 0:
+ * materialised, one exp2 per grid point; 1: the same inside the forward FFT
+ * pass A, the grid never stored; 2: materialised by running products over
+ * 16-point segments), spectrum blocks per row {2 ... 32} -- and keeps the
+ * fastest.  out7 (optional) = {own_fft,
+ * rfill_per, rnodes_threads, spec_blocks, rfill_mode, best ms, untuned ms}.
  * get/set_tuning read or impose the five knobs in that order (e.g. a tuning
  * saved from an earlier run).  Results change only by rounding (reduction
  * grouping, FFT implementation, exponential evaluation). */

@@ -56,6 +56,7 @@ SIGNATURES = {
     "pofd_like1_add_dataset": (I, [V, I, _dp, S, I, D, D]),
     "pofd_like1_set_rranges": (I, [V, _fp, U]),
     "pofd_like1_get_rrange": (I, [V, I, _dp]),
+    "pofd_like1_get_r": (I, [V, I, _fp, U, _dp]),
     "pofd_like1_dataset_info": (I, [V, I, I, _dp, V]),
     "pofd_like1_reserve": (I, [V, U]),
     "pofd_like1_loglike": (I, [V, _fp, U, C.POINTER(D), C.POINTER(I)]),

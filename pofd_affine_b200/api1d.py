@@ -235,6 +235,13 @@ class calcLike:
         th = _f32(p)
         check(lib().pofd_like1_set_rranges(self.h, th, th.size))
 
+    def getR(self, beamset, p):
+        """The R grid (times dflux) of a beam set for parameters p."""
+        th = _f32(p)
+        out = np.empty(self.fftsize)
+        check(lib().pofd_like1_get_r(self.h, int(beamset), th, th.size, out))
+        return out
+
     def getRRange(self, beamset):
         out = np.empty(2)
         check(lib().pofd_like1_get_rrange(self.h, int(beamset), out))
@@ -367,7 +374,7 @@ class calcLike:
         return th[0] if one else th
 
     TUNING_KEYS = ("own_fft", "rfill_per", "rnodes_threads", "spec_blocks",
-                   "rfill_fused")
+                   "rfill_mode")
 
     def autotune(self, thetas, reps=20):
         """Choose the launch shapes by timing the graph-captured launch

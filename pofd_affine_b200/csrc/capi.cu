@@ -535,7 +535,7 @@ int pofd_like1_get_tuning(const pofd_like1* L, int* knobs5) {
     knobs5[1] = t.rfill_per;
     knobs5[2] = t.rnodes_threads;
     knobs5[3] = t.spec_blocks;
-    knobs5[4] = t.rfill_fused;
+    knobs5[4] = t.rfill_mode;
     return POFD_OK;
   });
 }
@@ -548,7 +548,7 @@ int pofd_like1_set_tuning(pofd_like1* L, const int* knobs5) {
     t.rfill_per = knobs5[1];
     t.rnodes_threads = knobs5[2];
     t.spec_blocks = knobs5[3];
-    t.rfill_fused = knobs5[4];
+    t.rfill_mode = knobs5[4];
     L->eng->set_tuning(t);
     return POFD_OK;
   });
@@ -758,6 +758,17 @@ int pofd_like2_pd(pofd_like2* L, int beamset, int dataset, const float* theta,
     const int st = L->eng->pd_host(beamset, dataset, theta, npar, setlog != 0,
                                    pd_out, info16);
     if (st != 0) throw pofd::Error(st, "P(D) unwrap failed (split point or mean)");
+    return POFD_OK;
+  });
+}
+
+int pofd_like1_get_r(pofd_like1* L, int beamset, const float* theta, unsigned npar,
+                     double* out) {
+  return guard([&] {
+    need(L && theta && out, "null argument");
+    need(L->ctx->device >= 0, "host-only context has no GPU");
+    cudaSetDevice(L->ctx->device);
+    L->eng->rgrid_host(beamset, theta, npar, out);
     return POFD_OK;
   });
 }

@@ -449,10 +449,53 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
   }
 }
 
-// R-fill launch with PER grid points per thread (an autotuned knob).
-void launch_rfill(int per, dim3 grid, cudaStream_t st, const BSet1Dev* bsets, int B, int n,
-                  int NI, int nc2, int ntile, const int* mstatus, const double* spl,
+// The R grid materialised by running products: one thread per 16
+// consecutive grid points (GridFill1::segment16), with block partial moment
+// sums (one tile = NT * 16 points).
+__global__ void __launch_bounds__(NT)
+k_rfill1_seg(const BSet1Dev* __restrict__ bsets, int B, int n, int NI, int nc2, int ntile,
+             const int* __restrict__ mstatus, const double* __restrict__ spl,
+             double* __restrict__ rbuf, double* __restrict__ rpart) {
+  __shared__ double shr[32];
+  __shared__ dev::Exp2Table e2;
+  const int wb = blockIdx.y;
+  const int w = wb / B, b = wb - w * B;
+  if (mstatus[w] != 0) return;
+  e2.load();
+  __syncthreads();
+  const BSet1Dev& bs = bsets[b];
+  const GridFill1 rg(bs, spl + static_cast<size_t>(wb) * 2 * 4 * NI, NI, e2.t);
+  double* R = rbuf + static_cast<size_t>(wb) * nc2;
+  const int i0 = (blockIdx.x * NT + threadIdx.x) * 16;
+  double mn = 0.0, var = 0.0;
+  if (i0 + 16 <= n) {
+    double2 o[8];
+    rg.segment16(i0, bs.gidx, o, mn, var, -1, R);
+    double2* R2 = reinterpret_cast<double2*>(R + i0);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) R2[k] = o[k];
+  } else {
+    // the last, partial segment of an n that is not a multiple of 16
+    for (int i = i0; i < n; ++i) R[i] = rg.point(i, static_cast<double>(i), bs.gidx[i], mn, var);
+  }
+  mn = dev::block_sum<NT>(mn, shr);
+  var = dev::block_sum<NT>(var, shr);
+  if (threadIdx.x == 0) {
+    double* o = rpart + (static_cast<size_t>(wb) * ntile + blockIdx.x) * 2;
+    o[0] = mn;
+    o[1] = var;
+  }
+}
+
+// R-fill launch with PER grid points per thread (an autotuned knob), or
+// (seg) by running products over 16-point segments.
+void launch_rfill(int per, bool seg, dim3 grid, cudaStream_t st, const BSet1Dev* bsets, int B,
+                  int n, int NI, int nc2, int ntile, const int* mstatus, const double* spl,
                   double* rbuf, double* rpart) {
+  if (seg) {
+    k_rfill1_seg<<<grid, NT, 0, st>>>(bsets, B, n, NI, nc2, ntile, mstatus, spl, rbuf, rpart);
+    return;
+  }
   switch (per) {
     case 4: k_rfill1<4><<<grid, NT, 0, st>>>(bsets, B, n, NI, nc2, ntile, mstatus, spl, rbuf, rpart); break;
     case 16: k_rfill1<16><<<grid, NT, 0, st>>>(bsets, B, n, NI, nc2, ntile, mstatus, spl, rbuf, rpart); break;
@@ -681,25 +724,8 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
 // wrap - 1, which k_moments1 needs for its edge term, is stored at its place
 // in rbuf -- pass B overwrites rbuf with the spectrum only after
 // k_moments1 has read it.
-//
-// INC: the block first evaluates its whole tile (M1 rows of 2 CB
-// consecutive grid points) in segments of 16 points with
-// GridFill1::segment16 into a shared-memory tile, then reads its DFT
-// inputs from there.  Adjacent lanes take adjacent segments of one row, so
-// their interval-table and spline loads share cache lines.  The tile rows
-// are padded to CB + 4 complex values (consecutive rows 16 banks apart) and
-// the 8 values of segment g are rotated by g within their 8 slots, so that
-// neither the segment stores (lane = (row, segment)) nor the column reads
-// (lane = column) conflict on banks.
-template <int L1, int L2>
-__host__ __device__ constexpr int fftAR_tile() {
-  return (L1 * L2) * (256 / L2 + 4) > 256 * L1 ? (L1 * L2) * (256 / L2 + 4) : 256 * L1;
-}
-__device__ __forceinline__ int fftAR_slot(int b) {
-  return (b & ~7) | (((b & 7) + (b >> 3)) & 7);
-}
 
-template <int L1, int L2, bool INC>
+template <int L1, int L2>
 __global__ void __launch_bounds__(256, 2)
 k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
         const int* __restrict__ mstatus, const double* __restrict__ spl,
@@ -711,11 +737,10 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
   constexpr int m = M1 * M2;
   constexpr int CB = 256 / L2;
   constexpr int NH = m / 128;
-  constexpr int CBP = CB + 4;  // padded tile row (INC)
   extern __shared__ double2 fs[];  // [(n2 * L1 + k1) * CB + b], then H, L
   __shared__ dev::Exp2Table e2;
   __shared__ double shr[32];
-  double2* Hs = fs + (INC ? fftAR_tile<L1, L2>() : 256 * L1);
+  double2* Hs = fs + 256 * L1;
   const double2* Ls = Hs + NH;
   double2* Ts = Hs + NH + 128;  // inter-stage twiddles W_m^{(m / M1) n2 k1}
   const int row = blockIdx.y;
@@ -735,38 +760,18 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
   double2* dst = out + static_cast<size_t>(row) * rowsz;
   double mn = 0.0, var = 0.0;
   double2 v[L1];
-  if (INC) {
-    // the tile in segments of 16 grid points (8 complex inputs): row a of
-    // the m1 x 256 view holds grid indices 2 (a 256 + b0) .. + 2 CB - 1
-    constexpr int SPR = CB / 8;  // segments per tile row
-    for (int sgi = t; sgi < M1 * SPR; sgi += 256) {
-      const int a = sgi / SPR, g = sgi % SPR;
-      double2 o[8];
-      rg.segment16(2 * (a * M2 + b0) + 16 * g, gidx, o, mn, var, iw, Rrow);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) fs[a * CBP + 8 * g + ((k + g) & 7)] = o[k];
-    }
-    __syncthreads();
-  }
   {
     const int b = t % CB, n2 = t / CB;
-    if (INC) {
-      const int sb = fftAR_slot(b);
 #pragma unroll
-      for (int n1 = 0; n1 < L1; ++n1) v[n1] = fs[(L2 * n1 + n2) * CBP + sb];
-      __syncthreads();  // the tile is overwritten by the exchange below
-    } else {
-#pragma unroll
-      for (int n1 = 0; n1 < L1; ++n1) {
-        const int i = 2 * ((L2 * n1 + n2) * M2 + b0 + b);
-        const int2 q = __ldg(reinterpret_cast<const int2*>(gidx + i));
-        const double di = static_cast<double>(i);
-        const double r0 = rg.point(i, di, q.x, mn, var);
-        const double r1 = rg.point(i + 1, di + 1.0, q.y, mn, var);
-        if (i == iw) Rrow[i] = r0;
-        if (i + 1 == iw) Rrow[i + 1] = r1;
-        v[n1] = make_double2(r0, r1);
-      }
+    for (int n1 = 0; n1 < L1; ++n1) {
+      const int i = 2 * ((L2 * n1 + n2) * M2 + b0 + b);
+      const int2 q = __ldg(reinterpret_cast<const int2*>(gidx + i));
+      const double di = static_cast<double>(i);
+      const double r0 = rg.point(i, di, q.x, mn, var);
+      const double r1 = rg.point(i + 1, di + 1.0, q.y, mn, var);
+      if (i == iw) Rrow[i] = r0;
+      if (i + 1 == iw) Rrow[i + 1] = r1;
+      v[n1] = make_double2(r0, r1);
     }
     fft::dft<L1, -1>(v);
     if (L2 > 1) {
@@ -1496,28 +1501,14 @@ void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const in
 #undef POFD_FFTA
 }
 
-// Shared memory of the incremental fused fill: the padded tile replaces
-// the exchange area where it is larger.
-inline size_t fftAR_inc_smem(int m1) {
-  const size_t l1 = m1 < 16 ? m1 : 16, l2 = m1 < 16 ? 1 : m1 / 16;
-  const size_t tile = std::max(static_cast<size_t>(m1) * (256 / l2 + 4), 256 * l1);
-  return (tile + 2 * m1 + 128 + 256) * sizeof(double2);
-}
-// largest at m1 = 256 (tile 256 x 20)
-constexpr size_t kFftARIncSmemMax = (256 * 20 + 2 * 256 + 128 + 256) * sizeof(double2);
-
-// Fused R fill + forward pass A (inc: segment-wise running products);
-// returns the tiles per row (partial moment sums per row in rpart).
+// Fused R fill + forward pass A; returns the tiles per row (partial
+// moment sums per row in rpart).
 int launch_fftAR(int m1, int rows, cudaStream_t st, const BSet1Dev* bsets, int B, int NI,
                  int rowsz, const int* mstatus, const double* spl, double* rbuf, double* rpart,
-                 double2* out, const double2* WH, const double2* WL, bool inc) {
-#define POFD_FFTAR(L1, L2)                                                                  \
-  if (inc)                                                                                  \
-    k_fftAR<L1, L2, true><<<dim3(L2, rows), 256, fftAR_inc_smem(m1), st>>>(                 \
-        bsets, B, NI, rowsz, mstatus, spl, rbuf, rpart, out, WH, WL);                       \
-  else                                                                                      \
-    k_fftAR<L1, L2, false><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(                     \
-        bsets, B, NI, rowsz, mstatus, spl, rbuf, rpart, out, WH, WL);                       \
+                 double2* out, const double2* WH, const double2* WL) {
+#define POFD_FFTAR(L1, L2)                                                                 \
+  k_fftAR<L1, L2><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(bsets, B, NI, rowsz, mstatus, \
+                                                              spl, rbuf, rpart, out, WH, WL); \
   return L2
   switch (m1) {
     case 8: POFD_FFTAR(8, 1);
@@ -1531,19 +1522,14 @@ int launch_fftAR(int m1, int rows, cudaStream_t st, const BSet1Dev* bsets, int B
 #undef POFD_FFTAR
 }
 
-template <bool INC>
-void fftAR_attr_one() {
-  const int sm = static_cast<int>(INC ? std::max(kFftARIncSmemMax, kFftASmemMax) : kFftASmemMax);
-  cuda_check(cudaFuncSetAttribute(k_fftAR<8, 1, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 1, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 4, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 8, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 16, INC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-}
 void fftAR_attr() {
-  fftAR_attr_one<false>();
-  fftAR_attr_one<true>();
+  const int sm = static_cast<int>(kFftASmemMax);
+  cuda_check(cudaFuncSetAttribute(k_fftAR<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
 }
 
 template <int S>
@@ -1950,7 +1936,7 @@ void Engine1::build_static() {
   d_dsets_ = dalloc<DSet1Dev>(D_);
   static_allocs_.push_back(d_dsets_);
   cuda_check(cudaMemcpy(d_dsets_, h_dsets_.data(), D_ * sizeof(DSet1Dev), cudaMemcpyHostToDevice), "upload");
-  ntile_ = (n_ + NT * tune_.rfill_per - 1) / (NT * tune_.rfill_per);
+  ntile_ = (n_ + NT * rfill_points() - 1) / (NT * rfill_points());
   nchunk_ = (n_ + CHUNK - 1) / CHUNK;
   // own FFT: n = 2m, m = m1 * 256 with m1 a power of two in [8, 256]
   own_fft_ = fft_mode_ == 0 && n_ >= 4096 && n_ <= 131072 && (n_ & (n_ - 1)) == 0;
@@ -2052,12 +2038,12 @@ void Engine1::set_tuning(const Tune1& t) {
   if (t.rnodes_threads != 64 && t.rnodes_threads != 128 && t.rnodes_threads != 256)
     throw Error(POFD_E_ARG, "rnodes_threads must be 64, 128 or 256");
   if (t.spec_blocks < 1 || t.spec_blocks > 64) throw Error(POFD_E_ARG, "spec_blocks must be in [1, 64]");
-  if (t.rfill_fused < 0 || t.rfill_fused > 2) throw Error(POFD_E_ARG, "rfill_fused must be 0, 1 or 2");
+  if (t.rfill_mode < 0 || t.rfill_mode > 2) throw Error(POFD_E_ARG, "rfill_mode must be 0, 1 or 2");
   const bool fft_changed = (t.own_fft != 0) != (tune_.own_fft != 0);
   tune_ = t;
   tune_.own_fft = t.own_fft ? 1 : 0;
   if (fft_changed) set_fft_mode(tune_.own_fft ? 0 : 1);  // rebuilds tables, plans, work space
-  if (static_ok_) ntile_ = (n_ + NT * tune_.rfill_per - 1) / (NT * tune_.rfill_per);
+  if (static_ok_) ntile_ = (n_ + NT * rfill_points() - 1) / (NT * rfill_points());
   drop_graphs();
 }
 
@@ -2099,9 +2085,9 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
   }
   if (best.own_fft && own_possible) {
     for (int rf : {0, 1, 2}) {
-      if (rf == best.rfill_fused) continue;
+      if (rf == best.rfill_mode) continue;
       Tune1 t = best;
-      t.rfill_fused = rf;
+      t.rfill_mode = rf;
       trial(t);
     }
   }
@@ -2119,7 +2105,7 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     out7[1] = best.rfill_per;
     out7[2] = best.rnodes_threads;
     out7[3] = best.spec_blocks;
-    out7[4] = best.rfill_fused;
+    out7[4] = best.rfill_mode;
     out7[5] = best_ms;
     out7[6] = t_untuned;
   }
@@ -2370,10 +2356,10 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
     if (fused) {
       // R fill inside the forward pass A: the grid goes straight into tmp
       ntile = launch_fftAR(m1, P * B, st, d_bsets_, B, NI, rowsz, ws_.mstatus, ws_.spl,
-                           ws_.rbuf, ws_.rpart, tmp, d_wh_, d_wl_, tune_.rfill_fused == 2);
+                           ws_.rbuf, ws_.rpart, tmp, d_wh_, d_wl_);
     } else {
       dim3 grid(ntile_, P * B);
-      launch_rfill(tune_.rfill_per, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+      launch_rfill(tune_.rfill_per, tune_.rfill_mode == 2, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
@@ -2402,7 +2388,7 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
   } else {
     {
       dim3 grid(ntile_, P * B);
-      launch_rfill(tune_.rfill_per, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+      launch_rfill(tune_.rfill_per, tune_.rfill_mode == 2, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
@@ -2648,8 +2634,8 @@ void Engine1::rgrid_host(int bs, const float* theta, unsigned npar, double* out)
       d_bsets_, model_, B, NI, maxterms_, ws_.cnt, ws_.mstatus, ws_.nodes);
   k_rspline1<kSplineThreads><<<B * 2, kSplineThreads, (2 * static_cast<size_t>(NI) + 64) * sizeof(double), stream_>>>(
       d_bsets_, B, NI, ws_.mstatus, ws_.nodes, ws_.spl);
-  launch_rfill(tune_.rfill_per, dim3(ntile_, B), stream_, d_bsets_, B, n, NI, nc2,
-               static_cast<int>(ntile_), ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
+  launch_rfill(tune_.rfill_per, tune_.rfill_mode == 2, dim3(ntile_, B), stream_, d_bsets_, B, n,
+               NI, nc2, static_cast<int>(ntile_), ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
   cuda_check(cudaGetLastError(), "rgrid kernels");
   cuda_check(cudaMemcpyAsync(out, ws_.rbuf + static_cast<size_t>(bs) * nc2, n_ * sizeof(double),
                              cudaMemcpyDeviceToHost, stream_), "D2H R grid");

@@ -131,10 +131,11 @@ struct Tune1 {
   int rfill_per = 8;        // R grid points per thread of k_rfill1 (4, 8, 16)
   int rnodes_threads = 128; // threads per block of k_rnodes1 (64, 128, 256)
   int spec_blocks = 8;      // blocks per row of k_spectrum1f (2 ... 32)
-  int rfill_fused = 1;      // R grid fill inside the forward pass A (own
-                            // FFT): 0 no, 1 one exp2
-                            // per grid point, 2 running products over
-                            // segments of 16 points in one node interval
+  int rfill_mode = 1;       // R grid fill: 0 materialised, one exp2 per grid
+                            // point; 1 the same inside the forward FFT pass
+                            // A (own FFT), the grid never stored; 2
+                            // materialised by running products over
+                            // 16-point segments in one node interval
 };
 
 class Engine1 {
@@ -175,7 +176,7 @@ class Engine1 {
   }
   // the R grid fill runs inside the forward FFT pass A (own FFT, plain passes)
   bool fused_fill() const {
-    return own_fft_ && tune_.rfill_fused;
+    return own_fft_ && tune_.rfill_mode == 1;
   }
   // priors (calcLike::setSigmaPrior / setCFIRBPrior / setPoissonPrior /
   // setRegularizationAlpha and their unset forms, calcLike.h:251-269)
@@ -187,10 +188,12 @@ class Engine1 {
   // Times the full launch sequence (graph replays, CUDA events) for the
   // candidate values of each knob in turn on nprop host rows and keeps the
   // fastest; out (optional) receives {own_fft, rfill_per, rnodes_threads,
-  // spec_blocks, rfill_fused, best ms per launch, untuned ms per
+  // spec_blocks, rfill_mode, best ms per launch, untuned ms per
   // launch}.
   void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7);
   const Tune1& tuning() const { return tune_; }
+  // grid points per thread of the materialised R fill
+  int rfill_points() const { return tune_.rfill_mode == 2 ? 16 : tune_.rfill_per; }
   void set_tuning(const Tune1& t);
   // <S>, <S^2> of each proposal's model (calcLike::fillBonusParams,
   // calcLike.cc:958-980): host rows -> out[nprop][2]
