@@ -52,6 +52,8 @@ def args():
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes (skip the autotuner)")
     p.add_argument("--no-mcmc", action="store_true")
+    p.add_argument("--no-sharded", action="store_true",
+                   help="skip the walker-sharded ensemble run (N > 1)")
     p.add_argument("--mcmc-2d", type=int, default=1,
                    help="include the two-field 2D MCMC comparison")
     p.add_argument("--mcmc-steps", type=int, default=1500,
@@ -525,6 +527,44 @@ def _device_ms(fn, reps=50):
     return e0.elapsed_time(e1) / reps
 
 
+def sharded_ensemble(a, ctx, L, cfg, rk):
+    """One 128-walker stretch-move ensemble over the 1D workload's
+    likelihood with each half-step's 64 proposals split over the ranks
+    (shardedLike: each rank its rows, one NCCL all-gather of logL and
+    status), every rank running the same ensemble.  Reports steps/s (the
+    slowest rank's time) and whether the recorded chains are identical on
+    every rank (a checksum reduced with min and max over ranks)."""
+    import torch
+    from pofd_affine_b200.mcmc import affineEnsemble
+    from pofd_affine_b200.shard import shardedLike
+    S = shardedLike(ctx, L)
+    npar = cfg["theta0"].size
+    E = affineEnsemble(ctx, S, 128, npar, seed=123)
+    E.setParamFixed(npar - 1)
+    E.initChains(E.generateInitialPosition(cfg["theta0"], 0.02, rng=7))
+    E.doSteps(0, max(a.warmup, 3))
+    E.sync()
+    rk.barrier()
+    nsteps = 20
+    t0 = time.perf_counter()
+    E.doSteps(nsteps)
+    E.sync()
+    dt = rk.max_over_ranks(time.perf_counter() - t0)
+    ch, cl = E.getChain()
+    h = float(np.sum(ch.astype(np.float64) * np.arange(1, ch.size + 1).reshape(ch.shape))
+              + np.sum(cl))
+    lo = -rk.max_over_ranks(-h)
+    hi = rk.max_over_ranks(h)
+    del E, S
+    torch.cuda.synchronize()
+    return {"workload": "128 walkers on the 1D batched workload, 64 proposals "
+                        "per half-step split over %d ranks" % rk.world,
+            "steps": nsteps, "steps_per_s": nsteps / dt,
+            "evals_per_s": 128 * nsteps / dt,
+            "chains_identical_on_all_ranks": bool(lo == hi),
+            "scaling": "strong (one ensemble)"}
+
+
 def mcmc_1d(ctx):
     """Plain vs delayed-acceptance stretch move on the 1D plain fit (6
     knots, n = 4096, 40 walkers, fixed burn 200, 500 recorded steps), with
@@ -751,6 +791,11 @@ def main():
     nk = L.kernelsPerEval()
 
     extra = {}
+    if world > 1 and not a.no_sharded:
+        # every rank takes part (collectives); rank 0 reports
+        sh = sharded_ensemble(a, ctx, L, cfg, rk)
+        if rank == 0:
+            extra["sharded_ensemble"] = sh
     if rank == 0 and world == 1:
         if not a.no_2d:
             extra["workloads"] = {"2d": measure_2d(a, ctx, stream)}

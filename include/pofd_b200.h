@@ -462,6 +462,35 @@ typedef int (*pofd_batch_loglike_fn)(void* like, unsigned nprop,
                                      const float* theta_dev, unsigned npar,
                                      double* logl_dev, int* status_dev,
                                      void* stream);
+/* ------------------------------------------------------ several GPUs
+ * The batched likelihood split over the ranks (one process per GPU) of one
+ * node; replaces the reference's MPI master/worker farm
+ * (affineEnsemble.cc:1233-1521) for one ensemble.  Every rank runs the same
+ * ensemble (same seed) with a shard as its likelihood: rank r evaluates
+ * rows [P r / W, P (r + 1) / W) of each batch of P proposals with its own
+ * replica inner/inner_like (any pofd_batch_loglike_fn), then one NCCL
+ * all-gather on the caller's stream assembles the whole batch's logL and
+ * status on every rank, so the chains stay identical on every rank and to
+ * a single-GPU run's.  pofd_nccl_unique_id (on one rank, shared with the
+ * others by the caller) and pofd_shard_create (on every rank, concurrently)
+ * set up the communicator; pofd_shard_eval_batch_device has the
+ * pofd_batch_loglike_fn signature (a NULL stream is the context's stream,
+ * as for the likelihoods).  Batch sizes must first be seen outside a stream
+ * capture (buffers are sized then).  NCCL is opened at run time
+ * (libnccl.so.2).  pofd_shard_rows gives rank's rows [lo, hi) of a batch. */
+typedef struct pofd_shard pofd_shard;
+int pofd_shard_rows(unsigned nprop, int world, int rank, unsigned* lo,
+                    unsigned* hi);
+int pofd_nccl_unique_id(unsigned char* id_out /* 128 bytes */);
+int pofd_shard_create(pofd_ctx* ctx, const unsigned char* id, int rank,
+                      int world, pofd_batch_loglike_fn inner, void* inner_like,
+                      pofd_shard** out);
+int pofd_shard_destroy(pofd_shard* s);
+int pofd_shard_eval_batch_device(void* s, unsigned nprop,
+                                 const float* theta_dev, unsigned npar,
+                                 double* logl_dev, int* status_dev,
+                                 void* stream);
+
 /* Bonus-parameter hook: fills the bonus slots of nprop device rows that were
  * just evaluated (the slave's fillBonusParams after getLogLike,
  * affineEnsemble.cc:1490-1493).  Enqueue only, on stream. */

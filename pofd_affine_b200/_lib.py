@@ -166,6 +166,11 @@ SIGNATURES = {
     "pofd_pdfactory2_getpd": (I, [V, D, D, I, _dp, _dp]),
     "pofd_pdfactory2_get_r": (I, [V, _dp]),
     "pofd_acor": (I, [_fp, S, C.POINTER(D), C.POINTER(D), C.POINTER(D)]),
+    "pofd_shard_rows": (I, [U, I, I, C.POINTER(U), C.POINTER(U)]),
+    "pofd_nccl_unique_id": (I, [C.c_char_p]),
+    "pofd_shard_create": (I, [V, C.c_char_p, I, I, V, V, PV]),
+    "pofd_shard_destroy": (I, [V]),
+    "pofd_shard_eval_batch_device": (I, [V, U, V, U, V, V, V]),
 }
 
 # libpofd_b200_support.so (include/pofd_b200_support.h): measurement and

@@ -101,6 +101,8 @@ namespace pofd {
 // Lets entry points outside this file (the allocation-free one) report a
 // message through pofd_last_error().
 void set_last_error(const char* msg) { g_err = msg; }
+int ctx_device(const pofd_ctx* ctx) { return ctx->device; }
+cudaStream_t ctx_stream(const pofd_ctx* ctx) { return ctx->stream; }
 }  // namespace pofd
 
 extern "C" {

@@ -152,7 +152,11 @@ class affineEnsemble:
             fn = C.cast(lib().pofd_likesum_eval_batch_device, C.c_void_p)
             check(lib().pofd_ensemble_set_likelihood(h, fn, like.h))
         else:
-            raise PofdError(-10, "unsupported likelihood object")
+            from .shard import shardedLike
+            if not isinstance(like, shardedLike):
+                raise PofdError(-10, "unsupported likelihood object")
+            fn = C.cast(lib().pofd_shard_eval_batch_device, C.c_void_p)
+            check(lib().pofd_ensemble_set_likelihood(h, fn, like.h))
 
     def __del__(self):
         if getattr(self, "h", None):
