@@ -527,6 +527,73 @@ def _device_ms(fn, reps=50):
     return e0.elapsed_time(e1) / reps
 
 
+def setup_times(ctx, cfg, cfg2=None):
+    """Set-up cost of the data maps: mean subtraction and binning on the
+    host (addDataset from host arrays) against the GPU path (one H2D copy of
+    the pixels, then addDatasetDevice), for the 2000x2000 map of the 1D
+    workload and the 1500x1500 pair of the 2D one; both give identical bins
+    (the GPU tests check that).  Wall-clock seconds, best of three."""
+    import torch
+    from pofd_affine_b200 import beam, calcLike
+    m = np.ascontiguousarray(cfg["maps"][0], np.float64).ravel()
+    pinned = torch.from_numpy(m).pin_memory()
+    b = beam(cfg["beams"][0], cfg["pixsize"], True, cfg["nbeamhist"], 1e-5)
+
+    def fresh():
+        L = calcLike(ctx, cfg["knotpos"], cfg["fftsize"], cfg["ninterp"], True,
+                     cfg["nbins"])
+        L.addBeamSet(b)
+        return L
+    t_host, t_dev = [], []
+    for _ in range(3):
+        L = fresh()
+        t0 = time.perf_counter()
+        L.addDataset(0, m, cfg["sigmas"][0])
+        t_host.append(time.perf_counter() - t0)
+        L = fresh()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d = pinned.to("cuda", non_blocking=True)
+        torch.cuda.synchronize()
+        L.addDatasetDevice(0, d.data_ptr(), d.numel(), cfg["sigmas"][0])
+        t_dev.append(time.perf_counter() - t0)
+    out = {"map_2000x2000": {"host_s": min(t_host), "gpu_s": min(t_dev),
+                             "pixels": int(m.size), "nbins": cfg["nbins"]}}
+    if cfg2 is not None:
+        from pofd_affine_b200.api2d import calcLikeDouble, doublebeam
+        (m1, m2), (s1, s2) = cfg2["maps"][0], cfg2["sigmas"][0]
+        a1 = np.ascontiguousarray(m1, np.float64).ravel()
+        a2 = np.ascontiguousarray(m2, np.float64).ravel()
+        p1, p2 = torch.from_numpy(a1).pin_memory(), torch.from_numpy(a2).pin_memory()
+        bm = doublebeam(cfg2["beam1"], cfg2["beam2"], cfg2["pixsize"], True,
+                        cfg2["nbeamhist"], cfg2["minval"])
+
+        def fresh2():
+            L2 = calcLikeDouble(ctx, cfg2["knotpos"], cfg2["sigmapos"],
+                                cfg2["offsetpos"], cfg2["fftsize"], cfg2["nedge"],
+                                True, cfg2["nbins"])
+            L2.addBeamSet(bm)
+            return L2
+        t_host, t_dev = [], []
+        for _ in range(3):
+            L2 = fresh2()
+            t0 = time.perf_counter()
+            L2.addDataset(0, a1, a2, s1, s2)
+            t_host.append(time.perf_counter() - t0)
+            L2 = fresh2()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            d1 = p1.to("cuda", non_blocking=True)
+            d2 = p2.to("cuda", non_blocking=True)
+            torch.cuda.synchronize()
+            L2.addDatasetDevice(0, d1.data_ptr(), d2.data_ptr(), d1.numel(), s1, s2)
+            t_dev.append(time.perf_counter() - t0)
+        out["pair_1500x1500"] = {"host_s": min(t_host), "gpu_s": min(t_dev),
+                                 "pixels": int(a1.size),
+                                 "nbins": "%dx%d" % (cfg2["nbins"], cfg2["nbins"])}
+    return out
+
+
 def sharded_ensemble(a, ctx, L, cfg, rk):
     """One 128-walker stretch-move ensemble over the 1D workload's
     likelihood with each half-step's 64 proposals split over the ranks
@@ -799,6 +866,8 @@ def main():
     if rank == 0 and world == 1:
         if not a.no_2d:
             extra["workloads"] = {"2d": measure_2d(a, ctx, stream)}
+        from pofd_affine_b200 import synth as _s
+        extra["setup"] = setup_times(ctx, cfg, None if a.no_2d else _s.config_2d())
         if not a.no_mcmc:
             extra["mcmc"] = {"1d": mcmc_1d(ctx)}
             if a.mcmc_2d:

@@ -165,6 +165,22 @@ int pofd_like1_add_beamset(pofd_like1* L, const pofd_beam1* beam,
 int pofd_like1_add_dataset(pofd_like1* L, int beamset, const double* data,
                            size_t ndata, int meansub, double sigma_base,
                            double like_norm);
+/* The same for pixels already in device memory (data_dev[ndata], mean-
+ * subtracted in place when meansub): the mean subtraction and binning run
+ * on the GPU (fitsData::meanSubtract / applyBinning, fitsData.cc:393-437)
+ * with the host path's results bit for bit -- the mean is summed in pixel
+ * order, every bin index rounded as the host rounds it -- and only the bin
+ * counts come back.  An unbinned likelihood copies the pixels back. */
+int pofd_like1_add_dataset_device(pofd_like1* L, int beamset, double* data_dev,
+                                  size_t ndata, int meansub, double sigma_base,
+                                  double like_norm);
+/* The GPU ingestion on its own: optional mean subtraction (in place) and
+ * binning of ndata device values into nbins counts (bins_dev, device);
+ * info3 = {mean (0 without meansub), bincent0, bindelta}.  Synchronises
+ * stream (a cudaStream_t; NULL the legacy default stream). */
+int pofd_data_bin_device(double* data_dev, size_t ndata, int meansub,
+                         unsigned nbins, unsigned* bins_dev, double* info3,
+                         void* stream);
 int pofd_like1_set_rranges(pofd_like1* L, const float* theta, unsigned npar);
 /* range2 = {minRFlux, maxRFlux} of a beam set. */
 int pofd_like1_get_rrange(const pofd_like1* L, int beamset, double* range2);
@@ -295,6 +311,17 @@ int pofd_like2_add_dataset(pofd_like2* L, int beamset, const double* data1,
                            const double* data2, size_t ndata, int meansub,
                            double sigma_base1, double sigma_base2,
                            double like_norm);
+/* Two-band pixels in device memory: the GPU mean subtraction and 2D binning
+ * (fitsDataDouble.cc:557-608) with the host path's results bit for bit. */
+int pofd_like2_add_dataset_device(pofd_like2* L, int beamset, double* d1_dev,
+                                  double* d2_dev, size_t ndata, int meansub,
+                                  double sigma1, double sigma2,
+                                  double like_norm);
+/* The two-band ingestion on its own: counts [nbins1][nbins2] (bins_dev);
+ * info6 = {mean1, mean2, bincent01, bindelta1, bincent02, bindelta2}. */
+int pofd_data2_bin_device(double* d1_dev, double* d2_dev, size_t ndata,
+                          int meansub, unsigned nbins1, unsigned nbins2,
+                          unsigned* bins_dev, double* info6, void* stream);
 /* setRRanges (calcLikeDouble.h:279, calcLikeDouble.cc:496-534). */
 int pofd_like2_set_rranges(pofd_like2* L, const float* theta, unsigned npar);
 /* range4 = {minRFlux1, maxRFlux1, minRFlux2, maxRFlux2} */

@@ -54,6 +54,10 @@ SIGNATURES = {
     "pofd_like1_destroy": (I, [V]),
     "pofd_like1_add_beamset": (I, [V, V, D]),
     "pofd_like1_add_dataset": (I, [V, I, _dp, S, I, D, D]),
+    "pofd_like1_add_dataset_device": (I, [V, I, V, S, I, D, D]),
+    "pofd_data_bin_device": (I, [V, S, I, U, V, _dp, V]),
+    "pofd_data2_bin_device": (I, [V, V, S, I, U, U, V, _dp, V]),
+    "pofd_like2_add_dataset_device": (I, [V, I, V, V, S, I, D, D, D]),
     "pofd_like1_set_rranges": (I, [V, _fp, U]),
     "pofd_like1_get_rrange": (I, [V, I, _dp]),
     "pofd_like1_get_r": (I, [V, I, _fp, U, _dp]),

@@ -189,6 +189,15 @@ class calcLike:
                                            float(like_norm)))
         self.ndatasets[beamset] += 1
 
+    def addDatasetDevice(self, beamset, data_ptr, ndata, sigma_base,
+                         like_norm=1.0, meansub=True):
+        """A dataset whose ndata pixels are in device memory at data_ptr
+        (double; mean-subtracted in place when meansub): mean subtraction
+        and binning on the GPU, bit-identical to addDataset's."""
+        check(lib().pofd_like1_add_dataset_device(
+            self.h, int(beamset), C.c_void_p(int(data_ptr)), int(ndata),
+            int(bool(meansub)), float(sigma_base), float(like_norm)))
+
     def readDataFromArrays(self, datasets, beams, sigmas, like_norms=None,
                            meansub=True, exp_conf=0.0):
         """Group datasets by beam object, as readDataFromFiles groups by

@@ -127,6 +127,17 @@ class calcLikeDouble:
                                            int(meansub), float(sigma1),
                                            float(sigma2), float(like_norm)))
 
+    def addDatasetDevice(self, beamset, d1_ptr, d2_ptr, ndata, sigma1, sigma2,
+                         like_norm=1.0, meansub=True):
+        """A two-band dataset whose ndata pixels per band are in device
+        memory (double; mean-subtracted in place when meansub): mean
+        subtraction and 2D binning on the GPU, bit-identical to
+        addDataset's."""
+        check(lib().pofd_like2_add_dataset_device(
+            self.h, int(beamset), C.c_void_p(int(d1_ptr)), C.c_void_p(int(d2_ptr)),
+            int(ndata), int(bool(meansub)), float(sigma1), float(sigma2),
+            float(like_norm)))
+
     def readDataFromFiles(self, datafiles1, datafiles2, beamfiles1, beamfiles2,
                           sigmas1, sigmas2, like_norms, ignore_mask=False,
                           meansub=False, minbeamval=1e-6, histogram=False,

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUTDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUTDIR, "libpofd_b200.so")
 SOURCES = ["setup.cc", "fits.cc", "engine1d.cu", "engine2d.cu", "ensemble.cu", "surrogate.cu", "capi.cu",
-           "noalloc.cu", "shard.cu"]
+           "noalloc.cu", "shard.cu", "ingest.cu"]
 # measurement and test helpers, kept out of the likelihood's ABI
 SUPPORT_LIB = os.path.join(OUTDIR, "libpofd_b200_support.so")
 SUPPORT_SOURCES = [os.path.join("support", "support.cu")]

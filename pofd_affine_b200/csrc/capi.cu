@@ -381,6 +381,35 @@ int pofd_like1_add_dataset(pofd_like1* L, int beamset, const double* data,
   });
 }
 
+int pofd_like1_add_dataset_device(pofd_like1* L, int beamset, double* data_dev, size_t ndata,
+                                  int meansub, double sigma_base, double like_norm) {
+  return guard([&] {
+    need(L && data_dev, "null argument");
+    L->eng->add_dataset_device(beamset, data_dev, ndata, meansub != 0, sigma_base, like_norm);
+    return POFD_OK;
+  });
+}
+
+int pofd_data_bin_device(double* data_dev, size_t ndata, int meansub, unsigned nbins,
+                         unsigned* bins_dev, double* info3, void* stream) {
+  return guard([&] {
+    need(data_dev && bins_dev && info3, "null argument");
+    pofd::ingest_bin1(data_dev, ndata, meansub != 0, nbins, bins_dev, info3, stream);
+    return POFD_OK;
+  });
+}
+
+int pofd_data2_bin_device(double* d1_dev, double* d2_dev, size_t ndata, int meansub,
+                          unsigned nbins1, unsigned nbins2, unsigned* bins_dev, double* info6,
+                          void* stream) {
+  return guard([&] {
+    need(d1_dev && d2_dev && bins_dev && info6, "null argument");
+    pofd::ingest_bin2(d1_dev, d2_dev, ndata, meansub != 0, nbins1, nbins2, bins_dev, info6,
+                      stream);
+    return POFD_OK;
+  });
+}
+
 int pofd_like1_set_rranges(pofd_like1* L, const float* theta, unsigned npar) {
   return guard([&] {
     need(L && theta, "null argument");
@@ -683,6 +712,16 @@ int pofd_like2_add_dataset(pofd_like2* L, int beamset, const double* d1,
   return guard([&] {
     need(L && d1 && d2, "null argument");
     L->eng->add_dataset(beamset, d1, d2, nd, meansub != 0, sb1, sb2, like_norm);
+    return POFD_OK;
+  });
+}
+
+int pofd_like2_add_dataset_device(pofd_like2* L, int beamset, double* d1_dev, double* d2_dev,
+                                  size_t nd, int meansub, double sb1, double sb2,
+                                  double like_norm) {
+  return guard([&] {
+    need(L && d1_dev && d2_dev, "null argument");
+    L->eng->add_dataset_device(beamset, d1_dev, d2_dev, nd, meansub != 0, sb1, sb2, like_norm);
     return POFD_OK;
   });
 }

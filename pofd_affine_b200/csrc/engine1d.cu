@@ -1600,7 +1600,7 @@ void Engine1::refresh_set(HostSet& s) {
   for (size_t i = 0; i < s.data.size(); ++i) {
     const double var = s.sb[i] * s.sb[i] + s.exp_conf * s.exp_conf;
     if (var > 0) {
-      const double ndd = static_cast<double>(s.data[i].data.size());
+      const double ndd = static_cast<double>(s.data[i].count());
       s.lo[i] = -0.5 * ndd * (std::log(kTwoPi * var) + 1.0);
     }
   }
@@ -1625,6 +1625,51 @@ void Engine1::add_dataset(int bs, const double* data, size_t nd, bool meansub,
   d.data.assign(data, data + nd);
   if (meansub) d.meanSubtract();
   if (bin_data_) d.applyBinning(nbins_);
+  s.data.push_back(std::move(d));
+  s.sb.push_back(sigma_base);
+  s.lo.push_back(0.0);
+  s.ln.push_back(like_norm);
+  refresh_set(s);
+  static_ok_ = false;
+}
+
+// A dataset whose pixels are in device memory: mean subtraction and binning
+// on the GPU (ingest_bin1, bit-identical to the host path), only the counts
+// come back.  Unbinned likelihoods take the (mean-subtracted) pixels back.
+void Engine1::add_dataset_device(int bs, double* data_dev, size_t nd, bool meansub,
+                                 double sigma_base, double like_norm) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size()))
+    throw Error(POFD_E_ARG, "invalid beam set index");
+  if (nd == 0) throw Error(POFD_E_ARG, "No pixels in data");
+  if (device_ < 0) throw Error(POFD_E_CUDA, "host-only context has no GPU");
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  HostSet& s = sets_[bs];
+  Data1 d;
+  if (bin_data_) {
+    unsigned* bins = nullptr;
+    cuda_check(cudaMalloc(&bins, nbins_ * sizeof(unsigned)), "cudaMalloc");
+    double info[3];
+    try {
+      ingest_bin1(data_dev, nd, meansub, nbins_, bins, info, stream_);
+      d.bins.resize(nbins_);
+      cuda_check(cudaMemcpy(d.bins.data(), bins, nbins_ * sizeof(unsigned),
+                            cudaMemcpyDeviceToHost), "D2H bins");
+    } catch (...) {
+      cudaFree(bins);
+      throw;
+    }
+    cudaFree(bins);
+    d.binned = true;
+    d.nbins = nbins_;
+    d.bincent0 = info[1];
+    d.bindelta = info[2];
+    d.npix = nd;
+  } else {
+    d.data.resize(nd);
+    cuda_check(cudaMemcpy(d.data.data(), data_dev, nd * sizeof(double), cudaMemcpyDeviceToHost),
+               "D2H data");
+    if (meansub) d.meanSubtract();
+  }
   s.data.push_back(std::move(d));
   s.sb.push_back(sigma_base);
   s.lo.push_back(0.0);
@@ -1704,7 +1749,7 @@ void Engine1::dataset_info(int bs, int ds, double* o, uint32_t* bins) const {
     throw Error(POFD_E_ARG, "invalid dataset index");
   const Data1& d = s.data[ds];
   if (o) {
-    o[0] = static_cast<double>(d.data.size());
+    o[0] = static_cast<double>(d.count());
     o[1] = d.nbins;
     o[2] = d.bincent0;
     o[3] = d.bindelta;

@@ -150,6 +150,9 @@ class Engine1 {
   int add_beamset(const Beam1& bm, double exp_conf);
   void add_dataset(int bs, const double* data, size_t nd, bool meansub,
                    double sigma_base, double like_norm);
+  // pixels in device memory (mean-subtracted in place when meansub)
+  void add_dataset_device(int bs, double* data_dev, size_t nd, bool meansub,
+                          double sigma_base, double like_norm);
   void set_rranges(const float* theta, unsigned npar);
   void set_rrange_explicit(int bs, double minR, double maxR);
   void add_virtual_dataset(int bs, double sigma_base);

@@ -1616,7 +1616,7 @@ void Engine2::refresh_set(HostSet& s) {
     const double v2 = s.sb2[i] * s.sb2[i] + s.ec2 * s.ec2;
     const double sp = std::sqrt(v1 * v2);
     if (sp > 0) {
-      const double ndd = static_cast<double>(s.data[i].d1.size());
+      const double ndd = static_cast<double>(s.data[i].count());
       s.lo[i] = -ndd * (std::log(kTwoPi * sp) + 1.0);
     }
   }
@@ -1645,6 +1645,55 @@ void Engine2::add_dataset(int bs, const double* d1, const double* d2,
   d.d2.assign(d2, d2 + nd);
   if (meansub) d.meanSubtract();
   if (bin_data_) d.applyBinning(nbins_, nbins_);
+  s.data.push_back(std::move(d));
+  s.sb1.push_back(sigma1);
+  s.sb2.push_back(sigma2);
+  s.lo.push_back(0.0);
+  s.ln.push_back(like_norm);
+  refresh_set(s);
+  static_ok_ = false;
+}
+
+// A two-band dataset whose pixels are in device memory: mean subtraction
+// and binning on the GPU (ingest_bin2, bit-identical to the host path).
+void Engine2::add_dataset_device(int bs, double* d1_dev, double* d2_dev, size_t nd, bool meansub,
+                                 double sigma1, double sigma2, double like_norm) {
+  if (bs < 0 || bs >= static_cast<int>(sets_.size()))
+    throw Error(POFD_E_ARG, "invalid beam set index");
+  if (nd == 0) throw Error(POFD_E_ARG, "No pixels in data");
+  if (device_ < 0) throw Error(POFD_E_CUDA, "host-only context has no GPU");
+  ck(cudaSetDevice(device_), "cudaSetDevice");
+  HostSet& s = sets_[bs];
+  Data2 d;
+  if (bin_data_) {
+    const size_t nb = static_cast<size_t>(nbins_) * nbins_;
+    unsigned* bins = nullptr;
+    ck(cudaMalloc(&bins, nb * sizeof(unsigned)), "cudaMalloc");
+    double info[6];
+    try {
+      ingest_bin2(d1_dev, d2_dev, nd, meansub, nbins_, nbins_, bins, info, stream_);
+      d.bins.resize(nb);
+      ck(cudaMemcpy(d.bins.data(), bins, nb * sizeof(unsigned), cudaMemcpyDeviceToHost),
+         "D2H bins");
+    } catch (...) {
+      cudaFree(bins);
+      throw;
+    }
+    cudaFree(bins);
+    d.binned = true;
+    d.nbins1 = d.nbins2 = nbins_;
+    d.bc1 = info[2];
+    d.bd1 = info[3];
+    d.bc2 = info[4];
+    d.bd2 = info[5];
+    d.npix = nd;
+  } else {
+    d.d1.resize(nd);
+    d.d2.resize(nd);
+    ck(cudaMemcpy(d.d1.data(), d1_dev, nd * sizeof(double), cudaMemcpyDeviceToHost), "D2H data");
+    ck(cudaMemcpy(d.d2.data(), d2_dev, nd * sizeof(double), cudaMemcpyDeviceToHost), "D2H data");
+    if (meansub) d.meanSubtract();
+  }
   s.data.push_back(std::move(d));
   s.sb1.push_back(sigma1);
   s.sb2.push_back(sigma2);
@@ -1732,7 +1781,7 @@ void Engine2::dataset_info(int bs, int ds, double* o, uint32_t* bins) const {
   if (ds < 0 || ds >= static_cast<int>(s.data.size())) throw Error(POFD_E_ARG, "invalid dataset index");
   const Data2& d = s.data[ds];
   if (o) {
-    o[0] = static_cast<double>(d.d1.size()); o[1] = d.nbins1;
+    o[0] = static_cast<double>(d.count()); o[1] = d.nbins1;
     o[2] = d.bc1; o[3] = d.bc2; o[4] = d.bd1; o[5] = d.bd2;
     o[6] = s.lo[ds]; o[7] = s.sb1[ds]; o[8] = s.sb2[ds]; o[9] = s.ln[ds];
   }

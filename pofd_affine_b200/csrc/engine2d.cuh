@@ -117,6 +117,9 @@ class Engine2 {
   void add_dataset(int bs, const double* d1, const double* d2, size_t nd,
                    bool meansub, double sigma1, double sigma2,
                    double like_norm);
+  // pixels in device memory (mean-subtracted in place when meansub)
+  void add_dataset_device(int bs, double* d1_dev, double* d2_dev, size_t nd, bool meansub,
+                          double sigma1, double sigma2, double like_norm);
   void set_rranges(const float* theta, unsigned npar);
   // P(D) factory use: a dataset without pixels whose noise is set per call,
   // and explicit R ranges (PDFactoryDouble::initPD / getPD).

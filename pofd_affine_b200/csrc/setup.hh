@@ -70,7 +70,9 @@ struct SplineSystem {
 
 // Data set: mean-subtracted pixels, binned.
 struct Data1 {
-  std::vector<double> data;
+  std::vector<double> data;  // pixels (may be empty once binned elsewhere)
+  size_t npix = 0;           // pixel count when data is empty
+  size_t count() const { return data.empty() ? npix : data.size(); }
   bool binned = false;
   unsigned nbins = 0;
   std::vector<uint32_t> bins;
@@ -79,6 +81,15 @@ struct Data1 {
   std::pair<double, double> minmax() const;
   void applyBinning(unsigned nbins);
 };
+
+// Mean subtraction and binning of maps in device memory (ingest.cu),
+// bit-identical to Data1 / Data2's: info3 = {mean, bincent0, bindelta},
+// info6 = {mean1, mean2, bincent01, bindelta1, bincent02, bindelta2}.
+// stream: a cudaStream_t.
+void ingest_bin1(double* x_dev, size_t n, bool meansub, unsigned nb, unsigned* bins_dev,
+                 double* info3, void* stream);
+void ingest_bin2(double* x1_dev, double* x2_dev, size_t n, bool meansub, unsigned nb1,
+                 unsigned nb2, unsigned* bins_dev, double* info6, void* stream);
 
 // The wrapped R flux grid of PDFactory::initRFlux (PDFactory.cc:361-414).
 struct RGrid1 {
@@ -135,7 +146,9 @@ struct Beam2 {
 };
 
 struct Data2 {
-  std::vector<double> d1, d2;
+  std::vector<double> d1, d2;  // pixels (may be empty once binned elsewhere)
+  size_t npix = 0;             // pixel count when d1 is empty
+  size_t count() const { return d1.empty() ? npix : d1.size(); }
   unsigned nbins1 = 0, nbins2 = 0;
   std::vector<uint32_t> bins;
   double bc1 = 0, bc2 = 0, bd1 = 0, bd2 = 0;
