@@ -324,43 +324,29 @@ struct GridFill1 {
     return r;
   }
 
-  // R at the 16 consecutive grid indices i0 .. i0 + 15 (i0 a multiple of
-  // 16) into out[0..7] as complex pairs (R_i0 + i R_i0+1, ...), with their
-  // moment terms; R at index iw is also stored to Rrow.  When all 16 points
-  // lie in one node interval of one side, the cubic exponent v(t) of point
-  // i0 + t has constant third differences, so 2^v follows from three running
-  // products: R(t+1) = R(t) E1(t), E1(t+1) = E1(t) E2(t), E2(t+1) = E2(t) E3
-  // with E1(0) = 2^(v(1) - v(0)), E2(0) = 2^(second difference), E3 =
-  // 2^(third difference), the differences taken analytically from the
-  // cubic -- four exp2 per segment instead of sixteen, and no per-point
-  // cubic or table lookup.  The running products add at most ~16^3/6
-  // roundings (< 1e-13 relative) to each value.  Other segments (interval or
-  // side changes, uncovered points) evaluate every point directly.
-  __device__ __forceinline__ void segment16(int i0, const int* __restrict__ gidx, double2* out,
-                                            double& mn, double& var, int iw,
-                                            double* Rrow) const {
-    int q[16];
-    {
-      const int4* g4 = reinterpret_cast<const int4*>(gidx + i0);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int4 g = __ldg(g4 + k);
-        q[4 * k] = g.x;
-        q[4 * k + 1] = g.y;
-        q[4 * k + 2] = g.z;
-        q[4 * k + 3] = g.w;
-      }
-    }
-    bool uni = q[0] >= 0 && (i0 > wrap) == (i0 + 15 > wrap);
-#pragma unroll
-    for (int k = 1; k < 16; ++k) uni = uni && (q[k] == q[0]);
-    if (uni) {
-      const bool neg = i0 > wrap;
-      const double2* S = reinterpret_cast<const double2*>(S0 + (neg ? 4 * NI : 0)) + 2 * q[0];
+  // R at the 16 consecutive grid indices i0 .. i0 + 15 (all below n) into
+  // v[0..15], with their moment terms.  The node interval along each side
+  // is monotone in the grid index, so when both ends of the segment lie in
+  // the same covered interval of the same side, so do all 16 points; then
+  // the cubic exponent v(t) of point i0 + t has constant third differences,
+  // and 2^v follows from three running products: R(t+1) = R(t) E1(t),
+  // E1(t+1) = E1(t) E2(t), E2(t+1) = E2(t) E3 with E1(0) = 2^(v(1) - v(0)),
+  // E2(0) = 2^(second difference), E3 = 2^(third difference), the
+  // differences taken analytically from the cubic -- four exp2 per segment
+  // instead of sixteen, and no per-point cubic or table lookup.  The running
+  // products add at most ~16^3/6 roundings (< 1e-13 relative) to each
+  // value.  Other segments (interval or side changes, uncovered points)
+  // evaluate every point directly.
+  __device__ __forceinline__ void segment16(int i0, const int* __restrict__ gidx, double* v,
+                                            double& mn, double& var) const {
+    const int qa = __ldg(gidx + i0), qb = __ldg(gidx + i0 + 15);
+    const bool neg = i0 > wrap;
+    if (qa >= 0 && qa == qb && neg == (i0 + 15 > wrap)) {
+      const double2* S = reinterpret_cast<const double2*>(S0 + (neg ? 4 * NI : 0)) + 2 * qa;
       const double2 yb = S[0], cd = S[1];
       const double h = dflux;
       const double d0 = __dadd_rn(__dmul_rn(static_cast<double>(i0), dflux), neg ? off1 : off0) -
-                        (neg ? x1 : x0)[q[0]];
+                        (neg ? x1 : x0)[qa];
       const double v0 = yb.x + d0 * (yb.y + d0 * (cd.x + d0 * cd.y));
       const double D1 = h * (yb.y + cd.x * (2.0 * d0 + h) + cd.y * (3.0 * d0 * (d0 + h) + h * h));
       const double D2 = h * h * (2.0 * cd.x + 6.0 * cd.y * (d0 + h));
@@ -371,10 +357,9 @@ struct GridFill1 {
         double R = dev::exp2_tab(v0, e2) * dflux;
         double E1 = dev::exp2_tab(D1, e2), E2 = dev::exp2_tab(D2, e2);
         const double E3 = dev::exp2_tab(D3, e2);
-        double rv[16];
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
-          rv[k] = R;
+          v[k] = R;
           R *= E1;
           E1 *= E2;
           E2 *= E3;
@@ -384,25 +369,18 @@ struct GridFill1 {
           const int i = i0 + k;
           const double cf = neg ? static_cast<double>(i - wrap - 1) * dflux + minflux_R
                                 : __dmul_rn(static_cast<double>(i), dflux);
-          double prod = cf * rv[k];
+          double prod = cf * v[k];
           if (i == wrap) prod *= 0.5;
           mn += prod;
           var += cf * prod;
-          if (i == iw) Rrow[i] = rv[k];
         }
-#pragma unroll
-        for (int k = 0; k < 8; ++k) out[k] = make_double2(rv[2 * k], rv[2 * k + 1]);
         return;
       }
     }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int i = i0 + 2 * k;
-      const double r0 = point(i, static_cast<double>(i), q[2 * k], mn, var);
-      const double r1 = point(i + 1, static_cast<double>(i + 1), q[2 * k + 1], mn, var);
-      if (i == iw) Rrow[i] = r0;
-      if (i + 1 == iw) Rrow[i + 1] = r1;
-      out[k] = make_double2(r0, r1);
+    for (int k = 0; k < 16; ++k) {
+      const int i = i0 + k;
+      v[k] = point(i, static_cast<double>(i), __ldg(gidx + i), mn, var);
     }
   }
 };
@@ -450,12 +428,15 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
 }
 
 // The R grid materialised by running products: one thread per 16
-// consecutive grid points (GridFill1::segment16), with block partial moment
-// sums (one tile = NT * 16 points).
+// consecutive grid points (GridFill1::segment16), the block's 4096 values
+// staged in shared memory (segment stride 9 double2, so that neither the
+// per-thread stores nor the row reads conflict on banks) and written out
+// coalesced; block partial moment sums (one tile = NT * 16 points).
 __global__ void __launch_bounds__(NT)
 k_rfill1_seg(const BSet1Dev* __restrict__ bsets, int B, int n, int NI, int nc2, int ntile,
              const int* __restrict__ mstatus, const double* __restrict__ spl,
              double* __restrict__ rbuf, double* __restrict__ rpart) {
+  __shared__ double2 tile[NT * 9];
   __shared__ double shr[32];
   __shared__ dev::Exp2Table e2;
   const int wb = blockIdx.y;
@@ -466,17 +447,30 @@ k_rfill1_seg(const BSet1Dev* __restrict__ bsets, int B, int n, int NI, int nc2, 
   const BSet1Dev& bs = bsets[b];
   const GridFill1 rg(bs, spl + static_cast<size_t>(wb) * 2 * 4 * NI, NI, e2.t);
   double* R = rbuf + static_cast<size_t>(wb) * nc2;
-  const int i0 = (blockIdx.x * NT + threadIdx.x) * 16;
+  const int base = blockIdx.x * NT * 16;
+  const int i0 = base + threadIdx.x * 16;
   double mn = 0.0, var = 0.0;
+  double v[16];
   if (i0 + 16 <= n) {
-    double2 o[8];
-    rg.segment16(i0, bs.gidx, o, mn, var, -1, R);
-    double2* R2 = reinterpret_cast<double2*>(R + i0);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) R2[k] = o[k];
+    rg.segment16(i0, bs.gidx, v, mn, var);
   } else {
     // the last, partial segment of an n that is not a multiple of 16
-    for (int i = i0; i < n; ++i) R[i] = rg.point(i, static_cast<double>(i), bs.gidx[i], mn, var);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int i = i0 + k;
+      v[k] = (i < n) ? rg.point(i, static_cast<double>(i), bs.gidx[i], mn, var) : 0.0;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) tile[threadIdx.x * 9 + k] = make_double2(v[2 * k], v[2 * k + 1]);
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int p = threadIdx.x + NT * j;  // value pair of the tile
+    const int gi = base + 2 * p;
+    const double2 val = tile[(p >> 3) * 9 + (p & 7)];
+    if (gi + 1 < n) reinterpret_cast<double2*>(R)[gi >> 1] = val;
+    else if (gi < n) R[gi] = val.x;
   }
   mn = dev::block_sum<NT>(mn, shr);
   var = dev::block_sum<NT>(var, shr);

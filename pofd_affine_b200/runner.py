@@ -360,11 +360,18 @@ def _main(argv=None):
     p.add_argument("--pre", type=int, default=300)
     p.add_argument("--burn", type=int, default=None)
     p.add_argument("--da-scale", type=float, default=DA_SCALE_2D)
+    p.add_argument("--save", default=None,
+                   help="write the three chains (every --thin-th step) to this .npz")
+    p.add_argument("--thin", type=int, default=10)
     a = p.parse_args(argv)
     r = compare_two_fields_2d(Context(0), a.steps, a.pre, a.burn, plain_control=True,
                               da_scale=a.da_scale)
     summ = summarise(r)
     summ.update(steps=a.steps, pre=a.pre, burn=a.burn)
+    if a.save:
+        np.savez_compressed(a.save, **{
+            "%s_%s" % (k, f): r[k][f][::a.thin]
+            for k in ("plain", "da", "plain_control") for f in ("chain", "logl")})
     print(json.dumps(summ))
 
 
