@@ -271,21 +271,10 @@ k_rows2(const BSet2Dev* __restrict__ bsets, Model2Dev m, int B,
   if (lane == 0) rcnt[static_cast<size_t>(wb) * bs.nrows + r] = make_int2(npos, nneg);
 }
 
-// R(f1 row, f2 column j) from a row's compacted term lists
-// (numberCountsDoubleLogNormal.cc:1972-2002): (sum_k c0 2^{(log|f2| - c1)^2
-// c2}) / |f2|, over the list of column j's band-2 sign.
-__device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
-                                       const double* __restrict__ row, int2 nt, int j,
-                                       const double* tab) {
-  if (sgn1 < 0) return 0.0;
-  const double if2 = bs.colinv[j];
-  if (if2 == 0) return 0.0;
-  const int fs = bs.colsgn[j];
-  if (!bs.hassign[sgn1 + fs]) return 0.0;
-  const double* L = fs ? row + 3 * nt.x : row;
-  const int cnt = fs ? nt.y : nt.x;
-  const double lf2 = bs.collog[j];
-  // two partial sums over alternate terms: independent exp2 chains overlap
+// Sum over a row's compacted term list L[cnt] at column log-flux lf2 (two
+// partial sums over alternate terms: independent exp2 chains overlap).
+__device__ __forceinline__ double term_sum(const double* __restrict__ L, int cnt, double lf2,
+                                           const double* tab) {
   double wa = 0.0, wb = 0.0;
   int k = 0;
 #pragma unroll 2
@@ -299,12 +288,28 @@ __device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
     const double ta = lf2 - __ldg(L + 3 * k + 1);
     wa += __ldg(L + 3 * k) * dev::exp2_tab(ta * ta * __ldg(L + 3 * k + 2), tab);
   }
-  return (wa + wb) * if2;
+  return wa + wb;
+}
+
+// R(f1 row, f2 column j) from a row's compacted term lists
+// (numberCountsDoubleLogNormal.cc:1972-2002): (sum_k c0 2^{(log|f2| - c1)^2
+// c2}) / |f2|, over the list of column j's band-2 sign.
+__device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
+                                       const double* __restrict__ row, int2 nt, int j,
+                                       const double* tab) {
+  if (sgn1 < 0) return 0.0;
+  const double if2 = bs.colinv[j];
+  if (if2 == 0) return 0.0;
+  const int fs = bs.colsgn[j];
+  if (!bs.hassign[sgn1 + fs]) return 0.0;
+  return term_sum(fs ? row + 3 * nt.x : row, fs ? nt.y : nt.x, bs.collog[j], tab) * if2;
 }
 
 // Main R grid, rows 1..n-1 x columns 1..n-1 (row 0 and column 0 are the
 // edge cells), times dflux1*dflux2, with block partial sums of the
-// trapezoid moments of getRStats (PDFactoryDouble.cc:593-722).
+// trapezoid moments of getRStats (PDFactoryDouble.cc:593-722).  Each thread
+// owns one column for RB rows: the column's flux constants are read once,
+// each row's sign, term counts and terms are the same for the whole block.
 template <int RB>
 __global__ void __launch_bounds__(NT)
 k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
@@ -319,20 +324,38 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
   e2.load();
   __syncthreads();
   const BSet2Dev& bs = bsets[b];
+  const int nrows = bs.nrows, ts3 = 3 * bs.Ts;
+  const int* __restrict__ rowsgn = bs.rowsgn;
+  const double* __restrict__ rowflux = bs.rowflux;
   const int j = blockIdx.x * NT + threadIdx.x;
+  const bool jin = (j >= 1 && j < n);
+  double if2 = 0.0, lf2 = 0.0, cf2 = 0.0;
+  int fs = 0;
+  if (jin) {
+    if2 = bs.colinv[j];
+    lf2 = bs.collog[j];
+    fs = bs.colsgn[j];
+    cf2 = bs.rflux2[j];
+  }
+  const unsigned hsm = (bs.hassign[0] ? 1u : 0u) | (bs.hassign[1] ? 2u : 0u) |
+                       (bs.hassign[2] ? 4u : 0u) | (bs.hassign[3] ? 8u : 0u);
   const double fluxfac = bs.dflux1 * bs.dflux2;
-  const double cf2 = (j < n) ? bs.rflux2[j] : 0.0;
   const double wc = (j == n - 1) ? 0.5 : 1.0;
   double m1 = 0.0, v1 = 0.0, m2 = 0.0, v2 = 0.0;
   for (int rr = 0; rr < RB; ++rr) {
     const int r = 1 + blockIdx.y * RB + rr;
     if (r >= n) break;
-    const int sgn1 = bs.rowsgn[r];
-    const size_t ri = static_cast<size_t>(wb) * bs.nrows + r;
-    if (j >= 1 && j < n) {
-      const double R = r_at(bs, sgn1, rw + ri * bs.Ts * 3, rcnt[ri], j, e2.t) * fluxfac;
+    const int sgn1 = rowsgn[r];
+    const size_t ri = static_cast<size_t>(wb) * nrows + r;
+    if (jin) {
+      double R = 0.0;
+      if (sgn1 >= 0 && if2 != 0.0 && ((hsm >> (sgn1 + fs)) & 1u)) {
+        const int2 nt = rcnt[ri];
+        const double* L = rw + ri * ts3 + (fs ? 3 * nt.x : 0);
+        R = term_sum(L, fs ? nt.y : nt.x, lf2, e2.t) * if2 * fluxfac;
+      }
       rbuf[(static_cast<size_t>(wb) * n + r) * nc2 + j] = R;
-      const double cf1 = bs.rowflux[r];
+      const double cf1 = rowflux[r];
       const double cR = (r == n - 1) ? 0.5 * R : R;
       const double p1 = wc * cf1 * cR;
       const double p2 = wc * cf2 * cR;
@@ -372,16 +395,29 @@ k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   __syncthreads();
   const BSet2Dev& bs = bsets[b];
   const int ncol = n + nedge;
+  const int nrows = bs.nrows, ts3 = 3 * bs.Ts;
   const int j = blockIdx.x * NT + threadIdx.x;
+  const bool jin = j < ncol;
+  double if2 = 0.0, lf2 = 0.0;
+  int fs = 0;
+  if (jin) {
+    if2 = bs.colinv[j];
+    lf2 = bs.collog[j];
+    fs = bs.colsgn[j];
+  }
+  const unsigned hsm = (bs.hassign[0] ? 1u : 0u) | (bs.hassign[1] ? 2u : 0u) |
+                       (bs.hassign[2] ? 4u : 0u) | (bs.hassign[3] ? 8u : 0u);
   double acc = 0.0;
   for (int rr = 0; rr < ER; ++rr) {
     const int i = blockIdx.y * ER + rr;
     if (i >= nedge) break;
     const int r = n + i;
     const int sgn1 = bs.rowsgn[r];
-    const size_t ri = static_cast<size_t>(wb) * bs.nrows + r;
-    if (j < ncol) {
-      const double R = r_at(bs, sgn1, rw + ri * bs.Ts * 3, rcnt[ri], j, e2.t);
+    if (jin && sgn1 >= 0 && if2 != 0.0 && ((hsm >> (sgn1 + fs)) & 1u)) {
+      const size_t ri = static_cast<size_t>(wb) * nrows + r;
+      const int2 nt = rcnt[ri];
+      const double* L = rw + ri * ts3 + (fs ? 3 * nt.x : 0);
+      const double R = term_sum(L, fs ? nt.y : nt.x, lf2, e2.t) * if2;
       const double rf = bs.e1[i];
       acc += ((i == 0 || i == nedge - 1) ? 0.5 : 1.0) * rf * R;
     }
