@@ -240,7 +240,7 @@ def reference_arm(a, cfg):
     cpu = os.cpu_count() or 1
     from pofd_affine_b200 import synth
     O = _oracle1(cfg)
-    per_step = 2 * cpu  # bounded sample per step
+    per_step = BATCH  # the GPU arm's launch: ~0.1 s of host work per step
     th = synth.proposals(cfg["theta0"], per_step, 0.02, rng=99)
     for _ in range(a.warmup):
         O.loglike_batch(th, cpu)
@@ -255,7 +255,10 @@ def reference_arm(a, cfg):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD,
-                       "proposals_per_step": per_step},
+                       "proposals_per_step": per_step,
+                       "fftsize": cfg["fftsize"],
+                       "beam_sets": len(cfg["beams"]),
+                       "datasets": len(cfg["maps"])},
             "cpu_baseline": {"value": v, "unit": "evals/s", "cores": cpu,
                              "kind": "port",
                              "fft": CPU_FFT,
@@ -632,7 +635,7 @@ def sharded_ensemble(a, ctx, L, cfg, rk):
             "scaling": "strong (one ensemble)"}
 
 
-def mcmc_1d(ctx):
+def mcmc_1d(ctx, cpu=True):
     """Plain vs delayed-acceptance stretch move on the 1D plain fit (6
     knots, n = 4096, 40 walkers, fixed burn 200, 500 recorded steps), with
     the cost of one half-ensemble's exact likelihood and of its surrogate
@@ -677,7 +680,84 @@ def mcmc_1d(ctx):
         S.h, 20, C.c_void_p(th.data_ptr()), npar, C.c_void_p(ll.data_ptr()),
         C.c_void_p(st.data_ptr()), C.c_void_p(sp)))
     out["half_step_ms"] = {"exact_20": exact_ms, "surrogate_20": sur_ms}
+    if cpu:
+        c = cpu_mcmc_1d()
+        c["gpu_plain_ess_per_s_ratio"] = out["plain"]["ess_per_s"] / c["ess_per_s"]
+        out["cpu_plain"] = c
     return out
+
+
+def cpu_mcmc_1d(nthreads=None, nburn=200, nsteps=500, nwalkers=40):
+    """The plain stretch move of mcmc_1d on the host: the oracle's sampler
+    (the same Philox draws and acceptance rule as the GPU ensemble) over the
+    oracle port's likelihood, each half-ensemble's proposals farmed over
+    nthreads host threads (the reference's master/worker farm), the same
+    walkers, limits, burn-in and recorded steps as the GPU plain run, ESS
+    from the same estimator.  Reported twice: over the whole wall time, and
+    over the time spent inside the likelihood calls only (the share a
+    compiled sampler could not avoid)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sampler_oracle as so
+    from pofd_affine_b200 import synth
+    from pofd_affine_b200.mcmc import integrated_time
+    nthreads = nthreads or os.cpu_count() or 1
+    cfg = synth.config_1d_small(seed=1)
+    O = _oracle1(cfg)
+    th0 = np.asarray(cfg["theta0"], np.float32)
+    npar = th0.size
+    nk = npar - 1
+    state = np.zeros(npar, int)
+    state[nk] = so.FIXED
+    lo = np.full(npar, -np.inf, np.float32)
+    hi = np.full(npar, np.inf, np.float32)
+    lo[:nk], hi[:nk] = th0[:nk] - 2.0, th0[:nk] + 2.0
+    # the walkers of affineEnsemble.generateInitialPosition(theta0, 0.05,
+    # rng=21): the same draws in the same order
+    rng = np.random.default_rng(21)
+    w = np.empty((nwalkers, npar), np.float32)
+    for k in range(nwalkers):
+        for p in range(npar):
+            if state[p] & so.FIXED:
+                w[k, p] = th0[p]
+                continue
+            while True:
+                v = np.float32(th0[p] + 0.05 * rng.standard_normal())
+                if lo[p] <= v <= hi[p]:
+                    break
+            w[k, p] = v
+    t_like = [0.0]
+
+    def like(th):
+        t = time.perf_counter()
+        r = O.loglike_batch(np.ascontiguousarray(th, np.float32), nthreads)
+        t_like[0] += time.perf_counter() - t
+        return r
+
+    like(w[:nthreads])  # builds the thread copies (untimed)
+    t_like[0] = 0.0
+    t0 = time.perf_counter()
+    ll, st = like(w)
+    ch, cl, _ = so.stretch_run(w, ll, like, nburn, 21, state=state, lo=lo,
+                               hi=hi)
+    ch, cl, nacc = so.stretch_run(ch[-1], cl[-1], like, nsteps, 21,
+                                  state=state, lo=lo, hi=hi, step0=nburn)
+    wall = time.perf_counter() - t0
+    tau, _, conv = integrated_time(ch)
+    tau[nk] = np.nan
+    tmax = float(np.nanmax(tau))
+    ess = nwalkers * nsteps / tmax
+    return {"workload": "the 1D plain fit of mcmc_1d on the host: %d walkers, "
+                        "burn %d, %d recorded steps" % (nwalkers, nburn, nsteps),
+            "kind": "port", "cores": nthreads,
+            "sample": "oracle sampler (Python) over the oracle port's "
+                      "likelihood with a %s, each half-ensemble farmed over "
+                      "%d threads" % (CPU_FFT, nthreads),
+            "wall_s": wall, "likelihood_s": t_like[0],
+            "evals": nwalkers * (nburn + nsteps + 1),
+            "tau_max": tmax, "tau_converged": bool(np.all(conv[:nk])),
+            "acceptance": float(np.mean(nacc)) / nsteps,
+            "ess": ess, "ess_per_s": ess / wall,
+            "ess_per_s_likelihood_only": ess / t_like[0]}
 
 
 def mcmc_2d(ctx, nsteps=1500):
@@ -869,7 +949,7 @@ def main():
         from pofd_affine_b200 import synth as _s
         extra["setup"] = setup_times(ctx, cfg, None if a.no_2d else _s.config_2d())
         if not a.no_mcmc:
-            extra["mcmc"] = {"1d": mcmc_1d(ctx)}
+            extra["mcmc"] = {"1d": mcmc_1d(ctx, cpu=not a.no_cpu_baseline)}
             if a.mcmc_2d:
                 extra["mcmc"]["2d_two_fields"] = mcmc_2d(ctx, a.mcmc_steps)
 

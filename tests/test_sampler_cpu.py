@@ -85,3 +85,16 @@ def test_integrated_time_on_ar1_ensembles(rho):
     assert conv[0] and abs(tau[0] / exact - 1) < 0.1, (tau[0], exact)
     assert np.isnan(tau[1])
     assert win[0] >= 5 * tau[0]
+
+
+def test_host_mcmc_baseline_runs():
+    """The host plain-method baseline of the benchmark (oracle sampler over
+    the oracle likelihood, thread farm) on a short chain of the 1D plain
+    fit: every walker moves, the chain stays inside the knot limits and the
+    effective-sample bookkeeping is finite."""
+    import bench
+    r = bench.cpu_mcmc_1d(nthreads=2, nburn=5, nsteps=20, nwalkers=8)
+    assert r["evals"] == 8 * 26
+    assert 0.05 < r["acceptance"] < 0.95
+    assert np.isfinite(r["tau_max"]) and r["ess"] > 0
+    assert 0 < r["likelihood_s"] <= r["wall_s"]
