@@ -324,65 +324,60 @@ struct GridFill1 {
     return r;
   }
 
-  // R at the 16 consecutive grid indices i0 .. i0 + 15 (all below n) into
-  // v[0..15], with their moment terms.  The node interval along each side
-  // is monotone in the grid index, so when both ends of the segment lie in
-  // the same covered interval of the same side, so do all 16 points; then
-  // the cubic exponent v(t) of point i0 + t has constant third differences,
-  // and 2^v follows from three running products: R(t+1) = R(t) E1(t),
-  // E1(t+1) = E1(t) E2(t), E2(t+1) = E2(t) E3 with E1(0) = 2^(v(1) - v(0)),
-  // E2(0) = 2^(second difference), E3 = 2^(third difference), the
-  // differences taken analytically from the cubic -- four exp2 per segment
-  // instead of sixteen, and no per-point cubic or table lookup.  The running
-  // products add at most ~16^3/6 roundings (< 1e-13 relative) to each
-  // value.  Other segments (interval or side changes, uncovered points)
-  // evaluate every point directly.
-  __device__ __forceinline__ void segment16(int i0, const int* __restrict__ gidx, double* v,
-                                            double& mn, double& var) const {
-    const int qa = __ldg(gidx + i0), qb = __ldg(gidx + i0 + 15);
+  // R at the len (<= 16) consecutive grid indices of one run (i0, q) --
+  // points of one covered node interval q on one side of the wrap -- into
+  // the shared tile at out[pad(o + k)], with their moment terms.  The cubic
+  // exponent v(t) of point i0 + t has constant third differences, so 2^v
+  // follows from three running products: R(t+1) = R(t) E1(t), E1(t+1) =
+  // E1(t) E2(t), E2(t+1) = E2(t) E3, with E1(0) = 2^(v(1) - v(0)), E2(0) =
+  // 2^(second difference), E3 = 2^(third difference), the differences taken
+  // analytically from the cubic: four exp2 per run instead of one per
+  // point, and no per-point cubic or table lookup.  The products add at
+  // most ~16^3/6 roundings (< 1e-13 relative) to each value.  A run whose
+  // exponents leave the safe range goes point by point.
+  __device__ __forceinline__ void run_products(int i0, int len, int q, double* out, int o,
+                                               double& mn, double& var) const {
     const bool neg = i0 > wrap;
-    if (qa >= 0 && qa == qb && neg == (i0 + 15 > wrap)) {
-      const double2* S = reinterpret_cast<const double2*>(S0 + (neg ? 4 * NI : 0)) + 2 * qa;
-      const double2 yb = S[0], cd = S[1];
-      const double h = dflux;
-      const double d0 = __dadd_rn(__dmul_rn(static_cast<double>(i0), dflux), neg ? off1 : off0) -
-                        (neg ? x1 : x0)[qa];
-      const double v0 = yb.x + d0 * (yb.y + d0 * (cd.x + d0 * cd.y));
-      const double D1 = h * (yb.y + cd.x * (2.0 * d0 + h) + cd.y * (3.0 * d0 * (d0 + h) + h * h));
-      const double D2 = h * h * (2.0 * cd.x + 6.0 * cd.y * (d0 + h));
-      const double D3 = 6.0 * cd.y * h * h * h;
-      // (exponents far outside the P(D) range go point by point, as does a
-      // segment whose values would leave the double range)
-      if (fabs(v0) < 500.0 && fabs(D1) < 16.0 && fabs(D2) < 4.0 && fabs(D3) < 2.0) {
-        double R = dev::exp2_tab(v0, e2) * dflux;
-        double E1 = dev::exp2_tab(D1, e2), E2 = dev::exp2_tab(D2, e2);
-        const double E3 = dev::exp2_tab(D3, e2);
+    const double2* S = reinterpret_cast<const double2*>(S0 + (neg ? 4 * NI : 0)) + 2 * q;
+    const double2 yb = S[0], cd = S[1];
+    const double h = dflux;
+    const double d0 = __dadd_rn(__dmul_rn(static_cast<double>(i0), dflux), neg ? off1 : off0) -
+                      (neg ? x1 : x0)[q];
+    const double v0 = yb.x + d0 * (yb.y + d0 * (cd.x + d0 * cd.y));
+    const double D1 = h * (yb.y + cd.x * (2.0 * d0 + h) + cd.y * (3.0 * d0 * (d0 + h) + h * h));
+    const double D2 = h * h * (2.0 * cd.x + 6.0 * cd.y * (d0 + h));
+    const double D3 = 6.0 * cd.y * h * h * h;
+    if (fabs(v0) < 500.0 && fabs(D1) < 16.0 && fabs(D2) < 4.0 && fabs(D3) < 2.0) {
+      double R = dev::exp2_tab(v0, e2) * dflux;
+      double E1 = dev::exp2_tab(D1, e2), E2 = dev::exp2_tab(D2, e2);
+      const double E3 = dev::exp2_tab(D3, e2);
+      const double cb = neg ? minflux_R : 0.0;
+      const int ib = neg ? wrap + 1 : 0;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          v[k] = R;
-          R *= E1;
-          E1 *= E2;
-          E2 *= E3;
-        }
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          const int i = i0 + k;
-          const double cf = neg ? static_cast<double>(i - wrap - 1) * dflux + minflux_R
-                                : __dmul_rn(static_cast<double>(i), dflux);
-          double prod = cf * v[k];
-          if (i == wrap) prod *= 0.5;
-          mn += prod;
-          var += cf * prod;
-        }
-        return;
+      for (int k = 0; k < 16; ++k) {
+        if (k >= len) break;
+        const int i = i0 + k;
+        out[pad(o + k)] = R;
+        const double cf = neg ? static_cast<double>(i - ib) * dflux + cb
+                              : __dmul_rn(static_cast<double>(i), dflux);
+        double prod = cf * R;
+        if (i == wrap) prod *= 0.5;
+        mn += prod;
+        var += cf * prod;
+        R *= E1;
+        E1 *= E2;
+        E2 *= E3;
       }
+      return;
     }
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
+    for (int k = 0; k < len; ++k) {
       const int i = i0 + k;
-      v[k] = point(i, static_cast<double>(i), __ldg(gidx + i), mn, var);
+      out[pad(o + k)] = point(i, static_cast<double>(i), q, mn, var);
     }
   }
+  // shared tile index of span offset j: one pad word per 16 values, so that
+  // threads starting runs ~16 values apart do not share a bank
+  __device__ __forceinline__ static int pad(int j) { return j + (j >> 4); }
 };
 
 // The R grid materialised (cuFFT path, and the own path when the fill is
@@ -427,16 +422,22 @@ k_rfill1(const BSet1Dev* __restrict__ bsets, int B, int n, int NI,
   }
 }
 
-// The R grid materialised by running products: one thread per 16
-// consecutive grid points (GridFill1::segment16), the block's 4096 values
-// staged in shared memory (segment stride 9 double2, so that neither the
-// per-thread stores nor the row reads conflict on banks) and written out
-// coalesced; block partial moment sums (one tile = NT * 16 points).
+// The R grid materialised by running products over static runs (mode 2):
+// each beam set's grid is cut, at set-up, into runs of at most 16
+// consecutive points that share one node interval and one side of the wrap
+// (bs.runs: x = first index, y = (q + 1) << 8 | len << 2 | kind; kind 0:
+// uncovered, R = 0; 1: shorter than four points, evaluated point by point;
+// 2: running products, GridFill1::run_products).  Block k takes runs
+// [k NT, k NT + NT) of its row -- one per thread, so no thread's run crosses
+// an interval and warps do not diverge on interval changes -- stages their
+// contiguous span of the grid (at most 16 NT values) in shared memory and
+// writes it out coalesced; block partial moment sums (zero for blocks past
+// the row's runs).
 __global__ void __launch_bounds__(NT)
-k_rfill1_seg(const BSet1Dev* __restrict__ bsets, int B, int n, int NI, int nc2, int ntile,
+k_rfill1_run(const BSet1Dev* __restrict__ bsets, int B, int NI, int nc2, int ntile,
              const int* __restrict__ mstatus, const double* __restrict__ spl,
              double* __restrict__ rbuf, double* __restrict__ rpart) {
-  __shared__ double2 tile[NT * 9];
+  __shared__ double tile[NT * 17];
   __shared__ double shr[32];
   __shared__ dev::Exp2Table e2;
   const int wb = blockIdx.y;
@@ -445,32 +446,33 @@ k_rfill1_seg(const BSet1Dev* __restrict__ bsets, int B, int n, int NI, int nc2, 
   e2.load();
   __syncthreads();
   const BSet1Dev& bs = bsets[b];
-  const GridFill1 rg(bs, spl + static_cast<size_t>(wb) * 2 * 4 * NI, NI, e2.t);
-  double* R = rbuf + static_cast<size_t>(wb) * nc2;
-  const int base = blockIdx.x * NT * 16;
-  const int i0 = base + threadIdx.x * 16;
+  const int r0 = blockIdx.x * NT;
   double mn = 0.0, var = 0.0;
-  double v[16];
-  if (i0 + 16 <= n) {
-    rg.segment16(i0, bs.gidx, v, mn, var);
-  } else {
-    // the last, partial segment of an n that is not a multiple of 16
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const int i = i0 + k;
-      v[k] = (i < n) ? rg.point(i, static_cast<double>(i), bs.gidx[i], mn, var) : 0.0;
+  if (r0 < bs.nruns) {
+    const GridFill1 rg(bs, spl + static_cast<size_t>(wb) * 2 * 4 * NI, NI, e2.t);
+    const int r1 = min(r0 + NT, bs.nruns);
+    const int span0 = __ldg(&bs.runs[r0].x);
+    const int2 last = __ldg(&bs.runs[r1 - 1]);
+    const int span = last.x + ((last.y >> 2) & 31) - span0;
+    const int r = r0 + threadIdx.x;
+    if (r < r1) {
+      const int2 d = __ldg(&bs.runs[r]);
+      const int len = (d.y >> 2) & 31, kind = d.y & 3, q = (d.y >> 8) - 1;
+      const int o = d.x - span0;
+      if (kind == 2) {
+        rg.run_products(d.x, len, q, tile, o, mn, var);
+      } else if (kind == 1) {
+        for (int k = 0; k < len; ++k) {
+          const int i = d.x + k;
+          tile[GridFill1::pad(o + k)] = rg.point(i, static_cast<double>(i), q, mn, var);
+        }
+      } else {
+        for (int k = 0; k < len; ++k) tile[GridFill1::pad(o + k)] = 0.0;
+      }
     }
-  }
-#pragma unroll
-  for (int k = 0; k < 8; ++k) tile[threadIdx.x * 9 + k] = make_double2(v[2 * k], v[2 * k + 1]);
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int p = threadIdx.x + NT * j;  // value pair of the tile
-    const int gi = base + 2 * p;
-    const double2 val = tile[(p >> 3) * 9 + (p & 7)];
-    if (gi + 1 < n) reinterpret_cast<double2*>(R)[gi >> 1] = val;
-    else if (gi < n) R[gi] = val.x;
+    __syncthreads();
+    double* R = rbuf + static_cast<size_t>(wb) * nc2 + span0;
+    for (int j = threadIdx.x; j < span; j += NT) R[j] = tile[GridFill1::pad(j)];
   }
   mn = dev::block_sum<NT>(mn, shr);
   var = dev::block_sum<NT>(var, shr);
@@ -482,12 +484,12 @@ k_rfill1_seg(const BSet1Dev* __restrict__ bsets, int B, int n, int NI, int nc2, 
 }
 
 // R-fill launch with PER grid points per thread (an autotuned knob), or
-// (seg) by running products over 16-point segments.
+// (seg) by running products over the static runs.
 void launch_rfill(int per, bool seg, dim3 grid, cudaStream_t st, const BSet1Dev* bsets, int B,
                   int n, int NI, int nc2, int ntile, const int* mstatus, const double* spl,
                   double* rbuf, double* rpart) {
   if (seg) {
-    k_rfill1_seg<<<grid, NT, 0, st>>>(bsets, B, n, NI, nc2, ntile, mstatus, spl, rbuf, rpart);
+    k_rfill1_run<<<grid, NT, 0, st>>>(bsets, B, NI, nc2, ntile, mstatus, spl, rbuf, rpart);
     return;
   }
   switch (per) {
@@ -1766,11 +1768,17 @@ void Engine1::free_static() {
 
 // Upload the parameter-independent data: beam terms, interpolation nodes
 // and their spline factorisation, grid ranges, binned data.
+unsigned Engine1::fill_tiles() const {
+  const unsigned pts = NT * static_cast<unsigned>(tune_.rfill_per);
+  return tune_.rfill_mode == 2 ? runblk_ : (n_ + pts - 1) / pts;
+}
+
 void Engine1::build_static() {
   if (device_ < 0) throw Error(POFD_E_CUDA, "host-only context has no GPU");
   cuda_check(cudaSetDevice(device_), "cudaSetDevice");
   free_static();
   if (sets_.empty()) throw Error(POFD_E_ARG, "no beam sets");
+  runblk_ = 0;
   auto up = [&](const std::vector<double>& v) -> const double* {
     double* p = dalloc<double>(v.size() ? v.size() : 1);
     static_allocs_.push_back(p);
@@ -1938,6 +1946,28 @@ void Engine1::build_static() {
       }
     }
     bd.gidx = upi(gidx);
+    {
+      // runs for the running-product fill: cut at interval and side
+      // changes and after 16 points
+      std::vector<int> runs;
+      const int wrap = static_cast<int>(g.wrapRidx);
+      const int n = static_cast<int>(n_);
+      for (int i = 0; i < n;) {
+        const int q = gidx[i];
+        const bool neg = i > wrap;
+        int j = i + 1;
+        while (j < n && j - i < 16 && gidx[j] == q && (j > wrap) == neg) ++j;
+        const int len = j - i;
+        const int kind = q < 0 ? 0 : (len >= 4 ? 2 : 1);
+        runs.push_back(i);
+        runs.push_back(((q + 1) << 8) | (len << 2) | kind);
+        i = j;
+      }
+      bd.nruns = static_cast<int>(runs.size() / 2);
+      bd.runs = reinterpret_cast<const int2*>(upi(runs));
+      const unsigned nb = (static_cast<unsigned>(bd.nruns) + NT - 1) / NT;
+      if (nb > runblk_) runblk_ = nb;
+    }
     bd.ds_begin = static_cast<int>(h_dsets_.size());
     bd.nds = static_cast<int>(s.data.size());
     for (size_t i = 0; i < s.data.size(); ++i) {
@@ -1975,7 +2005,7 @@ void Engine1::build_static() {
   d_dsets_ = dalloc<DSet1Dev>(D_);
   static_allocs_.push_back(d_dsets_);
   cuda_check(cudaMemcpy(d_dsets_, h_dsets_.data(), D_ * sizeof(DSet1Dev), cudaMemcpyHostToDevice), "upload");
-  ntile_ = (n_ + NT * rfill_points() - 1) / (NT * rfill_points());
+  ntile_ = fill_tiles();
   nchunk_ = (n_ + CHUNK - 1) / CHUNK;
   // own FFT: n = 2m, m = m1 * 256 with m1 a power of two in [8, 256]
   own_fft_ = fft_mode_ == 0 && n_ >= 4096 && n_ <= 131072 && (n_ & (n_ - 1)) == 0;
@@ -2082,7 +2112,7 @@ void Engine1::set_tuning(const Tune1& t) {
   tune_ = t;
   tune_.own_fft = t.own_fft ? 1 : 0;
   if (fft_changed) set_fft_mode(tune_.own_fft ? 0 : 1);  // rebuilds tables, plans, work space
-  if (static_ok_) ntile_ = (n_ + NT * rfill_points() - 1) / (NT * rfill_points());
+  if (static_ok_) ntile_ = fill_tiles();
   drop_graphs();
 }
 
@@ -2293,9 +2323,10 @@ void Engine1::reserve(unsigned P) {
   ws_.nodes = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * NI);
   ws_.spl = dalloc<double>(static_cast<size_t>(P) * B_ * 2 * 4 * NI);
   ws_.rbuf = dalloc<double>(static_cast<size_t>(P) * B_ * nc2);
-  // room for the smallest tile the autotuner may pick
-  ws_.rpart = dalloc<double>(static_cast<size_t>(P) * B_ *
-                             ((n_ + NT * kMaxTilesPer - 1) / (NT * kMaxTilesPer)) * 2);
+  // room for the smallest tile the autotuner may pick, or the run blocks
+  ws_.rpart = dalloc<double>(
+      static_cast<size_t>(P) * B_ *
+      std::max<size_t>((n_ + NT * kMaxTilesPer - 1) / (NT * kMaxTilesPer), runblk_) * 2);
   if (own_fft_) {
     ws_.tmp = dalloc<double>(static_cast<size_t>(P) * std::max(B_, D_) * nc2);
     fftA_attr<-1>();

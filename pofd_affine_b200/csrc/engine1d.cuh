@@ -51,6 +51,11 @@ struct BSet1Dev {
   double maxsb;         // max sigma_base of the set
   int ds_begin, nds;
   const int* gidx;      // node interval of each grid point, -1 if uncovered
+  const int2* runs;     // the grid cut into runs of <= 16 points of one
+                        // interval and side: x = first index, y = (q + 1) << 8
+                        // | len << 2 | kind (0 uncovered, 1 point by point,
+                        // 2 running products)
+  int nruns;
 };
 
 struct DSet1Dev {
@@ -134,8 +139,8 @@ struct Tune1 {
   int rfill_mode = 1;       // R grid fill: 0 materialised, one exp2 per grid
                             // point; 1 the same inside the forward FFT pass
                             // A (own FFT), the grid never stored; 2
-                            // materialised by running products over
-                            // 16-point segments in one node interval
+                            // materialised by running products over runs
+                            // of <= 16 points in one node interval
 };
 
 class Engine1 {
@@ -196,7 +201,9 @@ class Engine1 {
   void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7);
   const Tune1& tuning() const { return tune_; }
   // grid points per thread of the materialised R fill
-  int rfill_points() const { return tune_.rfill_mode == 2 ? 16 : tune_.rfill_per; }
+  // blocks per row of the materialised R fill: PER points per thread, or
+  // (running products) NT runs per block
+  unsigned fill_tiles() const;
   void set_tuning(const Tune1& t);
   // <S>, <S^2> of each proposal's model (calcLike::fillBonusParams,
   // calcLike.cc:958-980): host rows -> out[nprop][2]
@@ -249,6 +256,7 @@ class Engine1 {
   std::vector<DSet1Dev> h_dsets_;
   unsigned B_ = 0, D_ = 0;
   unsigned ntile_ = 0, nchunk_ = 0;
+  unsigned runblk_ = 0;  // most run blocks of any beam set's grid
   int maxterms_ = 1;
   // work space
   Workspace1 ws_;
