@@ -361,19 +361,47 @@ __global__ void k_unscale(int M, int Mp, int ntiles, const float* __restrict__ y
   if (status) status[r] = POFD_OK;
 }
 
+// Appends the valid rows (status OK, finite logL) to the pair ring in row
+// order: one block walks the rows in chunks, a ballot prefix gives each
+// valid row its slot, so the ring's contents -- and every minibatch drawn
+// from it -- depend only on the inputs (ranks that train on the same pairs
+// train the same network).
 __global__ void k_append_pairs(int n, const float* __restrict__ theta, int npar,
                                const double* __restrict__ logl, const int* __restrict__ status,
                                float* __restrict__ ptheta, double* __restrict__ plogl,
                                unsigned* __restrict__ counters, unsigned cap) {
   // counters[0] = pairs written (ring), counters[1] = pairs held
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  if (status && status[r] != POFD_OK) return;
-  if (!isfinite(logl[r])) return;
-  const unsigned slot = atomicAdd(&counters[0], 1u) % cap;
-  for (int p = 0; p < npar; ++p) ptheta[static_cast<size_t>(slot) * npar + p] = theta[static_cast<size_t>(r) * npar + p];
-  plogl[slot] = logl[r];
-  atomicMax(&counters[1], min(slot + 1, cap));
+  __shared__ unsigned wsum[32];
+  __shared__ unsigned base;
+  if (threadIdx.x == 0) base = counters[0];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+    const int r = c0 + static_cast<int>(threadIdx.x);
+    const bool ok = r < n && (!status || status[r] == POFD_OK) && isfinite(logl[r]);
+    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+    if (lane == 0) wsum[wid] = __popc(bal);
+    __syncthreads();
+    unsigned off = base;
+    for (int k = 0; k < wid; ++k) off += wsum[k];
+    if (ok) {
+      const unsigned slot = (off + __popc(bal & ((1u << lane) - 1u))) % cap;
+      for (int p = 0; p < npar; ++p)
+        ptheta[static_cast<size_t>(slot) * npar + p] = theta[static_cast<size_t>(r) * npar + p];
+      plogl[slot] = logl[r];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tot = 0;
+      for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) tot += wsum[k];
+      base += tot;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    counters[0] = base;
+    counters[1] = min(max(counters[1], base), cap);
+  }
 }
 
 // ----------------------------------------------------------- tensor maps
@@ -663,8 +691,8 @@ void Surrogate::add_pairs(unsigned n, const float* theta, unsigned npar, const d
   if (npar != npar_) throw Error(POFD_E_ARG, "parameter count differs from the surrogate's");
   ck(cudaSetDevice(device_), "cudaSetDevice");
   if (!st) st = stream_;
-  k_append_pairs<<<(n + 127) / 128, 128, 0, st>>>(static_cast<int>(n), theta, static_cast<int>(npar),
-                                                  logl, status, ptheta_, plogl_, counters_, cap_);
+  k_append_pairs<<<1, 1024, 0, st>>>(static_cast<int>(n), theta, static_cast<int>(npar), logl,
+                                     status, ptheta_, plogl_, counters_, cap_);
   ck(cudaGetLastError(), "k_append_pairs");
 }
 

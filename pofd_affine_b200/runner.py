@@ -226,7 +226,8 @@ DA_SCALE_2D = 5.0      # stretch parameter of the delayed-acceptance steps
 
 
 def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
-                          train_iters=2000, da_scale=DA_SCALE_2D):
+                          train_iters=2000, da_scale=DA_SCALE_2D,
+                          refresh=DA_REFRESH):
     """Plain vs delayed acceptance on the two-field 2D fit (a 1500x1500 pair
     on a 2048^2 grid and an 800x600 pair on a 1024^2 grid in one summed
     likelihood, 14 free parameters, 128 walkers).
@@ -237,7 +238,8 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
     Laplace approximation there (finite-difference Hessian) and npre plain
     steps.  Each run then burns nburn steps (default: enough
     for 20k exact pairs, on which the surrogate first trains) and records
-    nsteps; the surrogate is retrained every 5k new exact evaluations, and
+    nsteps; the surrogate is retrained every `refresh` (5k) new exact
+    evaluations, and
     the delayed-acceptance steps use the stretch parameter da_scale (the
     plain steps the reference's 2).  With plain_control a second plain run
     (another seed) gives the plain-vs-plain agreement the DA-vs-plain
@@ -307,7 +309,7 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
     hold = (ch[pick], plain["logl"].reshape(-1)[pick])
     S = Surrogate(ctx, npar, list(range(nfree)), hidden=384, seed=9)
     da = run_da(ens(32, start), S, nburn, nsteps, train_iters=train_iters,
-                refresh=DA_REFRESH, holdout=hold, da_scale=da_scale)
+                refresh=refresh, holdout=hold, da_scale=da_scale)
     free = list(range(nfree))
     out = {"plain": plain, "da": da, "start_loglike": lopt,
            "agreement": posterior_agreement(da, plain, free)}
@@ -363,15 +365,21 @@ def _main(argv=None):
     p.add_argument("--save", default=None,
                    help="write the three chains (every --thin-th step) to this .npz")
     p.add_argument("--thin", type=int, default=10)
+    p.add_argument("--refresh", type=int, default=DA_REFRESH,
+                   help="retrain after this many new exact evaluations")
+    p.add_argument("--no-control", action="store_true",
+                   help="skip the second plain run")
     a = p.parse_args(argv)
-    r = compare_two_fields_2d(Context(0), a.steps, a.pre, a.burn, plain_control=True,
-                              da_scale=a.da_scale)
+    r = compare_two_fields_2d(Context(0), a.steps, a.pre, a.burn,
+                              plain_control=not a.no_control,
+                              da_scale=a.da_scale, refresh=a.refresh)
     summ = summarise(r)
     summ.update(steps=a.steps, pre=a.pre, burn=a.burn)
     if a.save:
         np.savez_compressed(a.save, **{
             "%s_%s" % (k, f): r[k][f][::a.thin]
-            for k in ("plain", "da", "plain_control") for f in ("chain", "logl")})
+            for k in ("plain", "da", "plain_control") if k in r
+            for f in ("chain", "logl")})
     print(json.dumps(summ))
 
 

@@ -86,6 +86,43 @@ def test_training_fits_a_log_density(gpu_ctx):
     assert after < 0.05 * np.std(ll), (after, np.std(ll))
 
 
+def test_pair_ring_order_and_training_are_deterministic(gpu_ctx):
+    """Pairs enter the ring in row order, invalid rows (bad status,
+    non-finite logL) skipped, wrapping at the capacity; two surrogates fed
+    the same pairs and trained with the same seed predict bit-identically
+    (what lets every rank of a sharded ensemble train the same network)."""
+    from pofd_affine_b200.surrogate import Surrogate
+    k = 6
+    th, ll, _, _ = _gauss_pairs(3000, k, 3)
+    thp = np.concatenate([th, np.ones((len(th), 1), np.float32)], 1)
+    st = np.zeros(len(th), np.int32)
+    st[::7] = -1
+    ll = ll.copy()
+    ll[5::11] = np.inf
+    ok = (st == 0) & np.isfinite(ll)
+    nets = []
+    for _ in range(2):
+        S = Surrogate(gpu_ctx, k + 1, list(range(k)), hidden=256, seed=3,
+                      capacity=2048)
+        for a in range(0, len(th), 1100):  # batches larger than one block
+            S.addPairs(thp[a:a + 1100], ll[a:a + 1100], st[a:a + 1100])
+        nets.append(S)
+    S = nets[0]
+    assert S.nPairs() == 2048
+    g_th, g_ll = S.getPairs()
+    v_th, v_ll = thp[ok], ll[ok]
+    nv = len(v_ll)
+    slot = np.arange(nv) % 2048
+    exp_th = np.empty((2048, k + 1), np.float32)
+    exp_ll = np.empty(2048)
+    exp_th[slot], exp_ll[slot] = v_th, v_ll  # later rows overwrite
+    assert np.array_equal(g_th, exp_th) and np.array_equal(g_ll, exp_ll)
+    for S in nets:
+        S.train(200, batch=512, lr=1e-3)
+    p0, p1 = nets[0].predict(thp[:256]), nets[1].predict(thp[:256])
+    assert np.array_equal(p0, p1)
+
+
 def test_delayed_acceptance_exact_posterior_and_gain(gpu_ctx):
     """DA keeps the exact posterior (means within 0.1 sigma of the plain
     run and of the truth) and accepts far more of its exact evaluations."""
