@@ -675,6 +675,14 @@ int pofd_ensemble_do_steps_da(pofd_ensemble* e, unsigned nsteps, int record);
  * affineEnsemble.cc:1346-1352); != 0 rejects the step and counts it
  * (pofd_ensemble_failures). */
 int pofd_ensemble_set_error_policy(pofd_ensemble* e, int reject_failures);
+/* Steps outside the parameter limits: reject_outside == 0 (default) redraws
+ * z up to 40 more times, as the reference's generateNewStep does
+ * (affineEnsemble.cc:1144-1228); != 0 rejects such a step at once, the
+ * limits acting as a prior that is zero outside them.  Redrawing makes the
+ * proposal depend on a walker's distance to a limit and biases the chain
+ * where the posterior reaches one; rejecting keeps the stretch move (plain
+ * and delayed acceptance alike) exact for the truncated posterior. */
+int pofd_ensemble_set_limit_policy(pofd_ensemble* e, int reject_outside);
 int pofd_ensemble_failures(pofd_ensemble* e, unsigned long long* n);
 /* Counters since init: [0] proposals, [1] stage-one passes, [2] exact
  * evaluations (padding included), [3] accepted moves. */

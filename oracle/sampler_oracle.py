@@ -57,10 +57,13 @@ def gen_z(a, x):
 
 
 def stretch_run(theta, logl, loglike_batch, nsteps, seed, scalefac=2.0,
-                state=None, lo=None, hi=None, temp=1.0, step0=0):
+                state=None, lo=None, hi=None, temp=1.0, step0=0,
+                reject_outside=False):
     """Runs nsteps full steps from walkers theta [nw, np] (float32) with
     log-likelihoods logl; loglike_batch(thetas) -> (logl, status).  Returns
-    the chain [nsteps, nw, np], its logl [nsteps, nw] and accept counts."""
+    the chain [nsteps, nw, np], its logl [nsteps, nw] and accept counts.
+    reject_outside: a step outside the limits is rejected instead of
+    redrawing z (the product's opt-in limit policy)."""
     theta = np.array(theta, dtype=np.float32)
     logl = np.array(logl, dtype=np.float64)
     nw, npar = theta.shape
@@ -97,17 +100,20 @@ def stretch_run(theta, logl, loglike_batch, nsteps, seed, scalefac=2.0,
                             y[p] = np.float32(z * theta[i, p]) + np.float32(omz * theta[j, p])
                             if not (lo[p] <= y[p] <= hi[p]):
                                 ok = False
-                    if ok or it > MAXITERS:
+                    if ok or reject_outside or it > MAXITERS:
                         break
                     z = gen_z(scalefac, draw(seed, step, i, (half << 16) | (it + 1))[0])
                     it += 1
                 if not ok:
-                    raise RuntimeError("Unable to generate new step")
+                    if not reject_outside:
+                        raise RuntimeError("Unable to generate new step")
+                    y = theta[i].copy()  # evaluated, then rejected
+                    z = np.float32(np.nan)
                 props.append(y)
                 zs.append(z)
             ln, st = loglike_batch(np.array(props))
             for t, i in enumerate(idx):
-                if st[t] == 1:
+                if st[t] == 1 or np.isnan(zs[t]):
                     continue
                 if st[t] != 0 or not math.isfinite(ln[t]):
                     raise RuntimeError("Invalid likelihood")

@@ -163,6 +163,7 @@ SIGNATURES = {
     "pofd_likesum_add_like2": (I, [V, V]),
     "pofd_likesum_eval_batch_device": (I, [V, U, V, U, V, V, V]),
     "pofd_ensemble_set_error_policy": (I, [V, I]),
+    "pofd_ensemble_set_limit_policy": (I, [V, I]),
     "pofd_ensemble_failures": (I, [V, C.POINTER(C.c_ulonglong)]),
     "pofd_pdfactory2_create": (I, [V, U, PV]),
     "pofd_pdfactory2_destroy": (I, [V]),

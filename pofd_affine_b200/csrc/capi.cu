@@ -1443,6 +1443,14 @@ int pofd_ensemble_set_error_policy(pofd_ensemble* e, int reject_failures) {
   });
 }
 
+int pofd_ensemble_set_limit_policy(pofd_ensemble* e, int reject_outside) {
+  return guard([&] {
+    need(e != nullptr, "null argument");
+    e->ens->set_limit_policy(reject_outside != 0);
+    return POFD_OK;
+  });
+}
+
 int pofd_ensemble_failures(pofd_ensemble* e, unsigned long long* n) {
   return guard([&] {
     need(e && n, "null argument");

@@ -98,8 +98,8 @@ struct PDInfo2 {
 // changes what is computed; the FFT mode changes the transform's rounding).
 struct Tune2 {
   int fft_mode = 1;     // see set_fft_mode
-  int rgrid_rows = 4;   // R-grid rows per block of k_rgrid2 (2, 4, 8)
-  int edge_rows = 8;    // band-1 edge rows per group of k_redge2 (4, 8, 16)
+  int rgrid_rows = 8;   // R-grid rows per block of k_rgrid2 (2, 4, 8)
+  int edge_rows = 16;   // band-1 edge rows per group of k_redge2 (4, 8, 16)
 };
 
 class Engine2 {

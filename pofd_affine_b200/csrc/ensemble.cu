@@ -80,9 +80,15 @@ __device__ __forceinline__ bool valid_param(float v, float lo, float hi) {
 
 // generateNewStep (affineEnsemble.cc:1144-1228) for one half of the
 // ensemble: walker i combines with a uniformly drawn partner of the other
-// half, retrying z up to 40 more times while the step is invalid.
+// half, retrying z up to 40 more times while the step is invalid.  With
+// reject_outside the first z is kept and a step outside the limits is
+// rejected (the limits act as a prior that is zero outside them): no
+// retries, no error.  Redrawing z until the step is inside makes the
+// proposal's normalisation depend on the walker's distance to a limit, which
+// breaks detailed balance for walkers near one; rejecting keeps the move
+// exact for the posterior truncated to the limits.
 __global__ void k_propose(int half, unsigned nw, unsigned np, double scalefac,
-                          unsigned long long seed,
+                          int reject_outside, unsigned long long seed,
                           const int* __restrict__ pstate,
                           const float* __restrict__ plo,
                           const float* __restrict__ phi,
@@ -121,16 +127,16 @@ __global__ void k_propose(int half, unsigned nw, unsigned np, double scalefac,
       }
       y[p] = v;
     }
-    if (ok || iter > kMaxIters) break;
+    if (ok || reject_outside || iter > kMaxIters) break;
     const uint4 rr = draw(seed, step, i, (static_cast<unsigned>(half) << 16) | (iter + 1));
     z = gen_z(scalefac, rr.x);
   }
   if (!ok) {
-    // "Unable to generate new step after 40 tries": evaluate the old
-    // position and reject it
+    // "Unable to generate new step after 40 tries" (or a step outside the
+    // limits under reject_outside): evaluate the old position and reject it
     for (unsigned p = 0; p < np; ++p) y[p] = xo[p];
     z = qnan;
-    if (atomicCAS(err, 0, 1) == 0) err[1] = static_cast<int>(i);
+    if (!reject_outside && atomicCAS(err, 0, 1) == 0) err[1] = static_cast<int>(i);
   }
   zout[t] = z;
 }
@@ -501,8 +507,8 @@ void Ensemble::launch_step(cudaStream_t st) {
   for (int half = 0; half < 2; ++half) {
     const unsigned nh = half ? nh1 : nh0;
     const unsigned g = (nh + ENT - 1) / ENT;
-    k_propose<<<g, ENT, 0, st>>>(half, nw_, np_, scalefac_, seed_, pstate_, plo_, phi_,
-                                 theta_, prop_, z_, ctr_, err_);
+    k_propose<<<g, ENT, 0, st>>>(half, nw_, np_, scalefac_, reject_outside_ ? 1 : 0, seed_,
+                                 pstate_, plo_, phi_, theta_, prop_, z_, ctr_, err_);
     ck(cudaGetLastError(), "k_propose");
     const int rc = fn_(like_, nh, prop_, np_, lnew_, snew_, st);
     if (rc < 0) throw Error(rc, "batched likelihood enqueue failed");
@@ -604,6 +610,11 @@ void Ensemble::set_error_policy(bool reject_failures) {
   drop_graph();
 }
 
+void Ensemble::set_limit_policy(bool reject_outside) {
+  reject_outside_ = reject_outside;
+  drop_graph();
+}
+
 unsigned long long Ensemble::failures() const {
   unsigned long long v = 0;
   ck(cudaSetDevice(device_), "cudaSetDevice");
@@ -642,8 +653,8 @@ void Ensemble::da_half(int half, double zexp, double invt) {
   const unsigned nh0 = nw_ / 2, nh = half ? nw_ - nh0 : nh0;
   const unsigned g = (nh + ENT - 1) / ENT;
   const double a = (da_scale_ > 1.0) ? da_scale_ : scalefac_;
-  k_propose<<<g, ENT, 0, stream_>>>(half, nw_, np_, a, seed_, pstate_, plo_, phi_, theta_,
-                                    prop_, z_, ctr_, err_);
+  k_propose<<<g, ENT, 0, stream_>>>(half, nw_, np_, a, reject_outside_ ? 1 : 0, seed_, pstate_,
+                                    plo_, phi_, theta_, prop_, z_, ctr_, err_);
   ck(cudaGetLastError(), "k_propose");
   int rc = sfn_(sur_, nh, prop_, np_, spred_, sst_, stream_);
   if (rc < 0) throw Error(rc, "first-stage evaluation failed");

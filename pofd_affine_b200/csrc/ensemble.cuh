@@ -64,6 +64,10 @@ class Ensemble {
   // false (default): a failed likelihood evaluation stops the run, as in the
   // reference; true: it rejects the step and is counted.
   void set_error_policy(bool reject_failures);
+  // false (default): a step outside the parameter limits redraws z, up to
+  // 40 times, as in the reference; true: it is rejected (exact for the
+  // posterior truncated to the limits).
+  void set_limit_policy(bool reject_outside);
   unsigned long long failures() const;
   unsigned nrecorded() const;
   void chain(float* theta, double* logl) const;
@@ -137,6 +141,7 @@ class Ensemble {
   int* hcount_ = nullptr;     // pinned
   unsigned long long stats_[4] = {0, 0, 0, 0};
   bool reject_fail_ = false;
+  bool reject_outside_ = false;
   unsigned long long* nfail_ = nullptr;
 };
 

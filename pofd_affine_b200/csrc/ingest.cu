@@ -28,7 +28,7 @@ namespace pofd {
 namespace {
 
 constexpr int INT = 256;       // threads per block
-constexpr int STAGE = 4096;    // values staged per round of the sequential sum
+constexpr int STAGE = 2048;    // values staged per round of the sequential sum
 
 void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -38,23 +38,47 @@ void ck(cudaError_t e, const char* what) {
   }
 }
 
-// out = (x[0] + x[1] + ... + x[n-1]) / n, added in index order.
-__global__ void __launch_bounds__(INT) k_seqmean(const double* __restrict__ x, size_t n,
+// out[b] = (x_b[0] + x_b[1] + ... + x_b[n-1]) / n, added in index order
+// (the rounding of the host set-up's sequential sum); block b takes array b
+// (xa, or xb for a second band).  The adds form one dependent chain, so one
+// thread does them, from registers eight values at a time, while warps
+// 1 .. 7 stage the next STAGE values into the other half of a double buffer.
+__global__ void __launch_bounds__(INT) k_seqmean(const double* __restrict__ xa,
+                                                 const double* __restrict__ xb, size_t n,
                                                  double* __restrict__ out) {
-  __shared__ double buf[STAGE];
+  __shared__ double buf[2][STAGE];
+  const double* __restrict__ x = blockIdx.x ? xb : xa;
+  const size_t nst = (n + STAGE - 1) / STAGE;
+  for (int i = threadIdx.x; i < static_cast<int>(min(static_cast<size_t>(STAGE), n)); i += INT)
+    buf[0][i] = x[i];
+  __syncthreads();
   double s = 0.0;
-  for (size_t base = 0; base < n; base += STAGE) {
-    const int m = static_cast<int>(min(static_cast<size_t>(STAGE), n - base));
-    __syncthreads();
-    for (int i = threadIdx.x; i < m; i += INT) buf[i] = x[base + i];
-    __syncthreads();
-    if (threadIdx.x == 0) {
+  for (size_t k = 0; k < nst; ++k) {
+    const size_t base = k * STAGE;
+    if (threadIdx.x >= 32) {
+      const size_t nb = base + STAGE;
+      if (nb < n) {
+        const int m2 = static_cast<int>(min(static_cast<size_t>(STAGE), n - nb));
+        double* d = buf[(k + 1) & 1];
+        for (int i = threadIdx.x - 32; i < m2; i += INT - 32) d[i] = x[nb + i];
+      }
+    } else if (threadIdx.x == 0) {
+      const int m = static_cast<int>(min(static_cast<size_t>(STAGE), n - base));
+      const double* b = buf[k & 1];
       int i = 0;
-      if (base == 0) s = buf[i++];
-      for (; i < m; ++i) s = __dadd_rn(s, buf[i]);
+      if (k == 0) s = b[i++];
+      for (; i + 8 <= m; i += 8) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = b[i + q];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s = __dadd_rn(s, v[q]);
+      }
+      for (; i < m; ++i) s = __dadd_rn(s, b[i]);
     }
+    __syncthreads();
   }
-  if (threadIdx.x == 0) *out = __ddiv_rn(s, static_cast<double>(n));
+  if (threadIdx.x == 0) out[blockIdx.x] = __ddiv_rn(s, static_cast<double>(n));
 }
 
 __global__ void k_subtract(double* __restrict__ x, size_t n, const double* __restrict__ m) {
@@ -179,7 +203,7 @@ void ingest_bin1(double* x, size_t n, bool meansub, unsigned nb, unsigned* bins,
      "cudaMallocAsync");
   double mean = 0.0;
   if (meansub) {
-    k_seqmean<<<1, INT, 0, st>>>(x, n, scratch);
+    k_seqmean<<<1, INT, 0, st>>>(x, x, n, scratch);
     k_subtract<<<grid_for(n, sms), INT, 0, st>>>(x, n, scratch);
     ck(cudaGetLastError(), "mean subtraction");
     ck(cudaMemcpyAsync(&mean, scratch, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
@@ -217,8 +241,7 @@ void ingest_bin2(double* x1, double* x2, size_t n, bool meansub, unsigned nb1, u
      "cudaMallocAsync");
   double means[2] = {0.0, 0.0};
   if (meansub) {
-    k_seqmean<<<1, INT, 0, st>>>(x1, n, scratch);
-    k_seqmean<<<1, INT, 0, st>>>(x2, n, scratch + 1);
+    k_seqmean<<<2, INT, 0, st>>>(x1, x2, n, scratch);
     k_subtract<<<grid_for(n, sms), INT, 0, st>>>(x1, n, scratch);
     k_subtract<<<grid_for(n, sms), INT, 0, st>>>(x2, n, scratch + 1);
     ck(cudaGetLastError(), "mean subtraction");

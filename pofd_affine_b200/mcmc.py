@@ -189,6 +189,14 @@ class affineEnsemble:
         check(lib().pofd_ensemble_set_error_policy(self.h,
                                                    1 if reject_failures else 0))
 
+    def setLimitPolicy(self, reject_outside):
+        """False (default): a step outside the parameter limits redraws z
+        (up to 40 times) as in the reference; True: it is rejected, which
+        keeps the move exact where the posterior reaches a limit."""
+        self.reject_outside = bool(reject_outside)
+        check(lib().pofd_ensemble_set_limit_policy(self.h,
+                                                   1 if reject_outside else 0))
+
     def getFailures(self):
         n = C.c_ulonglong()
         check(lib().pofd_ensemble_failures(self.h, C.byref(n)))

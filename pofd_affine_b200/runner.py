@@ -243,7 +243,10 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
     the delayed-acceptance steps use the stretch parameter da_scale (the
     plain steps the reference's 2).  With plain_control a second plain run
     (another seed) gives the plain-vs-plain agreement the DA-vs-plain
-    agreement is compared with."""
+    agreement is compared with.  Every run rejects steps outside the
+    parameter limits (affineEnsemble.setLimitPolicy): the third sigma knot's
+    posterior reaches its lower limit, where the reference's redrawing of z
+    biases a chain, and more so the wider the stretch."""
     from . import synth
     from .mcmc import affineEnsemble, likeSum
     from .surrogate import Surrogate
@@ -282,6 +285,10 @@ def compare_two_fields_2d(ctx, nsteps, npre, nburn=None, plain_control=False,
         for p, (lo, hi) in enumerate(lims):
             E.setParamLimits(p, lo, hi)
         E.setErrorPolicy(True)  # unphysical corners reject instead of stop
+        # the posterior of the third sigma knot reaches its lower limit:
+        # steps outside the limits are rejected (exact for the truncated
+        # posterior) rather than redrawn, for every run alike
+        E.setLimitPolicy(True)
         if start is None:
             # walkers drawn from the Laplace approximation at the maximum,
             # inside the limits

@@ -101,9 +101,10 @@ def test_pd_and_r_grid_match_oracle(orc, gpu_ctx, beams, case):
     pf = f.getPD(s["sig"][0], setLog=False)
     assert np.max(np.abs(pf.pd - po)) <= P_TOL * po.max()
     assert abs(pf.minflux - io["pd_minflux"]) <= 1e-10 * abs(io["pd_minflux"])
-    # every R fill: one exp2 per point (materialised), and by running
-    # products over 16-point segments
-    for mode in (0, 2):
+    # every R fill: one exp2 per point (materialised, or inside the forward
+    # FFT pass A), and by running products over runs of one node interval
+    d0 = G.getTuning()["rfill_mode"]
+    for mode in (0, 1, 2):
         G.setTuning(rfill_mode=mode)
         rg = G.getR(0, s["th"])
         assert np.max(np.abs(rg - ro)) <= 1e-12 * ro.max(), mode
@@ -112,7 +113,7 @@ def test_pd_and_r_grid_match_oracle(orc, gpu_ctx, beams, case):
         assert abs(im["mn"] - io["mn"]) <= 1e-12 * abs(io["mn"])
         assert abs(im["var_noi"] - io["var_noi"]) <= 1e-12 * io["var_noi"]
         assert np.max(np.abs(pm - po)) <= P_TOL * po.max()
-    G.setTuning(rfill_mode=1)
+    G.setTuning(rfill_mode=d0)
 
 
 def test_noiseless_factory(orc, gpu_ctx):

@@ -31,12 +31,13 @@ def test_own_fft_matches_cufft(orc, gpu_ctx, n):
     assert list(so) == list(sc)
     ok = so == 0
     assert np.max(np.abs(lo[ok] - lc[ok])) < 1e-7
-    # the R grid fill fused into the forward pass A with one exp2 per point
-    # (default) against the materialised fill, with one exp2 per point and by
-    # running products over 16-point segments: values within ~1e-13
-    # relative, moments grouped differently
-    assert L.getTuning()["rfill_mode"] == 1
-    for rf in (0, 2):
+    # the default R grid fill (running products over runs of one node
+    # interval) against the other two, one exp2 per point materialised or
+    # inside the forward pass A: values within ~1e-13 relative, moments
+    # grouped differently
+    d0 = L.getTuning()["rfill_mode"]
+    assert d0 == 2
+    for rf in (0, 1):
         L.setTuning(rfill_mode=rf)
         lu, su = L.getLogLikeBatch(th)
         pu, iu = L.getPD(1, 0, th[0], setLog=False)
@@ -44,7 +45,7 @@ def test_own_fft_matches_cufft(orc, gpu_ctx, n):
         assert np.max(np.abs(lu[ok] - lo[ok])) < 1e-7
         du = int(io["splitidx"] - iu["splitidx"])
         assert np.max(np.abs(np.roll(po, du) - pu)) <= 1e-10 * pu.max()
-    L.setTuning(rfill_mode=1)
+    L.setTuning(rfill_mode=d0)
     # where the P(D) tail lies at the transform's rounding floor (large n),
     # the first bin below the reference's split threshold is set by rounding
     # and can differ between any two FFTs; the unwrapped arrays are then the

@@ -52,6 +52,60 @@ def test_chain_matches_oracle_gauss(gpu_ctx, nw):
     assert np.all(np.isnan(ch[..., 4])) and np.all(ch[..., 3] == 7.0)
 
 
+def test_limit_policy_reject_matches_oracle(gpu_ctx):
+    """Steps outside the limits rejected instead of redrawn: the same chain
+    as the oracle's under that policy, draw for draw, with a wide stretch
+    and a limit through the middle of the posterior (many steps leave it)."""
+    import sampler_oracle as so
+    from pofd_affine_b200.mcmc import affineEnsemble, gaussLike
+    mu, cov = _gauss(3, seed=5)
+    nw = 16
+    G = gaussLike(gpu_ctx, mu, cov)
+    E = affineEnsemble(gpu_ctx, G, nw, 3, scalefac=5.0, seed=77)
+    E.setParamLimits(0, mu[0], np.inf)
+    E.setLimitPolicy(True)
+    w = E.generateInitialPosition(mu, np.ones(3), rng=3)
+    E.initChains(w)
+    E.doSteps(60)
+    ch, cl = E.getChain()
+    oc, ol, on = so.stretch_run(w, np.full(nw, -np.inf), _np_gauss(mu, cov),
+                                60, seed=77, scalefac=5.0, state=E.state,
+                                lo=E.lo, hi=E.hi, reject_outside=True)
+    assert np.array_equal(ch, oc, equal_nan=True)
+    assert np.allclose(cl, ol, rtol=1e-13, atol=0)
+    assert np.array_equal(E.getNAccept(), on)
+    assert np.all(ch[..., 0] >= mu[0])
+
+
+def test_limit_policy_reject_is_exact_at_a_limit(gpu_ctx):
+    """A Gaussian truncated at the mean of its first parameter: rejecting
+    steps outside the limit recovers the half-normal mean mu + sd sqrt(2/pi)
+    (to 0.03 sd, for a = 2 and a = 5), while the reference's redrawing of z
+    leaves that mean biased by more than 0.08 sd: walkers near the limit
+    see their out-of-range moves replaced by in-range ones, which breaks
+    detailed balance there."""
+    from pofd_affine_b200.mcmc import affineEnsemble, gaussLike
+    mu, cov = _gauss(3, seed=1)
+    sd0 = np.sqrt(cov[0, 0])
+    exact = mu[0] + sd0 * np.sqrt(2.0 / np.pi)
+    G = gaussLike(gpu_ctx, mu, cov)
+
+    def mean0(a, reject):
+        E = affineEnsemble(gpu_ctx, G, 64, 3, scalefac=a, seed=11)
+        E.setParamLimits(0, mu[0], np.inf)
+        E.setLimitPolicy(reject)
+        E.initChains(E.generateInitialPosition(mu, np.sqrt(np.diag(cov)), rng=5))
+        E.doSteps(6000, initsteps=500)
+        ch, _ = E.getChain()
+        return (ch[..., 0].astype(np.float64).mean() - exact) / sd0
+    for a in (2.0, 5.0):
+        b = mean0(a, True)
+        assert abs(b) < 0.03, (a, b)
+    b = mean0(2.0, False)
+    assert b > 0.08, b
+    print("limit at the mean: redraw bias %.3f sd" % b)
+
+
 def test_acor_and_posterior_gauss(gpu_ctx):
     import sampler_oracle as so
     from pofd_affine_b200.mcmc import affineEnsemble, gaussLike

@@ -98,3 +98,23 @@ def test_host_mcmc_baseline_runs():
     assert 0.05 < r["acceptance"] < 0.95
     assert np.isfinite(r["tau_max"]) and r["ess"] > 0
     assert 0 < r["likelihood_s"] <= r["wall_s"]
+
+
+def test_oracle_limit_policy_reject_stays_inside():
+    """The oracle's reject-outside limit policy (the product's opt-in
+    policy): a wide stretch with a limit through the posterior's middle
+    never leaves the limits and never raises, and only steps inside the
+    limits are accepted."""
+    import sampler_oracle as so
+
+    def ll(th):
+        d = th.astype(np.float64)
+        return -0.5 * (d * d).sum(1), np.zeros(len(th), int)
+    w = np.abs(np.random.default_rng(0).normal(size=(8, 2))).astype(np.float32)
+    lo = np.array([0.0, -np.inf], np.float32)
+    hi = np.array([np.inf, np.inf], np.float32)
+    ch, _, na = so.stretch_run(w, np.full(8, -np.inf), ll, 60, seed=3,
+                               scalefac=5.0, lo=lo, hi=hi,
+                               reject_outside=True)
+    assert ch[..., 0].min() >= 0.0
+    assert 0 < na.sum() < 8 * 60
