@@ -766,17 +766,19 @@ def mcmc_2d(ctx, nsteps=1500):
     shared equilibrated start, with a plain-vs-plain control
     (runner.compare_two_fields_2d, runner.summarise)."""
     from pofd_affine_b200 import runner
-    r = runner.compare_two_fields_2d(ctx, nsteps, 300, plain_control=True)
+    npre = 2000  # ~10 autocorrelation times: a shared start at equilibrium
+    r = runner.compare_two_fields_2d(ctx, nsteps, npre, plain_control=True)
     out = runner.summarise(r)
     out["workload"] = ("2D two-field fit: 1500x1500 pair on 2048^2 + 800x600 "
                        "pair on 1024^2 in one launch, 14 free parameters, "
                        "128 walkers, shared start (Powell maximum, walkers "
-                       "from its Laplace approximation, 300 plain steps, "
+                       "from its Laplace approximation, %d plain steps, "
                        "untimed), burn %d steps (20k exact pairs), %d "
                        "recorded steps; DA: MLP 14 -> 3x384 SiLU -> 1 trained "
                        "on the burn-in pairs, retrained every 5k exact "
-                       "evaluations, stretch a = %g (plain a = 2)"
-                       % (-(-runner.DA_PAIRS // 128), nsteps,
+                       "evaluations, stretch a = %g (plain a = 2); every "
+                       "run rejects steps outside the parameter limits"
+                       % (npre, -(-runner.DA_PAIRS // 128), nsteps,
                           runner.DA_SCALE_2D))
     return out
 
