@@ -307,11 +307,19 @@ __device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
 
 // Main R grid, rows 1..n-1 x columns 1..n-1 (row 0 and column 0 are the
 // edge cells), times dflux1*dflux2, with block partial sums of the
-// trapezoid moments of getRStats (PDFactoryDouble.cc:593-722).  Each thread
-// owns one column for RB rows: the column's flux constants are read once,
-// each row's sign, term counts and terms are the same for the whole block.
+// trapezoid moments of getRStats (PDFactoryDouble.cc:593-722).  A block
+// covers RG_COLS = RG_CPT * NT columns and RB rows; thread t owns columns
+// base + t + NT q (q < RG_CPT: each store of a warp stays coalesced) and
+// reads their flux constants once.  Per row the sign, the term counts and
+// the list address are read once per thread, and each colour term's
+// (c0, c1, c2) once for all the thread's columns of that term's band-2 sign
+// component: the terms of a cell are summed in the list's order
+// (numberCountsDoubleLogNormal.cc:1972-2002), the columns giving the
+// independent exp2 chains.
+constexpr int RG_CPT = 4;
+constexpr int RG_COLS = RG_CPT * NT;
 template <int RB>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
 k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
          const int* __restrict__ mstatus, const double* __restrict__ rw,
          const int2* __restrict__ rcnt, double* __restrict__ rbuf,
@@ -327,42 +335,75 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
   const int nrows = bs.nrows, ts3 = 3 * bs.Ts;
   const int* __restrict__ rowsgn = bs.rowsgn;
   const double* __restrict__ rowflux = bs.rowflux;
-  const int j = blockIdx.x * NT + threadIdx.x;
-  const bool jin = (j >= 1 && j < n);
-  double if2 = 0.0, lf2 = 0.0, cf2 = 0.0;
-  int fs = 0;
-  if (jin) {
-    if2 = bs.colinv[j];
-    lf2 = bs.collog[j];
-    fs = bs.colsgn[j];
-    cf2 = bs.rflux2[j];
+  const int j0 = blockIdx.x * RG_COLS + threadIdx.x;
+  double if2[RG_CPT], lf2[RG_CPT], cf2[RG_CPT];
+  unsigned cpos = 0, cneg = 0;  // columns (bits q) in each band-2 sign component
+#pragma unroll
+  for (int q = 0; q < RG_CPT; ++q) {
+    const int j = j0 + q * NT;
+    if2[q] = 0.0;
+    lf2[q] = 0.0;
+    cf2[q] = 0.0;
+    if (j >= 1 && j < n) {
+      if2[q] = bs.colinv[j];
+      lf2[q] = bs.collog[j];
+      cf2[q] = bs.rflux2[j];
+      if (if2[q] != 0.0) {
+        if (bs.colsgn[j]) cneg |= 1u << q;
+        else cpos |= 1u << q;
+      }
+    }
   }
   const unsigned hsm = (bs.hassign[0] ? 1u : 0u) | (bs.hassign[1] ? 2u : 0u) |
                        (bs.hassign[2] ? 4u : 0u) | (bs.hassign[3] ? 8u : 0u);
   const double fluxfac = bs.dflux1 * bs.dflux2;
-  const double wc = (j == n - 1) ? 0.5 : 1.0;
   double m1 = 0.0, v1 = 0.0, m2 = 0.0, v2 = 0.0;
   for (int rr = 0; rr < RB; ++rr) {
     const int r = 1 + blockIdx.y * RB + rr;
     if (r >= n) break;
     const int sgn1 = rowsgn[r];
     const size_t ri = static_cast<size_t>(wb) * nrows + r;
-    if (jin) {
-      double R = 0.0;
-      if (sgn1 >= 0 && if2 != 0.0 && ((hsm >> (sgn1 + fs)) & 1u)) {
-        const int2 nt = rcnt[ri];
-        const double* L = rw + ri * ts3 + (fs ? 3 * nt.x : 0);
-        R = term_sum(L, fs ? nt.y : nt.x, lf2, e2.t) * if2 * fluxfac;
+    double acc[RG_CPT];
+#pragma unroll
+    for (int q = 0; q < RG_CPT; ++q) acc[q] = 0.0;
+    if (sgn1 >= 0) {
+      const int2 nt = rcnt[ri];
+      const double* __restrict__ L = rw + ri * ts3;
+#pragma unroll
+      for (int fs = 0; fs < 2; ++fs) {
+        const unsigned cols = fs ? cneg : cpos;
+        if (!cols || !((hsm >> (sgn1 + fs)) & 1u)) continue;
+        const double* __restrict__ T = fs ? L + 3 * nt.x : L;
+        const int cnt = fs ? nt.y : nt.x;
+        for (int k = 0; k < cnt; ++k) {
+          const double c0 = __ldg(T + 3 * k), c1 = __ldg(T + 3 * k + 1),
+                       c2 = __ldg(T + 3 * k + 2);
+#pragma unroll
+          for (int q = 0; q < RG_CPT; ++q) {
+            if (!((cols >> q) & 1u)) continue;
+            const double t = lf2[q] - c1;
+            acc[q] += c0 * dev::exp2_tab(t * t * c2, e2.t);
+          }
+        }
       }
-      rbuf[(static_cast<size_t>(wb) * n + r) * nc2 + j] = R;
-      const double cf1 = rowflux[r];
-      const double cR = (r == n - 1) ? 0.5 * R : R;
+    }
+    const double cf1 = rowflux[r];
+    const double rw1 = (r == n - 1) ? 0.5 : 1.0;
+    double* Rrow = rbuf + (static_cast<size_t>(wb) * n + r) * nc2;
+#pragma unroll
+    for (int q = 0; q < RG_CPT; ++q) {
+      const int j = j0 + q * NT;
+      if (j < 1 || j >= n) continue;
+      const double R = acc[q] * if2[q] * fluxfac;
+      Rrow[j] = R;
+      const double cR = rw1 * R;
+      const double wc = (j == n - 1) ? 0.5 : 1.0;
       const double p1 = wc * cf1 * cR;
-      const double p2 = wc * cf2 * cR;
+      const double p2 = wc * cf2[q] * cR;
       m1 += p1;
       v1 += cf1 * p1;
       m2 += p2;
-      v2 += cf2 * p2;
+      v2 += cf2[q] * p2;
     }
   }
   m1 = dev::block_sum<NT>(m1, shr);
@@ -2296,17 +2337,18 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   mark(2);
   const int rb = tune_.rgrid_rows;
   const unsigned gy = static_cast<unsigned>((n - 1 + rb - 1) / rb);
+  const unsigned gxg = static_cast<unsigned>((n + RG_COLS - 1) / RG_COLS);
   switch (rb) {
     case 2:
-      k_rgrid2<2><<<dim3(gx_, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
+      k_rgrid2<2><<<dim3(gxg, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
                                                        ws_.rcnt, ws_.rbuf, ws_.rpart);
       break;
     case 8:
-      k_rgrid2<8><<<dim3(gx_, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
+      k_rgrid2<8><<<dim3(gxg, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
                                                        ws_.rcnt, ws_.rbuf, ws_.rpart);
       break;
     default:
-      k_rgrid2<4><<<dim3(gx_, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
+      k_rgrid2<4><<<dim3(gxg, gy, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, ws_.mstatus, ws_.rw,
                                                        ws_.rcnt, ws_.rbuf, ws_.rpart);
   }
   mark(3);
@@ -2334,7 +2376,7 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   {
     const int nfp = (n + NT - 1) / NT;
     k_rfinish2<<<dim3(nfp, P * B), NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0, ne, ngr,
-                                                static_cast<int>(gx_ * gy), ws_.mstatus,
+                                                static_cast<int>(gxg * gy), ws_.mstatus,
                                                 ws_.redge, ws_.epart, ws_.rpart, ws_.rbuf,
                                                 ws_.fpart);
     k_rfinal2<<<P * B, NT, 0, st>>>(d_bsets_, B, n, nc2, edge_ ? 1 : 0, ne, ngr, nfp,
