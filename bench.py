@@ -365,9 +365,25 @@ def stage_flops(stage, P, B, n):
     return None
 
 
-def read_traffic(stage):
-    """dram bytes per launch of a kernel from the committed ncu summary
-    (profiles/<kernel>_1d_batched.md, line 'traffic_bytes_per_launch: N')."""
+def read_traffic(stage, per_proposal=False):
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of a stage
+    from the committed ncu summaries: the line
+    'traffic_bytes_per_launch[<stage>]: N' -- or, for a stage captured on a
+    smaller batch than the bench's and scaled by the caller,
+    'traffic_bytes_per_proposal[<stage>]: N' -- in any profiles/*.md, else
+    'traffic_bytes_per_launch: N' in profiles/<stage>_1d_batched.md."""
+    import glob
+    key = "traffic_bytes_per_%s[%s]:" % (
+        "proposal" if per_proposal else "launch", stage)
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        try:
+            for line in open(path):
+                if line.strip().startswith(key):
+                    return float(line.split("]:")[1].split()[0])
+        except (OSError, ValueError):
+            pass
+    if per_proposal:
+        return None
     path = os.path.join(ROOT, "profiles", "%s_1d_batched.md" % stage)
     try:
         for line in open(path):
@@ -437,20 +453,24 @@ def roofline_2d(L, cfg, thetas, stages, P):
     if ms:
         flops = 25.0 * main * (n - 1) * P
         ach = flops / (ms * 1e-3) / 1e12
+        tp = read_traffic("k_rgrid2", per_proposal=True)
         out["roofline_rgrid2"] = {
             "bound": "fp64", "kernel": "k_rgrid2", "ms_per_launch": ms,
             "algorithmic_flops": flops, "achieved": ach, "peak": pk.value,
             "unit": "TFLOP/s", "frac": ach / pk.value,
+            "traffic": tp * P if tp else None,
             "peak_source": "measured (pofd_fp64_peak DFMA loop)"}
     ms = stages.get("k_r0sum2+k_colspec2")
     if ms:
         nds = len(cfg["maps"])
         nbytes = 16.0 * n * nc * (1 + nds) * P
         ach = nbytes / (ms * 1e-3) / 1e9
+        tp = read_traffic("k_colspec2", per_proposal=True)
         out["roofline_colspec2"] = {
             "bound": "hbm", "kernel": "k_r0sum2+k_colspec2", "ms_per_launch": ms,
             "algorithmic_bytes": nbytes, "achieved": ach, "peak": hbm_peak,
             "unit": "GB/s", "frac": ach / hbm_peak,
+            "traffic": tp * P if tp else None,
             "peak_source": "measured" if "hbm_gbs" in hb else "fallback"}
     return out
 

@@ -25,16 +25,6 @@ int pofd_fp64_peak(int device, double* tflops);
  * its absolute value). */
 int pofd_exp2_check(int device, int n, double lo, double hi, double* max_rel);
 
-/* Self-check of the table-driven e^x and sin / cos of the spectrum kernels
- * (e^x = 2^k T[j] 2^r on x log2(e) split into two doubles; sin and cos by
- * reduction to multiples of 2 pi / 256, a (cos, sin) table and Taylor
- * series) against the CUDA library's, over n arguments spread over
- * [lo, hi): the largest relative error of e^x (absolute below e^-708,
- * where the table form gives 0) and the largest absolute error of sin and
- * cos. */
-int pofd_trig_check(int device, int n, double lo, double hi, double* max_rel_exp,
-                    double* max_abs_sincos);
-
 /* A multivariate Gaussian test likelihood, log N(theta[0:k]; mean, icov^-1)
  * up to a constant (k <= 64), batched on the device with the
  * pofd_batch_loglike_fn signature (pofd_gauss_eval_batch_device; the work

@@ -183,7 +183,6 @@ SIGNATURES = {
 SUPPORT_SIGNATURES = {
     "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
     "pofd_exp2_check": (I, [I, I, D, D, C.POINTER(D)]),
-    "pofd_trig_check": (I, [I, I, D, D, C.POINTER(D), C.POINTER(D)]),
     "pofd_gauss_create": (I, [I, U, _dp, _dp, PV]),
     "pofd_gauss_destroy": (I, [V]),
     "pofd_gauss_eval_batch_device": (I, [V, U, V, U, V, V, V]),

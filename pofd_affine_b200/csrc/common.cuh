@@ -59,78 +59,6 @@ __device__ __forceinline__ double exp2_tab(double x, const double* __restrict__ 
   return (x < -1022.0) ? 0.0 : s;
 }
 
-// e^x by the same table: x log2(e) is formed as y + e with y = RN(x L_hi)
-// and e = (x L_hi - y) + x L_lo (one FMA recovers the product's rounding
-// error; L_hi + L_lo = log2(e) to ~1e-33), so that the reduction
-// 2^(y + e) = 2^k T[j] 2^(r + e) loses nothing to the scaling by log2(e)
-// even at |x| ~ 700.  Arguments below -708 give exactly 0 (the true values
-// are below 2^-1021 and never change the sums they enter); above 708 the
-// library exp is used.
-__device__ __forceinline__ double exp_tab(double x, const double* __restrict__ tab) {
-  if (x > 708.0) return exp(x);
-  const double lhi = 1.4426950408889634, llo = 2.0355273740931033e-17;
-  const double y = x * lhi;
-  const double e = fma(x, lhi, -y) + x * llo;
-  const double sh = 6755399441055744.0;
-  const double t = fma(y, 256.0, sh);
-  const double nd = t - sh;
-  const int n = __double2loint(t);
-  const double r = fma(nd, -0.00390625, y) + e;
-  double p = 9.6181291076284772e-03;
-  p = fma(p, r, 5.5504108664821580e-02);
-  p = fma(p, r, 2.4022650695910071e-01);
-  p = fma(p, r, 6.9314718055994531e-01);
-  p = fma(p, r, 1.0);
-  const double v = p * tab[n & 255];
-  const int k = n >> 8;
-  const double s = __hiloint2double(__double2hiint(v) + (k << 20), __double2loint(v));
-  return (x < -708.0) ? 0.0 : s;
-}
-
-// ------------------------------------------------------------- sin / cos
-// Table-driven sin and cos (the reduction-and-table scheme of Tang's exp
-// applied to the circle): x = k (2 pi / 256) + r, |r| <= pi / 256, with the
-// reduction done in three FMA steps on 2 pi / 256 = C1 + C2 + C3 (Cody and
-// Waite, "Software Manual for the Elementary Functions", 1980; C1 and C2
-// carry 31 significant bits, so k C1 and k C2 are exact for |k| < 2^22);
-// (cos, sin)(2 pi j / 256) for j = k mod 256 from a table built at block
-// start; sin r and cos r - 1 by their Taylor series to r^7 and r^6
-// (truncation < 2e-20); then the angle-sum formulas.  Absolute error a few
-// units of 2^-53.  For |x| > 65536 the library sincos is used.
-struct SinCosTable {
-  double2 t[256];  // (cos, sin)(2 pi j / 256)
-  __device__ __forceinline__ void load() {
-    for (int j = threadIdx.x; j < 256; j += blockDim.x) {
-      double sn, cs;
-      sincospi(static_cast<double>(j) / 128.0, &sn, &cs);
-      t[j] = make_double2(cs, sn);
-    }
-  }
-};
-
-__device__ __forceinline__ void sincos_tab(double x, const double2* __restrict__ tab, double* sn,
-                                           double* cs) {
-  if (!(fabs(x) <= 65536.0)) {
-    sincos(x, sn, cs);
-    return;
-  }
-  const double c1 = 0.024543692605220713, c2 = 9.495469545335112e-13,
-               c3 = -3.9191856348971346e-22, inv = 40.74366543152521;
-  const double sh = 6755399441055744.0;
-  const double t = fma(x, inv, sh);
-  const double kd = t - sh;
-  const int k = __double2loint(t);
-  double r = fma(-kd, c1, x);
-  r = fma(-kd, c2, r);
-  r = fma(-kd, c3, r);
-  const double r2 = r * r;
-  const double sr = fma(r * r2, fma(r2, fma(r2, -1.984126984126984e-04, 8.333333333333333e-03),
-                                    -1.6666666666666666e-01), r);
-  const double cm = r2 * fma(r2, fma(r2, -1.388888888888889e-03, 4.1666666666666664e-02), -0.5);
-  const double2 e = tab[k & 255];
-  *sn = fma(e.y, cm, fma(e.x, sr, e.y));
-  *cs = fma(e.x, cm, fma(-e.y, sr, e.x));
-}
 
 // -------------------------------------------------------------- reductions
 template <int NT>

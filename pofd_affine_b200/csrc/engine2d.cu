@@ -1260,8 +1260,7 @@ __global__ void k_reduce2(const BSet2Dev* __restrict__ bsets,
 // here: each block takes C = 256 / M adjacent columns (M = n / 16 threads
 // per column) into shared memory, runs the forward n-point DFT of every
 // column, forms per bin exp(R~ - R~00) with the shifts and one dataset's
-// noise (the work of k_spectrum2, same formulas; e^x and sin / cos by the
-// table-driven dev::exp_tab and dev::sincos_tab), runs the inverse column
+// noise (the work of k_spectrum2, same formulas), runs the inverse column
 // DFT and writes the columns of that dataset's half spectrum, which batched
 // 1D Z2D row transforms then take to the P(D).  So the spectrum costs no
 // HBM round trip of its own and the column passes of both 2D transforms
@@ -1415,12 +1414,8 @@ k_colspec2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dset
   const int w = wb / B, bsi = wb - w * B;
   if (mstatus[w] != 0) return;
   const int t = threadIdx.x;
-  __shared__ dev::Exp2Table e2;
-  __shared__ dev::SinCosTable sct;
   for (int i = t; i < N / 32 + 32; i += CS_THREADS)
     Hs[i] = (i < N / 32) ? WH[i] : WL[i - N / 32];
-  e2.load();
-  sct.load();
   const int c0 = blockIdx.x * C;      // first column of the block
   const int c = t / M, u = t % M;
   const BSet2Dev& bs = bsets[bsi];
@@ -1469,8 +1464,8 @@ k_colspec2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dset
       if (sh1) ival -= (i1 < nc) ? sf1 * static_cast<double>(i1) : -sf1 * static_cast<double>(N - i1);
       if (sh2) ival -= sf2 * static_cast<double>(i2);
       double sn, cs;
-      dev::sincos_tab(ival, sct.t, &sn, &cs);
-      const double ep = dev::exp_tab((X.x - r0) + nz, e2.t);
+      sincos(ival, &sn, &cs);
+      const double ep = exp((X.x - r0) + nz);
       buf[q] = make_double2(ep * cs, ep * sn);
     }
     for (int cc = 0; cc < C; ++cc) {
@@ -1499,8 +1494,8 @@ k_colspec2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dset
         if (sh1) ival -= sf1 * static_cast<double>(i1);
         if (sh2) ival -= sf2 * didx2;
         double sn, cs;
-        dev::sincos_tab(ival, sct.t, &sn, &cs);
-        const double ep = dev::exp_tab((X.x - r0) + nz, e2.t);
+        sincos(ival, &sn, &cs);
+        const double ep = exp((X.x - r0) + nz);
         if (j1 == i1) {
           b[si] = make_double2(ep * cs, 0.0);
         } else {
@@ -1509,8 +1504,8 @@ k_colspec2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dset
           if (sh1) iq -= -sf1 * static_cast<double>(N - j1);
           if (sh2) iq -= sf2 * didx2;
           double sq, cq;
-          dev::sincos_tab(iq, sct.t, &sq, &cq);
-          const double eq = dev::exp_tab((Xq.x - r0) + nz, e2.t);
+          sincos(iq, &sq, &cq);
+          const double eq = exp((Xq.x - r0) + nz);
           const double2 o = make_double2(0.5 * (ep * cs + eq * cq), 0.5 * (ep * sn - eq * sq));
           b[si] = o;
           b[sj] = make_double2(o.x, -o.y);

@@ -5,8 +5,6 @@
 //                      file carries HBM and BF16 figures only);
 //   * pofd_exp2_check  the table-driven exp2 of the R builders against the
 //                      CUDA library exp2;
-//   * pofd_trig_check  the table-driven e^x and sin / cos of the spectrum
-//                      kernels against the library's;
 //   * pofd_gauss_*     a multivariate Gaussian target with the batched
 //                      likelihood signature, for checking the sampler and
 //                      the surrogate on a known posterior.
@@ -54,39 +52,6 @@ __global__ void k_exp2_check(int n, double lo, double hi, double* __restrict__ o
   }
   worst = pofd::dev::block_max<256>(worst, sh);
   if (threadIdx.x == 0) out[blockIdx.x] = worst;
-}
-
-// The table-driven e^x and sin / cos of the spectrum kernels against the
-// library's, over n arguments spread over [lo, hi) as above: out[2 b] the
-// block's largest relative error of e^x (absolute below e^-708, where the
-// table form gives 0), out[2 b + 1] the largest absolute error of sin and
-// cos.
-__global__ void k_trig_check(int n, double lo, double hi, double* __restrict__ out) {
-  __shared__ pofd::dev::Exp2Table e2;
-  __shared__ pofd::dev::SinCosTable sc;
-  __shared__ double sh[32];
-  e2.load();
-  sc.load();
-  __syncthreads();
-  double we = 0.0, wt = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double u = (static_cast<double>(i) + 0.5 + 0.37 * sin(static_cast<double>(i))) /
-                     static_cast<double>(n);
-    const double x = lo + (hi - lo) * u;
-    const double a = pofd::dev::exp_tab(x, e2.t);
-    const double b = exp(x);
-    we = fmax(we, (x < -708.0) ? fabs(a - b) : fabs(a - b) / b);
-    double s1, c1, s2, c2;
-    pofd::dev::sincos_tab(x, sc.t, &s1, &c1);
-    sincos(x, &s2, &c2);
-    wt = fmax(wt, fmax(fabs(s1 - s2), fabs(c1 - c2)));
-  }
-  we = pofd::dev::block_max<256>(we, sh);
-  wt = pofd::dev::block_max<256>(wt, sh);
-  if (threadIdx.x == 0) {
-    out[2 * blockIdx.x] = we;
-    out[2 * blockIdx.x + 1] = wt;
-  }
 }
 
 constexpr unsigned kMaxDim = 64;
@@ -174,28 +139,6 @@ int pofd_exp2_check(int device, int n, double lo, double hi, double* max_rel) {
   double w = 0.0;
   for (double v : h) w = std::fmax(w, v);
   *max_rel = w;
-  return POFD_OK;
-}
-
-int pofd_trig_check(int device, int n, double lo, double hi, double* max_rel_exp,
-                    double* max_abs_sincos) {
-  if (!max_rel_exp || !max_abs_sincos || n <= 0 || !(lo < hi)) return POFD_E_ARG;
-  if (cudaSetDevice(device) != cudaSuccess) return POFD_E_CUDA;
-  const int blocks = 592;
-  double* d = nullptr;
-  if (cudaMalloc(&d, 2 * blocks * sizeof(double)) != cudaSuccess) return POFD_E_NOMEM;
-  k_trig_check<<<blocks, 256>>>(n, lo, hi, d);
-  double h[2 * blocks];
-  const cudaError_t e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
-  cudaFree(d);
-  if (e != cudaSuccess) return POFD_E_CUDA;
-  double we = 0.0, wt = 0.0;
-  for (int b = 0; b < blocks; ++b) {
-    we = std::fmax(we, h[2 * b]);
-    wt = std::fmax(wt, h[2 * b + 1]);
-  }
-  *max_rel_exp = we;
-  *max_abs_sincos = wt;
   return POFD_OK;
 }
 

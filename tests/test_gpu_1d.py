@@ -232,20 +232,3 @@ def test_table_exp2_against_library(gpu_ctx):
     assert support_lib().pofd_exp2_check(0, 1 << 16, -1100.0, -1022.5, C.byref(out)) == 0
     assert out.value == 0.0
 
-
-def test_table_exp_and_sincos_match_library():
-    """The table-driven e^x and sin / cos of the spectrum kernels against
-    the CUDA library's: e^x within ~5 ulp relative over the exponent range
-    the spectra use (and exactly 0 below -708, absolute error < 1e-307),
-    sin and cos within 5e-16 absolute for |x| up to 65536 (beyond, the
-    library is called)."""
-    import ctypes as C
-    from pofd_affine_b200._lib import support_lib
-    L = support_lib()
-    for lo, hi in ((-745.0, 0.0), (-40.0, 40.0), (-1e-3, 1e-3), (0.0, 708.0),
-                   (-65536.0, 65536.0), (-7.0, 7.0), (60000.0, 70000.0)):
-        re_, ab = C.c_double(), C.c_double()
-        assert L.pofd_trig_check(0, 1 << 22, lo, hi, C.byref(re_), C.byref(ab)) == 0
-        if hi <= 708.0:
-            assert re_.value < 1.2e-15, (lo, hi, re_.value)
-        assert ab.value < 5e-16, (lo, hi, ab.value)
