@@ -75,7 +75,10 @@ class beam:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_beam1_destroy(self.h)
+            try:
+                lib().pofd_beam1_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
     def info(self):
@@ -124,7 +127,10 @@ class PDFactory:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_pdfactory1_destroy(self.h)
+            try:
+                lib().pofd_pdfactory1_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
     def initPD(self, n, minflux, maxflux, knotpos, knotvals, bm):
@@ -169,7 +175,10 @@ class calcLike:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_like1_destroy(self.h)
+            try:
+                lib().pofd_like1_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
     # ---- set-up

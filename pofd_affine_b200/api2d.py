@@ -40,7 +40,10 @@ class doublebeam:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_beam2_destroy(self.h)
+            try:
+                lib().pofd_beam2_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
     def info(self):
@@ -61,7 +64,10 @@ class PDFactoryDouble:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_pdfactory2_destroy(self.h)
+            try:
+                lib().pofd_pdfactory2_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
     def initPD(self, n, minflux1, maxflux1, minflux2, maxflux2, knotpos,
@@ -108,7 +114,10 @@ class calcLikeDouble:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_like2_destroy(self.h)
+            try:
+                lib().pofd_like2_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
     def addBeamSet(self, bm, exp_conf1=0.0, exp_conf2=0.0):

@@ -89,8 +89,11 @@ class gaussLike:
 
     def __del__(self):
         if getattr(self, "h", None):
-            from ._lib import support_lib
-            support_lib().pofd_gauss_destroy(self.h)
+            try:
+                from ._lib import support_lib
+                support_lib().pofd_gauss_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
 
@@ -121,7 +124,10 @@ class likeSum:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_likesum_destroy(self.h)
+            try:
+                lib().pofd_likesum_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
 
@@ -160,7 +166,10 @@ class affineEnsemble:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_ensemble_destroy(self.h)
+            try:
+                lib().pofd_ensemble_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
     # ---------------------------------------------------------- set-up

@@ -114,5 +114,8 @@ class shardedLike:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_shard_destroy(self.h)
+            try:
+                lib().pofd_shard_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None

@@ -56,7 +56,10 @@ class Surrogate:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().pofd_surrogate_destroy(self.h)
+            try:
+                lib().pofd_surrogate_destroy(self.h)
+            except Exception:  # interpreter shutdown: the library is gone
+                pass
             self.h = None
 
     # ------------------------------------------------------------ pairs
