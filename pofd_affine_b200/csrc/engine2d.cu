@@ -271,40 +271,6 @@ k_rows2(const BSet2Dev* __restrict__ bsets, Model2Dev m, int B,
   if (lane == 0) rcnt[static_cast<size_t>(wb) * bs.nrows + r] = make_int2(npos, nneg);
 }
 
-// Sum over a row's compacted term list L[cnt] at column log-flux lf2 (two
-// partial sums over alternate terms: independent exp2 chains overlap).
-__device__ __forceinline__ double term_sum(const double* __restrict__ L, int cnt, double lf2,
-                                           const double* tab) {
-  double wa = 0.0, wb = 0.0;
-  int k = 0;
-#pragma unroll 2
-  for (; k + 1 < cnt; k += 2) {
-    const double ta = lf2 - __ldg(L + 3 * k + 1);
-    const double tb = lf2 - __ldg(L + 3 * k + 4);
-    wa += __ldg(L + 3 * k) * dev::exp2_tab(ta * ta * __ldg(L + 3 * k + 2), tab);
-    wb += __ldg(L + 3 * k + 3) * dev::exp2_tab(tb * tb * __ldg(L + 3 * k + 5), tab);
-  }
-  if (k < cnt) {
-    const double ta = lf2 - __ldg(L + 3 * k + 1);
-    wa += __ldg(L + 3 * k) * dev::exp2_tab(ta * ta * __ldg(L + 3 * k + 2), tab);
-  }
-  return wa + wb;
-}
-
-// R(f1 row, f2 column j) from a row's compacted term lists
-// (numberCountsDoubleLogNormal.cc:1972-2002): (sum_k c0 2^{(log|f2| - c1)^2
-// c2}) / |f2|, over the list of column j's band-2 sign.
-__device__ __forceinline__ double r_at(const BSet2Dev& bs, int sgn1,
-                                       const double* __restrict__ row, int2 nt, int j,
-                                       const double* tab) {
-  if (sgn1 < 0) return 0.0;
-  const double if2 = bs.colinv[j];
-  if (if2 == 0) return 0.0;
-  const int fs = bs.colsgn[j];
-  if (!bs.hassign[sgn1 + fs]) return 0.0;
-  return term_sum(fs ? row + 3 * nt.x : row, fs ? nt.y : nt.x, bs.collog[j], tab) * if2;
-}
-
 // Main R grid, rows 1..n-1 x columns 1..n-1 (row 0 and column 0 are the
 // edge cells), times dflux1*dflux2, with block partial sums of the
 // trapezoid moments of getRStats (PDFactoryDouble.cc:593-722).  A block
@@ -418,8 +384,10 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
 
 // Edge rows (band-1 fluxes below the first grid step) against every main and
 // edge column, weighted by the log-trapezoid factors of the band-1 edge
-// integral (PDFactoryDouble.cc:426-514).  One block per (column tile, group
-// of ER edge rows, proposal x beam set); the group partials are summed in
+// integral (PDFactoryDouble.cc:426-514).  One block per (tile of RG_COLS
+// columns, group of ER edge rows, proposal x beam set), the columns spread
+// over the threads as in k_rgrid2 so that each row's terms are read once per
+// thread for its RG_CPT columns; the group partials are summed in
 // k_rfinish2 into Rx (main columns) and the double integral r[0,0] (edge
 // columns).
 constexpr int ER_MIN = 4;    // fewest edge rows per group (sizes the partials)
@@ -437,42 +405,77 @@ k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   const BSet2Dev& bs = bsets[b];
   const int ncol = n + nedge;
   const int nrows = bs.nrows, ts3 = 3 * bs.Ts;
-  const int j = blockIdx.x * NT + threadIdx.x;
-  const bool jin = j < ncol;
-  double if2 = 0.0, lf2 = 0.0;
-  int fs = 0;
-  if (jin) {
-    if2 = bs.colinv[j];
-    lf2 = bs.collog[j];
-    fs = bs.colsgn[j];
+  const int j0 = blockIdx.x * RG_COLS + threadIdx.x;
+  double if2[RG_CPT], lf2[RG_CPT], acc[RG_CPT];
+  unsigned cpos = 0, cneg = 0;
+#pragma unroll
+  for (int q = 0; q < RG_CPT; ++q) {
+    const int j = j0 + q * NT;
+    if2[q] = 0.0;
+    lf2[q] = 0.0;
+    acc[q] = 0.0;
+    if (j < ncol) {
+      if2[q] = bs.colinv[j];
+      lf2[q] = bs.collog[j];
+      if (if2[q] != 0.0) {
+        if (bs.colsgn[j]) cneg |= 1u << q;
+        else cpos |= 1u << q;
+      }
+    }
   }
   const unsigned hsm = (bs.hassign[0] ? 1u : 0u) | (bs.hassign[1] ? 2u : 0u) |
                        (bs.hassign[2] ? 4u : 0u) | (bs.hassign[3] ? 8u : 0u);
-  double acc = 0.0;
   for (int rr = 0; rr < ER; ++rr) {
     const int i = blockIdx.y * ER + rr;
     if (i >= nedge) break;
     const int r = n + i;
     const int sgn1 = bs.rowsgn[r];
-    if (jin && sgn1 >= 0 && if2 != 0.0 && ((hsm >> (sgn1 + fs)) & 1u)) {
-      const size_t ri = static_cast<size_t>(wb) * nrows + r;
-      const int2 nt = rcnt[ri];
-      const double* L = rw + ri * ts3 + (fs ? 3 * nt.x : 0);
-      const double R = term_sum(L, fs ? nt.y : nt.x, lf2, e2.t) * if2;
-      const double rf = bs.e1[i];
-      acc += ((i == 0 || i == nedge - 1) ? 0.5 : 1.0) * rf * R;
+    if (sgn1 < 0) continue;
+    const size_t ri = static_cast<size_t>(wb) * nrows + r;
+    const int2 nt = rcnt[ri];
+    const double* __restrict__ L = rw + ri * ts3;
+    const double wr = ((i == 0 || i == nedge - 1) ? 0.5 : 1.0) * bs.e1[i];
+    double rs[RG_CPT];
+#pragma unroll
+    for (int q = 0; q < RG_CPT; ++q) rs[q] = 0.0;
+#pragma unroll
+    for (int fs = 0; fs < 2; ++fs) {
+      const unsigned cols = fs ? cneg : cpos;
+      if (!cols || !((hsm >> (sgn1 + fs)) & 1u)) continue;
+      const double* __restrict__ T = fs ? L + 3 * nt.x : L;
+      const int cnt = fs ? nt.y : nt.x;
+      for (int k = 0; k < cnt; ++k) {
+        const double a0 = __ldg(T + 3 * k), a1 = __ldg(T + 3 * k + 1), a2 = __ldg(T + 3 * k + 2);
+#pragma unroll
+        for (int q = 0; q < RG_CPT; ++q) {
+          if (!((cols >> q) & 1u)) continue;
+          const double t = lf2[q] - a1;
+          rs[q] += a0 * dev::exp2_tab(t * t * a2, e2.t);
+        }
+      }
     }
+#pragma unroll
+    for (int q = 0; q < RG_CPT; ++q) acc[q] += wr * (rs[q] * if2[q]);
   }
-  if (j < ncol) epart[(static_cast<size_t>(wb) * gridDim.y + blockIdx.y) * ncol + j] = acc;
+#pragma unroll
+  for (int q = 0; q < RG_CPT; ++q) {
+    const int j = j0 + q * NT;
+    if (j < ncol) epart[(static_cast<size_t>(wb) * gridDim.y + blockIdx.y) * ncol + j] = acc[q];
+  }
 }
 
 // Edge integral along band 2 for column 0 (PDFactoryDouble.cc:518-550):
-// one block per row, threads over the edge band-2 fluxes.
+// one warp per main row (NT / 32 rows per block, so that the exp2 table is
+// built once for several rows), each lane taking edge columns lane, lane +
+// 32, ...: the row's sign, term counts and each term's (c0, c1, c2) are read
+// once per lane for all its columns of one band-2 sign component; a warp
+// reduction gives the row's sum.
+constexpr int RY_ROWS = NT / 32;
+constexpr int RY_CPL = 8;  // edge columns per lane held at once
 __global__ void __launch_bounds__(NT)
 k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
       const int* __restrict__ mstatus, const double* __restrict__ rw,
       const int2* __restrict__ rcnt, double* __restrict__ redge) {
-  __shared__ double shr[32];
   const int wb = blockIdx.y;
   const int w = wb / B, b = wb - w * B;
   if (mstatus[w] != 0) return;
@@ -480,20 +483,63 @@ k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
   e2.load();
   __syncthreads();
   const BSet2Dev& bs = bsets[b];
-  const int r = blockIdx.x + 1;  // main rows 1..n-1
+  const int lane = threadIdx.x & 31;
+  const int r = 1 + blockIdx.x * RY_ROWS + (threadIdx.x >> 5);  // main rows 1..n-1
   if (r >= n) return;
   const int sgn1 = bs.rowsgn[r];
   const size_t ri = static_cast<size_t>(wb) * bs.nrows + r;
-  const double* row = rw + ri * bs.Ts * 3;
+  const double* __restrict__ row = rw + ri * bs.Ts * 3;
   const int2 nt = rcnt[ri];
-  double acc = 0.0;
-  for (int jj = threadIdx.x; jj < nedge; jj += NT) {
-    const double R = r_at(bs, sgn1, row, nt, n + jj, e2.t);
-    acc += (jj == 0 || jj == nedge - 1) ? 0.5 * R : R;
+  const unsigned hsm = (bs.hassign[0] ? 1u : 0u) | (bs.hassign[1] ? 2u : 0u) |
+                       (bs.hassign[2] ? 4u : 0u) | (bs.hassign[3] ? 8u : 0u);
+  double tot = 0.0;
+  for (int c0 = 0; c0 < nedge; c0 += 32 * RY_CPL) {
+    double lf2[RY_CPL], if2[RY_CPL], acc[RY_CPL];
+    unsigned cpos = 0, cneg = 0;
+#pragma unroll
+    for (int q = 0; q < RY_CPL; ++q) {
+      const int jj = c0 + lane + 32 * q;
+      lf2[q] = 0.0;
+      if2[q] = 0.0;
+      acc[q] = 0.0;
+      if (jj < nedge) {
+        const int j = n + jj;
+        if2[q] = bs.colinv[j];
+        lf2[q] = bs.collog[j];
+        if (if2[q] != 0.0) {
+          if (bs.colsgn[j]) cneg |= 1u << q;
+          else cpos |= 1u << q;
+        }
+      }
+    }
+    if (sgn1 >= 0) {
+#pragma unroll
+      for (int fs = 0; fs < 2; ++fs) {
+        const unsigned cols = fs ? cneg : cpos;
+        if (!cols || !((hsm >> (sgn1 + fs)) & 1u)) continue;
+        const double* __restrict__ T = fs ? row + 3 * nt.x : row;
+        const int cnt = fs ? nt.y : nt.x;
+        for (int k = 0; k < cnt; ++k) {
+          const double a0 = __ldg(T + 3 * k), a1 = __ldg(T + 3 * k + 1), a2 = __ldg(T + 3 * k + 2);
+#pragma unroll
+          for (int q = 0; q < RY_CPL; ++q) {
+            if (!((cols >> q) & 1u)) continue;
+            const double t = lf2[q] - a1;
+            acc[q] += a0 * dev::exp2_tab(t * t * a2, e2.t);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < RY_CPL; ++q) {
+      const int jj = c0 + lane + 32 * q;
+      if (jj >= nedge) continue;
+      const double R = acc[q] * if2[q];
+      tot += (jj == 0 || jj == nedge - 1) ? 0.5 * R : R;
+    }
   }
-  acc = dev::block_sum<NT>(acc, shr);
-  if (threadIdx.x == 0)
-    redge[static_cast<size_t>(wb) * (2 * n + 1) + n + r] = acc * bs.iRynorm;
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+  if (lane == 0) redge[static_cast<size_t>(wb) * (2 * n + 1) + n + r] = tot * bs.iRynorm;
 }
 
 // Edge cells into the grid (times dflux1*dflux2), the remaining moment
@@ -2350,7 +2396,7 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
   const int er = tune_.edge_rows;
   const int ngr = (ne + er - 1) / er;
   if (edge_) {
-    const unsigned gxe = static_cast<unsigned>((n + ne + NT - 1) / NT);
+    const unsigned gxe = static_cast<unsigned>((n + ne + RG_COLS - 1) / RG_COLS);
     switch (er) {
       case 4:
         k_redge2<4><<<dim3(gxe, ngr, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw,
@@ -2364,8 +2410,8 @@ void Engine2::launch_all(unsigned nprop, const float* theta, unsigned npar,
         k_redge2<8><<<dim3(gxe, ngr, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw,
                                                           ws_.rcnt, ws_.epart);
     }
-    k_ry2<<<dim3(n - 1, P * B), NT, 0, st>>>(d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.rcnt,
-                                             ws_.redge);
+    k_ry2<<<dim3((n - 1 + RY_ROWS - 1) / RY_ROWS, P * B), NT, 0, st>>>(
+        d_bsets_, B, n, ne, ws_.mstatus, ws_.rw, ws_.rcnt, ws_.redge);
   }
   mark(4);
   {
