@@ -241,8 +241,8 @@ int pofd_like1_fft_info(pofd_like1* L, int* own);
  * threads per block {64, 128, 256}, the R grid fill (rfill_mode 0:
  * materialised, one exp2 per grid point; 1: the same inside the forward FFT
  * pass A, the grid never stored; 2: materialised by running products over
- * runs of <= 16 points in one node interval), spectrum blocks per row
- * {2 ... 32} -- and keeps the
+ * runs of <= 16 points in one node interval; 3: those runs inside the
+ * forward FFT pass A), spectrum blocks per row {2 ... 32} -- and keeps the
  * fastest.  out7 (optional) = {own_fft,
  * rfill_per, rnodes_threads, spec_blocks, rfill_mode, best ms, untuned ms}.
  * get/set_tuning read or impose the five knobs in that order (e.g. a tuning

@@ -721,7 +721,7 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
 // in rbuf -- pass B overwrites rbuf with the spectrum only after
 // k_moments1 has read it.
 
-template <int L1, int L2>
+template <int L1, int L2, bool RUNS>
 __global__ void __launch_bounds__(256, 2)
 k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
         const int* __restrict__ mstatus, const double* __restrict__ spl,
@@ -745,8 +745,10 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
   const int b0 = blockIdx.x * CB;
   const int t = threadIdx.x;
   e2.load();
-  fft::load_tw2(Hs, WH, WL, NH, t, 256);
-  if (L2 > 1 && t < L1 * L2) Ts[t] = fft::tw2<-1>(WH, WL, (m / M1) * (t / L1) * (t % L1));
+  if (!RUNS) {
+    fft::load_tw2(Hs, WH, WL, NH, t, 256);
+    if (L2 > 1 && t < L1 * L2) Ts[t] = fft::tw2<-1>(WH, WL, (m / M1) * (t / L1) * (t % L1));
+  }
   __syncthreads();
   const BSet1Dev& bs = bsets[bset];
   const GridFill1 rg(bs, spl + static_cast<size_t>(row) * 2 * 4 * NI, NI, e2.t);
@@ -758,16 +760,53 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
   double2 v[L1];
   {
     const int b = t % CB, n2 = t / CB;
+    if (RUNS) {
+      // the block's inputs are M1 row segments of 2 CB consecutive grid
+      // points (segment r: [2 (256 r + b0), 2 (256 r + b0 + CB))); the
+      // static runs covering them (bs.aruns, this block's slice) are
+      // evaluated by running products into the padded staging area, which
+      // spans the exchange buffer and the twiddle tables (loaded after)
+      double* stage = reinterpret_cast<double*>(fs);
+      const int2* __restrict__ runs = bs.aruns + bs.arun_off[blockIdx.x];
+      const int nr = bs.arun_off[blockIdx.x + 1] - bs.arun_off[blockIdx.x];
+      for (int k = t; k < nr; k += 256) {
+        const int2 d = __ldg(runs + k);
+        const int len = (d.y >> 2) & 31, kind = d.y & 3, q = (d.y >> 8) - 1;
+        const int o = (d.x >> 9) * (2 * CB) + (d.x & 511) - 2 * b0;
+        if (kind == 2) {
+          rg.run_products(d.x, len, q, stage, o, mn, var);
+        } else if (kind == 1) {
+          for (int e = 0; e < len; ++e) {
+            const int i = d.x + e;
+            stage[GridFill1::pad(o + e)] = rg.point(i, static_cast<double>(i), q, mn, var);
+          }
+        } else {
+          for (int e = 0; e < len; ++e) stage[GridFill1::pad(o + e)] = 0.0;
+        }
+        if (iw >= d.x && iw < d.x + len) Rrow[iw] = stage[GridFill1::pad(o + iw - d.x)];
+      }
+      __syncthreads();
 #pragma unroll
-    for (int n1 = 0; n1 < L1; ++n1) {
-      const int i = 2 * ((L2 * n1 + n2) * M2 + b0 + b);
-      const int2 q = __ldg(reinterpret_cast<const int2*>(gidx + i));
-      const double di = static_cast<double>(i);
-      const double r0 = rg.point(i, di, q.x, mn, var);
-      const double r1 = rg.point(i + 1, di + 1.0, q.y, mn, var);
-      if (i == iw) Rrow[i] = r0;
-      if (i + 1 == iw) Rrow[i + 1] = r1;
-      v[n1] = make_double2(r0, r1);
+      for (int n1 = 0; n1 < L1; ++n1) {
+        const int p = (L2 * n1 + n2) * (2 * CB) + 2 * b;
+        v[n1] = make_double2(stage[GridFill1::pad(p)], stage[GridFill1::pad(p + 1)]);
+      }
+      __syncthreads();
+      fft::load_tw2(Hs, WH, WL, NH, t, 256);
+      if (L2 > 1 && t < L1 * L2) Ts[t] = fft::tw2<-1>(WH, WL, (m / M1) * (t / L1) * (t % L1));
+      __syncthreads();
+    } else {
+#pragma unroll
+      for (int n1 = 0; n1 < L1; ++n1) {
+        const int i = 2 * ((L2 * n1 + n2) * M2 + b0 + b);
+        const int2 q = __ldg(reinterpret_cast<const int2*>(gidx + i));
+        const double di = static_cast<double>(i);
+        const double r0 = rg.point(i, di, q.x, mn, var);
+        const double r1 = rg.point(i + 1, di + 1.0, q.y, mn, var);
+        if (i == iw) Rrow[i] = r0;
+        if (i + 1 == iw) Rrow[i + 1] = r1;
+        v[n1] = make_double2(r0, r1);
+      }
     }
     fft::dft<L1, -1>(v);
     if (L2 > 1) {
@@ -1499,12 +1538,16 @@ void launch_fftA(int m1, int rows, cudaStream_t st, int rowsz, int nrw, const in
 
 // Fused R fill + forward pass A; returns the tiles per row (partial
 // moment sums per row in rpart).
-int launch_fftAR(int m1, int rows, cudaStream_t st, const BSet1Dev* bsets, int B, int NI,
-                 int rowsz, const int* mstatus, const double* spl, double* rbuf, double* rpart,
-                 double2* out, const double2* WH, const double2* WL) {
-#define POFD_FFTAR(L1, L2)                                                                 \
-  k_fftAR<L1, L2><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(bsets, B, NI, rowsz, mstatus, \
-                                                              spl, rbuf, rpart, out, WH, WL); \
+int launch_fftAR(int m1, bool runs, int rows, cudaStream_t st, const BSet1Dev* bsets, int B,
+                 int NI, int rowsz, const int* mstatus, const double* spl, double* rbuf,
+                 double* rpart, double2* out, const double2* WH, const double2* WL) {
+#define POFD_FFTAR(L1, L2)                                                                  \
+  if (runs)                                                                                 \
+    k_fftAR<L1, L2, true><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(                      \
+        bsets, B, NI, rowsz, mstatus, spl, rbuf, rpart, out, WH, WL);                       \
+  else                                                                                      \
+    k_fftAR<L1, L2, false><<<dim3(L2, rows), 256, fftA_smem(m1), st>>>(                     \
+        bsets, B, NI, rowsz, mstatus, spl, rbuf, rpart, out, WH, WL);                       \
   return L2
   switch (m1) {
     case 8: POFD_FFTAR(8, 1);
@@ -1518,14 +1561,20 @@ int launch_fftAR(int m1, int rows, cudaStream_t st, const BSet1Dev* bsets, int B
 #undef POFD_FFTAR
 }
 
-void fftAR_attr() {
+template <bool RUNS>
+void fftAR_attr_runs() {
   const int sm = static_cast<int>(kFftASmemMax);
-  cuda_check(cudaFuncSetAttribute(k_fftAR<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
-  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<8, 1, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 1, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 4, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 8, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+  cuda_check(cudaFuncSetAttribute(k_fftAR<16, 16, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
+}
+
+void fftAR_attr() {
+  fftAR_attr_runs<false>();
+  fftAR_attr_runs<true>();
 }
 
 template <int S>
@@ -1770,7 +1819,7 @@ void Engine1::free_static() {
 // and their spline factorisation, grid ranges, binned data.
 unsigned Engine1::fill_tiles() const {
   const unsigned pts = NT * static_cast<unsigned>(tune_.rfill_per);
-  return tune_.rfill_mode == 2 ? runblk_ : (n_ + pts - 1) / pts;
+  return tune_.rfill_mode >= 2 ? runblk_ : (n_ + pts - 1) / pts;
 }
 
 void Engine1::build_static() {
@@ -1967,6 +2016,35 @@ void Engine1::build_static() {
       bd.runs = reinterpret_cast<const int2*>(upi(runs));
       const unsigned nb = (static_cast<unsigned>(bd.nruns) + NT - 1) / NT;
       if (nb > runblk_) runblk_ = nb;
+      // the same cut, per block of the own FFT's forward pass A (R fill
+      // mode 3): block bx's inputs are its M1 row segments of 2 CB
+      // consecutive grid points, [2 (256 r + bx CB), 2 (256 r + bx CB + CB))
+      bd.aruns = nullptr;
+      bd.arun_off = nullptr;
+      if (n >= 4096 && n <= 131072 && (n & (n - 1)) == 0) {
+        const int m1 = n / 512;
+        const int L2 = (m1 == 8) ? 1 : m1 / 16, CB = 256 / L2;
+        std::vector<int> ar, off(L2 + 1);
+        for (int bx = 0; bx < L2; ++bx) {
+          off[bx] = static_cast<int>(ar.size() / 2);
+          for (int r = 0; r < m1; ++r) {
+            const int s0 = 2 * (256 * r + bx * CB), s1 = s0 + 2 * CB;
+            for (int i = s0; i < s1;) {
+              const int q = gidx[i];
+              const bool neg = i > wrap;
+              int j = i + 1;
+              while (j < s1 && j - i < 16 && gidx[j] == q && (j > wrap) == neg) ++j;
+              const int len = j - i;
+              ar.push_back(i);
+              ar.push_back(((q + 1) << 8) | (len << 2) | (q < 0 ? 0 : (len >= 4 ? 2 : 1)));
+              i = j;
+            }
+          }
+        }
+        off[L2] = static_cast<int>(ar.size() / 2);
+        bd.aruns = reinterpret_cast<const int2*>(upi(ar));
+        bd.arun_off = upi(off);
+      }
     }
     bd.ds_begin = static_cast<int>(h_dsets_.size());
     bd.nds = static_cast<int>(s.data.size());
@@ -2107,7 +2185,7 @@ void Engine1::set_tuning(const Tune1& t) {
   if (t.rnodes_threads != 64 && t.rnodes_threads != 128 && t.rnodes_threads != 256)
     throw Error(POFD_E_ARG, "rnodes_threads must be 64, 128 or 256");
   if (t.spec_blocks < 1 || t.spec_blocks > 64) throw Error(POFD_E_ARG, "spec_blocks must be in [1, 64]");
-  if (t.rfill_mode < 0 || t.rfill_mode > 2) throw Error(POFD_E_ARG, "rfill_mode must be 0, 1 or 2");
+  if (t.rfill_mode < 0 || t.rfill_mode > 3) throw Error(POFD_E_ARG, "rfill_mode must be 0 ... 3");
   const bool fft_changed = (t.own_fft != 0) != (tune_.own_fft != 0);
   tune_ = t;
   tune_.own_fft = t.own_fft ? 1 : 0;
@@ -2153,7 +2231,7 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     trial(t);
   }
   if (best.own_fft && own_possible) {
-    for (int rf : {0, 1, 2}) {
+    for (int rf : {0, 1, 2, 3}) {
       if (rf == best.rfill_mode) continue;
       Tune1 t = best;
       t.rfill_mode = rf;
@@ -2425,11 +2503,11 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
     int ntile = static_cast<int>(ntile_);
     if (fused) {
       // R fill inside the forward pass A: the grid goes straight into tmp
-      ntile = launch_fftAR(m1, P * B, st, d_bsets_, B, NI, rowsz, ws_.mstatus, ws_.spl,
-                           ws_.rbuf, ws_.rpart, tmp, d_wh_, d_wl_);
+      ntile = launch_fftAR(m1, tune_.rfill_mode == 3, P * B, st, d_bsets_, B, NI, rowsz,
+                           ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart, tmp, d_wh_, d_wl_);
     } else {
       dim3 grid(ntile_, P * B);
-      launch_rfill(tune_.rfill_per, tune_.rfill_mode == 2, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+      launch_rfill(tune_.rfill_per, tune_.rfill_mode >= 2, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
@@ -2458,7 +2536,7 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
   } else {
     {
       dim3 grid(ntile_, P * B);
-      launch_rfill(tune_.rfill_per, tune_.rfill_mode == 2, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
+      launch_rfill(tune_.rfill_per, tune_.rfill_mode >= 2, grid, st, d_bsets_, B, n, NI, nc2, static_cast<int>(ntile_),
                    ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
     }
     mark(3);
@@ -2704,7 +2782,7 @@ void Engine1::rgrid_host(int bs, const float* theta, unsigned npar, double* out)
       d_bsets_, model_, B, NI, maxterms_, ws_.cnt, ws_.mstatus, ws_.nodes);
   k_rspline1<kSplineThreads><<<B * 2, kSplineThreads, (2 * static_cast<size_t>(NI) + 64) * sizeof(double), stream_>>>(
       d_bsets_, B, NI, ws_.mstatus, ws_.nodes, ws_.spl);
-  launch_rfill(tune_.rfill_per, tune_.rfill_mode == 2, dim3(ntile_, B), stream_, d_bsets_, B, n,
+  launch_rfill(tune_.rfill_per, tune_.rfill_mode >= 2, dim3(ntile_, B), stream_, d_bsets_, B, n,
                NI, nc2, static_cast<int>(ntile_), ws_.mstatus, ws_.spl, ws_.rbuf, ws_.rpart);
   cuda_check(cudaGetLastError(), "rgrid kernels");
   cuda_check(cudaMemcpyAsync(out, ws_.rbuf + static_cast<size_t>(bs) * nc2, n_ * sizeof(double),

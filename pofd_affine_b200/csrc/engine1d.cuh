@@ -56,6 +56,9 @@ struct BSet1Dev {
                         // | len << 2 | kind (0 uncovered, 1 point by point,
                         // 2 running products)
   int nruns;
+  const int2* aruns;    // the same cut per block of the forward pass A
+  const int* arun_off;  // (own FFT sizes): block bx's runs are
+                        // aruns[arun_off[bx] .. arun_off[bx + 1])
 };
 
 struct DSet1Dev {
@@ -140,7 +143,8 @@ struct Tune1 {
                             // point; 1 the same inside the forward FFT pass
                             // A (own FFT), the grid never stored; 2
                             // materialised by running products over runs
-                            // of <= 16 points in one node interval
+                            // of <= 16 points in one node interval; 3 the
+                            // runs inside the forward pass A (own FFT)
 };
 
 class Engine1 {
@@ -184,7 +188,7 @@ class Engine1 {
   }
   // the R grid fill runs inside the forward FFT pass A (own FFT, plain passes)
   bool fused_fill() const {
-    return own_fft_ && tune_.rfill_mode == 1;
+    return own_fft_ && (tune_.rfill_mode == 1 || tune_.rfill_mode == 3);
   }
   // priors (calcLike::setSigmaPrior / setCFIRBPrior / setPoissonPrior /
   // setRegularizationAlpha and their unset forms, calcLike.h:251-269)

@@ -103,8 +103,9 @@ def test_pd_and_r_grid_match_oracle(orc, gpu_ctx, beams, case):
     assert abs(pf.minflux - io["pd_minflux"]) <= 1e-10 * abs(io["pd_minflux"])
     # every R fill: one exp2 per point (materialised, or inside the forward
     # FFT pass A), and by running products over runs of one node interval
+    # (materialised, or inside the forward pass A)
     d0 = G.getTuning()["rfill_mode"]
-    for mode in (0, 1, 2):
+    for mode in (0, 1, 2, 3):
         G.setTuning(rfill_mode=mode)
         rg = G.getR(0, s["th"])
         assert np.max(np.abs(rg - ro)) <= 1e-12 * ro.max(), mode

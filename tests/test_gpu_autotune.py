@@ -31,7 +31,7 @@ def _setup(orc, ctx, n=8192):
                                          ("rnodes_threads", [64, 128, 256]),
                                          ("spec_blocks", [1, 2, 32]),
                                          ("own_fft", [0, 1]),
-                                         ("rfill_mode", [0, 1, 2])])
+                                         ("rfill_mode", [0, 1, 2, 3])])
 def test_every_knob_value_keeps_parity(orc, gpu_ctx, knob, values):
     L, O, th = _setup(orc, gpu_ctx)
     lo, _ = O.loglike_batch(th, 4)
@@ -51,7 +51,7 @@ def test_autotune_picks_from_the_candidates(orc, gpu_ctx):
     assert r["rnodes_threads"] in (64, 128, 256)
     assert r["spec_blocks"] in (1, 2, 4, 8, 16, 32)
     assert r["own_fft"] in (0, 1)
-    assert r["rfill_mode"] in (0, 1, 2)
+    assert r["rfill_mode"] in (0, 1, 2, 3)
     assert 0 < r["ms"] <= r["untuned_ms"]
     assert L.getTuning() == {k: r[k] for k in L.TUNING_KEYS}
     after, st = L.getLogLikeBatch(th)
