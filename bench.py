@@ -56,7 +56,7 @@ def args():
                    help="skip the walker-sharded ensemble run (N > 1)")
     p.add_argument("--mcmc-2d", type=int, default=1,
                    help="include the two-field 2D MCMC comparison")
-    p.add_argument("--mcmc-steps", type=int, default=1500,
+    p.add_argument("--mcmc-steps", type=int, default=3000,
                    help="recorded steps of each 2D MCMC run")
     p.add_argument("--profile-case", choices=["1d", "2d", "surrogate"],
                    help="run a small fixed workload for a profiler and exit "
@@ -780,7 +780,7 @@ def cpu_mcmc_1d(nthreads=None, nburn=200, nsteps=500, nwalkers=40):
             "ess_per_s_likelihood_only": ess / t_like[0]}
 
 
-def mcmc_2d(ctx, nsteps=1500):
+def mcmc_2d(ctx, nsteps=3000):
     """Plain vs delayed acceptance on the two-field 2D fit (2048^2 and
     1024^2 grids in one launch, 14 free parameters, 128 walkers), from a
     shared equilibrated start, with a plain-vs-plain control
