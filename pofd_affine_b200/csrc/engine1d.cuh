@@ -139,7 +139,7 @@ struct Tune1 {
   int rfill_per = 8;        // R grid points per thread of k_rfill1 (4, 8, 16)
   int rnodes_threads = 128; // threads per block of k_rnodes1 (64, 128, 256)
   int spec_blocks = 4;      // blocks per row of k_spectrum1f (2 ... 32)
-  int rfill_mode = 2;       // R grid fill: 0 materialised, one exp2 per grid
+  int rfill_mode = 3;       // R grid fill: 0 materialised, one exp2 per grid
                             // point; 1 the same inside the forward FFT pass
                             // A (own FFT), the grid never stored; 2
                             // materialised by running products over runs

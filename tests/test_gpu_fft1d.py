@@ -32,12 +32,13 @@ def test_own_fft_matches_cufft(orc, gpu_ctx, n):
     ok = so == 0
     assert np.max(np.abs(lo[ok] - lc[ok])) < 1e-7
     # the default R grid fill (running products over runs of one node
-    # interval) against the others -- one exp2 per point materialised or
-    # inside the forward pass A, the runs inside the forward pass A: values
-    # within ~1e-13 relative, moments grouped differently
+    # interval, inside the forward pass A) against the others -- one exp2
+    # per point materialised or inside the forward pass A, the runs
+    # materialised: values within ~1e-13 relative, moments grouped
+    # differently
     d0 = L.getTuning()["rfill_mode"]
-    assert d0 == 2
-    for rf in (0, 1, 3):
+    assert d0 == 3
+    for rf in (0, 1, 2):
         L.setTuning(rfill_mode=rf)
         lu, su = L.getLogLikeBatch(th)
         pu, iu = L.getPD(1, 0, th[0], setLog=False)
