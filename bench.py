@@ -348,16 +348,22 @@ def stage_bytes(stage, P, B, D, n, cuts=None):
     }.get(stage)
 
 
-def stage_flops(stage, P, B, n):
+def stage_flops(stage, P, B, n, rfill_mode=3):
     """Algorithmic FP64 flops per launch of the FP64-bound R-grid stages.
-    An R grid point costs 35 (grid flux and interval offset 3, the cubic 6,
-    the table exp2 21, the dflux scale 1, the two moment terms 4); every
-    grid point is counted (the R range, hence the grid, is set to the span
-    the spline covers).  A complex element of the fused forward pass A adds
-    5 log2(m1) (its m1-point DFT) + 12 (the inter-stage and outgoing
-    twiddle products)."""
+    One exp2 per point (fill modes 0 and 1): 35 per grid point (grid flux
+    and interval offset 3, the cubic 6, the table exp2 21, the dflux scale
+    1, the two moment terms 4).  Running products over runs of <= 16 points
+    (modes 2 and 3): 8 per point (three products, the grid flux and the
+    moment terms) plus, per run, the cubic's value and three differences at
+    its first point (≈ 29) and four table exp2 (84), counted for full
+    16-point runs -- 15 per point, a lower bound (runs cut at node
+    intervals are shorter).  Every grid point is counted (the R range, hence
+    the grid, is set to the span the spline covers).  A complex element of
+    the fused forward pass A adds 5 log2(m1) (its m1-point DFT) + 12 (the
+    inter-stage and outgoing twiddle products)."""
     m = n // 2
-    rpts = 35.0 * n * P * B
+    per_pt = 35.0 if rfill_mode in (0, 1) else 8.0 + 113.0 / 16.0
+    rpts = per_pt * n * P * B
     if stage == "k_rfill1":
         return rpts
     if stage == "k_fftAR1":
@@ -914,7 +920,8 @@ def main():
     peak_src = "measured" if "hbm_gbs" in hb else "fallback"
     cuts = noise_cuts(L, cfg, cfg["theta0"]) if L.ownFFT() else None
     nbytes = stage_bytes(dom, BATCH, B, D, n, cuts)
-    nflops = stage_flops(dom, BATCH, B, n)
+    rmode = L.getTuning()["rfill_mode"]
+    nflops = stage_flops(dom, BATCH, B, n, rmode)
     if nflops is not None:
         # FP64-bound R grid fill (fused with the forward pass A): algorithmic
         # FP64 flops against the measured FP64 FMA peak
@@ -925,7 +932,9 @@ def main():
                 "achieved": ach, "peak": pk.value, "unit": "TFLOP/s",
                 "frac": ach / pk.value,
                 "peak_source": "measured (pofd_fp64_peak DFMA loop)",
-                "algorithmic_flops": nflops, "traffic": read_traffic(dom)}
+                "algorithmic_flops": nflops,
+                # the run-based fills have their own captures
+                "traffic": read_traffic(dom + ("@runs" if rmode >= 2 else ""))}
     elif nbytes is not None:
         ach = nbytes / (own[dom] * 1e-3) / 1e9
         traffic = read_traffic(dom)
@@ -945,7 +954,7 @@ def main():
                 "traffic": read_traffic(dom)}
     # the longest HBM-bound stage beside it (the dominant one is FP64 bound)
     hbm_stages = {k: v for k, v in own.items()
-                  if stage_flops(k, BATCH, B, n) is None
+                  if stage_flops(k, BATCH, B, n, rmode) is None
                   and stage_bytes(k, BATCH, B, D, n, cuts) is not None}
     roof_hbm = None
     if hbm_stages:
