@@ -242,18 +242,16 @@ int pofd_like1_fft_info(pofd_like1* L, int* own);
  * materialised, one exp2 per grid point; 1: the same inside the forward FFT
  * pass A, the grid never stored; 2: materialised by running products over
  * runs of <= 16 points in one node interval; 3: those runs inside the
- * forward FFT pass A), spectrum blocks per row {2 ... 32}, R at the nodes
- * (rnodes_mode 0: one thread per node over the beam terms; 1: running
- * products along runs of nodes per term, for beams of <= 64 terms per
- * side) -- and keeps the fastest.  out8 (optional) = {own_fft, rfill_per,
- * rnodes_threads, spec_blocks, rfill_mode, rnodes_mode, best ms, untuned
- * ms}.  get/set_tuning read or impose the six knobs in that order (e.g. a
- * tuning saved from an earlier run).  Results change only by rounding
- * (reduction grouping, FFT implementation, exponential evaluation). */
+ * forward FFT pass A), spectrum blocks per row {2 ... 32} -- and keeps the
+ * fastest.  out7 (optional) = {own_fft,
+ * rfill_per, rnodes_threads, spec_blocks, rfill_mode, best ms, untuned ms}.
+ * get/set_tuning read or impose the five knobs in that order (e.g. a tuning
+ * saved from an earlier run).  Results change only by rounding (reduction
+ * grouping, FFT implementation, exponential evaluation). */
 int pofd_like1_autotune(pofd_like1* L, unsigned nprop, const float* theta,
-                        unsigned npar, int reps, double* out8);
-int pofd_like1_get_tuning(const pofd_like1* L, int* knobs6);
-int pofd_like1_set_tuning(pofd_like1* L, const int* knobs6);
+                        unsigned npar, int reps, double* out7);
+int pofd_like1_get_tuning(const pofd_like1* L, int* knobs5);
+int pofd_like1_set_tuning(pofd_like1* L, const int* knobs5);
 
 /* Priors added once to the summed log-likelihood, in the reference's order
  * (calcLike.cc:918-952): a Gaussian on the sigma multiplier about 1, on <S>

@@ -392,7 +392,7 @@ class calcLike:
         return th[0] if one else th
 
     TUNING_KEYS = ("own_fft", "rfill_per", "rnodes_threads", "spec_blocks",
-                   "rfill_mode", "rnodes_mode")
+                   "rfill_mode")
 
     def autotune(self, thetas, reps=20):
         """Choose the launch shapes by timing the graph-captured launch
@@ -401,13 +401,12 @@ class calcLike:
         th = np.ascontiguousarray(_f32(thetas))
         if th.ndim != 2:
             raise PofdError(-10, "thetas must be [nprop, npar]")
-        nk = len(self.TUNING_KEYS)
-        out = np.zeros(nk + 2)
+        out = np.zeros(7)
         check(lib().pofd_like1_autotune(self.h, th.shape[0], th.ravel(),
                                         th.shape[1], int(reps),
                                         out.ctypes.data_as(C.c_void_p)))
-        d = {k: int(v) for k, v in zip(self.TUNING_KEYS, out[:nk])}
-        d["ms"], d["untuned_ms"] = float(out[nk]), float(out[nk + 1])
+        d = {k: int(v) for k, v in zip(self.TUNING_KEYS, out[:5])}
+        d["ms"], d["untuned_ms"] = float(out[5]), float(out[6])
         return d
 
     def getTuning(self):

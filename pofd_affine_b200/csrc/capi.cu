@@ -548,40 +548,38 @@ int pofd_like1_fft_info(pofd_like1* L, int* own) {
 }
 
 int pofd_like1_autotune(pofd_like1* L, unsigned nprop, const float* theta, unsigned npar,
-                        int reps, double* out8) {
+                        int reps, double* out7) {
   return guard([&] {
     need(L && theta, "null argument");
     need(L->ctx->device >= 0, "host-only context has no GPU");
     cudaSetDevice(L->ctx->device);
-    L->eng->autotune(nprop, theta, npar, reps, out8);
+    L->eng->autotune(nprop, theta, npar, reps, out7);
     return POFD_OK;
   });
 }
 
-int pofd_like1_get_tuning(const pofd_like1* L, int* knobs6) {
+int pofd_like1_get_tuning(const pofd_like1* L, int* knobs5) {
   return guard([&] {
-    need(L && knobs6, "null argument");
+    need(L && knobs5, "null argument");
     const pofd::Tune1& t = L->eng->tuning();
-    knobs6[0] = t.own_fft;
-    knobs6[1] = t.rfill_per;
-    knobs6[2] = t.rnodes_threads;
-    knobs6[3] = t.spec_blocks;
-    knobs6[4] = t.rfill_mode;
-    knobs6[5] = t.rnodes_mode;
+    knobs5[0] = t.own_fft;
+    knobs5[1] = t.rfill_per;
+    knobs5[2] = t.rnodes_threads;
+    knobs5[3] = t.spec_blocks;
+    knobs5[4] = t.rfill_mode;
     return POFD_OK;
   });
 }
 
-int pofd_like1_set_tuning(pofd_like1* L, const int* knobs6) {
+int pofd_like1_set_tuning(pofd_like1* L, const int* knobs5) {
   return guard([&] {
-    need(L && knobs6, "null argument");
+    need(L && knobs5, "null argument");
     pofd::Tune1 t;
-    t.own_fft = knobs6[0];
-    t.rfill_per = knobs6[1];
-    t.rnodes_threads = knobs6[2];
-    t.spec_blocks = knobs6[3];
-    t.rfill_mode = knobs6[4];
-    t.rnodes_mode = knobs6[5];
+    t.own_fft = knobs5[0];
+    t.rfill_per = knobs5[1];
+    t.rnodes_threads = knobs5[2];
+    t.spec_blocks = knobs5[3];
+    t.rfill_mode = knobs5[4];
     L->eng->set_tuning(t);
     return POFD_OK;
   });

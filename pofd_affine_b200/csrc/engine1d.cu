@@ -196,87 +196,6 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
   nodes[static_cast<size_t>(row) * NI + i] = bs.prefac * workval;
 }
 
-// R at the interpolation nodes by running products (rnodes_mode 1).  The
-// nodes are log-spaced, so for one beam term j the spline argument
-// log2|x_i| + log2(1/eta_j) advances by the constant step h = +-dif from node
-// to node, and on one knot interval log2 n is a cubic in the node index:
-// 2^cubic follows from three running products (as in the R grid fill), four
-// exp2 per run instead of one per node.  A static work list per chunk of
-// RN_CH nodes holds (first node, term, run length <= 16, knot interval)
-// items for the valid nodes whose arguments lie in the knot range (the rest
-// contribute 0); each item's values w_j eta_j^-1 n(...) go to the shared
-// table val[term][node], and each node sums its column in term order (the
-// reference's order, numberCountsKnotsSpline.cc:495-526).  Used when every
-// side has at most RN_TMAX terms (histogrammed beams); else k_rnodes1.
-constexpr int RN_CH = 64;
-constexpr int RN_TMAX = 64;
-constexpr int RN_THREADS = 128;
-__global__ void __launch_bounds__(RN_THREADS)
-k_rnodes1r(const BSet1Dev* __restrict__ bsets, Model1Dev m, int B, int NI,
-           const double* __restrict__ cnt, const int* __restrict__ mstatus,
-           double* __restrict__ nodes) {
-  __shared__ double val[RN_TMAX * RN_CH];
-  __shared__ double s_lk[KMAX], s_cs[4 * KMAX], s_wie[RN_TMAX], s_le[RN_TMAX];
-  __shared__ dev::Exp2Table e2;
-  const int row = blockIdx.y;  // (w*B + b)*2 + side
-  const int side = row & 1;
-  const int wb = row >> 1;
-  const int w = wb / B, b = wb - w * B;
-  const BSet1Dev& bs = bsets[b];
-  const Side1Dev& sd = bs.side[side];
-  if (!sd.nodes || mstatus[w] != 0) return;
-  const int t = threadIdx.x;
-  const int K = m.K, nt = sd.nterms;
-  const double* cs = cnt + static_cast<size_t>(w) * 4 * KMAX;
-  for (int i = t; i < K; i += RN_THREADS) s_lk[i] = m.logknots[i];
-  for (int i = t; i < 4 * (K - 1); i += RN_THREADS) s_cs[i] = cs[i];
-  for (int j = t; j < nt; j += RN_THREADS) {
-    s_wie[j] = sd.w[j] * sd.ieta[j];
-    s_le[j] = sd.lie[j];
-  }
-  for (int i = t; i < nt * RN_CH; i += RN_THREADS) val[i] = 0.0;
-  e2.load();
-  __syncthreads();
-  const int c = blockIdx.x, i0 = c * RN_CH;
-  const int nn = min(RN_CH, NI - i0);
-  const double h = sd.lstep;
-  const int q1 = sd.rn_off[c + 1];
-  for (int q = sd.rn_off[c] + t; q < q1; q += RN_THREADS) {
-    const int2 d = __ldg(sd.rn_items + q);
-    const int i = d.x & 0xffff, j = d.x >> 16;
-    const int len = (d.y & 255) + 1, k = d.y >> 8;
-    const double* cc = s_cs + 4 * k;
-    double* out = val + j * RN_CH + (i - i0);
-    const double d0 = (__ldg(sd.lxa + i) + s_le[j]) - s_lk[k];
-    const double v0 = cc[0] + d0 * (cc[1] + d0 * (cc[2] + d0 * cc[3]));
-    const double D1 = h * (cc[1] + cc[2] * (2.0 * d0 + h) + cc[3] * (3.0 * d0 * (d0 + h) + h * h));
-    const double D2 = h * h * (2.0 * cc[2] + 6.0 * cc[3] * (d0 + h));
-    const double D3 = 6.0 * cc[3] * h * h * h;
-    if (fabs(v0) < 500.0 && fabs(D1) < 16.0 && fabs(D2) < 4.0 && fabs(D3) < 2.0) {
-      double R = dev::exp2_tab(v0, e2.t) * s_wie[j];
-      double E1 = dev::exp2_tab(D1, e2.t), E2 = dev::exp2_tab(D2, e2.t);
-      const double E3 = dev::exp2_tab(D3, e2.t);
-      for (int e = 0; e < len; ++e) {
-        out[e] = R;
-        R *= E1;
-        E1 *= E2;
-        E2 *= E3;
-      }
-    } else {
-      for (int e = 0; e < len; ++e) {
-        const double de = (__ldg(sd.lxa + i + e) + s_le[j]) - s_lk[k];
-        out[e] = s_wie[j] * dev::exp2_tab(cc[0] + de * (cc[1] + de * (cc[2] + de * cc[3])), e2.t);
-      }
-    }
-  }
-  __syncthreads();
-  for (int e = t; e < nn; e += RN_THREADS) {
-    double acc = 0.0;
-    for (int j = 0; j < nt; ++j) acc += val[j * RN_CH + e];
-    nodes[static_cast<size_t>(row) * NI + i0 + e] = bs.prefac * acc;
-  }
-}
-
 // Natural cubic spline through (x_i, log2 R_i) over the NI nodes: RHS of
 // the tridiagonal system, forward and back substitution against the
 // precomputed LDL^T factors as two block-wide affine-map scans, then the
@@ -1898,22 +1817,6 @@ void Engine1::free_static() {
 
 // Upload the parameter-independent data: beam terms, interpolation nodes
 // and their spline factorisation, grid ranges, binned data.
-// R at the nodes of `rows` (proposal, beam set, side) rows: the running-
-// product form where every side's terms fit (rnodes_mode 1), else one
-// thread per node.
-void Engine1::launch_rnodes(unsigned rows, cudaStream_t st) {
-  const int B = static_cast<int>(B_), NI = static_cast<int>(ninterp_);
-  if (tune_.rnodes_mode == 1 && rn_ok_) {
-    k_rnodes1r<<<dim3((NI + RN_CH - 1) / RN_CH, rows), RN_THREADS, 0, st>>>(
-        d_bsets_, model_, B, NI, ws_.cnt, ws_.mstatus, ws_.nodes);
-    return;
-  }
-  const size_t smem = (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double);
-  const int th = tune_.rnodes_threads;
-  k_rnodes1<<<dim3((NI + th - 1) / th, rows), th, smem, st>>>(d_bsets_, model_, B, NI, maxterms_,
-                                                              ws_.cnt, ws_.mstatus, ws_.nodes);
-}
-
 unsigned Engine1::fill_tiles() const {
   const unsigned pts = NT * static_cast<unsigned>(tune_.rfill_per);
   return tune_.rfill_mode >= 2 ? runblk_ : (n_ + pts - 1) / pts;
@@ -1925,7 +1828,6 @@ void Engine1::build_static() {
   free_static();
   if (sets_.empty()) throw Error(POFD_E_ARG, "no beam sets");
   runblk_ = 0;
-  rn_ok_ = true;
   auto up = [&](const std::vector<double>& v) -> const double* {
     double* p = dalloc<double>(v.size() ? v.size() : 1);
     static_allocs_.push_back(p);
@@ -2005,7 +1907,6 @@ void Engine1::build_static() {
         maxi -= dinterp;
         const double dif = (std::log2(maxi / mini)) * ininterpm1;
         for (unsigned i = 0; i < NI; ++i) x[i] = mini * std::exp2(static_cast<double>(i) * dif);
-        sd.lstep = dif;
       } else {
         double maxi = -knots_.front() * subedgemult;
         double mini = -knots_.back() * s.bm.maxneg();
@@ -2015,7 +1916,6 @@ void Engine1::build_static() {
         const double dif = (std::log2(mini / maxi)) * ininterpm1;
         for (unsigned i = 0; i < NI; ++i)
           x[i] = maxi * std::exp2(static_cast<double>(NI - i - 1) * dif);
-        sd.lstep = -dif;
       }
       SplineSystem sys;
       sys.factor(x);
@@ -2053,43 +1953,6 @@ void Engine1::build_static() {
         static_allocs_.push_back(d);
         cuda_check(cudaMemcpy(d, kt.data(), kt.size(), cudaMemcpyHostToDevice), "upload");
         sd.kidx = d;
-        // running-product work items (rnodes_mode 1): per chunk of RN_CH
-        // nodes, for every term in order, runs of <= 16 nodes that are
-        // inside the model's R range and share one knot interval
-        sd.rn_items = nullptr;
-        sd.rn_off = nullptr;
-        if (nt <= static_cast<size_t>(RN_TMAX) && NI < 65536) {
-          auto valid = [&](unsigned i) {
-            const double f = sys.x[i];
-            return side == 0 ? (f > 0 && s.bm.haspos && f <= bd.rr_hi)
-                             : (s.bm.hasneg && f < 0 && f >= bd.rr_lo);
-          };
-          const unsigned nch = (NI + RN_CH - 1) / RN_CH;
-          std::vector<int> items, off(nch + 1);
-          for (unsigned c = 0; c < nch; ++c) {
-            off[c] = static_cast<int>(items.size() / 2);
-            const unsigned i0 = c * RN_CH, i1 = std::min<unsigned>(NI, i0 + RN_CH);
-            for (size_t j = 0; j < nt; ++j) {
-              for (unsigned i = i0; i < i1;) {
-                const unsigned char k = kt[j * NI + i];
-                if (k == 255 || !valid(i)) {
-                  ++i;
-                  continue;
-                }
-                unsigned e = i + 1;
-                while (e < i1 && e - i < 16 && kt[j * NI + e] == k && valid(e)) ++e;
-                items.push_back(static_cast<int>(i | (j << 16)));
-                items.push_back(static_cast<int>((e - i - 1) | (static_cast<unsigned>(k) << 8)));
-                i = e;
-              }
-            }
-          }
-          off[nch] = static_cast<int>(items.size() / 2);
-          sd.rn_items = reinterpret_cast<const int2*>(upi(items));
-          sd.rn_off = upi(off);
-        } else {
-          rn_ok_ = false;
-        }
       }
       sd.nodes = 1;
       sd.nterms = static_cast<int>(tie.size());
@@ -2323,7 +2186,6 @@ void Engine1::set_tuning(const Tune1& t) {
     throw Error(POFD_E_ARG, "rnodes_threads must be 64, 128 or 256");
   if (t.spec_blocks < 1 || t.spec_blocks > 64) throw Error(POFD_E_ARG, "spec_blocks must be in [1, 64]");
   if (t.rfill_mode < 0 || t.rfill_mode > 3) throw Error(POFD_E_ARG, "rfill_mode must be 0 ... 3");
-  if (t.rnodes_mode != 0 && t.rnodes_mode != 1) throw Error(POFD_E_ARG, "rnodes_mode must be 0 or 1");
   const bool fft_changed = (t.own_fft != 0) != (tune_.own_fft != 0);
   tune_ = t;
   tune_.own_fft = t.own_fft ? 1 : 0;
@@ -2335,7 +2197,7 @@ void Engine1::set_tuning(const Tune1& t) {
 // Coordinate descent over the knobs, one pass, each candidate timed on the
 // captured graph of the whole sequence.  The FFT choice is tried only where
 // the own FFT supports the size.
-void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out8) {
+void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7) {
   NvtxRange nvtx_range("pofd like1 autotune");
   if (nprop == 0 || reps < 1) throw Error(POFD_E_ARG, "autotune needs rows and reps >= 1");
   if (!static_ok_ || ws_.P < nprop) reserve(std::max(nprop, ws_.P));
@@ -2362,19 +2224,11 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     t.rfill_per = per;
     trial(t);
   }
-  for (int rn : {0, 1}) {
-    if (rn == best.rnodes_mode) continue;
+  for (int th : {64, 128, 256}) {
+    if (th == best.rnodes_threads) continue;
     Tune1 t = best;
-    t.rnodes_mode = rn;
+    t.rnodes_threads = th;
     trial(t);
-  }
-  if (best.rnodes_mode == 0 || !rn_ok_) {
-    for (int th : {64, 128, 256}) {
-      if (th == best.rnodes_threads) continue;
-      Tune1 t = best;
-      t.rnodes_threads = th;
-      trial(t);
-    }
   }
   if (best.own_fft && own_possible) {
     for (int rf : {0, 1, 2, 3}) {
@@ -2393,15 +2247,14 @@ void Engine1::autotune(unsigned nprop, const float* theta, unsigned npar, int re
     }
   }
   set_tuning(best);
-  if (out8) {
-    out8[0] = best.own_fft;
-    out8[1] = best.rfill_per;
-    out8[2] = best.rnodes_threads;
-    out8[3] = best.spec_blocks;
-    out8[4] = best.rfill_mode;
-    out8[5] = best.rnodes_mode;
-    out8[6] = best_ms;
-    out8[7] = t_untuned;
+  if (out7) {
+    out7[0] = best.own_fft;
+    out7[1] = best.rfill_per;
+    out7[2] = best.rnodes_threads;
+    out7[3] = best.spec_blocks;
+    out7[4] = best.rfill_mode;
+    out7[5] = best_ms;
+    out7[6] = t_untuned;
   }
 }
 
@@ -2626,7 +2479,13 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
     k_bonus1<<<P, kBonusThreads, 0, st>>>(model_, const_cast<float*>(theta), static_cast<int>(npar),
                                           std::log2(10.0), ws_.cnt, ws_.mstatus, d_qu_, d_qs_,
                                           d_qw_, qper_, ws_.bonus, -1);
-  launch_rnodes(P * B * 2, st);
+  {
+    const size_t smem = (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double);
+    const int th = tune_.rnodes_threads;
+    dim3 grid((NI + th - 1) / th, P * B * 2);
+    k_rnodes1<<<grid, th, smem, st>>>(d_bsets_, model_, B, NI, maxterms_,
+                                      ws_.cnt, ws_.mstatus, ws_.nodes);
+  }
   mark(1);
   {
     const size_t smem = (2 * static_cast<size_t>(NI) + 64) * sizeof(double);
@@ -2918,7 +2777,9 @@ void Engine1::rgrid_host(int bs, const float* theta, unsigned npar, double* out)
   const int B = static_cast<int>(B_);
   k_model1<<<1, 32, 0, stream_>>>(model_, ws_.theta_in, static_cast<int>(npar),
                                   std::log2(10.0), ws_.cnt, ws_.mstatus, ws_.sigmult);
-  launch_rnodes(B * 2, stream_);
+  k_rnodes1<<<dim3((NI + 127) / 128, B * 2), 128,
+              (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double), stream_>>>(
+      d_bsets_, model_, B, NI, maxterms_, ws_.cnt, ws_.mstatus, ws_.nodes);
   k_rspline1<kSplineThreads><<<B * 2, kSplineThreads, (2 * static_cast<size_t>(NI) + 64) * sizeof(double), stream_>>>(
       d_bsets_, B, NI, ws_.mstatus, ws_.nodes, ws_.spl);
   launch_rfill(tune_.rfill_per, tune_.rfill_mode >= 2, dim3(ntile_, B), stream_, d_bsets_, B, n,

@@ -39,11 +39,6 @@ struct Side1Dev {
                               // node i (255: outside the knot range)
   int grid_lo, grid_hi; // inclusive grid index range filled from this side
   double grid_off;      // grid flux = i*dflux + grid_off
-  double lstep;         // log2|x| step from node i to i + 1
-  const int2* rn_items; // running-product work items of the nodes (NULL:
-  const int* rn_off;    // too many terms), per chunk of 64 nodes: chunk c
-                        // holds rn_items[rn_off[c] .. rn_off[c + 1]),
-                        // x = node | term << 16, y = (len - 1) | interval << 8
 };
 
 struct BSet1Dev {
@@ -144,9 +139,6 @@ struct Tune1 {
   int rfill_per = 8;        // R grid points per thread of k_rfill1 (4, 8, 16)
   int rnodes_threads = 128; // threads per block of k_rnodes1 (64, 128, 256)
   int spec_blocks = 4;      // blocks per row of k_spectrum1f (2 ... 32)
-  int rnodes_mode = 1;      // R at the nodes: 0 one thread per node over the
-                            // terms; 1 running products along runs of nodes
-                            // per term (beams of <= 64 terms per side)
   int rfill_mode = 3;       // R grid fill: 0 materialised, one exp2 per grid
                             // point; 1 the same inside the forward FFT pass
                             // A (own FFT), the grid never stored; 2
@@ -210,13 +202,12 @@ class Engine1 {
   // fastest; out (optional) receives {own_fft, rfill_per, rnodes_threads,
   // spec_blocks, rfill_mode, best ms per launch, untuned ms per
   // launch}.
-  void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out8);
+  void autotune(unsigned nprop, const float* theta, unsigned npar, int reps, double* out7);
   const Tune1& tuning() const { return tune_; }
   // grid points per thread of the materialised R fill
   // blocks per row of the materialised R fill: PER points per thread, or
   // (running products) NT runs per block
   unsigned fill_tiles() const;
-  void launch_rnodes(unsigned rows, cudaStream_t st);
   void set_tuning(const Tune1& t);
   // <S>, <S^2> of each proposal's model (calcLike::fillBonusParams,
   // calcLike.cc:958-980): host rows -> out[nprop][2]
@@ -270,7 +261,6 @@ class Engine1 {
   unsigned B_ = 0, D_ = 0;
   unsigned ntile_ = 0, nchunk_ = 0;
   unsigned runblk_ = 0;  // most run blocks of any beam set's grid
-  bool rn_ok_ = true;    // every side has node work items (rnodes_mode 1)
   int maxterms_ = 1;
   // work space
   Workspace1 ws_;

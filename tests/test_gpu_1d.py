@@ -56,18 +56,13 @@ def test_r_nodes_match_oracle(orc, gpu_ctx, beams):
         s = _spec(beam_pix=bp, ps=ps, nh=nh)
         O, G = _build(orc, gpu_ctx, s)
         sides = [False, True] if bp is not None else [False]
-        # both node forms: one thread per node over the terms, and running
-        # products along runs of nodes per term (histogrammed beams; a raw
-        # beam's many terms fall back to the first form)
-        for mode in (0, 1):
-            G.setTuning(rnodes_mode=mode)
-            for neg in sides:
-                xo, ro = O.rinterp(0, s["th"], s["ni"], neg)
-                xg, rg = G.getRNodes(0, s["th"], s["ni"], neg)
-                assert np.array_equal(xo, xg)
-                assert np.array_equal(ro == 0, rg == 0)
-                nz = ro > 0
-                assert np.max(np.abs(rg[nz] / ro[nz] - 1)) < 1e-12, (mode, neg)
+        for neg in sides:
+            xo, ro = O.rinterp(0, s["th"], s["ni"], neg)
+            xg, rg = G.getRNodes(0, s["th"], s["ni"], neg)
+            assert np.array_equal(xo, xg)
+            assert np.array_equal(ro == 0, rg == 0)
+            nz = ro > 0
+            assert np.max(np.abs(rg[nz] / ro[nz] - 1)) < 1e-12
 
 
 @pytest.mark.parametrize("case", ["hist", "raw", "neg", "n3000", "lownoise"])

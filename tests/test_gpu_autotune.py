@@ -31,8 +31,7 @@ def _setup(orc, ctx, n=8192):
                                          ("rnodes_threads", [64, 128, 256]),
                                          ("spec_blocks", [1, 2, 32]),
                                          ("own_fft", [0, 1]),
-                                         ("rfill_mode", [0, 1, 2, 3]),
-                                         ("rnodes_mode", [0, 1])])
+                                         ("rfill_mode", [0, 1, 2, 3])])
 def test_every_knob_value_keeps_parity(orc, gpu_ctx, knob, values):
     L, O, th = _setup(orc, gpu_ctx)
     lo, _ = O.loglike_batch(th, 4)
