@@ -1325,7 +1325,6 @@ __global__ void k_reduce2(const BSet2Dev* __restrict__ bsets,
 // those slots and end in natural order.  Twiddles W_n^j, j < n, come from
 // two shared tables H[j >> 5] L[j & 31] built on the host in long double.
 constexpr int CS_THREADS = 256;
-constexpr int CS_UNR = 4;  // spectrum bins per thread evaluated together
 
 __host__ __device__ constexpr int cs_slots(int n) { return 256 * (n / 256 + 1); }
 inline size_t colspec_smem(int n) {
@@ -1492,43 +1491,28 @@ k_colspec2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dset
     const bool noisy = (s1 > 0 || s2 > 0);
     const double sf1n = -0.5 * s1 * s1 * iflux1 * iflux1;
     const double sf2n = -0.5 * s2 * s2 * iflux2 * iflux2;
-    // CS_UNR slots per thread at a time, branch free up to the stores: the
-    // exp and sincos of the CS_UNR bins are independent chains the compiler
-    // can interleave (padding slots and bins outside this block's columns
-    // compute on zeros and are not stored)
-    for (int q0 = t; q0 < C * SL; q0 += CS_THREADS * CS_UNR) {
-      double2 X[CS_UNR];
-      double iv[CS_UNR], ex[CS_UNR];
-      bool act[CS_UNR], zer[CS_UNR];
-#pragma unroll
-      for (int r = 0; r < CS_UNR; ++r) {
-        const int q = q0 + r * CS_THREADS;
-        const int cc = q / SL, pos = q % SL;
-        const int pr = pos / (M3 + 1), k3 = pos % (M3 + 1);
-        const int i2 = c0 + cc;
-        act[r] = q < C * SL && k3 != M3 && i2 < nc && i2 != 0 && i2 != N / 2;
-        const int i1 = (pr >> 4) + 16 * ((pr & 15) + 16 * k3);
-        const double didx1 = (i1 < nc) ? static_cast<double>(i1) : static_cast<double>(N - i1);
-        const double didx2 = static_cast<double>(i2);
-        const double nz = noisy ? sf1n * didx1 * didx1 + sf2n * didx2 * didx2 : 0.0;
-        zer[r] = noisy && nz < -750.0;  // exactly 0 in the reference
-        X[r] = act[r] ? buf[q] : make_double2(0.0, 0.0);
-        double ival = X[r].y;
-        if (sh1) ival -= (i1 < nc) ? sf1 * static_cast<double>(i1) : -sf1 * static_cast<double>(N - i1);
-        if (sh2) ival -= sf2 * didx2;
-        iv[r] = act[r] ? ival : 0.0;
-        ex[r] = (act[r] && !zer[r]) ? (X[r].x - r0) + nz : 0.0;
+#pragma unroll 4
+    for (int q = t; q < C * SL; q += CS_THREADS) {
+      const int cc = q / SL, pos = q % SL;
+      const int pr = pos / (M3 + 1), k3 = pos % (M3 + 1);
+      const int i2 = c0 + cc;
+      if (k3 == M3 || i2 >= nc || i2 == 0 || i2 == N / 2) continue;
+      const int i1 = (pr >> 4) + 16 * ((pr & 15) + 16 * k3);
+      const double didx1 = (i1 < nc) ? static_cast<double>(i1) : static_cast<double>(N - i1);
+      const double didx2 = static_cast<double>(i2);
+      const double nz = noisy ? sf1n * didx1 * didx1 + sf2n * didx2 * didx2 : 0.0;
+      if (noisy && nz < -750.0) {  // exactly 0 in the reference
+        buf[q] = make_double2(0.0, 0.0);
+        continue;
       }
-#pragma unroll
-      for (int r = 0; r < CS_UNR; ++r) {
-        double sn, cs;
-        sincos(iv[r], &sn, &cs);
-        const double ep = exp(ex[r]);
-        X[r] = make_double2(ep * cs, ep * sn);
-      }
-#pragma unroll
-      for (int r = 0; r < CS_UNR; ++r)
-        if (act[r]) buf[q0 + r * CS_THREADS] = zer[r] ? make_double2(0.0, 0.0) : X[r];
+      const double2 X = buf[q];
+      double ival = X.y;
+      if (sh1) ival -= (i1 < nc) ? sf1 * static_cast<double>(i1) : -sf1 * static_cast<double>(N - i1);
+      if (sh2) ival -= sf2 * static_cast<double>(i2);
+      double sn, cs;
+      sincos(ival, &sn, &cs);
+      const double ep = exp((X.x - r0) + nz);
+      buf[q] = make_double2(ep * cs, ep * sn);
     }
     for (int cc = 0; cc < C; ++cc) {
       const int i2 = c0 + cc;
