@@ -23,6 +23,7 @@
 // batched cuFFT calls over P*B and P*D rows.
 #include "engine1d.cuh"
 
+#include <algorithm>
 #include <cstring>
 #include <sstream>
 
@@ -767,10 +768,10 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
       // evaluated by running products into the padded staging area, which
       // spans the exchange buffer and the twiddle tables (loaded after)
       double* stage = reinterpret_cast<double*>(fs);
-      const int2* __restrict__ runs = bs.aruns + bs.arun_off[blockIdx.x];
-      const int nr = bs.arun_off[blockIdx.x + 1] - bs.arun_off[blockIdx.x];
-      for (int k = t; k < nr; k += 256) {
-        const int2 d = __ldg(runs + k);
+      const int* __restrict__ toff = bs.arun_off + blockIdx.x * 257;
+      const int k1 = toff[t + 1];
+      for (int k = toff[t]; k < k1; ++k) {
+        const int2 d = __ldg(bs.aruns + k);
         const int len = (d.y >> 2) & 31, kind = d.y & 3, q = (d.y >> 8) - 1;
         const int o = (d.x >> 9) * (2 * CB) + (d.x & 511) - 2 * b0;
         if (kind == 2) {
@@ -2024,9 +2025,15 @@ void Engine1::build_static() {
       if (n >= 4096 && n <= 131072 && (n & (n - 1)) == 0) {
         const int m1 = n / 512;
         const int L2 = (m1 == 8) ? 1 : m1 / 16, CB = 256 / L2;
-        std::vector<int> ar, off(L2 + 1);
+        // each block's runs are dealt to its 256 threads longest first onto
+        // the least loaded thread (estimated cost: a running-product run
+        // ~100 instructions + 12 per point, a point-by-point run 60 per
+        // point, a zero run 2 per point), then stored in thread order:
+        // thread t of block bx takes aruns[arun_off[bx * 257 + t] ..
+        // arun_off[bx * 257 + t + 1])
+        std::vector<int> ar, off(static_cast<size_t>(L2) * 257);
         for (int bx = 0; bx < L2; ++bx) {
-          off[bx] = static_cast<int>(ar.size() / 2);
+          std::vector<std::pair<int, int>> blk;  // (first index, packed)
           for (int r = 0; r < m1; ++r) {
             const int s0 = 2 * (256 * r + bx * CB), s1 = s0 + 2 * CB;
             for (int i = s0; i < s1;) {
@@ -2035,13 +2042,37 @@ void Engine1::build_static() {
               int j = i + 1;
               while (j < s1 && j - i < 16 && gidx[j] == q && (j > wrap) == neg) ++j;
               const int len = j - i;
-              ar.push_back(i);
-              ar.push_back(((q + 1) << 8) | (len << 2) | (q < 0 ? 0 : (len >= 4 ? 2 : 1)));
+              blk.push_back({i, ((q + 1) << 8) | (len << 2) | (q < 0 ? 0 : (len >= 4 ? 2 : 1))});
               i = j;
             }
           }
+          auto cost = [](int packed) {
+            const int len = (packed >> 2) & 31, kind = packed & 3;
+            return kind == 2 ? 100 + 12 * len : (kind == 1 ? 60 * len : 2 * len);
+          };
+          std::vector<int> order(blk.size());
+          for (size_t k = 0; k < order.size(); ++k) order[k] = static_cast<int>(k);
+          std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return cost(blk[a].second) > cost(blk[b].second);
+          });
+          std::vector<std::vector<int>> per(256);
+          std::vector<long> load(256, 0);
+          for (int k : order) {
+            int tmin = 0;
+            for (int t2 = 1; t2 < 256; ++t2)
+              if (load[t2] < load[tmin]) tmin = t2;
+            per[tmin].push_back(k);
+            load[tmin] += cost(blk[k].second);
+          }
+          for (int t2 = 0; t2 < 256; ++t2) {
+            off[static_cast<size_t>(bx) * 257 + t2] = static_cast<int>(ar.size() / 2);
+            for (int k : per[t2]) {
+              ar.push_back(blk[k].first);
+              ar.push_back(blk[k].second);
+            }
+          }
+          off[static_cast<size_t>(bx) * 257 + 256] = static_cast<int>(ar.size() / 2);
         }
-        off[L2] = static_cast<int>(ar.size() / 2);
         bd.aruns = reinterpret_cast<const int2*>(upi(ar));
         bd.arun_off = upi(off);
       }

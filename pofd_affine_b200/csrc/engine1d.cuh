@@ -57,8 +57,9 @@ struct BSet1Dev {
                         // 2 running products)
   int nruns;
   const int2* aruns;    // the same cut per block of the forward pass A
-  const int* arun_off;  // (own FFT sizes): block bx's runs are
-                        // aruns[arun_off[bx] .. arun_off[bx + 1])
+  const int* arun_off;  // (own FFT sizes), balanced over the block's 256
+                        // threads: thread t of block bx takes aruns[
+                        // arun_off[257 bx + t] .. arun_off[257 bx + t + 1])
 };
 
 struct DSet1Dev {
