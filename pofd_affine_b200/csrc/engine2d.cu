@@ -1476,23 +1476,11 @@ k_colspec2(const BSet2Dev* __restrict__ bsets, const DSet2Dev* __restrict__ dset
   for (int dd = 0; dd < bs.nds; ++dd) {
     const int d = bs.ds_begin + dd;
     const DSet2Dev& ds = dsets[d];
-    // load the C columns (a warp covers 32 / C rows of C adjacent columns);
-    // every load of the thread is issued before the first store to shared
-    // memory, so their latencies overlap
-    {
-      constexpr int PER = C * N / CS_THREADS;
-      double2 ld[PER];
-#pragma unroll
-      for (int k = 0; k < PER; ++k) {
-        const int e = t + k * CS_THREADS;
-        const int i1 = e / C, i2 = c0 + e % C;
-        ld[k] = (i2 < nc) ? Y[static_cast<size_t>(i1) * nc + i2] : make_double2(0.0, 0.0);
-      }
-#pragma unroll
-      for (int k = 0; k < PER; ++k) {
-        const int e = t + k * CS_THREADS;
-        buf[(e % C) * SL + e / C] = ld[k];
-      }
+    // load the C columns (a warp covers 32 / C rows of C adjacent columns)
+    for (int e = t; e < C * N; e += CS_THREADS) {
+      const int i1 = e / C, cc = e % C;
+      const int i2 = c0 + cc;
+      buf[cc * SL + i1] = (i2 < nc) ? Y[static_cast<size_t>(i1) * nc + i2] : make_double2(0.0, 0.0);
     }
     __syncthreads();
     cs_forward<N>(buf, Hs, Ls, c, u);
