@@ -376,79 +376,6 @@ struct GridFill1 {
       out[pad(o + k)] = point(i, static_cast<double>(i), q, mn, var);
     }
   }
-  // The state of a run's running products at its first point (R, E1, E2,
-  // E3 as in run_products); false when its exponents leave the safe range.
-  __device__ __forceinline__ bool run_start(int i0, int q, double& R, double& E1, double& E2,
-                                            double& E3) const {
-    const bool neg = i0 > wrap;
-    const double2* S = reinterpret_cast<const double2*>(S0 + (neg ? 4 * NI : 0)) + 2 * q;
-    const double2 yb = S[0], cd = S[1];
-    const double h = dflux;
-    const double d0 = __dadd_rn(__dmul_rn(static_cast<double>(i0), dflux), neg ? off1 : off0) -
-                      (neg ? x1 : x0)[q];
-    const double v0 = yb.x + d0 * (yb.y + d0 * (cd.x + d0 * cd.y));
-    const double D1 = h * (yb.y + cd.x * (2.0 * d0 + h) + cd.y * (3.0 * d0 * (d0 + h) + h * h));
-    const double D2 = h * h * (2.0 * cd.x + 6.0 * cd.y * (d0 + h));
-    const double D3 = 6.0 * cd.y * h * h * h;
-    if (!(fabs(v0) < 500.0 && fabs(D1) < 16.0 && fabs(D2) < 4.0 && fabs(D3) < 2.0)) return false;
-    R = dev::exp2_tab(v0, e2) * dflux;
-    E1 = dev::exp2_tab(D1, e2);
-    E2 = dev::exp2_tab(D2, e2);
-    E3 = dev::exp2_tab(D3, e2);
-    return true;
-  }
-  // Two runs (i0a, lena) and (i0b, lenb) advanced in the same loop, so that
-  // their product chains overlap; each keeps its own moment sums, added to
-  // mn, var at the end (run_products' arithmetic otherwise).  Runs whose
-  // exponents leave the safe range go through run_products.
-  __device__ __forceinline__ void run_products2(int i0a, int lena, int qa, int oa, int i0b,
-                                                int lenb, int qb, int ob, double* out,
-                                                double& mn, double& var) const {
-    double Ra, E1a, E2a, E3a, Rb, E1b, E2b, E3b;
-    const bool oka = run_start(i0a, qa, Ra, E1a, E2a, E3a);
-    const bool okb = run_start(i0b, qb, Rb, E1b, E2b, E3b);
-    if (!oka || !okb) {
-      run_products(i0a, lena, qa, out, oa, mn, var);
-      run_products(i0b, lenb, qb, out, ob, mn, var);
-      return;
-    }
-    const bool nega = i0a > wrap, negb = i0b > wrap;
-    const double cba = nega ? minflux_R : 0.0, cbb = negb ? minflux_R : 0.0;
-    const int iba = nega ? wrap + 1 : 0, ibb = negb ? wrap + 1 : 0;
-    double mna = 0.0, vara = 0.0, mnb = 0.0, varb = 0.0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      if (k >= lena && k >= lenb) break;
-      if (k < lena) {
-        const int i = i0a + k;
-        out[pad(oa + k)] = Ra;
-        const double cf = nega ? static_cast<double>(i - iba) * dflux + cba
-                               : __dmul_rn(static_cast<double>(i), dflux);
-        double prod = cf * Ra;
-        if (i == wrap) prod *= 0.5;
-        mna += prod;
-        vara += cf * prod;
-        Ra *= E1a;
-        E1a *= E2a;
-        E2a *= E3a;
-      }
-      if (k < lenb) {
-        const int i = i0b + k;
-        out[pad(ob + k)] = Rb;
-        const double cf = negb ? static_cast<double>(i - ibb) * dflux + cbb
-                               : __dmul_rn(static_cast<double>(i), dflux);
-        double prod = cf * Rb;
-        if (i == wrap) prod *= 0.5;
-        mnb += prod;
-        varb += cf * prod;
-        Rb *= E1b;
-        E1b *= E2b;
-        E2b *= E3b;
-      }
-    }
-    mn += mna + mnb;
-    var += vara + varb;
-  }
   // shared tile index of span offset j: one pad word per 16 values, so that
   // threads starting runs ~16 values apart do not share a bank
   __device__ __forceinline__ static int pad(int j) { return j + (j >> 4); }
@@ -843,22 +770,7 @@ k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
       double* stage = reinterpret_cast<double*>(fs);
       const int* __restrict__ toff = bs.arun_off + blockIdx.x * 257;
       const int k1 = toff[t + 1];
-      int k = toff[t];
-      // two running-product runs at a time where the thread has them (each
-      // thread's runs are stored with those first)
-      for (; k + 1 < k1; k += 2) {
-        const int2 da = __ldg(bs.aruns + k), db = __ldg(bs.aruns + k + 1);
-        if ((da.y & 3) != 2 || (db.y & 3) != 2) break;
-        const int oa = (da.x >> 9) * (2 * CB) + (da.x & 511) - 2 * b0;
-        const int ob = (db.x >> 9) * (2 * CB) + (db.x & 511) - 2 * b0;
-        rg.run_products2(da.x, (da.y >> 2) & 31, (da.y >> 8) - 1, oa, db.x, (db.y >> 2) & 31,
-                         (db.y >> 8) - 1, ob, stage, mn, var);
-        if (iw >= da.x && iw < da.x + ((da.y >> 2) & 31))
-          Rrow[iw] = stage[GridFill1::pad(oa + iw - da.x)];
-        if (iw >= db.x && iw < db.x + ((db.y >> 2) & 31))
-          Rrow[iw] = stage[GridFill1::pad(ob + iw - db.x)];
-      }
-      for (; k < k1; ++k) {
+      for (int k = toff[t]; k < k1; ++k) {
         const int2 d = __ldg(bs.aruns + k);
         const int len = (d.y >> 2) & 31, kind = d.y & 3, q = (d.y >> 8) - 1;
         const int o = (d.x >> 9) * (2 * CB) + (d.x & 511) - 2 * b0;
@@ -2154,9 +2066,6 @@ void Engine1::build_static() {
           }
           for (int t2 = 0; t2 < 256; ++t2) {
             off[static_cast<size_t>(bx) * 257 + t2] = static_cast<int>(ar.size() / 2);
-            // running-product runs first: the kernel advances them in pairs
-            std::stable_partition(per[t2].begin(), per[t2].end(),
-                                  [&](int k) { return (blk[k].second & 3) == 2; });
             for (int k : per[t2]) {
               ar.push_back(blk[k].first);
               ar.push_back(blk[k].second);
