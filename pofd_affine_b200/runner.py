@@ -64,7 +64,7 @@ def run_plain(E, nburn, nsteps):
 
 def run_da(E, S, nburn, nsteps, train_iters=2000, batch=512, lr=1e-3,
            refresh=5000, refresh_iters=400, chunk=25, holdout=None,
-           da_scale=0.0):
+           da_scale=0.0, refresh_decay=False):
     """Burn-in with exact evaluations collected as training pairs, train,
     then delayed-acceptance steps in chunks, retraining on all pairs held
     after every `refresh` new exact evaluations.  The timed region includes
@@ -99,7 +99,11 @@ def run_da(E, S, nburn, nsteps, train_iters=2000, batch=512, lr=1e-3,
         if st["exact_evals"] - last >= refresh and done < nsteps:
             t1 = time.perf_counter()
             trained_on = S.nPairs()
-            S.train(refresh_iters, batch, lr)
+            # with refresh_decay the k-th retraining uses lr / (k + 1): the
+            # surrogate -- hence the first-stage kernel -- changes less and
+            # less (diminishing adaptation)
+            S.train(refresh_iters, batch,
+                    lr / (nrefresh + 1) if refresh_decay else lr)
             t_train += time.perf_counter() - t1
             last = st["exact_evals"]
             nrefresh += 1
