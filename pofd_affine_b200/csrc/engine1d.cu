@@ -158,15 +158,17 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
   const int K = m.K;
   double* s_lk = sm;
   double* s_cs = s_lk + KMAX;
-  double* s_wie = s_cs + 4 * KMAX;  // w_j eta_j^-1
-  double* s_le = s_wie + maxterms;
+  double* s_w = s_cs + 4 * KMAX;
+  double* s_le = s_w + maxterms;
+  double* s_ie = s_le + maxterms;
   const double* cs = cnt + static_cast<size_t>(w) * 4 * KMAX;
   for (int i = threadIdx.x; i < K; i += blockDim.x) s_lk[i] = m.logknots[i];
   for (int i = threadIdx.x; i < 4 * (K - 1); i += blockDim.x) s_cs[i] = cs[i];
   const int nt = sd.nterms;
   for (int i = threadIdx.x; i < nt; i += blockDim.x) {
-    s_wie[i] = sd.w[i] * sd.ieta[i];
+    s_w[i] = sd.w[i];
     s_le[i] = sd.lie[i];
+    s_ie[i] = sd.ieta[i];
   }
   __shared__ dev::Exp2Table e2;
   e2.load();
@@ -186,10 +188,10 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
       const int k = kt[static_cast<size_t>(j) * NI];
       if (k == 255) continue;
       const double delx = (lf + s_le[j]) - s_lk[k];
-      const double2* q = reinterpret_cast<const double2*>(s_cs) + 2 * k;
-      const double2 q01 = q[0], q23 = q[1];
-      workval += s_wie[j] *
-                 dev::exp2_tab(q01.x + delx * (q01.y + delx * (q23.x + delx * q23.y)), e2.t);
+      const double* q = s_cs + 4 * k;
+      const double cts =
+          dev::exp2_tab(q[0] + delx * (q[1] + delx * (q[2] + delx * q[3])), e2.t);
+      if (cts > 0) workval += s_w[j] * cts * s_ie[j];
     }
   }
   nodes[static_cast<size_t>(row) * NI + i] = bs.prefac * workval;
@@ -2456,7 +2458,7 @@ void Engine1::reserve(unsigned P) {
   ws_.logl = dalloc<double>(P + (P + 1) / 2);
   ws_.status = reinterpret_cast<int*>(ws_.logl + P);
   cuda_check(cudaFuncSetAttribute(k_rnodes1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>((KMAX + 4 * KMAX + 2 * MAXTERMS) * sizeof(double))),
+                                  static_cast<int>((KMAX + 4 * KMAX + 3 * MAXTERMS) * sizeof(double))),
              "smem attribute");
   cuda_check(cudaFuncSetAttribute(k_rspline1<kSplineThreads>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2509,7 +2511,7 @@ void Engine1::launch_all(unsigned nprop, const float* theta, unsigned npar,
                                           std::log2(10.0), ws_.cnt, ws_.mstatus, d_qu_, d_qs_,
                                           d_qw_, qper_, ws_.bonus, -1);
   {
-    const size_t smem = (KMAX + 4 * KMAX + 2 * static_cast<size_t>(maxterms_)) * sizeof(double);
+    const size_t smem = (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double);
     const int th = tune_.rnodes_threads;
     dim3 grid((NI + th - 1) / th, P * B * 2);
     k_rnodes1<<<grid, th, smem, st>>>(d_bsets_, model_, B, NI, maxterms_,
@@ -2807,7 +2809,7 @@ void Engine1::rgrid_host(int bs, const float* theta, unsigned npar, double* out)
   k_model1<<<1, 32, 0, stream_>>>(model_, ws_.theta_in, static_cast<int>(npar),
                                   std::log2(10.0), ws_.cnt, ws_.mstatus, ws_.sigmult);
   k_rnodes1<<<dim3((NI + 127) / 128, B * 2), 128,
-              (KMAX + 4 * KMAX + 2 * static_cast<size_t>(maxterms_)) * sizeof(double), stream_>>>(
+              (KMAX + 4 * KMAX + 3 * static_cast<size_t>(maxterms_)) * sizeof(double), stream_>>>(
       d_bsets_, model_, B, NI, maxterms_, ws_.cnt, ws_.mstatus, ws_.nodes);
   k_rspline1<kSplineThreads><<<B * 2, kSplineThreads, (2 * static_cast<size_t>(NI) + 64) * sizeof(double), stream_>>>(
       d_bsets_, B, NI, ws_.mstatus, ws_.nodes, ws_.spl);
