@@ -933,6 +933,14 @@ def main():
                 "frac": ach / pk.value,
                 "peak_source": "measured (pofd_fp64_peak DFMA loop)",
                 "algorithmic_flops": nflops,
+                "flops_basis": ("R fill by running products: 15 FP64 flops per "
+                                "grid point (three products, grid flux and moment "
+                                "terms, per-run set-up amortised)"
+                                if rmode >= 2 else
+                                "R fill with one table exp2 per grid point: 35 "
+                                "FP64 flops per point")
+                               + ("; plus the pass-A DFT, 5 log2(m1) + 12 per "
+                                  "complex element" if dom == "k_fftAR1" else ""),
                 # the run-based fills have their own captures
                 "traffic": read_traffic(dom + ("@runs" if rmode >= 2 else ""))}
     elif nbytes is not None:
