@@ -677,6 +677,9 @@ def mcmc_1d(ctx, cpu=True):
     L = synth.build_like1(cfg, ctx)
     npar = cfg["theta0"].size
     nk = npar - 1
+    # launch shapes for the half-ensemble batches the runs evaluate (at this
+    # size cuFFT can beat the own FFT)
+    tuning = L.autotune(synth.proposals(cfg["theta0"], 20, 0.02, rng=3), reps=20)
 
     def ens(seed):
         E = affineEnsemble(ctx, L, 40, npar, seed=seed)
@@ -706,6 +709,7 @@ def mcmc_1d(ctx, cpu=True):
         S.h, 20, C.c_void_p(th.data_ptr()), npar, C.c_void_p(ll.data_ptr()),
         C.c_void_p(st.data_ptr()), C.c_void_p(sp)))
     out["half_step_ms"] = {"exact_20": exact_ms, "surrogate_20": sur_ms}
+    out["autotune"] = tuning
     if cpu:
         c = cpu_mcmc_1d()
         c["gpu_plain_ess_per_s_ratio"] = out["plain"]["ess_per_s"] / c["ess_per_s"]
