@@ -226,11 +226,13 @@ int pofd_like1_profile(pofd_like1* L, unsigned nprop, const float* theta,
                        unsigned npar, int reps, double* stage_ms,
                        int* nstages);
 const char* pofd_like1_stage_name(const pofd_like1* L, int i);
-/* Transform used by the likelihood: mode 0 (default) runs this library's own
- * FP64 four-step FFT, fused with the R-grid fill and the spectrum, when the
- * FFT size is a power of two in [4096, 131072], and cuFFT otherwise; mode 1
- * always uses cuFFT.  pofd_like1_fft_info reports whether the own FFT is in
- * use.  The reference uses FFTW (PDFactory.cc:293-338). */
+/* Transform used by the likelihood.  By default (no mode set) this
+ * library's own FP64 four-step FFT, fused with the R-grid fill and the
+ * spectrum, runs when the FFT size is a power of two in [8192, 131072] and
+ * cuFFT otherwise (at n = 4096 batched cuFFT is the faster one); mode 0
+ * runs the own FFT whenever the size is a power of two in [4096, 131072];
+ * mode 1 always uses cuFFT.  pofd_like1_fft_info reports whether the own
+ * FFT is in use.  The reference uses FFTW (PDFactory.cc:293-338). */
 int pofd_like1_set_fft(pofd_like1* L, int mode);
 int pofd_like1_fft_info(pofd_like1* L, int* own);
 

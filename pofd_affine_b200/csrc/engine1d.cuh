@@ -292,7 +292,7 @@ class Engine1 {
   void drop_graphs();
   std::map<unsigned, Plans> plans_;
   FftWorkArea fftwork_;
-  int fft_mode_ = 0;
+  int fft_mode_ = -1;  // -1 automatic (own FFT from n = 8192), 0 own, 1 cuFFT
   bool own_fft_ = false;
   int sm_count_ = 148;
   double2* d_wh_ = nullptr;  // e^{-2 pi i 128 j / m}, j < m / 128

@@ -20,6 +20,7 @@ def test_own_fft_matches_cufft(orc, gpu_ctx, n):
     L.setRRanges(cfg["theta0"])
     th = synth.proposals(cfg["theta0"], 9, 0.03, rng=n)
     th[4, -1] = 1.1
+    L.setFFT(0)  # the own FFT (by default only from n = 8192)
     assert L.ownFFT()
     lo, so = L.getLogLikeBatch(th)
     po, io = L.getPD(1, 0, th[0], setLog=False)
@@ -76,3 +77,11 @@ def test_own_fft_not_used_for_other_sizes(gpu_ctx):
         L.addDataset(0, cfg["maps"][0], 0.0025)
         L.setRRanges(cfg["theta0"])
         assert not L.ownFFT()
+    # n = 4096: cuFFT by default (the faster one there), the own FFT on request
+    L = calcLike(gpu_ctx, cfg["knotpos"], 4096, 512, True, 300)
+    L.addBeamSet(beam(cfg["beams"][0], 6.0, True, 120))
+    L.addDataset(0, cfg["maps"][0], 0.0025)
+    L.setRRanges(cfg["theta0"])
+    assert not L.ownFFT() and L.getTuning()["own_fft"] == 0
+    L.setFFT(0)
+    assert L.ownFFT() and L.getTuning()["own_fft"] == 1
