@@ -25,6 +25,14 @@ int pofd_fp64_peak(int device, double* tflops);
  * its absolute value). */
 int pofd_exp2_check(int device, int n, double lo, double hi, double* max_rel);
 
+/* The tensor-core kernels' failure path, exercised without a fault: a kernel
+ * waits with their bounded mbarrier wait (limit try_wait rounds, 1..2^20) on
+ * a barrier of arrival count 1, on which nothing arrives (arrive = 0) or one
+ * thread arrives before the wait (arrive = 1).  *timed_out = 1 when the wait
+ * ran out and the kernel returned that status normally, 0 when it
+ * completed. */
+int pofd_wait_check(int device, unsigned limit, int arrive, int* timed_out);
+
 /* A multivariate Gaussian test likelihood, log N(theta[0:k]; mean, icov^-1)
  * up to a constant (k <= 64), batched on the device with the
  * pofd_batch_loglike_fn signature (pofd_gauss_eval_batch_device; the work

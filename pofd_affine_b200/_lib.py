@@ -183,6 +183,7 @@ SIGNATURES = {
 SUPPORT_SIGNATURES = {
     "pofd_fp64_peak": (I, [I, C.POINTER(D)]),
     "pofd_exp2_check": (I, [I, I, D, D, C.POINTER(D)]),
+    "pofd_wait_check": (I, [I, U, I, C.POINTER(I)]),
     "pofd_gauss_create": (I, [I, U, _dp, _dp, PV]),
     "pofd_gauss_destroy": (I, [V]),
     "pofd_gauss_eval_batch_device": (I, [V, U, V, U, V, V, V]),

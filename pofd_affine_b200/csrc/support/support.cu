@@ -5,6 +5,8 @@
 //                      file carries HBM and BF16 figures only);
 //   * pofd_exp2_check  the table-driven exp2 of the R builders against the
 //                      CUDA library exp2;
+//   * pofd_wait_check  the tensor-core kernels' bounded mbarrier wait running
+//                      out and reporting it;
 //   * pofd_gauss_*     a multivariate Gaussian target with the batched
 //                      likelihood signature, for checking the sampler and
 //                      the surrogate on a known posterior.
@@ -17,6 +19,7 @@
 
 #include "../../../include/pofd_b200_support.h"
 #include "../common.cuh"
+#include "../umma.cuh"
 
 namespace {
 
@@ -52,6 +55,29 @@ __global__ void k_exp2_check(int n, double lo, double hi, double* __restrict__ o
   }
   worst = pofd::dev::block_max<256>(worst, sh);
   if (threadIdx.x == 0) out[blockIdx.x] = worst;
+}
+
+// The tensor-core kernels' failure path without a fault: an mbarrier
+// (arrival count 1) waited on with the kernels' bounded wait (limit
+// try_wait rounds).  With arrive = 0 nothing ever arrives on it, and the
+// timeout must come back as a status the host reads, with the kernel
+// returning normally; with arrive = 1 thread 0 arrives first and the wait
+// must succeed.  No tensor memory is allocated here.
+__global__ void k_wait_check(unsigned limit, int arrive, int* __restrict__ out) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    pofd::umma::mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (arrive)
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(pofd::umma::smem_u32(&bar))
+                   : "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !pofd::umma::mbar_wait(&bar, 0u, limit)) atomicExch(&abort_flag, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) out[0] = abort_flag;
 }
 
 constexpr unsigned kMaxDim = 64;
@@ -140,6 +166,18 @@ int pofd_exp2_check(int device, int n, double lo, double hi, double* max_rel) {
   for (double v : h) w = std::fmax(w, v);
   *max_rel = w;
   return POFD_OK;
+}
+
+int pofd_wait_check(int device, unsigned limit, int arrive, int* timed_out) {
+  if (!timed_out || limit == 0 || limit > (1u << 20) || (arrive != 0 && arrive != 1))
+    return POFD_E_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return POFD_E_CUDA;
+  int* d = nullptr;
+  if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return POFD_E_NOMEM;
+  k_wait_check<<<1, 32>>>(limit, arrive, d);
+  const cudaError_t e = cudaMemcpy(timed_out, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? POFD_OK : POFD_E_CUDA;
 }
 
 int pofd_gauss_create(int device, unsigned k, const double* mean, const double* icov,

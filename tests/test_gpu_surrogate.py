@@ -31,6 +31,34 @@ def test_bf16_gemm_matches_float64(gpu_ctx, M, N, K):
     assert err < 1e-5, err
 
 
+def test_bounded_wait_times_out_with_a_status(gpu_ctx):
+    """The tensor-core kernels' mbarrier wait is bounded: on a barrier that
+    nothing arrives on it runs out and the kernel reports that as a status
+    the host reads (no trap, no fault); with one arrival it completes.  The
+    context stays usable afterwards: a tcgen05 GEMM still matches."""
+    import ctypes as C
+    import torch
+    from pofd_affine_b200._lib import support_lib
+    from pofd_affine_b200.surrogate import bf16_gemm
+    out = C.c_int(-1)
+    for limit in (1, 64, 4096):
+        assert support_lib().pofd_wait_check(0, limit, 0, C.byref(out)) == 0
+        assert out.value == 1, limit
+        assert support_lib().pofd_wait_check(0, limit, 1, C.byref(out)) == 0
+        assert out.value == 0, limit
+    assert support_lib().pofd_wait_check(0, 0, 0, C.byref(out)) != 0
+    assert support_lib().pofd_wait_check(0, (1 << 20) + 1, 0, C.byref(out)) != 0
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(5)
+    a = rng.normal(size=(128, 64)).astype(np.float32)
+    b = rng.normal(size=(64, 64)).astype(np.float32)
+    A = torch.from_numpy(a).cuda().to(torch.bfloat16).contiguous()
+    B = torch.from_numpy(b).cuda().to(torch.bfloat16).contiguous()
+    ref = _bf16_round(a) @ _bf16_round(b).T
+    err = np.max(np.abs(bf16_gemm(A, B).cpu().numpy() - ref)) / np.max(np.abs(ref))
+    assert err < 1e-5, err
+
+
 def _gauss_pairs(n, k, seed):
     rng = np.random.default_rng(seed)
     A = rng.normal(size=(k, k))
