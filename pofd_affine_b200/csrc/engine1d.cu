@@ -861,10 +861,13 @@ k_fftB(int m1, int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
        const int* __restrict__ kcut) {
   extern __shared__ double2 fs[];  // [(k1 * 16 + n2) * 17 + r], then T
   double2* Ts = fs + 16 * 16 * 17;  // inter-stage twiddles W_256^{n2 k1} (symmetric)
-  const int row = blockIdx.y;
+  // blocks take the rows last-written-first: the tail of pass A's output is
+  // still in L2 when this pass starts (and the P(D) scan after the inverse,
+  // in natural order, then starts on this pass's last-written rows)
+  const int row = gridDim.y - 1 - blockIdx.y;
   if (mstatus[row / nrows_per_w] != 0) return;
   const int rb = min(FRB, m1);
-  const int c0 = blockIdx.x * rb;
+  const int c0 = (gridDim.x - 1 - blockIdx.x) * rb;
   const int m = m1 * 256;
   const int t = threadIdx.x;
   const double2* src = in + static_cast<size_t>(row) * rowsz;
