@@ -182,9 +182,11 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
   const bool negb = !posb && (bs.hasneg && f < 0 && f >= bs.rr_lo);
   if (posb || negb) {
     // the knot interval and the range test of every term at this node come
-    // from the host-built table (the reference searches them per call)
+    // from the host-built table (the reference searches them per call);
+    // terms outside the node's first-to-last in-range span are not visited
     const unsigned char* __restrict__ kt = sd.kidx + i;
-    for (int j = 0; j < nt; ++j) {
+    const int2 jr = sd.jrange[i];
+    for (int j = jr.x; j < jr.y; ++j) {
       const int k = kt[static_cast<size_t>(j) * NI];
       if (k == 255) continue;
       const double delx = (lf + s_le[j]) - s_lk[k];
@@ -1957,6 +1959,24 @@ void Engine1::build_static() {
         static_allocs_.push_back(d);
         cuda_check(cudaMemcpy(d, kt.data(), kt.size(), cudaMemcpyHostToDevice), "upload");
         sd.kidx = d;
+        // per node, the first and one past the last term inside the knot
+        // range: the only terms the node's sum visits
+        std::vector<int2> jr(NI, make_int2(0, 0));
+        for (unsigned i = 0; i < NI; ++i) {
+          int lo = -1, hi = -1;
+          for (size_t j = 0; j < nt; ++j)
+            if (kt[j * NI + i] != 255) {
+              if (lo < 0) lo = static_cast<int>(j);
+              hi = static_cast<int>(j) + 1;
+            }
+          if (lo >= 0) jr[i] = make_int2(lo, hi);
+        }
+        int2* dj = nullptr;
+        cuda_check(cudaMalloc(&dj, jr.size() * sizeof(int2) + 16), "cudaMalloc");
+        static_allocs_.push_back(dj);
+        cuda_check(cudaMemcpy(dj, jr.data(), jr.size() * sizeof(int2), cudaMemcpyHostToDevice),
+                   "upload");
+        sd.jrange = dj;
       }
       sd.nodes = 1;
       sd.nterms = static_cast<int>(tie.size());

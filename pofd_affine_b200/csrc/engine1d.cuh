@@ -37,6 +37,8 @@ struct Side1Dev {
   const double* lie;    // log2 of the inverse beam terms
   const unsigned char* kidx;  // [nterms][ninterp] knot interval of term j at
                               // node i (255: outside the knot range)
+  const int2* jrange;         // [ninterp] first and one past the last term
+                              // inside the knot range at node i
   int grid_lo, grid_hi; // inclusive grid index range filled from this side
   double grid_off;      // grid flux = i*dflux + grid_off
 };
