@@ -725,7 +725,7 @@ k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
 // k_moments1 has read it.
 
 template <int L1, int L2, bool RUNS>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, RUNS ? 3 : 2)
 k_fftAR(const BSet1Dev* __restrict__ bsets, int B, int NI, int rowsz,
         const int* __restrict__ mstatus, const double* __restrict__ spl,
         double* __restrict__ rbuf, double* __restrict__ rpart,
@@ -1517,10 +1517,16 @@ T* dalloc(size_t n) {
 
 namespace {
 // exchange (256 L1 entries) plus the twiddle tables: H has m / 128 = 2 m1
-// entries, L 128, the inter-stage table 256
+// entries, L 128, the inter-stage table L1 L2 = m1; and at least the padded
+// staging area of the run-based fill, which spans the exchange buffer and
+// the tables (512 L1 values, one pad word per 16: 544 L1 doubles).  73.7 KB
+// at m1 = 128: three blocks per SM fit.
 constexpr size_t kFftASmemMax = (256 * 16 + 2 * 256 + 128 + 256) * sizeof(double2);
 inline size_t fftA_smem(int m1) {
-  return (256 * static_cast<size_t>(m1 < 16 ? m1 : 16) + 2 * m1 + 128 + 256) * sizeof(double2);
+  const size_t l1 = static_cast<size_t>(m1 < 16 ? m1 : 16);
+  const size_t tables = (256 * l1 + 2 * static_cast<size_t>(m1) + 128 + m1) * sizeof(double2);
+  const size_t staging = 544 * l1 * sizeof(double);
+  return tables > staging ? tables : staging;
 }
 
 template <int S>
@@ -1570,6 +1576,14 @@ int launch_fftAR(int m1, bool runs, int rows, cudaStream_t st, const BSet1Dev* b
 template <bool RUNS>
 void fftAR_attr_runs() {
   const int sm = static_cast<int>(kFftASmemMax);
+  // the run-based fill fits three blocks per SM (80 registers, 73.7 KB of
+  // dynamic shared memory at m1 = 128) when the carve-out is all shared
+  if (RUNS) {
+    const int c = cudaSharedmemCarveoutMaxShared;
+    cuda_check(cudaFuncSetAttribute(k_fftAR<16, 8, RUNS>, cudaFuncAttributePreferredSharedMemoryCarveout, c), "attr");
+    cuda_check(cudaFuncSetAttribute(k_fftAR<16, 4, RUNS>, cudaFuncAttributePreferredSharedMemoryCarveout, c), "attr");
+    cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2, RUNS>, cudaFuncAttributePreferredSharedMemoryCarveout, c), "attr");
+  }
   cuda_check(cudaFuncSetAttribute(k_fftAR<8, 1, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
   cuda_check(cudaFuncSetAttribute(k_fftAR<16, 1, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
   cuda_check(cudaFuncSetAttribute(k_fftAR<16, 2, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
