@@ -647,7 +647,7 @@ constexpr int FRB = 16;   // rows per pass-B block
 // Y[c][b].  Input rows are complex: for the forward transform the R grid
 // itself, whose real values R_{2j}, R_{2j+1} are z_j.
 template <int L1, int L2, int S>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, 3)
 k_fftA(int rowsz, int nrows_per_w, const int* __restrict__ mstatus,
        const double2* __restrict__ in, double2* __restrict__ out,
        const double2* __restrict__ WH, const double2* __restrict__ WL,
@@ -1600,6 +1600,12 @@ void fftAR_attr() {
 template <int S>
 void fftA_attr() {
   const int sm = static_cast<int>(kFftASmemMax);
+  {
+    const int c = cudaSharedmemCarveoutMaxShared;
+    cuda_check(cudaFuncSetAttribute(k_fftA<16, 8, S>, cudaFuncAttributePreferredSharedMemoryCarveout, c), "attr");
+    cuda_check(cudaFuncSetAttribute(k_fftA<16, 4, S>, cudaFuncAttributePreferredSharedMemoryCarveout, c), "attr");
+    cuda_check(cudaFuncSetAttribute(k_fftA<16, 2, S>, cudaFuncAttributePreferredSharedMemoryCarveout, c), "attr");
+  }
   cuda_check(cudaFuncSetAttribute(k_fftA<8, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
   cuda_check(cudaFuncSetAttribute(k_fftA<16, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
   cuda_check(cudaFuncSetAttribute(k_fftA<16, 2, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm), "attr");
