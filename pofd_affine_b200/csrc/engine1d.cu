@@ -204,7 +204,7 @@ __global__ void k_rnodes1(const BSet1Dev* __restrict__ bsets, Model1Dev m,
 // precomputed LDL^T factors as two block-wide affine-map scans, then the
 // per-interval (y, b, c, d) (PDFactory.cc:466-474, 522).
 template <int RT>
-__global__ void __launch_bounds__(RT)
+__global__ void __launch_bounds__(RT, 2048 / RT)
 k_rspline1(const BSet1Dev* __restrict__ bsets, int B, int NI,
            const int* __restrict__ mstatus, const double* __restrict__ nodes,
            double* __restrict__ spl) {
@@ -937,7 +937,7 @@ __device__ __forceinline__ double2 spec_p(double2 X, double r0, int k, int m, bo
   return p;
 }
 
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
 k_spectrum1f(const BSet1Dev* __restrict__ bsets, const DSet1Dev* __restrict__ dsets, int B,
              int D, int n, int rowsz, const int* __restrict__ mstatus,
              const double* __restrict__ sigmult, const double* __restrict__ mom,
