@@ -392,7 +392,7 @@ k_rgrid2(const BSet2Dev* __restrict__ bsets, int B, int n, int nc2,
 // columns).
 constexpr int ER_MIN = 4;    // fewest edge rows per group (sizes the partials)
 template <int ER>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
 k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
          const int* __restrict__ mstatus, const double* __restrict__ rw,
          const int2* __restrict__ rcnt, double* __restrict__ epart) {
@@ -472,7 +472,7 @@ k_redge2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
 // reduction gives the row's sum.
 constexpr int RY_ROWS = NT / 32;
 constexpr int RY_CPL = 8;  // edge columns per lane held at once
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
 k_ry2(const BSet2Dev* __restrict__ bsets, int B, int n, int nedge,
       const int* __restrict__ mstatus, const double* __restrict__ rw,
       const int2* __restrict__ rcnt, double* __restrict__ redge) {
