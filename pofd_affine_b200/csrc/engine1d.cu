@@ -1022,6 +1022,8 @@ struct SplitParams {
   long long botidx, topidx;
 };
 
+constexpr int kSearchPer = 8;  // values per thread per window of the split search
+
 __device__ __forceinline__ long long to_index(double v) {
   // (int) conversion of the reference, saturated so that huge values stay
   // out of range instead of wrapping.
@@ -1256,13 +1258,25 @@ k_pfinish1(const BSet1Dev* __restrict__ bsets,
   __syncthreads();
   int state = s_state;
   if (state == 0) {
-    // search down from topidx-1 for the first value below the jitter level
+    // search down from topidx-1 for the first value below the jitter level:
+    // windows of kSearchPer * NT values from the top, each thread's loads
+    // issued together; the highest hit of the first window with one is the
+    // first hit of the element-by-element search
     const double jitter = s_jitter;
     int found = -1;
-    for (long long top = sp.topidx - 1; top >= sp.botidx; top -= NT) {
-      const long long i = top - threadIdx.x;
+    for (long long top = sp.topidx - 1; top >= sp.botidx; top -= NT * kSearchPer) {
+      double pv[kSearchPer];
+#pragma unroll
+      for (int k = 0; k < kSearchPer; ++k) {
+        const long long i = top - threadIdx.x - static_cast<long long>(NT) * k;
+        pv[k] = (i >= sp.botidx) ? p[i] : 1.0e308;
+      }
       int hit = -1;
-      if (i >= sp.botidx && clip0(p[i]) < jitter) hit = static_cast<int>(i);
+#pragma unroll
+      for (int k = kSearchPer - 1; k >= 0; --k) {
+        const long long i = top - threadIdx.x - static_cast<long long>(NT) * k;
+        if (i >= sp.botidx && clip0(pv[k]) < jitter) hit = static_cast<int>(i);
+      }
       const int m = dev::block_max_int<NT>(hit, shi);
       if (m >= 0) { found = m; break; }
     }
