@@ -1,6 +1,6 @@
 """1D CUDA path against the oracle, through the C ABI.
 
-Tolerances (the north-star parity bar): R and the P(D) within 1e-10
+Tolerances (the parity bar of this path): R and the P(D) within 1e-10
 relative to their maxima (in practice ~1e-13), log-likelihood within 1e-6
 absolute.  Split indices must agree exactly (they do unless a P(D) value sits
 within rounding of the jitter threshold).
